@@ -1,0 +1,195 @@
+"""ctypes mirror of include/nrgpu.h and the loader of the CUDA library.
+
+The library is the product: ``baum_b200/libnrgpu.so`` built from
+``baum_b200/csrc`` for sm_100a.  There is no fallback; :func:`lib` raises if
+the library is missing or cannot be loaded.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libnrgpu.so")
+NVARS = 24
+
+# BSSN evolve-list order (reference bssn.c:315-322)
+BSSN_VARS = ["g11", "g12", "g13", "g22", "g23", "g33", "chi", "A11", "A12", "A13", "A22", "A23",
+             "A33", "K", "G1", "G2", "G3", "alpha", "beta1", "beta2", "beta3", "B1", "B2", "B3"]
+# the same list under the reference's variable names (bam_bssn.c, bam_adm.c)
+BSSN_BAM_NAMES = ["bssn_gxx", "bssn_gxy", "bssn_gxz", "bssn_gyy", "bssn_gyz", "bssn_gzz",
+                  "bssn_chi", "bssn_Axx", "bssn_Axy", "bssn_Axz", "bssn_Ayy", "bssn_Ayz",
+                  "bssn_Azz", "bssn_K", "bssn_Gx", "bssn_Gy", "bssn_Gz", "alpha", "betax",
+                  "betay", "betaz", "betadotx", "betadoty", "betadotz"]
+
+NRGPU_OK = 0
+ERRORS = {-1: "bad argument", -2: "CUDA error", -3: "NaN/Inf in rhs", -4: "out of device memory",
+          -5: "unsupported", -6: "device wait timed out"}
+PHYBOUND = 1
+
+
+class Box(C.Structure):
+    _fields_ = [("m", C.c_int), ("n", C.c_int), ("o", C.c_int), ("noffset", C.c_int),
+                ("x0", C.c_double), ("y0", C.c_double), ("z0", C.c_double)]
+
+
+class LevelDesc(C.Structure):
+    _fields_ = [("nboxes", C.c_int), ("box", C.POINTER(Box)), ("npoints", C.c_int),
+                ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
+                ("boundary", C.POINTER(C.c_int))]
+
+
+class BssnParams(C.Structure):
+    _fields_ = [("order_centered", C.c_int), ("order_advection", C.c_int),
+                ("advection_lopsided", C.c_int), ("advection_lopsided6", C.c_int),
+                ("order_dissipation", C.c_int), ("dissfactor", C.c_double),
+                ("forceKzerofactor", C.c_double), ("subtractA", C.c_int),
+                ("normalizedetg", C.c_int), ("oploglapse", C.c_int), ("oploglapse2", C.c_int),
+                ("oplogwithshift", C.c_int), ("harmoniclapse", C.c_int),
+                ("gamma0factor", C.c_double), ("gamma2factor", C.c_double),
+                ("withGadv", C.c_double), ("withShiftadv", C.c_double),
+                ("withBadv", C.c_double), ("withB", C.c_double),
+                ("lapseharmonicf", C.c_double), ("shiftalphapower", C.c_double),
+                ("shiftgammacoeff", C.c_double), ("shiftGalphapower", C.c_double),
+                ("shiftdriver", C.c_double), ("chiDivFloor", C.c_double),
+                ("chipsipower", C.c_double), ("bc_var0", C.c_double * NVARS),
+                ("bc_speed", C.c_double * NVARS)]
+
+
+def bssn_params(**over):
+    """Parameters of the single-puncture BSSN workload: 1+log withshift,
+    gamma0 withGadv withBadv withShiftadv, shiftdriver 2, 4th-order centred
+    and lopsided advection, KO6 with dissipation_factor 0.1 (dissfactor =
+    0.1/2^6, evolve.c:503), radiative boundary speeds from bssn.c:288-311."""
+    p = BssnParams()
+    p.order_centered = 4
+    p.order_advection = 4
+    p.advection_lopsided = 1
+    p.advection_lopsided6 = 2
+    p.order_dissipation = 6
+    p.dissfactor = 0.1 / 2.0 ** 6
+    p.forceKzerofactor = 1.0  # Getv("bssn_forceKzero","no") is 1 for the default "no"
+    p.subtractA = 1
+    p.normalizedetg = 1
+    p.oploglapse, p.oploglapse2, p.oplogwithshift, p.harmoniclapse = 1, 0, 1, 0
+    p.gamma0factor, p.gamma2factor = 1.0, 0.0
+    p.withGadv = p.withShiftadv = p.withBadv = p.withB = 1.0
+    p.lapseharmonicf = 2.0
+    p.shiftalphapower = 0.0
+    p.shiftgammacoeff = 0.75
+    p.shiftGalphapower = 0.0
+    p.shiftdriver = 2.0
+    p.chiDivFloor = -1000.0
+    p.chipsipower = -4.0
+    for k, v in over.items():
+        setattr(p, k, v)
+    set_bc_from_gauge(p)
+    return p
+
+
+def set_bc_from_gauge(p):
+    """Far limits and speeds of VarNameSetBoundaryInfo (bssn.c:269-311)."""
+    if p.oploglapse:
+        vg = p.lapseharmonicf ** 0.5
+    elif p.oploglapse2:
+        vg = (4.0 / 3.0) ** 0.5
+    else:
+        vg = 1.0
+    var0 = [0.0] * NVARS
+    speed = [1.0] * NVARS
+    for i in (0, 3, 5, 6, 17):   # gxx gyy gzz chi alpha -> far limit 1
+        var0[i] = 1.0
+    for i in (13, 6, 17):        # K chi alpha travel at the gauge speed
+        speed[i] = vg
+    p.bc_var0[:] = var0
+    p.bc_speed[:] = speed
+
+
+class Level:
+    """Host-side description of a level (keeps the ctypes arrays alive)."""
+
+    def __init__(self, boxes, dx, boundary, dy=None, dz=None):
+        import numpy as np
+        self.boxes = (Box * len(boxes))()
+        off = 0
+        for i, b in enumerate(boxes):
+            m, n, o, x0, y0, z0 = b
+            self.boxes[i] = Box(m, n, o, off, x0, y0, z0)
+            off += m * n * o
+        self.npoints = off
+        self.boundary = np.ascontiguousarray(boundary, dtype=np.int32)
+        assert self.boundary.size == off
+        self.desc = LevelDesc(len(boxes), self.boxes, off, dx, dy or dx, dz or dx,
+                              self.boundary.ctypes.data_as(C.POINTER(C.c_int)))
+        self.dx = dx
+
+    @staticmethod
+    def single_box(n, dx):
+        """A cubic single box of n^3 points, centred (grid.c:84-105), with
+        the outer layer flagged PHYBOUND (flag.c:23-36)."""
+        import numpy as np
+        x0 = -(n - 1) * dx / 2
+        b = np.zeros((n, n, n), dtype=np.int32)
+        b[0, :, :] = b[-1, :, :] = b[:, 0, :] = b[:, -1, :] = b[:, :, 0] = b[:, :, -1] = PHYBOUND
+        return Level([(n, n, n, x0, x0, x0)], dx, b.ravel())
+
+    def coords(self):
+        import numpy as np
+        xs, ys, zs = [], [], []
+        for b in self.boxes:
+            i = np.arange(b.m)
+            j = np.arange(b.n)
+            k = np.arange(b.o)
+            z, y, x = np.meshgrid(b.z0 + k * self.desc.dz, b.y0 + j * self.desc.dy,
+                                  b.x0 + i * self.desc.dx, indexing="ij")
+            xs.append(x.ravel()); ys.append(y.ravel()); zs.append(z.ravel())
+        return np.concatenate(xs), np.concatenate(ys), np.concatenate(zs)
+
+
+def ptr_array(ptrs):
+    arr = (C.c_void_p * len(ptrs))()
+    for i, p in enumerate(ptrs):
+        arr[i] = p
+    return arr
+
+
+_lib = None
+
+
+def lib():
+    """Load libnrgpu.so; raise if it is absent (no fallback exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBPATH):
+        raise RuntimeError("libnrgpu.so not built: run python -c 'import __graft_entry__ as g; g.build()'")
+    L = C.CDLL(LIBPATH)
+    vp = C.c_void_p
+    pp = C.POINTER(C.c_void_p)
+    sig = {
+        "nrgpu_abi_version": (C.c_int, []),
+        "nrgpu_last_error": (C.c_char_p, []),
+        "nrgpu_init": (C.c_int, [C.c_int]),
+        "nrgpu_bssn_params_default": (None, [C.POINTER(BssnParams)]),
+        "nrgpu_level_create": (C.c_int, [C.POINTER(LevelDesc), C.POINTER(vp)]),
+        "nrgpu_level_destroy": (C.c_int, [vp]),
+        "nrgpu_bssn_rhs": (C.c_int, [vp, pp, pp, C.c_double, pp, C.POINTER(BssnParams), vp]),
+        "nrgpu_bssn_boundary": (C.c_int, [vp, pp, pp, C.c_double, pp, C.POINTER(BssnParams), vp]),
+        "nrgpu_bssn_algcon": (C.c_int, [vp, pp, C.POINTER(BssnParams), vp]),
+        "nrgpu_vladd": (C.c_int, [vp, C.c_int, pp, C.c_double, pp, C.c_double, pp, vp]),
+        "nrgpu_bssn_rk4_step": (C.c_int, [vp, pp, C.c_double, C.POINTER(BssnParams), vp]),
+        "nrgpu_bssn_evolve_host": (C.c_int, [vp, pp, C.c_int, C.c_double, C.POINTER(BssnParams)]),
+        "nrgpu_level_nan_flag": (C.c_int, [vp, C.POINTER(C.c_int)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def check(status):
+    if status != NRGPU_OK:
+        msg = lib().nrgpu_last_error()
+        raise RuntimeError("nrgpu error %d (%s): %s" % (status, ERRORS.get(status, "?"),
+                                                        msg.decode() if msg else ""))
+    return status

@@ -1,0 +1,170 @@
+/* nrgpu.h -- C ABI of the B200 (sm_100a) hot path of BAM's Einstein
+ * evolution: the BSSN right-hand side over tVarList boxes, its radiative
+ * boundary, the RK4 substep update and the algebraic constraints.
+ *
+ * Everything here is plain C: pointers, sizes and POD structs.  A BAM
+ * project module (baum_b200/bam/nrgpu_bam.c) binds these entry points to the
+ * reference's callback registry; Python tests bind them with ctypes.
+ *
+ * Data contract (mirrors the reference's storage, bam_amr.h:10-131 and
+ * bam_amr_loops_box.h:54-68): one FP64 array per variable per level, all
+ * boxes of the level concatenated at box->noffset, x fastest inside a box
+ * (di = 1, dj = m, dk = m*n).  Variable lists are arrays of pointers in the
+ * reference's evolve-list order, e.g. for BSSN (bssn.c:315-322):
+ *   g11 g12 g13 g22 g23 g33 chi A11 A12 A13 A22 A23 A33 K G1 G2 G3
+ *   alpha beta1 beta2 beta3 B1 B2 B3                      (24 variables)
+ * "Device" pointers are CUDA global memory on the level's device; "host"
+ * pointers are ordinary (preferably pinned) host memory.
+ *
+ * Errors: every entry point returns an int status (NRGPU_OK = 0, negative on
+ * error) and never aborts; nrgpu_last_error() gives the message.  The BAM
+ * binding turns a negative status into errorexit(), which is what the
+ * reference does on failure (bam_main.h:112-117).
+ */
+#ifndef NRGPU_H
+#define NRGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NRGPU_ABI_VERSION 1
+
+enum {
+  NRGPU_OK = 0,
+  NRGPU_ERR_ARG = -1,         /* bad argument (null pointer, size, order) */
+  NRGPU_ERR_CUDA = -2,        /* a CUDA runtime call failed */
+  NRGPU_ERR_NAN = -3,         /* a NaN/Inf appeared in a right-hand side */
+  NRGPU_ERR_NOMEM = -4,       /* device allocation failed */
+  NRGPU_ERR_UNSUPPORTED = -5, /* feature outside the implemented set */
+  NRGPU_ERR_TIMEOUT = -6      /* a bounded device wait gave up */
+};
+
+/* boundary flag values (bam_amr.h:117-126) */
+enum {
+  NRGPU_REFBOUND = -1, NRGPU_NOTBOUND = 0, NRGPU_PHYBOUND = 1, NRGPU_GHOBOUND = 2,
+  NRGPU_SYMBOUND = 3
+};
+
+#define NRGPU_BSSN_NVARS 24
+
+/* one box of a level (tB, bam_amr.h:10-30) */
+typedef struct {
+  int m, n, o;        /* points per direction, outer boundary layer included */
+  int noffset;        /* offset of point (0,0,0) in the level arrays */
+  double x0, y0, z0;  /* coordinates of point (0,0,0) */
+} nrgpu_box;
+
+/* a level (tL, bam_amr.h:46-74): geometry plus the boundary flag of every
+ * point.  The flags are copied; the caller keeps ownership of its arrays. */
+typedef struct {
+  int nboxes;
+  const nrgpu_box *box;
+  int npoints;            /* sum over boxes of m*n*o */
+  double dx, dy, dz;
+  const int *boundary;    /* host array [npoints], tL.boundary */
+} nrgpu_level_desc;
+
+typedef struct nrgpu_level nrgpu_level;  /* opaque device mirror of a level */
+
+/* Parameters that bssn_rhs_movpunc_N reads from the parameter database at
+ * every call (bssn_rhs_movpunc_N.c:107-145).  The 0/1 "factors" are the
+ * values of the reference's Getv() token tests, as doubles where the
+ * reference multiplies with them. */
+typedef struct {
+  int order_centered;       /* 2, 4 or 6 */
+  int order_advection;      /* 2, 4 or 6 */
+  int advection_lopsided;   /* 4th-order stencil shift, bam_amr.c:50-57 */
+  int advection_lopsided6;  /* 6th-order stencil shift */
+  int order_dissipation;    /* 0 (off), 4 or 6 */
+  double dissfactor;        /* get_dissipation_factor(level), evolve.c:489 */
+  double forceKzerofactor;  /* Getv("bssn_forceKzero","no") */
+  int subtractA;            /* Getv("bssn_subtractA","yes") */
+  int normalizedetg;        /* Getv("bssn_normalizedetg","yes") */
+  int oploglapse, oploglapse2, oplogwithshift, harmoniclapse;
+  double gamma0factor, gamma2factor, withGadv, withShiftadv, withBadv, withB;
+  double lapseharmonicf, shiftalphapower, shiftgammacoeff, shiftGalphapower,
+         shiftdriver;
+  double chiDivFloor, chipsipower;
+  /* radiative boundary (set_boundary_rot_rad, radiative.c:105) per variable:
+   * far limit var0 and propagation speed v, VarNameSetBoundaryInfo
+   * (bssn.c:288-311) */
+  double bc_var0[NRGPU_BSSN_NVARS];
+  double bc_speed[NRGPU_BSSN_NVARS];
+} nrgpu_bssn_params;
+
+/* ---- library ---------------------------------------------------------- */
+
+int nrgpu_abi_version(void);
+const char *nrgpu_last_error(void);
+/* select and initialise the CUDA device used by later calls */
+int nrgpu_init(int device);
+
+/* Fill p with the values a BAM parfile of the C1 kind produces; the caller
+ * overrides fields.  Pure host code, usable without a GPU. */
+void nrgpu_bssn_params_default(nrgpu_bssn_params *p);
+
+/* ---- levels ----------------------------------------------------------- */
+
+/* Device mirror of a level: geometry, flags and per-point masks; allocates
+ * RK4 scratch lazily.  Replaces nothing in the reference (BAM keeps levels
+ * in host memory only). */
+int nrgpu_level_create(const nrgpu_level_desc *desc, nrgpu_level **out);
+int nrgpu_level_destroy(nrgpu_level *lev);
+
+/* ---- the hot path (device pointers) ------------------------------------- */
+
+/* BSSN right-hand side on the inner points (boundary flag 0).
+ * Replaces bssn_rhs_movpunc_N(unew, upre, c, ucur)
+ * (bssn_rhs_movpunc_N.c:27, registered as "geometry", bssn.c:17,325).
+ * c == 0: unew = rhs(ucur).  c != 0: unew = upre + c*rhs(ucur) followed by
+ * the trace/determinant fixes of the reference (:15151-15380).
+ * unew, upre, ucur: 24 device pointers each.  stream: a cudaStream_t or 0. */
+int nrgpu_bssn_rhs(nrgpu_level *lev, double *const *unew, double *const *upre,
+                   double c, double *const *ucur, const nrgpu_bssn_params *p,
+                   void *stream);
+
+/* Radiative boundary on the physical boundary points (flag PHYBOUND).
+ * Replaces set_boundary(unew, upre, c, ucur) (boundary.c:25) for
+ * boundary = radiative without rotation terms, i.e.
+ * set_boundary_rot_rad (radiative.c:105) with rot = 0 for every variable. */
+int nrgpu_bssn_boundary(nrgpu_level *lev, double *const *unew, double *const *upre,
+                        double c, double *const *ucur, const nrgpu_bssn_params *p,
+                        void *stream);
+
+/* det(g) = 1 and tr(A) = 0 on all points.  Replaces bssn_algcon
+ * (bssn_algcon.c:25) via bssn_algcon_wrapper (bssn.c:86). u: the 24-var list. */
+int nrgpu_bssn_algcon(nrgpu_level *lev, double *const *u, const nrgpu_bssn_params *p,
+                      void *stream);
+
+/* r = a*x + b*y over all points of n variables.  Replaces vladd
+ * (variables.c:650); with r == x and a == 1 it is vladdto (variables.c:721). */
+int nrgpu_vladd(nrgpu_level *lev, int nvars, double *const *r, double a,
+                double *const *x, double b, double *const *y, void *stream);
+
+/* One full RK4 step of the level in place: evolve_rk_rk4 (rk.c:220) with
+ * evolve_rhs (evolve.c:37) = RHS + radiative boundary in each stage, then the
+ * algebraic constraints (bssn_algcon_wrapper, bssn.c:86).  The four stages
+ * are fused kernels that also do the vladd/vladdto updates.  u: 24 device
+ * pointers.  Uses scratch owned by the level (allocated on first call). */
+int nrgpu_bssn_rk4_step(nrgpu_level *lev, double *const *u, double dt,
+                        const nrgpu_bssn_params *p, void *stream);
+
+/* nsteps RK4 steps starting from and returning to HOST arrays: uploads
+ * host_u (24 host pointers), steps on the device, downloads the result into
+ * host_u.  The end-to-end call of a host code that keeps its state in host
+ * memory. */
+int nrgpu_bssn_evolve_host(nrgpu_level *lev, double *const *host_u, int nsteps,
+                           double dt, const nrgpu_bssn_params *p);
+
+/* Device NaN/Inf flag of the level: set by the RHS kernels when any rhs is
+ * not finite (the reference prints per point, check.c:235).  Reads and
+ * clears it; *flag = 1 if set. */
+int nrgpu_level_nan_flag(nrgpu_level *lev, int *flag);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NRGPU_H */

@@ -1,0 +1,182 @@
+/* nrharness.c -- a BAM project compiled only into the oracle binary
+ * oracle/_ref/bam.  Test infrastructure, never product code.
+ *
+ * It does three things to make the reference's own CPU evolution and
+ * multigrid comparable with the GPU path, bit for bit in layout:
+ *   1. nrharness_data = fourier: after the evolution system's startup
+ *      (POST_INITIALDATA, bssn.c:260 / z4.c:176 run before this module),
+ *      overwrite every evolved variable with a flat background plus a sum of
+ *      seeded Fourier modes (the synthetic data of the batched FMR workload).
+ *      The generator (splitmix64 draws, mode layout) is restated in
+ *      baum_b200/synthetic.py so the GPU side can rebuild the same state.
+ *   2. nrharness_rhs = yes: evaluate the registered RHS once on the initial
+ *      state through the reference's evolve_rhs (evolve.c:37), including the
+ *      boundary callback, and dump it.
+ *   3. nrharness_dump = "i0 i1 ...": dump the evolved variables of every
+ *      level after those level iterations (POST_EVOLVE), and after the
+ *      initial data when 0 is listed.
+ * Dump format (little endian), one file per (tag, level):
+ *   int64 magic 0x3147524e ("NRG1"), l, nboxes, nvars, npoints, iteration
+ *   double time, dx, dy, dz, dt
+ *   per box: int64 m, n, o, noffset; double x0, y0, z0
+ *   per var: char name[32]
+ *   int32 boundary[npoints]
+ *   double data[nvars][npoints]
+ */
+#include "bam.h"
+#include "bam_nrharness.h"
+
+static unsigned long long sm_state;
+static unsigned long long splitmix64(void)
+{
+  unsigned long long z = (sm_state += 0x9E3779B97F4A7C15ULL);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+static double uniform01(void) { return (splitmix64() >> 11) * (1.0 / 9007199254740992.0); }
+
+static int is_unit_background(const char *name)
+{
+  const char *unit[] = {"bssn_gxx", "bssn_gyy", "bssn_gzz", "bssn_chi",
+                        "z4_gxx", "z4_gyy", "z4_gzz", "z4_chi", "alpha", 0};
+  int i;
+  for (i = 0; unit[i]; i++) if (!strcmp(name, unit[i])) return 1;
+  return 0;
+}
+
+static void dump_varlist(tL *level, tVarList *vl, const char *tag)
+{
+  char fn[1024];
+  FILE *f;
+  long long hdr[6];
+  double dh[5];
+  int b, v;
+  snprintf(fn, sizeof fn, "%s/%s_l%d.bin", Gets("nrharness_dir"), tag, level->l);
+  f = fopen(fn, "wb");
+  if (!f) errorexits("nrharness: cannot open %s", fn);
+  hdr[0] = 0x3147524e; hdr[1] = level->l; hdr[2] = level->nboxes; hdr[3] = vl->n;
+  hdr[4] = level->npoints; hdr[5] = level->iteration;  /* before the step */
+  fwrite(hdr, sizeof(long long), 6, f);
+  dh[0] = level->time; dh[1] = level->dx; dh[2] = level->dy; dh[3] = level->dz; dh[4] = level->dt;
+  fwrite(dh, sizeof(double), 5, f);
+  for (b = 0; b < level->nboxes; b++) {
+    tB *box = level->box[b];
+    long long bi[4] = {box->m, box->n, box->o, box->noffset};
+    double bx[3] = {box->x0, box->y0, box->z0};
+    fwrite(bi, sizeof(long long), 4, f);
+    fwrite(bx, sizeof(double), 3, f);
+  }
+  for (v = 0; v < vl->n; v++) {
+    char name[32];
+    memset(name, 0, sizeof name);
+    strncpy(name, VarName(vl->index[v]), 31);
+    fwrite(name, 1, 32, f);
+  }
+  fwrite(level->boundary, sizeof(int), level->npoints, f);
+  for (v = 0; v < vl->n; v++) {
+    double *p = level->v[vl->index[v]];
+    if (!p) errorexits("nrharness: variable %s not enabled", VarName(vl->index[v]));
+    fwrite(p, sizeof(double), level->npoints, f);
+  }
+  fclose(f);
+  printf("nrharness: wrote %s\n", fn);
+}
+
+static int dump_requested(int iteration)
+{
+  char s[32];
+  snprintf(s, sizeof s, "%d", iteration);
+  return Getv("nrharness_dump", s);
+}
+
+static void set_fourier(tL *level, tVarList *u)
+{
+  const int nmodes = Geti("nrharness_nmodes");
+  const double amp = Getd("nrharness_amp");
+  const double L = Getd("nrharness_length");
+  double k[64][3], cf, ph;
+  double *x = level->v[Ind("x")], *y = level->v[Ind("y")], *z = level->v[Ind("z")];
+  int m, v, i;
+  if (nmodes > 64) errorexit("nrharness: at most 64 modes");
+  sm_state = (unsigned long long)Geti("nrharness_seed");
+  for (m = 0; m < nmodes; m++)
+    for (i = 0; i < 3; i++) {
+      /* integer wave numbers in [-2, 2] per axis on the box length L */
+      int n = (int)(splitmix64() % 5ULL) - 2;
+      k[m][i] = 2.0 * PI * n / L;
+    }
+  for (v = 0; v < u->n; v++) {
+    double *p = level->v[u->index[v]];
+    double base = is_unit_background(VarName(u->index[v])) ? 1.0 : 0.0;
+    double c[64], phase[64];
+    for (m = 0; m < nmodes; m++) {
+      c[m] = 2.0 * uniform01() - 1.0;
+      phase[m] = 2.0 * PI * uniform01();
+    }
+    for (i = 0; i < level->npoints; i++) {
+      double s = 0;
+      for (m = 0; m < nmodes; m++)
+        s += c[m] * sin(k[m][0] * x[i] + k[m][1] * y[i] + k[m][2] * z[i] + phase[m]);
+      p[i] = base + amp * s;
+    }
+  }
+  (void)cf; (void)ph;
+}
+
+int nrharness_post_initialdata(tL *level)
+{
+  tVarList *u = 0;
+  evolve_vlretrieve(&u, 0, 0);
+  if (u) u->level = level;
+  if (Getv("nrharness_data", "fourier")) {
+    if (!u) errorexit("nrharness: no evolved variables");
+    set_fourier(level, u);
+  }
+  if (Getv("nrharness_mg", "yes")) {
+    tVarList *vl = vlalloc(level);
+    vlpush(vl, Ind("punctures_u"));
+    if (level->v[Ind("punctures_u")]) dump_varlist(level, vl, "mg_u");
+    vlfree(vl);
+  }
+  if (u && dump_requested(0)) dump_varlist(level, u, "state_it0");
+  if (u && Getv("nrharness_rhs", "yes")) {
+    tVarList *r = AddDuplicateEnable(u, "_nrh");
+    evolve_rhs(r, u, 0.0, u, 0);
+    dump_varlist(level, r, "rhs_it0");
+  }
+  return 0;
+}
+
+int nrharness_post_evolve(tL *level)
+{
+  tVarList *u = 0;
+  char tag[64];
+  evolve_vlretrieve(&u, 0, 0);
+  if (!u) return 0;
+  u->level = level;
+  /* POST_EVOLVE runs before the level's iteration counter is advanced
+     (main.c:466-474): this is the state after iteration+1 steps */
+  if (dump_requested(level->iteration + 1)) {
+    snprintf(tag, sizeof tag, "state_it%d", level->iteration + 1);
+    dump_varlist(level, u, tag);
+  }
+  return 0;
+}
+
+void bam_nrharness(void)
+{
+  if (!Getv("physics", "nrharness")) return;
+  printf("Adding nrharness (oracle dump harness)\n");
+  AddPar("nrharness_dir", ".", "directory for raw FP64 dumps");
+  AddPar("nrharness_dump", "none", "level iterations after which to dump the evolved variables");
+  AddPar("nrharness_rhs", "no", "dump one RHS evaluation of the initial state [no,yes]");
+  AddPar("nrharness_mg", "no", "dump punctures_u after the initial data solve [no,yes]");
+  AddPar("nrharness_data", "none", "synthetic data over the evolved variables [none,fourier]");
+  AddPar("nrharness_amp", "1e-3", "amplitude of the Fourier perturbation");
+  AddPar("nrharness_nmodes", "8", "number of Fourier modes");
+  AddPar("nrharness_seed", "1", "seed of the mode generator");
+  AddPar("nrharness_length", "16", "box length that sets the wave numbers");
+  AddFun(POST_INITIALDATA, nrharness_post_initialdata, "oracle harness: synthetic data and dumps");
+  AddFun(POST_EVOLVE, nrharness_post_evolve, "oracle harness: dumps");
+}

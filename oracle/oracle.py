@@ -1,0 +1,80 @@
+"""Loader for the CPU oracle (oracle/nr_oracle.c -> oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline leg of bench.py, never by the product package.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from baum_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SO = os.path.join(HERE, "liboracle.so")
+SRC = os.path.join(HERE, "nr_oracle.c")
+
+
+def build(force=False):
+    """Compile the restatement with gcc (-O2, OpenMP, no fast-math)."""
+    deps = [SRC, os.path.join(HERE, "..", "include", "nrgpu.h")]
+    if not force and os.path.exists(SO) and all(os.path.getmtime(SO) >= os.path.getmtime(d) for d in deps):
+        return SO
+    cmd = ["gcc", "-O2", "-std=gnu99", "-fopenmp", "-fPIC", "-shared", "-ffp-contract=off",
+           SRC, "-o", SO, "-lm"]
+    subprocess.run(cmd, check=True)
+    return SO
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(SO)
+        pp = C.POINTER(C.c_void_p)
+        LD = C.POINTER(abi.LevelDesc)
+        BP = C.POINTER(abi.BssnParams)
+        for name, args in {
+            "oracle_bssn_rhs": [LD, pp, pp, C.c_double, pp, BP],
+            "oracle_bssn_boundary": [LD, pp, pp, C.c_double, pp, BP],
+            "oracle_bssn_algcon": [LD, pp, BP],
+            "oracle_bssn_rk4_step": [LD, pp, C.c_double, BP],
+            "oracle_bssn_evolve": [LD, pp, C.c_double, C.c_int, BP],
+        }.items():
+            f = getattr(L, name)
+            f.restype = C.c_int
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptrs(arr):
+    """24 row pointers of a C-contiguous (24, npoints) float64 array."""
+    assert arr.dtype == np.float64 and arr.flags.c_contiguous
+    base = arr.ctypes.data
+    stride = arr.strides[0]
+    return abi.ptr_array([base + i * stride for i in range(arr.shape[0])])
+
+
+def bssn_rhs(level, u, params, c=0.0, upre=None, out=None):
+    """rhs (inner points) + radiative boundary of u[24, npoints] (c = 0)."""
+    out = np.zeros_like(u) if out is None else out
+    upre = u if upre is None else upre
+    pu, pn, pp_ = _ptrs(u), _ptrs(out), _ptrs(upre)
+    e = lib().oracle_bssn_rhs(C.byref(level.desc), pn, pp_, c, pu, C.byref(params))
+    if e:
+        raise RuntimeError("oracle rhs failed")
+    lib().oracle_bssn_boundary(C.byref(level.desc), pn, pp_, c, pu, C.byref(params))
+    return out
+
+
+def bssn_evolve(level, u, dt, nsteps, params):
+    """nsteps RK4 steps of u[24, npoints] in place."""
+    e = lib().oracle_bssn_evolve(C.byref(level.desc), _ptrs(u), dt, nsteps, C.byref(params))
+    if e:
+        raise RuntimeError("oracle evolve failed")
+    return u
