@@ -63,7 +63,7 @@ def bssn_params(**over):
     p.order_centered = 4
     p.order_advection = 4
     p.advection_lopsided = 1
-    p.advection_lopsided6 = 2
+    p.advection_lopsided6 = 3  # reference default, bam_amr.c:52
     p.order_dissipation = 6
     p.dissfactor = 0.1 / 2.0 ** 6
     p.forceKzerofactor = 1.0  # Getv("bssn_forceKzero","no") is 1 for the default "no"
@@ -178,6 +178,7 @@ def lib():
         "nrgpu_bssn_rk4_step": (C.c_int, [vp, pp, C.c_double, C.POINTER(BssnParams), vp]),
         "nrgpu_bssn_evolve_host": (C.c_int, [vp, pp, C.c_int, C.c_double, C.POINTER(BssnParams)]),
         "nrgpu_level_nan_flag": (C.c_int, [vp, C.POINTER(C.c_int)]),
+        "nrgpu_probe_fp64_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_float)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

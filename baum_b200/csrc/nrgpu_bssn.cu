@@ -1,0 +1,851 @@
+// nrgpu_bssn.cu -- BSSN right-hand side, radiative boundary, algebraic
+// constraints and the fused RK4 stages for B200 (sm_100a), FP64.
+//
+// The physics is the reference's bssn_rhs_movpunc_N (spec
+// bssn_rhs_movpunc_N.m:18-461), computed per inner point in one thread:
+//   centred FD of order 2/4/6 with the reference's order ladder near box
+//   edges (bssn_rhs_movpunc_N.m:32-110, boundaryNaway bam_amr_loops_box.h:215),
+//   lopsided advection with edge-shifted stencils (bam_amr_advection.h:72-192),
+//   BSSN algebra + 1+log / Gamma-driver gauge (bssn_rhs_movpunc_N.m:218-346),
+//   Kreiss-Oliger dissipation where the full stencil fits (:351-372).
+// The order of work inside a thread is chosen for register pressure, not the
+// reference's: each group of derivatives is consumed right after it is formed
+// (connection -> Ricci -> conformal factor -> lapse -> A -> shift), and the
+// advection and dissipation sums are added at the end, so that the 24 rhs
+// accumulators are the only long-lived state.  Algebraically this is the
+// reference's expression; it differs from it only in rounding.
+#include <cstdio>
+#include "nrgpu_level.cuh"
+
+namespace {
+
+enum { G11 = 0, CHI = 6, A11 = 7, KK = 13, GA1 = 14, ALPHA = 17, BETA1 = 18, BB1 = 21 };
+
+// ---- finite-difference numerators ------------------------------------------
+// first derivative numerator; the derivative is num / (den1 * h)
+template <int ORD>
+__device__ __forceinline__ double d1n(const double *__restrict__ f, int x, int s) {
+  if (ORD == 2) return ldg(f + x + s) - ldg(f + x - s);
+  if (ORD == 4)
+    return (ldg(f + x - 2 * s) - ldg(f + x + 2 * s)) + 8.0 * (ldg(f + x + s) - ldg(f + x - s));
+  return (ldg(f + x + 3 * s) - ldg(f + x - 3 * s)) + 9.0 * (ldg(f + x - 2 * s) - ldg(f + x + 2 * s)) +
+         45.0 * (ldg(f + x + s) - ldg(f + x - s));
+}
+template <int ORD> __host__ __device__ constexpr double den1() { return ORD == 2 ? 2.0 : ORD == 4 ? 12.0 : 60.0; }
+template <int ORD> __host__ __device__ constexpr double den2() { return ORD == 2 ? 1.0 : ORD == 4 ? 12.0 : 180.0; }
+
+// second derivative numerator; the derivative is num / (den2 * h^2)
+template <int ORD>
+__device__ __forceinline__ double d2n(const double *__restrict__ f, int x, int s) {
+  const double c = ldg(f + x);
+  if (ORD == 2) return ldg(f + x - s) - 2.0 * c + ldg(f + x + s);
+  if (ORD == 4)
+    return 16.0 * (ldg(f + x - s) + ldg(f + x + s)) - (ldg(f + x - 2 * s) + ldg(f + x + 2 * s)) - 30.0 * c;
+  return 2.0 * (ldg(f + x - 3 * s) + ldg(f + x + 3 * s)) - 27.0 * (ldg(f + x - 2 * s) + ldg(f + x + 2 * s)) +
+         270.0 * (ldg(f + x - s) + ldg(f + x + s)) - 490.0 * c;
+}
+
+// mixed derivative numerator: product of two first-derivative stencils
+// (discretize.m:68-71); the derivative is num / (den1^2 * h1 * h2)
+template <int ORD>
+__device__ __forceinline__ double d11n(const double *__restrict__ f, int x, int s1, int s2) {
+  if (ORD == 2) return d1n<2>(f, x + s1, s2) - d1n<2>(f, x - s1, s2);
+  if (ORD == 4)
+    return (d1n<4>(f, x - 2 * s1, s2) - d1n<4>(f, x + 2 * s1, s2)) +
+           8.0 * (d1n<4>(f, x + s1, s2) - d1n<4>(f, x - s1, s2));
+  return (d1n<6>(f, x + 3 * s1, s2) - d1n<6>(f, x - 3 * s1, s2)) +
+         9.0 * (d1n<6>(f, x - 2 * s1, s2) - d1n<6>(f, x + 2 * s1, s2)) +
+         45.0 * (d1n<6>(f, x + s1, s2) - d1n<6>(f, x - s1, s2));
+}
+
+// lopsided advection rows (numerators), row r = stencil shifted by r
+// (bam_amr_advection.h:28-66); denominators 2, 12, 60
+__constant__ double kAdv2[3][3] = {{3, -4, 1}, {1, 0, -1}, {-1, 4, -3}};
+__constant__ double kAdv4[5][5] = {{25, -48, 36, -16, 3}, {3, 10, -18, 6, -1}, {-1, 8, 0, -8, 1},
+                                   {1, -6, 18, -10, -3}, {-3, 16, -36, 48, -25}};
+__constant__ double kAdv6[7][7] = {{147, -360, 450, -400, 225, -72, 10}, {10, 77, -150, 100, -50, 15, -2},
+                                   {-2, 24, 35, -80, 30, -8, 1},        {1, -9, 45, 0, -45, 9, -1},
+                                   {-1, 8, -30, 80, -35, -24, 2},       {2, -15, 50, -100, 150, -77, -10},
+                                   {-10, 72, -225, 400, -450, 360, -147}};
+
+struct AdvDir {
+  int base;     // offset of tap 0 relative to the point
+  int step;     // +-stride between taps (0 when the shift is zero)
+  int row;      // stencil row
+};
+
+// direction setup of set_advectionN_onedir (bam_amr_advection.h:72-192)
+__device__ __forceinline__ AdvDir adv_dir(int i, int imax, double w, int q, int lop, int s) {
+  AdvDir a;
+  int rst = q - lop, offset, wsign;
+  if (w < 0) { wsign = -1; offset = (i >= rst) ? 0 : rst - i; }
+  else if (w > 0) { wsign = 1; offset = (imax - i >= rst) ? 0 : rst - (imax - i); }
+  else { wsign = 0; offset = 0; }
+  offset += lop;
+  a.row = offset;
+  a.step = wsign * s;
+  a.base = -offset * wsign * s;
+  return a;
+}
+
+template <int Q>
+__device__ __forceinline__ double adv_sum(const double *__restrict__ f, int x, const AdvDir ad[3],
+                                          const double cw[3]) {
+  double acc = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double t = 0.0;
+    const int p0 = x + ad[d].base;
+#pragma unroll
+    for (int n = 0; n <= Q; ++n) {
+      const double c = Q == 2 ? kAdv2[ad[d].row][n] : Q == 4 ? kAdv4[ad[d].row][n] : kAdv6[ad[d].row][n];
+      t += c * ldg(f + p0 + n * ad[d].step);
+    }
+    acc += cw[d] * t;
+  }
+  return acc;
+}
+
+// Kreiss-Oliger: sum over directions of undivided differences / h
+template <int OD>
+__device__ __forceinline__ double ko_sum(const double *__restrict__ f, int x, const int st[3],
+                                         const double ooh[3]) {
+  double acc = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int s = st[d];
+    double t;
+    if (OD == 4)
+      t = 6.0 * ldg(f + x) - 4.0 * (ldg(f + x - s) + ldg(f + x + s)) + (ldg(f + x - 2 * s) + ldg(f + x + 2 * s));
+    else
+      t = (ldg(f + x - 3 * s) + ldg(f + x + 3 * s)) - 6.0 * (ldg(f + x - 2 * s) + ldg(f + x + 2 * s)) +
+          15.0 * (ldg(f + x - s) + ldg(f + x + s)) - 20.0 * ldg(f + x);
+    acc += ooh[d] * t;
+  }
+  return OD == 4 ? -acc : acc;
+}
+
+struct PointCtx {
+  int ijk, i, j, k, imax, jmax, kmax, dist;
+  int st[3];
+  double h[3];
+};
+
+// ---- the per-point right-hand side -------------------------------------------
+template <int ORD>
+__device__ __forceinline__ void bssn_point(const CVarPtrs &U, const PointCtx &P,
+                                           const nrgpu_bssn_params &p, double r[NRGPU_NV]) {
+  const int x = P.ijk;
+  const double o1[3] = {1.0 / (den1<ORD>() * P.h[0]), 1.0 / (den1<ORD>() * P.h[1]),
+                        1.0 / (den1<ORD>() * P.h[2])};
+
+  double g[6], A[6];
+#pragma unroll
+  for (int a = 0; a < 6; ++a) { g[a] = ldg(U.p[G11 + a] + x); A[a] = ldg(U.p[A11 + a] + x); }
+  const double alpha = ldg(U.p[ALPHA] + x);
+  const double chi = ldg(U.p[CHI] + x);
+  double K = ldg(U.p[KK] + x);
+
+  // inverse conformal metric
+  const double detg = g[0] * g[3] * g[5] + 2.0 * g[1] * g[2] * g[4] - g[0] * g[4] * g[4] -
+                      g[3] * g[2] * g[2] - g[5] * g[1] * g[1];
+  const double detginv = 1.0 / detg;
+  double gi[6];
+  gi[0] = detginv * (g[3] * g[5] - g[4] * g[4]);
+  gi[1] = detginv * (g[2] * g[4] - g[1] * g[5]);
+  gi[2] = detginv * (g[1] * g[4] - g[2] * g[3]);
+  gi[3] = detginv * (g[0] * g[5] - g[2] * g[2]);
+  gi[4] = detginv * (g[1] * g[2] - g[0] * g[4]);
+  gi[5] = detginv * (g[0] * g[3] - g[1] * g[1]);
+
+  // connection: gdo[c][ab] = 1/2 (d_a g_bc + d_b g_ac - d_c g_ab), gam = ginv gdo
+  double gdo[3][6], gam[3][6], Gfg[3];
+  {
+    double dg[3][6];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int a = 0; a < 6; ++a) dg[c][a] = o1[c] * d1n<ORD>(U.p[G11 + a], x, P.st[c]);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = a; b < 3; ++b)
+          gdo[c][sy(a, b)] = 0.5 * (dg[a][sy(b, c)] + dg[b][sy(a, c)] - dg[c][sy(a, b)]);
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int a = 0; a < 6; ++a)
+      gam[c][a] = gi[sy(c, 0)] * gdo[0][a] + gi[sy(c, 1)] * gdo[1][a] + gi[sy(c, 2)] * gdo[2][a];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+    Gfg[a] = gi[0] * gam[a][0] + gi[3] * gam[a][3] + gi[5] * gam[a][5] +
+             2.0 * (gi[1] * gam[a][1] + gi[2] * gam[a][2] + gi[4] * gam[a][4]);
+
+  // Ricci tensor of the conformal metric plus, later, the chi part
+  double Rt[6];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = a; b < 3; ++b) {
+      double t = 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          double q = 0.0;
+#pragma unroll
+          for (int e = 0; e < 3; ++e)
+            q += gam[e][sy(c, a)] * gdo[b][sy(e, d)] + gam[e][sy(c, b)] * gdo[a][sy(e, d)] +
+                 gam[e][sy(a, d)] * gdo[e][sy(c, b)];
+          t += gi[sy(c, d)] * q;
+        }
+      Rt[sy(a, b)] = t;
+    }
+  {
+    // -1/2 ginv^cd d_c d_d g_ab, folded over the symmetric pair (c,d)
+    const double o2[3] = {1.0 / (den2<ORD>() * P.h[0] * P.h[0]), 1.0 / (den2<ORD>() * P.h[1] * P.h[1]),
+                          1.0 / (den2<ORD>() * P.h[2] * P.h[2])};
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int d = c; d < 3; ++d) {
+        const double w = (c == d ? -0.5 : -1.0) * gi[sy(c, d)] * (c == d ? o2[c] : o1[c] * o1[d]);
+#pragma unroll
+        for (int a = 0; a < 6; ++a) {
+          const double dd = c == d ? d2n<ORD>(U.p[G11 + a], x, P.st[c])
+                                   : d11n<ORD>(U.p[G11 + a], x, P.st[c], P.st[d]);
+          Rt[a] += w * dd;
+        }
+      }
+    // 1/2 (g_ca d_b G^c + g_cb d_a G^c + G^c (gdo_abc + gdo_bac))
+    double dG[3][3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) dG[b][c] = o1[b] * d1n<ORD>(U.p[GA1 + c], x, P.st[b]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = a; b < 3; ++b) {
+        double t2 = 0.0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          t2 += g[sy(c, a)] * dG[b][c] + g[sy(c, b)] * dG[a][c] +
+                Gfg[c] * (gdo[a][sy(b, c)] + gdo[b][sy(a, c)]);
+        Rt[sy(a, b)] += 0.5 * t2;
+      }
+  }
+
+  // conformal factor chi = psi^chipsipower
+  double chig = chi;
+  if (chig < p.chiDivFloor) chig = p.chiDivFloor;
+  const double oocp = 1.0 / p.chipsipower;
+  const double f = oocp * log(chig);
+  const double psim4 = exp(-4.0 * f);
+  double df[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) df[a] = oocp * (o1[a] * d1n<ORD>(U.p[CHI], x, P.st[a])) / chig;
+  double dfdf = 0.0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) dfdf += gi[sy(a, b)] * df[a] * df[b];
+  {
+    const double o2[3] = {1.0 / (den2<ORD>() * P.h[0] * P.h[0]), 1.0 / (den2<ORD>() * P.h[1] * P.h[1]),
+                          1.0 / (den2<ORD>() * P.h[2] * P.h[2])};
+    double cddf[6];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = a; b < 3; ++b) {
+        const double ddchi = a == b ? o2[a] * d2n<ORD>(U.p[CHI], x, P.st[a])
+                                    : o1[a] * o1[b] * d11n<ORD>(U.p[CHI], x, P.st[a], P.st[b]);
+        double t = oocp * ddchi / chig - p.chipsipower * df[a] * df[b];
+        t -= gam[0][sy(a, b)] * df[0] + gam[1][sy(a, b)] * df[1] + gam[2][sy(a, b)] * df[2];
+        cddf[sy(a, b)] = t;
+      }
+    const double trcddf = gi[0] * cddf[0] + gi[3] * cddf[3] + gi[5] * cddf[5] +
+                          2.0 * (gi[1] * cddf[1] + gi[2] * cddf[2] + gi[4] * cddf[4]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = a; b < 3; ++b) {
+        const int ab = sy(a, b);
+        Rt[ab] += 4.0 * df[a] * df[b] - 2.0 * cddf[ab] - 2.0 * g[ab] * trcddf - 4.0 * g[ab] * dfdf;
+      }
+  }
+
+  // derivatives of the lapse
+  double da[3], cdda[6];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) da[a] = o1[a] * d1n<ORD>(U.p[ALPHA], x, P.st[a]);
+  {
+    const double o2[3] = {1.0 / (den2<ORD>() * P.h[0] * P.h[0]), 1.0 / (den2<ORD>() * P.h[1] * P.h[1]),
+                          1.0 / (den2<ORD>() * P.h[2] * P.h[2])};
+    double dfda = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) dfda += gi[sy(a, b)] * df[a] * da[b];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = a; b < 3; ++b) {
+        const int ab = sy(a, b);
+        double t = a == b ? o2[a] * d2n<ORD>(U.p[ALPHA], x, P.st[a])
+                          : o1[a] * o1[b] * d11n<ORD>(U.p[ALPHA], x, P.st[a], P.st[b]);
+        t -= gam[0][ab] * da[0] + gam[1][ab] * da[1] + gam[2][ab] * da[2];
+        cdda[ab] = t - 2.0 * (df[a] * da[b] + df[b] * da[a] - g[ab] * dfda);
+      }
+  }
+  const double trcdda = psim4 * (gi[0] * cdda[0] + gi[3] * cdda[3] + gi[5] * cdda[5] +
+                                 2.0 * (gi[1] * cdda[1] + gi[2] * cdda[2] + gi[4] * cdda[4]));
+
+  K = K * p.forceKzerofactor;
+
+  // trace-free extrinsic curvature
+  double AAab[6], Ainv[6];
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = a; b < 3; ++b) {
+      double t = 0.0, t2 = 0.0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          t += gi[sy(c, d)] * A[sy(a, c)] * A[sy(d, b)];
+          t2 += gi[sy(a, c)] * gi[sy(b, d)] * A[sy(c, d)];
+        }
+      AAab[sy(a, b)] = t;
+      Ainv[sy(a, b)] = t2;
+    }
+  const double AAs = gi[0] * AAab[0] + gi[3] * AAab[3] + gi[5] * AAab[5] +
+                     2.0 * (gi[1] * AAab[1] + gi[2] * AAab[2] + gi[4] * AAab[4]);
+  const double Rsc = AAs - 2.0 * K * K / 3.0;
+
+  // rhs of g~ and A~ (advection added later)
+#pragma unroll
+  for (int a = 0; a < 6; ++a) {
+    r[G11 + a] = -2.0 * alpha * A[a];
+    r[A11 + a] = psim4 * (-cdda[a] + alpha * Rt[a]) - (1.0 / 3.0) * g[a] * (-trcdda + alpha * Rsc) +
+                 alpha * (K * A[a] - 2.0 * AAab[a]);
+  }
+  r[KK] = -trcdda + alpha * (AAs + K * K / 3.0);
+
+  // rhs of Gamma~ without advection: -2 Ainv da - 2 alpha divAinv + shift terms
+  double rG[3];
+  {
+    double dK[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) dK[a] = p.forceKzerofactor * (o1[a] * d1n<ORD>(U.p[KK], x, P.st[a]));
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      double t = 0.0, s = 0.0;
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        t += (2.0 / 3.0) * gi[sy(a, b)] * dK[b] - 6.0 * Ainv[sy(a, b)] * df[b];
+        s += Ainv[sy(a, b)] * da[b];
+      }
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) t -= gam[a][sy(b, c)] * Ainv[sy(b, c)];
+      rG[a] = -2.0 * s - 2.0 * alpha * t;
+    }
+  }
+
+  // shift terms: Lie-derivative corrections and pseudo-Lie of Gamma~
+  {
+    const double o2[3] = {1.0 / (den2<ORD>() * P.h[0] * P.h[0]), 1.0 / (den2<ORD>() * P.h[1] * P.h[1]),
+                          1.0 / (den2<ORD>() * P.h[2] * P.h[2])};
+    double db[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) db[a][c] = o1[a] * d1n<ORD>(U.p[BETA1 + c], x, P.st[a]);
+    const double divbeta = db[0][0] + db[1][1] + db[2][2];
+    const double totdivbeta = (2.0 / 3.0) * divbeta;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = a; b < 3; ++b) {
+        const int ab = sy(a, b);
+        double tg = -g[ab] * totdivbeta, tA = -A[ab] * totdivbeta;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          tg += db[a][c] * g[sy(b, c)] + db[b][c] * g[sy(a, c)];
+          tA += db[a][c] * A[sy(b, c)] + db[b][c] * A[sy(a, c)];
+        }
+        r[G11 + ab] += tg;
+        r[A11 + ab] += tA;
+      }
+    r[CHI] = (p.chipsipower / 6.0) * chig * divbeta - (p.chipsipower / 6.0) * chig * alpha * K;
+    // ddb[bc][a] = d_b d_c beta^a
+    double trddb[3] = {0.0, 0.0, 0.0};   // g^bc d_b d_c beta^a
+    double divdb[3] = {0.0, 0.0, 0.0};   // d_a d_b beta^b
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+      for (int c = b; c < 3; ++c)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const double dd = b == c ? o2[b] * d2n<ORD>(U.p[BETA1 + a], x, P.st[b])
+                                   : o1[b] * o1[c] * d11n<ORD>(U.p[BETA1 + a], x, P.st[b], P.st[c]);
+          trddb[a] += (b == c ? 1.0 : 2.0) * gi[sy(b, c)] * dd;
+          // d_b d_c beta^a contributes to divdb[b] when c == a and to divdb[c] when b == a
+          if (c == a) divdb[b] += dd;
+          if (b == a && b != c) divdb[c] += dd;
+        }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      double t = trddb[a];
+#pragma unroll
+      for (int b = 0; b < 3; ++b) t += gi[sy(a, b)] * ((1.0 / 3.0) * divdb[b]) - Gfg[b] * db[b][a];
+      rG[a] += t + Gfg[a] * totdivbeta;
+    }
+  }
+
+  // gauge
+  const double falpha = p.oploglapse * p.lapseharmonicf + p.oploglapse2 * 8.0 / (3.0 * (3.0 - alpha)) +
+                        p.harmoniclapse * alpha;
+  r[ALPHA] = -falpha * alpha * K;
+  const double betaF = p.shiftgammacoeff * pow(alpha, p.shiftalphapower);
+  const double bfac = p.gamma0factor + p.gamma2factor * betaF;
+  const double alphaG = p.shiftgammacoeff * pow(alpha, p.shiftGalphapower);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const double Ba = ldg(U.p[BB1 + a] + x), ba = ldg(U.p[BETA1 + a] + x), Ga = ldg(U.p[GA1 + a] + x);
+    r[BETA1 + a] = (p.gamma2factor + p.gamma0factor * betaF) * p.withB * Ba +
+                   (1.0 - p.withB) * (alphaG * Ga - p.shiftdriver * ba);
+    r[BB1 + a] = p.withB * (bfac * rG[a] - p.shiftdriver * Ba);
+    r[GA1 + a] = rG[a];
+  }
+
+  // advection beta^i d_i u with lopsided stencils (weights w = beta/dx)
+  {
+    const int lop = ORD == 2 ? 0 : (ORD == 6 ? p.advection_lopsided6 : p.advection_lopsided);
+    const int idx[3] = {P.i, P.j, P.k}, mx[3] = {P.imax, P.jmax, P.kmax};
+    AdvDir ad[3];
+    double cw[3];
+    const double oad = 1.0 / den1<ORD>();
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double w = ldg(U.p[BETA1 + d] + x) / P.h[d];
+      ad[d] = adv_dir(idx[d], mx[d], w, ORD, lop, P.st[d]);
+      const int ws = w < 0 ? -1 : (w > 0 ? 1 : 0);
+      cw[d] = -ws * w * oad;
+    }
+#pragma unroll
+    for (int a = 0; a < 6; ++a) {
+      r[G11 + a] += adv_sum<ORD>(U.p[G11 + a], x, ad, cw);
+      r[A11 + a] += adv_sum<ORD>(U.p[A11 + a], x, ad, cw);
+    }
+    r[KK] += adv_sum<ORD>(U.p[KK], x, ad, cw);
+    r[CHI] += adv_sum<ORD>(U.p[CHI], x, ad, cw);
+    r[ALPHA] += p.oplogwithshift * adv_sum<ORD>(U.p[ALPHA], x, ad, cw);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double aG = adv_sum<ORD>(U.p[GA1 + a], x, ad, cw);
+      r[GA1 + a] += aG;
+      r[BB1 + a] += p.withB * (bfac * (1.0 - p.withGadv) * aG +
+                               p.withBadv * adv_sum<ORD>(U.p[BB1 + a], x, ad, cw));
+      r[BETA1 + a] += p.withShiftadv * adv_sum<ORD>(U.p[BETA1 + a], x, ad, cw);
+    }
+  }
+
+  // Kreiss-Oliger dissipation where the full stencil fits
+  if ((p.order_dissipation == 4 && P.dist >= 2) || (p.order_dissipation == 6 && P.dist >= 3)) {
+    const double ooh[3] = {1.0 / P.h[0], 1.0 / P.h[1], 1.0 / P.h[2]};
+    const double e = p.dissfactor;
+    if (p.order_dissipation == 6) {
+#pragma unroll
+      for (int a = 0; a < 6; ++a) {
+        r[G11 + a] += e * ko_sum<6>(U.p[G11 + a], x, P.st, ooh);
+        r[A11 + a] += e * ko_sum<6>(U.p[A11 + a], x, P.st, ooh);
+      }
+#pragma unroll
+      for (int a = 0; a < 3; ++a) r[GA1 + a] += e * ko_sum<6>(U.p[GA1 + a], x, P.st, ooh);
+      r[KK] += e * ko_sum<6>(U.p[KK], x, P.st, ooh);
+      r[CHI] += e * ko_sum<6>(U.p[CHI], x, P.st, ooh);
+    } else {
+#pragma unroll
+      for (int a = 0; a < 6; ++a) {
+        r[G11 + a] += e * ko_sum<4>(U.p[G11 + a], x, P.st, ooh);
+        r[A11 + a] += e * ko_sum<4>(U.p[A11 + a], x, P.st, ooh);
+      }
+#pragma unroll
+      for (int a = 0; a < 3; ++a) r[GA1 + a] += e * ko_sum<4>(U.p[GA1 + a], x, P.st, ooh);
+      r[KK] += e * ko_sum<4>(U.p[KK], x, P.st, ooh);
+      r[CHI] += e * ko_sum<4>(U.p[CHI], x, P.st, ooh);
+    }
+  }
+  r[KK] *= p.forceKzerofactor;
+}
+
+// ---- epilogues ----------------------------------------------------------------
+enum { EPI_RHS = 0, EPI_ADDLINEAR = 1, EPI_RK = 2 };
+
+struct Epilogue {
+  int mode;
+  double c;        // EPI_ADDLINEAR: unew = upre + c rhs
+  double wacc;     // EPI_RK: acc += wacc * rhs
+  double cv;       // EPI_RK: vout = upre + cv * rhs (when has_v)
+  int has_v;
+};
+
+__device__ __forceinline__ void det_trace_fix(double n[NRGPU_NV], const nrgpu_bssn_params &p) {
+  double *g = n + G11, *A = n + A11;
+  const double detg = g[0] * g[3] * g[5] + 2.0 * g[1] * g[2] * g[4] - g[0] * g[4] * g[4] -
+                      g[3] * g[2] * g[2] - g[5] * g[1] * g[1];
+  const double detnginv = 1.0 / detg;
+  if (p.subtractA) {
+    const double gi0 = g[3] * g[5] - g[4] * g[4], gi1 = g[2] * g[4] - g[1] * g[5],
+                 gi2 = g[1] * g[4] - g[2] * g[3], gi3 = g[0] * g[5] - g[2] * g[2],
+                 gi4 = g[1] * g[2] - g[0] * g[4], gi5 = g[0] * g[3] - g[1] * g[1];
+    const double trA = detnginv * (gi0 * A[0] + gi3 * A[3] + gi5 * A[5] + 2.0 * (gi1 * A[1] + gi2 * A[2] + gi4 * A[4]));
+    const double aux = -trA / 3.0;
+#pragma unroll
+    for (int v = 0; v < 6; ++v) A[v] += aux * g[v];
+  }
+  if (p.normalizedetg) {
+    const double aux = cbrt(detnginv);
+#pragma unroll
+    for (int v = 0; v < 6; ++v) g[v] *= aux;
+  }
+}
+
+__device__ __forceinline__ void store(const double r[NRGPU_NV], int x, const VarPtrs &out, const CVarPtrs &pre,
+                                      const VarPtrs &acc, const Epilogue &E, const nrgpu_bssn_params &p) {
+  if (E.mode == EPI_RHS) {
+#pragma unroll
+    for (int v = 0; v < NRGPU_NV; ++v) out.p[v][x] = r[v];
+  } else if (E.mode == EPI_ADDLINEAR) {
+    double n[NRGPU_NV];
+#pragma unroll
+    for (int v = 0; v < NRGPU_NV; ++v) n[v] = ldg(pre.p[v] + x) + E.c * r[v];
+    n[KK] = p.forceKzerofactor * n[KK];
+    det_trace_fix(n, p);
+#pragma unroll
+    for (int v = 0; v < NRGPU_NV; ++v) out.p[v][x] = n[v];
+  } else {
+#pragma unroll
+    for (int v = 0; v < NRGPU_NV; ++v) {
+      acc.p[v][x] += E.wacc * r[v];
+      if (E.has_v) out.p[v][x] = ldg(pre.p[v] + x) + E.cv * r[v];
+    }
+  }
+}
+
+__device__ __forceinline__ int ladder(int order, int d) {
+  if (order == 2 || d == 1) return 2;
+  if (order == 4 || d == 2) return 4;
+  if (order == 6 || d == 3) return 6;
+  return 0;
+}
+
+// ---- kernels ----------------------------------------------------------------
+// one thread per point of the box interior (i,j,k in [1, m-2]); inner points
+// (flag 0) only, the flagged ones are handled by bssn_flagged_kernel
+__global__ void __launch_bounds__(128) bssn_rhs_kernel(CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPtrs acc,
+                                                      Epilogue E, const nrgpu_bssn_params p, BoxGeo box,
+                                                      const int *__restrict__ boundary, double dx, double dy,
+                                                      double dz, int *status) {
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = 1 + blockIdx.z;
+  if (i > box.m - 2 || j > box.n - 2 || k > box.o - 2) return;
+  PointCtx P;
+  P.i = i; P.j = j; P.k = k;
+  P.imax = box.m - 1; P.jmax = box.n - 1; P.kmax = box.o - 1;
+  P.st[0] = 1; P.st[1] = box.m; P.st[2] = box.m * box.n;
+  P.ijk = box.noffset + i + box.m * (j + box.n * k);
+  if (__ldg(boundary + P.ijk) != 0) return;
+  P.h[0] = dx; P.h[1] = dy; P.h[2] = dz;
+  int d = min(min(i, j), k);
+  d = min(d, min(min(P.imax - i, P.jmax - j), P.kmax - k));
+  P.dist = d;
+  const int oc = ladder(p.order_centered, d);
+  const int oa = ladder(p.order_advection, d);
+  if (oc == 0 || oc != oa) {  // mixed orders are refused at the entry point
+    atomicOr(status + 1, 1);
+    return;
+  }
+  double r[NRGPU_NV];
+  if (oc == 2) bssn_point<2>(U, P, p, r);
+  else if (oc == 4) bssn_point<4>(U, P, p, r);
+  else bssn_point<6>(U, P, p, r);
+  double s = 0.0;
+#pragma unroll
+  for (int v = 0; v < NRGPU_NV; ++v) s += r[v];
+  if (!isfinite(s)) atomicOr(status, 1);
+  store(r, P.ijk, out, pre, acc, E, p);
+}
+
+// computedel of radiative.c:19-42 on clipped neighbours
+__device__ __forceinline__ double computedel(const double *__restrict__ v, double w, int ccc, int mcc, int Mcc,
+                                             int pcc, int Pcc) {
+  if (w > 0) {
+    if (Mcc != ccc) return 3.0 * ldg(v + ccc) + ldg(v + Mcc) - 4.0 * ldg(v + mcc);
+    if (mcc != ccc) return ldg(v + pcc) - ldg(v + mcc);
+    return 4.0 * ldg(v + pcc) - ldg(v + Pcc) - 3.0 * ldg(v + ccc);
+  } else if (w < 0) {
+    if (Pcc != ccc) return 4.0 * ldg(v + pcc) - ldg(v + Pcc) - 3.0 * ldg(v + ccc);
+    if (mcc != ccc) return ldg(v + pcc) - ldg(v + mcc);
+    return 3.0 * ldg(v + ccc) + ldg(v + Mcc) - 4.0 * ldg(v + mcc);
+  } else {
+    if (pcc != ccc && mcc != ccc) return ldg(v + pcc) - ldg(v + mcc);
+    if (mcc == ccc) return 4.0 * ldg(v + pcc) - ldg(v + Pcc) - 3.0 * ldg(v + ccc);
+    return 3.0 * ldg(v + ccc) + ldg(v + Mcc) - 4.0 * ldg(v + mcc);
+  }
+}
+
+// one thread per (flagged point, variable): radiative rhs on PHYBOUND points
+// (set_boundary_rot_rad, radiative.c:105-300, rot = 0); other flags have a
+// zero rhs, which in the RK epilogue leaves acc unchanged and sets vout = pre
+__global__ void bssn_flagged_kernel(CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPtrs acc, Epilogue E,
+                                    const nrgpu_bssn_params p, const FlagPoint *__restrict__ pts, int npts,
+                                    const BoxGeo *__restrict__ boxes, double dx, double dy, double dz) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * NRGPU_NV) return;
+  const int v = t % NRGPU_NV;
+  const FlagPoint fp = pts[t / NRGPU_NV];
+  const int ccc = fp.ijk;
+  if (fp.flag != NRGPU_PHYBOUND) {
+    if (E.mode == EPI_RK && E.has_v) out.p[v][ccc] = ldg(pre.p[v] + ccc);
+    return;
+  }
+  const BoxGeo b = boxes[fp.box];
+  const int i = fp.i, j = fp.j, k = fp.k;
+  const int di = 1, dj = b.m, dk = b.m * b.n;
+  const int mcc = i > 0 ? ccc - di : ccc, pcc = i + 1 < b.m ? ccc + di : ccc;
+  const int cmc = j > 0 ? ccc - dj : ccc, cpc = j + 1 < b.n ? ccc + dj : ccc;
+  const int ccm = k > 0 ? ccc - dk : ccc, ccp = k + 1 < b.o ? ccc + dk : ccc;
+  const int Mcc = i > 1 ? mcc - di : ccc, Pcc = i + 2 < b.m ? pcc + di : ccc;
+  const int cMc = j > 1 ? cmc - dj : ccc, cPc = j + 2 < b.n ? cpc + dj : ccc;
+  const int ccM = k > 1 ? ccm - dk : ccc, ccP = k + 2 < b.o ? ccp + dk : ccc;
+  const double xx = b.x0 + i * dx, yy = b.y0 + j * dy, zz = b.z0 + k * dz;
+  const double rr = sqrt(xx * xx + yy * yy + zz * zz);
+  const double vv = p.bc_speed[v], var0 = p.bc_var0[v];
+  const double *var = U.p[v];
+  const double Wx = vv * xx / rr, Wy = vv * yy / rr, Wz = vv * zz / rr;
+  const double delx = computedel(var, Wx, ccc, mcc, Mcc, pcc, Pcc);
+  const double dely = computedel(var, Wy, ccc, cmc, cMc, cpc, cPc);
+  const double delz = computedel(var, Wz, ccc, ccm, ccM, ccp, ccP);
+  double rhs = -vv * (ldg(var + ccc) - var0) / rr;
+  rhs += -(Wx * delx * (1.0 / (2.0 * dx)) + Wy * dely * (1.0 / (2.0 * dy)) + Wz * delz * (1.0 / (2.0 * dz)));
+  if (E.mode == EPI_RHS) out.p[v][ccc] = rhs;
+  else if (E.mode == EPI_ADDLINEAR) out.p[v][ccc] = ldg(pre.p[v] + ccc) + E.c * rhs;
+  else {
+    acc.p[v][ccc] += E.wacc * rhs;
+    if (E.has_v) out.p[v][ccc] = ldg(pre.p[v] + ccc) + E.cv * rhs;
+  }
+}
+
+// bssn_algcon (bssn_algcon.c:25-230) on all points
+__global__ void bssn_algcon_kernel(VarPtrs u, int npoints, int subtractA, int normalizedetg) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= npoints) return;
+  double g[6], A[6];
+#pragma unroll
+  for (int v = 0; v < 6; ++v) { g[v] = u.p[G11 + v][q]; A[v] = u.p[A11 + v][q]; }
+  double detg = g[0] * g[3] * g[5] + 2.0 * g[1] * g[2] * g[4] - g[0] * g[4] * g[4] - g[3] * g[2] * g[2] -
+                g[5] * g[1] * g[1];
+  if (normalizedetg) {
+    const double eps = detg - 1.0;
+    const double aux = fabs(eps) < 1e-12 ? 1.0 - eps / 3.0 : 1.0 / cbrt(detg);
+#pragma unroll
+    for (int v = 0; v < 6; ++v) g[v] *= aux;
+    detg = g[0] * g[3] * g[5] + 2.0 * g[1] * g[2] * g[4] - g[0] * g[4] * g[4] - g[3] * g[2] * g[2] -
+           g[5] * g[1] * g[1];
+  }
+  if (subtractA) {
+    const double detginv = 1.0 / detg;
+    const double gi0 = g[3] * g[5] - g[4] * g[4], gi1 = g[2] * g[4] - g[1] * g[5],
+                 gi2 = g[1] * g[4] - g[2] * g[3], gi3 = g[0] * g[5] - g[2] * g[2],
+                 gi4 = g[1] * g[2] - g[0] * g[4], gi5 = g[0] * g[3] - g[1] * g[1];
+    const double trA = detginv * (gi0 * A[0] + gi3 * A[3] + gi5 * A[5] + 2.0 * (gi1 * A[1] + gi2 * A[2] + gi4 * A[4]));
+    const double aux = -trA / 3.0;
+#pragma unroll
+    for (int v = 0; v < 6; ++v) A[v] += aux * g[v];
+  }
+#pragma unroll
+  for (int v = 0; v < 6; ++v) { u.p[G11 + v][q] = g[v]; u.p[A11 + v][q] = A[v]; }
+}
+
+// r = a x + b y for n variables (vladd, variables.c:650)
+__global__ void vladd_kernel(VarPtrs r, CVarPtrs xv, CVarPtrs yv, double a, double b, int nvars, int npoints) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)nvars * npoints) return;
+  const int v = (int)(t / npoints), q = (int)(t % npoints);
+  double s = 0.0;
+  if (a != 0.0) s = a * xv.p[v][q];
+  if (b != 0.0) s += b * yv.p[v][q];
+  r.p[v][q] = s;
+}
+
+// copy 24 variables (vlcopy, variables.c:575)
+__global__ void vlcopy_kernel(VarPtrs dst, CVarPtrs src, int npoints) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)NRGPU_NV * npoints) return;
+  const int v = (int)(t / npoints), q = (int)(t % npoints);
+  dst.p[v][q] = src.p[v][q];
+}
+
+}  // namespace
+
+// ---- host side ----------------------------------------------------------------
+static int check_params(const nrgpu_bssn_params *p) {
+  if (!p) return nrgpu_set_error(NRGPU_ERR_ARG, "null parameters");
+  if (p->order_centered != 2 && p->order_centered != 4 && p->order_centered != 6)
+    return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "order_centered %d not in {2,4,6}", p->order_centered);
+  if (p->order_advection != p->order_centered)
+    return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "order_advection %d != order_centered %d",
+                           p->order_advection, p->order_centered);
+  if (p->order_dissipation != 0 && p->order_dissipation != 4 && p->order_dissipation != 6)
+    return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "order_dissipation %d not in {0,4,6}", p->order_dissipation);
+  if (p->advection_lopsided < 0 || p->advection_lopsided > 2 || p->advection_lopsided6 < 0 ||
+      p->advection_lopsided6 > 3)
+    return nrgpu_set_error(NRGPU_ERR_ARG, "advection lopsidedness out of range");
+  return NRGPU_OK;
+}
+
+static int fill_ptrs(VarPtrs *vp, double *const *src, const char *what) {
+  if (!src) return nrgpu_set_error(NRGPU_ERR_ARG, "null %s list", what);
+  for (int v = 0; v < NRGPU_NV; ++v) {
+    if (!src[v]) return nrgpu_set_error(NRGPU_ERR_ARG, "null %s[%d]", what, v);
+    vp->p[v] = src[v];
+  }
+  return NRGPU_OK;
+}
+
+static CVarPtrs cptrs(const VarPtrs &v) {
+  CVarPtrs c;
+  for (int i = 0; i < NRGPU_NV; ++i) c.p[i] = v.p[i];
+  return c;
+}
+
+// launch the interior and flagged kernels of one rhs evaluation
+static int launch_rhs(nrgpu_level *L, const CVarPtrs &U, const VarPtrs &out, const CVarPtrs &pre, const VarPtrs &acc,
+                      const Epilogue &E, const nrgpu_bssn_params &p, cudaStream_t st, bool interior, bool flagged) {
+  if (interior) {
+    for (int b = 0; b < L->nboxes; ++b) {
+      const BoxGeo &bx = L->hbox[b];
+      if (bx.m < 3 || bx.n < 3 || bx.o < 3) continue;
+      dim3 blk(32, 4, 1);
+      dim3 grd((bx.m - 2 + 31) / 32, (bx.n - 2 + 3) / 4, bx.o - 2);
+      bssn_rhs_kernel<<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
+                                           L->d_status);
+    }
+  }
+  if (flagged && L->nflagpts > 0) {
+    const int n = L->nflagpts * NRGPU_NV;
+    bssn_flagged_kernel<<<(n + 255) / 256, 256, 0, st>>>(U, out, pre, acc, E, p, L->d_flagpts, L->nflagpts,
+                                                          L->d_box, L->dx, L->dy, L->dz);
+  }
+  NRGPU_CUDA_TRY(cudaGetLastError());
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_bssn_rhs(nrgpu_level *L, double *const *unew, double *const *upre, double c,
+                              double *const *ucur, const nrgpu_bssn_params *p, void *stream) {
+  if (!L) return nrgpu_set_error(NRGPU_ERR_ARG, "null level");
+  int e;
+  if ((e = check_params(p))) return e;
+  VarPtrs n, pr, cu;
+  if ((e = fill_ptrs(&n, unew, "unew")) || (e = fill_ptrs(&cu, ucur, "ucur"))) return e;
+  if (c != 0.0) {
+    if ((e = fill_ptrs(&pr, upre, "upre"))) return e;
+  } else {
+    pr = cu;
+  }
+  Epilogue E = {c != 0.0 ? EPI_ADDLINEAR : EPI_RHS, c, 0.0, 0.0, 0};
+  return launch_rhs(L, cptrs(cu), n, cptrs(pr), n, E, *p, (cudaStream_t)stream, true, false);
+}
+
+extern "C" int nrgpu_bssn_boundary(nrgpu_level *L, double *const *unew, double *const *upre, double c,
+                                   double *const *ucur, const nrgpu_bssn_params *p, void *stream) {
+  if (!L) return nrgpu_set_error(NRGPU_ERR_ARG, "null level");
+  if (!p) return nrgpu_set_error(NRGPU_ERR_ARG, "null parameters");
+  int e;
+  VarPtrs n, pr, cu;
+  if ((e = fill_ptrs(&n, unew, "unew")) || (e = fill_ptrs(&cu, ucur, "ucur"))) return e;
+  if (c != 0.0) {
+    if ((e = fill_ptrs(&pr, upre, "upre"))) return e;
+  } else {
+    pr = cu;
+  }
+  Epilogue E = {c != 0.0 ? EPI_ADDLINEAR : EPI_RHS, c, 0.0, 0.0, 0};
+  return launch_rhs(L, cptrs(cu), n, cptrs(pr), n, E, *p, (cudaStream_t)stream, false, true);
+}
+
+extern "C" int nrgpu_bssn_algcon(nrgpu_level *L, double *const *u, const nrgpu_bssn_params *p, void *stream) {
+  if (!L || !p) return nrgpu_set_error(NRGPU_ERR_ARG, "null argument");
+  int e;
+  VarPtrs uu;
+  if ((e = fill_ptrs(&uu, u, "u"))) return e;
+  bssn_algcon_kernel<<<(L->npoints + 255) / 256, 256, 0, (cudaStream_t)stream>>>(uu, L->npoints, p->subtractA,
+                                                                                  p->normalizedetg);
+  NRGPU_CUDA_TRY(cudaGetLastError());
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_vladd(nrgpu_level *L, int nvars, double *const *r, double a, double *const *x, double b,
+                           double *const *y, void *stream) {
+  if (!L || !r || nvars < 1 || nvars > NRGPU_NV) return nrgpu_set_error(NRGPU_ERR_ARG, "bad vladd arguments");
+  VarPtrs rr = {}, xx = {}, yy = {};
+  for (int v = 0; v < nvars; ++v) {
+    rr.p[v] = r[v];
+    if (a != 0.0) {
+      if (!x || !x[v]) return nrgpu_set_error(NRGPU_ERR_ARG, "null x");
+      xx.p[v] = x[v];
+    }
+    if (b != 0.0) {
+      if (!y || !y[v]) return nrgpu_set_error(NRGPU_ERR_ARG, "null y");
+      yy.p[v] = y[v];
+    }
+  }
+  const long n = (long)nvars * L->npoints;
+  vladd_kernel<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(rr, cptrs(xx), cptrs(yy), a, b, nvars,
+                                                                              L->npoints);
+  NRGPU_CUDA_TRY(cudaGetLastError());
+  return NRGPU_OK;
+}
+
+int nrgpu_level_scratch(nrgpu_level *L, double **out);
+
+// fused RK4 (rk.c:220-257): stage s reads V_in, adds w_s*r to u and writes
+// V_out = P + c_s*r; both the interior and the flagged kernels do it
+extern "C" int nrgpu_bssn_rk4_step(nrgpu_level *L, double *const *u, double dt, const nrgpu_bssn_params *p,
+                                   void *stream) {
+  if (!L) return nrgpu_set_error(NRGPU_ERR_ARG, "null level");
+  int e;
+  if ((e = check_params(p))) return e;
+  VarPtrs U;
+  if ((e = fill_ptrs(&U, u, "u"))) return e;
+  double *scr = nullptr;
+  if ((e = nrgpu_level_scratch(L, &scr))) return e;
+  VarPtrs P, V1, V2;
+  const size_t np = (size_t)L->npoints;
+  for (int v = 0; v < NRGPU_NV; ++v) {
+    P.p[v] = scr + (0 * NRGPU_NV + v) * np;
+    V1.p[v] = scr + (1 * NRGPU_NV + v) * np;
+    V2.p[v] = scr + (2 * NRGPU_NV + v) * np;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const long n = (long)NRGPU_NV * L->npoints;
+  vlcopy_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(P, cptrs(U), L->npoints);
+  const CVarPtrs cP = cptrs(P);
+  Epilogue E1 = {EPI_RK, 0.0, dt / 6, dt / 2, 1};
+  Epilogue E2 = {EPI_RK, 0.0, dt / 3, dt / 2, 1};
+  Epilogue E3 = {EPI_RK, 0.0, dt / 3, dt, 1};
+  Epilogue E4 = {EPI_RK, 0.0, dt / 6, 0.0, 0};
+  if ((e = launch_rhs(L, cP, V1, cP, U, E1, *p, st, true, true))) return e;
+  if ((e = launch_rhs(L, cptrs(V1), V2, cP, U, E2, *p, st, true, true))) return e;
+  if ((e = launch_rhs(L, cptrs(V2), V1, cP, U, E3, *p, st, true, true))) return e;
+  if ((e = launch_rhs(L, cptrs(V1), V2, cP, U, E4, *p, st, true, true))) return e;
+  return nrgpu_bssn_algcon(L, u, p, stream);
+}

@@ -1,0 +1,28 @@
+// nrgpu_level.cuh -- device mirror of a BAM level (tL, bam_amr.h:46-74).
+#pragma once
+#include "nrgpu_common.cuh"
+
+// one point with a non-zero boundary flag: linear index, box-local ijk,
+// box number and flag; the boundary kernels walk this list
+struct FlagPoint {
+  int ijk, i, j, k;
+  int box, flag;
+};
+
+struct nrgpu_level {
+  int device;
+  int nboxes;
+  int npoints;
+  double dx, dy, dz;
+  BoxGeo *hbox;            // host copy of the boxes
+  int *d_boundary;         // [npoints] flags on the device
+  FlagPoint *d_flagpts;    // points with flag != 0
+  int nflagpts;
+  BoxGeo *d_box;           // boxes on the device
+  int *d_status;           // [0]: NaN flag, [1]: inner point without stencil room
+  // RK4 scratch: three full 24-variable lists, allocated on first use
+  double *scratch;
+  size_t scratch_points;
+  // device copy of a host state for the host-buffer entry points
+  double *hoststate;
+};

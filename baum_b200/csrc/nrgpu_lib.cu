@@ -1,0 +1,182 @@
+// nrgpu_lib.cu -- library state, errors, level mirrors and host-buffer calls.
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#include "nrgpu_level.cuh"
+
+static thread_local char g_err[512] = "";
+
+int nrgpu_set_error(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+extern "C" int nrgpu_abi_version(void) { return NRGPU_ABI_VERSION; }
+
+extern "C" const char *nrgpu_last_error(void) { return g_err; }
+
+extern "C" int nrgpu_init(int device) {
+  int n = 0;
+  NRGPU_CUDA_TRY(cudaGetDeviceCount(&n));
+  if (device < 0 || device >= n) return nrgpu_set_error(NRGPU_ERR_ARG, "device %d of %d", device, n);
+  NRGPU_CUDA_TRY(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  NRGPU_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10) return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "built for sm_100a, device is sm_%d%d",
+                                               prop.major, prop.minor);
+  return NRGPU_OK;
+}
+
+extern "C" void nrgpu_bssn_params_default(nrgpu_bssn_params *p) {
+  if (!p) return;
+  memset(p, 0, sizeof *p);
+  p->order_centered = 4;
+  p->order_advection = 4;
+  p->advection_lopsided = 1;
+  p->advection_lopsided6 = 3;  // reference default (bam_amr.c:52)
+  p->order_dissipation = 6;
+  p->dissfactor = 0.1 / 64.0;  // dissipation_factor / 2^order_dissipation (evolve.c:503)
+  p->forceKzerofactor = 1.0;   // Getv("bssn_forceKzero","no") for the default "no"
+  p->subtractA = 1;
+  p->normalizedetg = 1;
+  p->oploglapse = 1;
+  p->oplogwithshift = 1;
+  p->gamma0factor = 1.0;
+  p->withGadv = p->withShiftadv = p->withBadv = p->withB = 1.0;
+  p->lapseharmonicf = 2.0;
+  p->shiftgammacoeff = 0.75;
+  p->shiftdriver = 2.0;
+  p->chiDivFloor = -1000.0;
+  p->chipsipower = -4.0;
+  // VarNameSetBoundaryInfo (bssn.c:269-311); gauge speed sqrt(2) for 1+log
+  const double vg = 1.4142135623730951;
+  for (int v = 0; v < NRGPU_BSSN_NVARS; ++v) { p->bc_var0[v] = 0.0; p->bc_speed[v] = 1.0; }
+  const int unit[5] = {0, 3, 5, 6, 17};
+  for (int i = 0; i < 5; ++i) p->bc_var0[unit[i]] = 1.0;
+  p->bc_speed[13] = p->bc_speed[6] = p->bc_speed[17] = vg;
+}
+
+extern "C" int nrgpu_level_create(const nrgpu_level_desc *d, nrgpu_level **out) {
+  if (!d || !out || !d->box || !d->boundary || d->nboxes < 1 || d->npoints < 1)
+    return nrgpu_set_error(NRGPU_ERR_ARG, "bad level description");
+  long total = 0;
+  for (int b = 0; b < d->nboxes; ++b) {
+    const nrgpu_box &bx = d->box[b];
+    if (bx.m < 1 || bx.n < 1 || bx.o < 1 || bx.noffset != total)
+      return nrgpu_set_error(NRGPU_ERR_ARG, "box %d: bad size or offset", b);
+    total += (long)bx.m * bx.n * bx.o;
+  }
+  if (total != d->npoints || total > 0x7fffffffL)
+    return nrgpu_set_error(NRGPU_ERR_ARG, "npoints %d does not match the boxes (%ld)", d->npoints, total);
+  std::vector<FlagPoint> fl;
+  for (int b = 0; b < d->nboxes; ++b) {
+    const nrgpu_box &bx = d->box[b];
+    for (int k = 0; k < bx.o; ++k)
+      for (int j = 0; j < bx.n; ++j)
+        for (int i = 0; i < bx.m; ++i) {
+          const int ijk = bx.noffset + i + bx.m * (j + bx.n * k);
+          const int f = d->boundary[ijk];
+          if (f == 0) continue;
+          if (f != NRGPU_PHYBOUND && f != NRGPU_REFBOUND)
+            return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "boundary flag %d at point %d (only 0, PHYBOUND, REFBOUND)",
+                                   f, ijk);
+          fl.push_back(FlagPoint{ijk, i, j, k, b, f});
+        }
+  }
+  nrgpu_level *L = (nrgpu_level *)calloc(1, sizeof(nrgpu_level));
+  if (!L) return nrgpu_set_error(NRGPU_ERR_NOMEM, "host allocation");
+  cudaGetDevice(&L->device);
+  L->nboxes = d->nboxes;
+  L->npoints = d->npoints;
+  L->dx = d->dx; L->dy = d->dy; L->dz = d->dz;
+  L->hbox = (BoxGeo *)malloc(sizeof(BoxGeo) * d->nboxes);
+  for (int b = 0; b < d->nboxes; ++b)
+    L->hbox[b] = BoxGeo{d->box[b].m, d->box[b].n, d->box[b].o, d->box[b].noffset, d->box[b].x0, d->box[b].y0,
+                        d->box[b].z0};
+  L->nflagpts = (int)fl.size();
+  bool ok = cudaMalloc(&L->d_boundary, sizeof(int) * d->npoints) == cudaSuccess &&
+            cudaMalloc(&L->d_box, sizeof(BoxGeo) * d->nboxes) == cudaSuccess &&
+            cudaMalloc(&L->d_status, sizeof(int) * 4) == cudaSuccess &&
+            (fl.empty() || cudaMalloc(&L->d_flagpts, sizeof(FlagPoint) * fl.size()) == cudaSuccess);
+  if (ok)
+    ok = cudaMemcpy(L->d_boundary, d->boundary, sizeof(int) * d->npoints, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(L->d_box, L->hbox, sizeof(BoxGeo) * d->nboxes, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemset(L->d_status, 0, sizeof(int) * 4) == cudaSuccess &&
+         (fl.empty() ||
+          cudaMemcpy(L->d_flagpts, fl.data(), sizeof(FlagPoint) * fl.size(), cudaMemcpyHostToDevice) == cudaSuccess);
+  if (!ok) {
+    nrgpu_level_destroy(L);
+    return nrgpu_set_error(NRGPU_ERR_NOMEM, "device allocation of the level mirror failed");
+  }
+  *out = L;
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_level_destroy(nrgpu_level *L) {
+  if (!L) return NRGPU_OK;
+  cudaFree(L->d_boundary);
+  cudaFree(L->d_box);
+  cudaFree(L->d_status);
+  cudaFree(L->d_flagpts);
+  cudaFree(L->scratch);
+  cudaFree(L->hoststate);
+  free(L->hbox);
+  free(L);
+  return NRGPU_OK;
+}
+
+// three 24-variable lists of RK4 scratch, allocated once per level
+int nrgpu_level_scratch(nrgpu_level *L, double **out) {
+  if (!L->scratch) {
+    const size_t bytes = sizeof(double) * 3 * NRGPU_NV * (size_t)L->npoints;
+    if (cudaMalloc(&L->scratch, bytes) != cudaSuccess) {
+      L->scratch = nullptr;
+      cudaGetLastError();
+      return nrgpu_set_error(NRGPU_ERR_NOMEM, "RK4 scratch of %zu bytes", bytes);
+    }
+    L->scratch_points = (size_t)L->npoints;
+  }
+  *out = L->scratch;
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_level_nan_flag(nrgpu_level *L, int *flag) {
+  if (!L || !flag) return nrgpu_set_error(NRGPU_ERR_ARG, "null argument");
+  int h[2] = {0, 0};
+  NRGPU_CUDA_TRY(cudaMemcpy(h, L->d_status, sizeof h, cudaMemcpyDeviceToHost));
+  NRGPU_CUDA_TRY(cudaMemset(L->d_status, 0, sizeof h));
+  *flag = h[0] ? 1 : 0;
+  if (h[1]) return nrgpu_set_error(NRGPU_ERR_ARG, "an inner point had no room for its stencil");
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_bssn_evolve_host(nrgpu_level *L, double *const *host_u, int nsteps, double dt,
+                                      const nrgpu_bssn_params *p) {
+  if (!L || !host_u || nsteps < 0) return nrgpu_set_error(NRGPU_ERR_ARG, "bad arguments");
+  const size_t np = (size_t)L->npoints;
+  if (!L->hoststate && cudaMalloc(&L->hoststate, sizeof(double) * NRGPU_NV * np) != cudaSuccess) {
+    L->hoststate = nullptr;
+    cudaGetLastError();
+    return nrgpu_set_error(NRGPU_ERR_NOMEM, "state of %zu points", np);
+  }
+  double *buf = L->hoststate;
+  double *u[NRGPU_NV];
+  int e = NRGPU_OK;
+  for (int v = 0; v < NRGPU_NV && !e; ++v) {
+    u[v] = buf + v * np;
+    if (!host_u[v]) e = nrgpu_set_error(NRGPU_ERR_ARG, "null host_u[%d]", v);
+    else if (cudaMemcpyAsync(u[v], host_u[v], sizeof(double) * np, cudaMemcpyHostToDevice, 0) != cudaSuccess)
+      e = nrgpu_set_error(NRGPU_ERR_CUDA, "upload of variable %d", v);
+  }
+  for (int s = 0; s < nsteps && !e; ++s) e = nrgpu_bssn_rk4_step(L, u, dt, p, nullptr);
+  for (int v = 0; v < NRGPU_NV && !e; ++v)
+    if (cudaMemcpyAsync(host_u[v], u[v], sizeof(double) * np, cudaMemcpyDeviceToHost, 0) != cudaSuccess)
+      e = nrgpu_set_error(NRGPU_ERR_CUDA, "download of variable %d", v);
+  if (!e && cudaStreamSynchronize(0) != cudaSuccess) e = nrgpu_set_error(NRGPU_ERR_CUDA, "synchronize");
+  return e;
+}

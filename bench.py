@@ -1,0 +1,324 @@
+"""Benchmark of the BSSN evolution hot path on B200.
+
+Workload (one "step"): one RK4 step of the single Schwarzschild puncture,
+BSSN, 1+log withshift + Gamma-driver (eta = 2), 4th-order centred and
+lopsided advection, KO6 (dissipation_factor 0.1), radiative boundary, on a
+66^3 box (64^3 inner points, dx = 0.25): four fused rhs stages, boundary,
+RK updates and the algebraic constraints.  RHS point-updates per step =
+4 x 64^3.  Initial data: analytic Brill-Lindquist (synthetic, no files).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs independent replicas, one per GPU (the path does not shard).
+Prints one JSON line (rank 0).
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RHS point-updates/s at <=1e-12 rel err vs plain; V-cycles to 1e-10 residual"
+UNIT = "RHS point-updates/s"
+N_INNER = 64
+DX = 0.25
+DT = 0.25 * DX
+PTS_PER_RHS = N_INNER ** 3
+RHS_PER_STEP = 4
+# algorithmic FP64 work of one inner point: operators of the reference's
+# generated rhs (bssn_rhs_movpunc_N.c) on its 4th-order + KO6 path
+FLOP_PER_POINT = 4973
+# DRAM bytes of one interior rhs launch from the ncu capture summarised in
+# profiles/bssn_rhs_kernel_c1.md (None until captured)
+RHS_TRAFFIC_BYTES = None
+CONFIG = {"workload": "bssn_schwarzschild_64^3_rk4", "box": "66^3 (64^3 inner + boundary layer)",
+          "dx": DX, "dt": DT, "order": 4, "dissipation": "KO6 eps=0.1", "gauge": "1+log, Gamma-driver eta=2",
+          "l2": "flushed (256 MiB write) before every timed step", "parallelism": "replicas"}
+
+
+def sample_clocks_start():
+    if not shutil.which("nvidia-smi"):
+        return None
+    f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    idx = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0] or "0"
+    p = subprocess.Popen(["nvidia-smi", "-i", idx, "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                          "-lms", "200"], stdout=f, stderr=subprocess.DEVNULL)
+    return p, f
+
+
+def sample_clocks_stop(h):
+    if h is None:
+        return None
+    p, f = h
+    p.terminate()
+    try:
+        p.wait(timeout=5)
+    except subprocess.TimeoutExpired:
+        p.kill()
+    f.seek(0)
+    rows = [r.split(",") for r in f.read().strip().splitlines() if r.strip()]
+    f.close()
+    os.unlink(f.name)
+    sm, mx, reasons = [], [], set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for r in rows:
+        try:
+            sm.append(float(r[1]))
+            mx.append(float(r[2]))
+        except (ValueError, IndexError):
+            continue
+        for n, v in zip(names, r[5:9]):
+            if v.strip().lower() == "active":
+                reasons.add(n)
+    if not sm:
+        return None
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
+def reference_cpu(steps, warmup, cores=None, nxyz=N_INNER):
+    """Time the reference's own CPU evolution (oracle/_ref/bam, built from the
+    reference sources) on this host: same workload, all host threads."""
+    bam = os.path.join(ROOT, "oracle", "_ref", "bam")
+    cores = cores or os.cpu_count() or 1
+    if not os.path.exists(bam):
+        return None
+    par = """physics = adm bssn punctures
+mass1 = 1
+mass2 = 0
+punctures_solver = none
+bssn_initial_lapse = oochi05
+bssn_initial_shift = zero
+bssn_lapse = 1+log withshift
+bssn_shift = gamma0 withGadv withBadv withShiftadv
+bssn_shiftdriver = 2.0
+bssn_shiftgammacoeff = 0.75
+grid = box
+nxyz = %d
+dxyz = %g
+order_centered = 4
+order_advection = 4
+advection_lopsided = 1
+order_dissipation = 6
+dissipation_factor = 0.1
+evolution_method = rk
+evolution_method_rk = rk4
+dtfac = 0.25
+iterations = %d
+boundary = radiative
+bampi_timer_on = yes
+""" % (nxyz, DX, steps + warmup)
+    work = tempfile.mkdtemp(prefix="bamref_")
+    try:
+        with open(os.path.join(work, "c1.par"), "w") as f:
+            f.write(par)
+        t0 = time.time()
+        r = subprocess.run([bam, "-nt", str(cores), "c1.par"], cwd=work, capture_output=True, text=True)
+        wall = time.time() - t0
+        if r.returncode:
+            return None
+        txt = open(os.path.join(work, "c1", "timer.0")).read()
+        # level-0 timers printed (and reset) after each top-level iteration
+        blocks = re.split(r"Timers after top level iteration (\d+)", txt)
+        ev, rh = {}, {}
+        for i in range(1, len(blocks), 2):
+            it = int(blocks[i])
+            m = re.search(r"^ 0 evolve\s+([\d.]+)\s+(\d+)", blocks[i + 1], re.M)
+            n = re.search(r"^ 0 bssn_rhs\s+([\d.]+)\s+(\d+)", blocks[i + 1], re.M)
+            if m:
+                ev[it] = float(m.group(1))
+            if n:
+                rh[it] = float(n.group(1))
+        last = steps + warmup
+        t_ev = sum(ev[i] for i in range(warmup + 1, last + 1))
+        t_rh = sum(rh[i] for i in range(warmup + 1, last + 1))
+        pts = nxyz ** 3 * RHS_PER_STEP * steps
+        return {"value": pts / t_ev, "rhs_only_value": pts / t_rh if t_rh > 0 else None, "cores": cores,
+                "seconds": t_ev, "wall_s": wall,
+                "sample": "%d RK4 steps (after %d warm-up) of the %d^3-inner puncture box, reference "
+                          "timer 'evolve' (rhs + boundary + RK updates)" % (steps, warmup, nxyz)}
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+def oracle_port_cpu():
+    """Fallback CPU baseline: the oracle restatement, one RK4 step."""
+    from oracle import oracle
+    from baum_b200 import abi, punctures
+    lev, u = punctures.schwarzschild_c1(N_INNER, DX)
+    p = abi.bssn_params()
+    t0 = time.time()
+    oracle.bssn_evolve(lev, u, DT, 1, p)
+    t = time.time() - t0
+    return {"value": PTS_PER_RHS * RHS_PER_STEP / t, "cores": os.cpu_count() or 1,
+            "sample": "1 RK4 step of the 64^3-inner puncture box (oracle restatement, OpenMP)"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    steps = max(1, min(args.steps, 4))
+    warm = 1
+    res = reference_cpu(steps, warm)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/bam not built on this host"}))
+        return
+    line = {"metric": METRIC, "value": res["value"], "unit": UNIT, "impl": "reference", "n_gpus": world,
+            "steps": steps, "warmup": warm, "ms_per_step": 1e3 * res["seconds"] / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (analytic Brill-Lindquist puncture)", "config": CONFIG,
+            "cpu_baseline": {"value": res["value"], "unit": UNIT, "cores": res["cores"], "kind": "reference",
+                             "sample": res["sample"]},
+            "rhs_only_value": res["rhs_only_value"],
+            "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_ours(args, rank, world):
+    import numpy as np
+    import torch
+    from baum_b200 import abi, build, bssn, punctures
+
+    build.build()
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    L = abi.lib()
+    lev, u0 = punctures.schwarzschild_c1(N_INNER, DX)
+    p = abi.bssn_params()
+    dl = bssn.DeviceLevel(lev, dev)
+    u = torch.from_numpy(u0).cuda()
+    flush = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step():
+        bssn.evolve_rk_rk4(dl, u, DT, p, stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = sample_clocks_start() if rank == 0 else None
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for s in range(args.steps):
+        flush.zero_()
+        ev[s][0].record(stream)
+        step()
+        ev[s][1].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+
+    # dominant kernel alone: the interior rhs launch, timed with events on
+    # the launching stream, L2 flushed before each launch
+    r = dl.empty()
+    rev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(5)]
+    bssn.bssn_rhs_movpunc_N(dl, r, u, 0.0, u, p, stream)
+    for a, b in rev:
+        flush.zero_()
+        a.record(stream)
+        bssn.bssn_rhs_movpunc_N(dl, r, u, 0.0, u, p, stream)
+        b.record(stream)
+    torch.cuda.synchronize()
+    rhs_ms = sum(a.elapsed_time(b) for a, b in rev) / len(rev)
+    clocks = sample_clocks_stop(clk) if rank == 0 else None
+
+    # measured FP64 peak on this GPU (no FP64 entry in the peak list)
+    fl, pms = C.c_double(), C.c_float()
+    abi.check(L.nrgpu_probe_fp64_peak(4000, C.byref(fl), C.byref(pms)))
+    fp64_peak = fl.value / 1e12
+
+    # end to end: host state in pinned memory, one RK4 step per call with the
+    # upload and download inside the timed region
+    h = torch.from_numpy(u0.copy()).pin_memory()
+    bssn.evolve_host(dl, h, 1, DT, p)
+    e2e_t = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        bssn.evolve_host(dl, h, 1, DT, p)
+        e2e_t.append(time.perf_counter() - t0)
+    state_bytes = abi.NVARS * lev.npoints * 8
+
+    if dist:
+        t = torch.tensor([ms, sum(e2e_t)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_sum = t[0].item(), t[1].item()
+    else:
+        e2e_sum = sum(e2e_t)
+    if rank != 0:
+        return
+    units = PTS_PER_RHS * RHS_PER_STEP * args.steps * world
+    value = units / (ms * 1e-3)
+    achieved = FLOP_PER_POINT * PTS_PER_RHS / (rhs_ms * 1e-3) / 1e12
+    cpu = reference_cpu(4, 1) if world == 1 and not args.no_cpu else None
+    if cpu:
+        cpu = {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": "reference",
+               "sample": cpu["sample"]}
+    elif world == 1 and not args.no_cpu:
+        c = oracle_port_cpu()
+        cpu = {"value": c["value"], "unit": UNIT, "cores": c["cores"], "kind": "port", "sample": c["sample"]}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic Brill-Lindquist puncture)",
+        "config": CONFIG,
+        "roofline": {"bound": "fp64", "kernel": "bssn_rhs_kernel (interior rhs, one launch = 64^3 points)",
+                     "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
+                     "peak_source": "measured FP64 FMA probe on this GPU (nrgpu_probe_fp64_peak)",
+                     "flop_per_point": FLOP_PER_POINT, "launch_ms": rhs_ms, "traffic": RHS_TRAFFIC_BYTES},
+        "cpu_baseline": cpu,
+        "e2e": {"value": PTS_PER_RHS * RHS_PER_STEP * args.steps * world / e2e_sum, "unit": UNIT,
+                "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
+                "call": "nrgpu_bssn_evolve_host(nsteps=1) from pinned host memory"},
+        "gpu_launches": 10 * args.steps,
+        "clocks": clocks,
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

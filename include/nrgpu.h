@@ -164,6 +164,12 @@ int nrgpu_bssn_evolve_host(nrgpu_level *lev, double *const *host_u, int nsteps,
  * clears it; *flag = 1 if set. */
 int nrgpu_level_nan_flag(nrgpu_level *lev, int *flag);
 
+/* ---- diagnostics -------------------------------------------------------- */
+
+/* Measured FP64 FMA throughput of the current device (FLOP/s, 2 per FMA),
+ * the denominator of the FP64 roofline.  No counterpart in the reference. */
+int nrgpu_probe_fp64_peak(int iters, double *flops_per_s, float *ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -33,6 +33,7 @@ typedef fcdouble real;
 #define RPOW(x, y) fc_pow(x, y)
 #define RVAL(x) fc_val(x)
 #define OMP_FOR
+#define GV(x) ((real)(x))
 #else
 typedef double real;
 #define RLOG(x) log(x)
@@ -40,6 +41,7 @@ typedef double real;
 #define RPOW(x, y) pow(x, y)
 #define RVAL(x) (x)
 #define OMP_FOR _Pragma("omp parallel for schedule(static)")
+#define GV(x) (x)
 #endif
 
 enum { G11, G12, G13, G22, G23, G33, CHI, A11, A12, A13, A22, A23, A33, KK, GA1, GA2, GA3,
@@ -86,7 +88,7 @@ static real d1(const double *f, long ijk, long s, double h, int ord)
   double den = ord == 2 ? 2 : ord == 4 ? 12 : 60;
   real acc = 0;
   for (n = -r; n <= r; n++)
-    if (w[n + r] != 0) acc += w[n + r] * f[ijk + n * s];
+    if (w[n + r] != 0) acc += w[n + r] * GV(f[ijk + n * s]);
   return acc / (den * h);
 }
 
@@ -96,7 +98,7 @@ static real d2(const double *f, long ijk, long s, double h, int ord)
   const double *w = ord == 2 ? C2W2 : ord == 4 ? C2W4 : C2W6;
   double den = ord == 2 ? 1 : ord == 4 ? 12 : 180;
   real acc = 0;
-  for (n = -r; n <= r; n++) acc += w[n + r] * f[ijk + n * s];
+  for (n = -r; n <= r; n++) acc += w[n + r] * GV(f[ijk + n * s]);
   return acc / (den * h * h);
 }
 
@@ -112,7 +114,7 @@ static real d11(const double *f, long ijk, long s1, long s2, double h1, double h
     if (w[a + r] == 0) continue;
     for (b = -r; b <= r; b++) {
       if (w[b + r] == 0) continue;
-      acc += (w[a + r] * w[b + r]) * f[ijk + a * s1 + b * s2];
+      acc += (w[a + r] * w[b + r]) * GV(f[ijk + a * s1 + b * s2]);
     }
   }
   return acc / (den * h1 * den * h2);
@@ -147,7 +149,7 @@ static real adv_apply(const adv_t a[3], const double *f, long ijk)
   real acc = 0;
   int d, n;
   for (d = 0; d < 3; d++)
-    for (n = 0; n < a[d].nt; n++) acc += a[d].c[n] * f[ijk + a[d].off[n]];
+    for (n = 0; n < a[d].nt; n++) acc += a[d].c[n] * GV(f[ijk + a[d].off[n]]);
   return acc;
 }
 
@@ -158,7 +160,7 @@ static real ko(const double *f, long ijk, const long s[3], const double h[3], in
   real acc = 0;
   for (d = 0; d < 3; d++) {
     real t = 0;
-    for (n = -r; n <= r; n++) t += w[n + r] * f[ijk + n * s[d]];
+    for (n = -r; n <= r; n++) t += w[n + r] * GV(f[ijk + n * s[d]]);
     acc += t / h[d];
   }
   /* dissipation4 carries a minus sign, dissipation6 a plus (discretize.m:132-137) */
@@ -698,3 +700,21 @@ int oracle_bssn_evolve(const nrgpu_level_desc *L, double *const *u, double dt, i
   for (s = 0; s < nsteps; s++) e |= oracle_bssn_rk4_step(L, u, dt, p);
   return e;
 }
+
+#ifdef ORACLE_COUNT_FLOPS
+fc_counts g_fc;
+/* FLOPs and transcendental calls of one inner point at distance >= 3 from the
+ * box edge (full order, advection with a non-zero shift, dissipation on) */
+extern "C" void oracle_count_point(const nrgpu_level_desc *L, double *const *u, int i, int j, int k,
+                                   const nrgpu_bssn_params *p, long long *flops, long long *transc)
+{
+  const double h[3] = {L->dx, L->dy, L->dz};
+  int m = L->box[0].m, n = L->box[0].n, o = L->box[0].o;
+  long ijk = i + (long)m * (j + (long)n * k);
+  real r[NV];
+  g_fc.flops = g_fc.transc = 0;
+  bssn_point((const double *const *)u, ijk, i, j, k, m - 1, n - 1, o - 1, 1, m, (long)m * n, h, p, r);
+  *flops = g_fc.flops;
+  *transc = g_fc.transc;
+}
+#endif

@@ -1,0 +1,146 @@
+"""Regenerate the golden fixtures of tests/golden from the reference itself.
+
+Runs the reference CPU code, built single-rank as oracle/_ref/bam by
+oracle/build_ref.py, on small parfiles and stores its raw FP64 dumps
+(oracle/harness/nrharness.c) as compressed .npz files.  Needs the reference
+sources in this container; the fixtures it writes are committed so the tests
+never need the reference at run time.
+
+    python tests/golden/make_golden.py
+"""
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+from oracle import dumpfile  # noqa: E402
+
+BAM = os.path.join(ROOT, "oracle", "_ref", "bam")
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+BSSN_COMMON = """
+bssn_lapse = 1+log withshift
+bssn_shift = gamma0 withGadv withBadv withShiftadv
+bssn_shiftdriver = 2.0
+bssn_shiftgammacoeff = 0.75
+grid = box
+evolution_method = rk
+evolution_method_rk = rk4
+dtfac = 0.25
+boundary = radiative
+dissipation_factor = 0.1
+nrharness_dir = .
+"""
+
+CASES = {
+    # generic smooth data: every term of the rhs is active (advection too)
+    "bssn_fourier_o4": BSSN_COMMON + """
+physics = adm bssn nrharness
+adm_data = Minkowski
+nxyz = 10
+dxyz = 0.5
+order_centered = 4
+order_advection = 4
+advection_lopsided = 1
+order_dissipation = 6
+iterations = 2
+nrharness_dump = 0 2
+nrharness_rhs = yes
+nrharness_data = fourier
+nrharness_amp = 0.05
+nrharness_length = 4.5
+nrharness_seed = 7
+""",
+    "bssn_fourier_o6": BSSN_COMMON + """
+physics = adm bssn nrharness
+adm_data = Minkowski
+nxyz = 10
+dxyz = 0.5
+order_centered = 6
+order_advection = 6
+advection_lopsided6 = 2
+order_dissipation = 6
+iterations = 1
+nrharness_dump = 0 1
+nrharness_rhs = yes
+nrharness_data = fourier
+nrharness_amp = 0.05
+nrharness_length = 4.5
+nrharness_seed = 11
+""",
+    "bssn_fourier_o4_ko4": BSSN_COMMON + """
+physics = adm bssn nrharness
+adm_data = Minkowski
+nxyz = 10
+dxyz = 0.4
+order_centered = 4
+order_advection = 4
+advection_lopsided = 1
+order_dissipation = 4
+iterations = 0
+nrharness_dump = 0
+nrharness_rhs = yes
+nrharness_data = fourier
+nrharness_amp = 0.08
+nrharness_length = 3.6
+nrharness_seed = 3
+""",
+    # single Schwarzschild puncture, precollapsed lapse, zero shift
+    "bssn_punc_o4": BSSN_COMMON + """
+physics = adm bssn punctures nrharness
+mass1 = 1
+mass2 = 0
+punctures_solver = none
+bssn_initial_lapse = oochi05
+bssn_initial_shift = zero
+nxyz = 10
+dxyz = 0.5
+order_centered = 4
+order_advection = 4
+advection_lopsided = 1
+order_dissipation = 6
+iterations = 4
+nrharness_dump = 0 4
+""",
+}
+
+
+def run_case(name, par):
+    work = tempfile.mkdtemp(prefix="golden_")
+    try:
+        with open(os.path.join(work, name + ".par"), "w") as f:
+            f.write(par)
+        r = subprocess.run([BAM, "-nt", "4", name + ".par"], cwd=work, capture_output=True, text=True)
+        if r.returncode:
+            raise RuntimeError(r.stdout[-3000:] + r.stderr[-3000:])
+        arrays = {}
+        meta = None
+        for fn in sorted(os.listdir(work)):
+            if not fn.endswith(".bin"):
+                continue
+            d = dumpfile.read(os.path.join(work, fn))
+            tag = fn[:-4]
+            arrays[tag] = d["data"]
+            if meta is None:
+                meta = d
+        np.savez_compressed(os.path.join(OUT, name + ".npz"), boundary=meta["boundary"],
+                            boxes=np.array(meta["boxes"], dtype=np.float64),
+                            dx=meta["dx"], dt=meta["dt"] if meta["dt"] else 0.25 * meta["dx"],
+                            names=np.array(meta["names"]), **arrays)
+        with open(os.path.join(OUT, name + ".par"), "w") as f:
+            f.write(par.lstrip())
+        print("wrote", name, sorted(arrays))
+    finally:
+        shutil.rmtree(work)
+
+
+if __name__ == "__main__":
+    if not os.path.exists(BAM):
+        sys.exit("oracle/_ref/bam missing: run python oracle/build_ref.py first")
+    for n, p in CASES.items():
+        run_case(n, p)

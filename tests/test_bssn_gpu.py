@@ -1,0 +1,128 @@
+"""Parity of the CUDA BSSN path (through the C ABI) with the reference's
+outputs (golden fixtures) and with the CPU oracle.
+
+Tolerance: 1e-12 relative per variable (max-norm of the difference over the
+max-norm of the reference variable; fields that are round-off noise in the
+reference are compared against a floor of 1e-8, i.e. absolutely)."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden_level, load_golden, relerr
+from baum_b200 import abi, bssn, punctures
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+CASES = {
+    "bssn_fourier_o4": dict(),
+    "bssn_fourier_o6": dict(order_centered=6, order_advection=6, advection_lopsided6=2),
+    "bssn_fourier_o4_ko4": dict(order_dissipation=4, dissfactor=0.1 / 16),
+}
+
+
+def to_dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_rhs_matches_reference_and_oracle(gpu, case):
+    g = load_golden(case)
+    lev = golden_level(g)
+    p = abi.bssn_params(**CASES[case])
+    dl = bssn.DeviceLevel(lev)
+    u = to_dev(g["state_it0_l0"])
+    r = dl.empty()
+    bssn.evolve_rhs(dl, r, u, 0.0, u, p)
+    torch.cuda.synchronize()
+    r = r.cpu().numpy()
+    assert relerr(r, g["rhs_it0_l0"]).max() < TOL
+    ro = oracle.bssn_rhs(lev, np.ascontiguousarray(g["state_it0_l0"]), p)
+    assert relerr(r, ro).max() < TOL
+    assert not dl.nan_flag()
+
+
+@pytest.mark.parametrize("case,steps", [("bssn_fourier_o4", 2), ("bssn_fourier_o6", 1), ("bssn_punc_o4", 4)])
+def test_rk4_matches_reference(gpu, case, steps):
+    g = load_golden(case)
+    lev = golden_level(g)
+    p = abi.bssn_params(**CASES.get(case, {}))
+    dl = bssn.DeviceLevel(lev)
+    u = to_dev(g["state_it0_l0"])
+    for _ in range(steps):
+        bssn.evolve_rk_rk4(dl, u, float(g["dt"]), p)
+    torch.cuda.synchronize()
+    assert relerr(u.cpu().numpy(), g["state_it%d_l0" % steps]).max() < TOL
+
+
+def test_addlinear_matches_oracle(gpu):
+    """c != 0 branch: unew = upre + c*rhs with trace removal and det
+    normalisation (bssn_rhs_movpunc_N.m:432-450)."""
+    g = load_golden("bssn_fourier_o4")
+    lev = golden_level(g)
+    p = abi.bssn_params()
+    dl = bssn.DeviceLevel(lev)
+    u0 = np.ascontiguousarray(g["state_it0_l0"])
+    pre = u0 * 1.01
+    u, up, un = to_dev(u0), to_dev(pre), to_dev(u0)
+    bssn.evolve_rhs(dl, un, up, 0.05, u, p)
+    ro = oracle.bssn_rhs(lev, u0, p, c=0.05, upre=np.ascontiguousarray(pre), out=u0.copy())
+    assert relerr(un.cpu().numpy(), ro).max() < TOL
+
+
+def test_c1_schwarzschild_50_steps_matches_oracle(gpu):
+    """The single-puncture workload at full size: 64^3 inner points, dx=0.25,
+    RK4 with dt = 0.25 dx, 50 steps, every variable within 1e-12."""
+    lev, u0 = punctures.schwarzschild_c1()
+    p = abi.bssn_params()
+    dt = 0.25 * 0.25
+    dl = bssn.DeviceLevel(lev)
+    u = to_dev(u0)
+    for _ in range(50):
+        bssn.evolve_rk_rk4(dl, u, dt, p)
+    torch.cuda.synchronize()
+    ug = u.cpu().numpy()
+    uo = oracle.bssn_evolve(lev, np.ascontiguousarray(u0), dt, 50, p)
+    err = relerr(ug, uo)
+    assert err.max() < TOL, err
+    assert not dl.nan_flag()
+
+
+def test_evolve_host_matches_device_path(gpu):
+    lev, u0 = punctures.schwarzschild_c1(n_inner=24, dx=0.5)
+    p = abi.bssn_params()
+    dl = bssn.DeviceLevel(lev)
+    u = to_dev(u0)
+    for _ in range(3):
+        bssn.evolve_rk_rk4(dl, u, 0.125, p)
+    h = np.ascontiguousarray(u0.copy())
+    bssn.evolve_host(dl, h, 3, 0.125, p)
+    assert np.array_equal(h, u.cpu().numpy())
+
+
+def test_nan_in_state_raises_flag(gpu):
+    """A NaN planted in the input state (host side) is reported by the device
+    flag after the rhs (the reference prints it, check.c:235)."""
+    g = load_golden("bssn_fourier_o4")
+    lev = golden_level(g)
+    p = abi.bssn_params()
+    dl = bssn.DeviceLevel(lev)
+    s = np.ascontiguousarray(g["state_it0_l0"]).copy()
+    s[13, 555] = np.nan
+    u = to_dev(s)
+    r = dl.empty()
+    bssn.evolve_rhs(dl, r, u, 0.0, u, p)
+    assert dl.nan_flag()
+    assert not dl.nan_flag()   # reading clears it
+
+
+def test_bad_arguments_are_refused(gpu):
+    g = load_golden("bssn_fourier_o4")
+    lev = golden_level(g)
+    dl = bssn.DeviceLevel(lev)
+    u = to_dev(g["state_it0_l0"])
+    with pytest.raises(RuntimeError):
+        bssn.evolve_rhs(dl, u.clone(), u, 0.0, u, abi.bssn_params(order_centered=8, order_advection=8))
+    with pytest.raises(RuntimeError):
+        bssn.evolve_rhs(dl, u.clone(), u, 0.0, u, abi.bssn_params(order_advection=6))

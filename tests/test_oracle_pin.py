@@ -1,0 +1,56 @@
+"""The CPU oracle against the reference's own outputs (golden fixtures made by
+tests/golden/make_golden.py from oracle/_ref/bam)."""
+import numpy as np
+import pytest
+
+from conftest import golden_level, load_golden, relerr
+from oracle import oracle
+from baum_b200 import abi, punctures
+
+RHS_CASES = {
+    "bssn_fourier_o4": dict(),
+    "bssn_fourier_o6": dict(order_centered=6, order_advection=6, advection_lopsided6=2),
+    "bssn_fourier_o4_ko4": dict(order_dissipation=4, dissfactor=0.1 / 16),
+}
+
+
+@pytest.mark.parametrize("case", sorted(RHS_CASES))
+def test_oracle_rhs_matches_reference(case):
+    g = load_golden(case)
+    lev = golden_level(g)
+    p = abi.bssn_params(**RHS_CASES[case])
+    u = np.ascontiguousarray(g["state_it0_l0"])
+    r = oracle.bssn_rhs(lev, u, p)
+    err = relerr(r, g["rhs_it0_l0"])
+    assert err.max() < 1e-13, err
+
+
+@pytest.mark.parametrize("case,steps", [("bssn_fourier_o4", 2), ("bssn_fourier_o6", 1), ("bssn_punc_o4", 4)])
+def test_oracle_rk4_matches_reference(case, steps):
+    g = load_golden(case)
+    lev = golden_level(g)
+    over = RHS_CASES.get(case, {})
+    p = abi.bssn_params(**over)
+    u = np.ascontiguousarray(g["state_it0_l0"])
+    oracle.bssn_evolve(lev, u, float(g["dt"]), steps, p)
+    err = relerr(u, g["state_it%d_l0" % steps])
+    assert err.max() < 1e-13, err
+
+
+def test_brill_lindquist_matches_reference_initial_data():
+    g = load_golden("bssn_punc_o4")
+    lev = golden_level(g)
+    u = punctures.brill_lindquist_state(lev, [(1.0, 0.0, 0.0, 0.0)])
+    # Gamma~ of the reference is round-off noise (~1e-16) from adm_to_bssn
+    err = relerr(u, g["state_it0_l0"], floor=1e-3)
+    assert err.max() < 1e-12, err
+
+
+def test_oracle_detects_a_planted_mistake():
+    """A wrong KO factor in the oracle must be visible against the golden rhs
+    (the comparison is sensitive enough to catch a real defect)."""
+    g = load_golden("bssn_fourier_o4")
+    lev = golden_level(g)
+    p = abi.bssn_params(dissfactor=0.1 / 64 * 1.001)
+    r = oracle.bssn_rhs(lev, np.ascontiguousarray(g["state_it0_l0"]), p)
+    assert relerr(r, g["rhs_it0_l0"]).max() > 1e-9
