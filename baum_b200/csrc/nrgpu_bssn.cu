@@ -849,3 +849,149 @@ extern "C" int nrgpu_bssn_rk4_step(nrgpu_level *L, double *const *u, double dt, 
   if ((e = launch_rhs(L, cptrs(V1), V2, cP, U, E4, *p, st, true, true))) return e;
   return nrgpu_bssn_algcon(L, u, p, stream);
 }
+
+// ---- allocation-free RK4 step -------------------------------------------------
+// For callers that cannot allocate device memory themselves (a host code that
+// runs inside a memory pool it does not own, or under a policy that forbids
+// cudaMalloc after start-up): the RK4 step of one box with its three scratch
+// lists in a fixed device array that the library image carries.
+//
+// Limit: NRGPU_NOALLOC_MAX_POINTS points per box (m*n*o), i.e.
+// 3 * 24 * 16384 doubles = 9 MiB of device memory held by every GPU that
+// loads the library, until the process exits.  All calls share the array:
+// calls that overlap on the GPU (different streams, or host threads using the
+// same device) race on it and must be serialised by the caller.
+#define NRGPU_NOALLOC_MAX_POINTS 16384
+static __device__ __align__(256) double g_noalloc_scratch[3 * NRGPU_NV * NRGPU_NOALLOC_MAX_POINTS];
+static __device__ __align__(256) int g_noalloc_status[4];
+
+namespace {
+
+// interior of a single box whose outer layer is the physical boundary
+// (flag.c:23-36): every point with 1 <= i,j,k <= size-2 is an inner point
+__global__ void __launch_bounds__(128) bssn_rhs_box_kernel(CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPtrs acc,
+                                                          Epilogue E, const nrgpu_bssn_params p, BoxGeo box,
+                                                          double dx, double dy, double dz, int *status) {
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = 1 + blockIdx.z;
+  if (i > box.m - 2 || j > box.n - 2 || k > box.o - 2) return;
+  PointCtx P;
+  P.i = i; P.j = j; P.k = k;
+  P.imax = box.m - 1; P.jmax = box.n - 1; P.kmax = box.o - 1;
+  P.st[0] = 1; P.st[1] = box.m; P.st[2] = box.m * box.n;
+  P.ijk = box.noffset + i + box.m * (j + box.n * k);
+  P.h[0] = dx; P.h[1] = dy; P.h[2] = dz;
+  int d = min(min(i, j), k);
+  d = min(d, min(min(P.imax - i, P.jmax - j), P.kmax - k));
+  P.dist = d;
+  const int oc = ladder(p.order_centered, d);
+  if (oc == 0 || oc != ladder(p.order_advection, d)) {
+    atomicOr(status + 1, 1);
+    return;
+  }
+  double r[NRGPU_NV];
+  if (oc == 2) bssn_point<2>(U, P, p, r);
+  else if (oc == 4) bssn_point<4>(U, P, p, r);
+  else bssn_point<6>(U, P, p, r);
+  double s = 0.0;
+#pragma unroll
+  for (int v = 0; v < NRGPU_NV; ++v) s += r[v];
+  if (!isfinite(s)) atomicOr(status, 1);
+  store(r, P.ijk, out, pre, acc, E, p);
+}
+
+// radiative rhs on the outer layer of a single box, one thread per
+// (point, variable); interior points return at once
+__global__ void bssn_surface_kernel(CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPtrs acc, Epilogue E,
+                                    const nrgpu_bssn_params p, BoxGeo b, double dx, double dy, double dz) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long np = (long)b.m * b.n * b.o;
+  if (t >= np * NRGPU_NV) return;
+  const int v = (int)(t % NRGPU_NV);
+  const int q = (int)(t / NRGPU_NV);
+  const int i = q % b.m, j = (q / b.m) % b.n, k = q / (b.m * b.n);
+  if (i > 0 && j > 0 && k > 0 && i < b.m - 1 && j < b.n - 1 && k < b.o - 1) return;
+  const int ccc = b.noffset + q;
+  const int di = 1, dj = b.m, dk = b.m * b.n;
+  const int mcc = i > 0 ? ccc - di : ccc, pcc = i + 1 < b.m ? ccc + di : ccc;
+  const int cmc = j > 0 ? ccc - dj : ccc, cpc = j + 1 < b.n ? ccc + dj : ccc;
+  const int ccm = k > 0 ? ccc - dk : ccc, ccp = k + 1 < b.o ? ccc + dk : ccc;
+  const int Mcc = i > 1 ? mcc - di : ccc, Pcc = i + 2 < b.m ? pcc + di : ccc;
+  const int cMc = j > 1 ? cmc - dj : ccc, cPc = j + 2 < b.n ? cpc + dj : ccc;
+  const int ccM = k > 1 ? ccm - dk : ccc, ccP = k + 2 < b.o ? ccp + dk : ccc;
+  const double xx = b.x0 + i * dx, yy = b.y0 + j * dy, zz = b.z0 + k * dz;
+  const double rr = sqrt(xx * xx + yy * yy + zz * zz);
+  const double vv = p.bc_speed[v], var0 = p.bc_var0[v];
+  const double *var = U.p[v];
+  const double Wx = vv * xx / rr, Wy = vv * yy / rr, Wz = vv * zz / rr;
+  const double delx = computedel(var, Wx, ccc, mcc, Mcc, pcc, Pcc);
+  const double dely = computedel(var, Wy, ccc, cmc, cMc, cpc, cPc);
+  const double delz = computedel(var, Wz, ccc, ccm, ccM, ccp, ccP);
+  double rhs = -vv * (ldg(var + ccc) - var0) / rr;
+  rhs += -(Wx * delx * (1.0 / (2.0 * dx)) + Wy * dely * (1.0 / (2.0 * dy)) + Wz * delz * (1.0 / (2.0 * dz)));
+  acc.p[v][ccc] += E.wacc * rhs;
+  if (E.has_v) out.p[v][ccc] = ldg(pre.p[v] + ccc) + E.cv * rhs;
+}
+
+}  // namespace
+
+// device addresses of the static arrays, looked up once per device
+static double *g_noalloc_ptr[64];
+static int *g_noalloc_status_ptr[64];
+
+extern "C" int nrgpu_bssn_rk4_step_noalloc(const nrgpu_box *box, double dx, double dy, double dz,
+                                           double *const *u, double dt, const nrgpu_bssn_params *p,
+                                           void *stream) {
+  if (!box) return nrgpu_set_error(NRGPU_ERR_ARG, "null box");
+  int e;
+  if ((e = check_params(p))) return e;
+  VarPtrs U;
+  if ((e = fill_ptrs(&U, u, "u"))) return e;
+  if (box->m < 3 || box->n < 3 || box->o < 3 || box->noffset != 0)
+    return nrgpu_set_error(NRGPU_ERR_ARG, "box must be at least 3^3 points with noffset 0");
+  const long np = (long)box->m * box->n * box->o;
+  if (np > NRGPU_NOALLOC_MAX_POINTS)
+    return nrgpu_set_error(NRGPU_ERR_ARG, "box of %ld points exceeds the allocation-free limit of %d points", np,
+                           NRGPU_NOALLOC_MAX_POINTS);
+  if (!(dx > 0.0) || !(dy > 0.0) || !(dz > 0.0)) return nrgpu_set_error(NRGPU_ERR_ARG, "grid spacing must be > 0");
+  int dev = 0;
+  NRGPU_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return nrgpu_set_error(NRGPU_ERR_ARG, "device %d out of range", dev);
+  if (!g_noalloc_ptr[dev]) {
+    // set-up on the first call on this device, with this device current
+    void *sp = nullptr, *st = nullptr;
+    NRGPU_CUDA_TRY(cudaGetSymbolAddress(&sp, g_noalloc_scratch));
+    NRGPU_CUDA_TRY(cudaGetSymbolAddress(&st, g_noalloc_status));
+    g_noalloc_status_ptr[dev] = (int *)st;
+    g_noalloc_ptr[dev] = (double *)sp;
+  }
+  double *scr = g_noalloc_ptr[dev];
+  int *status = g_noalloc_status_ptr[dev];
+  cudaStream_t s = (cudaStream_t)stream;
+  NRGPU_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int) * 4, s));
+  VarPtrs P, V1, V2;
+  for (int v = 0; v < NRGPU_NV; ++v) {
+    P.p[v] = scr + (0 * NRGPU_NV + v) * np;
+    V1.p[v] = scr + (1 * NRGPU_NV + v) * np;
+    V2.p[v] = scr + (2 * NRGPU_NV + v) * np;
+  }
+  const BoxGeo bx{box->m, box->n, box->o, 0, box->x0, box->y0, box->z0};
+  vlcopy_kernel<<<(unsigned)((NRGPU_NV * np + 255) / 256), 256, 0, s>>>(P, cptrs(U), (int)np);
+  const CVarPtrs cP = cptrs(P);
+  const Epilogue Es[4] = {{EPI_RK, 0.0, dt / 6, dt / 2, 1},
+                          {EPI_RK, 0.0, dt / 3, dt / 2, 1},
+                          {EPI_RK, 0.0, dt / 3, dt, 1},
+                          {EPI_RK, 0.0, dt / 6, 0.0, 0}};
+  const CVarPtrs ins[4] = {cP, cptrs(V1), cptrs(V2), cptrs(V1)};
+  const VarPtrs outs[4] = {V1, V2, V1, V2};
+  const dim3 blk(32, 4, 1), grd((box->m - 2 + 31) / 32, (box->n - 2 + 3) / 4, box->o - 2);
+  const unsigned sgrid = (unsigned)((np * NRGPU_NV + 255) / 256);
+  for (int st = 0; st < 4; ++st) {
+    bssn_rhs_box_kernel<<<grd, blk, 0, s>>>(ins[st], outs[st], cP, U, Es[st], *p, bx, dx, dy, dz, status);
+    bssn_surface_kernel<<<sgrid, 256, 0, s>>>(ins[st], outs[st], cP, U, Es[st], *p, bx, dx, dy, dz);
+  }
+  bssn_algcon_kernel<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(U, (int)np, p->subtractA, p->normalizedetg);
+  NRGPU_CUDA_TRY(cudaGetLastError());
+  return NRGPU_OK;
+}

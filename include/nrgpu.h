@@ -164,6 +164,23 @@ int nrgpu_bssn_evolve_host(nrgpu_level *lev, double *const *host_u, int nsteps,
  * clears it; *flag = 1 if set. */
 int nrgpu_level_nan_flag(nrgpu_level *lev, int *flag);
 
+/* One RK4 step of a single box (outer layer = physical boundary, inner
+ * points elsewhere), exactly as nrgpu_bssn_rk4_step, for callers that cannot
+ * allocate device memory: embedded hosts whose device memory is owned by
+ * another runtime's pool, or a code that allocates nothing after start-up.
+ * The library neither allocates nor frees anything in this call; its three
+ * scratch lists live in a fixed device array of the library image, so the
+ * box may hold at most 16384 points (m*n*o; larger boxes are rejected with
+ * NRGPU_ERR_ARG) and every GPU that loads the library holds 9 MiB for it
+ * until exit.  The first call on a device looks up that array's address;
+ * make it before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller.  The caller
+ * passes u (24 device pointers, box->noffset == 0), updated in place.
+ * No counterpart in the reference. */
+int nrgpu_bssn_rk4_step_noalloc(const nrgpu_box *box, double dx, double dy, double dz,
+                                double *const *u, double dt, const nrgpu_bssn_params *p,
+                                void *stream);
+
 /* ---- diagnostics -------------------------------------------------------- */
 
 /* Measured FP64 FMA throughput of the current device (FLOP/s, 2 per FMA),
