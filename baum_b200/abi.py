@@ -8,7 +8,7 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIBPATH = os.path.join(HERE, "libnrgpu.so")
+LIBPATH = os.environ.get("NRGPU_LIBRARY") or os.path.join(HERE, "libnrgpu.so")
 NVARS = 24
 
 # BSSN evolve-list order (reference bssn.c:315-322)

@@ -132,10 +132,13 @@ struct PointCtx {
 };
 
 // ---- the per-point right-hand side -------------------------------------------
-template <int ORD>
+template <int ORD, int CSY = 0, int CSZ = 0>
 __device__ __forceinline__ void bssn_point(const CVarPtrs &U, const PointCtx &P,
                                            const nrgpu_bssn_params &p, double r[NRGPU_NV]) {
   const int x = P.ijk;
+  // strides: compile-time when the box size is known, so taps fold into
+  // immediate load offsets
+#define STR(c_) ((c_) == 0 ? 1 : (CSY > 0 ? ((c_) == 1 ? CSY : CSZ) : P.st[(c_)]))
   const double o1[3] = {1.0 / (den1<ORD>() * P.h[0]), 1.0 / (den1<ORD>() * P.h[1]),
                         1.0 / (den1<ORD>() * P.h[2])};
 
@@ -165,7 +168,7 @@ __device__ __forceinline__ void bssn_point(const CVarPtrs &U, const PointCtx &P,
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
-      for (int a = 0; a < 6; ++a) dg[c][a] = o1[c] * d1n<ORD>(U.p[G11 + a], x, P.st[c]);
+      for (int a = 0; a < 6; ++a) dg[c][a] = o1[c] * d1n<ORD>(U.p[G11 + a], x, STR(c));
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -215,8 +218,8 @@ __device__ __forceinline__ void bssn_point(const CVarPtrs &U, const PointCtx &P,
         const double w = (c == d ? -0.5 : -1.0) * gi[sy(c, d)] * (c == d ? o2[c] : o1[c] * o1[d]);
 #pragma unroll
         for (int a = 0; a < 6; ++a) {
-          const double dd = c == d ? d2n<ORD>(U.p[G11 + a], x, P.st[c])
-                                   : d11n<ORD>(U.p[G11 + a], x, P.st[c], P.st[d]);
+          const double dd = c == d ? d2n<ORD>(U.p[G11 + a], x, STR(c))
+                                   : d11n<ORD>(U.p[G11 + a], x, STR(c), STR(d));
           Rt[a] += w * dd;
         }
       }
@@ -225,7 +228,7 @@ __device__ __forceinline__ void bssn_point(const CVarPtrs &U, const PointCtx &P,
 #pragma unroll
     for (int b = 0; b < 3; ++b)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) dG[b][c] = o1[b] * d1n<ORD>(U.p[GA1 + c], x, P.st[b]);
+      for (int c = 0; c < 3; ++c) dG[b][c] = o1[b] * d1n<ORD>(U.p[GA1 + c], x, STR(b));
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -247,7 +250,7 @@ __device__ __forceinline__ void bssn_point(const CVarPtrs &U, const PointCtx &P,
   const double psim4 = exp(-4.0 * f);
   double df[3];
 #pragma unroll
-  for (int a = 0; a < 3; ++a) df[a] = oocp * (o1[a] * d1n<ORD>(U.p[CHI], x, P.st[a])) / chig;
+  for (int a = 0; a < 3; ++a) df[a] = oocp * (o1[a] * d1n<ORD>(U.p[CHI], x, STR(a))) / chig;
   double dfdf = 0.0;
 #pragma unroll
   for (int a = 0; a < 3; ++a)
@@ -261,8 +264,8 @@ __device__ __forceinline__ void bssn_point(const CVarPtrs &U, const PointCtx &P,
     for (int a = 0; a < 3; ++a)
 #pragma unroll
       for (int b = a; b < 3; ++b) {
-        const double ddchi = a == b ? o2[a] * d2n<ORD>(U.p[CHI], x, P.st[a])
-                                    : o1[a] * o1[b] * d11n<ORD>(U.p[CHI], x, P.st[a], P.st[b]);
+        const double ddchi = a == b ? o2[a] * d2n<ORD>(U.p[CHI], x, STR(a))
+                                    : o1[a] * o1[b] * d11n<ORD>(U.p[CHI], x, STR(a), STR(b));
         double t = oocp * ddchi / chig - p.chipsipower * df[a] * df[b];
         t -= gam[0][sy(a, b)] * df[0] + gam[1][sy(a, b)] * df[1] + gam[2][sy(a, b)] * df[2];
         cddf[sy(a, b)] = t;
@@ -281,7 +284,7 @@ __device__ __forceinline__ void bssn_point(const CVarPtrs &U, const PointCtx &P,
   // derivatives of the lapse
   double da[3], cdda[6];
 #pragma unroll
-  for (int a = 0; a < 3; ++a) da[a] = o1[a] * d1n<ORD>(U.p[ALPHA], x, P.st[a]);
+  for (int a = 0; a < 3; ++a) da[a] = o1[a] * d1n<ORD>(U.p[ALPHA], x, STR(a));
   {
     const double o2[3] = {1.0 / (den2<ORD>() * P.h[0] * P.h[0]), 1.0 / (den2<ORD>() * P.h[1] * P.h[1]),
                           1.0 / (den2<ORD>() * P.h[2] * P.h[2])};
@@ -295,8 +298,8 @@ __device__ __forceinline__ void bssn_point(const CVarPtrs &U, const PointCtx &P,
 #pragma unroll
       for (int b = a; b < 3; ++b) {
         const int ab = sy(a, b);
-        double t = a == b ? o2[a] * d2n<ORD>(U.p[ALPHA], x, P.st[a])
-                          : o1[a] * o1[b] * d11n<ORD>(U.p[ALPHA], x, P.st[a], P.st[b]);
+        double t = a == b ? o2[a] * d2n<ORD>(U.p[ALPHA], x, STR(a))
+                          : o1[a] * o1[b] * d11n<ORD>(U.p[ALPHA], x, STR(a), STR(b));
         t -= gam[0][ab] * da[0] + gam[1][ab] * da[1] + gam[2][ab] * da[2];
         cdda[ab] = t - 2.0 * (df[a] * da[b] + df[b] * da[a] - g[ab] * dfda);
       }
@@ -341,7 +344,7 @@ __device__ __forceinline__ void bssn_point(const CVarPtrs &U, const PointCtx &P,
   {
     double dK[3];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) dK[a] = p.forceKzerofactor * (o1[a] * d1n<ORD>(U.p[KK], x, P.st[a]));
+    for (int a = 0; a < 3; ++a) dK[a] = p.forceKzerofactor * (o1[a] * d1n<ORD>(U.p[KK], x, STR(a)));
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       double t = 0.0, s = 0.0;
@@ -366,7 +369,7 @@ __device__ __forceinline__ void bssn_point(const CVarPtrs &U, const PointCtx &P,
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) db[a][c] = o1[a] * d1n<ORD>(U.p[BETA1 + c], x, P.st[a]);
+      for (int c = 0; c < 3; ++c) db[a][c] = o1[a] * d1n<ORD>(U.p[BETA1 + c], x, STR(a));
     const double divbeta = db[0][0] + db[1][1] + db[2][2];
     const double totdivbeta = (2.0 / 3.0) * divbeta;
 #pragma unroll
@@ -393,8 +396,8 @@ __device__ __forceinline__ void bssn_point(const CVarPtrs &U, const PointCtx &P,
       for (int c = b; c < 3; ++c)
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-          const double dd = b == c ? o2[b] * d2n<ORD>(U.p[BETA1 + a], x, P.st[b])
-                                   : o1[b] * o1[c] * d11n<ORD>(U.p[BETA1 + a], x, P.st[b], P.st[c]);
+          const double dd = b == c ? o2[b] * d2n<ORD>(U.p[BETA1 + a], x, STR(b))
+                                   : o1[b] * o1[c] * d11n<ORD>(U.p[BETA1 + a], x, STR(b), STR(c));
           trddb[a] += (b == c ? 1.0 : 2.0) * gi[sy(b, c)] * dd;
           // d_b d_c beta^a contributes to divdb[b] when c == a and to divdb[c] when b == a
           if (c == a) divdb[b] += dd;
@@ -435,7 +438,7 @@ __device__ __forceinline__ void bssn_point(const CVarPtrs &U, const PointCtx &P,
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       const double w = ldg(U.p[BETA1 + d] + x) / P.h[d];
-      ad[d] = adv_dir(idx[d], mx[d], w, ORD, lop, P.st[d]);
+      ad[d] = adv_dir(idx[d], mx[d], w, ORD, lop, STR(d));
       const int ws = w < 0 ? -1 : (w > 0 ? 1 : 0);
       cw[d] = -ws * w * oad;
     }
@@ -460,30 +463,32 @@ __device__ __forceinline__ void bssn_point(const CVarPtrs &U, const PointCtx &P,
   // Kreiss-Oliger dissipation where the full stencil fits
   if ((p.order_dissipation == 4 && P.dist >= 2) || (p.order_dissipation == 6 && P.dist >= 3)) {
     const double ooh[3] = {1.0 / P.h[0], 1.0 / P.h[1], 1.0 / P.h[2]};
+    const int kst[3] = {STR(0), STR(1), STR(2)};
     const double e = p.dissfactor;
     if (p.order_dissipation == 6) {
 #pragma unroll
       for (int a = 0; a < 6; ++a) {
-        r[G11 + a] += e * ko_sum<6>(U.p[G11 + a], x, P.st, ooh);
-        r[A11 + a] += e * ko_sum<6>(U.p[A11 + a], x, P.st, ooh);
+        r[G11 + a] += e * ko_sum<6>(U.p[G11 + a], x, kst, ooh);
+        r[A11 + a] += e * ko_sum<6>(U.p[A11 + a], x, kst, ooh);
       }
 #pragma unroll
-      for (int a = 0; a < 3; ++a) r[GA1 + a] += e * ko_sum<6>(U.p[GA1 + a], x, P.st, ooh);
-      r[KK] += e * ko_sum<6>(U.p[KK], x, P.st, ooh);
-      r[CHI] += e * ko_sum<6>(U.p[CHI], x, P.st, ooh);
+      for (int a = 0; a < 3; ++a) r[GA1 + a] += e * ko_sum<6>(U.p[GA1 + a], x, kst, ooh);
+      r[KK] += e * ko_sum<6>(U.p[KK], x, kst, ooh);
+      r[CHI] += e * ko_sum<6>(U.p[CHI], x, kst, ooh);
     } else {
 #pragma unroll
       for (int a = 0; a < 6; ++a) {
-        r[G11 + a] += e * ko_sum<4>(U.p[G11 + a], x, P.st, ooh);
-        r[A11 + a] += e * ko_sum<4>(U.p[A11 + a], x, P.st, ooh);
+        r[G11 + a] += e * ko_sum<4>(U.p[G11 + a], x, kst, ooh);
+        r[A11 + a] += e * ko_sum<4>(U.p[A11 + a], x, kst, ooh);
       }
 #pragma unroll
-      for (int a = 0; a < 3; ++a) r[GA1 + a] += e * ko_sum<4>(U.p[GA1 + a], x, P.st, ooh);
-      r[KK] += e * ko_sum<4>(U.p[KK], x, P.st, ooh);
-      r[CHI] += e * ko_sum<4>(U.p[CHI], x, P.st, ooh);
+      for (int a = 0; a < 3; ++a) r[GA1 + a] += e * ko_sum<4>(U.p[GA1 + a], x, kst, ooh);
+      r[KK] += e * ko_sum<4>(U.p[KK], x, kst, ooh);
+      r[CHI] += e * ko_sum<4>(U.p[CHI], x, kst, ooh);
     }
   }
   r[KK] *= p.forceKzerofactor;
+#undef STR
 }
 
 // ---- epilogues ----------------------------------------------------------------
@@ -550,6 +555,9 @@ __device__ __forceinline__ int ladder(int order, int d) {
 // ---- kernels ----------------------------------------------------------------
 // one thread per point of the box interior (i,j,k in [1, m-2]); inner points
 // (flag 0) only, the flagged ones are handled by bssn_flagged_kernel
+// CSY, CSZ: the box strides dj = m and dk = m n when known at compile time
+// (0 = read them from the box)
+template <int CSY = 0, int CSZ = 0>
 __global__ void __launch_bounds__(128) bssn_rhs_kernel(CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPtrs acc,
                                                       Epilogue E, const nrgpu_bssn_params p, BoxGeo box,
                                                       const int *__restrict__ boundary, double dx, double dy,
@@ -575,9 +583,9 @@ __global__ void __launch_bounds__(128) bssn_rhs_kernel(CVarPtrs U, VarPtrs out, 
     return;
   }
   double r[NRGPU_NV];
-  if (oc == 2) bssn_point<2>(U, P, p, r);
-  else if (oc == 4) bssn_point<4>(U, P, p, r);
-  else bssn_point<6>(U, P, p, r);
+  if (oc == 2) bssn_point<2, CSY, CSZ>(U, P, p, r);
+  else if (oc == 4) bssn_point<4, CSY, CSZ>(U, P, p, r);
+  else bssn_point<6, CSY, CSZ>(U, P, p, r);
   double s = 0.0;
 #pragma unroll
   for (int v = 0; v < NRGPU_NV; ++v) s += r[v];
@@ -695,6 +703,7 @@ __global__ void vlcopy_kernel(VarPtrs dst, CVarPtrs src, int npoints) {
   dst.p[v][q] = src.p[v][q];
 }
 
+
 }  // namespace
 
 // ---- host side ----------------------------------------------------------------
@@ -737,8 +746,17 @@ static int launch_rhs(nrgpu_level *L, const CVarPtrs &U, const VarPtrs &out, con
       if (bx.m < 3 || bx.n < 3 || bx.o < 3) continue;
       dim3 blk(32, 4, 1);
       dim3 grd((bx.m - 2 + 31) / 32, (bx.n - 2 + 3) / 4, bx.o - 2);
-      bssn_rhs_kernel<<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
-                                           L->d_status);
+      // box strides as compile-time constants for the sizes of the standard
+      // workloads: every stencil tap becomes one load with an immediate offset
+      if (bx.m == 66 && bx.n == 66)
+        bssn_rhs_kernel<66, 66 * 66><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy,
+                                                           L->dz, L->d_status);
+      else if (bx.m == 162 && bx.n == 162)
+        bssn_rhs_kernel<162, 162 * 162><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx,
+                                                              L->dy, L->dz, L->d_status);
+      else
+        bssn_rhs_kernel<<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
+                                             L->d_status);
     }
   }
   if (flagged && L->nflagpts > 0) {

@@ -14,15 +14,16 @@ from baum_b200 import abi
 HERE = os.path.dirname(os.path.abspath(__file__))
 SO = os.path.join(HERE, "liboracle.so")
 SRC = os.path.join(HERE, "nr_oracle.c")
+MGSRC = os.path.join(HERE, "mg_oracle.c")
 
 
 def build(force=False):
     """Compile the restatement with gcc (-O2, OpenMP, no fast-math)."""
-    deps = [SRC, os.path.join(HERE, "..", "include", "nrgpu.h")]
+    deps = [SRC, MGSRC, os.path.join(HERE, "..", "include", "nrgpu.h")]
     if not force and os.path.exists(SO) and all(os.path.getmtime(SO) >= os.path.getmtime(d) for d in deps):
         return SO
     cmd = ["gcc", "-O2", "-std=gnu99", "-fopenmp", "-fPIC", "-shared", "-ffp-contract=off",
-           SRC, "-o", SO, "-lm"]
+           SRC, MGSRC, "-o", SO, "-lm"]
     subprocess.run(cmd, check=True)
     return SO
 
