@@ -103,6 +103,23 @@ def set_bc_from_gauge(p):
     p.bc_speed[:] = speed
 
 
+class MgParams(C.Structure):
+    _fields_ = [("npre", C.c_int), ("npost", C.c_int), ("exact_nmin", C.c_int), ("exact_nmax", C.c_int),
+                ("vcycle_nmin", C.c_int), ("vcycle_nmax", C.c_int), ("fullV", C.c_int),
+                ("size_nmin", C.c_int), ("levels_nmax", C.c_int), ("tol", C.c_double),
+                ("falloff", C.c_double), ("batch", C.c_int)]
+
+
+def mg_params(**over):
+    """The puncture-solve settings of the binary-puncture workload:
+    mg_relax_npre = npost = 3, mg_exact_nmin/nmax = 10/200, mg_size_nmin = 4,
+    mg_vcycle_nmax = 2000, full-V cycling, tolerance 1e-10, Robin falloff 1."""
+    p = MgParams(3, 3, 10, 200, 0, 2000, 1, 4, -1, 1e-10, 1.0, 8)
+    for k, v in over.items():
+        setattr(p, k, v)
+    return p
+
+
 class Level:
     """Host-side description of a level (keeps the ctypes arrays alive)."""
 
@@ -179,6 +196,13 @@ def lib():
         "nrgpu_bssn_evolve_host": (C.c_int, [vp, pp, C.c_int, C.c_double, C.POINTER(BssnParams)]),
         "nrgpu_level_nan_flag": (C.c_int, [vp, C.POINTER(C.c_int)]),
         "nrgpu_probe_fp64_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_float)]),
+        "nrgpu_mg_params_default": (None, [C.POINTER(MgParams)]),
+        "nrgpu_mg_create": (C.c_int, [C.c_int, C.c_double, C.POINTER(MgParams), C.POINTER(vp)]),
+        "nrgpu_mg_destroy": (C.c_int, [vp]),
+        "nrgpu_mg_solve": (C.c_int, [vp, vp, vp, vp, C.POINTER(C.c_int), C.POINTER(C.c_double), vp]),
+        "nrgpu_puncture_coefficients": (C.c_int, [C.c_int, C.c_double, C.c_int, C.POINTER(C.c_double),
+                                                  C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                                  C.POINTER(C.c_double), vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

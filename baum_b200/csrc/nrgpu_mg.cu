@@ -1,0 +1,657 @@
+// nrgpu_mg.cu -- the puncture initial-data multigrid on B200 (FP64).
+//
+// Restates the reference's FAS multigrid for the Hamiltonian constraint in
+// puncture form, L(u) = Laplace(u) + b (1 + a (1+u))^-7 = 0
+// (PunctureSolve.c:21-138; multigrid.c:35-123; solve.c:20-161;
+// fasmg.c:41-122; relax.c:174-190; residual.c:13-75;
+// restrictprolong.c:21-122; exactsolve.c:18-77; makestack.c:36-170;
+// robin.c:29-223), for one cubic box with a Robin outer boundary.
+//
+// Device design:
+//  * every stack level is a cube of m^3 points stored x fastest; the
+//    relaxation is undamped Jacobi, done as ping-pong between two arrays
+//    (the reference copies u to v and writes u; the values are the same);
+//  * the Robin condition is a gather over the boundary points with the normal
+//    neighbour and the factors 1-c, 1+c precomputed at set-up;
+//  * the coarse-grid right-hand side of FAS, fH = R fh + L R uh - R L uh,
+//    is one fused kernel;
+//  * the coarsest level (4^3 .. 10^3 points) is solved "exactly" by one
+//    thread block that sweeps, checks its residual and stops on the device;
+//  * residual norms are two-pass deterministic block reductions (warp
+//    shuffles, then one block) into a device scalar;
+//  * a device flag marks convergence of the finest level: every kernel of a
+//    V-cycle returns at once when it is set, so cycles are enqueued in
+//    batches (and captured as a CUDA graph) and the host reads the flag and
+//    the cycle counter once per batch.  The cycle count is exact.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#include "nrgpu_common.cuh"
+
+namespace {
+
+struct MgLevel {
+  int m;
+  long np;
+  double dx, x0;
+  double *u, *u2, *v, *w, *f, *a, *b;  // u2: ping-pong partner of u
+  int nb;                              // boundary points
+  int *bidx, *bnrm;                    // boundary point, its Robin normal neighbour
+  double *bc1, *bc2;                   // 1-c, 1+c of the u condition (far limit 0)
+};
+
+struct MgStatus {
+  double res;       // last finest-level residual (RMS over inner points)
+  int done;         // finest level converged: the rest of the batch is skipped
+  int ncycles;      // V cycles performed on the level being cycled
+  int exact_sweeps; // sweeps of the last coarsest solve
+  int pad;
+};
+
+constexpr int RB = 256;  // threads per block of the grid kernels
+
+__device__ __forceinline__ bool inner(int i, int j, int k, int m) {
+  return i > 0 && j > 0 && k > 0 && i < m - 1 && j < m - 1 && k < m - 1;
+}
+
+// Robin / Dirichlet gather on the boundary (set_boundary_robin): with far
+// limit 0 the Robin value is u_n (1-c)/(1+c); falloff 0 gives -u_n
+__global__ void robin_kernel(double *u, const int *__restrict__ bidx, const int *__restrict__ bnrm,
+                             const double *__restrict__ c1, const double *__restrict__ c2, int nb, int dirichlet,
+                             const int *__restrict__ done) {
+  if (done && *done) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nb) return;
+  const double un = u[bnrm[t]];
+  u[bidx[t]] = dirichlet ? -un : un * c1[t] / c2[t];
+}
+
+// the puncture operator at an inner point
+__device__ __forceinline__ double lop_point(const double *__restrict__ u, long q, int m, double cc, double cx,
+                                            double a, double b) {
+  const long mm = (long)m * m;
+  return cc * u[q] + cx * (u[q - 1] + u[q + 1]) + cx * (u[q - m] + u[q + m]) + cx * (u[q - mm] + u[q + mm]) +
+         b * pow(1.0 + a * (1.0 + u[q]), -7.0);
+}
+
+// one Jacobi sweep un = uo + (f - L uo)/L_ii on inner points (Lpuncture_GS)
+__global__ void jacobi_kernel(const double *__restrict__ uo, double *__restrict__ un, const double *__restrict__ f,
+                              const double *__restrict__ a, const double *__restrict__ b, int m, double cx,
+                              const int *__restrict__ done) {
+  if (done && *done) return;
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long np = (long)m * m * m;
+  if (q >= np) return;
+  const int i = q % m, j = (q / m) % m, k = q / ((long)m * m);
+  if (!inner(i, j, k, m)) return;
+  const double cc = -2.0 * (cx + cx + cx);
+  const double aq = a[q], bq = b[q], uq = uo[q];
+  const double lu = lop_point(uo, q, m, cc, cx, aq, bq);
+  const double lii = cc - 7.0 * bq * aq * pow(1.0 + aq * (1.0 + uq), -8.0);
+  un[q] = uq + (f[q] - lu) / lii;
+}
+
+// lu = L u on inner points (Lpuncture_nonlin, after its Robin call)
+__global__ void lop_kernel(const double *__restrict__ u, double *__restrict__ lu, const double *__restrict__ a,
+                           const double *__restrict__ b, int m, double cx, const int *__restrict__ done) {
+  if (done && *done) return;
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long np = (long)m * m * m;
+  if (q >= np) return;
+  const int i = q % m, j = (q / m) % m, k = q / ((long)m * m);
+  if (!inner(i, j, k, m)) return;
+  lu[q] = lop_point(u, q, m, -2.0 * (cx + cx + cx), cx, a[q], b[q]);
+}
+
+// block partial sums of (L u - f)^2 over inner points
+__global__ void residual_partial_kernel(const double *__restrict__ u, const double *__restrict__ f,
+                                        const double *__restrict__ a, const double *__restrict__ b, int m,
+                                        double cx, double *partial, const int *__restrict__ done) {
+  if (done && *done) return;
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long np = (long)m * m * m;
+  double s = 0.0;
+  if (q < np) {
+    const int i = q % m, j = (q / m) % m, k = q / ((long)m * m);
+    if (inner(i, j, k, m)) {
+      const double r = lop_point(u, q, m, -2.0 * (cx + cx + cx), cx, a[q], b[q]) - f[q];
+      s = r * r;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  __shared__ double ws[RB / 32];
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < RB / 32 ? ws[threadIdx.x] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+  }
+}
+
+// final reduction, RMS over the n inner points; when tol >= 0 this is the
+// convergence test of a V-cycle loop: res <= tol sets done, else counts a cycle
+__global__ void residual_final_kernel(const double *__restrict__ partial, int nparts, long ninner, MgStatus *st,
+                                      double tol, int count, int vnmax) {
+  if (st->done) return;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) s += partial[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  __shared__ double ws[32];
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += ws[w];
+    const double res = sqrt(t / (double)ninner);
+    st->res = res;
+    if (count) {
+      if (res <= tol) st->done = 1;        // converged: no further cycle
+      else if (st->ncycles >= vnmax) st->done = 2;  // cycle budget spent
+      else st->ncycles += 1;               // one more cycle follows
+    }
+  }
+}
+
+// 8-point average of the fine children of inner coarse points
+__global__ void restrict_kernel(const double *__restrict__ fv, double *__restrict__ cv, int mf, int mc, int off,
+                                const int *__restrict__ done) {
+  if (done && *done) return;
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long np = (long)mc * mc * mc;
+  if (q >= np) return;
+  const int I = q % mc, J = (q / mc) % mc, K = q / ((long)mc * mc);
+  if (!inner(I, J, K, mc)) return;
+  const long mf2 = (long)mf * mf;
+  const long f0 = (long)(2 * I - off) + mf * (long)(2 * J - off) + mf2 * (long)(2 * K - off);
+  cv[q] = 0.125 * (fv[f0] + fv[f0 + 1 + mf + mf2] + fv[f0 + 1] + fv[f0 + mf] + fv[f0 + mf2] + fv[f0 + 1 + mf] +
+                   fv[f0 + 1 + mf2] + fv[f0 + mf + mf2]);
+}
+
+// FAS coarse right-hand side at inner coarse points (finetocoarse):
+// fH = R fh + (L uH - R L uh), lu_h = L uh already on the fine level
+__global__ void coarse_rhs_kernel(const double *__restrict__ luh, const double *__restrict__ fh,
+                                  const double *__restrict__ uH, double *__restrict__ fH,
+                                  const double *__restrict__ aH, const double *__restrict__ bH, int mf, int mc,
+                                  int off, double cxH, const int *__restrict__ done) {
+  if (done && *done) return;
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long np = (long)mc * mc * mc;
+  if (q >= np) return;
+  const int I = q % mc, J = (q / mc) % mc, K = q / ((long)mc * mc);
+  if (!inner(I, J, K, mc)) return;
+  const long mf2 = (long)mf * mf;
+  const long f0 = (long)(2 * I - off) + mf * (long)(2 * J - off) + mf2 * (long)(2 * K - off);
+  const double Rlu = 0.125 * (luh[f0] + luh[f0 + 1 + mf + mf2] + luh[f0 + 1] + luh[f0 + mf] + luh[f0 + mf2] +
+                              luh[f0 + 1 + mf] + luh[f0 + 1 + mf2] + luh[f0 + mf + mf2]);
+  const double Rf = 0.125 * (fh[f0] + fh[f0 + 1 + mf + mf2] + fh[f0 + 1] + fh[f0 + mf] + fh[f0 + mf2] +
+                             fh[f0 + 1 + mf] + fh[f0 + 1 + mf2] + fh[f0 + mf + mf2]);
+  const double luH = lop_point(uH, q, mc, -2.0 * (cxH + cxH + cxH), cxH, aH[q], bH[q]);
+  fH[q] = Rf + (luH - Rlu);
+}
+
+// wH = uH (all points), vH = uH - wH helpers
+__global__ void copy_kernel(const double *__restrict__ s, double *__restrict__ d, long n, const int *__restrict__ done) {
+  if (done && *done) return;
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < n) d[q] = s[q];
+}
+__global__ void sub_inner_kernel(const double *__restrict__ x, const double *__restrict__ y, double *__restrict__ r,
+                                 int m, const int *__restrict__ done) {
+  if (done && *done) return;
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (long)m * m * m) return;
+  const int i = q % m, j = (q / m) % m, k = q / ((long)m * m);
+  if (inner(i, j, k, m)) r[q] = x[q] - y[q];
+}
+
+// trilinear prolongation of the coarse correction, added to the inner fine
+// points (mg_prolong_var + add); weights 1/4, 3/4 from the cell-centred
+// staggering, coarse index ci = floor((i + off') / 2)
+__global__ void prolong_add_kernel(const double *__restrict__ cv, double *__restrict__ uf, int mf, int mc,
+                                   double fx0, double fdx, double cx0, double cdx, int add,
+                                   const int *__restrict__ done) {
+  if (done && *done) return;
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (long)mf * mf * mf) return;
+  const int i = q % mf, j = (q / mf) % mf, k = q / ((long)mf * mf);
+  if (!inner(i, j, k, mf)) return;
+  const double xf = fx0 + i * fdx, yf = fx0 + j * fdx, zf = fx0 + k * fdx;
+  const int ci = (int)((xf - cx0) / cdx), cj = (int)((yf - cx0) / cdx), ck = (int)((zf - cx0) / cdx);
+  const double kx1 = (xf - (cx0 + ci * cdx)) / cdx, ky1 = (yf - (cx0 + cj * cdx)) / cdx,
+               kz1 = (zf - (cx0 + ck * cdx)) / cdx;
+  const double kx0 = 1 - kx1, ky0 = 1 - ky1, kz0 = 1 - kz1;
+  const long mc2 = (long)mc * mc;
+  const long c0 = ci + (long)mc * cj + mc2 * ck;
+  const double p = kx0 * ky0 * kz0 * cv[c0] + kx1 * ky0 * kz0 * cv[c0 + 1] + kx0 * ky1 * kz0 * cv[c0 + mc] +
+                   kx1 * ky1 * kz0 * cv[c0 + 1 + mc] + kx0 * ky0 * kz1 * cv[c0 + mc2] +
+                   kx1 * ky0 * kz1 * cv[c0 + 1 + mc2] + kx0 * ky1 * kz1 * cv[c0 + mc + mc2] +
+                   kx1 * ky1 * kz1 * cv[c0 + 1 + mc + mc2];
+  uf[q] = add ? uf[q] + p : p;
+}
+
+// "exact" solve of the coarsest level in one thread block (exactsolve):
+// findres, then Jacobi sweeps (each followed by the Robin condition) until
+// the residual drops below tol/10 after at least nmin sweeps, at most nmax
+__device__ void block_robin(double *u, const int *bidx, const int *bnrm, const double *c1, const double *c2, int nb) {
+  for (int t = threadIdx.x; t < nb; t += blockDim.x) u[bidx[t]] = u[bnrm[t]] * c1[t] / c2[t];
+}
+__device__ double block_residual(const double *u, const double *f, const double *a, const double *b, int m, double cx,
+                                 double *red) {
+  const long np = (long)m * m * m;
+  double s = 0.0;
+  long n = 0;
+  for (long q = threadIdx.x; q < np; q += blockDim.x) {
+    const int i = q % m, j = (q / m) % m, k = q / ((long)m * m);
+    if (!inner(i, j, k, m)) continue;
+    const double r = lop_point(u, q, m, -2.0 * (cx + cx + cx), cx, a[q], b[q]) - f[q];
+    s += r * r;
+  }
+  n = (long)(m - 2) * (m - 2) * (m - 2);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+  __syncthreads();
+  return sqrt(t / (double)n);
+}
+__global__ void exact_solve_kernel(double *u, double *u2, const double *f, const double *a, const double *b, int m,
+                                   double cx, const int *bidx, const int *bnrm, const double *c1, const double *c2,
+                                   int nb, int nmin, int nmax, double tol10, MgStatus *st) {
+  if (st->done) return;
+  __shared__ double red[32];
+  const long np = (long)m * m * m;
+  // findres applies the Robin condition to u first (Lpuncture_nonlin)
+  block_robin(u, bidx, bnrm, c1, c2, nb);
+  __syncthreads();
+  double *uo = u, *un = u2;
+  int i;
+  for (i = 1; i <= nmax; ++i) {
+    const double cc = -2.0 * (cx + cx + cx);
+    for (long q = threadIdx.x; q < np; q += blockDim.x) {
+      const int ii = q % m, jj = (q / m) % m, kk = q / ((long)m * m);
+      if (!inner(ii, jj, kk, m)) { un[q] = uo[q]; continue; }
+      const double lu = lop_point(uo, q, m, cc, cx, a[q], b[q]);
+      const double lii = cc - 7.0 * b[q] * a[q] * pow(1.0 + a[q] * (1.0 + uo[q]), -8.0);
+      un[q] = uo[q] + (f[q] - lu) / lii;
+    }
+    __syncthreads();
+    block_robin(un, bidx, bnrm, c1, c2, nb);
+    __syncthreads();
+    double *t = uo; uo = un; un = t;
+    if (i >= nmin) {
+      const double r = block_residual(uo, f, a, b, m, cx, red);
+      if (r < tol10) break;
+    }
+  }
+  // leave the result in u
+  if (uo != u) {
+    for (long q = threadIdx.x; q < np; q += blockDim.x) u[q] = uo[q];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) st->exact_sweeps = i;
+}
+
+__global__ void robin_factors_kernel(const int *bidx, const int *bnrm, double *c1, double *c2, int nb, int m, double x0,
+                                     double dx, double falloff) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nb) return;
+  const int q = bidx[t], n = bnrm[t];
+  const int i = q % m, j = (q / m) % m, k = q / (m * m);
+  const int ni = n % m, nj = (n / m) % m, nk = n / (m * m);
+  const double x1 = x0 + i * dx, y1 = x0 + j * dx, z1 = x0 + k * dx;
+  const double xa = x0 + ni * dx, ya = x0 + nj * dx, za = x0 + nk * dx;
+  const double x = 0.5 * (x1 + xa), y = 0.5 * (y1 + ya), z = 0.5 * (z1 + za);
+  const double vx = x1 - xa, vy = y1 - ya, vz = z1 - za;
+  const double c = 0.5 * falloff * (vx * x + vy * y + vz * z) / (x * x + y * y + z * z);
+  c1[t] = 1 - c;
+  c2[t] = 1 + c;
+}
+
+// Brill-Lindquist + Bowen-York coefficients (SetMWBL, SetBYK,
+// SetPunctureCoefficients): a = 1/(psi - 1), b = a^7 K_ij K^ij / 8
+struct Punctures {
+  int n;
+  double mass[8], pos[8][3], mom[8][3], spin[8][3];
+};
+__global__ void coefficients_kernel(Punctures P, int m, double dx, double *a, double *b) {
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (long)m * m * m) return;
+  const int i = q % m, j = (q / m) % m, k = q / ((long)m * m);
+  const double x0 = -(m - 1) * dx / 2;
+  const double x = x0 + i * dx, y = x0 + j * dx, z = x0 + k * dx;
+  double p = 0.0, K[6] = {0, 0, 0, 0, 0, 0};
+  for (int n = 0; n < P.n; ++n) {
+    const double xi = x - P.pos[n][0], yi = y - P.pos[n][1], zi = z - P.pos[n][2];
+    double r = sqrt(xi * xi + yi * yi + zi * zi);
+    if (!(r < -1e-10 || 0.0 < r - 1e-10)) r = 1e-13;  // dequal(r,0) -> EPSZERO
+    p += P.mass[n] * (1 / r) * 0.5;
+    const double N[3] = {xi / r, yi / r, zi / r};
+    const double *Pm = P.mom[n], *S = P.spin[n];
+    const double NP = N[0] * Pm[0] + N[1] * Pm[1] + N[2] * Pm[2];
+    const double eNS[3] = {N[1] * S[2] - N[2] * S[1], N[2] * S[0] - N[0] * S[2], N[0] * S[1] - N[1] * S[0]};
+    int c = 0;
+    for (int s = 0; s < 3; ++s)
+      for (int t = s; t < 3; ++t, ++c)
+        K[c] += 1.5 / (r * r) * (N[s] * Pm[t] + N[t] * Pm[s] - ((s == t) - N[s] * N[t]) * NP) -
+                3.0 / (r * r * r) * (eNS[s] * N[t] + eNS[t] * N[s]);
+  }
+  const double psi = p + 1.0;
+  const double aq = 1 / (psi - 1);
+  const double K2 = K[0] * K[0] + K[3] * K[3] + K[5] * K[5] + 2 * K[1] * K[1] + 2 * K[2] * K[2] + 2 * K[4] * K[4];
+  a[q] = aq;
+  b[q] = 0.125 * pow(aq, 7.0) * K2;
+}
+
+unsigned nblk(long n) { return (unsigned)((n + RB - 1) / RB); }
+
+}  // namespace
+
+// ---- host side ----------------------------------------------------------------
+struct nrgpu_mg {
+  int nl;  // levels, 0 = coarsest
+  MgLevel lv[16];
+  nrgpu_mg_params p;
+  MgStatus *st;       // device
+  double *partial;    // device block partial sums (finest level size)
+  int npartial;
+  cudaStream_t stream;  // library-owned (captured into CUDA graphs)
+  cudaGraph_t graph[16];
+  cudaGraphExec_t exec[16];
+};
+
+// stack sizes (coarsegridsize, makestack.c:36-79) for one process
+static int stack_sizes(int m, int size_nmin, int levels_nmax, int *sizes) {
+  int n = 0, l = 1;
+  sizes[n++] = m;
+  while (n < 16) {
+    if (levels_nmax != -1 && l > levels_nmax) break;
+    if ((m - 2) % 4) break;
+    const int mnew = m / 2 + 1;
+    if (mnew < size_nmin || mnew < 4) break;
+    sizes[n++] = m = mnew;
+    l++;
+  }
+  return n;
+}
+
+// find_robin_normal (robin.c:29-143) on the host: averaged unit directions to
+// the inner members of the 27-neighbourhood, then the grid direction with the
+// largest projection (first maximum in loop order)
+static void robin_normals(int m, std::vector<int> &bidx, std::vector<int> &bnrm) {
+  auto isb = [m](int i, int j, int k) { return i == 0 || j == 0 || k == 0 || i == m - 1 || j == m - 1 || k == m - 1; };
+  for (int k = 0; k < m; ++k)
+    for (int j = 0; j < m; ++j)
+      for (int i = 0; i < m; ++i) {
+        if (!isb(i, j, k)) continue;
+        double vx = 0, vy = 0, vz = 0, mx = 0;
+        int best = -1;
+        for (int pass = 0; pass < 2; ++pass)
+          for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+              for (int c = 0; c < 3; ++c) {
+                const int ii = i + a - 1, jj = j + b - 1, kk = k + c - 1;
+                if (ii < 0 || jj < 0 || kk < 0 || ii >= m || jj >= m || kk >= m) continue;
+                if (isb(ii, jj, kk)) continue;
+                const double s = sqrt((double)((a - 1) * (a - 1) + (b - 1) * (b - 1) + (c - 1) * (c - 1)));
+                if (pass == 0) {
+                  vx += (a - 1) / s; vy += (b - 1) / s; vz += (c - 1) / s;
+                } else {
+                  const double dot = (vx * (a - 1) + vy * (b - 1) + vz * (c - 1)) / s;
+                  if (dot > mx) { mx = dot; best = ii + m * (jj + m * kk); }
+                }
+              }
+        bidx.push_back(i + m * (j + m * k));
+        bnrm.push_back(best);
+      }
+}
+
+extern "C" void nrgpu_mg_params_default(nrgpu_mg_params *p) {
+  if (!p) return;
+  p->npre = 3;
+  p->npost = 3;
+  p->exact_nmin = 10;
+  p->exact_nmax = 200;
+  p->vcycle_nmin = 0;
+  p->vcycle_nmax = 2000;
+  p->fullV = 1;
+  p->size_nmin = 4;
+  p->levels_nmax = -1;
+  p->tol = 1e-10;
+  p->falloff = 1.0;
+  p->batch = 8;
+}
+
+extern "C" int nrgpu_mg_destroy(nrgpu_mg *M) {
+  if (!M) return NRGPU_OK;
+  for (int l = 0; l < M->nl; ++l) {
+    MgLevel &L = M->lv[l];
+    cudaFree(L.u); cudaFree(L.u2); cudaFree(L.v); cudaFree(L.w); cudaFree(L.f); cudaFree(L.a); cudaFree(L.b);
+    cudaFree(L.bidx); cudaFree(L.bnrm); cudaFree(L.bc1); cudaFree(L.bc2);
+    if (M->exec[l]) cudaGraphExecDestroy(M->exec[l]);
+    if (M->graph[l]) cudaGraphDestroy(M->graph[l]);
+  }
+  cudaFree(M->st);
+  cudaFree(M->partial);
+  if (M->stream) cudaStreamDestroy(M->stream);
+  free(M);
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_mg_create(int m, double dx, const nrgpu_mg_params *p, nrgpu_mg **out) {
+  if (!p || !out || m < 4 || !(dx > 0)) return nrgpu_set_error(NRGPU_ERR_ARG, "bad multigrid arguments");
+  if (p->npre < 0 || p->npost < 0 || p->exact_nmax < 1 || p->vcycle_nmax < 1 || p->batch < 1)
+    return nrgpu_set_error(NRGPU_ERR_ARG, "bad multigrid parameters");
+  if ((long)m * m * m > 0x7fffffffL) return nrgpu_set_error(NRGPU_ERR_ARG, "box too large");
+  int sizes[16];
+  const int nl = stack_sizes(m, p->size_nmin, p->levels_nmax, sizes);
+  nrgpu_mg *M = (nrgpu_mg *)calloc(1, sizeof(nrgpu_mg));
+  if (!M) return nrgpu_set_error(NRGPU_ERR_NOMEM, "host allocation");
+  M->nl = nl;
+  M->p = *p;
+  bool ok = true;
+  for (int l = 0; l < nl && ok; ++l) {
+    MgLevel &L = M->lv[l];
+    L.m = sizes[nl - 1 - l];
+    L.np = (long)L.m * L.m * L.m;
+    L.dx = dx * (double)(1 << (nl - 1 - l));
+    L.x0 = -(L.m - 1) * L.dx / 2;
+    const size_t by = sizeof(double) * L.np;
+    ok = cudaMalloc(&L.u, by) == cudaSuccess && cudaMalloc(&L.u2, by) == cudaSuccess &&
+         cudaMalloc(&L.v, by) == cudaSuccess && cudaMalloc(&L.w, by) == cudaSuccess &&
+         cudaMalloc(&L.f, by) == cudaSuccess && cudaMalloc(&L.a, by) == cudaSuccess &&
+         cudaMalloc(&L.b, by) == cudaSuccess;
+    if (!ok) break;
+    std::vector<int> bi, bn;
+    robin_normals(L.m, bi, bn);
+    L.nb = (int)bi.size();
+    ok = cudaMalloc(&L.bidx, sizeof(int) * L.nb) == cudaSuccess && cudaMalloc(&L.bnrm, sizeof(int) * L.nb) == cudaSuccess &&
+         cudaMalloc(&L.bc1, sizeof(double) * L.nb) == cudaSuccess &&
+         cudaMalloc(&L.bc2, sizeof(double) * L.nb) == cudaSuccess;
+    if (!ok) break;
+    cudaMemcpy(L.bidx, bi.data(), sizeof(int) * L.nb, cudaMemcpyHostToDevice);
+    cudaMemcpy(L.bnrm, bn.data(), sizeof(int) * L.nb, cudaMemcpyHostToDevice);
+    robin_factors_kernel<<<nblk(L.nb), RB>>>(L.bidx, L.bnrm, L.bc1, L.bc2, L.nb, L.m, L.x0, L.dx, p->falloff);
+    for (double *z : {L.u, L.u2, L.v, L.w, L.f, L.a, L.b}) cudaMemset(z, 0, by);
+  }
+  M->npartial = (int)nblk(M->lv[nl - 1].np);
+  ok = ok && cudaStreamCreateWithFlags(&M->stream, cudaStreamNonBlocking) == cudaSuccess &&
+       cudaMalloc(&M->st, sizeof(MgStatus)) == cudaSuccess &&
+       cudaMalloc(&M->partial, sizeof(double) * M->npartial) == cudaSuccess;
+  if (!ok || cudaDeviceSynchronize() != cudaSuccess) {
+    cudaGetLastError();
+    nrgpu_mg_destroy(M);
+    return nrgpu_set_error(NRGPU_ERR_NOMEM, "multigrid stack allocation failed");
+  }
+  *out = M;
+  return NRGPU_OK;
+}
+
+// ---- the cycle ------------------------------------------------------------------
+static void robin_u(nrgpu_mg *M, MgLevel &L, double *u, const int *done) {
+  robin_kernel<<<nblk(L.nb), RB, 0, M->stream>>>(u, L.bidx, L.bnrm, L.bc1, L.bc2, L.nb, 0, done);
+}
+static void robin_d(nrgpu_mg *M, MgLevel &L, double *u, const int *done) {
+  robin_kernel<<<nblk(L.nb), RB, 0, M->stream>>>(u, L.bidx, L.bnrm, L.bc1, L.bc2, L.nb, 1, done);
+}
+static double cxof(const MgLevel &L) { return 1 / (L.dx * L.dx); }
+
+static void sweeps(nrgpu_mg *M, MgLevel &L, int n, const int *done) {
+  for (int s = 0; s < n; ++s) {
+    jacobi_kernel<<<nblk(L.np), RB, 0, M->stream>>>(L.u, L.u2, L.f, L.a, L.b, L.m, cxof(L), done);
+    robin_u(M, L, L.u2, done);
+    std::swap(L.u, L.u2);
+  }
+}
+
+// the children of coarse point I are the fine points 2I-1 and 2I in each
+// direction: the stack levels are centred with m_fine = 2 m_coarse - 2, so
+// box_child_index gives (int)(2I - 1/2) = 2I - 1 for the inner I
+constexpr int kChildOff = 1;
+
+static void vcycle(nrgpu_mg *M, int l, const int *done) {
+  MgLevel &h = M->lv[l];
+  if (l == 0) {
+    exact_solve_kernel<<<1, 256, 0, M->stream>>>(h.u, h.u2, h.f, h.a, h.b, h.m, cxof(h), h.bidx, h.bnrm, h.bc1,
+                                                h.bc2, h.nb, M->p.exact_nmin, M->p.exact_nmax, M->p.tol / 10, M->st);
+    return;
+  }
+  MgLevel &H = M->lv[l - 1];
+  const int off = kChildOff;
+  double *const u_entry = h.u;
+  sweeps(M, h, M->p.npre, done);
+  // finetocoarse
+  robin_u(M, h, h.u, done);
+  lop_kernel<<<nblk(h.np), RB, 0, M->stream>>>(h.u, h.v, h.a, h.b, h.m, cxof(h), done);
+  restrict_kernel<<<nblk(H.np), RB, 0, M->stream>>>(h.u, H.u, h.m, H.m, off, done);
+  robin_u(M, H, H.u, done);
+  coarse_rhs_kernel<<<nblk(H.np), RB, 0, M->stream>>>(h.v, h.f, H.u, H.f, H.a, H.b, h.m, H.m, off, cxof(H), done);
+  copy_kernel<<<nblk(H.np), RB, 0, M->stream>>>(H.u, H.w, H.np, done);
+  vcycle(M, l - 1, done);
+  // coarsetofine
+  sub_inner_kernel<<<nblk(H.np), RB, 0, M->stream>>>(H.u, H.w, H.v, H.m, done);
+  robin_d(M, H, H.v, done);
+  prolong_add_kernel<<<nblk(h.np), RB, 0, M->stream>>>(H.v, h.u, h.m, H.m, h.x0, h.dx, H.x0, H.dx, 1, done);
+  robin_u(M, h, h.u, done);
+  sweeps(M, h, M->p.npost, done);
+  // an odd number of sweeps leaves u in the partner array: move it back so
+  // that every cycle starts and ends on the same buffers (graph replay)
+  if (h.u != u_entry) {
+    copy_kernel<<<nblk(h.np), RB, 0, M->stream>>>(h.u, u_entry, h.np, done);
+    std::swap(h.u, h.u2);
+  }
+}
+
+// residual test of level l (restau): Robin on u, RMS of L u - f
+static void restau(nrgpu_mg *M, int l, int count) {
+  MgLevel &h = M->lv[l];
+  const int *done = count ? &M->st->done : nullptr;
+  robin_u(M, h, h.u, done);
+  residual_partial_kernel<<<nblk(h.np), RB, 0, M->stream>>>(h.u, h.f, h.a, h.b, h.m, cxof(h), M->partial, done);
+  residual_final_kernel<<<1, 1024, 0, M->stream>>>(M->partial, (int)nblk(h.np), (long)(h.m - 2) * (h.m - 2) * (h.m - 2),
+                                                  M->st, M->p.tol, count, M->p.vcycle_nmax);
+}
+
+extern "C" int nrgpu_mg_solve(nrgpu_mg *M, const double *a, const double *b, double *u, int *ncycles, double *normres,
+                              void *stream) {
+  if (!M || !a || !b || !u) return nrgpu_set_error(NRGPU_ERR_ARG, "null multigrid argument");
+  if (M->p.vcycle_nmin != 0) return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "mg_vcycle_nmin must be 0");
+  // the caller's stream is drained first; the solve runs on the solver's own
+  // stream, which can be captured into CUDA graphs
+  NRGPU_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  const int top = M->nl - 1;
+  MgLevel &T = M->lv[top];
+  const size_t by = sizeof(double) * T.np;
+  NRGPU_CUDA_TRY(cudaMemcpyAsync(T.u, u, by, cudaMemcpyDeviceToDevice, M->stream));
+  NRGPU_CUDA_TRY(cudaMemcpyAsync(T.a, a, by, cudaMemcpyDeviceToDevice, M->stream));
+  NRGPU_CUDA_TRY(cudaMemcpyAsync(T.b, b, by, cudaMemcpyDeviceToDevice, M->stream));
+  // initializestack: restrict coefficients and u down the stack; v, w, f = 0
+  for (int l = top; l > 0; --l) {
+    MgLevel &h = M->lv[l], &H = M->lv[l - 1];
+    const int off = kChildOff;
+    restrict_kernel<<<nblk(H.np), RB, 0, M->stream>>>(h.a, H.a, h.m, H.m, off, nullptr);
+    restrict_kernel<<<nblk(H.np), RB, 0, M->stream>>>(h.b, H.b, h.m, H.m, off, nullptr);
+    restrict_kernel<<<nblk(H.np), RB, 0, M->stream>>>(h.u, H.u, h.m, H.m, off, nullptr);
+  }
+  for (int l = 0; l <= top; ++l) {
+    MgLevel &L = M->lv[l];
+    cudaMemsetAsync(L.v, 0, sizeof(double) * L.np, M->stream);
+    cudaMemsetAsync(L.w, 0, sizeof(double) * L.np, M->stream);
+    cudaMemsetAsync(L.f, 0, sizeof(double) * L.np, M->stream);
+  }
+  MgStatus h_st;
+  const int batch = M->p.batch;
+  for (int l = M->p.fullV ? 0 : top; l <= top; ++l) {
+    NRGPU_CUDA_TRY(cudaMemsetAsync(M->st, 0, sizeof(MgStatus), M->stream));
+    if (l == 0) {
+      // the coarsest level is tested once and, unless the test passes,
+      // solved once (solve.c:56-91: "for l == 0, solve is exact")
+      restau(M, 0, 1);
+      vcycle(M, 0, nullptr);
+    } else {
+      // V cycles in batches: test, cycle, test, cycle, ... ; the device flag
+      // turns the rest of a batch into no-ops once the test passes
+      int cycles = 0;
+      for (;;) {
+        if (!M->exec[l]) {
+          cudaGraph_t g;
+          NRGPU_CUDA_TRY(cudaStreamBeginCapture(M->stream, cudaStreamCaptureModeThreadLocal));
+          for (int s = 0; s < batch; ++s) {
+            restau(M, l, 1);
+            vcycle(M, l, &M->st->done);
+          }
+          NRGPU_CUDA_TRY(cudaStreamEndCapture(M->stream, &g));
+          M->graph[l] = g;
+          NRGPU_CUDA_TRY(cudaGraphInstantiate(&M->exec[l], g, 0));
+        }
+        NRGPU_CUDA_TRY(cudaGraphLaunch(M->exec[l], M->stream));
+        NRGPU_CUDA_TRY(cudaMemcpyAsync(&h_st, M->st, sizeof h_st, cudaMemcpyDeviceToHost, M->stream));
+        NRGPU_CUDA_TRY(cudaStreamSynchronize(M->stream));
+        cycles = h_st.ncycles;
+        if (h_st.done) break;
+      }
+      if (l == top) {
+        if (ncycles) *ncycles = cycles;
+        if (normres) *normres = h_st.res;
+      }
+    }
+    if (l < top) {
+      // prolong_u: trilinear onto the inner points of the next level, Robin
+      MgLevel &H = M->lv[l], &h = M->lv[l + 1];
+      prolong_add_kernel<<<nblk(h.np), RB, 0, M->stream>>>(H.u, h.u, h.m, H.m, h.x0, h.dx, H.x0, H.dx, 0, nullptr);
+      robin_u(M, h, h.u, nullptr);
+    }
+  }
+  NRGPU_CUDA_TRY(cudaMemcpyAsync(u, T.u, by, cudaMemcpyDeviceToDevice, M->stream));
+  NRGPU_CUDA_TRY(cudaStreamSynchronize(M->stream));
+  NRGPU_CUDA_TRY(cudaGetLastError());
+  // like the reference, running out of V cycles is not an error: the caller
+  // sees ncycles == vcycle_nmax and normres > tol
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_puncture_coefficients(int m, double dx, int npunc, const double *mass, const double *pos,
+                                           const double *mom, const double *spin, double *a, double *b, void *stream) {
+  if (m < 2 || npunc < 1 || npunc > 8 || !mass || !pos || !mom || !spin || !a || !b)
+    return nrgpu_set_error(NRGPU_ERR_ARG, "bad puncture arguments (1..8 punctures)");
+  Punctures P;
+  memset(&P, 0, sizeof P);
+  P.n = npunc;
+  for (int n = 0; n < npunc; ++n) {
+    P.mass[n] = mass[n];
+    for (int c = 0; c < 3; ++c) {
+      P.pos[n][c] = pos[3 * n + c];
+      P.mom[n][c] = mom[3 * n + c];
+      P.spin[n][c] = spin[3 * n + c];
+    }
+  }
+  coefficients_kernel<<<nblk((long)m * m * m), RB, 0, (cudaStream_t)stream>>>(P, m, dx, a, b);
+  NRGPU_CUDA_TRY(cudaGetLastError());
+  return NRGPU_OK;
+}

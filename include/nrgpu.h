@@ -181,6 +181,48 @@ int nrgpu_bssn_rk4_step_noalloc(const nrgpu_box *box, double dx, double dy, doub
                                 double *const *u, double dt, const nrgpu_bssn_params *p,
                                 void *stream);
 
+/* ---- puncture initial data: the multigrid ---------------------------------- */
+
+/* Parameters of the reference's multigrid (bam_multigrid.c:33-49) and of
+ * the puncture solve (bam_punctures.c:110-178). */
+typedef struct {
+  int npre, npost;             /* mg_relax_npre / mg_relax_npost */
+  int exact_nmin, exact_nmax;  /* mg_exact_nmin / mg_exact_nmax */
+  int vcycle_nmin, vcycle_nmax;/* mg_vcycle_nmin (must be 0) / mg_vcycle_nmax */
+  int fullV;                   /* mg_typeofcycles = fullV (1) or finest only (0) */
+  int size_nmin, levels_nmax;  /* mg_size_nmin / mg_levels_nmax */
+  double tol;                  /* punctures_tolerance, RMS residual */
+  double falloff;              /* punctures_robin_falloff of u */
+  int batch;                   /* V cycles per CUDA-graph launch (no counterpart) */
+} nrgpu_mg_params;
+
+typedef struct nrgpu_mg nrgpu_mg;  /* the multigrid stack on the device */
+
+void nrgpu_mg_params_default(nrgpu_mg_params *p);
+
+/* Build the stack for one cube of m^3 points (m - 2 divisible by 4 for each
+ * coarsening), spacing dx, centred on the origin: makestack
+ * (makestack.c:85-127) plus find_robin_normal on every level. */
+int nrgpu_mg_create(int m, double dx, const nrgpu_mg_params *p, nrgpu_mg **out);
+int nrgpu_mg_destroy(nrgpu_mg *mg);
+
+/* Solve L(u) = Laplace u + b (1 + a (1+u))^-7 = 0 with a Robin boundary for
+ * u by FAS multigrid.  Replaces multigrid(level, u, f, v, c, itmax, tol,
+ * &normres, Lpuncture_nonlin, Lpuncture_GS) (multigrid.c:35, called from
+ * PunctureSolve.c:282).  a, b, u: device arrays of m^3 doubles; u holds the
+ * initial guess and receives the solution.  *ncycles = finest-level V
+ * cycles, *normres = the final RMS residual. */
+int nrgpu_mg_solve(nrgpu_mg *mg, const double *a, const double *b, double *u, int *ncycles,
+                   double *normres, void *stream);
+
+/* Brill-Lindquist + Bowen-York coefficients a = 1/(psi_BL - 1) and
+ * b = a^7 K_ij K^ij / 8 on the m^3 cube (SetMWBL, SetBYK,
+ * SetPunctureCoefficients: ConformalFactor.c:147, ExtrinsicCurvature.c:142,
+ * Punctures.c:320).  Host arrays mass[n], pos/mom/spin[3n]; a, b device. */
+int nrgpu_puncture_coefficients(int m, double dx, int npunc, const double *mass,
+                                const double *pos, const double *mom, const double *spin,
+                                double *a, double *b, void *stream);
+
 /* ---- diagnostics -------------------------------------------------------- */
 
 /* Measured FP64 FMA throughput of the current device (FLOP/s, 2 per FMA),

@@ -121,6 +121,7 @@ static void robin(const mglevel *L, double *u, double falloff)
 {
   int m = L->m;
   long q;
+#pragma omp parallel for schedule(static)
   for (q = 0; q < L->np; q++) {
     long n;
     int i, j, k, ni, nj, nk;
@@ -153,6 +154,7 @@ static void lop(const mglevel *L, double *u, double *lu)
   double cx = 1 / (L->dx * L->dx), cc = -2 * (cx + cx + cx);
   long q;
   robin(L, u, FALLOFF_U);
+#pragma omp parallel for schedule(static)
   for (q = 0; q < L->np; q++) {
     if (L->flag[q]) continue;
     lu[q] = cc * u[q] + cx * (u[q - 1] + u[q + 1]) + cx * (u[q - m] + u[q + m]) +
@@ -166,6 +168,7 @@ static void lgs(const mglevel *L, const double *uo, double *un)
   int m = L->m;
   double cx = 1 / (L->dx * L->dx), cc = -2 * (cx + cx + cx);
   long q;
+#pragma omp parallel for schedule(static)
   for (q = 0; q < L->np; q++) {
     double lu, lii;
     if (L->flag[q]) continue;
@@ -210,6 +213,7 @@ static void restrict8(const mglevel *F, const double *fv, const mglevel *Cl, dou
 {
   int mc = Cl->m, mf = F->m;
   long q;
+#pragma omp parallel for schedule(static)
   for (q = 0; q < Cl->np; q++) {
     int I, J, K, i, j, k;
     long f0;
@@ -232,6 +236,7 @@ static void prolong2(const mglevel *Cl, const double *cv, const mglevel *F, doub
 {
   int mc = Cl->m, mf = F->m;
   long q;
+#pragma omp parallel for schedule(static)
   for (q = 0; q < F->np; q++) {
     int i, j, k, ci, cj, ck;
     long c0;

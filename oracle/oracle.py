@@ -79,3 +79,31 @@ def bssn_evolve(level, u, dt, nsteps, params):
     if e:
         raise RuntimeError("oracle evolve failed")
     return u
+
+
+def puncture_coefficients(m, dx, binary):
+    """a, b of the oracle on the m^3 cube."""
+    L = lib()
+    n = m ** 3
+    a = np.zeros(n)
+    b = np.zeros(n)
+    dp = lambda x: x.ctypes.data_as(C.POINTER(C.c_double))
+    L.oracle_puncture_coefficients(m, C.c_double(dx), len(binary.mass), dp(binary.mass), dp(binary.pos),
+                                   dp(binary.mom), dp(binary.spin), dp(a), dp(b))
+    return a, b
+
+
+def mg_solve(m, dx, a, b, u=None, params=None):
+    """The oracle multigrid; returns (u, V cycles, residual history)."""
+    from baum_b200 import abi
+    p = params or abi.mg_params()
+    L = lib()
+    u = np.zeros(m ** 3) if u is None else np.ascontiguousarray(u, dtype=np.float64).copy()
+    hist = np.zeros(p.vcycle_nmax + 1)
+    nl = C.c_int()
+    dp = lambda x: x.ctypes.data_as(C.POINTER(C.c_double))
+    L.oracle_mg_solve.restype = C.c_int
+    n = L.oracle_mg_solve(m, C.c_double(dx), dp(np.ascontiguousarray(a)), dp(np.ascontiguousarray(b)), dp(u),
+                          p.npre, p.npost, p.exact_nmin, p.exact_nmax, p.vcycle_nmin, p.vcycle_nmax, p.fullV,
+                          p.size_nmin, p.levels_nmax, C.c_double(p.tol), dp(hist), C.byref(nl))
+    return u, n, hist[:n + 1]

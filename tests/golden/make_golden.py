@@ -110,6 +110,62 @@ nrharness_dump = 0 4
 }
 
 
+MG_CASES = {
+    # Bowen-York binary with momenta and spins, multigrid to 1e-10 RMS
+    "mg_binary_34": """
+physics = adm punctures multigrid nrharness
+mass1 = 0.5
+px1 = 2.1
+my1 = 0.1
+sz1 = 0.1
+mass2 = 0.6
+px2 = -2.6
+my2 = -0.1
+sx2 = -0.05
+sz2 = 0.08
+punctures_solver = multigrid
+punctures_persist = yes
+punctures_tolerance = 1e-10
+grid = box
+nxyz = 32
+dxyz = 0.5
+mg_verbose = some
+mg_vcycle_nmax = 2000
+mg_relax_npre = 3
+mg_relax_npost = 3
+mg_size_nmin = 4
+mg_exact_nmin = 10
+mg_exact_nmax = 200
+iterations = 0
+nrharness_dir = .
+nrharness_mg = yes
+""",
+}
+
+
+def run_mg_case(name, par):
+    import re
+    work = tempfile.mkdtemp(prefix="golden_")
+    try:
+        with open(os.path.join(work, name + ".par"), "w") as f:
+            f.write(par)
+        r = subprocess.run([BAM, "-nt", "4", name + ".par"], cwd=work, capture_output=True, text=True)
+        if r.returncode:
+            raise RuntimeError(r.stdout[-3000:] + r.stderr[-3000:])
+        ncyc = int(re.search(r"after (\d+) V-cycles", r.stdout).group(1))
+        # residual table after the cycles: the finest level is the last row
+        block = r.stdout.split("V-cycles")[-1]
+        res = float(re.findall(r"l\d+\s+\d+x\s*\d+x\s*\d+\s+([0-9.e+-]+)", block)[-1])
+        d = dumpfile.read(os.path.join(work, "mg_u_l0.bin"))
+        np.savez_compressed(os.path.join(OUT, name + ".npz"), u=d["data"][0], dx=d["dx"],
+                            m=d["boxes"][0][0], vcycles=ncyc, residual=res)
+        with open(os.path.join(OUT, name + ".par"), "w") as f:
+            f.write(par.lstrip())
+        print("wrote", name, "V-cycles", ncyc, "residual", res)
+    finally:
+        shutil.rmtree(work)
+
+
 def run_case(name, par):
     work = tempfile.mkdtemp(prefix="golden_")
     try:
@@ -144,3 +200,5 @@ if __name__ == "__main__":
         sys.exit("oracle/_ref/bam missing: run python oracle/build_ref.py first")
     for n, p in CASES.items():
         run_case(n, p)
+    for n, p in MG_CASES.items():
+        run_mg_case(n, p)
