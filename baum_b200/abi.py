@@ -54,6 +54,32 @@ class BssnParams(C.Structure):
                 ("bc_speed", C.c_double * NVARS)]
 
 
+def getv(value, token):
+    """The reference's token test of a parameter string (GetvFlag,
+    parameters.c:883-900): only the FIRST occurrence of token as a substring
+    is examined, and it counts only if it is a whole word.  So "withB" is
+    false in "withBadv withB" but true in "withB withBadv"."""
+    i = value.find(token)
+    if i < 0:
+        return 0
+    start = i == 0 or value[i - 1] == " "
+    j = i + len(token)
+    end = j == len(value) or value[j] == " "
+    return 1 if start and end else 0
+
+
+def bssn_params_from_par(lapse="1+log withshift", shift="gamma0 withGadv withBadv withShiftadv", **over):
+    """Factors of bssn_rhs_movpunc_N from the bssn_lapse / bssn_shift strings
+    (bssn_rhs_movpunc_N.c:117-131)."""
+    f = dict(oploglapse=getv(lapse, "1+log"), oploglapse2=getv(lapse, "1+log2"),
+             oplogwithshift=getv(lapse, "withshift"), harmoniclapse=getv(lapse, "harmonic"),
+             gamma0factor=float(getv(shift, "gamma0")), gamma2factor=float(getv(shift, "gamma2")),
+             withGadv=float(getv(shift, "withGadv")), withShiftadv=float(getv(shift, "withShiftadv")),
+             withBadv=float(getv(shift, "withBadv")), withB=float(not getv(shift, "withoutB")))
+    f.update(over)
+    return bssn_params(**f)
+
+
 def bssn_params(**over):
     """Parameters of the single-puncture BSSN workload: 1+log withshift,
     gamma0 withGadv withBadv withShiftadv, shiftdriver 2, 4th-order centred
@@ -101,6 +127,79 @@ def set_bc_from_gauge(p):
         speed[i] = vg
     p.bc_var0[:] = var0
     p.bc_speed[:] = speed
+
+
+Z4_NVARS = 25
+# Z4c evolve-list order (reference z4.c:234-242)
+Z4_VARS = ["g11", "g12", "g13", "g22", "g23", "g33", "chi", "A11", "A12", "A13", "A22", "A23", "A33",
+           "Khat", "G1", "G2", "G3", "Theta", "alpha", "beta1", "beta2", "beta3", "B1", "B2", "B3"]
+
+
+class Z4Params(C.Structure):
+    _fields_ = [("order_centered", C.c_int), ("order_advection", C.c_int),
+                ("advection_lopsided", C.c_int), ("advection_lopsided6", C.c_int),
+                ("order_dissipation", C.c_int), ("dissfactor", C.c_double),
+                ("kappa1", C.c_double), ("kappa2", C.c_double), ("zeroThetaRHS", C.c_double),
+                ("useNPTs", C.c_int), ("subtractA", C.c_int), ("normalizedetg", C.c_int),
+                ("oploglapse", C.c_int), ("oploglapse2", C.c_int), ("oplogwithshift", C.c_int),
+                ("harmoniclapse", C.c_int), ("gamma0factor", C.c_double), ("gamma2factor", C.c_double),
+                ("withGadv", C.c_double), ("withShiftadv", C.c_double), ("withBadv", C.c_double),
+                ("withB", C.c_double), ("lapseharmonicf", C.c_double), ("shiftalphapower", C.c_double),
+                ("shiftgammacoeff", C.c_double), ("shiftdriver", C.c_double), ("chiDivFloor", C.c_double),
+                ("chipsipower", C.c_double), ("bc_var0", C.c_double * Z4_NVARS),
+                ("bc_speed", C.c_double * Z4_NVARS)]
+
+
+def z4_params(**over):
+    """Z4c settings of the precision-sweep and FMR workloads: z4_lapse =
+    1+log withshift, z4_shift = gamma0 withGadv withBadv withShiftadv withB,
+    shiftdriver 2, shiftgammacoeff 0.75, kappa1 = 0.02, kappa2 = 0, Theta
+    evolved (z4_zeroThetaRHS default "no" reads as 1), no non-principal
+    terms, 4th order + KO6 with dissipation_factor 0.1; boundary far limits
+    and speeds of z4.c:204-228."""
+    p = Z4Params()
+    p.order_centered = p.order_advection = 4
+    p.advection_lopsided = 1
+    p.advection_lopsided6 = 3
+    p.order_dissipation = 6
+    p.dissfactor = 0.1 / 2.0 ** 6
+    p.kappa1, p.kappa2 = 0.02, 0.0
+    p.zeroThetaRHS = 1.0
+    p.useNPTs = 0
+    p.subtractA = p.normalizedetg = 1
+    p.oploglapse, p.oploglapse2, p.oplogwithshift, p.harmoniclapse = 1, 0, 1, 0
+    p.gamma0factor, p.gamma2factor = 1.0, 0.0
+    p.withGadv = p.withShiftadv = p.withBadv = p.withB = 1.0
+    p.lapseharmonicf = 2.0
+    p.shiftalphapower = 0.0
+    p.shiftgammacoeff = 0.75
+    p.shiftdriver = 2.0
+    p.chiDivFloor = -1000.0
+    p.chipsipower = -4.0
+    for k, v in over.items():
+        setattr(p, k, v)
+    vg = p.lapseharmonicf ** 0.5 if p.oploglapse else ((4.0 / 3.0) ** 0.5 if p.oploglapse2 else 1.0)
+    var0 = [0.0] * Z4_NVARS
+    speed = [1.0] * Z4_NVARS
+    for i in (0, 3, 5, 6, 18):   # gxx gyy gzz chi alpha
+        var0[i] = 1.0
+    for i in (13, 6, 18):        # Khat chi alpha
+        speed[i] = vg
+    p.bc_var0[:] = var0
+    p.bc_speed[:] = speed
+    return p
+
+
+def z4_params_from_par(lapse="1+log withshift", shift="gamma0 withGadv withBadv withShiftadv withB", **over):
+    """Factors of z4_rhs_movpunc_N from the z4_lapse / z4_shift strings
+    (z4_rhs_movpunc_N.m:610-626), with the reference's token semantics."""
+    f = dict(oploglapse=getv(lapse, "1+log"), oploglapse2=getv(lapse, "1+log2"),
+             oplogwithshift=getv(lapse, "withshift"), harmoniclapse=getv(lapse, "harmonic"),
+             gamma0factor=float(getv(shift, "gamma0")), gamma2factor=float(getv(shift, "gamma2")),
+             withGadv=float(getv(shift, "withGadv")), withShiftadv=float(getv(shift, "withShiftadv")),
+             withBadv=float(getv(shift, "withBadv")), withB=float(getv(shift, "withB")))
+    f.update(over)
+    return z4_params(**f)
 
 
 class MgParams(C.Structure):
@@ -196,6 +295,9 @@ def lib():
         "nrgpu_bssn_evolve_host": (C.c_int, [vp, pp, C.c_int, C.c_double, C.POINTER(BssnParams)]),
         "nrgpu_level_nan_flag": (C.c_int, [vp, C.POINTER(C.c_int)]),
         "nrgpu_probe_fp64_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_float)]),
+        "nrgpu_z4_rhs": (C.c_int, [vp, pp, pp, C.c_double, pp, C.POINTER(Z4Params), vp]),
+        "nrgpu_z4_boundary": (C.c_int, [vp, pp, pp, C.c_double, pp, C.POINTER(Z4Params), vp]),
+        "nrgpu_z4_rk4_step": (C.c_int, [vp, pp, C.c_double, C.POINTER(Z4Params), vp]),
         "nrgpu_mg_params_default": (None, [C.POINTER(MgParams)]),
         "nrgpu_mg_create": (C.c_int, [C.c_int, C.c_double, C.POINTER(MgParams), C.POINTER(vp)]),
         "nrgpu_mg_destroy": (C.c_int, [vp]),

@@ -18,12 +18,12 @@ from . import abi
 NV = abi.NVARS
 
 
-def _ptrs(t):
-    if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous() and t.dim() == 2 and t.shape[0] == NV):
-        raise ValueError("a variable list is a contiguous float64 CUDA tensor of shape (24, npoints)")
+def _ptrs(t, nv=NV):
+    if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous() and t.dim() == 2 and t.shape[0] == nv):
+        raise ValueError("a variable list is a contiguous float64 CUDA tensor of shape (%d, npoints)" % nv)
     base = t.data_ptr()
     step = t.stride(0) * 8
-    return abi.ptr_array([base + i * step for i in range(NV)])
+    return abi.ptr_array([base + i * step for i in range(nv)])
 
 
 def _stream(stream):
@@ -56,8 +56,8 @@ class DeviceLevel:
         except Exception:
             pass
 
-    def empty(self):
-        return torch.zeros((NV, self.npoints), dtype=torch.float64, device="cuda")
+    def empty(self, nv=NV):
+        return torch.zeros((nv, self.npoints), dtype=torch.float64, device="cuda")
 
     def nan_flag(self):
         f = C.c_int()

@@ -704,6 +704,8 @@ __global__ void vlcopy_kernel(VarPtrs dst, CVarPtrs src, int npoints) {
 }
 
 
+#include "nrgpu_z4.cuh"
+
 }  // namespace
 
 // ---- host side ----------------------------------------------------------------
@@ -1010,6 +1012,133 @@ extern "C" int nrgpu_bssn_rk4_step_noalloc(const nrgpu_box *box, double dx, doub
     bssn_surface_kernel<<<sgrid, 256, 0, s>>>(ins[st], outs[st], cP, U, Es[st], *p, bx, dx, dy, dz);
   }
   bssn_algcon_kernel<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(U, (int)np, p->subtractA, p->normalizedetg);
+  NRGPU_CUDA_TRY(cudaGetLastError());
+  return NRGPU_OK;
+}
+
+// ---- Z4c ---------------------------------------------------------------------
+static int z4_check_params(const nrgpu_z4_params *p) {
+  if (!p) return nrgpu_set_error(NRGPU_ERR_ARG, "null parameters");
+  if (p->order_centered != 2 && p->order_centered != 4 && p->order_centered != 6)
+    return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "order_centered %d not in {2,4,6}", p->order_centered);
+  if (p->order_advection != p->order_centered)
+    return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "order_advection %d != order_centered %d", p->order_advection,
+                           p->order_centered);
+  if (p->order_dissipation != 0 && p->order_dissipation != 4 && p->order_dissipation != 6)
+    return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "order_dissipation %d not in {0,4,6}", p->order_dissipation);
+  if (p->useNPTs) return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "z4_useNPTs = yes is not supported");
+  if (p->advection_lopsided < 0 || p->advection_lopsided > 2 || p->advection_lopsided6 < 0 ||
+      p->advection_lopsided6 > 3)
+    return nrgpu_set_error(NRGPU_ERR_ARG, "advection lopsidedness out of range");
+  return NRGPU_OK;
+}
+
+static int z4_fill(ZVarPtrs *vp, double *const *src, const char *what) {
+  if (!src) return nrgpu_set_error(NRGPU_ERR_ARG, "null %s list", what);
+  for (int v = 0; v < ZNV; ++v) {
+    if (!src[v]) return nrgpu_set_error(NRGPU_ERR_ARG, "null %s[%d]", what, v);
+    vp->p[v] = src[v];
+  }
+  return NRGPU_OK;
+}
+static ZCVarPtrs z4_c(const ZVarPtrs &v) {
+  ZCVarPtrs c;
+  for (int i = 0; i < ZNV; ++i) c.p[i] = v.p[i];
+  return c;
+}
+
+static int z4_launch(nrgpu_level *L, const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVarPtrs &pre,
+                     const ZVarPtrs &acc, const Epilogue &E, const nrgpu_z4_params &p, cudaStream_t st, bool interior,
+                     bool flagged) {
+  if (interior) {
+    for (int b = 0; b < L->nboxes; ++b) {
+      const BoxGeo &bx = L->hbox[b];
+      if (bx.m < 3 || bx.n < 3 || bx.o < 3) continue;
+      dim3 blk(32, 4, 1);
+      dim3 grd((bx.m - 2 + 31) / 32, (bx.n - 2 + 3) / 4, bx.o - 2);
+      if (bx.m == 162 && bx.n == 162)
+        z4_rhs_kernel<162, 162 * 162><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy,
+                                                            L->dz, L->d_status);
+      else if (bx.m == 66 && bx.n == 66)
+        z4_rhs_kernel<66, 66 * 66><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy,
+                                                         L->dz, L->d_status);
+      else
+        z4_rhs_kernel<<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
+                                           L->d_status);
+    }
+  }
+  if (flagged && L->nflagpts > 0) {
+    const int n = L->nflagpts * ZNV;
+    z4_flagged_kernel<<<(n + 255) / 256, 256, 0, st>>>(U, out, pre, acc, E, p, L->d_flagpts, L->nflagpts, L->d_box,
+                                                        L->dx, L->dy, L->dz);
+  }
+  NRGPU_CUDA_TRY(cudaGetLastError());
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_z4_rhs(nrgpu_level *L, double *const *unew, double *const *upre, double c, double *const *ucur,
+                            const nrgpu_z4_params *p, void *stream) {
+  if (!L) return nrgpu_set_error(NRGPU_ERR_ARG, "null level");
+  int e;
+  if ((e = z4_check_params(p))) return e;
+  ZVarPtrs n, pr, cu;
+  if ((e = z4_fill(&n, unew, "unew")) || (e = z4_fill(&cu, ucur, "ucur"))) return e;
+  if (c != 0.0) {
+    if ((e = z4_fill(&pr, upre, "upre"))) return e;
+  } else {
+    pr = cu;
+  }
+  Epilogue E = {c != 0.0 ? EPI_ADDLINEAR : EPI_RHS, c, 0.0, 0.0, 0};
+  return z4_launch(L, z4_c(cu), n, z4_c(pr), n, E, *p, (cudaStream_t)stream, true, false);
+}
+
+extern "C" int nrgpu_z4_boundary(nrgpu_level *L, double *const *unew, double *const *upre, double c,
+                                 double *const *ucur, const nrgpu_z4_params *p, void *stream) {
+  if (!L || !p) return nrgpu_set_error(NRGPU_ERR_ARG, "null argument");
+  int e;
+  ZVarPtrs n, pr, cu;
+  if ((e = z4_fill(&n, unew, "unew")) || (e = z4_fill(&cu, ucur, "ucur"))) return e;
+  if (c != 0.0) {
+    if ((e = z4_fill(&pr, upre, "upre"))) return e;
+  } else {
+    pr = cu;
+  }
+  Epilogue E = {c != 0.0 ? EPI_ADDLINEAR : EPI_RHS, c, 0.0, 0.0, 0};
+  return z4_launch(L, z4_c(cu), n, z4_c(pr), n, E, *p, (cudaStream_t)stream, false, true);
+}
+
+// evolve_rk_rk4 (rk.c:220) for the Z4c list + z4_algcon_wrapper (z4.c:49)
+extern "C" int nrgpu_z4_rk4_step(nrgpu_level *L, double *const *u, double dt, const nrgpu_z4_params *p,
+                                 void *stream) {
+  if (!L) return nrgpu_set_error(NRGPU_ERR_ARG, "null level");
+  int e;
+  if ((e = z4_check_params(p))) return e;
+  ZVarPtrs U;
+  if ((e = z4_fill(&U, u, "u"))) return e;
+  double *scr = nullptr;
+  if ((e = nrgpu_level_scratch(L, &scr))) return e;
+  ZVarPtrs P, V1, V2;
+  const size_t np = (size_t)L->npoints;
+  for (int v = 0; v < ZNV; ++v) {
+    P.p[v] = scr + (0 * ZNV + v) * np;
+    V1.p[v] = scr + (1 * ZNV + v) * np;
+    V2.p[v] = scr + (2 * ZNV + v) * np;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const long n = (long)ZNV * L->npoints;
+  z4_copy_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(P, z4_c(U), L->npoints);
+  const ZCVarPtrs cP = z4_c(P);
+  Epilogue E1 = {EPI_RK, 0.0, dt / 6, dt / 2, 1};
+  Epilogue E2 = {EPI_RK, 0.0, dt / 3, dt / 2, 1};
+  Epilogue E3 = {EPI_RK, 0.0, dt / 3, dt, 1};
+  Epilogue E4 = {EPI_RK, 0.0, dt / 6, 0.0, 0};
+  if ((e = z4_launch(L, cP, V1, cP, U, E1, *p, st, true, true))) return e;
+  if ((e = z4_launch(L, z4_c(V1), V2, cP, U, E2, *p, st, true, true))) return e;
+  if ((e = z4_launch(L, z4_c(V2), V1, cP, U, E3, *p, st, true, true))) return e;
+  if ((e = z4_launch(L, z4_c(V1), V2, cP, U, E4, *p, st, true, true))) return e;
+  VarPtrs gA;
+  for (int v = 0; v < NRGPU_NV; ++v) gA.p[v] = U.p[v];  // g~ 0..5 and A~ 7..12 as in BSSN
+  bssn_algcon_kernel<<<(L->npoints + 255) / 256, 256, 0, st>>>(gA, L->npoints, p->subtractA, p->normalizedetg);
   NRGPU_CUDA_TRY(cudaGetLastError());
   return NRGPU_OK;
 }

@@ -130,10 +130,11 @@ extern "C" int nrgpu_level_destroy(nrgpu_level *L) {
   return NRGPU_OK;
 }
 
-// three 24-variable lists of RK4 scratch, allocated once per level
+// three variable lists of RK4 scratch (room for the 25 Z4c variables),
+// allocated once per level
 int nrgpu_level_scratch(nrgpu_level *L, double **out) {
   if (!L->scratch) {
-    const size_t bytes = sizeof(double) * 3 * NRGPU_NV * (size_t)L->npoints;
+    const size_t bytes = sizeof(double) * 3 * NRGPU_Z4_NVARS * (size_t)L->npoints;
     if (cudaMalloc(&L->scratch, bytes) != cudaSuccess) {
       L->scratch = nullptr;
       cudaGetLastError();

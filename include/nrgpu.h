@@ -95,6 +95,27 @@ typedef struct {
   double bc_speed[NRGPU_BSSN_NVARS];
 } nrgpu_bssn_params;
 
+#define NRGPU_Z4_NVARS 25
+
+/* Parameters that z4_rhs_movpunc_N reads (z4_rhs_movpunc_N.m:600-640).
+ * Z4c evolve list (z4.c:234-242): g11..g33 chi A11..A33 Khat G1..G3 Theta
+ * alpha beta1..3 B1..3 (25 variables). */
+typedef struct {
+  int order_centered, order_advection, advection_lopsided, advection_lopsided6;
+  int order_dissipation;    /* 0, 4 or 6; applied to all 25 variables */
+  double dissfactor;
+  double kappa1, kappa2;    /* z4_kappa1, z4_kappa2 */
+  double zeroThetaRHS;      /* Getv("z4_zeroThetaRHS","no"): 1 for the default */
+  int useNPTs;              /* Getv("z4_useNPTs","yes"): must be 0 */
+  int subtractA, normalizedetg;
+  int oploglapse, oploglapse2, oplogwithshift, harmoniclapse;
+  double gamma0factor, gamma2factor, withGadv, withShiftadv, withBadv, withB;
+  double lapseharmonicf, shiftalphapower, shiftgammacoeff, shiftdriver;
+  double chiDivFloor, chipsipower;
+  double bc_var0[NRGPU_Z4_NVARS];
+  double bc_speed[NRGPU_Z4_NVARS];
+} nrgpu_z4_params;
+
 /* ---- library ---------------------------------------------------------- */
 
 int nrgpu_abi_version(void);
@@ -180,6 +201,20 @@ int nrgpu_level_nan_flag(nrgpu_level *lev, int *flag);
 int nrgpu_bssn_rk4_step_noalloc(const nrgpu_box *box, double dx, double dy, double dz,
                                 double *const *u, double dt, const nrgpu_bssn_params *p,
                                 void *stream);
+
+/* ---- Z4c (device pointers, 25-variable lists) -------------------------------- */
+
+/* Replaces z4_rhs_movpunc_N(unew, upre, c, ucur) (z4_rhs_movpunc_N.c:23,
+ * registered as "geometry" by z4_startup, z4.c:246); same semantics as
+ * nrgpu_bssn_rhs.  z4_useNPTs must be off. */
+int nrgpu_z4_rhs(nrgpu_level *lev, double *const *unew, double *const *upre, double c,
+                 double *const *ucur, const nrgpu_z4_params *p, void *stream);
+/* Replaces set_boundary for the Z4c list ("geometry_bound", z4.c:248). */
+int nrgpu_z4_boundary(nrgpu_level *lev, double *const *unew, double *const *upre, double c,
+                      double *const *ucur, const nrgpu_z4_params *p, void *stream);
+/* evolve_rk_rk4 (rk.c:220) of the Z4c list + z4_algcon_wrapper (z4.c:49). */
+int nrgpu_z4_rk4_step(nrgpu_level *lev, double *const *u, double dt, const nrgpu_z4_params *p,
+                      void *stream);
 
 /* ---- puncture initial data: the multigrid ---------------------------------- */
 

@@ -559,9 +559,9 @@ static double computedel(const double *var, double vx, long ccc, long mcc, long 
 #undef LFT
 }
 
-/* set_boundary_rot_rad (radiative.c:105) without rotation, all variables */
-int oracle_bssn_boundary(const nrgpu_level_desc *L, double *const *unew, double *const *upre,
-                         double c, double *const *ucur, const nrgpu_bssn_params *p)
+/* set_boundary_rot_rad (radiative.c:105) without rotation, nv variables */
+static int boundary_nv(const nrgpu_level_desc *L, int nv, double *const *unew, double *const *upre,
+                       double c, double *const *ucur, const double *bvar0, const double *bspeed)
 {
   int b;
   const double oo2d[3] = {1 / (2 * L->dx), 1 / (2 * L->dy), 1 / (2 * L->dz)};
@@ -585,9 +585,9 @@ int oracle_bssn_boundary(const nrgpu_level_desc *L, double *const *unew, double 
       double x = L->box[b].x0 + i * L->dx, y = L->box[b].y0 + j * L->dy,
              z = L->box[b].z0 + k * L->dz;
       double rr = sqrt(x * x + y * y + z * z);
-      for (v = 0; v < NV; v++) {
+      for (v = 0; v < nv; v++) {
         const double *var = ucur[v];
-        double vv = p->bc_speed[v], var0 = p->bc_var0[v];
+        double vv = bspeed[v], var0 = bvar0[v];
         double Wx = vv * x / rr, Wy = vv * y / rr, Wz = vv * z / rr;
         double delx = computedel(var, Wx, ccc, mcc, Mcc, pcc, Pcc);
         double dely = computedel(var, Wy, ccc, cmc, cMc, cpc, cPc);
@@ -599,6 +599,12 @@ int oracle_bssn_boundary(const nrgpu_level_desc *L, double *const *unew, double 
     }
   }
   return 0;
+}
+
+int oracle_bssn_boundary(const nrgpu_level_desc *L, double *const *unew, double *const *upre,
+                         double c, double *const *ucur, const nrgpu_bssn_params *p)
+{
+  return boundary_nv(L, NV, unew, upre, c, ucur, p->bc_var0, p->bc_speed);
 }
 
 /* bssn_algcon (bssn_algcon.c:25) on all points */
@@ -640,15 +646,21 @@ int oracle_bssn_algcon(const nrgpu_level_desc *L, double *const *u, const nrgpu_
 }
 
 /* r = a x + b y over all points (vladd, variables.c:650) */
-static void vladd(long np, double *const *r, double a, double *const *x, double b,
-                  double *const *y)
+static void vladd_nv(long np, int nv, double *const *r, double a, double *const *x, double b,
+                     double *const *y)
 {
   int v;
-  for (v = 0; v < NV; v++) {
+  for (v = 0; v < nv; v++) {
     long q;
     OMP_FOR
     for (q = 0; q < np; q++) r[v][q] = a * x[v][q] + b * y[v][q];
   }
+}
+
+static void vladd(long np, double *const *r, double a, double *const *x, double b,
+                  double *const *y)
+{
+  vladd_nv(np, NV, r, a, x, b, y);
 }
 
 static int rhs_stage(const nrgpu_level_desc *L, double *const *r, double *const *upre,
@@ -718,3 +730,415 @@ extern "C" void oracle_count_point(const nrgpu_level_desc *L, double *const *u, 
   *transc = g_fc.transc;
 }
 #endif
+
+/* ======================================================================
+ * Z4c: z4_rhs_movpunc_N (spec z4_rhs_movpunc_N.m:18-520, non-shell branch,
+ * useNPTs = 0), boundary = set_boundary (z4.c:248), algcon z4_algcon
+ * (identical operations to bssn_algcon on g~ and A~).
+ * Variables: g11..g33 chi A11..A33 Khat G1..G3 Theta alpha beta1..3 B1..3.
+ * ====================================================================== */
+enum { ZG11, ZCHI = 6, ZA11 = 7, ZKHAT = 13, ZGA1 = 14, ZTHETA = 17, ZALPHA = 18, ZBETA1 = 19,
+       ZBB1 = 22, ZNV = 25 };
+
+static int z4_point(const double *const *u, long ijk, int i, int j, int k, int imax, int jmax,
+                    int kmax, long di, long dj, long dk, const double h[3],
+                    const nrgpu_z4_params *p, real r[ZNV])
+{
+  const long s[3] = {di, dj, dk};
+  int a, b, c, d, e, ord, aord;
+  int dist = i;
+  if (j < dist) dist = j;
+  if (k < dist) dist = k;
+  if (imax - i < dist) dist = imax - i;
+  if (jmax - j < dist) dist = jmax - j;
+  if (kmax - k < dist) dist = kmax - k;
+  ord = ladder(p->order_centered, dist);
+  aord = ladder(p->order_advection, dist);
+  if (!ord || !aord || p->useNPTs) return -1;
+
+  real g[6], A[6], Gv[3], beta[3], B[3];
+  real alpha = u[ZALPHA][ijk], chi = u[ZCHI][ijk], Khat = u[ZKHAT][ijk], Theta = u[ZTHETA][ijk];
+  for (a = 0; a < 6; a++) { g[a] = u[ZG11 + a][ijk]; A[a] = u[ZA11 + a][ijk]; }
+  for (a = 0; a < 3; a++) {
+    Gv[a] = u[ZGA1 + a][ijk]; beta[a] = u[ZBETA1 + a][ijk]; B[a] = u[ZBB1 + a][ijk];
+  }
+
+  real da[3], dda[6], db[3][3], ddb[6][3], delg[3][6], deldelg[6][6], delG[3][3], dKhat[3],
+      dchi[3], ddchi[6], dTheta[3];
+  for (a = 0; a < 3; a++) {
+    da[a] = d1(u[ZALPHA], ijk, s[a], h[a], ord);
+    dKhat[a] = d1(u[ZKHAT], ijk, s[a], h[a], ord);
+    dchi[a] = d1(u[ZCHI], ijk, s[a], h[a], ord);
+    dTheta[a] = d1(u[ZTHETA], ijk, s[a], h[a], ord);
+    for (c = 0; c < 3; c++) {
+      db[a][c] = d1(u[ZBETA1 + c], ijk, s[a], h[a], ord);
+      delG[a][c] = d1(u[ZGA1 + c], ijk, s[a], h[a], ord);
+    }
+    for (c = 0; c < 6; c++) delg[a][c] = d1(u[ZG11 + c], ijk, s[a], h[a], ord);
+  }
+  for (a = 0; a < 3; a++)
+    for (b = a; b < 3; b++) {
+      int ab = SY[a][b];
+      if (a == b) {
+        dda[ab] = d2(u[ZALPHA], ijk, s[a], h[a], ord);
+        ddchi[ab] = d2(u[ZCHI], ijk, s[a], h[a], ord);
+        for (c = 0; c < 3; c++) ddb[ab][c] = d2(u[ZBETA1 + c], ijk, s[a], h[a], ord);
+        for (c = 0; c < 6; c++) deldelg[ab][c] = d2(u[ZG11 + c], ijk, s[a], h[a], ord);
+      } else {
+        dda[ab] = d11(u[ZALPHA], ijk, s[a], s[b], h[a], h[b], ord);
+        ddchi[ab] = d11(u[ZCHI], ijk, s[a], s[b], h[a], h[b], ord);
+        for (c = 0; c < 3; c++) ddb[ab][c] = d11(u[ZBETA1 + c], ijk, s[a], s[b], h[a], h[b], ord);
+        for (c = 0; c < 6; c++)
+          deldelg[ab][c] = d11(u[ZG11 + c], ijk, s[a], s[b], h[a], h[b], ord);
+      }
+    }
+
+  adv_t av[3];
+  {
+    const int idx[3] = {i, j, k}, mx[3] = {imax, jmax, kmax};
+    const int lop = aord == 6 ? p->advection_lopsided6 : p->advection_lopsided;
+    for (a = 0; a < 3; a++) adv_dir(&av[a], idx[a], mx[a], beta[a] / h[a], aord, lop, s[a]);
+  }
+  real lieg[6], lieA[6], lieKhat, liechi, liealpha, advG[3], advbeta[3], advB[3], advTheta;
+  for (a = 0; a < 6; a++) {
+    lieg[a] = adv_apply(av, u[ZG11 + a], ijk);
+    lieA[a] = adv_apply(av, u[ZA11 + a], ijk);
+  }
+  lieKhat = adv_apply(av, u[ZKHAT], ijk);
+  liechi = adv_apply(av, u[ZCHI], ijk);
+  liealpha = adv_apply(av, u[ZALPHA], ijk);
+  advTheta = adv_apply(av, u[ZTHETA], ijk);
+  for (a = 0; a < 3; a++) {
+    advG[a] = adv_apply(av, u[ZGA1 + a], ijk);
+    advbeta[a] = adv_apply(av, u[ZBETA1 + a], ijk);
+    advB[a] = adv_apply(av, u[ZBB1 + a], ijk);
+  }
+
+  real K = Khat + 2 * Theta;
+  real detg = g[0] * g[3] * g[5] + 2 * g[1] * g[2] * g[4] - g[0] * g[4] * g[4] - g[3] * g[2] * g[2] -
+              g[5] * g[1] * g[1];
+  real detginv = 1 / detg;
+  real ginv[6];
+  ginv[0] = detginv * (g[3] * g[5] - g[4] * g[4]);
+  ginv[1] = detginv * (g[2] * g[4] - g[1] * g[5]);
+  ginv[2] = detginv * (g[1] * g[4] - g[2] * g[3]);
+  ginv[3] = detginv * (g[0] * g[5] - g[2] * g[2]);
+  ginv[4] = detginv * (g[1] * g[2] - g[0] * g[4]);
+  ginv[5] = detginv * (g[0] * g[3] - g[1] * g[1]);
+#define GI(x, y) ginv[SY[x][y]]
+#define GG(x, y) g[SY[x][y]]
+#define AAi(x, y) A[SY[x][y]]
+  real gammado[3][6], gamma[3][6], Gfromg[3];
+  for (c = 0; c < 3; c++)
+    for (a = 0; a < 3; a++)
+      for (b = a; b < 3; b++)
+        gammado[c][SY[a][b]] = 0.5 * (delg[a][SY[b][c]] + delg[b][SY[a][c]] - delg[c][SY[a][b]]);
+  for (c = 0; c < 3; c++)
+    for (a = 0; a < 6; a++) {
+      real t = 0;
+      for (d = 0; d < 3; d++) t += GI(c, d) * gammado[d][a];
+      gamma[c][a] = t;
+    }
+  for (a = 0; a < 3; a++) {
+    real t = 0;
+    for (b = 0; b < 3; b++)
+      for (c = 0; c < 3; c++) t += GI(b, c) * gamma[a][SY[b][c]];
+    Gfromg[a] = t;
+  }
+#define GAM(x, y, z) gamma[x][SY[y][z]]
+#define GDO(x, y, z) gammado[x][SY[y][z]]
+  real Rab[6];
+  for (a = 0; a < 3; a++)
+    for (b = a; b < 3; b++) {
+      real t = 0, t2 = 0;
+      for (c = 0; c < 3; c++)
+        for (d = 0; d < 3; d++) {
+          real q = -0.5 * deldelg[SY[c][d]][SY[a][b]];
+          for (e = 0; e < 3; e++)
+            q += GAM(e, c, a) * GDO(b, e, d) + GAM(e, c, b) * GDO(a, e, d) + GAM(e, a, d) * GDO(e, c, b);
+          t += GI(c, d) * q;
+        }
+      for (c = 0; c < 3; c++)
+        t2 += GG(c, a) * delG[b][c] + GG(c, b) * delG[a][c] + Gfromg[c] * (GDO(a, b, c) + GDO(b, a, c));
+      Rab[SY[a][b]] = t + 0.5 * t2;
+    }
+
+  real chiguarded = chi;
+  if (chiguarded < p->chiDivFloor) chiguarded = p->chiDivFloor;
+  real oochipsipower = 1 / p->chipsipower;
+  real f = oochipsipower * RLOG(chiguarded);
+  real psim4 = REXP(-4 * f);
+  real df[3], ddf[6], cddf[6];
+  for (a = 0; a < 3; a++) df[a] = oochipsipower * dchi[a] / chiguarded;
+  for (a = 0; a < 3; a++)
+    for (b = a; b < 3; b++)
+      ddf[SY[a][b]] = oochipsipower * ddchi[SY[a][b]] / chiguarded - p->chipsipower * df[a] * df[b];
+  real trcddf = 0, dfdf = 0, dfda = 0;
+  for (a = 0; a < 3; a++)
+    for (b = a; b < 3; b++) {
+      real t = ddf[SY[a][b]];
+      for (c = 0; c < 3; c++) t -= GAM(c, a, b) * df[c];
+      cddf[SY[a][b]] = t;
+    }
+  for (a = 0; a < 3; a++)
+    for (b = 0; b < 3; b++) {
+      trcddf += GI(a, b) * cddf[SY[a][b]];
+      dfdf += GI(a, b) * df[a] * df[b];
+      dfda += GI(a, b) * df[a] * da[b];
+    }
+  real Rphi[6], cdda[6];
+  for (a = 0; a < 3; a++)
+    for (b = a; b < 3; b++) {
+      int ab = SY[a][b];
+      Rphi[ab] = 4 * df[a] * df[b] - 2 * cddf[ab] - 2 * g[ab] * trcddf - 4 * g[ab] * dfdf;
+      real t = dda[ab];
+      for (c = 0; c < 3; c++) t -= GAM(c, a, b) * da[c];
+      cdda[ab] = t - 2 * (df[a] * da[b] + df[b] * da[a] - g[ab] * dfda);
+    }
+  real trcdda = 0;
+  for (a = 0; a < 3; a++)
+    for (b = 0; b < 3; b++) trcdda += GI(a, b) * cdda[SY[a][b]];
+  trcdda = psim4 * trcdda;
+
+  real AAab[6], Ainv[6], cAA = 0, divAinv[3];
+  for (a = 0; a < 3; a++)
+    for (b = a; b < 3; b++) {
+      real t = 0, t2 = 0;
+      for (c = 0; c < 3; c++)
+        for (d = 0; d < 3; d++) {
+          t += GI(c, d) * AAi(a, c) * AAi(d, b);
+          t2 += GI(a, c) * GI(b, d) * AAi(c, d);
+        }
+      AAab[SY[a][b]] = t;
+      Ainv[SY[a][b]] = t2;
+    }
+  for (a = 0; a < 3; a++)
+    for (b = 0; b < 3; b++) cAA += GI(a, b) * AAab[SY[a][b]];
+  for (a = 0; a < 3; a++) {
+    real t = 0;
+    for (b = 0; b < 3; b++)
+      for (c = 0; c < 3; c++) t += GAM(a, b, c) * Ainv[SY[b][c]];
+    for (b = 0; b < 3; b++)
+      t += -1.5 * Ainv[SY[a][b]] * dchi[b] / chiguarded -
+           (1.0 / 3.0) * GI(a, b) * (2 * dKhat[b] + dTheta[b]);
+    divAinv[a] = t;
+  }
+  real Rhat = 0;
+  for (a = 0; a < 3; a++)
+    for (b = 0; b < 3; b++) Rhat += GI(a, b) * (Rab[SY[a][b]] + Rphi[SY[a][b]]);
+  Rhat = psim4 * Rhat;
+  real Hhat = Rhat + 2 * K * K / 3 - cAA;
+
+  real divbeta = db[0][0] + db[1][1] + db[2][2];
+  real totdivbeta = (2.0 / 3.0) * divbeta;
+  real ootddivbeta[3];
+  for (a = 0; a < 3; a++)
+    ootddivbeta[a] = (1.0 / 3.0) * (ddb[SY[a][0]][0] + ddb[SY[a][1]][1] + ddb[SY[a][2]][2]);
+  for (a = 0; a < 3; a++)
+    for (b = a; b < 3; b++) {
+      int ab = SY[a][b];
+      real tg = lieg[ab] - g[ab] * totdivbeta, tA = lieA[ab] - A[ab] * totdivbeta;
+      for (c = 0; c < 3; c++) {
+        tg += db[a][c] * GG(b, c) + db[b][c] * GG(a, c);
+        tA += db[a][c] * AAi(b, c) + db[b][c] * AAi(a, c);
+      }
+      lieg[ab] = tg;
+      lieA[ab] = tA;
+    }
+  liechi = liechi + (p->chipsipower / 6) * chiguarded * divbeta;
+  real pseudolieG[3];
+  for (a = 0; a < 3; a++) {
+    real t = 0;
+    for (b = 0; b < 3; b++)
+      for (c = 0; c < 3; c++) t += GI(b, c) * ddb[SY[b][c]][a];
+    for (b = 0; b < 3; b++) t += GI(a, b) * ootddivbeta[b] - Gfromg[b] * db[b][a];
+    pseudolieG[a] = t + Gfromg[a] * totdivbeta + advG[a];
+  }
+
+  real rg[6], rA[6], rG[3], rKhat, rchi, rTheta;
+  for (a = 0; a < 6; a++) {
+    rg[a] = -2 * alpha * A[a] + lieg[a];
+    rA[a] = psim4 * (-cdda[a] + alpha * (Rab[a] + Rphi[a])) - (1.0 / 3.0) * g[a] * (-trcdda + alpha * Rhat) +
+            alpha * (K * A[a] - 2 * AAab[a]) + lieA[a];
+  }
+  for (a = 0; a < 3; a++) {
+    real t = 0;
+    for (b = 0; b < 3; b++) t += Ainv[SY[a][b]] * da[b];
+    rG[a] = -2 * t + 2 * alpha * divAinv[a] - 2 * alpha * p->kappa1 * (Gv[a] - Gfromg[a]) + pseudolieG[a];
+  }
+  rKhat = -trcdda + alpha * (cAA + K * K / 3) + lieKhat + p->kappa1 * (1 - p->kappa2) * alpha * Theta;
+  rchi = (-p->chipsipower / 6) * chiguarded * alpha * K + liechi;
+  rTheta = (alpha * (Hhat / 2 - (2 + p->kappa2) * p->kappa1 * Theta) + advTheta) * p->zeroThetaRHS;
+
+  real falpha = p->oploglapse * p->lapseharmonicf + p->oploglapse2 * 8.0 / (3 * (3 - alpha)) +
+                p->harmoniclapse * alpha;
+  real ralpha = p->oplogwithshift * liealpha - falpha * alpha * Khat;
+  real rbeta[3], rB[3];
+  if (p->withB != 0) {
+    real betaF = p->shiftgammacoeff * RPOW(alpha, p->shiftalphapower);
+    for (a = 0; a < 3; a++) {
+      rbeta[a] = (p->gamma2factor + p->gamma0factor * betaF) * B[a] + p->withShiftadv * advbeta[a];
+      rB[a] = (p->gamma0factor + p->gamma2factor * betaF) * (rG[a] - p->withGadv * advG[a]) -
+              p->shiftdriver * B[a] + p->withBadv * advB[a];
+    }
+  } else {
+    for (a = 0; a < 3; a++) {
+      rB[a] = 0;
+      rbeta[a] = Gv[a] + p->withShiftadv * advbeta[a] - p->shiftdriver * beta[a];
+    }
+  }
+
+  if ((p->order_dissipation == 4 && dist >= 2) || (p->order_dissipation == 6 && dist >= 3)) {
+    const int od = p->order_dissipation;
+    const double e_ = p->dissfactor;
+    for (a = 0; a < 6; a++) {
+      rg[a] += e_ * ko(u[ZG11 + a], ijk, s, h, od);
+      rA[a] += e_ * ko(u[ZA11 + a], ijk, s, h, od);
+    }
+    for (a = 0; a < 3; a++) {
+      rG[a] += e_ * ko(u[ZGA1 + a], ijk, s, h, od);
+      rbeta[a] += e_ * ko(u[ZBETA1 + a], ijk, s, h, od);
+      rB[a] += e_ * ko(u[ZBB1 + a], ijk, s, h, od);
+    }
+    rKhat += e_ * ko(u[ZKHAT], ijk, s, h, od);
+    rchi += e_ * ko(u[ZCHI], ijk, s, h, od);
+    rTheta += e_ * ko(u[ZTHETA], ijk, s, h, od);
+    ralpha += e_ * ko(u[ZALPHA], ijk, s, h, od);
+  }
+
+  for (a = 0; a < 6; a++) { r[ZG11 + a] = rg[a]; r[ZA11 + a] = rA[a]; }
+  r[ZCHI] = rchi;
+  r[ZKHAT] = rKhat;
+  r[ZTHETA] = rTheta;
+  r[ZALPHA] = ralpha;
+  for (a = 0; a < 3; a++) {
+    r[ZGA1 + a] = rG[a];
+    r[ZBETA1 + a] = rbeta[a];
+    r[ZBB1 + a] = rB[a];
+  }
+  return 0;
+#undef GI
+#undef GG
+#undef AAi
+#undef GAM
+#undef GDO
+}
+
+static void z4_addlinear(double *const *unew, double *const *upre, long ijk, double c, const real r[ZNV],
+                         const nrgpu_z4_params *p)
+{
+  double n[ZNV];
+  int v;
+  for (v = 0; v < ZNV; v++) n[v] = upre[v][ijk] + c * RVAL(r[v]);
+  double *g = n + ZG11, *A = n + ZA11;
+  double detg = g[0] * g[3] * g[5] + 2 * g[1] * g[2] * g[4] - g[0] * g[4] * g[4] -
+                g[3] * g[2] * g[2] - g[5] * g[1] * g[1];
+  double detnginv = 1 / detg;
+  if (p->subtractA) {
+    double gi[6];
+    gi[0] = (g[3] * g[5] - g[4] * g[4]);
+    gi[1] = (g[2] * g[4] - g[1] * g[5]);
+    gi[2] = (g[1] * g[4] - g[2] * g[3]);
+    gi[3] = (g[0] * g[5] - g[2] * g[2]);
+    gi[4] = (g[1] * g[2] - g[0] * g[4]);
+    gi[5] = (g[0] * g[3] - g[1] * g[1]);
+    double trA = detnginv * (gi[0] * A[0] + gi[3] * A[3] + gi[5] * A[5] +
+                             2 * (gi[1] * A[1] + gi[2] * A[2] + gi[4] * A[4]));
+    double aux = -trA / 3;
+    for (v = 0; v < 6; v++) A[v] += aux * g[v];
+  }
+  if (p->normalizedetg) {
+    double aux = pow(detnginv, 1.0 / 3.0);
+    for (v = 0; v < 6; v++) g[v] *= aux;
+  }
+  for (v = 0; v < ZNV; v++) unew[v][ijk] = n[v];
+}
+
+int oracle_z4_rhs(const nrgpu_level_desc *L, double *const *unew, double *const *upre, double c,
+                  double *const *ucur, const nrgpu_z4_params *p)
+{
+  int b, err = 0;
+  const double h[3] = {L->dx, L->dy, L->dz};
+  for (b = 0; b < L->nboxes; b++) {
+    int m, n, o;
+    long off = box_of(L, b, &m, &n, &o);
+    long np = (long)m * n * o, q;
+    OMP_FOR
+    for (q = 0; q < np; q++) {
+      int k = (int)(q / ((long)m * n)), j = (int)((q / m) % n), i = (int)(q % m);
+      long ijk = off + q;
+      real r[ZNV];
+      int v;
+      if (L->boundary[ijk]) continue;
+      if (z4_point((const double *const *)ucur, ijk, i, j, k, m - 1, n - 1, o - 1, 1, m, (long)m * n, h, p, r)) {
+        err = -1;
+        continue;
+      }
+      if (c == 0.0)
+        for (v = 0; v < ZNV; v++) unew[v][ijk] = RVAL(r[v]);
+      else
+        z4_addlinear(unew, upre, ijk, c, r, p);
+    }
+  }
+  return err;
+}
+
+int oracle_z4_boundary(const nrgpu_level_desc *L, double *const *unew, double *const *upre, double c,
+                       double *const *ucur, const nrgpu_z4_params *p)
+{
+  return boundary_nv(L, ZNV, unew, upre, c, ucur, p->bc_var0, p->bc_speed);
+}
+
+/* z4_algcon on the g~ and A~ of a Z4c list: same operations as bssn_algcon */
+static void z4_algcon(const nrgpu_level_desc *L, double *const *u, const nrgpu_z4_params *p)
+{
+  nrgpu_bssn_params q;
+  double *bl[NV];
+  int v;
+  memset(&q, 0, sizeof q);
+  q.subtractA = p->subtractA;
+  q.normalizedetg = p->normalizedetg;
+  for (v = 0; v < NV; v++) bl[v] = u[v];  /* g at 0..5, A at 7..12 in both lists */
+  oracle_bssn_algcon(L, bl, &q);
+}
+
+int oracle_z4_rk4_step(const nrgpu_level_desc *L, double *const *u, double dt, const nrgpu_z4_params *p)
+{
+  long np = L->npoints;
+  double *buf = (double *)malloc(sizeof(double) * 3 * ZNV * np);
+  double *P[ZNV], *R[ZNV], *V[ZNV];
+  int v, e = 0;
+  if (!buf) return -4;
+  for (v = 0; v < ZNV; v++) {
+    P[v] = buf + (0 * ZNV + v) * np;
+    R[v] = buf + (1 * ZNV + v) * np;
+    V[v] = buf + (2 * ZNV + v) * np;
+    memcpy(P[v], u[v], sizeof(double) * np);
+    memset(R[v], 0, sizeof(double) * np);
+  }
+#define ZSTAGE(cur)                                   \
+  e |= oracle_z4_rhs(L, R, P, 0.0, cur, p);           \
+  oracle_z4_boundary(L, R, P, 0.0, cur, p);
+  ZSTAGE(u);
+  vladd_nv(np, ZNV, u, 1.0, u, dt / 6, R);
+  vladd_nv(np, ZNV, V, 1.0, P, dt / 2, R);
+  ZSTAGE(V);
+  vladd_nv(np, ZNV, u, 1.0, u, dt / 3, R);
+  vladd_nv(np, ZNV, V, 1.0, P, dt / 2, R);
+  ZSTAGE(V);
+  vladd_nv(np, ZNV, u, 1.0, u, dt / 3, R);
+  vladd_nv(np, ZNV, V, 1.0, P, dt, R);
+  ZSTAGE(V);
+  vladd_nv(np, ZNV, u, 1.0, u, dt / 6, R);
+#undef ZSTAGE
+  z4_algcon(L, u, p);
+  free(buf);
+  return e;
+}
+
+int oracle_z4_evolve(const nrgpu_level_desc *L, double *const *u, double dt, int nsteps, const nrgpu_z4_params *p)
+{
+  int s, e = 0;
+  for (s = 0; s < nsteps; s++) e |= oracle_z4_rk4_step(L, u, dt, p);
+  return e;
+}

@@ -45,6 +45,9 @@ def lib():
             "oracle_bssn_algcon": [LD, pp, BP],
             "oracle_bssn_rk4_step": [LD, pp, C.c_double, BP],
             "oracle_bssn_evolve": [LD, pp, C.c_double, C.c_int, BP],
+            "oracle_z4_rhs": [LD, pp, pp, C.c_double, pp, C.POINTER(abi.Z4Params)],
+            "oracle_z4_boundary": [LD, pp, pp, C.c_double, pp, C.POINTER(abi.Z4Params)],
+            "oracle_z4_evolve": [LD, pp, C.c_double, C.c_int, C.POINTER(abi.Z4Params)],
         }.items():
             f = getattr(L, name)
             f.restype = C.c_int
@@ -107,3 +110,20 @@ def mg_solve(m, dx, a, b, u=None, params=None):
                           p.npre, p.npost, p.exact_nmin, p.exact_nmax, p.vcycle_nmin, p.vcycle_nmax, p.fullV,
                           p.size_nmin, p.levels_nmax, C.c_double(p.tol), dp(hist), C.byref(nl))
     return u, n, hist[:n + 1]
+
+
+def z4_rhs(level, u, params, c=0.0, upre=None, out=None):
+    """Z4c rhs (inner points) + radiative boundary of u[25, npoints]."""
+    out = np.zeros_like(u) if out is None else out
+    upre = u if upre is None else upre
+    pu, pn, pp_ = _ptrs(u), _ptrs(out), _ptrs(upre)
+    if lib().oracle_z4_rhs(C.byref(level.desc), pn, pp_, c, pu, C.byref(params)):
+        raise RuntimeError("oracle z4 rhs failed")
+    lib().oracle_z4_boundary(C.byref(level.desc), pn, pp_, c, pu, C.byref(params))
+    return out
+
+
+def z4_evolve(level, u, dt, nsteps, params):
+    if lib().oracle_z4_evolve(C.byref(level.desc), _ptrs(u), dt, nsteps, C.byref(params)):
+        raise RuntimeError("oracle z4 evolve failed")
+    return u

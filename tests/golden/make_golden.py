@@ -110,6 +110,70 @@ nrharness_dump = 0 4
 }
 
 
+Z4_COMMON = """
+physics = adm z4 nrharness
+adm_data = Minkowski
+z4_lapse = 1+log withshift
+z4_shift = gamma0 withGadv withBadv withShiftadv withB
+z4_shiftdriver = 2.0
+z4_shiftgammacoeff = 0.75
+z4_kappa1 = 0.02
+z4_kappa2 = 0.0
+grid = box
+evolution_method = rk
+evolution_method_rk = rk4
+dtfac = 0.25
+boundary = radiative
+dissipation_factor = 0.1
+nrharness_dir = .
+nrharness_data = fourier
+nrharness_amp = 0.05
+"""
+
+CASES.update({
+    "z4_fourier_o4": Z4_COMMON + """
+nxyz = 10
+dxyz = 0.5
+order_centered = 4
+order_advection = 4
+advection_lopsided = 1
+order_dissipation = 6
+iterations = 2
+nrharness_dump = 0 2
+nrharness_rhs = yes
+nrharness_length = 4.5
+nrharness_seed = 5
+""",
+    # B-driver branch: "withB" must come before "withBadv" for the
+    # reference's first-occurrence token test to see it
+    "z4_fourier_o4_B": Z4_COMMON.replace("gamma0 withGadv withBadv withShiftadv withB",
+                                         "gamma0 withB withGadv withBadv withShiftadv") + """
+nxyz = 10
+dxyz = 0.5
+order_centered = 4
+order_advection = 4
+advection_lopsided = 1
+order_dissipation = 4
+iterations = 1
+nrharness_dump = 0 1
+nrharness_rhs = yes
+nrharness_length = 4.5
+nrharness_seed = 13
+""",
+    "z4_fourier_o6": Z4_COMMON + """
+nxyz = 10
+dxyz = 0.5
+order_centered = 6
+order_advection = 6
+order_dissipation = 6
+iterations = 1
+nrharness_dump = 0 1
+nrharness_rhs = yes
+nrharness_length = 4.5
+nrharness_seed = 9
+""",
+})
+
 MG_CASES = {
     # Bowen-York binary with momenta and spins, multigrid to 1e-10 RMS
     "mg_binary_34": """

@@ -1,0 +1,55 @@
+"""Parity of the CUDA Z4c path with the reference (golden) and the oracle."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden_level, load_golden, relerr
+from oracle import oracle
+from baum_b200 import abi, punctures, z4
+from test_z4_oracle_pin import Z4_CASES, z4_case
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+@pytest.mark.parametrize("case", sorted(Z4_CASES))
+def test_z4_rhs_and_rk4_match_reference(gpu, case):
+    g = load_golden(case)
+    lev = golden_level(g)
+    p, steps = z4_case(case)
+    dl = z4.DeviceLevel(lev)
+    u = torch.from_numpy(np.ascontiguousarray(g["state_it0_l0"])).cuda()
+    r = dl.empty(25)
+    z4.evolve_rhs(dl, r, u, 0.0, u, p)
+    torch.cuda.synchronize()
+    assert relerr(r.cpu().numpy(), g["rhs_it0_l0"]).max() < TOL
+    for _ in range(steps):
+        z4.evolve_rk_rk4(dl, u, float(g["dt"]), p)
+    torch.cuda.synchronize()
+    assert relerr(u.cpu().numpy(), g["state_it%d_l0" % steps]).max() < TOL
+    assert not dl.nan_flag()
+
+
+def z4_binary_state(level, punctures_list):
+    """Brill-Lindquist data in the Z4c list (Khat = Theta = 0)."""
+    b = punctures.brill_lindquist_state(level, punctures_list)
+    u = np.zeros((25, b.shape[1]))
+    u[:17] = b[:17]        # g chi A K(->Khat) G
+    u[18:] = b[17:]        # alpha beta B
+    return u
+
+
+def test_z4_c4_sixth_order_matches_oracle(gpu):
+    """The precision-sweep configuration at reduced size: Z4c, 6th order,
+    Brill-Lindquist binary m = 0.5 each at x = +-5; 40^3 inner points,
+    3 RK4 steps, every variable within 1e-12 of the oracle."""
+    lev = abi.Level.single_box(42, 0.4)
+    u0 = z4_binary_state(lev, [(0.5, 5.0, 0.0, 0.0), (0.5, -5.0, 0.0, 0.0)])
+    p = abi.z4_params(order_centered=6, order_advection=6)
+    dl = z4.DeviceLevel(lev)
+    u = torch.from_numpy(u0.copy()).cuda()
+    for _ in range(3):
+        z4.evolve_rk_rk4(dl, u, 0.1, p)
+    torch.cuda.synchronize()
+    uo = oracle.z4_evolve(lev, np.ascontiguousarray(u0.copy()), 0.1, 3, p)
+    assert relerr(u.cpu().numpy(), uo).max() < TOL
