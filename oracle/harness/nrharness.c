@@ -83,6 +83,40 @@ static void dump_varlist(tL *level, tVarList *vl, const char *tag)
   printf("nrharness: wrote %s\n", fn);
 }
 
+/* ADM variables (bssn_to_adm / z4_to_adm have run at POST_EVOLVE, before
+ * this module) and the constraints of adm_constraints_N (adm.c:14-74),
+ * dumped together */
+void adm_constraints_N(tVarList *ucon, tVarList *uadm);
+static void dump_constraints(tL *level, const char *tag)
+{
+  tVarList *con = vlalloc(level), *adm = vlalloc(level), *all = vlalloc(level);
+  vlpush(con, Ind("ham"));
+  vlpush(con, Ind("momx"));
+  if (Getv("adm_normalizedConstraints", "yes")) {
+    vlpush(con, Ind("normham"));
+    vlpush(con, Ind("normmomx"));
+  }
+  enablevarlist(con);
+  vlpush(adm, Ind("adm_gxx"));
+  vlpush(adm, Ind("adm_Kxx"));
+  vlpush(adm, Ind("adm_psi"));
+  vlpush(adm, Ind("adm_dpsiopsix"));
+  vlpush(adm, Ind("adm_ddpsiopsixx"));
+  adm_constraints_N(con, adm);
+  vlpush(all, Ind("adm_gxx"));
+  vlpush(all, Ind("adm_Kxx"));
+  vlpush(all, Ind("ham"));
+  vlpush(all, Ind("momx"));
+  if (Getv("adm_normalizedConstraints", "yes")) {
+    vlpush(all, Ind("normham"));
+    vlpush(all, Ind("normmomx"));
+  }
+  dump_varlist(level, all, tag);
+  vlfree(con);
+  vlfree(adm);
+  vlfree(all);
+}
+
 static int dump_requested(int iteration)
 {
   char s[32];
@@ -160,6 +194,10 @@ int nrharness_post_evolve(tL *level)
   if (dump_requested(level->iteration + 1)) {
     snprintf(tag, sizeof tag, "state_it%d", level->iteration + 1);
     dump_varlist(level, u, tag);
+    if (Getv("nrharness_constraints", "yes")) {
+      snprintf(tag, sizeof tag, "con_it%d", level->iteration + 1);
+      dump_constraints(level, tag);
+    }
   }
   return 0;
 }
@@ -172,6 +210,7 @@ void bam_nrharness(void)
   AddPar("nrharness_dump", "none", "level iterations after which to dump the evolved variables");
   AddPar("nrharness_rhs", "no", "dump one RHS evaluation of the initial state [no,yes]");
   AddPar("nrharness_mg", "no", "dump punctures_u after the initial data solve [no,yes]");
+  AddPar("nrharness_constraints", "no", "with each state dump also dump ADM variables and constraints [no,yes]");
   AddPar("nrharness_data", "none", "synthetic data over the evolved variables [none,fourier]");
   AddPar("nrharness_amp", "1e-3", "amplitude of the Fourier perturbation");
   AddPar("nrharness_nmodes", "8", "number of Fourier modes");

@@ -15,15 +15,16 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 SO = os.path.join(HERE, "liboracle.so")
 SRC = os.path.join(HERE, "nr_oracle.c")
 MGSRC = os.path.join(HERE, "mg_oracle.c")
+ADMSRC = os.path.join(HERE, "adm_oracle.c")
 
 
 def build(force=False):
     """Compile the restatement with gcc (-O2, OpenMP, no fast-math)."""
-    deps = [SRC, MGSRC, os.path.join(HERE, "..", "include", "nrgpu.h")]
+    deps = [SRC, MGSRC, ADMSRC, os.path.join(HERE, "..", "include", "nrgpu.h")]
     if not force and os.path.exists(SO) and all(os.path.getmtime(SO) >= os.path.getmtime(d) for d in deps):
         return SO
     cmd = ["gcc", "-O2", "-std=gnu99", "-fopenmp", "-fPIC", "-shared", "-ffp-contract=off",
-           SRC, MGSRC, "-o", SO, "-lm"]
+           SRC, MGSRC, ADMSRC, "-o", SO, "-lm"]
     subprocess.run(cmd, check=True)
     return SO
 
@@ -48,6 +49,9 @@ def lib():
             "oracle_z4_rhs": [LD, pp, pp, C.c_double, pp, C.POINTER(abi.Z4Params)],
             "oracle_z4_boundary": [LD, pp, pp, C.c_double, pp, C.POINTER(abi.Z4Params)],
             "oracle_z4_evolve": [LD, pp, C.c_double, C.c_int, C.POINTER(abi.Z4Params)],
+            "oracle_to_adm": [LD, pp, pp, C.c_double],
+            "oracle_adm_constraints": [LD, pp, pp, C.c_int, C.c_int],
+            "oracle_norms": [LD, pp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)],
         }.items():
             f = getattr(L, name)
             f.restype = C.c_int
@@ -127,3 +131,31 @@ def z4_evolve(level, u, dt, nsteps, params):
     if lib().oracle_z4_evolve(C.byref(level.desc), _ptrs(u), dt, nsteps, C.byref(params)):
         raise RuntimeError("oracle z4 evolve failed")
     return u
+
+
+def to_adm(level, u, chipsipower=-4.0):
+    """ADM g_ij, K_ij (12, npoints) from a BSSN or Z4c state (first 14 rows)."""
+    adm = np.zeros((12, u.shape[1]))
+    lib().oracle_to_adm(C.byref(level.desc), _ptrs(np.ascontiguousarray(u)), _ptrs(adm), chipsipower)
+    return adm
+
+
+def adm_constraints(level, adm, order_centered, mode=0, out=None):
+    """ham, mom_i (and normham, normmom_i for mode 1 / 2 = term by term) on
+    the flag-0 points; other points of out are left as they are."""
+    nout = 8 if mode else 4
+    out = np.zeros((nout, adm.shape[1])) if out is None else out
+    if lib().oracle_adm_constraints(C.byref(level.desc), _ptrs(np.ascontiguousarray(adm)), _ptrs(out),
+                                    order_centered, mode):
+        raise RuntimeError("oracle constraints failed")
+    return out
+
+
+def norms(level, v):
+    """(RMS, max |.|) of each row of v over the flag-0 points."""
+    v = np.ascontiguousarray(v, dtype=np.float64).reshape(-1, level.npoints)
+    n2 = np.zeros(v.shape[0])
+    ni = np.zeros(v.shape[0])
+    dp = lambda x: x.ctypes.data_as(C.POINTER(C.c_double))
+    lib().oracle_norms(C.byref(level.desc), _ptrs(v), v.shape[0], dp(n2), dp(ni))
+    return n2, ni

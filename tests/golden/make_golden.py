@@ -6,7 +6,7 @@ oracle/build_ref.py, on small parfiles and stores its raw FP64 dumps
 sources in this container; the fixtures it writes are committed so the tests
 never need the reference at run time.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]
 """
 import os
 import shutil
@@ -107,6 +107,25 @@ order_dissipation = 6
 iterations = 4
 nrharness_dump = 0 4
 """,
+    # puncture with generic shift and KO: ADM variables and constraints
+    "bssn_punc_con": BSSN_COMMON + """
+physics = adm bssn punctures nrharness
+mass1 = 1
+mass2 = 0
+punctures_solver = none
+bssn_initial_lapse = oochi05
+bssn_initial_shift = zero
+nxyz = 12
+dxyz = 0.5
+order_centered = 4
+order_advection = 4
+advection_lopsided = 1
+order_dissipation = 6
+iterations = 3
+nrharness_dump = 3
+nrharness_constraints = yes
+adm_normalizedConstraints = yes
+""",
 }
 
 
@@ -159,6 +178,20 @@ nrharness_dump = 0 1
 nrharness_rhs = yes
 nrharness_length = 4.5
 nrharness_seed = 13
+""",
+    # ADM variables from the Z4c state and term-by-term normalised constraints
+    "z4_fourier_con": Z4_COMMON + """
+nxyz = 12
+dxyz = 0.4
+order_centered = 6
+order_advection = 6
+order_dissipation = 6
+iterations = 2
+nrharness_dump = 2
+nrharness_constraints = yes
+adm_normalizedConstraints = yes TermByTerm
+nrharness_length = 4.8
+nrharness_seed = 21
 """,
     "z4_fourier_o6": Z4_COMMON + """
 nxyz = 10
@@ -262,7 +295,10 @@ def run_case(name, par):
 if __name__ == "__main__":
     if not os.path.exists(BAM):
         sys.exit("oracle/_ref/bam missing: run python oracle/build_ref.py first")
+    only = set(sys.argv[1:])  # optional: regenerate only the named cases
     for n, p in CASES.items():
-        run_case(n, p)
+        if not only or n in only:
+            run_case(n, p)
     for n, p in MG_CASES.items():
-        run_mg_case(n, p)
+        if not only or n in only:
+            run_mg_case(n, p)
