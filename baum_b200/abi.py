@@ -302,6 +302,9 @@ def lib():
         "nrgpu_mg_create": (C.c_int, [C.c_int, C.c_double, C.POINTER(MgParams), C.POINTER(vp)]),
         "nrgpu_mg_destroy": (C.c_int, [vp]),
         "nrgpu_mg_solve": (C.c_int, [vp, vp, vp, vp, C.POINTER(C.c_int), C.POINTER(C.c_double), vp]),
+        "nrgpu_to_adm": (C.c_int, [vp, pp, pp, C.c_double, vp]),
+        "nrgpu_adm_constraints": (C.c_int, [vp, pp, pp, C.c_int, C.c_int, vp]),
+        "nrgpu_norms": (C.c_int, [vp, pp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), vp]),
         "nrgpu_puncture_coefficients": (C.c_int, [C.c_int, C.c_double, C.c_int, C.POINTER(C.c_double),
                                                   C.POINTER(C.c_double), C.POINTER(C.c_double),
                                                   C.POINTER(C.c_double), vp, vp, vp]),

@@ -1,0 +1,77 @@
+"""Host-side mirror of the reference's ADM diagnostics over the C ABI.
+
+``bssn_to_adm_vl`` / ``z4_to_adm_vl`` (bssn.c:132-197, z4.c:93-124) fill the
+ADM metric and extrinsic curvature from the conformal variables at
+POST_EVOLVE; ``computeadmconstraints`` (adm.c:14-74) evaluates
+``adm_constraints_N`` on them at output time; the 0d output reduces the
+results with ``bampi_allreduce_norm2`` / ``_normInf`` (reduce.c:209-266,
+output0d.c:62-73).  A variable list here is a contiguous float64 CUDA
+tensor of shape (nvars, npoints); all arithmetic runs in libnrgpu.so.
+"""
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import abi
+from .bssn import _ptrs, _stream
+
+ADM_VARS = ["adm_gxx", "adm_gxy", "adm_gxz", "adm_gyy", "adm_gyz", "adm_gzz",
+            "adm_Kxx", "adm_Kxy", "adm_Kxz", "adm_Kyy", "adm_Kyz", "adm_Kzz"]
+CON_VARS = ["ham", "momx", "momy", "momz", "normham", "normmomx", "normmomy", "normmomz"]
+
+# adm_normalizedConstraints (bam_adm.c:40) -> constraint mode
+PLAIN, NORMALIZED, TERMBYTERM = 0, 1, 2
+
+
+def normalized_mode(value):
+    """The mode for a value of adm_normalizedConstraints, with the
+    reference's token tests (adm_constraints_N.c:62-63)."""
+    if not abi.getv(value, "yes"):
+        return PLAIN
+    return TERMBYTERM if abi.getv(value, "TermByTerm") else NORMALIZED
+
+
+def bssn_to_adm_vl(dl, u, adm=None, chipsipower=-4.0, stream=None):
+    """ADM g_ij, K_ij (12, npoints) from a BSSN (24) or Z4c (25) state."""
+    if not (u.is_cuda and u.dtype == torch.float64 and u.is_contiguous() and u.dim() == 2 and u.shape[0] >= 14):
+        raise ValueError("u is a contiguous float64 CUDA tensor of shape (>= 14, npoints)")
+    adm = dl.empty(12) if adm is None else adm
+    abi.check(abi.lib().nrgpu_to_adm(dl.handle, _ptrs(u, u.shape[0]), _ptrs(adm, 12), float(chipsipower),
+                                     _stream(stream)))
+    return adm
+
+
+z4_to_adm_vl = bssn_to_adm_vl
+
+
+def adm_constraints_N(dl, ucon, uadm, order_centered, mode=PLAIN, stream=None):
+    """ham, mom_i (+ normalised ones for mode != PLAIN) into ucon on the
+    flag-0 points (adm_constraints_N.c:22)."""
+    nout = 8 if mode else 4
+    if ucon.shape[0] < nout:
+        raise ValueError("ucon needs %d rows" % nout)
+    abi.check(abi.lib().nrgpu_adm_constraints(dl.handle, _ptrs(uadm, 12), _ptrs(ucon, ucon.shape[0]),
+                                              int(order_centered), int(mode), _stream(stream)))
+    return ucon
+
+
+def norms(dl, v, stream=None):
+    """(norm2, normInf) numpy arrays of each row of v over the flag-0 points."""
+    n = v.shape[0]
+    n2 = np.zeros(n)
+    ni = np.zeros(n)
+    dp = lambda x: x.ctypes.data_as(C.POINTER(C.c_double))
+    abi.check(abi.lib().nrgpu_norms(dl.handle, _ptrs(v, n), n, dp(n2), dp(ni), _stream(stream)))
+    return n2, ni
+
+
+def computeadmconstraints(dl, u, order_centered, mode=PLAIN, chipsipower=-4.0, stream=None):
+    """to_adm + constraints + norms of one level: returns (adm, con,
+    {name: (norm2, normInf)}), the numbers the reference writes to its
+    ham / mom 0d output files."""
+    adm = bssn_to_adm_vl(dl, u, chipsipower=chipsipower, stream=stream)
+    con = dl.empty(8 if mode else 4)
+    adm_constraints_N(dl, con, adm, order_centered, mode, stream)
+    n2, ni = norms(dl, con, stream)
+    return adm, con, {name: (n2[i], ni[i]) for i, name in enumerate(CON_VARS[:con.shape[0]])}

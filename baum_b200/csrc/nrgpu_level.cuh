@@ -25,4 +25,7 @@ struct nrgpu_level {
   size_t scratch_points;
   // device copy of a host state for the host-buffer entry points
   double *hoststate;
+  // points with boundary flag 0, and the norm reduction buffer (first use)
+  long ninner;
+  double *d_red;
 };

@@ -99,6 +99,7 @@ extern "C" int nrgpu_level_create(const nrgpu_level_desc *d, nrgpu_level **out) 
     L->hbox[b] = BoxGeo{d->box[b].m, d->box[b].n, d->box[b].o, d->box[b].noffset, d->box[b].x0, d->box[b].y0,
                         d->box[b].z0};
   L->nflagpts = (int)fl.size();
+  L->ninner = (long)d->npoints - (long)fl.size();
   bool ok = cudaMalloc(&L->d_boundary, sizeof(int) * d->npoints) == cudaSuccess &&
             cudaMalloc(&L->d_box, sizeof(BoxGeo) * d->nboxes) == cudaSuccess &&
             cudaMalloc(&L->d_status, sizeof(int) * 4) == cudaSuccess &&
@@ -125,6 +126,7 @@ extern "C" int nrgpu_level_destroy(nrgpu_level *L) {
   cudaFree(L->d_flagpts);
   cudaFree(L->scratch);
   cudaFree(L->hoststate);
+  cudaFree(L->d_red);
   free(L->hbox);
   free(L);
   return NRGPU_OK;

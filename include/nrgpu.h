@@ -258,6 +258,36 @@ int nrgpu_puncture_coefficients(int m, double dx, int npunc, const double *mass,
                                 const double *pos, const double *mom, const double *spin,
                                 double *a, double *b, void *stream);
 
+/* ---- ADM diagnostics ------------------------------------------------------
+ * ADM metric and extrinsic curvature from the conformal variables:
+ * bssn_to_adm_vl (projects/bssn/bssn.c:132-197) and z4_to_adm_vl
+ * (projects/z4/z4.c:93-124), psi = chi^(1/chipsipower),
+ * g_ij = psi^4 g~_ij, K_ij = psi^4 A~_ij + K g_ij / 3, on every point.
+ * u: the first 14 evolved variables of either system (g~ 6, chi, A~ 6, K;
+ * for Z4c the K slot is Khat, as in the reference); adm: g 6 then K 6. */
+int nrgpu_to_adm(nrgpu_level *L, const double *const *u, double *const *adm, double chipsipower, void *stream);
+
+/* adm_normalizedConstraints (projects/adm/bam_adm.c:40): no, yes,
+ * "yes TermByTerm" */
+enum { NRGPU_CON_PLAIN = 0, NRGPU_CON_NORMALIZED = 1, NRGPU_CON_TERMBYTERM = 2 };
+
+/* Hamiltonian and momentum constraints of the ADM variables:
+ * adm_constraints_N (projects/adm/adm_constraints_N.c:22, called by
+ * computeadmconstraints, adm.c:14-74) without matter and with usepsi = 0,
+ * on the points with boundary flag 0, centred order_centered with the
+ * order ladder at box edges.  con: ham, mom1, mom2, mom3 and, for
+ * mode != NRGPU_CON_PLAIN, normham, normmom1..3.  Flagged points of con are
+ * not written. */
+int nrgpu_adm_constraints(nrgpu_level *L, const double *const *adm, double *const *con, int order_centered,
+                          int mode, void *stream);
+
+/* norm2 (RMS) and normInf (max |u|) of nvars (<= 32) variables over the
+ * points with boundary flag 0: bampi_allreduce_norm2 / bampi_allreduce_normInf
+ * (main/bampi/reduce.c:209-266) on one rank.  Waits for the stream; the
+ * results are in norm2[nvars], norminf[nvars] on return. */
+int nrgpu_norms(nrgpu_level *L, const double *const *vars, int nvars, double *norm2, double *norminf,
+                void *stream);
+
 /* ---- diagnostics -------------------------------------------------------- */
 
 /* Measured FP64 FMA throughput of the current device (FLOP/s, 2 per FMA),
