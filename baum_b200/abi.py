@@ -305,6 +305,18 @@ def lib():
         "nrgpu_to_adm": (C.c_int, [vp, pp, pp, C.c_double, vp]),
         "nrgpu_adm_constraints": (C.c_int, [vp, pp, pp, C.c_int, C.c_int, vp]),
         "nrgpu_norms": (C.c_int, [vp, pp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), vp]),
+        "nrgpu_mlp_nparams": (C.c_int, []),
+        "nrgpu_mlp_create": (C.c_int, [C.c_int, C.POINTER(vp)]),
+        "nrgpu_mlp_destroy": (C.c_int, [vp]),
+        "nrgpu_mlp_set_params": (C.c_int, [vp, C.POINTER(C.c_float), C.c_int]),
+        "nrgpu_mlp_get_params": (C.c_int, [vp, C.POINTER(C.c_float), C.c_int]),
+        "nrgpu_mlp_set_conditions": (C.c_int, [vp, C.POINTER(C.c_double), C.c_int]),
+        "nrgpu_mlp_features": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, C.c_double, vp]),
+        "nrgpu_mlp_copy_features": (C.c_int, [vp, C.c_int, C.POINTER(C.c_uint16)]),
+        "nrgpu_mlp_train_step": (C.c_int, [vp, vp, C.c_int, C.c_float, C.c_int, C.POINTER(C.c_float), vp]),
+        "nrgpu_mlp_gradients": (C.c_int, [vp, C.POINTER(C.c_float), C.c_int]),
+        "nrgpu_mlp_forward": (C.c_int, [vp, C.c_int, vp, vp]),
+        "nrgpu_mlp_predict_u": (C.c_int, [vp, C.POINTER(C.c_double), C.c_int, C.c_double, C.c_double, vp, vp]),
         "nrgpu_puncture_coefficients": (C.c_int, [C.c_int, C.c_double, C.c_int, C.POINTER(C.c_double),
                                                   C.POINTER(C.c_double), C.POINTER(C.c_double),
                                                   C.POINTER(C.c_double), vp, vp, vp]),

@@ -1,0 +1,291 @@
+"""Learned warm start of the puncture multigrid (no counterpart in the reference).
+
+A coordinate MLP conditioned on the binary's parameters (masses, positions,
+Bowen-York momenta and spins) predicts the correction u of the puncture
+method; the multigrid then runs V cycles from that guess on the finest level
+(cycle type "V", not the full-V driver, which would overwrite the guess from
+the coarsest level up: solve.c:40,89-91, utility.c:61-82), to the same
+1e-10 RMS residual.  The multigrid stays the judge: the guess only changes
+where it starts.
+
+Everything numeric runs in libnrgpu.so (nrgpu_mlp_*, nrgpu_mg_*): features,
+the BF16 tensor-core products, the backward pass, Adam, the inference into
+an FP64 u.  This module generates the training set with the GPU multigrid,
+trains, evaluates and stores the weights.
+
+    python -m baum_b200.warmstart --sets 2000 --out <dir>
+"""
+import argparse
+import ctypes as C
+import functools
+import json
+import os
+import time
+
+import numpy as np
+import torch
+
+from . import abi
+from .punctures import Binary, Multigrid
+
+WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "warmstart_c2.npz")
+USCALE = 0.1
+C2_M, C2_DX = 130, 0.125   # nxyz = 128 inner + Robin layer, x in [-8.06, 8.06]
+
+
+def cond_vector(b):
+    """The 20-double conditioning vector of a binary (two punctures)."""
+    if len(b.mass) != 2:
+        raise ValueError("the warm start is trained for two punctures")
+    return np.concatenate([b.mass, b.pos.ravel(), b.mom.ravel(), b.spin.ravel()]).astype(np.float64)
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class Network:
+    """The device network (nrgpu_mlp): parameters, training, inference."""
+
+    def __init__(self, max_batch=16384, params=None, uscale=USCALE):
+        L = abi.lib()
+        self.nparams = L.nrgpu_mlp_nparams()
+        h = C.c_void_p()
+        abi.check(L.nrgpu_mlp_create(int(max_batch), C.byref(h)))
+        self.handle, self.max_batch, self.uscale = h, max_batch, uscale
+        if params is not None:
+            self.set_params(params)
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        abi.check(abi.lib().nrgpu_mlp_set_params(self.handle, p.ctypes.data_as(C.POINTER(C.c_float)), p.size))
+
+    def params(self):
+        p = np.zeros(self.nparams, dtype=np.float32)
+        abi.check(abi.lib().nrgpu_mlp_get_params(self.handle, p.ctypes.data_as(C.POINTER(C.c_float)), p.size))
+        return p
+
+    def gradients(self):
+        g = np.zeros(self.nparams, dtype=np.float32)
+        abi.check(abi.lib().nrgpu_mlp_gradients(self.handle, g.ctypes.data_as(C.POINTER(C.c_float)), g.size))
+        return g
+
+    def set_conditions(self, conds):
+        """The (nsets, 20) table of conditioning vectors rows refer to."""
+        conds = np.ascontiguousarray(np.atleast_2d(conds), dtype=np.float64)
+        abi.check(abi.lib().nrgpu_mlp_set_conditions(self.handle, conds.ctypes.data_as(C.POINTER(C.c_double)),
+                                                     conds.shape[0]))
+
+    def features(self, set_idx, pt_idx, m, dx):
+        """Feature rows of the batch: set_idx, pt_idx int32 CUDA tensors."""
+        abi.check(abi.lib().nrgpu_mlp_features(self.handle, C.c_void_p(set_idx.data_ptr()),
+                                               C.c_void_p(pt_idx.data_ptr()), int(pt_idx.numel()), int(m),
+                                               float(dx), _stream()))
+
+    def copy_features(self, n):
+        """The last n feature rows as float64 (exact BF16 values)."""
+        h = np.zeros((n, 32), dtype=np.uint16)
+        abi.check(abi.lib().nrgpu_mlp_copy_features(self.handle, n, h.ctypes.data_as(C.POINTER(C.c_uint16))))
+        return (h.astype(np.uint32) << 16).view(np.float32).astype(np.float64)
+
+    def train_step(self, y, lr, update=True, want_loss=False):
+        loss = C.c_float()
+        abi.check(abi.lib().nrgpu_mlp_train_step(self.handle, C.c_void_p(y.data_ptr()), int(y.numel()),
+                                                 float(lr), int(update), C.byref(loss) if want_loss else None,
+                                                 _stream()))
+        return loss.value if want_loss else None
+
+    def forward(self, n):
+        out = torch.empty(n, dtype=torch.float32, device="cuda")
+        abi.check(abi.lib().nrgpu_mlp_forward(self.handle, int(n), C.c_void_p(out.data_ptr()), _stream()))
+        return out
+
+    def predict_u(self, binary, m, dx, out=None):
+        """The warm start u (m^3 FP64 CUDA tensor) for one binary."""
+        cv = cond_vector(binary)
+        u = torch.empty(m ** 3, dtype=torch.float64, device="cuda") if out is None else out
+        abi.check(abi.lib().nrgpu_mlp_predict_u(self.handle, cv.ctypes.data_as(C.POINTER(C.c_double)), int(m),
+                                                float(dx), float(self.uscale), C.c_void_p(u.data_ptr()),
+                                                _stream()))
+        return u
+
+    def save(self, path, **meta):
+        os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+        np.savez_compressed(path, params=self.params(), uscale=self.uscale, meta=json.dumps(meta))
+
+    @staticmethod
+    def load(path=WEIGHTS, max_batch=65536):
+        z = np.load(path)
+        return Network(max_batch, z["params"], float(z["uscale"]))
+
+    def close(self):
+        if self.handle:
+            abi.lib().nrgpu_mlp_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def init_params(rng):
+    """Weights of variance 1/fan_in, zero biases, a small output layer (the
+    flat layout of nrgpu_mlp: W1 [32][128], b1, W2..W4 [128][128] with
+    biases, w5 [128], b5)."""
+    parts = []
+    for l in range(4):
+        k = 32 if l == 0 else 128
+        parts += [rng.standard_normal(k * 128) / np.sqrt(k), np.zeros(128)]
+    parts += [0.01 * rng.standard_normal(128), np.zeros(1)]
+    return np.concatenate(parts).astype(np.float32)
+
+
+@functools.lru_cache(maxsize=2)
+def grid_coords(m, dx):
+    h0 = -0.5 * (m - 1) * dx
+    i = np.arange(m ** 3)
+    return h0 + (i % m) * dx, h0 + ((i // m) % m) * dx, h0 + (i // (m * m)) * dx
+
+
+def sample_points(b, m, dx, n, rng, near=2.5):
+    """n grid points: half uniform over the cube, half within `near` of a
+    puncture (where u varies fastest)."""
+    x, y, z = grid_coords(m, dx)
+    close = np.zeros(x.size, dtype=bool)
+    for p in b.pos:
+        close |= (x - p[0]) ** 2 + (y - p[1]) ** 2 + (z - p[2]) ** 2 < near * near
+    cand = np.flatnonzero(close)
+    k = n // 2
+    return np.concatenate([rng.integers(0, m ** 3, n - k), rng.choice(cand, k, replace=len(cand) < k)])
+
+
+def solve_binary(mg, b, u=None):
+    """GPU multigrid of binary b from u (zeros by default); returns (u,
+    V cycles, residual)."""
+    a, bb = mg.coefficients(b)
+    if u is None:
+        u = torch.zeros(mg.m ** 3, dtype=torch.float64, device="cuda")
+    n, res = mg.solve(a, bb, u)
+    return u, n, res
+
+
+def generate(binaries, m=C2_M, dx=C2_DX, npts=16384, cycles=80, seed=0, log=print):
+    """Training set: each binary solved by the GPU full-V multigrid (capped
+    at `cycles` V cycles, residual ~1e-8), npts sampled points per binary.
+    Returns (conds[nsets,20], set_idx, pt_idx, y = u / USCALE)."""
+    rng = np.random.default_rng(seed)
+    mg = Multigrid(m, dx, abi.mg_params(vcycle_nmax=cycles))
+    conds, sets, pts, ys = [], [], [], []
+    t0 = time.time()
+    for s, b in enumerate(binaries):
+        u, n, res = solve_binary(mg, b)
+        uh = u.cpu().numpy()
+        idx = sample_points(b, m, dx, npts, rng)
+        conds.append(cond_vector(b))
+        sets.append(np.full(npts, s, dtype=np.int32))
+        pts.append(idx.astype(np.int32))
+        ys.append((uh[idx] / USCALE).astype(np.float32))
+        if log and (s % 200 == 0 or s == len(binaries) - 1):
+            log("  set %d/%d: %d V cycles, residual %.2e, max|u| %.3f (%.0f s)"
+                % (s + 1, len(binaries), n, res, np.abs(uh).max(), time.time() - t0))
+    mg.close()
+    return np.array(conds), np.concatenate(sets), np.concatenate(pts), np.concatenate(ys)
+
+
+def train(net, data, m=C2_M, dx=C2_DX, epochs=12, batch=16384, lr0=2e-3, lr1=2e-5, seed=1, log=print):
+    """Adam with a cosine rate from lr0 to lr1 over all steps; the rows are
+    reshuffled every epoch.  Returns the per-epoch mean sampled losses."""
+    conds, sets, pts, ys = data
+    net.set_conditions(conds)
+    rng = np.random.default_rng(seed)
+    n = (len(ys) // batch) * batch
+    steps = epochs * (n // batch)
+    hist, k = [], 0
+    for e in range(epochs):
+        perm = rng.permutation(len(ys))[:n]
+        ds = torch.from_numpy(sets[perm]).cuda()
+        dp = torch.from_numpy(pts[perm]).cuda()
+        dy = torch.from_numpy(ys[perm]).cuda()
+        tot, cnt = 0.0, 0
+        for i in range(0, n, batch):
+            lr = lr1 + 0.5 * (lr0 - lr1) * (1.0 + np.cos(np.pi * k / steps))
+            net.features(ds[i:i + batch], dp[i:i + batch], m, dx)
+            want = (i // batch) % 50 == 0
+            l = net.train_step(dy[i:i + batch], lr, want_loss=want)
+            if want:
+                tot, cnt = tot + l, cnt + 1
+            k += 1
+        hist.append(tot / max(1, cnt))
+        if log:
+            log("  epoch %d: loss %.3e (lr %.1e)" % (e + 1, hist[-1], lr))
+    torch.cuda.synchronize()
+    return hist
+
+
+def evaluate(net, binaries, m=C2_M, dx=C2_DX, nmax=2000, log=print):
+    """V cycles to 1e-10 for each binary: full-V from u = 0 (the reference's
+    default), V cycles from u = 0, V cycles from the network's u."""
+    mg = Multigrid(m, dx, abi.mg_params(vcycle_nmax=nmax))
+    mgv = Multigrid(m, dx, abi.mg_params(vcycle_nmax=nmax, fullV=0))
+    rows = []
+    for b in binaries:
+        _, n_full, r_full = solve_binary(mg, b)
+        u0, n_v, r_v = solve_binary(mgv, b)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g = net.predict_u(b, m, dx)
+        torch.cuda.synchronize()
+        t_inf = time.perf_counter() - t0
+        err = (g - u0).norm().item() / u0.norm().item()
+        t0 = time.perf_counter()
+        _, n_w, r_w = solve_binary(mgv, b, u=g)
+        torch.cuda.synchronize()
+        t_w = time.perf_counter() - t0
+        rows.append({"cond": cond_vector(b).tolist(), "fullV_from_zero": n_full, "V_from_zero": n_v,
+                     "V_from_mlp": n_w, "res_fullV": r_full, "res_V": r_v, "res_mlp": r_w,
+                     "mlp_rel_l2_error": err, "inference_ms": 1e3 * t_inf, "solve_from_mlp_ms": 1e3 * t_w})
+        if log:
+            log("  fullV %4d  V %4d  V(mlp) %4d   |u_mlp-u|/|u| %.2e" % (n_full, n_v, n_w, err))
+    mg.close()
+    mgv.close()
+    return rows
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--sets", type=int, default=2000)
+    ap.add_argument("--heldout", type=int, default=12)
+    ap.add_argument("--npts", type=int, default=16384)
+    ap.add_argument("--cycles", type=int, default=80)
+    ap.add_argument("--epochs", type=int, default=12)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--out", default=os.path.dirname(WEIGHTS))
+    a = ap.parse_args()
+    torch.cuda.set_device(0)
+    abi.check(abi.lib().nrgpu_init(0))
+    rng = np.random.default_rng(a.seed)
+    train_b = [Binary.sample(rng) for _ in range(a.sets)]
+    held_b = [Binary.sample(np.random.default_rng(a.seed + 1 + i)) for i in range(a.heldout)]
+    t0 = time.time()
+    print("generating %d solutions at %d^3" % (a.sets, C2_M), flush=True)
+    data = generate(train_b, npts=a.npts, cycles=a.cycles, seed=a.seed)
+    t_gen = time.time() - t0
+    net = Network(16384, init_params(np.random.default_rng(a.seed + 7)))
+    t0 = time.time()
+    hist = train(net, data, epochs=a.epochs)
+    t_train = time.time() - t0
+    path = os.path.join(a.out, "warmstart_c2.npz")
+    net.save(path, sets=a.sets, npts=a.npts, cycles=a.cycles, epochs=a.epochs, seed=a.seed, m=C2_M, dx=C2_DX)
+    print("evaluating on %d held-out binaries" % a.heldout, flush=True)
+    rows = evaluate(Network.load(path), held_b)
+    rep = {"train_seconds": t_train, "generate_seconds": t_gen, "loss_history": hist, "heldout": rows,
+           "weights": path}
+    with open(os.path.join(a.out, "warmstart_report.json"), "w") as f:
+        json.dump(rep, f, indent=1)
+    print(json.dumps({k: v for k, v in rep.items() if k != "heldout"}))
+
+
+if __name__ == "__main__":
+    main()

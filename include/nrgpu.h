@@ -25,6 +25,7 @@
 #define NRGPU_H
 
 #include <stddef.h>
+#include <stdint.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -287,6 +288,45 @@ int nrgpu_adm_constraints(nrgpu_level *L, const double *const *adm, double *cons
  * results are in norm2[nvars], norminf[nvars] on return. */
 int nrgpu_norms(nrgpu_level *L, const double *const *vars, int nvars, double *norm2, double *norminf,
                 void *stream);
+
+/* ---- learned warm start of the puncture solve ----------------------------
+ * No counterpart in the reference.  A coordinate MLP (NRGPU_MLP_IN features
+ * -> 4 hidden layers of NRGPU_MLP_HIDDEN, SiLU -> 1) conditioned on the
+ * binary's parameters predicts the correction u that PunctureData
+ * (Punctures.c:439) otherwise solves for from u = 0.  BF16 products with
+ * FP32 accumulation on the tensor cores; FP32 master weights and Adam.
+ * A conditioning vector is 20 doubles: m1 m2, pos1 pos2, mom1 mom2,
+ * spin1 spin2 (the parameters of ReadPunctureParameters, Punctures.c:221). */
+#define NRGPU_MLP_IN 32
+#define NRGPU_MLP_HIDDEN 128
+typedef struct nrgpu_mlp nrgpu_mlp;
+int nrgpu_mlp_nparams(void);
+int nrgpu_mlp_create(int max_batch, nrgpu_mlp **out);
+int nrgpu_mlp_destroy(nrgpu_mlp *mlp);
+int nrgpu_mlp_set_params(nrgpu_mlp *mlp, const float *host_params, int n);
+int nrgpu_mlp_get_params(nrgpu_mlp *mlp, float *host_params, int n);
+/* the table of nsets conditioning vectors (host, copied) that feature rows
+ * refer to */
+int nrgpu_mlp_set_conditions(nrgpu_mlp *mlp, const double *host_cond, int nsets);
+/* feature rows of n points: row r is grid point d_pt[r] (x fastest) of the
+ * m^3 cube of spacing dx centred on the origin, for binary d_set[r] of the
+ * conditioning table (d_set, d_pt: device int arrays) */
+int nrgpu_mlp_features(nrgpu_mlp *mlp, const int *d_set, const int *d_pt, int n, int m, double dx, void *stream);
+/* the last n feature rows as BF16 bit patterns (host [n][NRGPU_MLP_IN]) */
+int nrgpu_mlp_copy_features(nrgpu_mlp *mlp, int n, uint16_t *host);
+/* one step on the last feature rows against targets d_y[n] (device):
+ * forward, MSE loss, backward, and with update != 0 an Adam step of rate
+ * lr.  The loss is written to *loss (host) when loss != NULL. */
+int nrgpu_mlp_train_step(nrgpu_mlp *mlp, const float *d_y, int n, float lr, int update, float *loss,
+                         void *stream);
+/* the gradients of the last train step, in the parameter layout */
+int nrgpu_mlp_gradients(nrgpu_mlp *mlp, float *host_grad, int n);
+/* network output of the last feature rows into d_out[n] (device) */
+int nrgpu_mlp_forward(nrgpu_mlp *mlp, int n, float *d_out, void *stream);
+/* the warm start: u[m^3] (device, FP64) = uscale * network output at every
+ * point of the m^3 cube, for one binary (replaces the conditioning table) */
+int nrgpu_mlp_predict_u(nrgpu_mlp *mlp, const double *host_cond, int m, double dx, double uscale, double *u,
+                        void *stream);
 
 /* ---- diagnostics -------------------------------------------------------- */
 

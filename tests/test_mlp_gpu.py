@@ -1,0 +1,100 @@
+"""The warm-start network on the GPU (nrgpu_mlp_*, BF16 tensor-core products
+with FP32 accumulation) against its CPU FP64 oracle with the same BF16
+operand rounding (oracle/mlp_oracle.py): features bit-exact, forward and
+gradients within the FP32-accumulation error; training reduces the loss;
+and the trained weights shipped with the package at least halve the
+multigrid V cycles to the 1e-10 residual on binaries it was not trained on."""
+import numpy as np
+import pytest
+import torch
+
+from baum_b200 import warmstart
+from baum_b200.punctures import Binary
+from oracle import mlp_oracle as mo
+
+pytestmark = pytest.mark.gpu
+
+
+def case(n=2048, m=130, dx=0.125, seed=11):
+    rng = np.random.default_rng(seed)
+    bins = [Binary.sample(rng) for _ in range(3)]
+    conds = np.array([warmstart.cond_vector(b) for b in bins])
+    sets = rng.integers(0, 3, n).astype(np.int32)
+    pts = rng.integers(0, m ** 3, n).astype(np.int32)
+    return rng, conds, sets, pts, m, dx
+
+
+def net_with(rng, conds, sets, pts, m, dx, scale_out=30.0):
+    p = mo.init_params(rng)
+    p[mo.OFF["w5"][0]:mo.OFF["w5"][0] + mo.HID] *= scale_out
+    p32 = p.astype(np.float32)
+    net = warmstart.Network(4096, p32)
+    net.set_conditions(conds)
+    net.features(torch.from_numpy(sets).cuda(), torch.from_numpy(pts).cuda(), m, dx)
+    return net, p32.astype(np.float64)
+
+
+def test_features_are_bit_exact(gpu):
+    rng, conds, sets, pts, m, dx = case()
+    net, _ = net_with(rng, conds, sets, pts, m, dx)
+    X = net.copy_features(len(pts))
+    Xo = mo.features(conds, pts, m, dx, set_idx=sets)
+    assert np.array_equal(X, Xo)
+
+
+def test_forward_matches_oracle(gpu):
+    rng, conds, sets, pts, m, dx = case()
+    net, p = net_with(rng, conds, sets, pts, m, dx)
+    out = net.forward(len(pts)).cpu().numpy().astype(np.float64)
+    ref, _ = mo.forward(p, mo.features(conds, pts, m, dx, set_idx=sets))
+    assert np.abs(out - ref).max() <= 2e-3 * np.abs(ref).max()
+
+
+def test_gradients_match_oracle(gpu):
+    rng, conds, sets, pts, m, dx = case()
+    net, p = net_with(rng, conds, sets, pts, m, dx)
+    y = (0.1 * rng.standard_normal(len(pts))).astype(np.float32)
+    loss = net.train_step(torch.from_numpy(y).cuda(), 0.0, update=False, want_loss=True)
+    g = net.gradients().astype(np.float64)
+    lo, go = mo.loss_and_grad(p, mo.features(conds, pts, m, dx, set_idx=sets), y.astype(np.float64))
+    assert abs(loss - lo) <= 1e-4 * lo
+    for name, (o, s) in mo.OFF.items():
+        k = int(np.prod(s))
+        a, b = g[o:o + k], go[o:o + k]
+        assert np.linalg.norm(a - b) <= 1e-2 * np.linalg.norm(b) + 1e-9, name
+    # the parameters are untouched without update
+    assert np.array_equal(net.params(), p.astype(np.float32))
+
+
+def test_training_reduces_loss(gpu):
+    rng, conds, sets, pts, m, dx = case(n=4096)
+    net, _ = net_with(rng, conds, sets, pts, m, dx, scale_out=1.0)
+    # a smooth target of the features: the first puncture's m / (r + m)
+    X = mo.features(conds, pts, m, dx, set_idx=sets)
+    y = torch.from_numpy((X[:, 7] - 0.3).astype(np.float32)).cuda()
+    first = net.train_step(y, 1e-3, want_loss=True)
+    for _ in range(300):
+        last = net.train_step(y, 1e-3, want_loss=True)
+    assert last < 0.05 * first
+
+
+def test_predict_u_matches_oracle(gpu):
+    net = warmstart.Network.load()
+    b = Binary.sample(np.random.default_rng(99))
+    m, dx = 66, 0.25
+    u = net.predict_u(b, m, dx).cpu().numpy()
+    idx = np.random.default_rng(1).integers(0, m ** 3, 4096)
+    ref, _ = mo.forward(net.params().astype(np.float64), mo.features(warmstart.cond_vector(b), idx, m, dx))
+    assert np.abs(u[idx] - net.uscale * ref).max() <= 2e-3 * np.abs(net.uscale * ref).max()
+
+
+def test_warm_start_halves_vcycles(gpu):
+    """Binaries of the workload's distribution outside the training seeds,
+    at the workload's 130^3 grid: V cycles from the network's u versus V
+    cycles from u = 0 and the reference's full-V from u = 0."""
+    net = warmstart.Network.load()
+    rng = np.random.default_rng(424242)
+    rows = warmstart.evaluate(net, [Binary.sample(rng) for _ in range(2)], nmax=2000, log=None)
+    for r in rows:
+        assert r["res_mlp"] <= 1e-10
+        assert 2 * r["V_from_mlp"] <= min(r["V_from_zero"], r["fullV_from_zero"]), r
