@@ -119,10 +119,13 @@ def main():
             jobs.append((src, o, os.path.join(ref, d)))
     jobs.append((os.path.join(HERE, "harness", "nrharness.c"), os.path.join(obj, "harness__nrharness.o"),
                  os.path.join(HERE, "harness")))
+    jobs.append((os.path.join(HERE, "mpi_stub", "mpi_stub.c"), os.path.join(obj, "mpi_stub.o"),
+                 os.path.join(HERE, "mpi_stub")))
+    stub_h = os.path.join(HERE, "mpi_stub", "mpi.h")
 
     def compile_one(job):
         src, o, incdir = job
-        if os.path.exists(o) and os.path.getmtime(o) >= os.path.getmtime(src):
+        if os.path.exists(o) and os.path.getmtime(o) >= max(os.path.getmtime(src), os.path.getmtime(stub_h)):
             return None
         cmd = base + ["-I" + incdir, "-c", src, "-o", o]
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -173,6 +173,15 @@ int nrharness_post_initialdata(tL *level)
     if (level->v[Ind("punctures_u")]) dump_varlist(level, vl, "mg_u");
     vlfree(vl);
   }
+  if (Getv("nrharness_flags", "yes")) {
+    /* refinement flags of setRPflags (flag.c:122-255): flagprolong on levels
+       with a parent, flagrestrict on levels with a child */
+    tVarList *vl = vlalloc(level);
+    if (level->v[Ind("flagprolong")]) vlpush(vl, Ind("flagprolong"));
+    if (level->v[Ind("flagrestrict")]) vlpush(vl, Ind("flagrestrict"));
+    if (vl->n) dump_varlist(level, vl, "flags");
+    vlfree(vl);
+  }
   if (u && dump_requested(0)) dump_varlist(level, u, "state_it0");
   if (u && Getv("nrharness_rhs", "yes")) {
     tVarList *r = AddDuplicateEnable(u, "_nrh");
@@ -210,6 +219,7 @@ void bam_nrharness(void)
   AddPar("nrharness_dump", "none", "level iterations after which to dump the evolved variables");
   AddPar("nrharness_rhs", "no", "dump one RHS evaluation of the initial state [no,yes]");
   AddPar("nrharness_mg", "no", "dump punctures_u after the initial data solve [no,yes]");
+  AddPar("nrharness_flags", "no", "dump the refinement flags of every level after the initial data [no,yes]");
   AddPar("nrharness_constraints", "no", "with each state dump also dump ADM variables and constraints [no,yes]");
   AddPar("nrharness_data", "none", "synthetic data over the evolved variables [none,fourier]");
   AddPar("nrharness_amp", "1e-3", "amplitude of the Fourier perturbation");

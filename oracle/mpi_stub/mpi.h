@@ -1,7 +1,7 @@
 /* mpi.h -- single-rank stand-in for MPI, used only to build the reference
  * CPU code (BAM) as the oracle binary oracle/_ref/bam.  No MPI library exists
- * in this image; BAM at one rank only needs these calls to behave as the
- * identity (point-to-point never happens, reductions copy send to receive).
+ * in this image; at one rank reductions copy send to receive and
+ * point-to-point messages go to self (mpi_stub.c).
  * This is test infrastructure, not product code. */
 #ifndef NRGPU_ORACLE_MPI_STUB_H
 #define NRGPU_ORACLE_MPI_STUB_H
@@ -50,21 +50,17 @@ static inline int MPI_Allgather(const void *s, int n, MPI_Datatype t, void *r, i
   (void)rn; (void)rt; (void)c; nrgpu_stub_copy(s, r, n, t); return 0; }
 static inline int MPI_Bcast(void *b, int n, MPI_Datatype t, int root, MPI_Comm c) {
   (void)b; (void)n; (void)t; (void)root; (void)c; return 0; }
-/* point-to-point never happens at one rank; fail loudly if it does */
-static inline int nrgpu_stub_p2p(const char *what) {
-  fprintf(stderr, "mpi stub: %s called at one rank\n", what); exit(3); return 1; }
-static inline int MPI_Send(const void *b, int n, MPI_Datatype t, int d, int tag, MPI_Comm c) {
-  (void)b;(void)n;(void)t;(void)d;(void)tag;(void)c; return nrgpu_stub_p2p("MPI_Send"); }
-static inline int MPI_Recv(void *b, int n, MPI_Datatype t, int s, int tag, MPI_Comm c, MPI_Status *st) {
-  (void)b;(void)n;(void)t;(void)s;(void)tag;(void)c;(void)st; return nrgpu_stub_p2p("MPI_Recv"); }
-static inline int MPI_Isend(const void *b, int n, MPI_Datatype t, int d, int tag, MPI_Comm c, MPI_Request *q) {
-  (void)b;(void)n;(void)t;(void)d;(void)tag;(void)c;(void)q; return nrgpu_stub_p2p("MPI_Isend"); }
-static inline int MPI_Irecv(void *b, int n, MPI_Datatype t, int s, int tag, MPI_Comm c, MPI_Request *q) {
-  (void)b;(void)n;(void)t;(void)s;(void)tag;(void)c;(void)q; return nrgpu_stub_p2p("MPI_Irecv"); }
-static inline int MPI_Waitall(int n, MPI_Request *q, MPI_Status *st) { (void)n;(void)q;(void)st; return 0; }
-static inline int MPI_Probe(int s, int tag, MPI_Comm c, MPI_Status *st) {
-  (void)s;(void)tag;(void)c;(void)st; return nrgpu_stub_p2p("MPI_Probe"); }
-static inline int MPI_Get_count(const MPI_Status *st, MPI_Datatype t, int *n) { (void)st;(void)t; *n = 0; return 0; }
+/* point-to-point at one rank: messages to self, matched by tag in order
+ * (oracle/mpi_stub/mpi_stub.c); an unmatched receive at a wait is a
+ * deadlock and exits */
+int MPI_Send(const void *b, int n, MPI_Datatype t, int d, int tag, MPI_Comm c);
+int MPI_Recv(void *b, int n, MPI_Datatype t, int s, int tag, MPI_Comm c, MPI_Status *st);
+int MPI_Isend(const void *b, int n, MPI_Datatype t, int d, int tag, MPI_Comm c, MPI_Request *q);
+int MPI_Irecv(void *b, int n, MPI_Datatype t, int s, int tag, MPI_Comm c, MPI_Request *q);
+int MPI_Waitall(int n, MPI_Request *q, MPI_Status *st);
+int MPI_Probe(int s, int tag, MPI_Comm c, MPI_Status *st);
+static inline int MPI_Get_count(const MPI_Status *st, MPI_Datatype t, int *n) {
+  *n = st ? st->count / t : 0; return 0; }
 static inline int MPI_Sendrecv_replace(void *b, int n, MPI_Datatype t, int d, int stag, int s, int rtag,
                                        MPI_Comm c, MPI_Status *st) {
   (void)b;(void)n;(void)t;(void)d;(void)stag;(void)s;(void)rtag;(void)c;(void)st; return 0; }

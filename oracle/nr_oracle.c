@@ -672,8 +672,10 @@ static int rhs_stage(const nrgpu_level_desc *L, double *const *r, double *const 
 }
 
 /* evolve_rk_rk4 (rk.c:220-257) + algcon, u updated in place */
-int oracle_bssn_rk4_step(const nrgpu_level_desc *L, double *const *u, double dt,
-                         const nrgpu_bssn_params *p)
+/* the four RK4 stages of evolve_rk_rk4 (rk.c:220-257) without the
+ * algebraic constraints that bssn_algcon_wrapper applies afterwards */
+int oracle_bssn_rk4_stages(const nrgpu_level_desc *L, double *const *u, double dt,
+                           const nrgpu_bssn_params *p)
 {
   long np = L->npoints;
   double *buf = (double *)malloc(sizeof(double) * 3 * NV * np);
@@ -700,8 +702,15 @@ int oracle_bssn_rk4_step(const nrgpu_level_desc *L, double *const *u, double dt,
   vladd(np, V, 1.0, P, dt, R);
   e |= rhs_stage(L, R, P, V, p);
   vladd(np, u, 1.0, u, dt / 6, R);
-  oracle_bssn_algcon(L, u, p);
   free(buf);
+  return e;
+}
+
+int oracle_bssn_rk4_step(const nrgpu_level_desc *L, double *const *u, double dt,
+                         const nrgpu_bssn_params *p)
+{
+  int e = oracle_bssn_rk4_stages(L, u, dt, p);
+  oracle_bssn_algcon(L, u, p);
   return e;
 }
 
@@ -1090,7 +1099,7 @@ int oracle_z4_boundary(const nrgpu_level_desc *L, double *const *unew, double *c
 }
 
 /* z4_algcon on the g~ and A~ of a Z4c list: same operations as bssn_algcon */
-static void z4_algcon(const nrgpu_level_desc *L, double *const *u, const nrgpu_z4_params *p)
+void oracle_z4_algcon(const nrgpu_level_desc *L, double *const *u, const nrgpu_z4_params *p)
 {
   nrgpu_bssn_params q;
   double *bl[NV];
@@ -1102,7 +1111,7 @@ static void z4_algcon(const nrgpu_level_desc *L, double *const *u, const nrgpu_z
   oracle_bssn_algcon(L, bl, &q);
 }
 
-int oracle_z4_rk4_step(const nrgpu_level_desc *L, double *const *u, double dt, const nrgpu_z4_params *p)
+int oracle_z4_rk4_stages(const nrgpu_level_desc *L, double *const *u, double dt, const nrgpu_z4_params *p)
 {
   long np = L->npoints;
   double *buf = (double *)malloc(sizeof(double) * 3 * ZNV * np);
@@ -1131,8 +1140,14 @@ int oracle_z4_rk4_step(const nrgpu_level_desc *L, double *const *u, double dt, c
   ZSTAGE(V);
   vladd_nv(np, ZNV, u, 1.0, u, dt / 6, R);
 #undef ZSTAGE
-  z4_algcon(L, u, p);
   free(buf);
+  return e;
+}
+
+int oracle_z4_rk4_step(const nrgpu_level_desc *L, double *const *u, double dt, const nrgpu_z4_params *p)
+{
+  int e = oracle_z4_rk4_stages(L, u, dt, p);
+  oracle_z4_algcon(L, u, p);
   return e;
 }
 

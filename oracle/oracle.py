@@ -16,15 +16,16 @@ SO = os.path.join(HERE, "liboracle.so")
 SRC = os.path.join(HERE, "nr_oracle.c")
 MGSRC = os.path.join(HERE, "mg_oracle.c")
 ADMSRC = os.path.join(HERE, "adm_oracle.c")
+FMRSRC = os.path.join(HERE, "fmr_oracle.c")
 
 
 def build(force=False):
     """Compile the restatement with gcc (-O2, OpenMP, no fast-math)."""
-    deps = [SRC, MGSRC, ADMSRC, os.path.join(HERE, "..", "include", "nrgpu.h")]
+    deps = [SRC, MGSRC, ADMSRC, FMRSRC, os.path.join(HERE, "..", "include", "nrgpu.h")]
     if not force and os.path.exists(SO) and all(os.path.getmtime(SO) >= os.path.getmtime(d) for d in deps):
         return SO
     cmd = ["gcc", "-O2", "-std=gnu99", "-fopenmp", "-fPIC", "-shared", "-ffp-contract=off",
-           SRC, MGSRC, ADMSRC, "-o", SO, "-lm"]
+           SRC, MGSRC, ADMSRC, FMRSRC, "-o", SO, "-lm"]
     subprocess.run(cmd, check=True)
     return SO
 
@@ -50,6 +51,8 @@ def lib():
             "oracle_z4_boundary": [LD, pp, pp, C.c_double, pp, C.POINTER(abi.Z4Params)],
             "oracle_z4_evolve": [LD, pp, C.c_double, C.c_int, C.POINTER(abi.Z4Params)],
             "oracle_to_adm": [LD, pp, pp, C.c_double],
+            "oracle_fmr_flags": [LD, LD, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)],
+            "oracle_fmr_restrict_prolong": [LD, LD, C.c_int, pp, pp, C.c_int, C.c_int],
             "oracle_adm_constraints": [LD, pp, pp, C.c_int, C.c_int],
             "oracle_norms": [LD, pp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)],
         }.items():
@@ -159,3 +162,75 @@ def norms(level, v):
     dp = lambda x: x.ctypes.data_as(C.POINTER(C.c_double))
     lib().oracle_norms(C.byref(level.desc), _ptrs(v), v.shape[0], dp(n2), dp(ni))
     return n2, ni
+
+
+def fmr_flags(coarse, fine, nbuffer):
+    """(flagprolong of the fine level, flagrestrict of the coarse level)."""
+    fp = np.zeros(fine.npoints)
+    cr = np.zeros(coarse.npoints)
+    dp = lambda x: x.ctypes.data_as(C.POINTER(C.c_double))
+    if lib().oracle_fmr_flags(C.byref(coarse.desc), C.byref(fine.desc), nbuffer, dp(fp), dp(cr)):
+        raise RuntimeError("fine level does not nest in the coarse one")
+    return fp, cr
+
+
+def fmr_restrict_prolong(coarse, fine, uc, uf, order=4, nbuffer=3):
+    """restrict_prolong_varlist in place on uc (nv, npc) and uf (nv, npf)."""
+    e = lib().oracle_fmr_restrict_prolong(C.byref(coarse.desc), C.byref(fine.desc), uc.shape[0], _ptrs(uc),
+                                          _ptrs(uf), order, nbuffer)
+    if e:
+        raise RuntimeError("oracle restrict/prolong failed (%d)" % e)
+
+
+class FmrState:
+    """Host state of a multi-level evolution for the oracle driver: per
+    level u, the previous step's copy and the time interpolant.
+
+    advance() restates advance_levelandsublevels (main.c:397-418): step the
+    level, then its child twice (once for levels below lbo), then restrict
+    and prolong with the parent (restrict_prolong_evolve, inject.c:116-132;
+    the parent's u when both are at the same time, parentaligned
+    inject.c:10-21, else its time interpolant).  snap(l, iteration, u) is
+    called right after each level step, where the reference's POST_EVOLVE
+    functions run."""
+
+    def __init__(self, levels, u0, system, params, dt, lbo=0, order_ti=3, order_rp=4, nbuffer=3):
+        self.levels, self.system, self.params = levels, system, params
+        self.nv = u0[0].shape[0]
+        self.u = [np.ascontiguousarray(x, dtype=np.float64).copy() for x in u0]
+        self.up = [np.zeros_like(x) for x in self.u]
+        self.upp = [np.zeros_like(x) for x in self.u]
+        self.dt = [float(x) for x in dt]
+        self.iteration = [0] * len(levels)
+        self.lbo, self.order_ti, self.order_rp, self.nbuffer = lbo, order_ti, order_rp, nbuffer
+
+    def step_level(self, l):
+        f = lib().oracle_fmr_evolve_level
+        f.restype = C.c_int
+        child = l < len(self.levels) - 1
+        e = f(C.byref(self.levels[l].desc), self.system, C.byref(self.params[l]), self.nv, _ptrs(self.u[l]),
+              _ptrs(self.up[l]), _ptrs(self.upp[l]), C.c_double(self.dt[l]), self.iteration[l], int(child),
+              self.order_ti)
+        if e:
+            raise RuntimeError("oracle level step failed (%d)" % e)
+        self.iteration[l] += 1
+
+    def _advance(self, l, snap):
+        self.step_level(l)
+        if snap:
+            snap(l, self.iteration[l], self.u[l])
+        if l < len(self.levels) - 1:
+            self._advance(l + 1, snap)
+            if l >= self.lbo:
+                self._advance(l + 1, snap)
+        if l > 0:
+            tl = self.iteration[l] * self.dt[l]
+            tp = self.iteration[l - 1] * self.dt[l - 1]
+            aligned = not (tl < tp - 1e-10 or tp < tl - 1e-10)
+            uc = self.u[l - 1] if aligned else self.upp[l - 1]
+            fmr_restrict_prolong(self.levels[l - 1], self.levels[l], uc, self.u[l], self.order_rp, self.nbuffer)
+
+    def advance(self, nsteps=1, snap=None):
+        for _ in range(nsteps):
+            self._advance(0, snap)
+        return self.u

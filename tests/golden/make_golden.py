@@ -240,6 +240,68 @@ nrharness_mg = yes
 }
 
 
+# three nested levels, Berger-Oliger subcycling on every level, 4th-order
+# restriction/prolongation with 3 buffer points, 3rd-order time
+# interpolation; Fourier data on a flat background (the batched FMR
+# workload at small size)
+FMR_CASES = {
+    "z4_fmr3": Z4_COMMON + """
+grid = box
+amr = bo newfmr
+amr_fmr = nestedboxes
+amr_lmax = 2
+amr_nbuffer = 3
+nxyz = 16
+dxyz = 0.5
+order_centered = 4
+order_advection = 4
+advection_lopsided = 1
+order_dissipation = 6
+iterations = 2
+mass1 = 1
+mass2 = 0
+nrharness_length = 16
+nrharness_seed = 1
+nrharness_flags = yes
+nrharness_dump = 0 2 4 8
+""",
+}
+# the dumps and fields kept: the end of the second coarse step on every
+# level and the finest level after its second step; g11, chi, A12, Khat,
+# Gamma1, Theta, alpha, beta1 (the initial state is regenerated by
+# baum_b200/synthetic.py, bit for bit)
+FMR_KEEP = {"state_it2_l0", "state_it4_l1", "state_it8_l2", "state_it2_l2"}
+FMR_VARS = [0, 6, 8, 13, 14, 17, 18, 19]
+
+
+def run_fmr_case(name, par):
+    work = tempfile.mkdtemp(prefix="golden_")
+    try:
+        with open(os.path.join(work, name + ".par"), "w") as f:
+            f.write(par)
+        r = subprocess.run([BAM, "-nt", "4", name + ".par"], cwd=work, capture_output=True, text=True)
+        if r.returncode:
+            raise RuntimeError(r.stdout[-3000:] + r.stderr[-3000:])
+        arrays = {}
+        for l in range(3):
+            d = dumpfile.read(os.path.join(work, "state_it0_l%d.bin" % l))
+            arrays["boxes_l%d" % l] = np.array(d["boxes"], dtype=np.float64)
+            arrays["dx_l%d" % l] = d["dx"]
+            arrays["boundary_l%d" % l] = d["boundary"]
+            fl = dumpfile.read(os.path.join(work, "flags_l%d.bin" % l))
+            for nm, a in zip(fl["names"], fl["data"]):
+                arrays["%s_l%d" % (nm, l)] = a.astype(np.int8)
+        for tag in sorted(FMR_KEEP):
+            d = dumpfile.read(os.path.join(work, tag + ".bin"))
+            arrays[tag] = d["data"][FMR_VARS]
+        np.savez_compressed(os.path.join(OUT, name + ".npz"), vars=np.array(FMR_VARS), **arrays)
+        with open(os.path.join(OUT, name + ".par"), "w") as f:
+            f.write(par.lstrip())
+        print("wrote", name, sorted(arrays))
+    finally:
+        shutil.rmtree(work)
+
+
 def run_mg_case(name, par):
     import re
     work = tempfile.mkdtemp(prefix="golden_")
@@ -302,3 +364,6 @@ if __name__ == "__main__":
     for n, p in MG_CASES.items():
         if not only or n in only:
             run_mg_case(n, p)
+    for n, p in FMR_CASES.items():
+        if not only or n in only:
+            run_fmr_case(n, p)
