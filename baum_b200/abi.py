@@ -209,6 +209,23 @@ class MgParams(C.Structure):
                 ("falloff", C.c_double), ("batch", C.c_int)]
 
 
+class FmrParams(C.Structure):
+    _fields_ = [("system", C.c_int), ("lbo", C.c_int), ("order_timeinterpolation", C.c_int),
+                ("order_RP", C.c_int), ("nbuffer", C.c_int), ("use_graph", C.c_int)]
+
+
+SYSTEM_BSSN, SYSTEM_Z4C = 0, 1
+
+
+def fmr_params(**over):
+    """amr = bo with lbo 0, order_timeinterpolation 3, order_RP 4,
+    amr_nbuffer 3, Z4c, coarse steps replayed from a CUDA graph."""
+    p = FmrParams(SYSTEM_Z4C, 0, 3, 4, 3, 1)
+    for k, v in over.items():
+        setattr(p, k, v)
+    return p
+
+
 def mg_params(**over):
     """The puncture-solve settings of the binary-puncture workload:
     mg_relax_npre = npost = 3, mg_exact_nmin/nmax = 10/200, mg_size_nmin = 4,
@@ -317,6 +334,14 @@ def lib():
         "nrgpu_mlp_gradients": (C.c_int, [vp, C.POINTER(C.c_float), C.c_int]),
         "nrgpu_mlp_forward": (C.c_int, [vp, C.c_int, vp, vp]),
         "nrgpu_mlp_predict_u": (C.c_int, [vp, C.POINTER(C.c_double), C.c_int, C.c_double, C.c_double, vp, vp]),
+        "nrgpu_fmr_params_default": (C.c_int, [C.POINTER(FmrParams)]),
+        "nrgpu_fmr_create": (C.c_int, [C.c_int, C.POINTER(LevelDesc), C.POINTER(C.c_double), vp,
+                                       C.POINTER(FmrParams), C.POINTER(vp)]),
+        "nrgpu_fmr_destroy": (C.c_int, [vp]),
+        "nrgpu_fmr_flags": (C.c_int, [vp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+        "nrgpu_fmr_restrict_prolong": (C.c_int, [vp, C.c_int, pp, pp, vp]),
+        "nrgpu_fmr_advance": (C.c_int, [vp, pp, C.c_int, vp]),
+        "nrgpu_fmr_iteration": (C.c_int, [vp, C.c_int]),
         "nrgpu_puncture_coefficients": (C.c_int, [C.c_int, C.c_double, C.c_int, C.POINTER(C.c_double),
                                                   C.POINTER(C.c_double), C.POINTER(C.c_double),
                                                   C.POINTER(C.c_double), vp, vp, vp]),

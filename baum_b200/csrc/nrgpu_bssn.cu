@@ -803,8 +803,10 @@ int nrgpu_level_scratch(nrgpu_level *L, double **out);
 
 // fused RK4 (rk.c:220-257): stage s reads V_in, adds w_s*r to u and writes
 // V_out = P + c_s*r; both the interior and the flagged kernels do it
-extern "C" int nrgpu_bssn_rk4_step(nrgpu_level *L, double *const *u, double dt, const nrgpu_bssn_params *p,
-                                   void *stream) {
+// the four RK4 stages of evolve_rk_rk4 (rk.c:220-257) without the algebraic
+// constraints; the mesh-refinement driver puts the time interpolation between
+int nrgpu_bssn_rk4_stages(nrgpu_level *L, double *const *u, double dt, const nrgpu_bssn_params *p,
+                          cudaStream_t st) {
   if (!L) return nrgpu_set_error(NRGPU_ERR_ARG, "null level");
   int e;
   if ((e = check_params(p))) return e;
@@ -819,7 +821,6 @@ extern "C" int nrgpu_bssn_rk4_step(nrgpu_level *L, double *const *u, double dt, 
     V1.p[v] = scr + (1 * NRGPU_NV + v) * np;
     V2.p[v] = scr + (2 * NRGPU_NV + v) * np;
   }
-  cudaStream_t st = (cudaStream_t)stream;
   const long n = (long)NRGPU_NV * L->npoints;
   vlcopy_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(P, cptrs(U), L->npoints);
   const CVarPtrs cP = cptrs(P);
@@ -831,6 +832,13 @@ extern "C" int nrgpu_bssn_rk4_step(nrgpu_level *L, double *const *u, double dt, 
   if ((e = launch_rhs(L, cptrs(V1), V2, cP, U, E2, *p, st, true, true))) return e;
   if ((e = launch_rhs(L, cptrs(V2), V1, cP, U, E3, *p, st, true, true))) return e;
   if ((e = launch_rhs(L, cptrs(V1), V2, cP, U, E4, *p, st, true, true))) return e;
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_bssn_rk4_step(nrgpu_level *L, double *const *u, double dt, const nrgpu_bssn_params *p,
+                                   void *stream) {
+  int e = nrgpu_bssn_rk4_stages(L, u, dt, p, (cudaStream_t)stream);
+  if (e) return e;
   return nrgpu_bssn_algcon(L, u, p, stream);
 }
 
@@ -1072,8 +1080,7 @@ extern "C" int nrgpu_z4_boundary(nrgpu_level *L, double *const *unew, double *co
 }
 
 // evolve_rk_rk4 (rk.c:220) for the Z4c list + z4_algcon_wrapper (z4.c:49)
-extern "C" int nrgpu_z4_rk4_step(nrgpu_level *L, double *const *u, double dt, const nrgpu_z4_params *p,
-                                 void *stream) {
+int nrgpu_z4_rk4_stages(nrgpu_level *L, double *const *u, double dt, const nrgpu_z4_params *p, cudaStream_t st) {
   if (!L) return nrgpu_set_error(NRGPU_ERR_ARG, "null level");
   int e;
   if ((e = z4_check_params(p))) return e;
@@ -1088,7 +1095,6 @@ extern "C" int nrgpu_z4_rk4_step(nrgpu_level *L, double *const *u, double dt, co
     V1.p[v] = scr + (1 * ZNV + v) * np;
     V2.p[v] = scr + (2 * ZNV + v) * np;
   }
-  cudaStream_t st = (cudaStream_t)stream;
   const long n = (long)ZNV * L->npoints;
   z4_copy_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(P, z4_c(U), L->npoints);
   const ZCVarPtrs cP = z4_c(P);
@@ -1100,9 +1106,21 @@ extern "C" int nrgpu_z4_rk4_step(nrgpu_level *L, double *const *u, double dt, co
   if ((e = z4_launch(L, z4_c(V1), V2, cP, U, E2, *p, st, true, true))) return e;
   if ((e = z4_launch(L, z4_c(V2), V1, cP, U, E3, *p, st, true, true))) return e;
   if ((e = z4_launch(L, z4_c(V1), V2, cP, U, E4, *p, st, true, true))) return e;
+  return NRGPU_OK;
+}
+
+// z4_algcon (z4_algcon.c:22): the operations of bssn_algcon on g~ and A~
+int nrgpu_z4_algcon(nrgpu_level *L, double *const *u, const nrgpu_z4_params *p, cudaStream_t st) {
   VarPtrs gA;
-  for (int v = 0; v < NRGPU_NV; ++v) gA.p[v] = U.p[v];  // g~ 0..5 and A~ 7..12 as in BSSN
+  for (int v = 0; v < NRGPU_NV; ++v) gA.p[v] = u[v];  // g~ 0..5 and A~ 7..12 as in BSSN
   bssn_algcon_kernel<<<(L->npoints + 255) / 256, 256, 0, st>>>(gA, L->npoints, p->subtractA, p->normalizedetg);
   NRGPU_CUDA_TRY(cudaGetLastError());
   return NRGPU_OK;
+}
+
+extern "C" int nrgpu_z4_rk4_step(nrgpu_level *L, double *const *u, double dt, const nrgpu_z4_params *p,
+                                 void *stream) {
+  int e = nrgpu_z4_rk4_stages(L, u, dt, p, (cudaStream_t)stream);
+  if (e) return e;
+  return nrgpu_z4_algcon(L, u, p, (cudaStream_t)stream);
 }

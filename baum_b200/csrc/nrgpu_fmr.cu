@@ -1,0 +1,546 @@
+// nrgpu_fmr.cu -- fixed mesh refinement around the evolution (sm_100a), FP64:
+// the Berger-Oliger recursion of nested boxes with Lagrange restriction and
+// prolongation and time interpolation of the parent to the child's half step.
+//   flags            setRPflags (flag.c:122-255), host, once
+//   restrict_kernel  restrict_boxtobox_N (interpolate_boxtobox_N.c:1055-1223)
+//   prolong_kernel   prolong_boxtobox_N (interpolate_boxtobox_N.c:585-869)
+//   ti_start/finish  evolve.c:292-340, 371-380 (orders 2 and 3)
+//   nrgpu_fmr_advance advance_levelandsublevels (main.c:397-418) with
+//                    restrict_prolong_evolve (inject.c:116-132)
+// The reference does restriction and prolongation as three 1-D sweeps
+// through temporary arrays (z, then y, then x).  Here one thread computes one
+// output point of one variable as the same nested sums in the same order,
+// with explicit round-to-nearest multiplies and adds (no contraction into
+// FMA), so that restriction, prolongation and time interpolation give the
+// reference's values bit for bit from the same inputs; nothing is staged
+// through global temporaries.
+#include <string.h>
+#include <vector>
+#include "nrgpu_level.cuh"
+
+namespace {
+
+constexpr int kMaxLevels = 16;
+constexpr int kMaxVars = NRGPU_Z4_NVARS;
+constexpr int kMaxOrder = 8;
+
+struct Ptrs {
+  double *p[kMaxVars];
+};
+
+struct Box3 {
+  int n[3];
+  long off;
+};
+
+__device__ __forceinline__ long at3(const Box3 &b, int i, int j, int k) {
+  return b.off + i + (long)b.n[0] * (j + (long)b.n[1] * k);
+}
+
+struct RGeom {  // restriction of one child into its parent
+  int ic[6];    // coarse bounding box of flagrestrict >= 3
+  int if0[3];   // fine point of the first stencil of ic[0], ic[2], ic[4]
+  double w[kMaxOrder];
+};
+
+struct PGeom {  // prolongation of a parent into its child
+  int fb[6];    // fine bounding box of 1 <= flagprolong <= nbuffer
+  int f0[6];    // fine bounding box of the other points (skipped pairs)
+  int cs[3];    // coarse start of the first output pair per direction
+  double c1[kMaxOrder], c2[kMaxOrder];
+};
+
+template <int N>
+__device__ __forceinline__ double dot_rn(const double *w, const double *u) {
+  double s = 0.0;
+#pragma unroll
+  for (int p = 0; p < N; ++p) s = __dadd_rn(s, __dmul_rn(w[p], u[p]));
+  return s;
+}
+
+// one thread per (coarse output point, variable)
+template <int N>
+__global__ void restrict_kernel(Ptrs uc, Ptrs uf, Box3 cb, Box3 fb, RGeom G, int npts) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= npts) return;
+  const int v = blockIdx.y;
+  const int nI = G.ic[1] - G.ic[0] + 1, nJ = G.ic[3] - G.ic[2] + 1;
+  const int I = G.ic[0] + q % nI, J = G.ic[2] + (q / nI) % nJ, K = G.ic[4] + q / (nI * nJ);
+  const int fx = G.if0[0] + 2 * (I - G.ic[0]), fy = G.if0[1] + 2 * (J - G.ic[2]), fz = G.if0[2] + 2 * (K - G.ic[4]);
+  const double *f = uf.p[v];
+  double sx[N], sy[N], sz[N];
+#pragma unroll
+  for (int px = 0; px < N; ++px) {
+#pragma unroll
+    for (int py = 0; py < N; ++py) {
+#pragma unroll
+      for (int pz = 0; pz < N; ++pz) sz[pz] = __ldg(f + at3(fb, fx + px, fy + py, fz + pz));
+      sy[py] = dot_rn<N>(G.w, sz);
+    }
+    sx[px] = dot_rn<N>(G.w, sy);
+  }
+  uc.p[v][at3(cb, I, J, K)] = dot_rn<N>(G.w, sx);
+}
+
+// one thread per (fine point of the prolongation box, variable)
+template <int N>
+__global__ void prolong_kernel(Ptrs uc, Ptrs uf, Box3 cb, Box3 fb, PGeom G, int npts) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= npts) return;
+  const int v = blockIdx.y;
+  const int nI = G.fb[1] - G.fb[0] + 1, nJ = G.fb[3] - G.fb[2] + 1;
+  const int t[3] = {q % nI, (q / nI) % nJ, q / (nI * nJ)};
+  const int i = G.fb[0] + t[0], j = G.fb[2] + t[1], k = G.fb[4] + t[2];
+  // the reference tests the inner box on the first point of each x pair
+  const int i0 = G.fb[0] + 2 * (t[0] / 2);
+  if (i0 >= G.f0[0] && i0 <= G.f0[1] && j >= G.f0[2] && j <= G.f0[3] && k >= G.f0[4] && k <= G.f0[5]) return;
+  int s[3];
+  const double *w[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    s[d] = G.cs[d] + t[d] / 2 + (t[d] & 1);
+    w[d] = (t[d] & 1) ? G.c2 : G.c1;
+  }
+  const double *c = uc.p[v];
+  double sx[N], sy[N], sz[N];
+#pragma unroll
+  for (int px = 0; px < N; ++px) {
+#pragma unroll
+    for (int py = 0; py < N; ++py) {
+#pragma unroll
+      for (int pz = 0; pz < N; ++pz) sz[pz] = __ldg(c + at3(cb, s[0] + px, s[1] + py, s[2] + pz));
+      sy[py] = dot_rn<N>(w[2], sz);
+    }
+    sx[px] = dot_rn<N>(w[1], sy);
+  }
+  uf.p[v][at3(fb, i, j, k)] = dot_rn<N>(w[0], sx);
+}
+
+// vladd (variables.c:575-650) with its special cases, and the u_p copy of
+// the RK4 step: upp = ca u + cb up; up = u
+__global__ void ti_start_kernel(Ptrs u, double *up, double *upp, double ca, double cb, long np, int nv) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= np * nv) return;
+  const int v = (int)(t / np);
+  const long i = t - (long)v * np;
+  const double a = u.p[v][i];
+  const double b = up[t];
+  double r;
+  if (ca == 0.0 && cb == 0.0) r = 0.0;
+  else if (ca == 0.0) r = __dmul_rn(cb, b);
+  else if (cb == 0.0) r = __dmul_rn(ca, a);
+  else r = __dadd_rn(__dmul_rn(ca, a), __dmul_rn(cb, b));
+  upp[t] = r;
+  up[t] = a;
+}
+
+// upp = 1.0 upp + c u
+__global__ void ti_finish_kernel(Ptrs u, double *upp, double c, long np, int nv) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= np * nv) return;
+  const int v = (int)(t / np);
+  const long i = t - (long)v * np;
+  upp[t] = __dadd_rn(__dmul_rn(1.0, upp[t]), __dmul_rn(c, u.p[v][i]));
+}
+
+}  // namespace
+
+struct nrgpu_fmr {
+  int nl, nv;
+  nrgpu_fmr_params p;
+  nrgpu_level *L[kMaxLevels];
+  Box3 box[kMaxLevels];
+  double x0[kMaxLevels][3], dx[kMaxLevels][3];
+  double dt[kMaxLevels];
+  nrgpu_bssn_params bp[kMaxLevels];
+  nrgpu_z4_params zp[kMaxLevels];
+  std::vector<double> fp[kMaxLevels], fr[kMaxLevels];  // flagprolong, flagrestrict
+  bool has_r[kMaxLevels], has_p[kMaxLevels];           // per fine level
+  RGeom rg[kMaxLevels];
+  PGeom pg[kMaxLevels];
+  int nr[kMaxLevels], npro[kMaxLevels];
+  double *up[kMaxLevels], *upp[kMaxLevels];  // u(n-1) copy and time interpolant
+  int iteration[kMaxLevels];
+  // graph of one coarse step for one set of state pointers
+  cudaGraph_t graph;
+  cudaGraphExec_t exec;
+  std::vector<double *> graph_u;
+};
+
+namespace {
+
+// coefficients_lagrange_N (lagrange.c:13-27) on unit spacing from 0
+void lagrange(int n, double x, double *c) {
+  for (int i = 0; i < n; i++) {
+    double d = 1;
+    for (int j = 0; j < n; j++)
+      if (j != i) d *= (x - 0.0 - j * 1.0) / ((i - j) * 1.0);
+    c[i] = d;
+  }
+}
+
+// box.c:284-307
+int parent_index(double cx0, double cdx, double fx0, double fdx, int fi) {
+  return (int)(0.5 + (fx0 + fi * fdx - cx0) / cdx);
+}
+int point_index(double X0, double dX, double x0, double dx, int i) { return (int)((x0 + i * dx - X0) / dX); }
+
+long hat(const Box3 &b, int i, int j, int k) { return b.off + i + (long)b.n[0] * (j + (long)b.n[1] * k); }
+
+// setRPflags (flag.c:122-255) between level l-1 and l; then the bounding
+// boxes of restrict_varlist_boxtobox_N and prolong_varlist_boxtobox_N
+int setup_pair(nrgpu_fmr *F, int l) {
+  const Box3 &f = F->box[l], &c = F->box[l - 1];
+  const int nbuf = F->p.nbuffer, b = F->p.order_RP / 2;
+  const long npf = (long)f.n[0] * f.n[1] * f.n[2];
+  std::vector<double> &fp = F->fp[l], &cr = F->fr[l - 1];
+  fp.assign(npf, 0.0);
+  cr.assign((size_t)c.n[0] * c.n[1] * c.n[2], 0.0);
+  for (int k = 0; k < f.n[2]; k++)
+    for (int j = 0; j < f.n[1]; j++)
+      for (int i = 0; i < f.n[0]; i++) {
+        const int idx[3] = {i, j, k};
+        long m[3];
+        for (int d = 0; d < 3; d++) {
+          const double lo = F->x0[l][d], hi = F->x0[l][d] + (f.n[d] - 1) * F->dx[l][d];
+          const double x = F->x0[l][d] + idx[d] * F->dx[l][d];
+          m[d] = npf;
+          int n = (int)(1.5 + (x - lo) / F->dx[l][d]);
+          if (n <= nbuf) m[d] = n;
+          n = (int)(1.5 - (x - hi) / F->dx[l][d]);
+          if (n <= nbuf) m[d] = n;
+        }
+        long ii = m[0] < m[1] ? m[0] : m[1];
+        ii = ii < m[2] ? ii : m[2];
+        fp[hat(f, i, j, k) - f.off] = ii < npf ? (double)ii : 0.0;
+      }
+  for (int pass = 0; pass < 2; pass++)
+    for (int k = 0; k < f.n[2]; k++)
+      for (int j = 0; j < f.n[1]; j++)
+        for (int i = 0; i < f.n[0]; i++) {
+          const int pi = parent_index(F->x0[l - 1][0], F->dx[l - 1][0], F->x0[l][0], F->dx[l][0], i);
+          const int pj = parent_index(F->x0[l - 1][1], F->dx[l - 1][1], F->x0[l][1], F->dx[l][1], j);
+          const int pk = parent_index(F->x0[l - 1][2], F->dx[l - 1][2], F->x0[l][2], F->dx[l][2], k);
+          if (pi < 0 || pj < 0 || pk < 0 || pi >= c.n[0] || pj >= c.n[1] || pk >= c.n[2])
+            return nrgpu_set_error(NRGPU_ERR_ARG, "level %d does not nest in level %d", l, l - 1);
+          const double p = fp[hat(f, i, j, k) - f.off];
+          double &r = cr[hat(c, pi, pj, pk) - c.off];
+          if (pass == 0 && p == 0) r = 3;
+          if (pass == 1) {
+            if (p >= 3) r = 2;
+            else if (p == 2) r = 1;
+          }
+        }
+  // restriction box
+  int ic[6] = {1 << 30, -(1 << 30), 1 << 30, -(1 << 30), 1 << 30, -(1 << 30)};
+  long n = 0;
+  for (int k = 0; k < c.n[2]; k++)
+    for (int j = 0; j < c.n[1]; j++)
+      for (int i = 0; i < c.n[0]; i++)
+        if (cr[hat(c, i, j, k) - c.off] >= 3) {
+          const int idx[3] = {i, j, k};
+          for (int d = 0; d < 3; d++) {
+            ic[2 * d] = idx[d] < ic[2 * d] ? idx[d] : ic[2 * d];
+            ic[2 * d + 1] = idx[d] > ic[2 * d + 1] ? idx[d] : ic[2 * d + 1];
+          }
+          n++;
+        }
+  F->has_r[l] = n > 0;
+  if (n) {
+    RGeom &G = F->rg[l];
+    memcpy(G.ic, ic, sizeof ic);
+    for (int d = 0; d < 3; d++) {
+      const int lo = point_index(F->x0[l][d], F->dx[l][d], F->x0[l - 1][d], F->dx[l - 1][d], ic[2 * d]) - b + 1;
+      const int hi = point_index(F->x0[l][d], F->dx[l][d], F->x0[l - 1][d], F->dx[l - 1][d], ic[2 * d + 1]) + b;
+      if (lo < 0 || hi >= f.n[d])
+        return nrgpu_set_error(NRGPU_ERR_ARG, "restriction: boxes too small (level %d)", l);
+      G.if0[d] = lo;
+    }
+    lagrange(F->p.order_RP, F->p.order_RP / 2.0 - 0.5, G.w);
+    F->nr[l] = (ic[1] - ic[0] + 1) * (ic[3] - ic[2] + 1) * (ic[5] - ic[4] + 1);
+  }
+  // prolongation boxes
+  PGeom &P = F->pg[l];
+  int fb[6] = {1 << 30, -(1 << 30), 1 << 30, -(1 << 30), 1 << 30, -(1 << 30)};
+  int f0[6] = {1 << 30, -(1 << 30), 1 << 30, -(1 << 30), 1 << 30, -(1 << 30)};
+  n = 0;
+  for (int k = 0; k < f.n[2]; k++)
+    for (int j = 0; j < f.n[1]; j++)
+      for (int i = 0; i < f.n[0]; i++) {
+        const int idx[3] = {i, j, k};
+        const double p = fp[hat(f, i, j, k) - f.off];
+        int *bb = (p > 0 && nbuf >= p) ? fb : f0;
+        if (bb == fb) n++;
+        for (int d = 0; d < 3; d++) {
+          bb[2 * d] = idx[d] < bb[2 * d] ? idx[d] : bb[2 * d];
+          bb[2 * d + 1] = idx[d] > bb[2 * d + 1] ? idx[d] : bb[2 * d + 1];
+        }
+      }
+  F->has_p[l] = n > 0;
+  if (n) {
+    memcpy(P.fb, fb, sizeof fb);
+    memcpy(P.f0, f0, sizeof f0);
+    for (int d = 0; d < 3; d++) {
+      const int lo = point_index(F->x0[l - 1][d], F->dx[l - 1][d], F->x0[l][d], F->dx[l][d], fb[2 * d]) - b + 1;
+      const int hi = point_index(F->x0[l - 1][d], F->dx[l - 1][d], F->x0[l][d], F->dx[l][d], fb[2 * d + 1]) + b;
+      if (lo < 0 || hi >= c.n[d])
+        return nrgpu_set_error(NRGPU_ERR_ARG, "prolongation: boxes too small (level %d)", l);
+      if ((fb[2 * d + 1] - fb[2 * d] + 1) % 2)
+        return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "level %d is not made of whole parent cells", l);
+      // the output pairs start on a lower child (fine point a quarter coarse
+      // cell below its parent), as prolong_boxtobox_N assumes
+      if (point_index(F->x0[l - 1][d], F->dx[l - 1][d], F->x0[l][d], F->dx[l][d], fb[2 * d]) !=
+          parent_index(F->x0[l - 1][d], F->dx[l - 1][d], F->x0[l][d], F->dx[l][d], fb[2 * d]) - 1)
+        return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "level %d is not aligned with its parent's cells", l);
+      P.cs[d] = lo;
+    }
+    lagrange(F->p.order_RP, F->p.order_RP / 2.0 - 0.25, P.c1);
+    lagrange(F->p.order_RP, F->p.order_RP / 2.0 - 0.75, P.c2);
+    F->npro[l] = (fb[1] - fb[0] + 1) * (fb[3] - fb[2] + 1) * (fb[5] - fb[4] + 1);
+  }
+  return NRGPU_OK;
+}
+
+int fill(Ptrs *P, double *const *u, int nv) {
+  for (int v = 0; v < kMaxVars; ++v) P->p[v] = v < nv ? u[v] : nullptr;
+  for (int v = 0; v < nv; ++v)
+    if (!u[v]) return nrgpu_set_error(NRGPU_ERR_ARG, "null variable pointer %d", v);
+  return NRGPU_OK;
+}
+
+// restrict_prolong_varlist between level l and its parent (nbuffer 3)
+int restrict_prolong(nrgpu_fmr *F, int l, const Ptrs &uc, const Ptrs &uf, cudaStream_t st) {
+  const int o = F->p.order_RP;
+  if (F->has_r[l]) {
+    const dim3 g((F->nr[l] + 127) / 128, F->nv);
+    if (o == 2) restrict_kernel<2><<<g, 128, 0, st>>>(uc, uf, F->box[l - 1], F->box[l], F->rg[l], F->nr[l]);
+    else if (o == 4) restrict_kernel<4><<<g, 128, 0, st>>>(uc, uf, F->box[l - 1], F->box[l], F->rg[l], F->nr[l]);
+    else restrict_kernel<6><<<g, 128, 0, st>>>(uc, uf, F->box[l - 1], F->box[l], F->rg[l], F->nr[l]);
+    NRGPU_CUDA_TRY(cudaGetLastError());
+  }
+  if (F->has_p[l]) {
+    const dim3 g((F->npro[l] + 127) / 128, F->nv);
+    if (o == 2) prolong_kernel<2><<<g, 128, 0, st>>>(uc, uf, F->box[l - 1], F->box[l], F->pg[l], F->npro[l]);
+    else if (o == 4) prolong_kernel<4><<<g, 128, 0, st>>>(uc, uf, F->box[l - 1], F->box[l], F->pg[l], F->npro[l]);
+    else prolong_kernel<6><<<g, 128, 0, st>>>(uc, uf, F->box[l - 1], F->box[l], F->pg[l], F->npro[l]);
+    NRGPU_CUDA_TRY(cudaGetLastError());
+  }
+  return NRGPU_OK;
+}
+
+Ptrs upp_ptrs(nrgpu_fmr *F, int l) {
+  Ptrs P;
+  const long np = F->L[l]->npoints;
+  for (int v = 0; v < kMaxVars; ++v) P.p[v] = v < F->nv ? F->upp[l] + (long)v * np : nullptr;
+  return P;
+}
+
+// one step of level l: evolve() with the time interpolation of a level with
+// a child around the RK4 stages, then the algebraic constraints
+int step_level(nrgpu_fmr *F, int l, double *const *u, cudaStream_t st) {
+  const bool child = l < F->nl - 1;
+  const long np = F->L[l]->npoints;
+  Ptrs U;
+  int e = fill(&U, u, F->nv);
+  if (e) return e;
+  const unsigned nb = (unsigned)((np * F->nv + 255) / 256);
+  int o = 0;
+  if (child) {
+    o = F->iteration[l] + 2 > F->p.order_timeinterpolation ? F->p.order_timeinterpolation : F->iteration[l] + 2;
+    const double ca = o == 2 ? 0.5 : 0.75, cb = o == 2 ? 0.0 : -0.125;
+    ti_start_kernel<<<nb, 256, 0, st>>>(U, F->up[l], F->upp[l], ca, cb, np, F->nv);
+    NRGPU_CUDA_TRY(cudaGetLastError());
+  }
+  if (F->p.system == NRGPU_SYSTEM_BSSN) e = nrgpu_bssn_rk4_stages(F->L[l], u, F->dt[l], &F->bp[l], st);
+  else e = nrgpu_z4_rk4_stages(F->L[l], u, F->dt[l], &F->zp[l], st);
+  if (e) return e;
+  if (child) {
+    ti_finish_kernel<<<nb, 256, 0, st>>>(U, F->upp[l], o == 2 ? 1.0 / 2 : 3. / 8, np, F->nv);
+    NRGPU_CUDA_TRY(cudaGetLastError());
+  }
+  if (F->p.system == NRGPU_SYSTEM_BSSN) e = nrgpu_bssn_algcon(F->L[l], u, &F->bp[l], st);
+  else e = nrgpu_z4_algcon(F->L[l], u, &F->zp[l], st);
+  if (e) return e;
+  F->iteration[l]++;
+  return NRGPU_OK;
+}
+
+// advance_levelandsublevels (main.c:397-418)
+int advance(nrgpu_fmr *F, int l, double *const *u, cudaStream_t st) {
+  int e = step_level(F, l, u + l * F->nv, st);
+  if (e) return e;
+  if (l < F->nl - 1) {
+    if ((e = advance(F, l + 1, u, st))) return e;
+    if (l >= F->p.lbo && (e = advance(F, l + 1, u, st))) return e;
+  }
+  if (l > 0) {
+    // parentaligned (inject.c:10-21): dequal of the level times
+    const double tl = F->iteration[l] * F->dt[l], tp = F->iteration[l - 1] * F->dt[l - 1];
+    const bool aligned = !(tl < tp - 1e-10 || tp < tl - 1e-10);
+    Ptrs uc, uf;
+    if ((e = fill(&uf, u + l * F->nv, F->nv))) return e;
+    if (aligned) {
+      if ((e = fill(&uc, u + (l - 1) * F->nv, F->nv))) return e;
+    } else {
+      uc = upp_ptrs(F, l - 1);
+    }
+    if ((e = restrict_prolong(F, l, uc, uf, st))) return e;
+  }
+  return NRGPU_OK;
+}
+
+}  // namespace
+
+extern "C" int nrgpu_fmr_params_default(nrgpu_fmr_params *p) {
+  if (!p) return nrgpu_set_error(NRGPU_ERR_ARG, "null params");
+  p->system = NRGPU_SYSTEM_Z4C;
+  p->lbo = 0;
+  p->order_timeinterpolation = 3;
+  p->order_RP = 4;
+  p->nbuffer = 3;
+  p->use_graph = 1;
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_fmr_destroy(nrgpu_fmr *F) {
+  if (!F) return NRGPU_OK;
+  if (F->exec) cudaGraphExecDestroy(F->exec);
+  if (F->graph) cudaGraphDestroy(F->graph);
+  for (int l = 0; l < F->nl; ++l) {
+    cudaFree(F->up[l]);
+    cudaFree(F->upp[l]);
+    nrgpu_level_destroy(F->L[l]);
+  }
+  delete F;
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_fmr_create(int nl, const nrgpu_level_desc *levels, const double *dt, const void *sysparams,
+                                const nrgpu_fmr_params *p, nrgpu_fmr **out) {
+  if (!levels || !dt || !sysparams || !p || !out || nl < 1 || nl > kMaxLevels)
+    return nrgpu_set_error(NRGPU_ERR_ARG, "bad arguments (1 <= nlevels <= %d)", kMaxLevels);
+  if (p->system != NRGPU_SYSTEM_BSSN && p->system != NRGPU_SYSTEM_Z4C)
+    return nrgpu_set_error(NRGPU_ERR_ARG, "system %d", p->system);
+  if (p->order_timeinterpolation < 2 || p->order_timeinterpolation > 3)
+    return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "order_timeinterpolation %d (2 or 3)", p->order_timeinterpolation);
+  if (p->order_RP != 2 && p->order_RP != 4 && p->order_RP != 6)
+    return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "order_RP %d (2, 4 or 6)", p->order_RP);
+  if (p->nbuffer < 1 || p->lbo < 0) return nrgpu_set_error(NRGPU_ERR_ARG, "nbuffer %d, lbo %d", p->nbuffer, p->lbo);
+  nrgpu_fmr *F = new nrgpu_fmr();
+  memset(F->L, 0, sizeof F->L);
+  memset(F->up, 0, sizeof F->up);
+  memset(F->upp, 0, sizeof F->upp);
+  memset(F->iteration, 0, sizeof F->iteration);
+  F->graph = nullptr;
+  F->exec = nullptr;
+  F->nl = nl;
+  F->p = *p;
+  F->nv = p->system == NRGPU_SYSTEM_BSSN ? NRGPU_NV : NRGPU_Z4_NVARS;
+  int e = NRGPU_OK;
+  for (int l = 0; l < nl && !e; ++l) {
+    const nrgpu_level_desc &d = levels[l];
+    if (d.nboxes != 1) e = nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "level %d: one box per level", l);
+    else if (dt[l] <= 0) e = nrgpu_set_error(NRGPU_ERR_ARG, "level %d: dt %g", l, dt[l]);
+    if (e) break;
+    F->box[l] = Box3{{d.box[0].m, d.box[0].n, d.box[0].o}, 0};
+    F->x0[l][0] = d.box[0].x0; F->x0[l][1] = d.box[0].y0; F->x0[l][2] = d.box[0].z0;
+    F->dx[l][0] = d.dx; F->dx[l][1] = d.dy; F->dx[l][2] = d.dz;
+    F->dt[l] = dt[l];
+    if (p->system == NRGPU_SYSTEM_BSSN) F->bp[l] = ((const nrgpu_bssn_params *)sysparams)[l];
+    else F->zp[l] = ((const nrgpu_z4_params *)sysparams)[l];
+    if ((e = nrgpu_level_create(&d, &F->L[l]))) break;
+    double *scr;
+    if ((e = nrgpu_level_scratch(F->L[l], &scr))) break;  // no allocation later, inside a graph capture
+    if (l > 0 && (e = setup_pair(F, l))) break;
+    if (l < nl - 1) {
+      const size_t bytes = sizeof(double) * F->nv * (size_t)d.npoints;
+      if (cudaMalloc(&F->up[l], bytes) != cudaSuccess || cudaMalloc(&F->upp[l], bytes) != cudaSuccess) {
+        cudaGetLastError();
+        e = nrgpu_set_error(NRGPU_ERR_NOMEM, "time interpolation buffers of level %d", l);
+      } else if (cudaMemset(F->up[l], 0, bytes) != cudaSuccess || cudaMemset(F->upp[l], 0, bytes) != cudaSuccess) {
+        e = nrgpu_set_error(NRGPU_ERR_CUDA, "memset");
+      }
+    }
+  }
+  if (e) {
+    nrgpu_fmr_destroy(F);
+    return e;
+  }
+  *out = F;
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_fmr_flags(nrgpu_fmr *F, int l, double *flagprolong, double *flagrestrict) {
+  if (!F || l < 0 || l >= F->nl) return nrgpu_set_error(NRGPU_ERR_ARG, "bad level");
+  const size_t np = (size_t)F->L[l]->npoints;
+  if (flagprolong) {
+    if (l == 0) memset(flagprolong, 0, sizeof(double) * np);
+    else memcpy(flagprolong, F->fp[l].data(), sizeof(double) * np);
+  }
+  if (flagrestrict) {
+    if (l == F->nl - 1) memset(flagrestrict, 0, sizeof(double) * np);
+    else memcpy(flagrestrict, F->fr[l].data(), sizeof(double) * np);
+  }
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_fmr_restrict_prolong(nrgpu_fmr *F, int lfine, double *const *uc, double *const *uf,
+                                          void *stream) {
+  if (!F || !uc || !uf || lfine < 1 || lfine >= F->nl) return nrgpu_set_error(NRGPU_ERR_ARG, "bad arguments");
+  Ptrs C, P;
+  int e;
+  if ((e = fill(&C, uc, F->nv)) || (e = fill(&P, uf, F->nv))) return e;
+  return restrict_prolong(F, lfine, C, P, (cudaStream_t)stream);
+}
+
+extern "C" int nrgpu_fmr_iteration(nrgpu_fmr *F, int l) {
+  if (!F || l < 0 || l >= F->nl) return -1;
+  return F->iteration[l];
+}
+
+extern "C" int nrgpu_fmr_advance(nrgpu_fmr *F, double *const *u, int nsteps, void *stream) {
+  if (!F || !u || nsteps < 0) return nrgpu_set_error(NRGPU_ERR_ARG, "bad arguments");
+  const cudaStream_t st = (cudaStream_t)stream;
+  const int ntot = F->nl * F->nv;
+  for (int s = 0; s < nsteps; ++s) {
+    // the launch sequence of a coarse step is the same for every step once
+    // no level is in its first iteration (time interpolation order) and
+    // the state pointers are the same
+    bool steady = true;
+    for (int l = 0; l < F->nl; ++l) steady = steady && F->iteration[l] >= 1;
+    if (!F->p.use_graph || !steady) {
+      int e = advance(F, 0, u, st);
+      if (e) return e;
+      continue;
+    }
+    if (!F->exec || F->graph_u.size() != (size_t)ntot || memcmp(F->graph_u.data(), u, sizeof(double *) * ntot)) {
+      if (F->exec) cudaGraphExecDestroy(F->exec);
+      if (F->graph) cudaGraphDestroy(F->graph);
+      F->exec = nullptr;
+      F->graph = nullptr;
+      int it[kMaxLevels];
+      memcpy(it, F->iteration, sizeof it);
+      NRGPU_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      int e = advance(F, 0, u, st);
+      cudaGraph_t g = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(st, &g);
+      memcpy(F->iteration, it, sizeof it);  // the capture ran nothing
+      if (e) {
+        if (g) cudaGraphDestroy(g);
+        return e;
+      }
+      if (ce != cudaSuccess) return nrgpu_set_error(NRGPU_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+      F->graph = g;
+      NRGPU_CUDA_TRY(cudaGraphInstantiate(&F->exec, g, 0));
+      F->graph_u.assign(u, u + ntot);
+    }
+    NRGPU_CUDA_TRY(cudaGraphLaunch(F->exec, st));
+    // the iteration counters advance as the recursion would have
+    for (int l = 0; l < F->nl; ++l) {
+      int times = 1;
+      for (int q = 1; q <= l; ++q) times *= (q - 1 >= F->p.lbo) ? 2 : 1;
+      F->iteration[l] += times;
+    }
+  }
+  return NRGPU_OK;
+}

@@ -29,3 +29,12 @@ struct nrgpu_level {
   long ninner;
   double *d_red;
 };
+
+// library-internal pieces shared by the entry points and the mesh-refinement
+// driver (nrgpu_bssn.cu)
+int nrgpu_bssn_rk4_stages(nrgpu_level *L, double *const *u, double dt, const nrgpu_bssn_params *p,
+                          cudaStream_t st);
+int nrgpu_z4_rk4_stages(nrgpu_level *L, double *const *u, double dt, const nrgpu_z4_params *p, cudaStream_t st);
+int nrgpu_z4_algcon(nrgpu_level *L, double *const *u, const nrgpu_z4_params *p, cudaStream_t st);
+// the level's three RK4 scratch lists, allocated on first use (nrgpu_lib.cu)
+int nrgpu_level_scratch(nrgpu_level *L, double **out);

@@ -1,0 +1,99 @@
+"""Host-side mirror of the reference's mesh refinement around the evolution.
+
+``Hierarchy`` holds the nested boxes of a grid (one box per level, each made
+of whole cells of its parent: the single-rank grid of amr = bo newfmr,
+amr_fmr = nestedboxes) on the device and advances them by coarse steps:
+advance_levelandsublevels (main.c:397-418) with the time interpolation of
+evolve (evolve.c:292-340, 371-380) and restrict_prolong_evolve
+(inject.c:116-132).  ``restrict_prolong_varlist`` is inject.c:63-100 with
+nbuffer 3.  All arithmetic runs in libnrgpu.so (nrgpu_fmr_*).
+"""
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import abi
+from .bssn import _ptrs, _stream
+
+
+class Hierarchy:
+    def __init__(self, levels, dt, sysparams, params=None):
+        """levels: abi.Level per level, coarsest first; dt: per-level time
+        steps; sysparams: per-level abi.BssnParams or abi.Z4Params."""
+        self.levels = levels
+        self.params = params or abi.fmr_params(
+            system=abi.SYSTEM_BSSN if isinstance(sysparams[0], abi.BssnParams) else abi.SYSTEM_Z4C)
+        self.nv = abi.NVARS if self.params.system == abi.SYSTEM_BSSN else abi.Z4_NVARS
+        nl = len(levels)
+        self._descs = (abi.LevelDesc * nl)(*[lv.desc for lv in levels])
+        self._dt = (C.c_double * nl)(*dt)
+        self._sp = (type(sysparams[0]) * nl)(*sysparams)
+        h = C.c_void_p()
+        abi.check(abi.lib().nrgpu_fmr_create(nl, self._descs, self._dt, C.cast(self._sp, C.c_void_p),
+                                             C.byref(self.params), C.byref(h)))
+        self.handle = h
+        self._uptrs = None
+
+    def empty(self):
+        """One zero (nvars, npoints) float64 CUDA tensor per level."""
+        return [torch.zeros((self.nv, lv.npoints), dtype=torch.float64, device="cuda") for lv in self.levels]
+
+    def flags(self, l):
+        """(flagprolong, flagrestrict) of level l as numpy arrays."""
+        n = self.levels[l].npoints
+        fp, fr = np.zeros(n), np.zeros(n)
+        dp = lambda x: x.ctypes.data_as(C.POINTER(C.c_double))
+        abi.check(abi.lib().nrgpu_fmr_flags(self.handle, l, dp(fp), dp(fr)))
+        return fp, fr
+
+    def restrict_prolong_varlist(self, lfine, uc, uf, stream=None):
+        abi.check(abi.lib().nrgpu_fmr_restrict_prolong(self.handle, lfine, _ptrs(uc, self.nv), _ptrs(uf, self.nv),
+                                                       _stream(stream)))
+
+    def advance(self, u, nsteps=1, stream=None):
+        """nsteps coarse steps of the per-level states u (list of tensors)."""
+        ptrs = [t.data_ptr() + v * t.stride(0) * 8 for t in u for v in range(self.nv)]
+        for t in u:
+            if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous() and t.shape[0] == self.nv):
+                raise ValueError("each level state is a contiguous float64 CUDA tensor (nvars, npoints)")
+        self._uptrs = abi.ptr_array(ptrs)
+        abi.check(abi.lib().nrgpu_fmr_advance(self.handle, self._uptrs, int(nsteps), _stream(stream)))
+        return u
+
+    def iteration(self, l):
+        return abi.lib().nrgpu_fmr_iteration(self.handle, l)
+
+    def close(self):
+        if self.handle:
+            abi.lib().nrgpu_fmr_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def nested_levels(sizes, dx0):
+    """Boxes of a nested grid centred on the origin: sizes[l] points per
+    direction on level l (level 0 with its physical boundary layer, 4n+2,
+    grid.c:84-99; finer levels multiples of 4, so that each is made of whole
+    parent cells), spacing dx0 / 2^l.  Flags as the reference sets them:
+    PHYBOUND on the outer layer of level 0, REFBOUND on the outer layer of
+    finer levels (box.c:543-552)."""
+    out = []
+    for l, m in enumerate(sizes):
+        if l == 0 and m % 4 != 2:
+            raise ValueError("level 0 has 4n+2 points per direction")
+        if l > 0 and (m % 4 or m // 2 + 6 > sizes[l - 1]):
+            raise ValueError("level %d: a multiple of 4 that nests in level %d with room for the stencils" % (l, l - 1))
+        dx = dx0 / 2 ** l
+        x0 = -0.5 * (m - 1) * dx
+        i = np.arange(m)
+        edge = (i == 0) | (i == m - 1)
+        e3 = edge[None, None, :] | edge[None, :, None] | edge[:, None, None]
+        flags = np.where(e3, 1 if l == 0 else -1, 0).astype(np.int32).ravel()
+        out.append(abi.Level([(m, m, m, x0, x0, x0)], dx, flags))
+    return out

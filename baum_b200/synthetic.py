@@ -55,3 +55,23 @@ def fourier_state(x, y, z, nvars, unit_rows, nmodes=8, amp=1e-3, length=16.0, se
             s += c[m] * np.sin(k[m, 0] * x + k[m, 1] * y + k[m, 2] * z + ph[m])
         u[v] = (1.0 if v in unit_rows else 0.0) + amp * s
     return u
+
+
+def fourier_state_device(x, y, z, nvars, unit_rows, nmodes=8, amp=1e-3, length=16.0, seed=1):
+    """The same state built on the device from CUDA coordinate tensors (the
+    same draws; the sums run in torch, so the last bits may differ from
+    fourier_state)."""
+    import torch
+    g = SplitMix64(seed)
+    k = [[0.0] * 3 for _ in range(nmodes)]
+    for m in range(nmodes):
+        for i in range(3):
+            k[m][i] = 2.0 * np.pi * (int(g.next() % 5) - 2) / length
+    u = torch.empty((nvars, x.numel()), dtype=torch.float64, device=x.device)
+    for v in range(nvars):
+        cp = [(2.0 * g.uniform01() - 1.0, 2.0 * np.pi * g.uniform01()) for _ in range(nmodes)]
+        s = torch.zeros_like(x)
+        for m, (c, ph) in enumerate(cp):
+            s += c * torch.sin(k[m][0] * x + k[m][1] * y + k[m][2] * z + ph)
+        u[v] = (1.0 if v in unit_rows else 0.0) + amp * s
+    return u

@@ -239,6 +239,55 @@ def gpu_mg(m, dx, binaries):
     return out
 
 
+# the batched FMR workload: 7 nested 2:1 levels of uneven size, Z4c 4th
+# order + KO6, Berger-Oliger subcycling on every level, order_RP 4,
+# amr_nbuffer 3, 3rd-order time interpolation, Fourier data of amplitude
+# 1e-3 (8 modes) on a flat background.  Level 0: 160^3 inner points and the
+# physical boundary layer; finer levels: interiors 128, 160, 96, 128, 64, 96
+# plus 4 points per side (3 prolonged buffer points and the refinement
+# boundary).
+FMR_SIZES = [162, 136, 168, 104, 136, 72, 104]
+FMR_DX0 = 0.5
+
+
+def gpu_fmr(steps=2):
+    import torch
+    from baum_b200 import abi, fmr, synthetic
+    levels = fmr.nested_levels(FMR_SIZES, FMR_DX0)
+    params = [abi.z4_params_from_par(dissfactor=(0.1 if l == 0 else 0.02) / 64) for l in range(len(levels))]
+    dt = [0.25 * FMR_DX0 / 2 ** l for l in range(len(levels))]
+    def state(lev):
+        x, y, z = (torch.from_numpy(c).cuda() for c in lev.coords())
+        return synthetic.fourier_state_device(x, y, z, abi.Z4_NVARS, synthetic.Z4_UNIT, 8, 1e-3, 16.0, 1)
+    inner = [int((lev.boundary == 0).sum()) for lev in levels]
+    upd_per_coarse = sum(n * 4 * 2 ** l for l, n in enumerate(inner))
+    out = {"workload": "7 nested 2:1 levels, Z4c 4th order + KO6, Berger-Oliger, order_RP 4, nbuffer 3, "
+                       "box points per side %s, dx0 %.3g, Fourier data 1e-3" % (FMR_SIZES, FMR_DX0),
+           "rhs_point_updates_per_coarse_step": upd_per_coarse}
+    for use_graph in (1, 0):
+        H = fmr.Hierarchy(levels, dt, params, abi.fmr_params(use_graph=use_graph))
+        u = [state(lev) for lev in levels]
+        H.advance(u, 1)   # first coarse step: 2nd-order time interpolation, no graph
+        H.advance(u, 1)   # graph capture (with use_graph)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        H.advance(u, steps)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / steps
+        key = "graph" if use_graph else "launches"
+        out[key] = {"ms_per_coarse_step": ms, "value": upd_per_coarse / (ms * 1e-3)}
+        finite = all(bool(torch.isfinite(t).all()) for t in u)
+        out[key]["finite"] = finite
+        H.close()
+        del u
+        torch.cuda.empty_cache()
+    out["value"] = out["graph"]["value"]
+    out["unit"] = UNIT
+    return out
+
+
 def oracle_port_cpu():
     """Fallback CPU baseline: the oracle restatement, one RK4 step."""
     from oracle import oracle
@@ -367,6 +416,7 @@ def run_ours(args, rank, world):
     mg130 = gpu_mg(130, 0.125, bins)
     mg66 = gpu_mg(66, 0.25, bins[:1])
     ref66 = reference_mg(bins[0], 64, 0.25) if not args.no_cpu else None
+    fmr_line = gpu_fmr(2)
     multigrid = {
         "workload": "binary punctures, Bowen-York, 130^3 points (129^3 cells), dx=0.125, tol 1e-10 RMS, full-V",
         "vcycles": [r["vcycles"] for r in mg130], "ms": [round(r["ms"], 2) for r in mg130],
@@ -393,6 +443,7 @@ def run_ours(args, rank, world):
         "gpu_launches": 10 * args.steps,
         "clocks": clocks,
         "multigrid": multigrid,
+        "fmr": fmr_line,
     }
     print(json.dumps(line))
 

@@ -259,6 +259,50 @@ int nrgpu_puncture_coefficients(int m, double dx, int npunc, const double *mass,
                                 const double *pos, const double *mom, const double *spin,
                                 double *a, double *b, void *stream);
 
+/* ---- fixed mesh refinement -----------------------------------------------
+ * Nested boxes, one box per level, each level's box made of whole cells of
+ * its parent (the single-rank grid of amr = bo newfmr, amr_fmr =
+ * nestedboxes).  The library derives the refinement flags (setRPflags,
+ * main/amr/flag.c:122-255) from the boxes, and advances the whole hierarchy
+ * by coarse steps: advance_levelandsublevels (main/main/main.c:397-418) with
+ * the time interpolation of evolve (utility/evolve/evolve.c:292-340,
+ * 371-380) and restrict_prolong_evolve (main/amr/inject.c:116-132) through
+ * restrict_boxtobox_N / prolong_boxtobox_N
+ * (utility/interpolate/interpolate_boxtobox_N.c:585-1223). */
+enum { NRGPU_SYSTEM_BSSN = 0, NRGPU_SYSTEM_Z4C = 1 };
+
+typedef struct {
+  int system;                   /* NRGPU_SYSTEM_BSSN or NRGPU_SYSTEM_Z4C */
+  int lbo;                      /* levels l >= lbo subcycle (regrid.c:51-78) */
+  int order_timeinterpolation;  /* 2 or 3 (bam_main.c:62, default 3) */
+  int order_RP;                 /* 2, 4 or 6 (bam_main.c:58, default 4) */
+  int nbuffer;                  /* amr_nbuffer (bam_amr.c) */
+  int use_graph;                /* capture the coarse steps after the first
+                                   in a CUDA graph and replay it */
+} nrgpu_fmr_params;
+
+typedef struct nrgpu_fmr nrgpu_fmr;
+
+/* levels[0] is the coarsest; dt[l] the level's time step (tL.dt);
+ * sysparams: nlevels nrgpu_bssn_params or nrgpu_z4_params, one per level
+ * (the dissipation factor differs between levels, evolve.c:486-530). */
+int nrgpu_fmr_params_default(nrgpu_fmr_params *p);
+int nrgpu_fmr_create(int nlevels, const nrgpu_level_desc *levels, const double *dt, const void *sysparams,
+                     const nrgpu_fmr_params *p, nrgpu_fmr **out);
+int nrgpu_fmr_destroy(nrgpu_fmr *fmr);
+/* the refinement flags of level l (host arrays of the level's npoints, NULL
+ * to skip): flagprolong (levels with a parent), flagrestrict (with a child) */
+int nrgpu_fmr_flags(nrgpu_fmr *fmr, int l, double *flagprolong, double *flagrestrict);
+/* restrict_prolong_varlist (inject.c:63-100) with nbuffer 3 between level
+ * lfine and its parent: restrict lfine's uf into uc, then prolong uc into
+ * lfine's buffer zone (nvars device pointers each) */
+int nrgpu_fmr_restrict_prolong(nrgpu_fmr *fmr, int lfine, double *const *uc, double *const *uf, void *stream);
+/* nsteps coarse steps of the hierarchy; u holds nlevels * nvars device
+ * pointers, level-major.  The caller keeps the same u for a run. */
+int nrgpu_fmr_advance(nrgpu_fmr *fmr, double *const *u, int nsteps, void *stream);
+/* level iterations done so far (tL.iteration) */
+int nrgpu_fmr_iteration(nrgpu_fmr *fmr, int l);
+
 /* ---- ADM diagnostics ------------------------------------------------------
  * ADM metric and extrinsic curvature from the conformal variables:
  * bssn_to_adm_vl (projects/bssn/bssn.c:132-197) and z4_to_adm_vl

@@ -1,0 +1,100 @@
+"""The mesh-refinement driver on the GPU (nrgpu_fmr_*) against the reference
+(refinement flags of its 3-level run) and the CPU oracle (restriction and
+prolongation bit for bit; the Berger-Oliger evolution of all levels within
+the oracle's own tolerance to the reference), and the graph replay of the
+coarse steps against plain launches."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_golden
+from test_fmr_oracle_pin import FMR_TOL, fmr_case
+from baum_b200 import abi, fmr, synthetic
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def to_dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def test_geometry_builder_matches_reference():
+    g, levels, _, _, _ = fmr_case()
+    built = fmr.nested_levels([18, 24, 24], 0.5)
+    for a, b in zip(built, levels):
+        assert np.array_equal(a.boundary, b.boundary)
+        assert (a.boxes[0].m, a.boxes[0].x0, a.desc.dx) == (b.boxes[0].m, b.boxes[0].x0, b.desc.dx)
+
+
+def test_flags_match_reference(gpu):
+    g, levels, u0, params, dt = fmr_case()
+    H = fmr.Hierarchy(levels, dt, params)
+    for l in range(3):
+        fp, fr = H.flags(l)
+        assert np.array_equal(fp, g["flagprolong_l%d" % l])
+        assert np.array_equal(fr, g["flagrestrict_l%d" % l])
+
+
+@pytest.mark.parametrize("order", [2, 4, 6])
+def test_restrict_prolong_is_bit_exact(gpu, order):
+    levels = fmr.nested_levels([26, 32, 32], 0.5)
+    params = [abi.z4_params()] * 3
+    H = fmr.Hierarchy(levels, [0.1, 0.05, 0.025], params, abi.fmr_params(order_RP=order))
+    rng = np.random.default_rng(order)
+    for l in (1, 2):
+        uc = rng.standard_normal((abi.Z4_NVARS, levels[l - 1].npoints))
+        uf = rng.standard_normal((abi.Z4_NVARS, levels[l].npoints))
+        dc, df = to_dev(uc), to_dev(uf)
+        H.restrict_prolong_varlist(l, dc, df)
+        oracle.fmr_restrict_prolong(levels[l - 1], levels[l], uc, uf, order, 3)
+        assert np.array_equal(dc.cpu().numpy(), uc)
+        assert np.array_equal(df.cpu().numpy(), uf)
+
+
+def test_three_level_evolution_matches_oracle(gpu):
+    g, levels, u0, params, dt = fmr_case()
+    H = fmr.Hierarchy(levels, dt, params, abi.fmr_params(use_graph=0))
+    u = [to_dev(x) for x in u0]
+    H.advance(u, 2)
+    assert [H.iteration(l) for l in range(3)] == [2, 4, 8]
+    st = oracle.FmrState(levels, u0, 1, params, dt)
+    st.advance(2)
+    for l in range(3):
+        a, b = u[l].cpu().numpy(), st.u[l]
+        err = np.abs(a - b).max(axis=1) / np.maximum(np.abs(b).max(axis=1), 1e-8)
+        assert err.max() < FMR_TOL, (l, err.max())
+
+
+def test_graph_replay_is_identical_to_launches(gpu):
+    g, levels, u0, params, dt = fmr_case()
+    runs = []
+    for use_graph in (0, 1):
+        H = fmr.Hierarchy(levels, dt, params, abi.fmr_params(use_graph=use_graph))
+        u = [to_dev(x) for x in u0]
+        H.advance(u, 1)
+        H.advance(u, 3)
+        torch.cuda.synchronize()
+        runs.append([x.cpu().numpy() for x in u])
+        assert [H.iteration(l) for l in range(3)] == [4, 8, 16]
+    for a, b in zip(*runs):
+        assert np.array_equal(a, b)
+
+
+def test_bssn_hierarchy_matches_oracle(gpu):
+    levels = fmr.nested_levels([22, 28, 24], 0.5)
+    params = [abi.bssn_params(dissfactor=(0.1 if l == 0 else 0.02) / 64) for l in range(3)]
+    dt = [0.125 / 2 ** l for l in range(3)]
+    u0 = []
+    for lev in levels:
+        x, y, z = lev.coords()
+        u0.append(synthetic.fourier_state(x, y, z, abi.NVARS, synthetic.BSSN_UNIT, 8, 0.05, 16.0, 3))
+    H = fmr.Hierarchy(levels, dt, params)
+    u = [to_dev(x) for x in u0]
+    H.advance(u, 2)
+    st = oracle.FmrState(levels, u0, 0, params, dt)
+    st.advance(2)
+    for l in range(3):
+        a, b = u[l].cpu().numpy(), st.u[l]
+        err = np.abs(a - b).max(axis=1) / np.maximum(np.abs(b).max(axis=1), 1e-8)
+        assert err.max() < FMR_TOL, (l, err.max())
