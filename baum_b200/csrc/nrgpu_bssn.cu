@@ -89,6 +89,27 @@ __device__ __forceinline__ double ko_sum(const double *__restrict__ f, int x, co
   return OD == 4 ? -acc : acc;
 }
 
+// Kreiss-Oliger with FP32 sums of centre-relative taps (the weights sum to
+// zero); P = 0 keeps FP64
+template <int OD, int P>
+__device__ __forceinline__ double ko_p(const double *__restrict__ f, int x, const int st[3], const double ooh[3]) {
+  if (P == 0) return ko_sum<OD>(f, x, st, ooh);
+  const double c = ldg(f + x);
+  double acc = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int s = st[d];
+    float t;
+    if (OD == 4)
+      t = -4.0f * (tapf(f, x, -1, s, c) + tapf(f, x, 1, s, c)) + (tapf(f, x, -2, s, c) + tapf(f, x, 2, s, c));
+    else
+      t = (tapf(f, x, -3, s, c) + tapf(f, x, 3, s, c)) - 6.0f * (tapf(f, x, -2, s, c) + tapf(f, x, 2, s, c)) +
+          15.0f * (tapf(f, x, -1, s, c) + tapf(f, x, 1, s, c));
+    acc += ooh[d] * (double)t;
+  }
+  return OD == 4 ? -acc : acc;
+}
+
 struct PointCtx {
   int ijk, i, j, k, imax, jmax, kmax, dist;
   int st[3];
@@ -999,6 +1020,7 @@ static int z4_check_params(const nrgpu_z4_params *p) {
   if (p->order_dissipation != 0 && p->order_dissipation != 4 && p->order_dissipation != 6)
     return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "order_dissipation %d not in {0,4,6}", p->order_dissipation);
   if (p->useNPTs) return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "z4_useNPTs = yes is not supported");
+  if (p->precision < 0 || p->precision > 2) return nrgpu_set_error(NRGPU_ERR_ARG, "precision %d", p->precision);
   if (p->advection_lopsided < 0 || p->advection_lopsided > 2 || p->advection_lopsided6 < 0 ||
       p->advection_lopsided6 > 3)
     return nrgpu_set_error(NRGPU_ERR_ARG, "advection lopsidedness out of range");
@@ -1028,7 +1050,21 @@ static int z4_launch(nrgpu_level *L, const ZCVarPtrs &U, const ZVarPtrs &out, co
       if (bx.m < 3 || bx.n < 3 || bx.o < 3) continue;
       dim3 blk(32, 4, 1);
       dim3 grd((bx.m - 2 + 31) / 32, (bx.n - 2 + 3) / 4, bx.o - 2);
-      if (bx.m == 162 && bx.n == 162)
+      if (p.precision == 1) {
+        if (bx.m == 162 && bx.n == 162)
+          z4_rhs_kernel<162, 162 * 162, 1><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx,
+                                                                 L->dy, L->dz, L->d_status);
+        else
+          z4_rhs_kernel<0, 0, 1><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
+                                                       L->d_status);
+      } else if (p.precision == 2) {
+        if (bx.m == 162 && bx.n == 162)
+          z4_rhs_kernel<162, 162 * 162, 2><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx,
+                                                                 L->dy, L->dz, L->d_status);
+        else
+          z4_rhs_kernel<0, 0, 2><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
+                                                       L->d_status);
+      } else if (bx.m == 162 && bx.n == 162)
         z4_rhs_kernel<162, 162 * 162><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy,
                                                             L->dz, L->d_status);
       else if (bx.m == 66 && bx.n == 66)

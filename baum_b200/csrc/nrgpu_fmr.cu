@@ -165,6 +165,10 @@ struct nrgpu_fmr {
   cudaGraph_t graph;
   cudaGraphExec_t exec;
   std::vector<double *> graph_u;
+  // the graph is captured and replayed on the driver's own stream, ordered
+  // after the caller's stream and before the caller's next work by events
+  cudaStream_t gst;
+  cudaEvent_t ev_in, ev_out;
 };
 
 namespace {
@@ -406,6 +410,9 @@ extern "C" int nrgpu_fmr_destroy(nrgpu_fmr *F) {
   if (!F) return NRGPU_OK;
   if (F->exec) cudaGraphExecDestroy(F->exec);
   if (F->graph) cudaGraphDestroy(F->graph);
+  if (F->gst) cudaStreamDestroy(F->gst);
+  if (F->ev_in) cudaEventDestroy(F->ev_in);
+  if (F->ev_out) cudaEventDestroy(F->ev_out);
   for (int l = 0; l < F->nl; ++l) {
     cudaFree(F->up[l]);
     cudaFree(F->upp[l]);
@@ -433,6 +440,8 @@ extern "C" int nrgpu_fmr_create(int nl, const nrgpu_level_desc *levels, const do
   memset(F->iteration, 0, sizeof F->iteration);
   F->graph = nullptr;
   F->exec = nullptr;
+  F->gst = nullptr;
+  F->ev_in = F->ev_out = nullptr;
   F->nl = nl;
   F->p = *p;
   F->nv = p->system == NRGPU_SYSTEM_BSSN ? NRGPU_NV : NRGPU_Z4_NVARS;
@@ -462,6 +471,10 @@ extern "C" int nrgpu_fmr_create(int nl, const nrgpu_level_desc *levels, const do
       }
     }
   }
+  if (!e && (cudaStreamCreateWithFlags(&F->gst, cudaStreamNonBlocking) != cudaSuccess ||
+             cudaEventCreateWithFlags(&F->ev_in, cudaEventDisableTiming) != cudaSuccess ||
+             cudaEventCreateWithFlags(&F->ev_out, cudaEventDisableTiming) != cudaSuccess))
+    e = nrgpu_set_error(NRGPU_ERR_CUDA, "stream/event creation");
   if (e) {
     nrgpu_fmr_destroy(F);
     return e;
@@ -520,10 +533,10 @@ extern "C" int nrgpu_fmr_advance(nrgpu_fmr *F, double *const *u, int nsteps, voi
       F->graph = nullptr;
       int it[kMaxLevels];
       memcpy(it, F->iteration, sizeof it);
-      NRGPU_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      int e = advance(F, 0, u, st);
+      NRGPU_CUDA_TRY(cudaStreamBeginCapture(F->gst, cudaStreamCaptureModeThreadLocal));
+      int e = advance(F, 0, u, F->gst);
       cudaGraph_t g = nullptr;
-      const cudaError_t ce = cudaStreamEndCapture(st, &g);
+      const cudaError_t ce = cudaStreamEndCapture(F->gst, &g);
       memcpy(F->iteration, it, sizeof it);  // the capture ran nothing
       if (e) {
         if (g) cudaGraphDestroy(g);
@@ -534,7 +547,11 @@ extern "C" int nrgpu_fmr_advance(nrgpu_fmr *F, double *const *u, int nsteps, voi
       NRGPU_CUDA_TRY(cudaGraphInstantiate(&F->exec, g, 0));
       F->graph_u.assign(u, u + ntot);
     }
-    NRGPU_CUDA_TRY(cudaGraphLaunch(F->exec, st));
+    NRGPU_CUDA_TRY(cudaEventRecord(F->ev_in, st));
+    NRGPU_CUDA_TRY(cudaStreamWaitEvent(F->gst, F->ev_in, 0));
+    NRGPU_CUDA_TRY(cudaGraphLaunch(F->exec, F->gst));
+    NRGPU_CUDA_TRY(cudaEventRecord(F->ev_out, F->gst));
+    NRGPU_CUDA_TRY(cudaStreamWaitEvent(st, F->ev_out, 0));
     // the iteration counters advance as the recursion would have
     for (int l = 0; l < F->nl; ++l) {
       int times = 1;

@@ -21,7 +21,7 @@ struct ZCVarPtrs {
   const double *p[ZNV];
 };
 
-template <int ORD, int CSY = 0, int CSZ = 0>
+template <int ORD, int CSY = 0, int CSZ = 0, int PREC = 0>
 __device__ __forceinline__ void z4_point(const ZCVarPtrs &U, const PointCtx &P, const nrgpu_z4_params &p,
                                          double r[ZNV]) {
   const int x = P.ijk;
@@ -58,7 +58,7 @@ __device__ __forceinline__ void z4_point(const ZCVarPtrs &U, const PointCtx &P, 
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
-      for (int a = 0; a < 6; ++a) dg[c][a] = o1[c] * d1n<ORD>(U.p[ZG11 + a], x, ZSTR(c));
+      for (int a = 0; a < 6; ++a) dg[c][a] = o1[c] * d1p<ORD, PREC>(U.p[ZG11 + a], x, ZSTR(c));
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -104,7 +104,7 @@ __device__ __forceinline__ void z4_point(const ZCVarPtrs &U, const PointCtx &P, 
       const double w = (c == d ? -0.5 : -1.0) * gi[sy(c, d)] * (c == d ? o2[c] : o1[c] * o1[d]);
 #pragma unroll
       for (int a = 0; a < 6; ++a) {
-        const double dd = c == d ? d2n<ORD>(U.p[ZG11 + a], x, ZSTR(c)) : d11n<ORD>(U.p[ZG11 + a], x, ZSTR(c), ZSTR(d));
+        const double dd = c == d ? d2p<ORD, PREC>(U.p[ZG11 + a], x, ZSTR(c)) : d11p<ORD, PREC>(U.p[ZG11 + a], x, ZSTR(c), ZSTR(d));
         Rt[a] += w * dd;
       }
     }
@@ -113,7 +113,7 @@ __device__ __forceinline__ void z4_point(const ZCVarPtrs &U, const PointCtx &P, 
 #pragma unroll
     for (int b = 0; b < 3; ++b)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) dG[b][c] = o1[b] * d1n<ORD>(U.p[ZGA1 + c], x, ZSTR(b));
+      for (int c = 0; c < 3; ++c) dG[b][c] = o1[b] * d1p<ORD, PREC>(U.p[ZGA1 + c], x, ZSTR(b));
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -134,7 +134,7 @@ __device__ __forceinline__ void z4_point(const ZCVarPtrs &U, const PointCtx &P, 
   double df[3], dchic[3];  // dchic = d chi / chiguarded
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const double dc = o1[a] * d1n<ORD>(U.p[ZCHI], x, ZSTR(a));
+    const double dc = o1[a] * d1p<ORD, PREC>(U.p[ZCHI], x, ZSTR(a));
     df[a] = oocp * dc / chig;
     dchic[a] = dc / chig;
   }
@@ -149,8 +149,8 @@ __device__ __forceinline__ void z4_point(const ZCVarPtrs &U, const PointCtx &P, 
     for (int a = 0; a < 3; ++a)
 #pragma unroll
       for (int b = a; b < 3; ++b) {
-        const double ddchi = a == b ? o2[a] * d2n<ORD>(U.p[ZCHI], x, ZSTR(a))
-                                    : o1[a] * o1[b] * d11n<ORD>(U.p[ZCHI], x, ZSTR(a), ZSTR(b));
+        const double ddchi = a == b ? o2[a] * d2p<ORD, PREC>(U.p[ZCHI], x, ZSTR(a))
+                                    : o1[a] * o1[b] * d11p<ORD, PREC>(U.p[ZCHI], x, ZSTR(a), ZSTR(b));
         double t = oocp * ddchi / chig - p.chipsipower * df[a] * df[b];
         t -= gam[0][sy(a, b)] * df[0] + gam[1][sy(a, b)] * df[1] + gam[2][sy(a, b)] * df[2];
         cddf[sy(a, b)] = t;
@@ -171,7 +171,7 @@ __device__ __forceinline__ void z4_point(const ZCVarPtrs &U, const PointCtx &P, 
   // lapse
   double da[3], cdda[6];
 #pragma unroll
-  for (int a = 0; a < 3; ++a) da[a] = o1[a] * d1n<ORD>(U.p[ZALPHA], x, ZSTR(a));
+  for (int a = 0; a < 3; ++a) da[a] = o1[a] * d1p<ORD, PREC>(U.p[ZALPHA], x, ZSTR(a));
   {
     double dfda = 0.0;
 #pragma unroll
@@ -183,8 +183,8 @@ __device__ __forceinline__ void z4_point(const ZCVarPtrs &U, const PointCtx &P, 
 #pragma unroll
       for (int b = a; b < 3; ++b) {
         const int ab = sy(a, b);
-        double t = a == b ? o2[a] * d2n<ORD>(U.p[ZALPHA], x, ZSTR(a))
-                          : o1[a] * o1[b] * d11n<ORD>(U.p[ZALPHA], x, ZSTR(a), ZSTR(b));
+        double t = a == b ? o2[a] * d2p<ORD, PREC>(U.p[ZALPHA], x, ZSTR(a))
+                          : o1[a] * o1[b] * d11p<ORD, PREC>(U.p[ZALPHA], x, ZSTR(a), ZSTR(b));
         t -= gam[0][ab] * da[0] + gam[1][ab] * da[1] + gam[2][ab] * da[2];
         cdda[ab] = t - 2.0 * (df[a] * da[b] + df[b] * da[a] - g[ab] * dfda);
       }
@@ -228,8 +228,8 @@ __device__ __forceinline__ void z4_point(const ZCVarPtrs &U, const PointCtx &P, 
     double dKhat[3], dTheta[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      dKhat[a] = o1[a] * d1n<ORD>(U.p[ZKHAT], x, ZSTR(a));
-      dTheta[a] = o1[a] * d1n<ORD>(U.p[ZTHETA], x, ZSTR(a));
+      dKhat[a] = o1[a] * d1p<ORD, PREC>(U.p[ZKHAT], x, ZSTR(a));
+      dTheta[a] = o1[a] * d1p<ORD, PREC>(U.p[ZTHETA], x, ZSTR(a));
     }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -254,7 +254,7 @@ __device__ __forceinline__ void z4_point(const ZCVarPtrs &U, const PointCtx &P, 
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) db[a][c] = o1[a] * d1n<ORD>(U.p[ZBETA1 + c], x, ZSTR(a));
+      for (int c = 0; c < 3; ++c) db[a][c] = o1[a] * d1p<ORD, PREC>(U.p[ZBETA1 + c], x, ZSTR(a));
     const double divbeta = db[0][0] + db[1][1] + db[2][2];
     const double totdivbeta = (2.0 / 3.0) * divbeta;
 #pragma unroll
@@ -279,8 +279,8 @@ __device__ __forceinline__ void z4_point(const ZCVarPtrs &U, const PointCtx &P, 
       for (int c = b; c < 3; ++c)
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-          const double dd = b == c ? o2[b] * d2n<ORD>(U.p[ZBETA1 + a], x, ZSTR(b))
-                                   : o1[b] * o1[c] * d11n<ORD>(U.p[ZBETA1 + a], x, ZSTR(b), ZSTR(c));
+          const double dd = b == c ? o2[b] * d2p<ORD, PREC>(U.p[ZBETA1 + a], x, ZSTR(b))
+                                   : o1[b] * o1[c] * d11p<ORD, PREC>(U.p[ZBETA1 + a], x, ZSTR(b), ZSTR(c));
           trddb[a] += (b == c ? 1.0 : 2.0) * gi[sy(b, c)] * dd;
           if (c == a) divdb[b] += dd;
           if (b == a && b != c) divdb[c] += dd;
@@ -352,10 +352,10 @@ __device__ __forceinline__ void z4_point(const ZCVarPtrs &U, const PointCtx &P, 
     const double e = p.dissfactor;
     if (p.order_dissipation == 6) {
 #pragma unroll
-      for (int v = 0; v < ZNV; ++v) r[v] += e * ko_sum<6>(U.p[v], x, kst, ooh);
+      for (int v = 0; v < ZNV; ++v) r[v] += e * ko_p<6, PREC>(U.p[v], x, kst, ooh);
     } else {
 #pragma unroll
-      for (int v = 0; v < ZNV; ++v) r[v] += e * ko_sum<4>(U.p[v], x, kst, ooh);
+      for (int v = 0; v < ZNV; ++v) r[v] += e * ko_p<4, PREC>(U.p[v], x, kst, ooh);
     }
   }
 #undef ZSTR
@@ -385,7 +385,7 @@ __device__ __forceinline__ void z4_store(const double r[ZNV], int x, const ZVarP
   }
 }
 
-template <int CSY = 0, int CSZ = 0>
+template <int CSY = 0, int CSZ = 0, int PREC = 0>
 __global__ void __launch_bounds__(128) z4_rhs_kernel(ZCVarPtrs U, ZVarPtrs out, ZCVarPtrs pre, ZVarPtrs acc, Epilogue E,
                                                     const nrgpu_z4_params p, BoxGeo box,
                                                     const int *__restrict__ boundary, double dx, double dy, double dz,
@@ -410,9 +410,9 @@ __global__ void __launch_bounds__(128) z4_rhs_kernel(ZCVarPtrs U, ZVarPtrs out, 
     return;
   }
   double r[ZNV];
-  if (oc == 4) z4_point<4, CSY, CSZ>(U, P, p, r);
-  else if (oc == 2) z4_point<2, CSY, CSZ>(U, P, p, r);
-  else z4_point<6, CSY, CSZ>(U, P, p, r);
+  if (oc == 4) z4_point<4, CSY, CSZ, PREC>(U, P, p, r);
+  else if (oc == 2) z4_point<2, CSY, CSZ, PREC>(U, P, p, r);
+  else z4_point<6, CSY, CSZ, PREC>(U, P, p, r);
   double s = 0.0;
 #pragma unroll
   for (int v = 0; v < ZNV; ++v) s += r[v];

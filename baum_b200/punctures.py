@@ -26,6 +26,16 @@ def brill_lindquist_state(level, punctures):
     return u
 
 
+def z4_brill_lindquist_state(level, punctures):
+    """The same data in the Z4c evolve list (Khat = K = 0, Theta = 0 inserted
+    before alpha, z4.c:234-242).  Returns a (25, npoints) array."""
+    b = brill_lindquist_state(level, punctures)
+    u = np.zeros((abi.Z4_NVARS, b.shape[1]))
+    u[:17] = b[:17]
+    u[18:] = b[17:]
+    return u
+
+
 def schwarzschild_c1(n_inner=64, dx=0.25):
     """The single-puncture workload: nxyz = n_inner gives an (n_inner+2)^3
     box (grid.c:84-99), M = 1 at the origin (never on a grid point)."""

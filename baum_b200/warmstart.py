@@ -149,15 +149,15 @@ def grid_coords(m, dx):
     return h0 + (i % m) * dx, h0 + ((i // m) % m) * dx, h0 + (i // (m * m)) * dx
 
 
-def sample_points(b, m, dx, n, rng, near=2.5):
-    """n grid points: half uniform over the cube, half within `near` of a
-    puncture (where u varies fastest)."""
+def sample_points(b, m, dx, n, rng, near=2.5, frac_near=0.5):
+    """n grid points: a fraction frac_near within `near` of a puncture (where
+    u varies fastest), the rest uniform over the cube."""
     x, y, z = grid_coords(m, dx)
     close = np.zeros(x.size, dtype=bool)
     for p in b.pos:
         close |= (x - p[0]) ** 2 + (y - p[1]) ** 2 + (z - p[2]) ** 2 < near * near
     cand = np.flatnonzero(close)
-    k = n // 2
+    k = int(n * frac_near)
     return np.concatenate([rng.integers(0, m ** 3, n - k), rng.choice(cand, k, replace=len(cand) < k)])
 
 
@@ -171,7 +171,7 @@ def solve_binary(mg, b, u=None):
     return u, n, res
 
 
-def generate(binaries, m=C2_M, dx=C2_DX, npts=16384, cycles=80, seed=0, log=print):
+def generate(binaries, m=C2_M, dx=C2_DX, npts=16384, cycles=80, seed=0, frac_near=0.5, log=print):
     """Training set: each binary solved by the GPU full-V multigrid (capped
     at `cycles` V cycles, residual ~1e-8), npts sampled points per binary.
     Returns (conds[nsets,20], set_idx, pt_idx, y = u / USCALE)."""
@@ -182,7 +182,7 @@ def generate(binaries, m=C2_M, dx=C2_DX, npts=16384, cycles=80, seed=0, log=prin
     for s, b in enumerate(binaries):
         u, n, res = solve_binary(mg, b)
         uh = u.cpu().numpy()
-        idx = sample_points(b, m, dx, npts, rng)
+        idx = sample_points(b, m, dx, npts, rng, frac_near=frac_near)
         conds.append(cond_vector(b))
         sets.append(np.full(npts, s, dtype=np.int32))
         pts.append(idx.astype(np.int32))
@@ -261,6 +261,8 @@ def main():
     ap.add_argument("--cycles", type=int, default=80)
     ap.add_argument("--epochs", type=int, default=12)
     ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--frac-near", type=float, default=0.5)
+    ap.add_argument("--eval-nmax", type=int, default=2000)
     ap.add_argument("--out", default=os.path.dirname(WEIGHTS))
     a = ap.parse_args()
     torch.cuda.set_device(0)
@@ -270,16 +272,17 @@ def main():
     held_b = [Binary.sample(np.random.default_rng(a.seed + 1 + i)) for i in range(a.heldout)]
     t0 = time.time()
     print("generating %d solutions at %d^3" % (a.sets, C2_M), flush=True)
-    data = generate(train_b, npts=a.npts, cycles=a.cycles, seed=a.seed)
+    data = generate(train_b, npts=a.npts, cycles=a.cycles, seed=a.seed, frac_near=a.frac_near)
     t_gen = time.time() - t0
     net = Network(16384, init_params(np.random.default_rng(a.seed + 7)))
     t0 = time.time()
     hist = train(net, data, epochs=a.epochs)
     t_train = time.time() - t0
     path = os.path.join(a.out, "warmstart_c2.npz")
-    net.save(path, sets=a.sets, npts=a.npts, cycles=a.cycles, epochs=a.epochs, seed=a.seed, m=C2_M, dx=C2_DX)
+    net.save(path, sets=a.sets, npts=a.npts, cycles=a.cycles, epochs=a.epochs, seed=a.seed, m=C2_M, dx=C2_DX,
+             frac_near=a.frac_near)
     print("evaluating on %d held-out binaries" % a.heldout, flush=True)
-    rows = evaluate(Network.load(path), held_b)
+    rows = evaluate(Network.load(path), held_b, nmax=a.eval_nmax)
     rep = {"train_seconds": t_train, "generate_seconds": t_gen, "loss_history": hist, "heldout": rows,
            "weights": path}
     with open(os.path.join(a.out, "warmstart_report.json"), "w") as f:

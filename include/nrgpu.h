@@ -115,6 +115,12 @@ typedef struct {
   double chiDivFloor, chipsipower;
   double bc_var0[NRGPU_Z4_NVARS];
   double bc_speed[NRGPU_Z4_NVARS];
+  /* arithmetic of the finite differences (no counterpart in the reference):
+   * 0 FP64 throughout; 1 Kreiss-Oliger sums in FP32; 2 Kreiss-Oliger and
+   * the centred first/second derivative sums in FP32.  The taps enter as
+   * FP64 differences to the centre value rounded to FP32; state, algebra,
+   * advection and RK4 stay FP64. */
+  int precision;
 } nrgpu_z4_params;
 
 /* ---- library ---------------------------------------------------------- */
