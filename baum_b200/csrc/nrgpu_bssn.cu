@@ -543,7 +543,7 @@ __device__ __forceinline__ int ladder(int order, int d) {
 // CSY, CSZ: the box strides dj = m and dk = m n when known at compile time
 // (0 = read them from the box)
 template <int CSY = 0, int CSZ = 0>
-__global__ void __launch_bounds__(128) bssn_rhs_kernel(CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPtrs acc,
+__global__ void __launch_bounds__(128, NRGPU_RHS_MINBLOCKS) bssn_rhs_kernel(CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPtrs acc,
                                                       Epilogue E, const nrgpu_bssn_params p, BoxGeo box,
                                                       const int *__restrict__ boundary, double dx, double dy,
                                                       double dz, int *status) {
@@ -1067,6 +1067,13 @@ static int z4_launch(nrgpu_level *L, const ZCVarPtrs &U, const ZVarPtrs &out, co
       } else if (bx.m == 162 && bx.n == 162)
         z4_rhs_kernel<162, 162 * 162><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy,
                                                             L->dz, L->d_status);
+#define NRGPU_Z4_FIXED(M_)                                                                                   \
+      else if (bx.m == M_ && bx.n == M_)                                                                    \
+        z4_rhs_kernel<M_, M_ * M_><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, \
+                                                        L->dz, L->d_status);
+      // the finer-level boxes of the batched mesh-refinement workload
+      NRGPU_Z4_FIXED(168) NRGPU_Z4_FIXED(136) NRGPU_Z4_FIXED(104) NRGPU_Z4_FIXED(72)
+#undef NRGPU_Z4_FIXED
       else if (bx.m == 66 && bx.n == 66)
         z4_rhs_kernel<66, 66 * 66><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy,
                                                          L->dz, L->d_status);

@@ -6,6 +6,12 @@
 
 #define NRGPU_NV 24
 
+// minimum resident blocks of 128 threads per SM for the rhs kernels
+// (__launch_bounds__): 1 leaves the compiler 255 registers per thread
+#ifndef NRGPU_RHS_MINBLOCKS
+#define NRGPU_RHS_MINBLOCKS 1
+#endif
+
 // 24 device pointers passed by value as a kernel parameter
 struct VarPtrs {
   double *p[NRGPU_NV];

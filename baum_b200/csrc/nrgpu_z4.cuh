@@ -386,7 +386,7 @@ __device__ __forceinline__ void z4_store(const double r[ZNV], int x, const ZVarP
 }
 
 template <int CSY = 0, int CSZ = 0, int PREC = 0>
-__global__ void __launch_bounds__(128) z4_rhs_kernel(ZCVarPtrs U, ZVarPtrs out, ZCVarPtrs pre, ZVarPtrs acc, Epilogue E,
+__global__ void __launch_bounds__(128, NRGPU_RHS_MINBLOCKS) z4_rhs_kernel(ZCVarPtrs U, ZVarPtrs out, ZCVarPtrs pre, ZVarPtrs acc, Epilogue E,
                                                     const nrgpu_z4_params p, BoxGeo box,
                                                     const int *__restrict__ boundary, double dx, double dy, double dz,
                                                     int *status) {

@@ -76,3 +76,17 @@ def test_fp32_stencil_option_error(gpu, precision, bound):
     err = relerr(out[1], out[0])
     assert np.isfinite(out[1]).all()
     assert 0 < err.max() < bound
+
+
+def test_z4_fixed_stride_box_matches_oracle(gpu):
+    """A box size with compile-time strides (72^3, a finer level of the
+    batched refinement workload): one RK4 step against the oracle."""
+    lev = abi.Level.single_box(72, 0.3)
+    u0 = z4_binary_state(lev, [(0.5, 3.0, 0.0, 0.0), (0.5, -3.0, 0.0, 0.0)])
+    p = abi.z4_params()
+    dl = z4.DeviceLevel(lev)
+    u = torch.from_numpy(u0.copy()).cuda()
+    z4.evolve_rk_rk4(dl, u, 0.075, p)
+    torch.cuda.synchronize()
+    uo = oracle.z4_evolve(lev, np.ascontiguousarray(u0.copy()), 0.075, 1, p)
+    assert relerr(u.cpu().numpy(), uo).max() < TOL
