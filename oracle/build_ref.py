@@ -61,14 +61,17 @@ MODULES = [
 FINAL = {"main", "adm", "evolve"}  # modules with a bam_<name>_final()
 
 
-def write_generated(ref, gen):
+def write_generated(ref, gen, extra=()):
+    """extra: (name, header) of further modules, initialised last."""
     os.makedirs(gen, exist_ok=True)
-    names = [os.path.basename(d) for d, _ in MODULES] + ["nrharness"]
+    names = [os.path.basename(d) for d, _ in MODULES] + ["nrharness"] + [n for n, _ in extra]
     inc = ["/* module list for the oracle build (written by oracle/build_ref.py) */"]
     for d, _ in MODULES:
         n = os.path.basename(d)
         inc.append('#include "%s/%s/bam_%s.h"' % (ref, d, n))
     inc.append('#include "%s/harness/bam_nrharness.h"' % HERE)
+    for _, h in extra:
+        inc.append('#include "%s"' % h)
     init = []
     fin = []
     # the reference calls every module initializer except main's in list order
@@ -150,6 +153,39 @@ def main():
     r = subprocess.run([a.cc, "-fopenmp", "-o", exe] + entry +
                        ["-Wl,--start-group", lib, "-Wl,--end-group", "-lm"],
                        capture_output=True, text=True)
+    if r.returncode:
+        print(r.stderr[-6000:])
+        return 1
+    print("build_ref: built", exe)
+    return build_gpu_variant(ref, a, base, obj, entry, lib)
+
+
+def build_gpu_variant(ref, a, base, obj, entry, lib):
+    """oracle/_ref/bam_gpu: the same reference with the B200 binding module
+    (baum_b200/bam/nrgpu_bam.c) linked against baum_b200/libnrgpu.so, the
+    drop-in as a maintainer would add it.  Built only when the library is."""
+    repo = os.path.dirname(HERE)
+    so = os.path.join(repo, "baum_b200", "libnrgpu.so")
+    if not os.path.exists(so):
+        print("build_ref: baum_b200/libnrgpu.so not built; oracle/_ref/bam_gpu skipped")
+        return 0
+    gen = os.path.join(OUT, "gen_gpu")
+    write_generated(ref, gen, [("nrgpu", os.path.join(repo, "baum_b200", "bam", "bam_nrgpu.h"))])
+    bgen = [x if not x.startswith("-I" + os.path.join(OUT, "gen")) else "-I" + gen for x in base]
+    main_o = os.path.join(obj, "gpu__main.o")
+    bind_o = os.path.join(obj, "gpu__nrgpu_bam.o")
+    for src, o, inc in [(os.path.join(ref, "src/main/main/main.c"), main_o, os.path.join(ref, "src/main/main")),
+                        (os.path.join(repo, "baum_b200", "bam", "nrgpu_bam.c"), bind_o,
+                         os.path.join(ref, "src/projects/bssn"))]:
+        r = subprocess.run(bgen + ["-I" + inc, "-c", src, "-o", o], capture_output=True, text=True)
+        if r.returncode:
+            print(r.stderr[-4000:])
+            return 1
+    cuda = "/usr/local/cuda/lib64"
+    exe = os.path.join(OUT, "bam_gpu")
+    r = subprocess.run([a.cc, "-fopenmp", "-o", exe, main_o, bind_o, "-Wl,--start-group", lib, "-Wl,--end-group",
+                        "-L" + os.path.dirname(so), "-lnrgpu", "-Wl,-rpath,$ORIGIN/../../baum_b200",
+                        "-L" + cuda, "-lcudart", "-Wl,-rpath," + cuda, "-lm"], capture_output=True, text=True)
     if r.returncode:
         print(r.stderr[-6000:])
         return 1
