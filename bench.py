@@ -39,7 +39,10 @@ RHS_PER_STEP = 4
 FLOP_PER_POINT = 4973
 # DRAM bytes of one interior rhs launch from the ncu capture summarised in
 # profiles/bssn_rhs_kernel_c1.md (None until captured)
-RHS_TRAFFIC_BYTES = None
+# DRAM bytes of one RK-stage launch of bssn_rhs_kernel on the 64^3 box
+# (dram__bytes_read.sum + dram__bytes_write.sum, mean of two captured
+# launches: 168.6 MB and 232.7 MB; profiles/bssn_rhs_kernel_c1.md)
+RHS_TRAFFIC_BYTES = 200.6e6
 CONFIG = {"workload": "bssn_schwarzschild_64^3_rk4", "box": "66^3 (64^3 inner + boundary layer)",
           "dx": DX, "dt": DT, "order": 4, "dissipation": "KO6 eps=0.1", "gauge": "1+log, Gamma-driver eta=2",
           "l2": "flushed (256 MiB write) before every timed step", "parallelism": "replicas"}
