@@ -291,6 +291,99 @@ def gpu_fmr(steps=2):
     return out
 
 
+FMR_REF_PAR = """physics = adm z4 nrharness
+adm_data = Minkowski
+z4_lapse = 1+log withshift
+z4_shift = gamma0 withGadv withBadv withShiftadv withB
+z4_shiftdriver = 2.0
+z4_shiftgammacoeff = 0.75
+z4_kappa1 = 0.02
+z4_kappa2 = 0.0
+grid = box
+amr = bo newfmr
+amr_fmr = nestedboxes
+amr_lmax = 2
+amr_nbuffer = 3
+nxyz = %d
+dxyz = 0.5
+order_centered = 4
+order_advection = 4
+advection_lopsided = 1
+order_dissipation = 6
+dissipation_factor = 0.1
+evolution_method = rk
+evolution_method_rk = rk4
+dtfac = 0.25
+boundary = radiative
+iterations = %d
+mass1 = 1
+mass2 = 0
+nrharness_dir = .
+nrharness_data = fourier
+nrharness_amp = 1e-3
+nrharness_length = 16
+nrharness_flags = yes
+"""
+
+
+def fmr_same_grid(nxyz=48, cores=None):
+    """The reference's own 3-level Berger-Oliger Z4c run (oracle/_ref/bam,
+    all host threads) against this build on the grid the reference made:
+    the GPU reads the reference's level boxes and flags from its dumps.  A
+    coarse step's time is the difference of a 3- and a 1-iteration run."""
+    import torch
+    from baum_b200 import abi, fmr, synthetic
+    from oracle import dumpfile
+    bam = os.path.join(ROOT, "oracle", "_ref", "bam")
+    if not os.path.exists(bam):
+        return None
+    cores = cores or os.cpu_count() or 1
+    walls, work = {}, None
+    for its in (1, 3):
+        work = tempfile.mkdtemp(prefix="bamfmr_")
+        with open(os.path.join(work, "f.par"), "w") as f:
+            f.write(FMR_REF_PAR % (nxyz, its))
+        t0 = time.time()
+        r = subprocess.run([bam, "-nt", str(cores), "f.par"], cwd=work, capture_output=True, text=True)
+        walls[its] = time.time() - t0
+        if r.returncode:
+            shutil.rmtree(work, ignore_errors=True)
+            return None
+        if its == 1:
+            levels = []
+            for l in range(3):
+                d = dumpfile.read(os.path.join(work, "flags_l%d.bin" % l))
+                b = d["boxes"][0]
+                levels.append(abi.Level([(int(b[0]), int(b[1]), int(b[2]), b[4], b[5], b[6])], float(d["dx"]),
+                                        d["boundary"]))
+        shutil.rmtree(work, ignore_errors=True)
+    ref_s = (walls[3] - walls[1]) / 2
+    inner = [int((lev.boundary == 0).sum()) for lev in levels]
+    upd = sum(n * 4 * 2 ** l for l, n in enumerate(inner))
+    params = [abi.z4_params_from_par(dissfactor=(0.1 if l == 0 else 0.02) / 64) for l in range(3)]
+    dt = [0.25 * lev.desc.dx for lev in levels]
+    H = fmr.Hierarchy(levels, dt, params)
+    u = []
+    for lev in levels:
+        x, y, z = (torch.from_numpy(c).cuda() for c in lev.coords())
+        u.append(synthetic.fourier_state_device(x, y, z, abi.Z4_NVARS, synthetic.Z4_UNIT, 8, 1e-3, 16.0, 1))
+    H.advance(u, 2)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    H.advance(u, 4)
+    b.record()
+    torch.cuda.synchronize()
+    gpu_ms = a.elapsed_time(b) / 4
+    H.close()
+    return {"workload": "reference's 3-level Z4c grid, nxyz %d, dxyz 0.5, boxes per side %s"
+                        % (nxyz, [lev.boxes[0].m for lev in levels]),
+            "rhs_point_updates_per_coarse_step": upd,
+            "gpu": {"ms_per_coarse_step": gpu_ms, "value": upd / (gpu_ms * 1e-3)},
+            "reference": {"s_per_coarse_step": ref_s, "value": upd / ref_s, "cores": cores,
+                          "timing": "wall time of a 3-iteration minus a 1-iteration run, over 2"}}
+
+
 def oracle_port_cpu():
     """Fallback CPU baseline: the oracle restatement, one RK4 step."""
     from oracle import oracle
@@ -420,6 +513,8 @@ def run_ours(args, rank, world):
     mg66 = gpu_mg(66, 0.25, bins[:1])
     ref66 = reference_mg(bins[0], 64, 0.25) if not args.no_cpu else None
     fmr_line = gpu_fmr(2)
+    if world == 1 and not args.no_cpu:
+        fmr_line["same_grid_reference"] = fmr_same_grid()
     multigrid = {
         "workload": "binary punctures, Bowen-York, 130^3 points (129^3 cells), dx=0.125, tol 1e-10 RMS, full-V",
         "vcycles": [r["vcycles"] for r in mg130], "ms": [round(r["ms"], 2) for r in mg130],
