@@ -15,6 +15,10 @@
  *                           (evolve.c:231-235) and the host state is refreshed
  *                           after every step for ANALYZE/OUTPUT/checkpoint.
  *                           Set bssn_register_algcon = no with this mode.
+ *   nrgpu_mode = fmr        the whole Berger-Oliger step of all levels (one
+ *                           box each) runs on the GPU at level 0's EVOLVE
+ *                           hook; set bssn/z4_register_algcon = no.
+ * physics with z4 selects the Z4c system (resident and fmr modes).
  *
  * Parameters are read exactly where bssn_rhs_movpunc_N reads them
  * (bssn_rhs_movpunc_N.c:107-145), the boundary speeds and far limits from the
@@ -27,8 +31,15 @@
 #include "../../../include/nrgpu.h"
 
 #define NV NRGPU_BSSN_NVARS
+#define ZNV NRGPU_Z4_NVARS
+
+/* defined by the z4 project (z4.c:8) when it is linked; the weak reference
+ * lets a BSSN-only tree link this module too */
+extern int METRIC_z4_INDX_VAR __attribute__((weak));
 
 static int nrgpu_mode_resident = 0;
+static int nrgpu_mode_fmr = 0;
+static int nrgpu_system_z4 = 0;
 
 typedef struct {
   tL *bamlevel;
@@ -92,6 +103,48 @@ static void read_params(tL *level, tVarList *u, nrgpu_bssn_params *p)
   }
 }
 
+/* the parameters z4_rhs_movpunc_N reads (z4_rhs_movpunc_N.c:109-138) */
+static void read_params_z4(tL *level, tVarList *u, nrgpu_z4_params *p)
+{
+  int j;
+  memset(p, 0, sizeof *p);
+  p->order_centered = Geti("order_centered");
+  p->order_advection = Geti("order_advection");
+  p->advection_lopsided = Geti("advection_lopsided");
+  p->advection_lopsided6 = Geti("advection_lopsided6");
+  p->order_dissipation = Geti("order_dissipation");
+  p->dissfactor = get_dissipation_factor(level);
+  p->kappa1 = Getd("z4_kappa1");
+  p->kappa2 = Getd("z4_kappa2");
+  p->zeroThetaRHS = Getv("z4_zeroThetaRHS", "no");
+  p->useNPTs = Getv("z4_useNPTs", "yes");
+  p->subtractA = Getv("z4_subtractA", "yes");
+  p->normalizedetg = Getv("z4_normalizedetg", "yes");
+  p->oploglapse = Getv("z4_lapse", "1+log");
+  p->oploglapse2 = Getv("z4_lapse", "1+log2");
+  p->oplogwithshift = Getv("z4_lapse", "withshift");
+  p->harmoniclapse = Getv("z4_lapse", "harmonic");
+  p->gamma0factor = Getv("z4_shift", "gamma0");
+  p->gamma2factor = Getv("z4_shift", "gamma2");
+  p->withGadv = Getv("z4_shift", "withGadv");
+  p->withShiftadv = Getv("z4_shift", "withShiftadv");
+  p->withBadv = Getv("z4_shift", "withBadv");
+  p->withB = Getv("z4_shift", "withB");
+  p->lapseharmonicf = Getd("z4_lapseharmonicf");
+  p->shiftalphapower = Getd("z4_shiftalphapower");
+  p->shiftgammacoeff = Getd("z4_shiftgammacoeff");
+  p->shiftdriver = Getd("z4_shiftdriver");
+  p->chiDivFloor = Getd("z4_chi_div_floor");
+  p->chipsipower = Getd("z4_chi_psipower");
+  if (Getv("z4_forceKzero", "yes")) errorexit("nrgpu: z4_forceKzero is not supported");
+  if (level->shells) errorexit("nrgpu: shells are not supported");
+  for (j = 0; j < ZNV; j++) {
+    int i = u->index[METRIC_z4_INDX_VAR + j];
+    p->bc_var0[j] = VarFarLimit(i);
+    p->bc_speed[j] = Getv("boundary_radconstant", VarName(i)) ? 0.0 : VarPropSpeed(i);
+  }
+}
+
 static nrgpu_slot *slot_of(tL *level)
 {
   nrgpu_slot *s = &slots[level->l];
@@ -115,26 +168,29 @@ static nrgpu_slot *slot_of(tL *level)
     s->bamlevel = level;
     s->npoints = level->npoints;
     s->uploaded = 0;
-    if (cudaMalloc((void **)&s->d_state, sizeof(double) * NV * level->npoints) ||
-        cudaMalloc((void **)&s->d_a, sizeof(double) * NV * level->npoints) ||
-        cudaMalloc((void **)&s->d_b, sizeof(double) * NV * level->npoints) ||
-        cudaMalloc((void **)&s->d_c, sizeof(double) * NV * level->npoints))
+    if (cudaMalloc((void **)&s->d_state, sizeof(double) * ZNV * level->npoints) ||
+        cudaMalloc((void **)&s->d_a, sizeof(double) * ZNV * level->npoints) ||
+        cudaMalloc((void **)&s->d_b, sizeof(double) * ZNV * level->npoints) ||
+        cudaMalloc((void **)&s->d_c, sizeof(double) * ZNV * level->npoints))
       errorexit("nrgpu: device allocation failed");
   }
   return s;
 }
 
+static int nvars(void) { return nrgpu_system_z4 ? ZNV : NV; }
+static int first_var(void) { return nrgpu_system_z4 ? METRIC_z4_INDX_VAR : METRIC_bssn_INDX_VAR; }
+
 static void lists(double *base, int npoints, double **ptr)
 {
   int j;
-  for (j = 0; j < NV; j++) ptr[j] = base + (size_t)j * npoints;
+  for (j = 0; j < nvars(); j++) ptr[j] = base + (size_t)j * npoints;
 }
 
 static void copy_vl(tL *level, tVarList *vl, double *dev, int to_device)
 {
   int j;
-  for (j = 0; j < NV; j++) {
-    double *h = level->v[vl->index[METRIC_bssn_INDX_VAR + j]];
+  for (j = 0; j < nvars(); j++) {
+    double *h = level->v[vl->index[first_var() + j]];
     double *d = dev + (size_t)j * level->npoints;
     if (cudaMemcpy(to_device ? (void *)d : (void *)h, to_device ? (void *)h : (void *)d,
                    sizeof(double) * level->npoints, to_device ? 1 : 2))
@@ -185,22 +241,96 @@ int nrgpu_evolve_resident(tL *level)
 {
   tVarList *u = 0;
   nrgpu_slot *s;
-  nrgpu_bssn_params p;
-  double *st[NV];
+  double *st[ZNV];
   if (!nrgpu_mode_resident) return 0;
   evolve_vlretrieve(&u, 0, 0);
   if (!u) errorexit("nrgpu: no evolution list");
   u->level = level;
   timer_start(level, "evolve");
   s = slot_of(level);
-  read_params(level, u, &p);
   lists(s->d_state, level->npoints, st);
   if (!s->uploaded) {
     copy_vl(level, u, s->d_state, 1);
     s->uploaded = 1;
   }
-  check(nrgpu_bssn_rk4_step(s->lev, st, level->dt, &p, 0), "rk4");
+  if (nrgpu_system_z4) {
+    nrgpu_z4_params p;
+    read_params_z4(level, u, &p);
+    check(nrgpu_z4_rk4_step(s->lev, st, level->dt, &p, 0), "rk4");
+  } else {
+    nrgpu_bssn_params p;
+    read_params(level, u, &p);
+    check(nrgpu_bssn_rk4_step(s->lev, st, level->dt, &p, 0), "rk4");
+  }
   copy_vl(level, u, s->d_state, 0);
+  timer_stop(level, "evolve");
+  return 0;
+}
+
+/* EVOLVE hook of the mesh-refinement mode, on level 0: one coarse step of
+ * every level (advance_levelandsublevels, main.c:397-418, with the time
+ * interpolation and restrict_prolong_evolve) on the device, then every
+ * level's state back to the host arrays.  BAM still walks the finer levels:
+ * their EVOLVE is a no-op here and in evolve() (null "geometry"), so BAM
+ * never allocates the time interpolant; its restrict_prolong_evolve then
+ * does nothing at unaligned times (restrict_varlist/prolong_varlist return
+ * on a null list) and, at aligned times, recomputes from the host arrays
+ * exactly what the device already did.  POST_EVOLVE, ANALYZE and OUTPUT see
+ * every level at the end of the coarse step. */
+static nrgpu_fmr *fmr_h = 0;
+static double *fmr_state[64];
+
+int nrgpu_evolve_fmr(tL *level)
+{
+  tG *g = level->grid;
+  tVarList *u = 0;
+  int l, nl, nv = nvars();
+  double *ptrs[64 * ZNV];
+  if (!nrgpu_mode_fmr || level->l != 0) return 0;
+  nl = g->lmax + 1;
+  if (g->lmin != 0 || nl > 16) errorexit("nrgpu: levels 0..lmax with lmax < 16");
+  evolve_vlretrieve(&u, 0, 0);
+  if (!u) errorexit("nrgpu: no evolution list");
+  timer_start(level, "evolve");
+  if (!fmr_h) {
+    nrgpu_level_desc d[16];
+    nrgpu_box box[16];
+    double dt[16];
+    nrgpu_bssn_params bp[16];
+    nrgpu_z4_params zp[16];
+    nrgpu_fmr_params fp;
+    for (l = 0; l < nl; l++) {
+      tL *lv = g->level[l];
+      tB *bx;
+      if (lv->nboxes != 1) errorexit("nrgpu: the refinement mode takes one box per level");
+      bx = lv->box[0];
+      box[l].m = bx->m; box[l].n = bx->n; box[l].o = bx->o; box[l].noffset = bx->noffset;
+      box[l].x0 = bx->x0; box[l].y0 = bx->y0; box[l].z0 = bx->z0;
+      d[l].nboxes = 1; d[l].box = &box[l]; d[l].npoints = lv->npoints;
+      d[l].dx = lv->dx; d[l].dy = lv->dy; d[l].dz = lv->dz; d[l].boundary = lv->boundary;
+      dt[l] = lv->dt;
+      u->level = lv;
+      if (nrgpu_system_z4) read_params_z4(lv, u, &zp[l]);
+      else read_params(lv, u, &bp[l]);
+      if (cudaMalloc((void **)&fmr_state[l], sizeof(double) * nv * lv->npoints))
+        errorexit("nrgpu: device allocation failed");
+      copy_vl(lv, u, fmr_state[l], 1);
+    }
+    nrgpu_fmr_params_default(&fp);
+    fp.system = nrgpu_system_z4 ? NRGPU_SYSTEM_Z4C : NRGPU_SYSTEM_BSSN;
+    fp.lbo = g->lbo;
+    fp.order_timeinterpolation = Geti("order_timeinterpolation");
+    fp.order_RP = Geti("order_RP");
+    fp.nbuffer = Geti("amr_nbuffer");
+    check(nrgpu_fmr_create(nl, d, dt, nrgpu_system_z4 ? (void *)zp : (void *)bp, &fp, &fmr_h), "fmr");
+  }
+  for (l = 0; l < nl; l++) lists(fmr_state[l], g->level[l]->npoints, ptrs + l * nv);
+  check(nrgpu_fmr_advance(fmr_h, ptrs, 1, 0), "fmr advance");
+  for (l = 0; l < nl; l++) {
+    u->level = g->level[l];
+    copy_vl(g->level[l], u, fmr_state[l], 0);
+  }
+  u->level = level;
   timer_stop(level, "evolve");
   return 0;
 }
@@ -209,17 +339,22 @@ int nrgpu_startup(tL *level)
 {
   if (level->l != 0) return 0;
   check(nrgpu_init(Geti("nrgpu_device")), "init");
-  if (Getv("nrgpu_mode", "resident")) {
-    nrgpu_mode_resident = 1;
+  nrgpu_system_z4 = Getv("physics", "z4");
+  if (nrgpu_system_z4 && !&METRIC_z4_INDX_VAR) errorexit("nrgpu: physics z4 without the z4 project");
+  if (Getv("nrgpu_mode", "resident") || Getv("nrgpu_mode", "fmr")) {
+    nrgpu_mode_resident = Getv("nrgpu_mode", "resident");
+    nrgpu_mode_fmr = Getv("nrgpu_mode", "fmr");
     set_rhs_func_register("geometry", 0);  /* evolve() returns at once */
-    if (Getv("bssn_register_algcon", "yes"))
-      errorexit("nrgpu: resident mode runs algcon on the GPU, set bssn_register_algcon = no");
+    if (Getv(nrgpu_system_z4 ? "z4_register_algcon" : "bssn_register_algcon", "yes"))
+      errorexit("nrgpu: the GPU runs the algebraic constraints in this mode, set bssn/z4_register_algcon = no");
+  } else if (nrgpu_system_z4) {
+    errorexit("nrgpu: for z4 use nrgpu_mode = resident or fmr");
   } else {
     set_rhs_func_register("geometry", nrgpu_bssn_evolve_cb);
     set_rhs_func_register("geometry_bound", nrgpu_bssn_boundary_cb);
   }
-  printf("nrgpu: %s mode on device %d\n", nrgpu_mode_resident ? "resident" : "callback",
-         Geti("nrgpu_device"));
+  printf("nrgpu: %s mode on device %d\n",
+         nrgpu_mode_fmr ? "fmr" : (nrgpu_mode_resident ? "resident" : "callback"), Geti("nrgpu_device"));
   return 0;
 }
 
@@ -227,8 +362,9 @@ void bam_nrgpu(void)
 {
   if (!Getv("physics", "nrgpu")) return;
   printf("Adding nrgpu (B200 evolution path)\n");
-  AddPar("nrgpu_mode", "callback", "how the GPU path plugs in [callback,resident]");
+  AddPar("nrgpu_mode", "callback", "how the GPU path plugs in [callback,resident,fmr]");
   AddPar("nrgpu_device", "0", "CUDA device");
   AddFun(POST_INITIALDATA, nrgpu_startup, "nrgpu: register the GPU evolution");
   AddFun(EVOLVE, nrgpu_evolve_resident, "nrgpu: resident RK4 step");
+  AddFun(EVOLVE, nrgpu_evolve_fmr, "nrgpu: one coarse step of all levels");
 }

@@ -542,8 +542,8 @@ __device__ __forceinline__ int ladder(int order, int d) {
 // (flag 0) only, the flagged ones are handled by bssn_flagged_kernel
 // CSY, CSZ: the box strides dj = m and dk = m n when known at compile time
 // (0 = read them from the box)
-template <int CSY = 0, int CSZ = 0>
-__global__ void __launch_bounds__(128, NRGPU_RHS_MINBLOCKS) bssn_rhs_kernel(CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPtrs acc,
+template <int CSY = 0, int CSZ = 0, int MAXO = 6, int MINB = NRGPU_RHS_MINBLOCKS>
+__global__ void __launch_bounds__(128, MINB) bssn_rhs_kernel(CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPtrs acc,
                                                       Epilogue E, const nrgpu_bssn_params p, BoxGeo box,
                                                       const int *__restrict__ boundary, double dx, double dy,
                                                       double dz, int *status) {
@@ -569,8 +569,8 @@ __global__ void __launch_bounds__(128, NRGPU_RHS_MINBLOCKS) bssn_rhs_kernel(CVar
   }
   double r[NRGPU_NV];
   if (oc == 2) bssn_point<2, CSY, CSZ>(U, P, p, r);
-  else if (oc == 4) bssn_point<4, CSY, CSZ>(U, P, p, r);
-  else bssn_point<6, CSY, CSZ>(U, P, p, r);
+  else if (oc == 4 || MAXO < 6) bssn_point<4, CSY, CSZ>(U, P, p, r);
+  else bssn_point<MAXO, CSY, CSZ>(U, P, p, r);
   double s = 0.0;
 #pragma unroll
   for (int v = 0; v < NRGPU_NV; ++v) s += r[v];
@@ -735,12 +735,20 @@ static int launch_rhs(nrgpu_level *L, const CVarPtrs &U, const VarPtrs &out, con
       dim3 grd((bx.m - 2 + 31) / 32, (bx.n - 2 + 3) / 4, bx.o - 2);
       // box strides as compile-time constants for the sizes of the standard
       // workloads: every stencil tap becomes one load with an immediate offset
-      if (bx.m == 66 && bx.n == 66)
+      // and, for runs of order <= 4, kernels without the 6th-order path
+      const bool o4 = p.order_centered <= 4;
+      if (bx.m == 66 && bx.n == 66 && o4)
+        bssn_rhs_kernel<66, 66 * 66, 4><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx,
+                                                              L->dy, L->dz, L->d_status);
+      else if (bx.m == 66 && bx.n == 66)
         bssn_rhs_kernel<66, 66 * 66><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy,
                                                            L->dz, L->d_status);
       else if (bx.m == 162 && bx.n == 162)
         bssn_rhs_kernel<162, 162 * 162><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx,
                                                               L->dy, L->dz, L->d_status);
+      else if (o4)
+        bssn_rhs_kernel<0, 0, 4><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy,
+                                                       L->dz, L->d_status);
       else
         bssn_rhs_kernel<<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
                                              L->d_status);
@@ -1041,6 +1049,27 @@ static ZCVarPtrs z4_c(const ZVarPtrs &v) {
   return c;
 }
 
+// FP64 interior launch with compile-time strides for the box sizes of the
+// workloads (66, 162, and the finer levels of the batched refinement step),
+// generic strides otherwise; MAXO = 4 for runs of order <= 4 leaves the
+// 6th-order path out of the kernel (fewer registers, less spilling)
+template <int MAXO>
+static void z4_interior_fp64(const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVarPtrs &pre, const ZVarPtrs &acc,
+                             const Epilogue &E, const nrgpu_z4_params &p, const BoxGeo &bx, nrgpu_level *L, dim3 grd,
+                             dim3 blk, cudaStream_t st) {
+#define NRGPU_Z4_FIXED(M_)                                                                                   \
+  if (bx.m == M_ && bx.n == M_) {                                                                           \
+    z4_rhs_kernel<M_, M_ * M_, 0, MAXO><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, \
+                                                             L->dy, L->dz, L->d_status);                    \
+    return;                                                                                                  \
+  }
+  NRGPU_Z4_FIXED(162) NRGPU_Z4_FIXED(168) NRGPU_Z4_FIXED(136) NRGPU_Z4_FIXED(104) NRGPU_Z4_FIXED(72)
+  NRGPU_Z4_FIXED(66)
+#undef NRGPU_Z4_FIXED
+  z4_rhs_kernel<0, 0, 0, MAXO><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
+                                                    L->d_status);
+}
+
 static int z4_launch(nrgpu_level *L, const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVarPtrs &pre,
                      const ZVarPtrs &acc, const Epilogue &E, const nrgpu_z4_params &p, cudaStream_t st, bool interior,
                      bool flagged) {
@@ -1064,22 +1093,11 @@ static int z4_launch(nrgpu_level *L, const ZCVarPtrs &U, const ZVarPtrs &out, co
         else
           z4_rhs_kernel<0, 0, 2><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
                                                        L->d_status);
-      } else if (bx.m == 162 && bx.n == 162)
-        z4_rhs_kernel<162, 162 * 162><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy,
-                                                            L->dz, L->d_status);
-#define NRGPU_Z4_FIXED(M_)                                                                                   \
-      else if (bx.m == M_ && bx.n == M_)                                                                    \
-        z4_rhs_kernel<M_, M_ * M_><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, \
-                                                        L->dz, L->d_status);
-      // the finer-level boxes of the batched mesh-refinement workload
-      NRGPU_Z4_FIXED(168) NRGPU_Z4_FIXED(136) NRGPU_Z4_FIXED(104) NRGPU_Z4_FIXED(72)
-#undef NRGPU_Z4_FIXED
-      else if (bx.m == 66 && bx.n == 66)
-        z4_rhs_kernel<66, 66 * 66><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy,
-                                                         L->dz, L->d_status);
-      else
-        z4_rhs_kernel<<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
-                                           L->d_status);
+      } else if (p.order_centered <= 4) {
+        z4_interior_fp64<4>(U, out, pre, acc, E, p, bx, L, grd, blk, st);
+      } else {
+        z4_interior_fp64<6>(U, out, pre, acc, E, p, bx, L, grd, blk, st);
+      }
     }
   }
   if (flagged && L->nflagpts > 0) {

@@ -385,7 +385,7 @@ __device__ __forceinline__ void z4_store(const double r[ZNV], int x, const ZVarP
   }
 }
 
-template <int CSY = 0, int CSZ = 0, int PREC = 0>
+template <int CSY = 0, int CSZ = 0, int PREC = 0, int MAXO = 6>
 __global__ void __launch_bounds__(128, NRGPU_RHS_MINBLOCKS) z4_rhs_kernel(ZCVarPtrs U, ZVarPtrs out, ZCVarPtrs pre, ZVarPtrs acc, Epilogue E,
                                                     const nrgpu_z4_params p, BoxGeo box,
                                                     const int *__restrict__ boundary, double dx, double dy, double dz,
@@ -410,9 +410,11 @@ __global__ void __launch_bounds__(128, NRGPU_RHS_MINBLOCKS) z4_rhs_kernel(ZCVarP
     return;
   }
   double r[ZNV];
-  if (oc == 4) z4_point<4, CSY, CSZ, PREC>(U, P, p, r);
+  // MAXO = 4 leaves the 6th-order path out of kernels for 4th-order runs
+  // (the ladder never asks for more than the requested order)
+  if (oc == 4 || (MAXO < 6 && oc == 6)) z4_point<4, CSY, CSZ, PREC>(U, P, p, r);
   else if (oc == 2) z4_point<2, CSY, CSZ, PREC>(U, P, p, r);
-  else z4_point<6, CSY, CSZ, PREC>(U, P, p, r);
+  else z4_point<MAXO, CSY, CSZ, PREC>(U, P, p, r);
   double s = 0.0;
 #pragma unroll
   for (int v = 0; v < ZNV; ++v) s += r[v];

@@ -76,3 +76,84 @@ def test_bam_with_the_gpu_path_matches_bam(gpu, cpu_state, mode, extra):
     u, out = run(BAM_GPU, " nrgpu", extra)
     assert "nrgpu: %s mode" % mode in out
     assert relerr(u, cpu_state).max() < 1e-12
+
+
+FMR_PAR = """physics = adm z4 nrharness%s
+adm_data = Minkowski
+z4_lapse = 1+log withshift
+z4_shift = gamma0 withGadv withBadv withShiftadv withB
+z4_shiftdriver = 2.0
+z4_shiftgammacoeff = 0.75
+z4_kappa1 = 0.02
+z4_kappa2 = 0.0
+grid = box
+amr = bo newfmr
+amr_fmr = nestedboxes
+amr_lmax = 2
+amr_nbuffer = 3
+nxyz = 16
+dxyz = 0.5
+order_centered = 4
+order_advection = 4
+advection_lopsided = 1
+order_dissipation = 6
+dissipation_factor = 0.1
+evolution_method = rk
+evolution_method_rk = rk4
+dtfac = 0.25
+boundary = radiative
+iterations = 2
+mass1 = 1
+mass2 = 0
+nrharness_dir = .
+nrharness_data = fourier
+nrharness_amp = 0.05
+nrharness_length = 16
+nrharness_dump = 2 4 8
+%s
+"""
+
+
+def run_fmr(binary, extra_physics, extra):
+    work = tempfile.mkdtemp(prefix="bamgpu_")
+    try:
+        with open(os.path.join(work, "t.par"), "w") as f:
+            f.write(FMR_PAR % (extra_physics, extra))
+        r = subprocess.run([binary, "-nt", "4", "t.par"], cwd=work, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+        return [dumpfile.read(os.path.join(work, "state_it%d_l%d.bin" % (2 * 2 ** l, l))) for l in range(3)], r.stdout
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+def test_bam_fmr_mode_matches_bam(gpu, cpu_state):
+    """nrgpu_mode = fmr: the whole Berger-Oliger step of the 3-level Z4c grid
+    on the GPU at level 0's EVOLVE hook.  BAM dumps every level right after
+    the level's own step (POST_EVOLVE), before its child restricts into it
+    and before its parent prolongs into its buffer zone; with the GPU hook
+    the host arrays already hold the end of the coarse step.  So the levels
+    are compared, after 2 coarse steps, on the points that this last
+    restriction and prolongation do not write, within the refinement
+    tolerance of the oracle pin (2e-11)."""
+    from baum_b200 import abi
+    from oracle import oracle
+    ref, _ = run_fmr(BAM, "", "")
+    got, out = run_fmr(BAM_GPU, " nrgpu", "nrgpu_mode = fmr\nz4_register_algcon = no")
+    assert "nrgpu: fmr mode" in out
+    levels = []
+    for d in ref:
+        b = d["boxes"][0]
+        levels.append(abi.Level([(int(b[0]), int(b[1]), int(b[2]), b[4], b[5], b[6])], float(d["dx"]),
+                                d["boundary"]))
+    keep = [np.ones(lv.npoints, dtype=bool) for lv in levels]
+    for l in (1, 2):
+        uc = np.zeros((1, levels[l - 1].npoints))
+        uf = np.ones((1, levels[l].npoints))
+        oracle.fmr_restrict_prolong(levels[l - 1], levels[l], uc, uf, 4, 3)
+        keep[l - 1] &= uc[0] < 0.5     # restricted parent points
+        keep[l] &= uf[0] > 0.5         # prolonged buffer points (prolongation of zeros)
+    for l in range(3):
+        a, b = got[l]["data"][:, keep[l]], ref[l]["data"][:, keep[l]]
+        err = np.abs(a - b).max(axis=1) / np.maximum(np.abs(b).max(axis=1), 1e-8)
+        assert keep[l].sum() > 0.3 * levels[l].npoints
+        assert err.max() < 2e-11, (l, err.max())
