@@ -211,7 +211,8 @@ class MgParams(C.Structure):
 
 class FmrParams(C.Structure):
     _fields_ = [("system", C.c_int), ("lbo", C.c_int), ("order_timeinterpolation", C.c_int),
-                ("order_RP", C.c_int), ("nbuffer", C.c_int), ("use_graph", C.c_int)]
+                ("order_RP", C.c_int), ("nbuffer", C.c_int), ("use_graph", C.c_int),
+                ("autotune", C.c_int)]
 
 
 SYSTEM_BSSN, SYSTEM_Z4C = 0, 1
@@ -219,8 +220,9 @@ SYSTEM_BSSN, SYSTEM_Z4C = 0, 1
 
 def fmr_params(**over):
     """amr = bo with lbo 0, order_timeinterpolation 3, order_RP 4,
-    amr_nbuffer 3, Z4c, coarse steps replayed from a CUDA graph."""
-    p = FmrParams(SYSTEM_Z4C, 0, 3, 4, 3, 1)
+    amr_nbuffer 3, Z4c, coarse steps replayed from a CUDA graph, each
+    level's rhs block shape picked by the autotuner."""
+    p = FmrParams(SYSTEM_Z4C, 0, 3, 4, 3, 1, 1)
     for k, v in over.items():
         setattr(p, k, v)
     return p
@@ -342,6 +344,9 @@ def lib():
         "nrgpu_fmr_restrict_prolong": (C.c_int, [vp, C.c_int, pp, pp, vp]),
         "nrgpu_fmr_advance": (C.c_int, [vp, pp, C.c_int, vp]),
         "nrgpu_fmr_iteration": (C.c_int, [vp, C.c_int]),
+        "nrgpu_fmr_block": (C.c_int, [vp, C.c_int]),
+        "nrgpu_level_autotune": (C.c_int, [vp, C.c_int, vp, vp, C.POINTER(C.c_int)]),
+        "nrgpu_level_block": (C.c_int, [vp, C.c_int]),
         "nrgpu_puncture_coefficients": (C.c_int, [C.c_int, C.c_double, C.c_int, C.POINTER(C.c_double),
                                                   C.POINTER(C.c_double), C.POINTER(C.c_double),
                                                   C.POINTER(C.c_double), vp, vp, vp]),

@@ -59,6 +59,18 @@ class DeviceLevel:
     def empty(self, nv=NV):
         return torch.zeros((nv, self.npoints), dtype=torch.float64, device="cuda")
 
+    def set_block(self, blk_x):
+        """Run the rhs kernels in blocks of blk_x x (128 / blk_x) threads."""
+        abi.check(abi.lib().nrgpu_level_block(self.handle, int(blk_x)))
+
+    def autotune(self, system, params, stream=None):
+        """Time the rhs block shapes for this level and keep the fastest;
+        returns its x extent."""
+        b = C.c_int()
+        abi.check(abi.lib().nrgpu_level_autotune(self.handle, int(system), C.byref(params), _stream(stream),
+                                                 C.byref(b)))
+        return b.value
+
     def nan_flag(self):
         f = C.c_int()
         abi.check(abi.lib().nrgpu_level_nan_flag(self.handle, C.byref(f)))

@@ -479,12 +479,18 @@ __device__ __forceinline__ void bssn_point(const CVarPtrs &U, const PointCtx &P,
 // ---- epilogues ----------------------------------------------------------------
 enum { EPI_RHS = 0, EPI_ADDLINEAR = 1, EPI_RK = 2 };
 
+// EPI_RK accumulator modes: ACC_ADD acc += wacc rhs; ACC_INIT acc = upre +
+// wacc rhs (the first stage, so that the step needs no copy of u); ACC_FINAL
+// out = acc + wacc rhs (the last stage writes u from the accumulator)
+enum { ACC_ADD = 0, ACC_INIT = 1, ACC_FINAL = 2 };
+
 struct Epilogue {
   int mode;
   double c;        // EPI_ADDLINEAR: unew = upre + c rhs
   double wacc;     // EPI_RK: acc += wacc * rhs
   double cv;       // EPI_RK: vout = upre + cv * rhs (when has_v)
   int has_v;
+  int accmode;     // EPI_RK: ACC_ADD / ACC_INIT / ACC_FINAL
 };
 
 __device__ __forceinline__ void det_trace_fix(double n[NRGPU_NV], const nrgpu_bssn_params &p) {
@@ -521,6 +527,16 @@ __device__ __forceinline__ void store(const double r[NRGPU_NV], int x, const Var
     det_trace_fix(n, p);
 #pragma unroll
     for (int v = 0; v < NRGPU_NV; ++v) out.p[v][x] = n[v];
+  } else if (E.accmode == ACC_FINAL) {
+#pragma unroll
+    for (int v = 0; v < NRGPU_NV; ++v) out.p[v][x] = acc.p[v][x] + E.wacc * r[v];
+  } else if (E.accmode == ACC_INIT) {
+#pragma unroll
+    for (int v = 0; v < NRGPU_NV; ++v) {
+      const double u0 = ldg(pre.p[v] + x);
+      acc.p[v][x] = u0 + E.wacc * r[v];
+      if (E.has_v) out.p[v][x] = u0 + E.cv * r[v];
+    }
   } else {
 #pragma unroll
     for (int v = 0; v < NRGPU_NV; ++v) {
@@ -546,10 +562,10 @@ template <int CSY = 0, int CSZ = 0, int MAXO = 6, int MINB = NRGPU_RHS_MINBLOCKS
 __global__ void __launch_bounds__(128, MINB) bssn_rhs_kernel(CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPtrs acc,
                                                       Epilogue E, const nrgpu_bssn_params p, BoxGeo box,
                                                       const int *__restrict__ boundary, double dx, double dy,
-                                                      double dz, int *status) {
+                                                      double dz, int *status, int k0) {
   const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = 1 + blockIdx.z;
+  const int k = k0 + blockIdx.z;
   if (i > box.m - 2 || j > box.n - 2 || k > box.o - 2) return;
   PointCtx P;
   P.i = i; P.j = j; P.k = k;
@@ -608,7 +624,11 @@ __global__ void bssn_flagged_kernel(CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPt
   const FlagPoint fp = pts[t / NRGPU_NV];
   const int ccc = fp.ijk;
   if (fp.flag != NRGPU_PHYBOUND) {
-    if (E.mode == EPI_RK && E.has_v) out.p[v][ccc] = ldg(pre.p[v] + ccc);
+    if (E.mode == EPI_RK) {
+      if (E.accmode == ACC_INIT) acc.p[v][ccc] = ldg(pre.p[v] + ccc);
+      else if (E.accmode == ACC_FINAL) out.p[v][ccc] = acc.p[v][ccc];
+      if (E.has_v) out.p[v][ccc] = ldg(pre.p[v] + ccc);
+    }
     return;
   }
   const BoxGeo b = boxes[fp.box];
@@ -632,16 +652,21 @@ __global__ void bssn_flagged_kernel(CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPt
   rhs += -(Wx * delx * (1.0 / (2.0 * dx)) + Wy * dely * (1.0 / (2.0 * dy)) + Wz * delz * (1.0 / (2.0 * dz)));
   if (E.mode == EPI_RHS) out.p[v][ccc] = rhs;
   else if (E.mode == EPI_ADDLINEAR) out.p[v][ccc] = ldg(pre.p[v] + ccc) + E.c * rhs;
-  else {
+  else if (E.accmode == ACC_FINAL) out.p[v][ccc] = acc.p[v][ccc] + E.wacc * rhs;
+  else if (E.accmode == ACC_INIT) {
+    const double u0 = ldg(pre.p[v] + ccc);
+    acc.p[v][ccc] = u0 + E.wacc * rhs;
+    if (E.has_v) out.p[v][ccc] = u0 + E.cv * rhs;
+  } else {
     acc.p[v][ccc] += E.wacc * rhs;
     if (E.has_v) out.p[v][ccc] = ldg(pre.p[v] + ccc) + E.cv * rhs;
   }
 }
 
-// bssn_algcon (bssn_algcon.c:25-230) on all points
-__global__ void bssn_algcon_kernel(VarPtrs u, int npoints, int subtractA, int normalizedetg) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= npoints) return;
+// bssn_algcon (bssn_algcon.c:25-230) on the points q0 <= q < q1
+__global__ void bssn_algcon_kernel(VarPtrs u, int q0, int q1, int subtractA, int normalizedetg) {
+  const int q = q0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= q1) return;
   double g[6], A[6];
 #pragma unroll
   for (int v = 0; v < 6; ++v) { g[v] = u.p[G11 + v][q]; A[v] = u.p[A11 + v][q]; }
@@ -725,33 +750,39 @@ static CVarPtrs cptrs(const VarPtrs &v) {
 }
 
 // launch the interior and flagged kernels of one rhs evaluation
+// (kb <= k <= ke: the planes of the interior launch, whole boxes by default)
 static int launch_rhs(nrgpu_level *L, const CVarPtrs &U, const VarPtrs &out, const CVarPtrs &pre, const VarPtrs &acc,
-                      const Epilogue &E, const nrgpu_bssn_params &p, cudaStream_t st, bool interior, bool flagged) {
+                      const Epilogue &E, const nrgpu_bssn_params &p, cudaStream_t st, bool interior, bool flagged,
+                      int kb = 1, int ke = 1 << 30) {
   if (interior) {
     for (int b = 0; b < L->nboxes; ++b) {
       const BoxGeo &bx = L->hbox[b];
       if (bx.m < 3 || bx.n < 3 || bx.o < 3) continue;
-      dim3 blk(32, 4, 1);
-      dim3 grd((bx.m - 2 + 31) / 32, (bx.n - 2 + 3) / 4, bx.o - 2);
+      const int k0 = max(kb, 1), k1 = min(ke, bx.o - 2);
+      if (k1 < k0) continue;
+      // the block shape of the level (32 x 4, or what nrgpu_level_autotune
+      // measured fastest for this box); 128 threads, one point each
+      dim3 blk(L->blk_x, 128 / L->blk_x, 1);
+      dim3 grd((bx.m - 2 + blk.x - 1) / blk.x, (bx.n - 2 + blk.y - 1) / blk.y, k1 - k0 + 1);
       // box strides as compile-time constants for the sizes of the standard
       // workloads: every stencil tap becomes one load with an immediate offset
       // and, for runs of order <= 4, kernels without the 6th-order path
       const bool o4 = p.order_centered <= 4;
       if (bx.m == 66 && bx.n == 66 && o4)
         bssn_rhs_kernel<66, 66 * 66, 4><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx,
-                                                              L->dy, L->dz, L->d_status);
+                                                              L->dy, L->dz, L->d_status, k0);
       else if (bx.m == 66 && bx.n == 66)
         bssn_rhs_kernel<66, 66 * 66><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy,
-                                                           L->dz, L->d_status);
+                                                           L->dz, L->d_status, k0);
       else if (bx.m == 162 && bx.n == 162)
         bssn_rhs_kernel<162, 162 * 162><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx,
-                                                              L->dy, L->dz, L->d_status);
+                                                              L->dy, L->dz, L->d_status, k0);
       else if (o4)
         bssn_rhs_kernel<0, 0, 4><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy,
-                                                       L->dz, L->d_status);
+                                                       L->dz, L->d_status, k0);
       else
         bssn_rhs_kernel<<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
-                                             L->d_status);
+                                             L->d_status, k0);
     }
   }
   if (flagged && L->nflagpts > 0) {
@@ -800,7 +831,7 @@ extern "C" int nrgpu_bssn_algcon(nrgpu_level *L, double *const *u, const nrgpu_b
   int e;
   VarPtrs uu;
   if ((e = fill_ptrs(&uu, u, "u"))) return e;
-  bssn_algcon_kernel<<<(L->npoints + 255) / 256, 256, 0, (cudaStream_t)stream>>>(uu, L->npoints, p->subtractA,
+  bssn_algcon_kernel<<<(L->npoints + 255) / 256, 256, 0, (cudaStream_t)stream>>>(uu, 0, L->npoints, p->subtractA,
                                                                                   p->normalizedetg);
   NRGPU_CUDA_TRY(cudaGetLastError());
   return NRGPU_OK;
@@ -1012,7 +1043,7 @@ extern "C" int nrgpu_bssn_rk4_step_noalloc(const nrgpu_box *box, double dx, doub
     bssn_rhs_box_kernel<<<grd, blk, 0, s>>>(ins[st], outs[st], cP, U, Es[st], *p, bx, dx, dy, dz, status);
     bssn_surface_kernel<<<sgrid, 256, 0, s>>>(ins[st], outs[st], cP, U, Es[st], *p, bx, dx, dy, dz);
   }
-  bssn_algcon_kernel<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(U, (int)np, p->subtractA, p->normalizedetg);
+  bssn_algcon_kernel<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(U, 0, (int)np, p->subtractA, p->normalizedetg);
   NRGPU_CUDA_TRY(cudaGetLastError());
   return NRGPU_OK;
 }
@@ -1077,8 +1108,10 @@ static int z4_launch(nrgpu_level *L, const ZCVarPtrs &U, const ZVarPtrs &out, co
     for (int b = 0; b < L->nboxes; ++b) {
       const BoxGeo &bx = L->hbox[b];
       if (bx.m < 3 || bx.n < 3 || bx.o < 3) continue;
-      dim3 blk(32, 4, 1);
-      dim3 grd((bx.m - 2 + 31) / 32, (bx.n - 2 + 3) / 4, bx.o - 2);
+      // the block shape of the level (32 x 4, or what nrgpu_level_autotune
+      // measured fastest for this box); 128 threads, one point each
+      dim3 blk(L->blk_x, 128 / L->blk_x, 1);
+      dim3 grd((bx.m - 2 + blk.x - 1) / blk.x, (bx.n - 2 + blk.y - 1) / blk.y, bx.o - 2);
       if (p.precision == 1) {
         if (bx.m == 162 && bx.n == 162)
           z4_rhs_kernel<162, 162 * 162, 1><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx,
@@ -1174,7 +1207,8 @@ int nrgpu_z4_rk4_stages(nrgpu_level *L, double *const *u, double dt, const nrgpu
 int nrgpu_z4_algcon(nrgpu_level *L, double *const *u, const nrgpu_z4_params *p, cudaStream_t st) {
   VarPtrs gA;
   for (int v = 0; v < NRGPU_NV; ++v) gA.p[v] = u[v];  // g~ 0..5 and A~ 7..12 as in BSSN
-  bssn_algcon_kernel<<<(L->npoints + 255) / 256, 256, 0, st>>>(gA, L->npoints, p->subtractA, p->normalizedetg);
+  bssn_algcon_kernel<<<(L->npoints + 255) / 256, 256, 0, st>>>(gA, 0, L->npoints, p->subtractA,
+                                                                p->normalizedetg);
   NRGPU_CUDA_TRY(cudaGetLastError());
   return NRGPU_OK;
 }
@@ -1184,4 +1218,84 @@ extern "C" int nrgpu_z4_rk4_step(nrgpu_level *L, double *const *u, double dt, co
   int e = nrgpu_z4_rk4_stages(L, u, dt, p, (cudaStream_t)stream);
   if (e) return e;
   return nrgpu_z4_algcon(L, u, p, (cudaStream_t)stream);
+}
+
+// ---- block-shape autotuner (no counterpart in the reference) -------------------
+// The rhs kernels compute one point per thread in 128-thread blocks; which
+// x extent (8 .. 128) runs fastest depends on the box size and the order.
+// The tuner times each shape on a flat state in the level's own scratch
+// (user data untouched), keeps the fastest in the level, and returns it.
+namespace {
+__global__ void flat_state_kernel(double *base, int nv, long np, int alpha) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)nv * np) return;
+  const int v = (int)(t / np);
+  base[t] = (v == 0 || v == 3 || v == 5 || v == 6 || v == alpha) ? 1.0 : 0.0;
+}
+}  // namespace
+
+extern "C" int nrgpu_level_autotune(nrgpu_level *L, int system, const void *params, void *stream, int *best_x) {
+  if (!L || !params || (system != NRGPU_SYSTEM_BSSN && system != NRGPU_SYSTEM_Z4C))
+    return nrgpu_set_error(NRGPU_ERR_ARG, "bad autotune arguments");
+  int e;
+  if (system == NRGPU_SYSTEM_BSSN && (e = check_params((const nrgpu_bssn_params *)params))) return e;
+  if (system == NRGPU_SYSTEM_Z4C && (e = z4_check_params((const nrgpu_z4_params *)params))) return e;
+  double *scr = nullptr;
+  if ((e = nrgpu_level_scratch(L, &scr))) return e;
+  const cudaStream_t st = (cudaStream_t)stream;
+  const long np = L->npoints;
+  const int nv = system == NRGPU_SYSTEM_BSSN ? NRGPU_NV : ZNV;
+  flat_state_kernel<<<(unsigned)((nv * np + 255) / 256), 256, 0, st>>>(scr, nv, np,
+                                                                       system == NRGPU_SYSTEM_BSSN ? 17 : 18);
+  NRGPU_CUDA_TRY(cudaGetLastError());
+  const Epilogue E = {EPI_RHS, 0.0, 0.0, 0.0, 0};
+  cudaEvent_t a, b;
+  NRGPU_CUDA_TRY(cudaEventCreate(&a));
+  NRGPU_CUDA_TRY(cudaEventCreate(&b));
+  const int cand[5] = {32, 64, 16, 128, 8};
+  float best = 1e30f;
+  int bx = 32;
+  for (int c = 0; c < 5 && !e; ++c) {
+    L->blk_x = cand[c];
+    for (int rep = 0; rep < 4 && !e; ++rep) {
+      if (rep == 1) cudaEventRecord(a, st);
+      if (system == NRGPU_SYSTEM_BSSN) {
+        VarPtrs P, O;
+        for (int v = 0; v < NRGPU_NV; ++v) {
+          P.p[v] = scr + (long)v * np;
+          O.p[v] = scr + (long)(ZNV + v) * np;
+        }
+        e = launch_rhs(L, cptrs(P), O, cptrs(P), O, E, *(const nrgpu_bssn_params *)params, st, true, false);
+      } else {
+        ZVarPtrs P, O;
+        for (int v = 0; v < ZNV; ++v) {
+          P.p[v] = scr + (long)v * np;
+          O.p[v] = scr + (long)(ZNV + v) * np;
+        }
+        e = z4_launch(L, z4_c(P), O, z4_c(P), O, E, *(const nrgpu_z4_params *)params, st, true, false);
+      }
+    }
+    cudaEventRecord(b, st);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    if (ms < best) {
+      best = ms;
+      bx = cand[c];
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  L->blk_x = bx;
+  if (best_x) *best_x = bx;
+  if (e) return e;
+  NRGPU_CUDA_TRY(cudaStreamSynchronize(st));
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_level_block(nrgpu_level *L, int blk_x) {
+  if (!L || (blk_x != 8 && blk_x != 16 && blk_x != 32 && blk_x != 64 && blk_x != 128))
+    return nrgpu_set_error(NRGPU_ERR_ARG, "block x extent %d (8, 16, 32, 64 or 128)", blk_x);
+  L->blk_x = blk_x;
+  return NRGPU_OK;
 }

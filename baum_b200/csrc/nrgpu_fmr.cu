@@ -403,6 +403,7 @@ extern "C" int nrgpu_fmr_params_default(nrgpu_fmr_params *p) {
   p->order_RP = 4;
   p->nbuffer = 3;
   p->use_graph = 1;
+  p->autotune = 1;
   return NRGPU_OK;
 }
 
@@ -461,6 +462,11 @@ extern "C" int nrgpu_fmr_create(int nl, const nrgpu_level_desc *levels, const do
     double *scr;
     if ((e = nrgpu_level_scratch(F->L[l], &scr))) break;  // no allocation later, inside a graph capture
     if (l > 0 && (e = setup_pair(F, l))) break;
+    if (p->autotune &&
+        (e = nrgpu_level_autotune(F->L[l], p->system,
+                                  p->system == NRGPU_SYSTEM_BSSN ? (const void *)&F->bp[l] : (const void *)&F->zp[l],
+                                  nullptr, nullptr)))
+      break;
     if (l < nl - 1) {
       const size_t bytes = sizeof(double) * F->nv * (size_t)d.npoints;
       if (cudaMalloc(&F->up[l], bytes) != cudaSuccess || cudaMalloc(&F->upp[l], bytes) != cudaSuccess) {
@@ -504,6 +510,11 @@ extern "C" int nrgpu_fmr_restrict_prolong(nrgpu_fmr *F, int lfine, double *const
   int e;
   if ((e = fill(&C, uc, F->nv)) || (e = fill(&P, uf, F->nv))) return e;
   return restrict_prolong(F, lfine, C, P, (cudaStream_t)stream);
+}
+
+extern "C" int nrgpu_fmr_block(nrgpu_fmr *F, int l) {
+  if (!F || l < 0 || l >= F->nl) return -1;
+  return F->L[l]->blk_x;
 }
 
 extern "C" int nrgpu_fmr_iteration(nrgpu_fmr *F, int l) {

@@ -28,6 +28,8 @@ struct nrgpu_level {
   // points with boundary flag 0, and the norm reduction buffer (first use)
   long ninner;
   double *d_red;
+  // x extent of the rhs kernels' 128-thread blocks (y = 128 / blk_x)
+  int blk_x;
 };
 
 // library-internal pieces shared by the entry points and the mesh-refinement

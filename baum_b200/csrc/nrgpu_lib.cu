@@ -100,6 +100,7 @@ extern "C" int nrgpu_level_create(const nrgpu_level_desc *d, nrgpu_level **out) 
                         d->box[b].z0};
   L->nflagpts = (int)fl.size();
   L->ninner = (long)d->npoints - (long)fl.size();
+  L->blk_x = 32;
   bool ok = cudaMalloc(&L->d_boundary, sizeof(int) * d->npoints) == cudaSuccess &&
             cudaMalloc(&L->d_box, sizeof(BoxGeo) * d->nboxes) == cudaSuccess &&
             cudaMalloc(&L->d_status, sizeof(int) * 4) == cudaSuccess &&

@@ -64,6 +64,10 @@ class Hierarchy:
     def iteration(self, l):
         return abi.lib().nrgpu_fmr_iteration(self.handle, l)
 
+    def block(self, l):
+        """The rhs block x extent level l runs with (8 .. 128, 128 threads)."""
+        return abi.lib().nrgpu_fmr_block(self.handle, l)
+
     def close(self):
         if self.handle:
             abi.lib().nrgpu_fmr_destroy(self.handle)

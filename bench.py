@@ -267,8 +267,11 @@ def gpu_fmr(steps=2):
     out = {"workload": "7 nested 2:1 levels, Z4c 4th order + KO6, Berger-Oliger, order_RP 4, nbuffer 3, "
                        "box points per side %s, dx0 %.3g, Fourier data 1e-3" % (FMR_SIZES, FMR_DX0),
            "rhs_point_updates_per_coarse_step": upd_per_coarse}
-    for use_graph in (1, 0):
-        H = fmr.Hierarchy(levels, dt, params, abi.fmr_params(use_graph=use_graph))
+    # the product configuration (graph + per-level tuned block shapes), then
+    # plain launches, then the graph with every level at the 32 x 4 default
+    for key, use_graph, tune in (("graph", 1, 1), ("launches", 0, 1), ("graph_untuned_32x4", 1, 0)):
+        H = fmr.Hierarchy(levels, dt, params, abi.fmr_params(use_graph=use_graph, autotune=tune))
+        blocks = [H.block(l) for l in range(len(levels))]
         u = [state(lev) for lev in levels]
         H.advance(u, 1)   # first coarse step: 2nd-order time interpolation, no graph
         H.advance(u, 1)   # graph capture (with use_graph)
@@ -279,8 +282,7 @@ def gpu_fmr(steps=2):
         b.record()
         torch.cuda.synchronize()
         ms = a.elapsed_time(b) / steps
-        key = "graph" if use_graph else "launches"
-        out[key] = {"ms_per_coarse_step": ms, "value": upd_per_coarse / (ms * 1e-3)}
+        out[key] = {"ms_per_coarse_step": ms, "value": upd_per_coarse / (ms * 1e-3), "block_x": blocks}
         finite = all(bool(torch.isfinite(t).all()) for t in u)
         out[key]["finite"] = finite
         H.close()

@@ -275,8 +275,6 @@ int nrgpu_puncture_coefficients(int m, double dx, int npunc, const double *mass,
  * 371-380) and restrict_prolong_evolve (main/amr/inject.c:116-132) through
  * restrict_boxtobox_N / prolong_boxtobox_N
  * (utility/interpolate/interpolate_boxtobox_N.c:585-1223). */
-enum { NRGPU_SYSTEM_BSSN = 0, NRGPU_SYSTEM_Z4C = 1 };
-
 typedef struct {
   int system;                   /* NRGPU_SYSTEM_BSSN or NRGPU_SYSTEM_Z4C */
   int lbo;                      /* levels l >= lbo subcycle (regrid.c:51-78) */
@@ -285,6 +283,8 @@ typedef struct {
   int nbuffer;                  /* amr_nbuffer (bam_amr.c) */
   int use_graph;                /* capture the coarse steps after the first
                                    in a CUDA graph and replay it */
+  int autotune;                 /* pick each level's rhs block shape with
+                                   nrgpu_level_autotune at creation */
 } nrgpu_fmr_params;
 
 typedef struct nrgpu_fmr nrgpu_fmr;
@@ -308,6 +308,22 @@ int nrgpu_fmr_restrict_prolong(nrgpu_fmr *fmr, int lfine, double *const *uc, dou
 int nrgpu_fmr_advance(nrgpu_fmr *fmr, double *const *u, int nsteps, void *stream);
 /* level iterations done so far (tL.iteration) */
 int nrgpu_fmr_iteration(nrgpu_fmr *fmr, int l);
+/* the rhs block x extent level l runs with */
+int nrgpu_fmr_block(nrgpu_fmr *fmr, int l);
+
+/* the evolution systems */
+enum { NRGPU_SYSTEM_BSSN = 0, NRGPU_SYSTEM_Z4C = 1 };
+
+/* ---- launch-shape autotuner (no counterpart in the reference) -------------
+ * The rhs kernels compute one point per thread in blocks of 128 threads.
+ * nrgpu_level_autotune times the x extents 8, 16, 32, 64, 128 for the
+ * level's boxes and the given system (NRGPU_SYSTEM_BSSN / _Z4C, below) and
+ * parameters on a flat state in the level's RK4 scratch (the user's arrays
+ * are not touched), keeps the fastest for the level and returns it in
+ * *best_x (may be NULL).  Waits for the stream.  nrgpu_level_block sets the
+ * extent directly (default 32).  Results do not depend on the shape. */
+int nrgpu_level_autotune(nrgpu_level *L, int system, const void *params, void *stream, int *best_x);
+int nrgpu_level_block(nrgpu_level *L, int blk_x);
 
 /* ---- ADM diagnostics ------------------------------------------------------
  * ADM metric and extrinsic curvature from the conformal variables:
