@@ -344,9 +344,10 @@ def lib():
         "nrgpu_fmr_restrict_prolong": (C.c_int, [vp, C.c_int, pp, pp, vp]),
         "nrgpu_fmr_advance": (C.c_int, [vp, pp, C.c_int, vp]),
         "nrgpu_fmr_iteration": (C.c_int, [vp, C.c_int]),
-        "nrgpu_fmr_block": (C.c_int, [vp, C.c_int]),
+        "nrgpu_fmr_block": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int)]),
         "nrgpu_level_autotune": (C.c_int, [vp, C.c_int, vp, vp, C.POINTER(C.c_int)]),
-        "nrgpu_level_block": (C.c_int, [vp, C.c_int]),
+        "nrgpu_level_block": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
+        "nrgpu_level_get_block": (C.c_int, [vp, C.POINTER(C.c_int)]),
         "nrgpu_puncture_coefficients": (C.c_int, [C.c_int, C.c_double, C.c_int, C.POINTER(C.c_double),
                                                   C.POINTER(C.c_double), C.POINTER(C.c_double),
                                                   C.POINTER(C.c_double), vp, vp, vp]),

@@ -48,6 +48,7 @@ typedef struct {
   double *d_state;  /* [NV][npoints] resident state (resident mode) */
   double *d_a, *d_b, *d_c;
   int uploaded;
+  int tuned;        /* rhs block shape picked by nrgpu_level_autotune */
 } nrgpu_slot;
 
 static nrgpu_slot slots[64];
@@ -168,6 +169,7 @@ static nrgpu_slot *slot_of(tL *level)
     s->bamlevel = level;
     s->npoints = level->npoints;
     s->uploaded = 0;
+    s->tuned = 0;
     if (cudaMalloc((void **)&s->d_state, sizeof(double) * ZNV * level->npoints) ||
         cudaMalloc((void **)&s->d_a, sizeof(double) * ZNV * level->npoints) ||
         cudaMalloc((void **)&s->d_b, sizeof(double) * ZNV * level->npoints) ||
@@ -256,10 +258,14 @@ int nrgpu_evolve_resident(tL *level)
   if (nrgpu_system_z4) {
     nrgpu_z4_params p;
     read_params_z4(level, u, &p);
+    if (!s->tuned) check(nrgpu_level_autotune(s->lev, NRGPU_SYSTEM_Z4C, &p, 0, 0), "autotune");
+    s->tuned = 1;
     check(nrgpu_z4_rk4_step(s->lev, st, level->dt, &p, 0), "rk4");
   } else {
     nrgpu_bssn_params p;
     read_params(level, u, &p);
+    if (!s->tuned) check(nrgpu_level_autotune(s->lev, NRGPU_SYSTEM_BSSN, &p, 0, 0), "autotune");
+    s->tuned = 1;
     check(nrgpu_bssn_rk4_step(s->lev, st, level->dt, &p, 0), "rk4");
   }
   copy_vl(level, u, s->d_state, 0);

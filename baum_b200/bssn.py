@@ -59,17 +59,21 @@ class DeviceLevel:
     def empty(self, nv=NV):
         return torch.zeros((nv, self.npoints), dtype=torch.float64, device="cuda")
 
-    def set_block(self, blk_x):
-        """Run the rhs kernels in blocks of blk_x x (128 / blk_x) threads."""
-        abi.check(abi.lib().nrgpu_level_block(self.handle, int(blk_x)))
+    def set_block(self, bx, by, bz=1):
+        """Run the rhs kernels in blocks of bx x by x bz = 128 threads."""
+        abi.check(abi.lib().nrgpu_level_block(self.handle, int(bx), int(by), int(bz)))
+
+    def block(self):
+        b = (C.c_int * 3)()
+        abi.check(abi.lib().nrgpu_level_get_block(self.handle, b))
+        return tuple(b)
 
     def autotune(self, system, params, stream=None):
         """Time the rhs block shapes for this level and keep the fastest;
-        returns its x extent."""
-        b = C.c_int()
-        abi.check(abi.lib().nrgpu_level_autotune(self.handle, int(system), C.byref(params), _stream(stream),
-                                                 C.byref(b)))
-        return b.value
+        returns it as (x, y, z)."""
+        b = (C.c_int * 3)()
+        abi.check(abi.lib().nrgpu_level_autotune(self.handle, int(system), C.byref(params), _stream(stream), b))
+        return tuple(b)
 
     def nan_flag(self):
         f = C.c_int()
@@ -107,14 +111,21 @@ def evolve_rk_rk4(dl, u, dt, params, stream=None):
 
 
 def evolve_host(dl, host_u, nsteps, dt, params):
-    """nsteps RK4 steps of a host state (numpy or CPU tensor (24, npoints)),
-    uploaded and downloaded inside the call (nrgpu_bssn_evolve_host)."""
+    """nsteps RK4 steps of a host state (numpy or CPU tensor (24, npoints),
+    or a list of 24 contiguous float64 numpy arrays, one per variable, as
+    BAM keeps them), uploaded and downloaded inside the call
+    (nrgpu_bssn_evolve_host)."""
     import numpy as np
-    if isinstance(host_u, torch.Tensor):
-        base, step = host_u.data_ptr(), host_u.stride(0) * 8
+    if isinstance(host_u, (list, tuple)):
+        if len(host_u) != NV or not all(a.dtype == np.float64 and a.flags.c_contiguous for a in host_u):
+            raise ValueError("24 contiguous float64 arrays")
+        ptrs = abi.ptr_array([a.ctypes.data for a in host_u])
     else:
-        assert host_u.dtype == np.float64 and host_u.flags.c_contiguous
-        base, step = host_u.ctypes.data, host_u.strides[0]
-    ptrs = abi.ptr_array([base + i * step for i in range(NV)])
+        if isinstance(host_u, torch.Tensor):
+            base, step = host_u.data_ptr(), host_u.stride(0) * 8
+        else:
+            assert host_u.dtype == np.float64 and host_u.flags.c_contiguous
+            base, step = host_u.ctypes.data, host_u.strides[0]
+        ptrs = abi.ptr_array([base + i * step for i in range(NV)])
     abi.check(abi.lib().nrgpu_bssn_evolve_host(dl.handle, ptrs, int(nsteps), float(dt), C.byref(params)))
     return host_u

@@ -562,11 +562,11 @@ template <int CSY = 0, int CSZ = 0, int MAXO = 6, int MINB = NRGPU_RHS_MINBLOCKS
 __global__ void __launch_bounds__(128, MINB) bssn_rhs_kernel(CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPtrs acc,
                                                       Epilogue E, const nrgpu_bssn_params p, BoxGeo box,
                                                       const int *__restrict__ boundary, double dx, double dy,
-                                                      double dz, int *status, int k0) {
+                                                      double dz, int *status, int k0, int k1) {
   const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = k0 + blockIdx.z;
-  if (i > box.m - 2 || j > box.n - 2 || k > box.o - 2) return;
+  const int k = k0 + blockIdx.z * blockDim.z + threadIdx.z;
+  if (i > box.m - 2 || j > box.n - 2 || k > k1) return;
   PointCtx P;
   P.i = i; P.j = j; P.k = k;
   P.imax = box.m - 1; P.jmax = box.n - 1; P.kmax = box.o - 1;
@@ -760,29 +760,29 @@ static int launch_rhs(nrgpu_level *L, const CVarPtrs &U, const VarPtrs &out, con
       if (bx.m < 3 || bx.n < 3 || bx.o < 3) continue;
       const int k0 = max(kb, 1), k1 = min(ke, bx.o - 2);
       if (k1 < k0) continue;
-      // the block shape of the level (32 x 4, or what nrgpu_level_autotune
+      // the block shape of the level (32 x 4 x 1, or what nrgpu_level_autotune
       // measured fastest for this box); 128 threads, one point each
-      dim3 blk(L->blk_x, 128 / L->blk_x, 1);
-      dim3 grd((bx.m - 2 + blk.x - 1) / blk.x, (bx.n - 2 + blk.y - 1) / blk.y, k1 - k0 + 1);
+      const dim3 blk(L->blk[0], L->blk[1], L->blk[2]);
+      const dim3 grd((bx.m - 2 + blk.x - 1) / blk.x, (bx.n - 2 + blk.y - 1) / blk.y, (k1 - k0 + blk.z) / blk.z);
       // box strides as compile-time constants for the sizes of the standard
       // workloads: every stencil tap becomes one load with an immediate offset
       // and, for runs of order <= 4, kernels without the 6th-order path
       const bool o4 = p.order_centered <= 4;
       if (bx.m == 66 && bx.n == 66 && o4)
         bssn_rhs_kernel<66, 66 * 66, 4><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx,
-                                                              L->dy, L->dz, L->d_status, k0);
+                                                              L->dy, L->dz, L->d_status, k0, k1);
       else if (bx.m == 66 && bx.n == 66)
         bssn_rhs_kernel<66, 66 * 66><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy,
-                                                           L->dz, L->d_status, k0);
+                                                           L->dz, L->d_status, k0, k1);
       else if (bx.m == 162 && bx.n == 162)
         bssn_rhs_kernel<162, 162 * 162><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx,
-                                                              L->dy, L->dz, L->d_status, k0);
+                                                              L->dy, L->dz, L->d_status, k0, k1);
       else if (o4)
         bssn_rhs_kernel<0, 0, 4><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy,
-                                                       L->dz, L->d_status, k0);
+                                                       L->dz, L->d_status, k0, k1);
       else
         bssn_rhs_kernel<<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
-                                             L->d_status, k0);
+                                             L->d_status, k0, k1);
     }
   }
   if (flagged && L->nflagpts > 0) {
@@ -861,6 +861,51 @@ extern "C" int nrgpu_vladd(nrgpu_level *L, int nvars, double *const *r, double a
 
 int nrgpu_level_scratch(nrgpu_level *L, double **out);
 
+// The RK4 step of rk.c:220-257 without a copy of u: u itself is the stage
+// input of stage 1 and the "P" of every stage (only read until stage 4);
+// stage 1 initialises the accumulator A = u + dt/6 r1, stages 2-3 add to it,
+// and stage 4 writes u = A + dt/6 r4.  Per point the floating-point
+// operations are those of P + c r and u += w r in the reference's order.
+struct RkLists {
+  VarPtrs U, A, V1, V2;
+};
+
+static RkLists rk_lists(const VarPtrs &U, double *scr, long np) {
+  RkLists R;
+  R.U = U;
+  for (int v = 0; v < NRGPU_NV; ++v) {
+    R.A.p[v] = scr + (0 * NRGPU_NV + v) * np;
+    R.V1.p[v] = scr + (1 * NRGPU_NV + v) * np;
+    R.V2.p[v] = scr + (2 * NRGPU_NV + v) * np;
+  }
+  return R;
+}
+
+// stage sg (0..3) of the step, on the planes kb..ke of the interior and/or
+// the flagged points
+static int rk_stage(nrgpu_level *L, const RkLists &R, int sg, double dt, const nrgpu_bssn_params &p,
+                    cudaStream_t st, bool interior, bool flagged, int kb = 1, int ke = 1 << 30) {
+  const CVarPtrs cU = cptrs(R.U);
+  switch (sg) {
+    case 0: {
+      const Epilogue E = {EPI_RK, 0.0, dt / 6, dt / 2, 1, ACC_INIT};
+      return launch_rhs(L, cU, R.V1, cU, R.A, E, p, st, interior, flagged, kb, ke);
+    }
+    case 1: {
+      const Epilogue E = {EPI_RK, 0.0, dt / 3, dt / 2, 1, ACC_ADD};
+      return launch_rhs(L, cptrs(R.V1), R.V2, cU, R.A, E, p, st, interior, flagged, kb, ke);
+    }
+    case 2: {
+      const Epilogue E = {EPI_RK, 0.0, dt / 3, dt, 1, ACC_ADD};
+      return launch_rhs(L, cptrs(R.V2), R.V1, cU, R.A, E, p, st, interior, flagged, kb, ke);
+    }
+    default: {
+      const Epilogue E = {EPI_RK, 0.0, dt / 6, 0.0, 0, ACC_FINAL};
+      return launch_rhs(L, cptrs(R.V1), R.U, cU, R.A, E, p, st, interior, flagged, kb, ke);
+    }
+  }
+}
+
 // fused RK4 (rk.c:220-257): stage s reads V_in, adds w_s*r to u and writes
 // V_out = P + c_s*r; both the interior and the flagged kernels do it
 // the four RK4 stages of evolve_rk_rk4 (rk.c:220-257) without the algebraic
@@ -874,24 +919,9 @@ int nrgpu_bssn_rk4_stages(nrgpu_level *L, double *const *u, double dt, const nrg
   if ((e = fill_ptrs(&U, u, "u"))) return e;
   double *scr = nullptr;
   if ((e = nrgpu_level_scratch(L, &scr))) return e;
-  VarPtrs P, V1, V2;
-  const size_t np = (size_t)L->npoints;
-  for (int v = 0; v < NRGPU_NV; ++v) {
-    P.p[v] = scr + (0 * NRGPU_NV + v) * np;
-    V1.p[v] = scr + (1 * NRGPU_NV + v) * np;
-    V2.p[v] = scr + (2 * NRGPU_NV + v) * np;
-  }
-  const long n = (long)NRGPU_NV * L->npoints;
-  vlcopy_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(P, cptrs(U), L->npoints);
-  const CVarPtrs cP = cptrs(P);
-  Epilogue E1 = {EPI_RK, 0.0, dt / 6, dt / 2, 1};
-  Epilogue E2 = {EPI_RK, 0.0, dt / 3, dt / 2, 1};
-  Epilogue E3 = {EPI_RK, 0.0, dt / 3, dt, 1};
-  Epilogue E4 = {EPI_RK, 0.0, dt / 6, 0.0, 0};
-  if ((e = launch_rhs(L, cP, V1, cP, U, E1, *p, st, true, true))) return e;
-  if ((e = launch_rhs(L, cptrs(V1), V2, cP, U, E2, *p, st, true, true))) return e;
-  if ((e = launch_rhs(L, cptrs(V2), V1, cP, U, E3, *p, st, true, true))) return e;
-  if ((e = launch_rhs(L, cptrs(V1), V2, cP, U, E4, *p, st, true, true))) return e;
+  RkLists R = rk_lists(U, scr, L->npoints);
+  for (int sg = 0; sg < 4; ++sg)
+    if ((e = rk_stage(L, R, sg, dt, *p, st, true, true))) return e;
   return NRGPU_OK;
 }
 
@@ -900,6 +930,152 @@ extern "C" int nrgpu_bssn_rk4_step(nrgpu_level *L, double *const *u, double dt, 
   int e = nrgpu_bssn_rk4_stages(L, u, dt, p, (cudaStream_t)stream);
   if (e) return e;
   return nrgpu_bssn_algcon(L, u, p, stream);
+}
+
+// ---- steps on host buffers ------------------------------------------------------
+// The state crosses PCIe once up before the first step and once down after
+// the last.  On a single-box level the box is cut into NRGPU_HOST_SLABS z
+// slabs: stage 1 of the first step runs on the planes of a slab as soon as
+// the uploads cover its stencils (H planes past it), so the upload of the
+// later slabs overlaps it; stage 4 of the last step, and the algebraic
+// constraints, run slab by slab after the flagged points, and each slab's
+// download overlaps the work on the slabs after it.  The per-point
+// arithmetic is that of nrgpu_bssn_rk4_step.
+static int host_streams(nrgpu_level *L) {
+  if (L->hs_comp) return NRGPU_OK;
+  // blocking streams: ordered after earlier work on the legacy default stream
+  NRGPU_CUDA_TRY(cudaStreamCreate(&L->hs_copy));
+  NRGPU_CUDA_TRY(cudaStreamCreate(&L->hs_comp));
+  for (int q = 0; q < NRGPU_HOST_SLABS; ++q) {
+    NRGPU_CUDA_TRY(cudaEventCreateWithFlags(&L->hev_in[q], cudaEventDisableTiming));
+    NRGPU_CUDA_TRY(cudaEventCreateWithFlags(&L->hev_out[q], cudaEventDisableTiming));
+  }
+  return NRGPU_OK;
+}
+
+// planes [off, off + n) of the 24 variables between the device state (pitch
+// np) and the host arrays: one 2D copy when the host arrays lie at one
+// pitch (hpitch > 0 bytes: a (24, np) array or rows of a larger one), else
+// one copy per variable (each cudaMemcpyAsync costs a few microseconds, so
+// the slabs are only used with the 2D form)
+static int copy_planes(double *dev, double *const *host, long hpitch, long np, long off, long n, bool up,
+                       cudaStream_t st) {
+  const cudaMemcpyKind kind = up ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+  if (hpitch > 0) {
+    double *h0 = host[0] + off, *d0 = dev + off;
+    if (cudaMemcpy2DAsync(up ? (void *)d0 : (void *)h0, up ? np * sizeof(double) : (size_t)hpitch,
+                          up ? (const void *)h0 : (const void *)d0, up ? (size_t)hpitch : np * sizeof(double),
+                          n * sizeof(double), NRGPU_NV, kind, st) != cudaSuccess)
+      return nrgpu_set_error(NRGPU_ERR_CUDA, "%s of planes", up ? "upload" : "download");
+    return NRGPU_OK;
+  }
+  for (int v = 0; v < NRGPU_NV; ++v) {
+    double *h = host[v] + off, *d = dev + v * np + off;
+    if (cudaMemcpyAsync(up ? (void *)d : (void *)h, up ? (const void *)h : (const void *)d, sizeof(double) * n, kind,
+                        st) != cudaSuccess)
+      return nrgpu_set_error(NRGPU_ERR_CUDA, "%s of variable %d", up ? "upload" : "download", v);
+  }
+  return NRGPU_OK;
+}
+
+// the common pitch in bytes of the host arrays, or 0
+static long host_pitch(double *const *host, long np) {
+  const long pb = (long)((const char *)host[1] - (const char *)host[0]);
+  if (pb < np * (long)sizeof(double) || pb >= (1L << 31) || pb % sizeof(double)) return 0;
+  for (int v = 2; v < NRGPU_NV; ++v)
+    if ((const char *)host[v] - (const char *)host[0] != pb * v) return 0;
+  return pb;
+}
+
+extern "C" int nrgpu_bssn_evolve_host(nrgpu_level *L, double *const *host_u, int nsteps, double dt,
+                                      const nrgpu_bssn_params *p) {
+  if (!L || !host_u || nsteps < 0) return nrgpu_set_error(NRGPU_ERR_ARG, "bad arguments");
+  int e;
+  if ((e = check_params(p))) return e;
+  for (int v = 0; v < NRGPU_NV; ++v)
+    if (!host_u[v]) return nrgpu_set_error(NRGPU_ERR_ARG, "null host_u[%d]", v);
+  const long np = L->npoints;
+  if (!L->hoststate && cudaMalloc(&L->hoststate, sizeof(double) * NRGPU_NV * np) != cudaSuccess) {
+    L->hoststate = nullptr;
+    cudaGetLastError();
+    return nrgpu_set_error(NRGPU_ERR_NOMEM, "state of %ld points", np);
+  }
+  double *scr = nullptr;
+  if ((e = nrgpu_level_scratch(L, &scr))) return e;
+  if ((e = host_streams(L))) return e;
+  const cudaStream_t cs = L->hs_copy, ks = L->hs_comp;
+  double *u[NRGPU_NV];
+  VarPtrs U;
+  for (int v = 0; v < NRGPU_NV; ++v) U.p[v] = u[v] = L->hoststate + v * np;
+  const RkLists R = rk_lists(U, scr, np);
+
+  // slabs of ps planes; H = the stencils' reach in planes
+  const BoxGeo &b0 = L->hbox[0];
+  const long hp = host_pitch(host_u, np);
+  const bool pipe = L->nboxes == 1 && b0.o >= 2 * NRGPU_HOST_SLABS && nsteps > 0 && hp > 0;
+  const int ps = pipe ? (b0.o + NRGPU_HOST_SLABS - 1) / NRGPU_HOST_SLABS : b0.o;
+  const int ns = pipe ? (b0.o + ps - 1) / ps : 1;
+  const long mn = pipe ? (long)b0.m * b0.n : 0;
+  const int H = max(max(p->order_advection, p->order_centered / 2 + 1), p->order_dissipation / 2 + 1);
+
+  // upload (whole state when not pipelined)
+  for (int q = 0; q < ns && !e; ++q) {
+    const long off = pipe ? q * ps * mn : 0, n = pipe ? min(ps, b0.o - q * ps) * mn : np;
+    if (!(e = copy_planes(L->hoststate, host_u, hp, np, off, n, true, cs)))
+      if (cudaEventRecord(L->hev_in[q], cs) != cudaSuccess) e = nrgpu_set_error(NRGPU_ERR_CUDA, "event");
+  }
+  if (!e && nsteps == 0) e = copy_planes(L->hoststate, host_u, hp, np, 0, np, false, cs);
+
+  int waited = -1;  // last upload slab the compute stream has waited for
+  for (int t = 0; t < nsteps && !e; ++t) {
+    const bool first = t == 0, last = t == nsteps - 1;
+    // stage 1
+    if (first && pipe) {
+      for (int q = 0; q < ns && !e; ++q) {
+        const int kb = q * ps, ke = min(b0.o, kb + ps) - 1;
+        const int need = min(ns - 1, min(b0.o - 1, ke + H) / ps);
+        for (; waited < need; ++waited) cudaStreamWaitEvent(ks, L->hev_in[waited + 1], 0);
+        e = rk_stage(L, R, 0, dt, *p, ks, true, false, kb, ke);
+      }
+      for (; waited < ns - 1; ++waited) cudaStreamWaitEvent(ks, L->hev_in[waited + 1], 0);
+      if (!e) e = rk_stage(L, R, 0, dt, *p, ks, false, true);
+    } else {
+      if (first) cudaStreamWaitEvent(ks, L->hev_in[0], 0);
+      e = rk_stage(L, R, 0, dt, *p, ks, true, true);
+    }
+    for (int sg = 1; sg < 3 && !e; ++sg) e = rk_stage(L, R, sg, dt, *p, ks, true, true);
+    if (e) break;
+    // stage 4 and the algebraic constraints; the download
+    if (last && pipe) {
+      e = rk_stage(L, R, 3, dt, *p, ks, false, true);
+      for (int q = 0; q < ns && !e; ++q) {
+        const int kb = q * ps, ke = min(b0.o, kb + ps) - 1;
+        if ((e = rk_stage(L, R, 3, dt, *p, ks, true, false, kb, ke))) break;
+        const int q0 = (int)(kb * mn), q1 = (int)((ke + 1) * mn);
+        bssn_algcon_kernel<<<(unsigned)((q1 - q0 + 255) / 256), 256, 0, ks>>>(U, q0, q1, p->subtractA,
+                                                                              p->normalizedetg);
+        if (cudaEventRecord(L->hev_out[q], ks) != cudaSuccess || cudaStreamWaitEvent(cs, L->hev_out[q], 0))
+          e = nrgpu_set_error(NRGPU_ERR_CUDA, "event");
+        else
+          e = copy_planes(L->hoststate, host_u, hp, np, kb * mn, (ke + 1 - kb) * mn, false, cs);
+      }
+    } else {
+      if (!(e = rk_stage(L, R, 3, dt, *p, ks, true, true))) {
+        bssn_algcon_kernel<<<(unsigned)((np + 255) / 256), 256, 0, ks>>>(U, 0, (int)np, p->subtractA,
+                                                                        p->normalizedetg);
+        if (last) {
+          if (cudaEventRecord(L->hev_out[0], ks) != cudaSuccess || cudaStreamWaitEvent(cs, L->hev_out[0], 0))
+            e = nrgpu_set_error(NRGPU_ERR_CUDA, "event");
+          else
+            e = copy_planes(L->hoststate, host_u, hp, np, 0, np, false, cs);
+        }
+      }
+    }
+  }
+  const cudaError_t c1 = cudaStreamSynchronize(ks), c2 = cudaStreamSynchronize(cs);
+  if (!e && (c1 != cudaSuccess || c2 != cudaSuccess || cudaGetLastError() != cudaSuccess))
+    e = nrgpu_set_error(NRGPU_ERR_CUDA, "host-buffer step: %s", cudaGetErrorString(c1 != cudaSuccess ? c1 : c2));
+  return e;
 }
 
 // ---- allocation-free RK4 step -------------------------------------------------
@@ -1091,14 +1267,14 @@ static void z4_interior_fp64(const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVa
 #define NRGPU_Z4_FIXED(M_)                                                                                   \
   if (bx.m == M_ && bx.n == M_) {                                                                           \
     z4_rhs_kernel<M_, M_ * M_, 0, MAXO><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, \
-                                                             L->dy, L->dz, L->d_status);                    \
+                                                             L->dy, L->dz, L->d_status, 1, bx.o - 2);                    \
     return;                                                                                                  \
   }
   NRGPU_Z4_FIXED(162) NRGPU_Z4_FIXED(168) NRGPU_Z4_FIXED(136) NRGPU_Z4_FIXED(104) NRGPU_Z4_FIXED(72)
   NRGPU_Z4_FIXED(66)
 #undef NRGPU_Z4_FIXED
   z4_rhs_kernel<0, 0, 0, MAXO><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
-                                                    L->d_status);
+                                                    L->d_status, 1, bx.o - 2);
 }
 
 static int z4_launch(nrgpu_level *L, const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVarPtrs &pre,
@@ -1108,24 +1284,24 @@ static int z4_launch(nrgpu_level *L, const ZCVarPtrs &U, const ZVarPtrs &out, co
     for (int b = 0; b < L->nboxes; ++b) {
       const BoxGeo &bx = L->hbox[b];
       if (bx.m < 3 || bx.n < 3 || bx.o < 3) continue;
-      // the block shape of the level (32 x 4, or what nrgpu_level_autotune
+      // the block shape of the level (32 x 4 x 1, or what nrgpu_level_autotune
       // measured fastest for this box); 128 threads, one point each
-      dim3 blk(L->blk_x, 128 / L->blk_x, 1);
-      dim3 grd((bx.m - 2 + blk.x - 1) / blk.x, (bx.n - 2 + blk.y - 1) / blk.y, bx.o - 2);
+      const dim3 blk(L->blk[0], L->blk[1], L->blk[2]);
+      const dim3 grd((bx.m - 2 + blk.x - 1) / blk.x, (bx.n - 2 + blk.y - 1) / blk.y, (bx.o - 2 + blk.z - 1) / blk.z);
       if (p.precision == 1) {
         if (bx.m == 162 && bx.n == 162)
           z4_rhs_kernel<162, 162 * 162, 1><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx,
-                                                                 L->dy, L->dz, L->d_status);
+                                                                 L->dy, L->dz, L->d_status, 1, bx.o - 2);
         else
           z4_rhs_kernel<0, 0, 1><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
-                                                       L->d_status);
+                                                       L->d_status, 1, bx.o - 2);
       } else if (p.precision == 2) {
         if (bx.m == 162 && bx.n == 162)
           z4_rhs_kernel<162, 162 * 162, 2><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx,
-                                                                 L->dy, L->dz, L->d_status);
+                                                                 L->dy, L->dz, L->d_status, 1, bx.o - 2);
         else
           z4_rhs_kernel<0, 0, 2><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
-                                                       L->d_status);
+                                                       L->d_status, 1, bx.o - 2);
       } else if (p.order_centered <= 4) {
         z4_interior_fp64<4>(U, out, pre, acc, E, p, bx, L, grd, blk, st);
       } else {
@@ -1234,7 +1410,7 @@ __global__ void flat_state_kernel(double *base, int nv, long np, int alpha) {
 }
 }  // namespace
 
-extern "C" int nrgpu_level_autotune(nrgpu_level *L, int system, const void *params, void *stream, int *best_x) {
+extern "C" int nrgpu_level_autotune(nrgpu_level *L, int system, const void *params, void *stream, int *best_block) {
   if (!L || !params || (system != NRGPU_SYSTEM_BSSN && system != NRGPU_SYSTEM_Z4C))
     return nrgpu_set_error(NRGPU_ERR_ARG, "bad autotune arguments");
   int e;
@@ -1252,11 +1428,15 @@ extern "C" int nrgpu_level_autotune(nrgpu_level *L, int system, const void *para
   cudaEvent_t a, b;
   NRGPU_CUDA_TRY(cudaEventCreate(&a));
   NRGPU_CUDA_TRY(cudaEventCreate(&b));
-  const int cand[5] = {32, 64, 16, 128, 8};
+  // 128-thread shapes: flat (x, y) and with a z extent (a smaller stencil
+  // footprint per block, so more of each variable's taps hit in L1)
+  static const int cand[][3] = {{32, 4, 1}, {64, 2, 1}, {16, 8, 1}, {8, 16, 1}, {128, 1, 1}, {16, 4, 2},
+                                {8, 8, 2},  {32, 2, 2}, {8, 4, 4},  {4, 8, 4}, {16, 2, 4},  {4, 4, 8}};
+  const int ncand = (int)(sizeof cand / sizeof cand[0]);
   float best = 1e30f;
-  int bx = 32;
-  for (int c = 0; c < 5 && !e; ++c) {
-    L->blk_x = cand[c];
+  int bb = 0;
+  for (int c = 0; c < ncand && !e; ++c) {
+    for (int a = 0; a < 3; ++a) L->blk[a] = cand[c][a];
     for (int rep = 0; rep < 4 && !e; ++rep) {
       if (rep == 1) cudaEventRecord(a, st);
       if (system == NRGPU_SYSTEM_BSSN) {
@@ -1281,21 +1461,30 @@ extern "C" int nrgpu_level_autotune(nrgpu_level *L, int system, const void *para
     cudaEventElapsedTime(&ms, a, b);
     if (ms < best) {
       best = ms;
-      bx = cand[c];
+      bb = c;
     }
   }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
-  L->blk_x = bx;
-  if (best_x) *best_x = bx;
+  for (int q = 0; q < 3; ++q) {
+    L->blk[q] = cand[bb][q];
+    if (best_block) best_block[q] = cand[bb][q];
+  }
   if (e) return e;
   NRGPU_CUDA_TRY(cudaStreamSynchronize(st));
   return NRGPU_OK;
 }
 
-extern "C" int nrgpu_level_block(nrgpu_level *L, int blk_x) {
-  if (!L || (blk_x != 8 && blk_x != 16 && blk_x != 32 && blk_x != 64 && blk_x != 128))
-    return nrgpu_set_error(NRGPU_ERR_ARG, "block x extent %d (8, 16, 32, 64 or 128)", blk_x);
-  L->blk_x = blk_x;
+extern "C" int nrgpu_level_block(nrgpu_level *L, int bx, int by, int bz) {
+  auto pow2 = [](int v) { return v >= 1 && v <= 128 && (v & (v - 1)) == 0; };
+  if (!L || !pow2(bx) || !pow2(by) || !pow2(bz) || bx * by * bz != 128)
+    return nrgpu_set_error(NRGPU_ERR_ARG, "block %d x %d x %d (powers of two, 128 threads)", bx, by, bz);
+  L->blk[0] = bx; L->blk[1] = by; L->blk[2] = bz;
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_level_get_block(nrgpu_level *L, int *block) {
+  if (!L || !block) return nrgpu_set_error(NRGPU_ERR_ARG, "null argument");
+  for (int q = 0; q < 3; ++q) block[q] = L->blk[q];
   return NRGPU_OK;
 }

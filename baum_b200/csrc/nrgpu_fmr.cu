@@ -512,9 +512,9 @@ extern "C" int nrgpu_fmr_restrict_prolong(nrgpu_fmr *F, int lfine, double *const
   return restrict_prolong(F, lfine, C, P, (cudaStream_t)stream);
 }
 
-extern "C" int nrgpu_fmr_block(nrgpu_fmr *F, int l) {
-  if (!F || l < 0 || l >= F->nl) return -1;
-  return F->L[l]->blk_x;
+extern "C" int nrgpu_fmr_block(nrgpu_fmr *F, int l, int *block) {
+  if (!F || l < 0 || l >= F->nl) return nrgpu_set_error(NRGPU_ERR_ARG, "no level %d", l);
+  return nrgpu_level_get_block(F->L[l], block);
 }
 
 extern "C" int nrgpu_fmr_iteration(nrgpu_fmr *F, int l) {

@@ -9,6 +9,9 @@ struct FlagPoint {
   int box, flag;
 };
 
+// z slabs of the pipelined host-buffer step (nrgpu_bssn_evolve_host)
+#define NRGPU_HOST_SLABS 8
+
 struct nrgpu_level {
   int device;
   int nboxes;
@@ -28,8 +31,12 @@ struct nrgpu_level {
   // points with boundary flag 0, and the norm reduction buffer (first use)
   long ninner;
   double *d_red;
-  // x extent of the rhs kernels' 128-thread blocks (y = 128 / blk_x)
-  int blk_x;
+  // extents of the rhs kernels' 128-thread blocks (x, y, z)
+  int blk[3];
+  // copy and compute streams, and per-slab events, of the pipelined
+  // host-buffer step (created on first use)
+  cudaStream_t hs_copy, hs_comp;
+  cudaEvent_t hev_in[NRGPU_HOST_SLABS], hev_out[NRGPU_HOST_SLABS];
 };
 
 // library-internal pieces shared by the entry points and the mesh-refinement

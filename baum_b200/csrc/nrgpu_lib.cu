@@ -100,7 +100,7 @@ extern "C" int nrgpu_level_create(const nrgpu_level_desc *d, nrgpu_level **out) 
                         d->box[b].z0};
   L->nflagpts = (int)fl.size();
   L->ninner = (long)d->npoints - (long)fl.size();
-  L->blk_x = 32;
+  L->blk[0] = 32; L->blk[1] = 4; L->blk[2] = 1;
   bool ok = cudaMalloc(&L->d_boundary, sizeof(int) * d->npoints) == cudaSuccess &&
             cudaMalloc(&L->d_box, sizeof(BoxGeo) * d->nboxes) == cudaSuccess &&
             cudaMalloc(&L->d_status, sizeof(int) * 4) == cudaSuccess &&
@@ -128,6 +128,12 @@ extern "C" int nrgpu_level_destroy(nrgpu_level *L) {
   cudaFree(L->scratch);
   cudaFree(L->hoststate);
   cudaFree(L->d_red);
+  for (int q = 0; q < NRGPU_HOST_SLABS; ++q) {
+    if (L->hev_in[q]) cudaEventDestroy(L->hev_in[q]);
+    if (L->hev_out[q]) cudaEventDestroy(L->hev_out[q]);
+  }
+  if (L->hs_copy) cudaStreamDestroy(L->hs_copy);
+  if (L->hs_comp) cudaStreamDestroy(L->hs_comp);
   free(L->hbox);
   free(L);
   return NRGPU_OK;
@@ -159,28 +165,3 @@ extern "C" int nrgpu_level_nan_flag(nrgpu_level *L, int *flag) {
   return NRGPU_OK;
 }
 
-extern "C" int nrgpu_bssn_evolve_host(nrgpu_level *L, double *const *host_u, int nsteps, double dt,
-                                      const nrgpu_bssn_params *p) {
-  if (!L || !host_u || nsteps < 0) return nrgpu_set_error(NRGPU_ERR_ARG, "bad arguments");
-  const size_t np = (size_t)L->npoints;
-  if (!L->hoststate && cudaMalloc(&L->hoststate, sizeof(double) * NRGPU_NV * np) != cudaSuccess) {
-    L->hoststate = nullptr;
-    cudaGetLastError();
-    return nrgpu_set_error(NRGPU_ERR_NOMEM, "state of %zu points", np);
-  }
-  double *buf = L->hoststate;
-  double *u[NRGPU_NV];
-  int e = NRGPU_OK;
-  for (int v = 0; v < NRGPU_NV && !e; ++v) {
-    u[v] = buf + v * np;
-    if (!host_u[v]) e = nrgpu_set_error(NRGPU_ERR_ARG, "null host_u[%d]", v);
-    else if (cudaMemcpyAsync(u[v], host_u[v], sizeof(double) * np, cudaMemcpyHostToDevice, 0) != cudaSuccess)
-      e = nrgpu_set_error(NRGPU_ERR_CUDA, "upload of variable %d", v);
-  }
-  for (int s = 0; s < nsteps && !e; ++s) e = nrgpu_bssn_rk4_step(L, u, dt, p, nullptr);
-  for (int v = 0; v < NRGPU_NV && !e; ++v)
-    if (cudaMemcpyAsync(host_u[v], u[v], sizeof(double) * np, cudaMemcpyDeviceToHost, 0) != cudaSuccess)
-      e = nrgpu_set_error(NRGPU_ERR_CUDA, "download of variable %d", v);
-  if (!e && cudaStreamSynchronize(0) != cudaSuccess) e = nrgpu_set_error(NRGPU_ERR_CUDA, "synchronize");
-  return e;
-}

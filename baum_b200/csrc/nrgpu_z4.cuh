@@ -389,11 +389,11 @@ template <int CSY = 0, int CSZ = 0, int PREC = 0, int MAXO = 6>
 __global__ void __launch_bounds__(128, NRGPU_RHS_MINBLOCKS) z4_rhs_kernel(ZCVarPtrs U, ZVarPtrs out, ZCVarPtrs pre, ZVarPtrs acc, Epilogue E,
                                                     const nrgpu_z4_params p, BoxGeo box,
                                                     const int *__restrict__ boundary, double dx, double dy, double dz,
-                                                    int *status) {
+                                                    int *status, int k0, int k1) {
   const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = 1 + blockIdx.z;
-  if (i > box.m - 2 || j > box.n - 2 || k > box.o - 2) return;
+  const int k = k0 + blockIdx.z * blockDim.z + threadIdx.z;
+  if (i > box.m - 2 || j > box.n - 2 || k > k1) return;
   PointCtx P;
   P.i = i; P.j = j; P.k = k;
   P.imax = box.m - 1; P.jmax = box.n - 1; P.kmax = box.o - 1;

@@ -65,8 +65,10 @@ class Hierarchy:
         return abi.lib().nrgpu_fmr_iteration(self.handle, l)
 
     def block(self, l):
-        """The rhs block x extent level l runs with (8 .. 128, 128 threads)."""
-        return abi.lib().nrgpu_fmr_block(self.handle, l)
+        """The rhs block shape (x, y, z) level l runs with (128 threads)."""
+        b = (C.c_int * 3)()
+        abi.check(abi.lib().nrgpu_fmr_block(self.handle, l, b))
+        return tuple(b)
 
     def close(self):
         if self.handle:

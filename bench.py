@@ -37,8 +37,6 @@ RHS_PER_STEP = 4
 # algorithmic FP64 work of one inner point: operators of the reference's
 # generated rhs (bssn_rhs_movpunc_N.c) on its 4th-order + KO6 path
 FLOP_PER_POINT = 4973
-# DRAM bytes of one interior rhs launch from the ncu capture summarised in
-# profiles/bssn_rhs_kernel_c1.md (None until captured)
 # DRAM bytes of one RK-stage launch of bssn_rhs_kernel on the 64^3 box
 # (dram__bytes_read.sum + dram__bytes_write.sum, mean of two captured
 # launches: 168.6 MB and 232.7 MB; profiles/bssn_rhs_kernel_c1.md)
@@ -271,7 +269,7 @@ def gpu_fmr(steps=2):
     # plain launches, then the graph with every level at the 32 x 4 default
     for key, use_graph, tune in (("graph", 1, 1), ("launches", 0, 1), ("graph_untuned_32x4", 1, 0)):
         H = fmr.Hierarchy(levels, dt, params, abi.fmr_params(use_graph=use_graph, autotune=tune))
-        blocks = [H.block(l) for l in range(len(levels))]
+        blocks = ["%dx%dx%d" % H.block(l) for l in range(len(levels))]
         u = [state(lev) for lev in levels]
         H.advance(u, 1)   # first coarse step: 2nd-order time interpolation, no graph
         H.advance(u, 1)   # graph capture (with use_graph)
@@ -282,7 +280,7 @@ def gpu_fmr(steps=2):
         b.record()
         torch.cuda.synchronize()
         ms = a.elapsed_time(b) / steps
-        out[key] = {"ms_per_coarse_step": ms, "value": upd_per_coarse / (ms * 1e-3), "block_x": blocks}
+        out[key] = {"ms_per_coarse_step": ms, "value": upd_per_coarse / (ms * 1e-3), "blocks": blocks}
         finite = all(bool(torch.isfinite(t).all()) for t in u)
         out[key]["finite"] = finite
         H.close()
@@ -434,6 +432,7 @@ def run_ours(args, rank, world):
     u = torch.from_numpy(u0).cuda()
     flush = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream()
+    block = dl.autotune(abi.SYSTEM_BSSN, p, stream)   # the level's rhs block shape
 
     def step():
         bssn.evolve_rk_rk4(dl, u, DT, p, stream)
@@ -535,12 +534,13 @@ def run_ours(args, rank, world):
         "roofline": {"bound": "fp64", "kernel": "bssn_rhs_kernel (interior rhs, one launch = 64^3 points)",
                      "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
                      "peak_source": "measured FP64 FMA probe on this GPU (nrgpu_probe_fp64_peak)",
-                     "flop_per_point": FLOP_PER_POINT, "launch_ms": rhs_ms, "traffic": RHS_TRAFFIC_BYTES},
+                     "flop_per_point": FLOP_PER_POINT, "launch_ms": rhs_ms, "traffic": RHS_TRAFFIC_BYTES,
+                     "block": "%dx%dx%d" % block},
         "cpu_baseline": cpu,
         "e2e": {"value": PTS_PER_RHS * RHS_PER_STEP * args.steps * world / e2e_sum, "unit": UNIT,
                 "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
                 "call": "nrgpu_bssn_evolve_host(nsteps=1) from pinned host memory"},
-        "gpu_launches": 10 * args.steps,
+        "gpu_launches": 9 * args.steps,   # 4 stages x (interior + flagged) + algcon
         "clocks": clocks,
         "multigrid": multigrid,
         "fmr": fmr_line,

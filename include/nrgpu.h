@@ -183,7 +183,11 @@ int nrgpu_bssn_rk4_step(nrgpu_level *lev, double *const *u, double dt,
 /* nsteps RK4 steps starting from and returning to HOST arrays: uploads
  * host_u (24 host pointers), steps on the device, downloads the result into
  * host_u.  The end-to-end call of a host code that keeps its state in host
- * memory. */
+ * memory.  When the 24 arrays lie at one pitch (rows of one array) and the
+ * level is one box of at least 16 planes, the box is copied as z slabs
+ * (one 2D copy per slab) and the copies overlap the first stage of the
+ * first step and the last stage of the last step; results are identical
+ * either way.  Pinned host memory gives full PCIe bandwidth. */
 int nrgpu_bssn_evolve_host(nrgpu_level *lev, double *const *host_u, int nsteps,
                            double dt, const nrgpu_bssn_params *p);
 
@@ -308,22 +312,25 @@ int nrgpu_fmr_restrict_prolong(nrgpu_fmr *fmr, int lfine, double *const *uc, dou
 int nrgpu_fmr_advance(nrgpu_fmr *fmr, double *const *u, int nsteps, void *stream);
 /* level iterations done so far (tL.iteration) */
 int nrgpu_fmr_iteration(nrgpu_fmr *fmr, int l);
-/* the rhs block x extent level l runs with */
-int nrgpu_fmr_block(nrgpu_fmr *fmr, int l);
+/* the rhs block shape (x, y, z) level l runs with, into block[3] */
+int nrgpu_fmr_block(nrgpu_fmr *fmr, int l, int *block);
 
 /* the evolution systems */
 enum { NRGPU_SYSTEM_BSSN = 0, NRGPU_SYSTEM_Z4C = 1 };
 
 /* ---- launch-shape autotuner (no counterpart in the reference) -------------
  * The rhs kernels compute one point per thread in blocks of 128 threads.
- * nrgpu_level_autotune times the x extents 8, 16, 32, 64, 128 for the
- * level's boxes and the given system (NRGPU_SYSTEM_BSSN / _Z4C, below) and
- * parameters on a flat state in the level's RK4 scratch (the user's arrays
- * are not touched), keeps the fastest for the level and returns it in
- * *best_x (may be NULL).  Waits for the stream.  nrgpu_level_block sets the
- * extent directly (default 32).  Results do not depend on the shape. */
-int nrgpu_level_autotune(nrgpu_level *L, int system, const void *params, void *stream, int *best_x);
-int nrgpu_level_block(nrgpu_level *L, int blk_x);
+ * nrgpu_level_autotune times twelve block shapes (x, y, z extents, from
+ * 32 x 4 x 1 and 8 x 16 x 1 to 8 x 4 x 4 and 4 x 4 x 8) for the level's boxes
+ * and the given system (NRGPU_SYSTEM_BSSN / _Z4C) and parameters, on a flat
+ * state in the level's RK4 scratch (the user's arrays are not touched),
+ * keeps the fastest for the level and returns it in best_block[3] (may be
+ * NULL).  Waits for the stream.  nrgpu_level_block sets a shape directly
+ * (powers of two, bx by bz = 128; default 32 x 4 x 1).  Results do not
+ * depend on the shape. */
+int nrgpu_level_autotune(nrgpu_level *L, int system, const void *params, void *stream, int *best_block);
+int nrgpu_level_block(nrgpu_level *L, int bx, int by, int bz);
+int nrgpu_level_get_block(nrgpu_level *L, int *block);
 
 /* ---- ADM diagnostics ------------------------------------------------------
  * ADM metric and extrinsic curvature from the conformal variables:

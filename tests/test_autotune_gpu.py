@@ -9,7 +9,8 @@ import torch
 from baum_b200 import abi, bssn, fmr, synthetic, z4
 
 pytestmark = pytest.mark.gpu
-SHAPES = (8, 16, 32, 64, 128)
+SHAPES = ((32, 4, 1), (64, 2, 1), (16, 8, 1), (8, 16, 1), (128, 1, 1), (16, 4, 2), (8, 8, 2), (32, 2, 2),
+          (8, 4, 4), (4, 8, 4), (16, 2, 4), (4, 4, 8))
 
 
 def fourier(level, nv, unit):
@@ -19,15 +20,16 @@ def fourier(level, nv, unit):
 
 @pytest.mark.parametrize("system", ["bssn", "z4c"])
 def test_every_block_shape_gives_identical_states(gpu, system):
-    lev = abi.Level.single_box(37, 0.4)   # 37 - 2 = 35 inner points: ragged in every shape
+    lev = abi.Level.single_box(37, 0.4)   # 35 inner points per side: ragged in every shape
     if system == "bssn":
         mod, nv, p, u0 = bssn, abi.NVARS, abi.bssn_params(), fourier(lev, abi.NVARS, synthetic.BSSN_UNIT)
     else:
         mod, nv, p, u0 = z4, abi.Z4_NVARS, abi.z4_params(), fourier(lev, abi.Z4_NVARS, synthetic.Z4_UNIT)
     out = []
-    for bx in SHAPES:
+    for shape in SHAPES:
         dl = mod.DeviceLevel(lev)
-        dl.set_block(bx)
+        dl.set_block(*shape)
+        assert dl.block() == shape
         u = torch.from_numpy(u0.copy()).cuda()
         for _ in range(2):
             mod.evolve_rk_rk4(dl, u, 0.05, p)
@@ -47,8 +49,11 @@ def test_tuner_picks_a_shape_and_leaves_the_state(gpu):
     assert best in SHAPES
     assert np.array_equal(u.cpu().numpy(), u0)
     assert not dl.nan_flag()
+    assert dl.block() == best
     with pytest.raises(RuntimeError):
-        dl.set_block(48)
+        dl.set_block(48, 2, 1)
+    with pytest.raises(RuntimeError):
+        dl.set_block(32, 4, 2)
     with pytest.raises(RuntimeError):
         dl.autotune(7, abi.z4_params())
 
@@ -62,7 +67,7 @@ def test_tuned_hierarchy_equals_untuned(gpu):
     for tune in (0, 1):
         H = fmr.Hierarchy(levels, dt, params, abi.fmr_params(autotune=tune))
         if not tune:
-            assert [H.block(l) for l in range(3)] == [32, 32, 32]
+            assert [H.block(l) for l in range(3)] == [(32, 4, 1)] * 3
         else:
             assert all(H.block(l) in SHAPES for l in range(3))
         u = [torch.from_numpy(x.copy()).cuda() for x in u0]

@@ -89,16 +89,31 @@ def test_c1_schwarzschild_50_steps_matches_oracle(gpu):
     assert not dl.nan_flag()
 
 
-def test_evolve_host_matches_device_path(gpu):
-    lev, u0 = punctures.schwarzschild_c1(n_inner=24, dx=0.5)
-    p = abi.bssn_params()
+@pytest.mark.parametrize("n_inner,nsteps,order", [(24, 3, 4), (24, 1, 4), (24, 0, 4), (40, 1, 6), (30, 2, 6),
+                                                   (10, 2, 4)])
+def test_evolve_host_matches_device_path(gpu, n_inner, nsteps, order):
+    """The host-buffer call equals the device step bit for bit: z slabs
+    whose 2D-copy upload and download overlap the first and last stages
+    (a (24, n) host array), whole-variable copies (separate host arrays),
+    and a box below 16 planes (not cut into slabs)."""
+    lev, u0 = punctures.schwarzschild_c1(n_inner=n_inner, dx=0.5)
+    p = abi.bssn_params(**(CASES["bssn_fourier_o6"] if order == 6 else {}))
     dl = bssn.DeviceLevel(lev)
     u = to_dev(u0)
-    for _ in range(3):
+    for _ in range(nsteps):
         bssn.evolve_rk_rk4(dl, u, 0.125, p)
     h = np.ascontiguousarray(u0.copy())
-    bssn.evolve_host(dl, h, 3, 0.125, p)
+    bssn.evolve_host(dl, h, nsteps, 0.125, p)
     assert np.array_equal(h, u.cpu().numpy())
+    # one array per variable at irregular gaps (no common pitch: whole-variable copies)
+    n = u0.shape[1]
+    buf = np.zeros(abi.NVARS * n + abi.NVARS ** 2)
+    rows = [buf[v * n + v * v:(v + 1) * n + v * v] for v in range(abi.NVARS)]
+    for v in range(abi.NVARS):
+        rows[v][:] = u0[v]
+    bssn.evolve_host(dl, rows, nsteps, 0.125, p)
+    assert np.array_equal(np.stack(rows), h)
+    assert not dl.nan_flag()
 
 
 def test_nan_in_state_raises_flag(gpu):
