@@ -559,7 +559,7 @@ __device__ __forceinline__ int ladder(int order, int d) {
 // CSY, CSZ: the box strides dj = m and dk = m n when known at compile time
 // (0 = read them from the box)
 template <int CSY = 0, int CSZ = 0, int MAXO = 6, int MINB = NRGPU_RHS_MINBLOCKS>
-__global__ void __launch_bounds__(128, MINB) bssn_rhs_kernel(CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPtrs acc,
+__global__ void __launch_bounds__(256, MINB) bssn_rhs_kernel(CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPtrs acc,
                                                       Epilogue E, const nrgpu_bssn_params p, BoxGeo box,
                                                       const int *__restrict__ boundary, double dx, double dy,
                                                       double dz, int *status, int k0, int k1) {
@@ -761,7 +761,7 @@ static int launch_rhs(nrgpu_level *L, const CVarPtrs &U, const VarPtrs &out, con
       const int k0 = max(kb, 1), k1 = min(ke, bx.o - 2);
       if (k1 < k0) continue;
       // the block shape of the level (32 x 4 x 1, or what nrgpu_level_autotune
-      // measured fastest for this box); 128 threads, one point each
+      // measured fastest for this box); 128 or 256 threads, one point each
       const dim3 blk(L->blk[0], L->blk[1], L->blk[2]);
       const dim3 grd((bx.m - 2 + blk.x - 1) / blk.x, (bx.n - 2 + blk.y - 1) / blk.y, (k1 - k0 + blk.z) / blk.z);
       // box strides as compile-time constants for the sizes of the standard
@@ -1285,7 +1285,7 @@ static int z4_launch(nrgpu_level *L, const ZCVarPtrs &U, const ZVarPtrs &out, co
       const BoxGeo &bx = L->hbox[b];
       if (bx.m < 3 || bx.n < 3 || bx.o < 3) continue;
       // the block shape of the level (32 x 4 x 1, or what nrgpu_level_autotune
-      // measured fastest for this box); 128 threads, one point each
+      // measured fastest for this box); 128 or 256 threads, one point each
       const dim3 blk(L->blk[0], L->blk[1], L->blk[2]);
       const dim3 grd((bx.m - 2 + blk.x - 1) / blk.x, (bx.n - 2 + blk.y - 1) / blk.y, (bx.o - 2 + blk.z - 1) / blk.z);
       if (p.precision == 1) {
@@ -1358,24 +1358,24 @@ int nrgpu_z4_rk4_stages(nrgpu_level *L, double *const *u, double dt, const nrgpu
   if ((e = z4_fill(&U, u, "u"))) return e;
   double *scr = nullptr;
   if ((e = nrgpu_level_scratch(L, &scr))) return e;
-  ZVarPtrs P, V1, V2;
+  // the RK4 step without a copy of u, as for BSSN (rk_stage): u is the
+  // stage-1 input and "P"; A accumulates; stage 4 writes u = A + dt/6 r4
+  ZVarPtrs A, V1, V2;
   const size_t np = (size_t)L->npoints;
   for (int v = 0; v < ZNV; ++v) {
-    P.p[v] = scr + (0 * ZNV + v) * np;
+    A.p[v] = scr + (0 * ZNV + v) * np;
     V1.p[v] = scr + (1 * ZNV + v) * np;
     V2.p[v] = scr + (2 * ZNV + v) * np;
   }
-  const long n = (long)ZNV * L->npoints;
-  z4_copy_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(P, z4_c(U), L->npoints);
-  const ZCVarPtrs cP = z4_c(P);
-  Epilogue E1 = {EPI_RK, 0.0, dt / 6, dt / 2, 1};
-  Epilogue E2 = {EPI_RK, 0.0, dt / 3, dt / 2, 1};
-  Epilogue E3 = {EPI_RK, 0.0, dt / 3, dt, 1};
-  Epilogue E4 = {EPI_RK, 0.0, dt / 6, 0.0, 0};
-  if ((e = z4_launch(L, cP, V1, cP, U, E1, *p, st, true, true))) return e;
-  if ((e = z4_launch(L, z4_c(V1), V2, cP, U, E2, *p, st, true, true))) return e;
-  if ((e = z4_launch(L, z4_c(V2), V1, cP, U, E3, *p, st, true, true))) return e;
-  if ((e = z4_launch(L, z4_c(V1), V2, cP, U, E4, *p, st, true, true))) return e;
+  const ZCVarPtrs cU = z4_c(U);
+  const Epilogue E1 = {EPI_RK, 0.0, dt / 6, dt / 2, 1, ACC_INIT};
+  const Epilogue E2 = {EPI_RK, 0.0, dt / 3, dt / 2, 1, ACC_ADD};
+  const Epilogue E3 = {EPI_RK, 0.0, dt / 3, dt, 1, ACC_ADD};
+  const Epilogue E4 = {EPI_RK, 0.0, dt / 6, 0.0, 0, ACC_FINAL};
+  if ((e = z4_launch(L, cU, V1, cU, A, E1, *p, st, true, true))) return e;
+  if ((e = z4_launch(L, z4_c(V1), V2, cU, A, E2, *p, st, true, true))) return e;
+  if ((e = z4_launch(L, z4_c(V2), V1, cU, A, E3, *p, st, true, true))) return e;
+  if ((e = z4_launch(L, z4_c(V1), U, cU, A, E4, *p, st, true, true))) return e;
   return NRGPU_OK;
 }
 
@@ -1428,10 +1428,15 @@ extern "C" int nrgpu_level_autotune(nrgpu_level *L, int system, const void *para
   cudaEvent_t a, b;
   NRGPU_CUDA_TRY(cudaEventCreate(&a));
   NRGPU_CUDA_TRY(cudaEventCreate(&b));
-  // 128-thread shapes: flat (x, y) and with a z extent (a smaller stencil
-  // footprint per block, so more of each variable's taps hit in L1)
+  // 128- and 256-thread shapes, flat (x, y) and with a z extent.  The
+  // kernels wait on L1/L2: the larger and the more cubic the block, the
+  // smaller its stencil halo per point, so more taps hit in L1 (a 256-thread
+  // block at 255 registers is one block per SM, the same 8 warps as two
+  // 128-thread blocks)
   static const int cand[][3] = {{32, 4, 1}, {64, 2, 1}, {16, 8, 1}, {8, 16, 1}, {128, 1, 1}, {16, 4, 2},
-                                {8, 8, 2},  {32, 2, 2}, {8, 4, 4},  {4, 8, 4}, {16, 2, 4},  {4, 4, 8}};
+                                {8, 8, 2},  {32, 2, 2}, {8, 4, 4},  {4, 8, 4}, {16, 2, 4},  {4, 4, 8},
+                                {64, 4, 1}, {32, 8, 1}, {16, 8, 2}, {32, 4, 2}, {16, 4, 4}, {8, 8, 4},
+                                {64, 2, 2}, {128, 2, 1}};
   const int ncand = (int)(sizeof cand / sizeof cand[0]);
   float best = 1e30f;
   int bb = 0;
@@ -1476,9 +1481,9 @@ extern "C" int nrgpu_level_autotune(nrgpu_level *L, int system, const void *para
 }
 
 extern "C" int nrgpu_level_block(nrgpu_level *L, int bx, int by, int bz) {
-  auto pow2 = [](int v) { return v >= 1 && v <= 128 && (v & (v - 1)) == 0; };
-  if (!L || !pow2(bx) || !pow2(by) || !pow2(bz) || bx * by * bz != 128)
-    return nrgpu_set_error(NRGPU_ERR_ARG, "block %d x %d x %d (powers of two, 128 threads)", bx, by, bz);
+  auto pow2 = [](int v) { return v >= 1 && v <= 256 && (v & (v - 1)) == 0; };
+  if (!L || !pow2(bx) || !pow2(by) || !pow2(bz) || (bx * by * bz != 128 && bx * by * bz != 256))
+    return nrgpu_set_error(NRGPU_ERR_ARG, "block %d x %d x %d (powers of two, 128 or 256 threads)", bx, by, bz);
   L->blk[0] = bx; L->blk[1] = by; L->blk[2] = bz;
   return NRGPU_OK;
 }

@@ -376,6 +376,16 @@ __device__ __forceinline__ void z4_store(const double r[ZNV], int x, const ZVarP
     det_trace_fix(n, q);  // g~ at 0..5 and A~ at 7..12 in both lists
 #pragma unroll
     for (int v = 0; v < ZNV; ++v) out.p[v][x] = n[v];
+  } else if (E.accmode == ACC_FINAL) {
+#pragma unroll
+    for (int v = 0; v < ZNV; ++v) out.p[v][x] = acc.p[v][x] + E.wacc * r[v];
+  } else if (E.accmode == ACC_INIT) {
+#pragma unroll
+    for (int v = 0; v < ZNV; ++v) {
+      const double u0 = ldg(pre.p[v] + x);
+      acc.p[v][x] = u0 + E.wacc * r[v];
+      if (E.has_v) out.p[v][x] = u0 + E.cv * r[v];
+    }
   } else {
 #pragma unroll
     for (int v = 0; v < ZNV; ++v) {
@@ -386,7 +396,7 @@ __device__ __forceinline__ void z4_store(const double r[ZNV], int x, const ZVarP
 }
 
 template <int CSY = 0, int CSZ = 0, int PREC = 0, int MAXO = 6>
-__global__ void __launch_bounds__(128, NRGPU_RHS_MINBLOCKS) z4_rhs_kernel(ZCVarPtrs U, ZVarPtrs out, ZCVarPtrs pre, ZVarPtrs acc, Epilogue E,
+__global__ void __launch_bounds__(256, NRGPU_RHS_MINBLOCKS) z4_rhs_kernel(ZCVarPtrs U, ZVarPtrs out, ZCVarPtrs pre, ZVarPtrs acc, Epilogue E,
                                                     const nrgpu_z4_params p, BoxGeo box,
                                                     const int *__restrict__ boundary, double dx, double dy, double dz,
                                                     int *status, int k0, int k1) {
@@ -432,7 +442,11 @@ __global__ void z4_flagged_kernel(ZCVarPtrs U, ZVarPtrs out, ZCVarPtrs pre, ZVar
   const FlagPoint fp = pts[t / ZNV];
   const int ccc = fp.ijk;
   if (fp.flag != NRGPU_PHYBOUND) {
-    if (E.mode == EPI_RK && E.has_v) out.p[v][ccc] = ldg(pre.p[v] + ccc);
+    if (E.mode == EPI_RK) {
+      if (E.accmode == ACC_INIT) acc.p[v][ccc] = ldg(pre.p[v] + ccc);
+      else if (E.accmode == ACC_FINAL) out.p[v][ccc] = acc.p[v][ccc];
+      if (E.has_v) out.p[v][ccc] = ldg(pre.p[v] + ccc);
+    }
     return;
   }
   const BoxGeo b = boxes[fp.box];
@@ -456,15 +470,14 @@ __global__ void z4_flagged_kernel(ZCVarPtrs U, ZVarPtrs out, ZCVarPtrs pre, ZVar
   rhs += -(Wx * delx * (1.0 / (2.0 * dx)) + Wy * dely * (1.0 / (2.0 * dy)) + Wz * delz * (1.0 / (2.0 * dz)));
   if (E.mode == EPI_RHS) out.p[v][ccc] = rhs;
   else if (E.mode == EPI_ADDLINEAR) out.p[v][ccc] = ldg(pre.p[v] + ccc) + E.c * rhs;
-  else {
+  else if (E.accmode == ACC_FINAL) out.p[v][ccc] = acc.p[v][ccc] + E.wacc * rhs;
+  else if (E.accmode == ACC_INIT) {
+    const double u0 = ldg(pre.p[v] + ccc);
+    acc.p[v][ccc] = u0 + E.wacc * rhs;
+    if (E.has_v) out.p[v][ccc] = u0 + E.cv * rhs;
+  } else {
     acc.p[v][ccc] += E.wacc * rhs;
     if (E.has_v) out.p[v][ccc] = ldg(pre.p[v] + ccc) + E.cv * rhs;
   }
 }
 
-__global__ void z4_copy_kernel(ZVarPtrs dst, ZCVarPtrs src, int npoints) {
-  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long)ZNV * npoints) return;
-  const int v = (int)(t / npoints), q = (int)(t % npoints);
-  dst.p[v][q] = src.p[v][q];
-}

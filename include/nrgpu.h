@@ -319,15 +319,16 @@ int nrgpu_fmr_block(nrgpu_fmr *fmr, int l, int *block);
 enum { NRGPU_SYSTEM_BSSN = 0, NRGPU_SYSTEM_Z4C = 1 };
 
 /* ---- launch-shape autotuner (no counterpart in the reference) -------------
- * The rhs kernels compute one point per thread in blocks of 128 threads.
- * nrgpu_level_autotune times twelve block shapes (x, y, z extents, from
- * 32 x 4 x 1 and 8 x 16 x 1 to 8 x 4 x 4 and 4 x 4 x 8) for the level's boxes
+ * The rhs kernels compute one point per thread in blocks of 128 or 256
+ * threads.  nrgpu_level_autotune times twenty block shapes (x, y, z
+ * extents, from 32 x 4 x 1 and 8 x 16 x 1 to 8 x 4 x 4, 16 x 8 x 2 and
+ * 8 x 8 x 4) for the level's boxes
  * and the given system (NRGPU_SYSTEM_BSSN / _Z4C) and parameters, on a flat
  * state in the level's RK4 scratch (the user's arrays are not touched),
  * keeps the fastest for the level and returns it in best_block[3] (may be
  * NULL).  Waits for the stream.  nrgpu_level_block sets a shape directly
- * (powers of two, bx by bz = 128; default 32 x 4 x 1).  Results do not
- * depend on the shape. */
+ * (powers of two, bx by bz = 128 or 256; default 32 x 4 x 1).  Results do
+ * not depend on the shape. */
 int nrgpu_level_autotune(nrgpu_level *L, int system, const void *params, void *stream, int *best_block);
 int nrgpu_level_block(nrgpu_level *L, int bx, int by, int bz);
 int nrgpu_level_get_block(nrgpu_level *L, int *block);
