@@ -37,10 +37,10 @@ RHS_PER_STEP = 4
 # algorithmic FP64 work of one inner point: operators of the reference's
 # generated rhs (bssn_rhs_movpunc_N.c) on its 4th-order + KO6 path
 FLOP_PER_POINT = 4973
-# DRAM bytes of one RK-stage launch of bssn_rhs_kernel on the 64^3 box
-# (dram__bytes_read.sum + dram__bytes_write.sum, mean of two captured
-# launches: 168.6 MB and 232.7 MB; profiles/bssn_rhs_kernel_c1.md)
-RHS_TRAFFIC_BYTES = 200.6e6
+# DRAM bytes of one RK-stage launch of bssn_rhs_kernel on the 64^3 box, block 16 x 8 x 2
+# (dram__bytes_read.sum + dram__bytes_write.sum, mean of the two captured
+# launches, stages 1 and 2: 120.5 MB and 232.7 MB; profiles/bssn_rhs_kernel_c1.md)
+RHS_TRAFFIC_BYTES = 176.6e6
 CONFIG = {"workload": "bssn_schwarzschild_64^3_rk4", "box": "66^3 (64^3 inner + boundary layer)",
           "dx": DX, "dt": DT, "order": 4, "dissipation": "KO6 eps=0.1", "gauge": "1+log, Gamma-driver eta=2",
           "l2": "flushed (256 MiB write) before every timed step", "parallelism": "replicas"}
@@ -470,6 +470,13 @@ def run_ours(args, rank, world):
     torch.cuda.synchronize()
     rhs_ms = sum(a.elapsed_time(b) for a, b in rev) / len(rev)
     clocks = sample_clocks_stop(clk) if rank == 0 else None
+    if args.case == "c1-step":
+        if rank == 0:
+            units = PTS_PER_RHS * RHS_PER_STEP * args.steps * world
+            print(json.dumps({"case": "c1-step", "value": units / (ms * 1e-3), "unit": UNIT,
+                              "ms_per_step": ms / args.steps, "rhs_launch_ms": rhs_ms,
+                              "block": "%dx%dx%d" % block, "clocks": clocks}))
+        return
 
     # measured FP64 peak on this GPU (no FP64 entry in the peak list)
     fl, pms = C.c_double(), C.c_float()
@@ -590,8 +597,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--case", default="c1", choices=["c1", "z4c160"],
-                    help="c1: the benchmark line; z4c160: the 160^3 Z4c box alone")
+    ap.add_argument("--case", default="c1", choices=["c1", "c1-step", "z4c160"],
+                    help="c1: the benchmark line; c1-step: only the 64^3 BSSN RK4 steps and the rhs "
+                         "launches of that line (for profiling); z4c160: the 160^3 Z4c box alone")
     args = ap.parse_args()
     if args.case == "z4c160":
         run_z4c160(args)
