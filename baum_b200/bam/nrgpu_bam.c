@@ -20,6 +20,19 @@
  *                           hook; set bssn/z4_register_algcon = no.
  * physics with z4 selects the Z4c system (resident and fmr modes).
  *
+ *   nrgpu_multigrid = yes   the puncture initial-data solve (punctures_solver
+ *                           = multigrid, PunctureSolve.c:282) runs on the
+ *                           GPU (nrgpu_mg_solve) when the grid is one cubic
+ *                           box centred on the origin with the second-order
+ *                           puncture operator, a Robin boundary and V cycles;
+ *                           otherwise BAM's own multigrid runs.  The solver is
+ *                           reached through PickEllipticSolver's function
+ *                           pointer (Punctures.c:283-311): a tree carrying
+ *                           this module adds the keyword there
+ *                           (punctures_solver = multigrid -> nrgpu_multigrid),
+ *                           or links with -Wl,--wrap=multigrid, which sends
+ *                           the pointer to __wrap_multigrid below.
+ *
  * Parameters are read exactly where bssn_rhs_movpunc_N reads them
  * (bssn_rhs_movpunc_N.c:107-145), the boundary speeds and far limits from the
  * variable database (VarFarLimit/VarPropSpeed, variables.c:246-248), and the
@@ -56,6 +69,7 @@ static nrgpu_slot slots[64];
 /* cudart entry points used by this module (declared here so no CUDA header
  * is needed to compile a BAM project) */
 extern int cudaMalloc(void **p, size_t n);
+extern int cudaFree(void *p);
 extern int cudaMemcpy(void *d, const void *s, size_t n, int kind);
 extern int cudaDeviceSynchronize(void);
 
@@ -341,6 +355,98 @@ int nrgpu_evolve_fmr(tL *level)
   return 0;
 }
 
+/* ---- puncture initial data: the multigrid on the device --------------------- */
+
+typedef void (*mg_operator)(tL *, tVarList *, tVarList *);
+/* the second-order puncture operator and its relaxation (PunctureSolve.c:21,108) */
+void Lpuncture_nonlin(tL *level, tVarList *vllu, tVarList *vlu);
+void Lpuncture_GS(tL *level, tVarList *vlv, tVarList *vlu);
+/* BAM's own multigrid (multigrid.c:35).  A build linked with
+ * -Wl,--wrap=multigrid compiles this module with NRGPU_WRAP_MULTIGRID: every
+ * reference to multigrid then lands on __wrap_multigrid, and BAM's solver is
+ * __real_multigrid. */
+#ifdef NRGPU_WRAP_MULTIGRID
+int __real_multigrid(tL *level, tVarList *u, tVarList *f, tVarList *v, tVarList *c, int itmax, double tol,
+                     double *normres, mg_operator lop, mg_operator lgs);
+#define HOST_MULTIGRID __real_multigrid
+#else
+int multigrid(tL *level, tVarList *u, tVarList *f, tVarList *v, tVarList *c, int itmax, double tol,
+              double *normres, mg_operator lop, mg_operator lgs);
+#define HOST_MULTIGRID multigrid
+#endif
+
+/* multigrid(level, u, f, v, c, itmax, tol, &normres, lop, lgs) of the puncture
+ * solve: c = (punctures_a, punctures_b), u = punctures_u holds the initial
+ * guess and receives the solution; f and v are the reference's work lists
+ * (f = 0 on every level, multigrid.c:97-104), not needed on the device */
+int nrgpu_multigrid(tL *level, tVarList *u, tVarList *f, tVarList *v, tVarList *c, int itmax, double tol,
+                    double *normres, mg_operator lop, mg_operator lgs)
+{
+  const char *why = 0;
+  tG *g = level->grid;
+  tB *box = level->nboxes == 1 ? level->box[0] : 0;
+  nrgpu_mg_params mp;
+  nrgpu_mg *mg = 0;
+  double *d = 0, res = 0.0;
+  int ncyc = 0, m = 0, i;
+  size_t n, bytes;
+
+  if (!Getv("nrgpu_multigrid", "yes")) why = "nrgpu_multigrid = no";
+  else if (lop != Lpuncture_nonlin || lgs != Lpuncture_GS) why = "not the second-order puncture operator";
+  else if (g->lmin != g->lmax || !box || !c || c->n < 2) why = "more than one level or box";
+  else if (!Getv("punctures_boundary", "robin")) why = "punctures_boundary is not robin";
+  else if (!Getv("mg_setbound", "set_boundary_elliptic")) why = "mg_setbound";
+  else if (Geti("mg_wcycle_nmax") > 0 || Geti("mg_vcycle_nmin") != 0) why = "W cycles or mg_vcycle_nmin";
+  else if (box->m != box->n || box->m != box->o || level->dx != level->dy || level->dx != level->dz)
+    why = "not a cube";
+  else if (fabs(box->x0 + 0.5 * (box->m - 1) * level->dx) > 1e-12 * level->dx ||
+           fabs(box->y0 + 0.5 * (box->n - 1) * level->dy) > 1e-12 * level->dy ||
+           fabs(box->z0 + 0.5 * (box->o - 1) * level->dz) > 1e-12 * level->dz)
+    why = "box not centred on the origin";
+  if (!why) {
+    m = box->m;
+    nrgpu_mg_params_default(&mp);
+    mp.npre = Geti("mg_relax_npre");
+    mp.npost = Geti("mg_relax_npost");
+    mp.exact_nmin = Geti("mg_exact_nmin");
+    mp.exact_nmax = Geti("mg_exact_nmax");
+    mp.vcycle_nmin = Geti("mg_vcycle_nmin");
+    mp.vcycle_nmax = Geti("mg_vcycle_nmax");
+    mp.fullV = Getv("mg_typeofcycles", "fullV");
+    mp.size_nmin = Geti("mg_size_nmin");
+    mp.levels_nmax = Geti("mg_levels_nmax");
+    mp.tol = tol;
+    mp.falloff = Getd("punctures_robin_falloff");
+    if (nrgpu_mg_create(m, level->dx, &mp, &mg) != NRGPU_OK) why = (const char *)nrgpu_last_error();
+  }
+  if (why) {
+    printf("nrgpu: multigrid on the host (%s)\n", why);
+    return HOST_MULTIGRID(level, u, f, v, c, itmax, tol, normres, lop, lgs);
+  }
+  n = (size_t)m * m * m;
+  bytes = sizeof(double) * n;
+  if (cudaMalloc((void **)&d, 3 * bytes)) errorexit("nrgpu: device allocation failed");
+  for (i = 0; i < 2; i++)
+    if (cudaMemcpy(d + i * n, level->v[c->index[i]], bytes, 1)) errorexit("nrgpu: copy failed");
+  if (cudaMemcpy(d + 2 * n, level->v[u->index[0]], bytes, 1)) errorexit("nrgpu: copy failed");
+  check(nrgpu_mg_solve(mg, d, d + n, d + 2 * n, &ncyc, &res, 0), "multigrid");
+  if (cudaMemcpy(level->v[u->index[0]], d + 2 * n, bytes, 2)) errorexit("nrgpu: copy failed");
+  cudaFree(d);
+  nrgpu_mg_destroy(mg);
+  if (normres) *normres = res;
+  printf("nrgpu_multigrid: %d V-cycles on the GPU, residual %.3e\n", ncyc, res);
+  return 0;
+}
+
+#ifdef NRGPU_WRAP_MULTIGRID
+/* the wrapped entry of a build linked with -Wl,--wrap=multigrid */
+int __wrap_multigrid(tL *level, tVarList *u, tVarList *f, tVarList *v, tVarList *c, int itmax, double tol,
+                     double *normres, mg_operator lop, mg_operator lgs)
+{
+  return nrgpu_multigrid(level, u, f, v, c, itmax, tol, normres, lop, lgs);
+}
+#endif
+
 int nrgpu_startup(tL *level)
 {
   if (level->l != 0) return 0;
@@ -370,6 +476,7 @@ void bam_nrgpu(void)
   printf("Adding nrgpu (B200 evolution path)\n");
   AddPar("nrgpu_mode", "callback", "how the GPU path plugs in [callback,resident,fmr]");
   AddPar("nrgpu_device", "0", "CUDA device");
+  AddPar("nrgpu_multigrid", "no", "puncture initial-data multigrid on the GPU [no,yes]");
   AddFun(POST_INITIALDATA, nrgpu_startup, "nrgpu: register the GPU evolution");
   AddFun(EVOLVE, nrgpu_evolve_resident, "nrgpu: resident RK4 step");
   AddFun(EVOLVE, nrgpu_evolve_fmr, "nrgpu: one coarse step of all levels");

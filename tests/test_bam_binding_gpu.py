@@ -157,3 +157,41 @@ def test_bam_fmr_mode_matches_bam(gpu, cpu_state):
         err = np.abs(a - b).max(axis=1) / np.maximum(np.abs(b).max(axis=1), 1e-8)
         assert keep[l].sum() > 0.3 * levels[l].npoints
         assert err.max() < 2e-11, (l, err.max())
+
+
+def run_mg(binary, extra_physics, extra):
+    """The reference's puncture solve of tests/golden/mg_binary_34.par (a
+    Bowen-York binary on a 34^3 grid, full-V multigrid to 1e-10); returns
+    punctures_u after the solve and the run's stdout."""
+    par = open(os.path.join(ROOT, "tests", "golden", "mg_binary_34.par")).read()
+    par = par.replace("physics = adm punctures multigrid nrharness",
+                      "physics = adm punctures multigrid nrharness" + extra_physics) + extra + "\n"
+    work = tempfile.mkdtemp(prefix="bamgpu_")
+    try:
+        with open(os.path.join(work, "t.par"), "w") as f:
+            f.write(par)
+        r = subprocess.run([binary, "-nt", "4", "t.par"], cwd=work, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+        return dumpfile.read(os.path.join(work, "mg_u_l0.bin"))["data"][0], r.stdout
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+def test_bam_multigrid_on_the_gpu_matches_bam(gpu, cpu_state):
+    """nrgpu_multigrid = yes: BAM's punctures_solver = multigrid call
+    (PunctureSolve.c:282) runs nrgpu_mg_solve; the same number of V cycles as
+    BAM's own multigrid and the same u to 1e-10 relative (the tolerance of
+    the multigrid parity tests)."""
+    import re
+    u_ref, out_ref = run_mg(BAM, "", "")
+    u_gpu, out_gpu = run_mg(BAM_GPU, " nrgpu", "nrgpu_multigrid = yes")
+    n_ref = int(re.search(r"after (\d+) V-cycles", out_ref).group(1))
+    m = re.search(r"nrgpu_multigrid: (\d+) V-cycles on the GPU, residual ([0-9.e+-]+)", out_gpu)
+    assert m, out_gpu[-2000:]
+    assert int(m.group(1)) == n_ref
+    assert float(m.group(2)) <= 1e-10
+    assert np.abs(u_gpu - u_ref).max() <= 1e-10 * np.abs(u_ref).max()
+    # switched off, the wrapped build runs BAM's own solver
+    u_host, out_host = run_mg(BAM_GPU, " nrgpu", "nrgpu_multigrid = no")
+    assert "multigrid on the host" in out_host
+    assert np.abs(u_host - u_ref).max() <= 1e-12 * np.abs(u_ref).max()   # OpenMP sums may reorder
