@@ -67,39 +67,85 @@ __global__ void robin_kernel(double *u, const int *__restrict__ bidx, const int 
   u[bidx[t]] = dirichlet ? -un : un * c1[t] / c2[t];
 }
 
+// w^-7 and w^-8 by multiplication: the reference's pow(w, -7.0) and
+// pow(w, -8.0) (PunctureSolve.c:38-41) within a few ulp, at a few FLOPs
+// instead of an FP64 pow (log + exp) per point and sweep
+__device__ __forceinline__ double inv_pow7(double w) {
+  const double r = 1.0 / w, r2 = r * r, r4 = r2 * r2;
+  return r4 * r2 * r;
+}
+__device__ __forceinline__ double inv_pow8(double w) {
+  const double r = 1.0 / w, r2 = r * r, r4 = r2 * r2;
+  return r4 * r4;
+}
+
 // the puncture operator at an inner point
 __device__ __forceinline__ double lop_point(const double *__restrict__ u, long q, int m, double cc, double cx,
                                             double a, double b) {
   const long mm = (long)m * m;
   return cc * u[q] + cx * (u[q - 1] + u[q + 1]) + cx * (u[q - m] + u[q + m]) + cx * (u[q - mm] + u[q + mm]) +
-         b * pow(1.0 + a * (1.0 + u[q]), -7.0);
+         b * inv_pow7(1.0 + a * (1.0 + u[q]));
 }
 
-// one Jacobi sweep un = uo + (f - L uo)/L_ii on inner points (Lpuncture_GS)
+// The boundary condition fused into the kernel that produces the inner
+// values it reads.  Set_boundary_robin writes u[b] = u[n] (1-c)/(1+c) (or
+// -u[n] for the Dirichlet correction) from the boundary point's inward normal
+// neighbour n, which is always an inner point.  A fused kernel runs np + nb
+// threads: thread q < np computes inner point q, thread np + t recomputes the
+// value of the normal neighbour of boundary point t with the same
+// arithmetic and writes the boundary value from it.  Out-of-place kernels
+// only (the recomputation reads the kernel's inputs, never its outputs), so
+// the result is bit-identical to the kernel followed by robin_kernel.
+struct RobinFuse {
+  const int *bidx, *bnrm;
+  const double *c1, *c2;
+  int nb;         // 0: no boundary threads
+  int dirichlet;  // -u[n] instead of u[n] c1 / c2
+};
+
+// thread -> (point whose value is computed, boundary slot or -1); false past the end
+__device__ __forceinline__ bool fused_point(int t, int np, const RobinFuse &R, int &q, int &slot) {
+  if (t < np) {
+    q = t;
+    slot = -1;
+    return true;
+  }
+  if (t < np + R.nb) {
+    slot = t - np;
+    q = R.bnrm[slot];
+    return true;
+  }
+  return false;
+}
+__device__ __forceinline__ void fused_store(double *out, int q, int slot, double v, const RobinFuse &R) {
+  if (slot < 0) out[q] = v;
+  else out[R.bidx[slot]] = R.dirichlet ? -v : v * R.c1[slot] / R.c2[slot];
+}
+
+// one Jacobi sweep un = uo + (f - L uo)/L_ii on inner points (Lpuncture_GS),
+// followed by the Robin condition on un (relax.c:19-43 then robin.c:146-223)
 __global__ void jacobi_kernel(const double *__restrict__ uo, double *__restrict__ un, const double *__restrict__ f,
                               const double *__restrict__ a, const double *__restrict__ b, int m, double cx,
-                              const int *__restrict__ done) {
+                              RobinFuse R, const int *__restrict__ done) {
   if (done && *done) return;
-  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long np = (long)m * m * m;
-  if (q >= np) return;
-  const int i = q % m, j = (q / m) % m, k = q / ((long)m * m);
+  int q, slot;
+  if (!fused_point(blockIdx.x * blockDim.x + threadIdx.x, m * m * m, R, q, slot)) return;
+  const int i = q % m, j = (q / m) % m, k = q / (m * m);
   if (!inner(i, j, k, m)) return;
   const double cc = -2.0 * (cx + cx + cx);
   const double aq = a[q], bq = b[q], uq = uo[q];
   const double lu = lop_point(uo, q, m, cc, cx, aq, bq);
-  const double lii = cc - 7.0 * bq * aq * pow(1.0 + aq * (1.0 + uq), -8.0);
-  un[q] = uq + (f[q] - lu) / lii;
+  const double lii = cc - 7.0 * bq * aq * inv_pow8(1.0 + aq * (1.0 + uq));
+  fused_store(un, q, slot, uq + (f[q] - lu) / lii, R);
 }
 
 // lu = L u on inner points (Lpuncture_nonlin, after its Robin call)
 __global__ void lop_kernel(const double *__restrict__ u, double *__restrict__ lu, const double *__restrict__ a,
                            const double *__restrict__ b, int m, double cx, const int *__restrict__ done) {
   if (done && *done) return;
-  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long np = (long)m * m * m;
-  if (q >= np) return;
-  const int i = q % m, j = (q / m) % m, k = q / ((long)m * m);
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= m * m * m) return;
+  const int i = q % m, j = (q / m) % m, k = q / (m * m);
   if (!inner(i, j, k, m)) return;
   lu[q] = lop_point(u, q, m, -2.0 * (cx + cx + cx), cx, a[q], b[q]);
 }
@@ -109,11 +155,11 @@ __global__ void residual_partial_kernel(const double *__restrict__ u, const doub
                                         const double *__restrict__ a, const double *__restrict__ b, int m,
                                         double cx, double *partial, const int *__restrict__ done) {
   if (done && *done) return;
-  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
   const long np = (long)m * m * m;
   double s = 0.0;
   if (q < np) {
-    const int i = q % m, j = (q / m) % m, k = q / ((long)m * m);
+    const int i = q % m, j = (q / m) % m, k = q / (m * m);
     if (inner(i, j, k, m)) {
       const double r = lop_point(u, q, m, -2.0 * (cx + cx + cx), cx, a[q], b[q]) - f[q];
       s = r * r;
@@ -158,18 +204,20 @@ __global__ void residual_final_kernel(const double *__restrict__ partial, int np
 }
 
 // 8-point average of the fine children of inner coarse points
+// (mg_restrict_var), with the Robin condition on the result when R.nb > 0
 __global__ void restrict_kernel(const double *__restrict__ fv, double *__restrict__ cv, int mf, int mc, int off,
-                                const int *__restrict__ done) {
+                                RobinFuse R, const int *__restrict__ done) {
   if (done && *done) return;
-  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long np = (long)mc * mc * mc;
-  if (q >= np) return;
-  const int I = q % mc, J = (q / mc) % mc, K = q / ((long)mc * mc);
+  int q, slot;
+  if (!fused_point(blockIdx.x * blockDim.x + threadIdx.x, mc * mc * mc, R, q, slot)) return;
+  const int I = q % mc, J = (q / mc) % mc, K = q / (mc * mc);
   if (!inner(I, J, K, mc)) return;
   const long mf2 = (long)mf * mf;
   const long f0 = (long)(2 * I - off) + mf * (long)(2 * J - off) + mf2 * (long)(2 * K - off);
-  cv[q] = 0.125 * (fv[f0] + fv[f0 + 1 + mf + mf2] + fv[f0 + 1] + fv[f0 + mf] + fv[f0 + mf2] + fv[f0 + 1 + mf] +
-                   fv[f0 + 1 + mf2] + fv[f0 + mf + mf2]);
+  fused_store(cv, q, slot,
+              0.125 * (fv[f0] + fv[f0 + 1 + mf + mf2] + fv[f0 + 1] + fv[f0 + mf] + fv[f0 + mf2] + fv[f0 + 1 + mf] +
+                       fv[f0 + 1 + mf2] + fv[f0 + mf + mf2]),
+              R);
 }
 
 // FAS coarse right-hand side at inner coarse points (finetocoarse):
@@ -179,10 +227,9 @@ __global__ void coarse_rhs_kernel(const double *__restrict__ luh, const double *
                                   const double *__restrict__ aH, const double *__restrict__ bH, int mf, int mc,
                                   int off, double cxH, const int *__restrict__ done) {
   if (done && *done) return;
-  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long np = (long)mc * mc * mc;
-  if (q >= np) return;
-  const int I = q % mc, J = (q / mc) % mc, K = q / ((long)mc * mc);
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= mc * mc * mc) return;
+  const int I = q % mc, J = (q / mc) % mc, K = q / (mc * mc);
   if (!inner(I, J, K, mc)) return;
   const long mf2 = (long)mf * mf;
   const long f0 = (long)(2 * I - off) + mf * (long)(2 * J - off) + mf2 * (long)(2 * K - off);
@@ -201,12 +248,12 @@ __global__ void copy_kernel(const double *__restrict__ s, double *__restrict__ d
   if (q < n) d[q] = s[q];
 }
 __global__ void sub_inner_kernel(const double *__restrict__ x, const double *__restrict__ y, double *__restrict__ r,
-                                 int m, const int *__restrict__ done) {
+                                 int m, RobinFuse R, const int *__restrict__ done) {
   if (done && *done) return;
-  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= (long)m * m * m) return;
-  const int i = q % m, j = (q / m) % m, k = q / ((long)m * m);
-  if (inner(i, j, k, m)) r[q] = x[q] - y[q];
+  int q, slot;
+  if (!fused_point(blockIdx.x * blockDim.x + threadIdx.x, m * m * m, R, q, slot)) return;
+  const int i = q % m, j = (q / m) % m, k = q / (m * m);
+  if (inner(i, j, k, m)) fused_store(r, q, slot, x[q] - y[q], R);
 }
 
 // trilinear prolongation of the coarse correction, added to the inner fine
@@ -216,9 +263,9 @@ __global__ void prolong_add_kernel(const double *__restrict__ cv, double *__rest
                                    double fx0, double fdx, double cx0, double cdx, int add,
                                    const int *__restrict__ done) {
   if (done && *done) return;
-  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= (long)mf * mf * mf) return;
-  const int i = q % mf, j = (q / mf) % mf, k = q / ((long)mf * mf);
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= mf * mf * mf) return;
+  const int i = q % mf, j = (q / mf) % mf, k = q / (mf * mf);
   if (!inner(i, j, k, mf)) return;
   const double xf = fx0 + i * fdx, yf = fx0 + j * fdx, zf = fx0 + k * fdx;
   const int ci = (int)((xf - cx0) / cdx), cj = (int)((yf - cx0) / cdx), ck = (int)((zf - cx0) / cdx);
@@ -246,7 +293,7 @@ __device__ double block_residual(const double *u, const double *f, const double 
   double s = 0.0;
   long n = 0;
   for (long q = threadIdx.x; q < np; q += blockDim.x) {
-    const int i = q % m, j = (q / m) % m, k = q / ((long)m * m);
+    const int i = q % m, j = (q / m) % m, k = q / (m * m);
     if (!inner(i, j, k, m)) continue;
     const double r = lop_point(u, q, m, -2.0 * (cx + cx + cx), cx, a[q], b[q]) - f[q];
     s += r * r;
@@ -275,10 +322,10 @@ __global__ void exact_solve_kernel(double *u, double *u2, const double *f, const
   for (i = 1; i <= nmax; ++i) {
     const double cc = -2.0 * (cx + cx + cx);
     for (long q = threadIdx.x; q < np; q += blockDim.x) {
-      const int ii = q % m, jj = (q / m) % m, kk = q / ((long)m * m);
+      const int ii = q % m, jj = (q / m) % m, kk = q / (m * m);
       if (!inner(ii, jj, kk, m)) { un[q] = uo[q]; continue; }
       const double lu = lop_point(uo, q, m, cc, cx, a[q], b[q]);
-      const double lii = cc - 7.0 * b[q] * a[q] * pow(1.0 + a[q] * (1.0 + uo[q]), -8.0);
+      const double lii = cc - 7.0 * b[q] * a[q] * inv_pow8(1.0 + a[q] * (1.0 + uo[q]));
       un[q] = uo[q] + (f[q] - lu) / lii;
     }
     __syncthreads();
@@ -296,6 +343,79 @@ __global__ void exact_solve_kernel(double *u, double *u2, const double *f, const
     __syncthreads();
   }
   if (threadIdx.x == 0) st->exact_sweeps = i;
+}
+
+// The coarsest solve by one warp with the whole level in shared memory
+// (levels of up to NRGPU_MG_WARP_SOLVE_MAX points): the sweeps, Robin
+// updates and residual tests of exact_solve_kernel, synchronised by
+// __syncwarp instead of block barriers and global-memory round trips.  The
+// coarsest level is a handful of inner points (8 on the 4^3 level) swept up
+// to exact_nmax times per V cycle, so the sweep's latency is the cost.
+constexpr int NRGPU_MG_WARP_SOLVE_MAX = 1000;
+__global__ void __launch_bounds__(32) exact_solve_warp_kernel(double *u, const double *f, const double *a,
+                                                              const double *b, int m, double cx, const int *bidx,
+                                                              const int *bnrm, const double *c1, const double *c2,
+                                                              int nb, int nmin, int nmax, double tol10, MgStatus *st) {
+  if (st->done) return;
+  extern __shared__ double sm[];
+  const int np = m * m * m, lane = threadIdx.x;
+  double *su = sm, *sv = su + np, *sa = sv + np, *sb = sa + np, *sf = sb + np, *sc1 = sf + np, *sc2 = sc1 + nb;
+  int *sbi = (int *)(sc2 + nb), *sbn = sbi + nb;
+  for (int q = lane; q < np; q += 32) {
+    su[q] = u[q];
+    sa[q] = a[q];
+    sb[q] = b[q];
+    sf[q] = f[q];
+  }
+  for (int t = lane; t < nb; t += 32) {
+    sc1[t] = c1[t];
+    sc2[t] = c2[t];
+    sbi[t] = bidx[t];
+    sbn[t] = bnrm[t];
+  }
+  __syncwarp();
+  // findres applies the Robin condition to u first (Lpuncture_nonlin)
+  for (int t = lane; t < nb; t += 32) su[sbi[t]] = su[sbn[t]] * sc1[t] / sc2[t];
+  __syncwarp();
+  const int mi = m - 2, ni = mi * mi * mi;
+  const double cc = -2.0 * (cx + cx + cx);
+  double *uo = su, *un = sv;
+  int it;
+  for (it = 1; it <= nmax; ++it) {
+    for (int p = lane; p < ni; p += 32) {
+      const int q = (1 + p % mi) + m * ((1 + (p / mi) % mi) + m * (1 + p / (mi * mi)));
+      const double aq = sa[q], bq = sb[q], uq = uo[q];
+      const double lu = lop_point(uo, q, m, cc, cx, aq, bq);
+      const double lii = cc - 7.0 * bq * aq * inv_pow8(1.0 + aq * (1.0 + uq));
+      un[q] = uq + (sf[q] - lu) / lii;
+    }
+    __syncwarp();
+    // every point outside the inner cube is a boundary point: the Robin
+    // condition writes all of them from the new inner values
+    for (int t = lane; t < nb; t += 32) un[sbi[t]] = un[sbn[t]] * sc1[t] / sc2[t];
+    __syncwarp();
+    double *tt = uo;
+    uo = un;
+    un = tt;
+    if (it >= nmin) {
+      double s = 0.0;
+      for (int p = lane; p < ni; p += 32) {
+        const int q = (1 + p % mi) + m * ((1 + (p / mi) % mi) + m * (1 + p / (mi * mi)));
+        const double r = lop_point(uo, q, m, cc, cx, sa[q], sb[q]) - sf[q];
+        s += r * r;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (sqrt(s / (double)ni) < tol10) break;
+    }
+  }
+  for (int q = lane; q < np; q += 32) u[q] = uo[q];
+  if (lane == 0) st->exact_sweeps = it;
+}
+
+static size_t warp_solve_smem(int m, int nb) {
+  const size_t np = (size_t)m * m * m;
+  return sizeof(double) * (5 * np + 2 * (size_t)nb) + sizeof(int) * 2 * (size_t)nb;
 }
 
 __global__ void robin_factors_kernel(const int *bidx, const int *bnrm, double *c1, double *c2, int nb, int m, double x0,
@@ -480,6 +600,12 @@ extern "C" int nrgpu_mg_create(int m, double dx, const nrgpu_mg_params *p, nrgpu
     robin_factors_kernel<<<nblk(L.nb), RB>>>(L.bidx, L.bnrm, L.bc1, L.bc2, L.nb, L.m, L.x0, L.dx, p->falloff);
     for (double *z : {L.u, L.u2, L.v, L.w, L.f, L.a, L.b}) cudaMemset(z, 0, by);
   }
+  if (ok && M->lv[0].np <= NRGPU_MG_WARP_SOLVE_MAX) {
+    const size_t sm = warp_solve_smem(M->lv[0].m, M->lv[0].nb);
+    if (sm > 48 * 1024)
+      ok = cudaFuncSetAttribute(exact_solve_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) ==
+           cudaSuccess;
+  }
   M->npartial = (int)nblk(M->lv[nl - 1].np);
   ok = ok && cudaStreamCreateWithFlags(&M->stream, cudaStreamNonBlocking) == cudaSuccess &&
        cudaMalloc(&M->st, sizeof(MgStatus)) == cudaSuccess &&
@@ -497,15 +623,17 @@ extern "C" int nrgpu_mg_create(int m, double dx, const nrgpu_mg_params *p, nrgpu
 static void robin_u(nrgpu_mg *M, MgLevel &L, double *u, const int *done) {
   robin_kernel<<<nblk(L.nb), RB, 0, M->stream>>>(u, L.bidx, L.bnrm, L.bc1, L.bc2, L.nb, 0, done);
 }
-static void robin_d(nrgpu_mg *M, MgLevel &L, double *u, const int *done) {
-  robin_kernel<<<nblk(L.nb), RB, 0, M->stream>>>(u, L.bidx, L.bnrm, L.bc1, L.bc2, L.nb, 1, done);
-}
 static double cxof(const MgLevel &L) { return 1 / (L.dx * L.dx); }
+static RobinFuse robin_of(const MgLevel &L, int dirichlet) {
+  return RobinFuse{L.bidx, L.bnrm, L.bc1, L.bc2, L.nb, dirichlet};
+}
+static const RobinFuse kNoRobin = {nullptr, nullptr, nullptr, nullptr, 0, 0};
 
+// Jacobi sweeps, each with its Robin condition fused in
 static void sweeps(nrgpu_mg *M, MgLevel &L, int n, const int *done) {
   for (int s = 0; s < n; ++s) {
-    jacobi_kernel<<<nblk(L.np), RB, 0, M->stream>>>(L.u, L.u2, L.f, L.a, L.b, L.m, cxof(L), done);
-    robin_u(M, L, L.u2, done);
+    jacobi_kernel<<<nblk(L.np + L.nb), RB, 0, M->stream>>>(L.u, L.u2, L.f, L.a, L.b, L.m, cxof(L), robin_of(L, 0),
+                                                           done);
     std::swap(L.u, L.u2);
   }
 }
@@ -518,25 +646,31 @@ constexpr int kChildOff = 1;
 static void vcycle(nrgpu_mg *M, int l, const int *done) {
   MgLevel &h = M->lv[l];
   if (l == 0) {
-    exact_solve_kernel<<<1, 256, 0, M->stream>>>(h.u, h.u2, h.f, h.a, h.b, h.m, cxof(h), h.bidx, h.bnrm, h.bc1,
-                                                h.bc2, h.nb, M->p.exact_nmin, M->p.exact_nmax, M->p.tol / 10, M->st);
+    if (h.np <= NRGPU_MG_WARP_SOLVE_MAX)
+      exact_solve_warp_kernel<<<1, 32, warp_solve_smem(h.m, h.nb), M->stream>>>(
+          h.u, h.f, h.a, h.b, h.m, cxof(h), h.bidx, h.bnrm, h.bc1, h.bc2, h.nb, M->p.exact_nmin, M->p.exact_nmax,
+          M->p.tol / 10, M->st);
+    else
+      exact_solve_kernel<<<1, 256, 0, M->stream>>>(h.u, h.u2, h.f, h.a, h.b, h.m, cxof(h), h.bidx, h.bnrm, h.bc1,
+                                                  h.bc2, h.nb, M->p.exact_nmin, M->p.exact_nmax, M->p.tol / 10,
+                                                  M->st);
     return;
   }
   MgLevel &H = M->lv[l - 1];
   const int off = kChildOff;
   double *const u_entry = h.u;
   sweeps(M, h, M->p.npre, done);
-  // finetocoarse
-  robin_u(M, h, h.u, done);
+  // finetocoarse: Lpuncture_nonlin's Robin call on u repeats what the last
+  // sweep wrote (boundary values from the same inner values), so it is only
+  // needed without pre-sweeps
+  if (M->p.npre == 0) robin_u(M, h, h.u, done);
   lop_kernel<<<nblk(h.np), RB, 0, M->stream>>>(h.u, h.v, h.a, h.b, h.m, cxof(h), done);
-  restrict_kernel<<<nblk(H.np), RB, 0, M->stream>>>(h.u, H.u, h.m, H.m, off, done);
-  robin_u(M, H, H.u, done);
+  restrict_kernel<<<nblk(H.np + H.nb), RB, 0, M->stream>>>(h.u, H.u, h.m, H.m, off, robin_of(H, 0), done);
   coarse_rhs_kernel<<<nblk(H.np), RB, 0, M->stream>>>(h.v, h.f, H.u, H.f, H.a, H.b, h.m, H.m, off, cxof(H), done);
   copy_kernel<<<nblk(H.np), RB, 0, M->stream>>>(H.u, H.w, H.np, done);
   vcycle(M, l - 1, done);
   // coarsetofine
-  sub_inner_kernel<<<nblk(H.np), RB, 0, M->stream>>>(H.u, H.w, H.v, H.m, done);
-  robin_d(M, H, H.v, done);
+  sub_inner_kernel<<<nblk(H.np + H.nb), RB, 0, M->stream>>>(H.u, H.w, H.v, H.m, robin_of(H, 1), done);
   prolong_add_kernel<<<nblk(h.np), RB, 0, M->stream>>>(H.v, h.u, h.m, H.m, h.x0, h.dx, H.x0, H.dx, 1, done);
   robin_u(M, h, h.u, done);
   sweeps(M, h, M->p.npost, done);
@@ -575,9 +709,9 @@ extern "C" int nrgpu_mg_solve(nrgpu_mg *M, const double *a, const double *b, dou
   for (int l = top; l > 0; --l) {
     MgLevel &h = M->lv[l], &H = M->lv[l - 1];
     const int off = kChildOff;
-    restrict_kernel<<<nblk(H.np), RB, 0, M->stream>>>(h.a, H.a, h.m, H.m, off, nullptr);
-    restrict_kernel<<<nblk(H.np), RB, 0, M->stream>>>(h.b, H.b, h.m, H.m, off, nullptr);
-    restrict_kernel<<<nblk(H.np), RB, 0, M->stream>>>(h.u, H.u, h.m, H.m, off, nullptr);
+    restrict_kernel<<<nblk(H.np), RB, 0, M->stream>>>(h.a, H.a, h.m, H.m, off, kNoRobin, nullptr);
+    restrict_kernel<<<nblk(H.np), RB, 0, M->stream>>>(h.b, H.b, h.m, H.m, off, kNoRobin, nullptr);
+    restrict_kernel<<<nblk(H.np), RB, 0, M->stream>>>(h.u, H.u, h.m, H.m, off, kNoRobin, nullptr);
   }
   for (int l = 0; l <= top; ++l) {
     MgLevel &L = M->lv[l];
