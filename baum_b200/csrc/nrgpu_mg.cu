@@ -376,19 +376,39 @@ __global__ void __launch_bounds__(32) exact_solve_warp_kernel(double *u, const d
   __syncwarp();
   // findres applies the Robin condition to u first (Lpuncture_nonlin)
   for (int t = lane; t < nb; t += 32) su[sbi[t]] = su[sbn[t]] * sc1[t] / sc2[t];
-  __syncwarp();
   const int mi = m - 2, ni = mi * mi * mi;
+  int *sq = sbn + nb;  // the inner points' indices
+  for (int p = lane; p < ni; p += 32) sq[p] = (1 + p % mi) + m * ((1 + (p / mi) % mi) + m * (1 + p / (mi * mi)));
+  __syncwarp();
   const double cc = -2.0 * (cx + cx + cx);
   double *uo = su, *un = sv;
+  // Pass `it` evaluates L u_{it-1} once: its residual is the test after
+  // sweep it-1 (from nmin sweeps on), and the same value gives sweep it.
+  // This is the reference's sweep-then-test loop with the operator of the
+  // test shared by the next sweep; results are identical.
   int it;
-  for (it = 1; it <= nmax; ++it) {
+  for (it = 1; it <= nmax + 1; ++it) {
+    double s = 0.0;
     for (int p = lane; p < ni; p += 32) {
-      const int q = (1 + p % mi) + m * ((1 + (p / mi) % mi) + m * (1 + p / (mi * mi)));
+      const int q = sq[p];
       const double aq = sa[q], bq = sb[q], uq = uo[q];
       const double lu = lop_point(uo, q, m, cc, cx, aq, bq);
-      const double lii = cc - 7.0 * bq * aq * inv_pow8(1.0 + aq * (1.0 + uq));
-      un[q] = uq + (sf[q] - lu) / lii;
+      const double r = lu - sf[q];
+      s += r * r;
+      if (it <= nmax) {
+        const double lii = cc - 7.0 * bq * aq * inv_pow8(1.0 + aq * (1.0 + uq));
+        un[q] = uq + (sf[q] - lu) / lii;
+      }
     }
+    if (it - 1 >= nmin && it > 1) {  // the first test follows the first sweep
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (sqrt(s / (double)ni) < tol10) {
+        it -= 1;  // sweeps done
+        break;
+      }
+    }
+    if (it > nmax) break;  // nmax sweeps and no pass: the loop ends at nmax + 1
     __syncwarp();
     // every point outside the inner cube is a boundary point: the Robin
     // condition writes all of them from the new inner values
@@ -397,25 +417,15 @@ __global__ void __launch_bounds__(32) exact_solve_warp_kernel(double *u, const d
     double *tt = uo;
     uo = un;
     un = tt;
-    if (it >= nmin) {
-      double s = 0.0;
-      for (int p = lane; p < ni; p += 32) {
-        const int q = (1 + p % mi) + m * ((1 + (p / mi) % mi) + m * (1 + p / (mi * mi)));
-        const double r = lop_point(uo, q, m, cc, cx, sa[q], sb[q]) - sf[q];
-        s += r * r;
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (sqrt(s / (double)ni) < tol10) break;
-    }
   }
+  __syncwarp();
   for (int q = lane; q < np; q += 32) u[q] = uo[q];
   if (lane == 0) st->exact_sweeps = it;
 }
 
 static size_t warp_solve_smem(int m, int nb) {
-  const size_t np = (size_t)m * m * m;
-  return sizeof(double) * (5 * np + 2 * (size_t)nb) + sizeof(int) * 2 * (size_t)nb;
+  const size_t np = (size_t)m * m * m, ni = (size_t)(m - 2) * (m - 2) * (m - 2);
+  return sizeof(double) * (5 * np + 2 * (size_t)nb) + sizeof(int) * (2 * (size_t)nb + ni);
 }
 
 __global__ void robin_factors_kernel(const int *bidx, const int *bnrm, double *c1, double *c2, int nb, int m, double x0,
