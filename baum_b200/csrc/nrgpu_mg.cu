@@ -139,17 +139,6 @@ __global__ void jacobi_kernel(const double *__restrict__ uo, double *__restrict_
   fused_store(un, q, slot, uq + (f[q] - lu) / lii, R);
 }
 
-// lu = L u on inner points (Lpuncture_nonlin, after its Robin call)
-__global__ void lop_kernel(const double *__restrict__ u, double *__restrict__ lu, const double *__restrict__ a,
-                           const double *__restrict__ b, int m, double cx, const int *__restrict__ done) {
-  if (done && *done) return;
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= m * m * m) return;
-  const int i = q % m, j = (q / m) % m, k = q / (m * m);
-  if (!inner(i, j, k, m)) return;
-  lu[q] = lop_point(u, q, m, -2.0 * (cx + cx + cx), cx, a[q], b[q]);
-}
-
 // block partial sums of (L u - f)^2 over inner points
 __global__ void residual_partial_kernel(const double *__restrict__ u, const double *__restrict__ f,
                                         const double *__restrict__ a, const double *__restrict__ b, int m,
@@ -220,25 +209,50 @@ __global__ void restrict_kernel(const double *__restrict__ fv, double *__restric
               R);
 }
 
-// FAS coarse right-hand side at inner coarse points (finetocoarse):
-// fH = R fh + (L uH - R L uh), lu_h = L uh already on the fine level
-__global__ void coarse_rhs_kernel(const double *__restrict__ luh, const double *__restrict__ fh,
-                                  const double *__restrict__ uH, double *__restrict__ fH,
-                                  const double *__restrict__ aH, const double *__restrict__ bH, int mf, int mc,
-                                  int off, double cxH, const int *__restrict__ done) {
+// finetocoarse (solve.c) in one pass over the coarse points: uH = R uh
+// (mg_restrict_var) with the Robin condition, and the two restrictions of
+// the FAS right-hand side, R fh into fH and R L uh into vH, with L uh
+// (Lpuncture_nonlin) evaluated at the eight children.  The children of the
+// inner coarse points are exactly the inner fine points, so every fine
+// operator value is computed once; the sums run in the order of
+// mg_restrict_var's eight terms.
+__global__ void fine_to_coarse_kernel(const double *__restrict__ uh, const double *__restrict__ fh,
+                                      const double *__restrict__ ah, const double *__restrict__ bh,
+                                      double *__restrict__ uH, double *__restrict__ RfH, double *__restrict__ RluH,
+                                      int mf, int mc, int off, double cxh, RobinFuse R, const int *__restrict__ done) {
   if (done && *done) return;
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= mc * mc * mc) return;
+  int q, slot;
+  if (!fused_point(blockIdx.x * blockDim.x + threadIdx.x, mc * mc * mc, R, q, slot)) return;
   const int I = q % mc, J = (q / mc) % mc, K = q / (mc * mc);
   if (!inner(I, J, K, mc)) return;
   const long mf2 = (long)mf * mf;
   const long f0 = (long)(2 * I - off) + mf * (long)(2 * J - off) + mf2 * (long)(2 * K - off);
-  const double Rlu = 0.125 * (luh[f0] + luh[f0 + 1 + mf + mf2] + luh[f0 + 1] + luh[f0 + mf] + luh[f0 + mf2] +
-                              luh[f0 + 1 + mf] + luh[f0 + 1 + mf2] + luh[f0 + mf + mf2]);
-  const double Rf = 0.125 * (fh[f0] + fh[f0 + 1 + mf + mf2] + fh[f0 + 1] + fh[f0 + mf] + fh[f0 + mf2] +
-                             fh[f0 + 1 + mf] + fh[f0 + 1 + mf2] + fh[f0 + mf + mf2]);
+  const long c[8] = {f0, f0 + 1 + mf + mf2, f0 + 1, f0 + mf, f0 + mf2, f0 + 1 + mf, f0 + 1 + mf2, f0 + mf + mf2};
+  fused_store(uH, q, slot,
+              0.125 * (uh[c[0]] + uh[c[1]] + uh[c[2]] + uh[c[3]] + uh[c[4]] + uh[c[5]] + uh[c[6]] + uh[c[7]]), R);
+  if (slot >= 0) return;
+  const double cch = -2.0 * (cxh + cxh + cxh);
+  double lu[8];
+#pragma unroll
+  for (int n = 0; n < 8; ++n) lu[n] = lop_point(uh, c[n], mf, cch, cxh, ah[c[n]], bh[c[n]]);
+  RluH[q] = 0.125 * (lu[0] + lu[1] + lu[2] + lu[3] + lu[4] + lu[5] + lu[6] + lu[7]);
+  RfH[q] = 0.125 * (fh[c[0]] + fh[c[1]] + fh[c[2]] + fh[c[3]] + fh[c[4]] + fh[c[5]] + fh[c[6]] + fh[c[7]]);
+}
+
+// the FAS coarse right-hand side fH = R fh + (L uH - R L uh) at inner coarse
+// points (fH holds R fh, RluH holds R L uh), and wH = uH at every point
+__global__ void coarse_rhs_kernel(const double *__restrict__ uH, double *__restrict__ fH,
+                                  const double *__restrict__ RluH, double *__restrict__ wH,
+                                  const double *__restrict__ aH, const double *__restrict__ bH, int mc, double cxH,
+                                  const int *__restrict__ done) {
+  if (done && *done) return;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= mc * mc * mc) return;
+  wH[q] = uH[q];
+  const int I = q % mc, J = (q / mc) % mc, K = q / (mc * mc);
+  if (!inner(I, J, K, mc)) return;
   const double luH = lop_point(uH, q, mc, -2.0 * (cxH + cxH + cxH), cxH, aH[q], bH[q]);
-  fH[q] = Rf + (luH - Rlu);
+  fH[q] = fH[q] + (luH - RluH[q]);
 }
 
 // wH = uH (all points), vH = uH - wH helpers
@@ -674,10 +688,9 @@ static void vcycle(nrgpu_mg *M, int l, const int *done) {
   // sweep wrote (boundary values from the same inner values), so it is only
   // needed without pre-sweeps
   if (M->p.npre == 0) robin_u(M, h, h.u, done);
-  lop_kernel<<<nblk(h.np), RB, 0, M->stream>>>(h.u, h.v, h.a, h.b, h.m, cxof(h), done);
-  restrict_kernel<<<nblk(H.np + H.nb), RB, 0, M->stream>>>(h.u, H.u, h.m, H.m, off, robin_of(H, 0), done);
-  coarse_rhs_kernel<<<nblk(H.np), RB, 0, M->stream>>>(h.v, h.f, H.u, H.f, H.a, H.b, h.m, H.m, off, cxof(H), done);
-  copy_kernel<<<nblk(H.np), RB, 0, M->stream>>>(H.u, H.w, H.np, done);
+  fine_to_coarse_kernel<<<nblk(H.np + H.nb), RB, 0, M->stream>>>(h.u, h.f, h.a, h.b, H.u, H.f, H.v, h.m, H.m, off,
+                                                                 cxof(h), robin_of(H, 0), done);
+  coarse_rhs_kernel<<<nblk(H.np), RB, 0, M->stream>>>(H.u, H.f, H.v, H.w, H.a, H.b, H.m, cxof(H), done);
   vcycle(M, l - 1, done);
   // coarsetofine
   sub_inner_kernel<<<nblk(H.np + H.nb), RB, 0, M->stream>>>(H.u, H.w, H.v, H.m, robin_of(H, 1), done);
