@@ -597,12 +597,39 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--case", default="c1", choices=["c1", "c1-step", "z4c160"],
+    ap.add_argument("--case", default="c1", choices=["c1", "c1-step", "mg", "z4c160"],
                     help="c1: the benchmark line; c1-step: only the 64^3 BSSN RK4 steps and the rhs "
-                         "launches of that line (for profiling); z4c160: the 160^3 Z4c box alone")
+                         "launches of that line (for profiling); mg: only the 130^3 multigrid solve of the "
+                         "first seeded binary (for profiling); z4c160: the 160^3 Z4c box alone")
+    ap.add_argument("--mg-cycles", type=int, default=0,
+                    help="with --case mg: run exactly this many V cycles from the finest level (profiling)")
     args = ap.parse_args()
     if args.case == "z4c160":
         run_z4c160(args)
+        return
+    if args.case == "mg":
+        import torch
+        from baum_b200 import build
+        build.build()
+        torch.cuda.set_device(0)
+        if args.mg_cycles:
+            # profiling: exactly K V cycles from the finest level (no full-V
+            # start, tolerance 0): the first kernels are the 130^3 sweeps
+            from baum_b200 import abi, punctures
+            mg = punctures.Multigrid(130, 0.125, abi.mg_params(fullV=0, tol=0.0, vcycle_nmax=args.mg_cycles))
+            a, bb = mg.coefficients(mg_binaries(1)[0])
+            u = torch.zeros(130 ** 3, dtype=torch.float64, device="cuda")
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            n, res = mg.solve(a, bb, u)
+            torch.cuda.synchronize()
+            print(json.dumps({"case": "mg", "vcycles": n, "ms": 1e3 * (time.perf_counter() - t0), "residual": res}))
+            mg.close()
+            return
+        r = gpu_mg(130, 0.125, mg_binaries(1))[0]
+        print(json.dumps({"case": "mg", "workload": "binary punctures, Bowen-York, 130^3 points, dx=0.125, "
+                                                     "tol 1e-10 RMS, full-V", "seed": MG_BINARIES_SEED, **r,
+                          "ms_per_vcycle": r["ms"] / max(1, r["vcycles"])}))
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
