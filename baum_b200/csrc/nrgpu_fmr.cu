@@ -15,6 +15,7 @@
 // reference's values bit for bit from the same inputs; nothing is staged
 // through global temporaries.
 #include <string.h>
+#include <algorithm>
 #include <vector>
 #include "nrgpu_level.cuh"
 
@@ -145,20 +146,28 @@ __global__ void ti_finish_kernel(Ptrs u, double *upp, double c, long np, int nv)
 
 }  // namespace
 
+// one fine box and the coarse box that holds it (BAM's box->pr): the
+// restriction and prolongation geometry of the pair
+struct FmrPair {
+  int fbox, cbox;
+  bool has_r, has_p;
+  RGeom rg;
+  PGeom pg;
+  int nr, npro;
+};
+
 struct nrgpu_fmr {
   int nl, nv;
   nrgpu_fmr_params p;
   nrgpu_level *L[kMaxLevels];
-  Box3 box[kMaxLevels];
-  double x0[kMaxLevels][3], dx[kMaxLevels][3];
+  std::vector<Box3> box[kMaxLevels];                   // the level's boxes
+  std::vector<double> bx0[kMaxLevels];                 // their origins, 3 per box
+  double dx[kMaxLevels][3];
   double dt[kMaxLevels];
   nrgpu_bssn_params bp[kMaxLevels];
   nrgpu_z4_params zp[kMaxLevels];
-  std::vector<double> fp[kMaxLevels], fr[kMaxLevels];  // flagprolong, flagrestrict
-  bool has_r[kMaxLevels], has_p[kMaxLevels];           // per fine level
-  RGeom rg[kMaxLevels];
-  PGeom pg[kMaxLevels];
-  int nr[kMaxLevels], npro[kMaxLevels];
+  std::vector<double> fp[kMaxLevels], fr[kMaxLevels];  // flagprolong, flagrestrict (level-wide)
+  std::vector<FmrPair> pairs[kMaxLevels];              // per fine level, one per fine box
   double *up[kMaxLevels], *upp[kMaxLevels];  // u(n-1) copy and time interpolant
   int iteration[kMaxLevels];
   // graph of one coarse step for one set of state pointers
@@ -191,23 +200,49 @@ int point_index(double X0, double dX, double x0, double dx, int i) { return (int
 
 long hat(const Box3 &b, int i, int j, int k) { return b.off + i + (long)b.n[0] * (j + (long)b.n[1] * k); }
 
-// setRPflags (flag.c:122-255) between level l-1 and l; then the bounding
-// boxes of restrict_varlist_boxtobox_N and prolong_varlist_boxtobox_N
-int setup_pair(nrgpu_fmr *F, int l) {
-  const Box3 &f = F->box[l], &c = F->box[l - 1];
+// the coarse box of level l-1 that holds every parent point of fine box fb
+int parent_box(const nrgpu_fmr *F, int l, int fb) {
+  const Box3 &f = F->box[l][fb];
+  const double *fx0 = &F->bx0[l][3 * fb];
+  for (int cb = 0; cb < (int)F->box[l - 1].size(); ++cb) {
+    const Box3 &c = F->box[l - 1][cb];
+    const double *cx0 = &F->bx0[l - 1][3 * cb];
+    bool ok = true;
+    for (int d = 0; d < 3 && ok; ++d) {
+      const int lo = parent_index(cx0[d], F->dx[l - 1][d], fx0[d], F->dx[l][d], 0);
+      const int hi = parent_index(cx0[d], F->dx[l - 1][d], fx0[d], F->dx[l][d], f.n[d] - 1);
+      ok = lo >= 0 && hi < c.n[d];
+    }
+    if (ok) return cb;
+  }
+  return -1;
+}
+
+// setRPflags (flag.c:122-255) of one fine box and its parent box, then the
+// bounding boxes of restrict_varlist_boxtobox_N and prolong_varlist_boxtobox_N
+// (interpolate_boxtobox_N.c:870-1370, forallboxes(lf)).  With several fine
+// boxes the reference sets each box's flagrestrict on a ghost parent of that
+// box; here each pair's coarse flags are kept apart (cr) for its restriction
+// box, and their union goes to the level's flagrestrict.
+int setup_one_pair(nrgpu_fmr *F, int l, int fbi, std::vector<double> &cr) {
+  FmrPair P;
+  P.fbox = fbi;
+  P.cbox = parent_box(F, l, fbi);
+  if (P.cbox < 0) return nrgpu_set_error(NRGPU_ERR_ARG, "box %d of level %d does not nest in level %d", fbi, l, l - 1);
+  const Box3 &f = F->box[l][fbi], &c = F->box[l - 1][P.cbox];
+  const double *fx0 = &F->bx0[l][3 * fbi], *cx0 = &F->bx0[l - 1][3 * P.cbox];
   const int nbuf = F->p.nbuffer, b = F->p.order_RP / 2;
   const long npf = (long)f.n[0] * f.n[1] * f.n[2];
-  std::vector<double> &fp = F->fp[l], &cr = F->fr[l - 1];
-  fp.assign(npf, 0.0);
-  cr.assign((size_t)c.n[0] * c.n[1] * c.n[2], 0.0);
+  std::vector<double> &fp = F->fp[l];
+  std::fill(cr.begin(), cr.end(), 0.0);
   for (int k = 0; k < f.n[2]; k++)
     for (int j = 0; j < f.n[1]; j++)
       for (int i = 0; i < f.n[0]; i++) {
         const int idx[3] = {i, j, k};
         long m[3];
         for (int d = 0; d < 3; d++) {
-          const double lo = F->x0[l][d], hi = F->x0[l][d] + (f.n[d] - 1) * F->dx[l][d];
-          const double x = F->x0[l][d] + idx[d] * F->dx[l][d];
+          const double lo = fx0[d], hi = fx0[d] + (f.n[d] - 1) * F->dx[l][d];
+          const double x = fx0[d] + idx[d] * F->dx[l][d];
           m[d] = npf;
           int n = (int)(1.5 + (x - lo) / F->dx[l][d]);
           if (n <= nbuf) m[d] = n;
@@ -216,32 +251,34 @@ int setup_pair(nrgpu_fmr *F, int l) {
         }
         long ii = m[0] < m[1] ? m[0] : m[1];
         ii = ii < m[2] ? ii : m[2];
-        fp[hat(f, i, j, k) - f.off] = ii < npf ? (double)ii : 0.0;
+        fp[hat(f, i, j, k)] = ii < npf ? (double)ii : 0.0;
       }
   for (int pass = 0; pass < 2; pass++)
     for (int k = 0; k < f.n[2]; k++)
       for (int j = 0; j < f.n[1]; j++)
         for (int i = 0; i < f.n[0]; i++) {
-          const int pi = parent_index(F->x0[l - 1][0], F->dx[l - 1][0], F->x0[l][0], F->dx[l][0], i);
-          const int pj = parent_index(F->x0[l - 1][1], F->dx[l - 1][1], F->x0[l][1], F->dx[l][1], j);
-          const int pk = parent_index(F->x0[l - 1][2], F->dx[l - 1][2], F->x0[l][2], F->dx[l][2], k);
-          if (pi < 0 || pj < 0 || pk < 0 || pi >= c.n[0] || pj >= c.n[1] || pk >= c.n[2])
-            return nrgpu_set_error(NRGPU_ERR_ARG, "level %d does not nest in level %d", l, l - 1);
-          const double p = fp[hat(f, i, j, k) - f.off];
-          double &r = cr[hat(c, pi, pj, pk) - c.off];
+          const int pi = parent_index(cx0[0], F->dx[l - 1][0], fx0[0], F->dx[l][0], i);
+          const int pj = parent_index(cx0[1], F->dx[l - 1][1], fx0[1], F->dx[l][1], j);
+          const int pk = parent_index(cx0[2], F->dx[l - 1][2], fx0[2], F->dx[l][2], k);
+          const double p = fp[hat(f, i, j, k)];
+          double &r = cr[hat(c, pi, pj, pk)];
           if (pass == 0 && p == 0) r = 3;
           if (pass == 1) {
             if (p >= 3) r = 2;
             else if (p == 2) r = 1;
           }
         }
-  // restriction box
+  for (int k = 0; k < c.n[2]; k++)
+    for (int j = 0; j < c.n[1]; j++)
+      for (int i = 0; i < c.n[0]; i++)
+        if (cr[hat(c, i, j, k)] != 0) F->fr[l - 1][hat(c, i, j, k)] = cr[hat(c, i, j, k)];
+  // restriction box (the parent box's points with this pair's flag >= 3)
   int ic[6] = {1 << 30, -(1 << 30), 1 << 30, -(1 << 30), 1 << 30, -(1 << 30)};
   long n = 0;
   for (int k = 0; k < c.n[2]; k++)
     for (int j = 0; j < c.n[1]; j++)
       for (int i = 0; i < c.n[0]; i++)
-        if (cr[hat(c, i, j, k) - c.off] >= 3) {
+        if (cr[hat(c, i, j, k)] >= 3) {
           const int idx[3] = {i, j, k};
           for (int d = 0; d < 3; d++) {
             ic[2 * d] = idx[d] < ic[2 * d] ? idx[d] : ic[2 * d];
@@ -249,22 +286,23 @@ int setup_pair(nrgpu_fmr *F, int l) {
           }
           n++;
         }
-  F->has_r[l] = n > 0;
+  P.has_r = n > 0;
+  P.nr = 0;
   if (n) {
-    RGeom &G = F->rg[l];
+    RGeom &G = P.rg;
     memcpy(G.ic, ic, sizeof ic);
     for (int d = 0; d < 3; d++) {
-      const int lo = point_index(F->x0[l][d], F->dx[l][d], F->x0[l - 1][d], F->dx[l - 1][d], ic[2 * d]) - b + 1;
-      const int hi = point_index(F->x0[l][d], F->dx[l][d], F->x0[l - 1][d], F->dx[l - 1][d], ic[2 * d + 1]) + b;
+      const int lo = point_index(fx0[d], F->dx[l][d], cx0[d], F->dx[l - 1][d], ic[2 * d]) - b + 1;
+      const int hi = point_index(fx0[d], F->dx[l][d], cx0[d], F->dx[l - 1][d], ic[2 * d + 1]) + b;
       if (lo < 0 || hi >= f.n[d])
         return nrgpu_set_error(NRGPU_ERR_ARG, "restriction: boxes too small (level %d)", l);
       G.if0[d] = lo;
     }
     lagrange(F->p.order_RP, F->p.order_RP / 2.0 - 0.5, G.w);
-    F->nr[l] = (ic[1] - ic[0] + 1) * (ic[3] - ic[2] + 1) * (ic[5] - ic[4] + 1);
+    P.nr = (ic[1] - ic[0] + 1) * (ic[3] - ic[2] + 1) * (ic[5] - ic[4] + 1);
   }
   // prolongation boxes
-  PGeom &P = F->pg[l];
+  PGeom &Q = P.pg;
   int fb[6] = {1 << 30, -(1 << 30), 1 << 30, -(1 << 30), 1 << 30, -(1 << 30)};
   int f0[6] = {1 << 30, -(1 << 30), 1 << 30, -(1 << 30), 1 << 30, -(1 << 30)};
   n = 0;
@@ -272,7 +310,7 @@ int setup_pair(nrgpu_fmr *F, int l) {
     for (int j = 0; j < f.n[1]; j++)
       for (int i = 0; i < f.n[0]; i++) {
         const int idx[3] = {i, j, k};
-        const double p = fp[hat(f, i, j, k) - f.off];
+        const double p = fp[hat(f, i, j, k)];
         int *bb = (p > 0 && nbuf >= p) ? fb : f0;
         if (bb == fb) n++;
         for (int d = 0; d < 3; d++) {
@@ -280,27 +318,42 @@ int setup_pair(nrgpu_fmr *F, int l) {
           bb[2 * d + 1] = idx[d] > bb[2 * d + 1] ? idx[d] : bb[2 * d + 1];
         }
       }
-  F->has_p[l] = n > 0;
+  P.has_p = n > 0;
+  P.npro = 0;
   if (n) {
-    memcpy(P.fb, fb, sizeof fb);
-    memcpy(P.f0, f0, sizeof f0);
+    memcpy(Q.fb, fb, sizeof fb);
+    memcpy(Q.f0, f0, sizeof f0);
     for (int d = 0; d < 3; d++) {
-      const int lo = point_index(F->x0[l - 1][d], F->dx[l - 1][d], F->x0[l][d], F->dx[l][d], fb[2 * d]) - b + 1;
-      const int hi = point_index(F->x0[l - 1][d], F->dx[l - 1][d], F->x0[l][d], F->dx[l][d], fb[2 * d + 1]) + b;
+      const int lo = point_index(cx0[d], F->dx[l - 1][d], fx0[d], F->dx[l][d], fb[2 * d]) - b + 1;
+      const int hi = point_index(cx0[d], F->dx[l - 1][d], fx0[d], F->dx[l][d], fb[2 * d + 1]) + b;
       if (lo < 0 || hi >= c.n[d])
         return nrgpu_set_error(NRGPU_ERR_ARG, "prolongation: boxes too small (level %d)", l);
       if ((fb[2 * d + 1] - fb[2 * d] + 1) % 2)
         return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "level %d is not made of whole parent cells", l);
       // the output pairs start on a lower child (fine point a quarter coarse
       // cell below its parent), as prolong_boxtobox_N assumes
-      if (point_index(F->x0[l - 1][d], F->dx[l - 1][d], F->x0[l][d], F->dx[l][d], fb[2 * d]) !=
-          parent_index(F->x0[l - 1][d], F->dx[l - 1][d], F->x0[l][d], F->dx[l][d], fb[2 * d]) - 1)
+      if (point_index(cx0[d], F->dx[l - 1][d], fx0[d], F->dx[l][d], fb[2 * d]) !=
+          parent_index(cx0[d], F->dx[l - 1][d], fx0[d], F->dx[l][d], fb[2 * d]) - 1)
         return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "level %d is not aligned with its parent's cells", l);
-      P.cs[d] = lo;
+      Q.cs[d] = lo;
     }
-    lagrange(F->p.order_RP, F->p.order_RP / 2.0 - 0.25, P.c1);
-    lagrange(F->p.order_RP, F->p.order_RP / 2.0 - 0.75, P.c2);
-    F->npro[l] = (fb[1] - fb[0] + 1) * (fb[3] - fb[2] + 1) * (fb[5] - fb[4] + 1);
+    lagrange(F->p.order_RP, F->p.order_RP / 2.0 - 0.25, Q.c1);
+    lagrange(F->p.order_RP, F->p.order_RP / 2.0 - 0.75, Q.c2);
+    P.npro = (fb[1] - fb[0] + 1) * (fb[3] - fb[2] + 1) * (fb[5] - fb[4] + 1);
+  }
+  F->pairs[l].push_back(P);
+  return NRGPU_OK;
+}
+
+// the pairs of level l with level l-1
+int setup_pair(nrgpu_fmr *F, int l) {
+  F->fp[l].assign(F->L[l]->npoints, 0.0);
+  F->fr[l - 1].assign(F->L[l - 1]->npoints, 0.0);
+  F->pairs[l].clear();
+  std::vector<double> cr(F->L[l - 1]->npoints, 0.0);
+  for (int fb = 0; fb < (int)F->box[l].size(); ++fb) {
+    const int e = setup_one_pair(F, l, fb, cr);
+    if (e) return e;
   }
   return NRGPU_OK;
 }
@@ -312,21 +365,26 @@ int fill(Ptrs *P, double *const *u, int nv) {
   return NRGPU_OK;
 }
 
-// restrict_prolong_varlist between level l and its parent (nbuffer 3)
+// restrict_prolong_varlist between level l and its parent (nbuffer 3):
+// every pair restricted, then every pair prolonged (inject.c:63-100)
 int restrict_prolong(nrgpu_fmr *F, int l, const Ptrs &uc, const Ptrs &uf, cudaStream_t st) {
   const int o = F->p.order_RP;
-  if (F->has_r[l]) {
-    const dim3 g((F->nr[l] + 127) / 128, F->nv);
-    if (o == 2) restrict_kernel<2><<<g, 128, 0, st>>>(uc, uf, F->box[l - 1], F->box[l], F->rg[l], F->nr[l]);
-    else if (o == 4) restrict_kernel<4><<<g, 128, 0, st>>>(uc, uf, F->box[l - 1], F->box[l], F->rg[l], F->nr[l]);
-    else restrict_kernel<6><<<g, 128, 0, st>>>(uc, uf, F->box[l - 1], F->box[l], F->rg[l], F->nr[l]);
+  for (const FmrPair &P : F->pairs[l]) {
+    if (!P.has_r) continue;
+    const Box3 &cb = F->box[l - 1][P.cbox], &fb = F->box[l][P.fbox];
+    const dim3 g((P.nr + 127) / 128, F->nv);
+    if (o == 2) restrict_kernel<2><<<g, 128, 0, st>>>(uc, uf, cb, fb, P.rg, P.nr);
+    else if (o == 4) restrict_kernel<4><<<g, 128, 0, st>>>(uc, uf, cb, fb, P.rg, P.nr);
+    else restrict_kernel<6><<<g, 128, 0, st>>>(uc, uf, cb, fb, P.rg, P.nr);
     NRGPU_CUDA_TRY(cudaGetLastError());
   }
-  if (F->has_p[l]) {
-    const dim3 g((F->npro[l] + 127) / 128, F->nv);
-    if (o == 2) prolong_kernel<2><<<g, 128, 0, st>>>(uc, uf, F->box[l - 1], F->box[l], F->pg[l], F->npro[l]);
-    else if (o == 4) prolong_kernel<4><<<g, 128, 0, st>>>(uc, uf, F->box[l - 1], F->box[l], F->pg[l], F->npro[l]);
-    else prolong_kernel<6><<<g, 128, 0, st>>>(uc, uf, F->box[l - 1], F->box[l], F->pg[l], F->npro[l]);
+  for (const FmrPair &P : F->pairs[l]) {
+    if (!P.has_p) continue;
+    const Box3 &cb = F->box[l - 1][P.cbox], &fb = F->box[l][P.fbox];
+    const dim3 g((P.npro + 127) / 128, F->nv);
+    if (o == 2) prolong_kernel<2><<<g, 128, 0, st>>>(uc, uf, cb, fb, P.pg, P.npro);
+    else if (o == 4) prolong_kernel<4><<<g, 128, 0, st>>>(uc, uf, cb, fb, P.pg, P.npro);
+    else prolong_kernel<6><<<g, 128, 0, st>>>(uc, uf, cb, fb, P.pg, P.npro);
     NRGPU_CUDA_TRY(cudaGetLastError());
   }
   return NRGPU_OK;
@@ -449,11 +507,17 @@ extern "C" int nrgpu_fmr_create(int nl, const nrgpu_level_desc *levels, const do
   int e = NRGPU_OK;
   for (int l = 0; l < nl && !e; ++l) {
     const nrgpu_level_desc &d = levels[l];
-    if (d.nboxes != 1) e = nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "level %d: one box per level", l);
+    if (d.nboxes < 1 || !d.box) e = nrgpu_set_error(NRGPU_ERR_ARG, "level %d: no boxes", l);
     else if (dt[l] <= 0) e = nrgpu_set_error(NRGPU_ERR_ARG, "level %d: dt %g", l, dt[l]);
     if (e) break;
-    F->box[l] = Box3{{d.box[0].m, d.box[0].n, d.box[0].o}, 0};
-    F->x0[l][0] = d.box[0].x0; F->x0[l][1] = d.box[0].y0; F->x0[l][2] = d.box[0].z0;
+    F->box[l].clear();
+    F->bx0[l].clear();
+    for (int b = 0; b < d.nboxes; ++b) {
+      F->box[l].push_back(Box3{{d.box[b].m, d.box[b].n, d.box[b].o}, (long)d.box[b].noffset});
+      F->bx0[l].push_back(d.box[b].x0);
+      F->bx0[l].push_back(d.box[b].y0);
+      F->bx0[l].push_back(d.box[b].z0);
+    }
     F->dx[l][0] = d.dx; F->dx[l][1] = d.dy; F->dx[l][2] = d.dz;
     F->dt[l] = dt[l];
     if (p->system == NRGPU_SYSTEM_BSSN) F->bp[l] = ((const nrgpu_bssn_params *)sysparams)[l];

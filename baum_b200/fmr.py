@@ -1,8 +1,8 @@
 """Host-side mirror of the reference's mesh refinement around the evolution.
 
-``Hierarchy`` holds the nested boxes of a grid (one box per level, each made
-of whole cells of its parent: the single-rank grid of amr = bo newfmr,
-amr_fmr = nestedboxes) on the device and advances them by coarse steps:
+``Hierarchy`` holds the nested boxes of a grid (one or several separate
+boxes per level, each made of whole cells of the coarser box that holds it:
+the single-rank grid of amr = bo newfmr, amr_fmr = nestedboxes) on the device and advances them by coarse steps:
 advance_levelandsublevels (main.c:397-418) with the time interpolation of
 evolve (evolve.c:292-340, 371-380) and restrict_prolong_evolve
 (inject.c:116-132).  ``restrict_prolong_varlist`` is inject.c:63-100 with

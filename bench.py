@@ -569,6 +569,7 @@ def run_z4c160(args):
     u0 = punctures.z4_brill_lindquist_state(lev, [(0.5, 5.0, 0.0, 0.0), (0.5, -5.0, 0.0, 0.0)])
     p = abi.z4_params(order_centered=6, order_advection=6)
     dl = z4.DeviceLevel(lev)
+    block = dl.autotune(abi.SYSTEM_Z4C, p)
     u = torch.from_numpy(u0).cuda()
     flush = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device="cuda")
     for _ in range(args.warmup):
@@ -583,7 +584,8 @@ def run_z4c160(args):
     torch.cuda.synchronize()
     ms = sum(a.elapsed_time(b) for a, b in ev) / args.steps
     pts = n ** 3
-    print(json.dumps({"case": "z4c160", "metric": "RHS point-updates/s", "value": 4 * pts / (ms * 1e-3),
+    print(json.dumps({"case": "z4c160", "block": "%dx%dx%d" % block, "metric": "RHS point-updates/s",
+                      "value": 4 * pts / (ms * 1e-3),
                       "unit": UNIT, "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
                       "dtype": "f64", "config": {"workload": "Z4c 6th order + KO6, 160^3 inner, dx 0.15, "
                                                              "BL binary m=0.5 at x=+-5", "l2": "flushed"},

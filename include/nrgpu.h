@@ -270,10 +270,12 @@ int nrgpu_puncture_coefficients(int m, double dx, int npunc, const double *mass,
                                 double *a, double *b, void *stream);
 
 /* ---- fixed mesh refinement -----------------------------------------------
- * Nested boxes, one box per level, each level's box made of whole cells of
- * its parent (the single-rank grid of amr = bo newfmr, amr_fmr =
- * nestedboxes).  The library derives the refinement flags (setRPflags,
- * main/amr/flag.c:122-255) from the boxes, and advances the whole hierarchy
+ * Nested boxes, one or several boxes per level (separate boxes, such as a
+ * binary's two punctures on the finer levels), each box made of whole cells
+ * of the coarser box that holds it (the single-rank grid of amr = bo
+ * newfmr, amr_fmr = nestedboxes).  The library derives the refinement flags
+ * (setRPflags, main/amr/flag.c:122-255) per fine box and its parent box
+ * from the boxes, and advances the whole hierarchy
  * by coarse steps: advance_levelandsublevels (main/main/main.c:397-418) with
  * the time interpolation of evolve (utility/evolve/evolve.c:292-340,
  * 371-380) and restrict_prolong_evolve (main/amr/inject.c:116-132) through
@@ -301,7 +303,9 @@ int nrgpu_fmr_create(int nlevels, const nrgpu_level_desc *levels, const double *
                      const nrgpu_fmr_params *p, nrgpu_fmr **out);
 int nrgpu_fmr_destroy(nrgpu_fmr *fmr);
 /* the refinement flags of level l (host arrays of the level's npoints, NULL
- * to skip): flagprolong (levels with a parent), flagrestrict (with a child) */
+ * to skip): flagprolong (levels with a parent), flagrestrict (with a child;
+ * with several child boxes the union of their pairs' flags, which the
+ * reference keeps on a ghost parent of each child box instead) */
 int nrgpu_fmr_flags(nrgpu_fmr *fmr, int l, double *flagprolong, double *flagrestrict);
 /* restrict_prolong_varlist (inject.c:63-100) with nbuffer 3 between level
  * lfine and its parent: restrict lfine's uf into uc, then prolong uc into

@@ -6,7 +6,8 @@
  * TEST INFRASTRUCTURE ONLY: loaded by tests/ (through oracle/oracle.py) as
  * the checker of the CUDA path; the product never links or calls it.
  *
- * Restates, FP64, for one box per level (the single-rank nested-box grid):
+ * Restates, FP64, for one or several boxes per level (the single-rank
+ * nested-box grid; several boxes where the punctures' boxes do not merge):
  *   setRPflags               flag.c:122-255 (flagprolong on the child,
  *                            flagrestrict on the parent)
  *   restrict_varlist_boxtobox_N / restrict_boxtobox_N
@@ -24,6 +25,13 @@
  *   evolve                   evolve.c:292-340,371-380 (time interpolation
  *                            orders 2 and 3 around the RK4 step; the
  *                            algebraic constraints come after it)
+ * With several boxes on a level, each fine box pairs with the coarse box
+ * that holds it (BAM's box->pr): the flags, the restriction box and the
+ * prolongation box are those of the pair (the reference computes them on a
+ * ghost parent of each fine box, flag.c:122-255 with
+ * interpolate_boxtobox_N.c:870-1370 looping forallboxes(lf)), every pair
+ * is restricted before any is prolonged (restrict_prolong_varlist,
+ * inject.c:63-100).
  * The Berger-Oliger recursion that strings these together
  * (advance_levelandsublevels, main.c:397-418) is restated in oracle/oracle.py.
  * Every sum runs in the reference's order, so restriction, prolongation and
@@ -65,24 +73,41 @@ static int point_index(double X0, double dX, double x0, double dx, int i)
 
 typedef struct { int n[3]; double x0[3], dx[3]; long off; } box_t;
 
-static box_t box_of(const nrgpu_level_desc *L)
+static box_t box_of(const nrgpu_level_desc *L, int ib)
 {
   box_t b;
-  b.n[0] = L->box[0].m; b.n[1] = L->box[0].n; b.n[2] = L->box[0].o;
-  b.x0[0] = L->box[0].x0; b.x0[1] = L->box[0].y0; b.x0[2] = L->box[0].z0;
+  b.n[0] = L->box[ib].m; b.n[1] = L->box[ib].n; b.n[2] = L->box[ib].o;
+  b.x0[0] = L->box[ib].x0; b.x0[1] = L->box[ib].y0; b.x0[2] = L->box[ib].z0;
   b.dx[0] = L->dx; b.dx[1] = L->dy; b.dx[2] = L->dz;
-  b.off = L->box[0].noffset;
+  b.off = L->box[ib].noffset;
   return b;
 }
 
 static long at(const box_t *b, int i, int j, int k) { return b->off + i + (long)b->n[0] * (j + (long)b->n[1] * k); }
 
-/* setRPflags (flag.c:122-255) for one box per level, no symmetry */
-int oracle_fmr_flags(const nrgpu_level_desc *C, const nrgpu_level_desc *F, int nbuffer, double *fp, double *cr)
+/* the coarse box holding every parent point of the fine box (box->pr) */
+static int parent_box(const nrgpu_level_desc *C, const box_t *f)
 {
-  box_t f = box_of(F), c = box_of(C);
+  for (int ib = 0; ib < C->nboxes; ib++) {
+    box_t c = box_of(C, ib);
+    int ok = 1;
+    for (int d = 0; d < 3; d++) {
+      int lo = parent_index(c.x0[d], c.dx[d], f->x0[d], f->dx[d], 0);
+      int hi = parent_index(c.x0[d], c.dx[d], f->x0[d], f->dx[d], f->n[d] - 1);
+      if (lo < 0 || hi >= c.n[d]) ok = 0;
+    }
+    if (ok) return ib;
+  }
+  return -1;
+}
+
+/* setRPflags (flag.c:122-255) of one fine box and its parent box, no
+ * symmetry: flagprolong over the fine box, flagrestrict on the parent box
+ * (the caller clears cr) */
+static int pair_flags(const box_t *cp, const box_t *fp_box, int nbuffer, double *fp, double *cr)
+{
+  box_t f = *fp_box, c = *cp;
   int np = f.n[0] * f.n[1] * f.n[2];
-  for (long q = 0; q < C->npoints; q++) cr[q] = 0;
   for (int k = 0; k < f.n[2]; k++)
     for (int j = 0; j < f.n[1]; j++)
       for (int i = 0; i < f.n[0]; i++) {
@@ -122,12 +147,27 @@ int oracle_fmr_flags(const nrgpu_level_desc *C, const nrgpu_level_desc *F, int n
   return 0;
 }
 
-/* restriction of nv variables from the child F into the parent C
- * (restrict_varlist_boxtobox_N with nbuffer >= 3, i.e. flagrestrict >= 3) */
-static int restrict_level(const nrgpu_level_desc *C, const nrgpu_level_desc *F, const double *cr, int nv,
-                          double *const *uc, double *const *uf, int order)
+/* setRPflags of every fine box: fp over the fine level, cr over the coarse
+ * level (with several fine boxes, the union of the pairs' flags) */
+int oracle_fmr_flags(const nrgpu_level_desc *C, const nrgpu_level_desc *F, int nbuffer, double *fp, double *cr)
 {
-  box_t f = box_of(F), c = box_of(C);
+  for (long q = 0; q < C->npoints; q++) cr[q] = 0;
+  for (int ib = 0; ib < F->nboxes; ib++) {
+    box_t f = box_of(F, ib);
+    int pb = parent_box(C, &f);
+    if (pb < 0) return -1;
+    box_t c = box_of(C, pb);
+    if (pair_flags(&c, &f, nbuffer, fp, cr)) return -1;
+  }
+  return 0;
+}
+
+/* restriction of nv variables from the fine box f into its parent box c
+ * (restrict_varlist_boxtobox_N with nbuffer >= 3, i.e. flagrestrict >= 3) */
+static int restrict_pair(const box_t *cp, const box_t *fp_box, const double *cr, int nv, double *const *uc,
+                         double *const *uf, int order)
+{
+  box_t f = *fp_box, c = *cp;
   const int b = order / 2;
   int ic[6] = {1 << 30, -(1 << 30), 1 << 30, -(1 << 30), 1 << 30, -(1 << 30)};
   long n = 0;
@@ -173,12 +213,12 @@ static int restrict_level(const nrgpu_level_desc *C, const nrgpu_level_desc *F, 
   return 0;
 }
 
-/* prolongation of nv variables from the parent C into the child F
+/* prolongation of nv variables from the parent box c into the fine box f
  * (prolong_varlist_boxtobox_N with nbuffer >= 3) */
-static int prolong_level(const nrgpu_level_desc *C, const nrgpu_level_desc *F, const double *fp, int nv,
-                         double *const *uc, double *const *uf, int order, int amr_nbuffer)
+static int prolong_pair(const box_t *cp, const box_t *fp_box, const double *fp, int nv, double *const *uc,
+                        double *const *uf, int order, int amr_nbuffer)
 {
-  box_t f = box_of(F), c = box_of(C);
+  box_t f = *fp_box, c = *cp;
   const int b = order / 2;
   int ifb[6] = {1 << 30, -(1 << 30), 1 << 30, -(1 << 30), 1 << 30, -(1 << 30)};
   int if0[6] = {1 << 30, -(1 << 30), 1 << 30, -(1 << 30), 1 << 30, -(1 << 30)};
@@ -242,9 +282,24 @@ int oracle_fmr_restrict_prolong(const nrgpu_level_desc *C, const nrgpu_level_des
                                 double *const *uf, int order, int amr_nbuffer)
 {
   double *fp = malloc(sizeof(double) * F->npoints), *cr = malloc(sizeof(double) * C->npoints);
-  int e = oracle_fmr_flags(C, F, amr_nbuffer, fp, cr);
-  if (!e) e = restrict_level(C, F, cr, nv, uc, uf, order);
-  if (!e) e = prolong_level(C, F, fp, nv, uc, uf, order, amr_nbuffer);
+  int e = 0;
+  /* every pair is restricted, with its own flags, before any is prolonged */
+  for (int ib = 0; ib < F->nboxes && !e; ib++) {
+    box_t f = box_of(F, ib);
+    int pb = parent_box(C, &f);
+    if (pb < 0) {
+      e = -1;
+      break;
+    }
+    box_t c = box_of(C, pb);
+    for (long q = 0; q < C->npoints; q++) cr[q] = 0;
+    e = pair_flags(&c, &f, amr_nbuffer, fp, cr);
+    if (!e) e = restrict_pair(&c, &f, cr, nv, uc, uf, order);
+  }
+  for (int ib = 0; ib < F->nboxes && !e; ib++) {
+    box_t f = box_of(F, ib), c = box_of(C, parent_box(C, &f));
+    e = prolong_pair(&c, &f, fp, nv, uc, uf, order, amr_nbuffer);
+  }
   free(fp);
   free(cr);
   return e;

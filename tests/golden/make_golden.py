@@ -266,12 +266,27 @@ nrharness_flags = yes
 nrharness_dump = 0 2 4 8
 """,
 }
+# a binary on the same kind of grid: the punctures' level-1 boxes merge
+# into one 60x40x40 box, the level-2 boxes (40^3 around x = +-2.75) stay
+# apart, so level 2 has two boxes (FlagRegridPunctures, FlagRegrid.c:34-160;
+# the puncture data are replaced by the Fourier data, the punctures only
+# place the boxes)
+FMR_CASES["z4_fmr3_binary"] = FMR_CASES["z4_fmr3"].replace(
+    "physics = adm z4 nrharness", "physics = adm z4 punctures nrharness").replace(
+    "nxyz = 16", "nxyz = 32").replace("mass1 = 1\nmass2 = 0", """mass1 = 0.5
+px1 = 2.75
+mass2 = 0.5
+px2 = -2.75
+punctures_solver = none""")
 # the dumps and fields kept: the end of the second coarse step on every
 # level and the finest level after its second step; g11, chi, A12, Khat,
 # Gamma1, Theta, alpha, beta1 (the initial state is regenerated by
-# baum_b200/synthetic.py, bit for bit)
+# baum_b200/synthetic.py, bit for bit); for the binary, chi and alpha at the
+# end of the second coarse step (the fixture stays near 4 MB)
 FMR_KEEP = {"state_it2_l0", "state_it4_l1", "state_it8_l2", "state_it2_l2"}
 FMR_VARS = [0, 6, 8, 13, 14, 17, 18, 19]
+FMR_KEEP_BY_CASE = {"z4_fmr3": (FMR_KEEP, FMR_VARS),
+                    "z4_fmr3_binary": ({"state_it2_l0", "state_it4_l1", "state_it8_l2"}, [6, 18])}
 
 
 def run_fmr_case(name, par):
@@ -291,10 +306,11 @@ def run_fmr_case(name, par):
             fl = dumpfile.read(os.path.join(work, "flags_l%d.bin" % l))
             for nm, a in zip(fl["names"], fl["data"]):
                 arrays["%s_l%d" % (nm, l)] = a.astype(np.int8)
-        for tag in sorted(FMR_KEEP):
+        keep, fvars = FMR_KEEP_BY_CASE[name]
+        for tag in sorted(keep):
             d = dumpfile.read(os.path.join(work, tag + ".bin"))
-            arrays[tag] = d["data"][FMR_VARS]
-        np.savez_compressed(os.path.join(OUT, name + ".npz"), vars=np.array(FMR_VARS), **arrays)
+            arrays[tag] = d["data"][fvars]
+        np.savez_compressed(os.path.join(OUT, name + ".npz"), vars=np.array(fvars), **arrays)
         with open(os.path.join(OUT, name + ".par"), "w") as f:
             f.write(par.lstrip())
         print("wrote", name, sorted(arrays))

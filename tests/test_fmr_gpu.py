@@ -98,3 +98,46 @@ def test_bssn_hierarchy_matches_oracle(gpu):
         a, b = u[l].cpu().numpy(), st.u[l]
         err = np.abs(a - b).max(axis=1) / np.maximum(np.abs(b).max(axis=1), 1e-8)
         assert err.max() < FMR_TOL, (l, err.max())
+
+
+def test_binary_grid_on_the_gpu(gpu):
+    """The binary's grid of the reference (level 2 in two boxes around the
+    punctures): flags and one restriction/prolongation bit for bit against
+    the oracle, the first box's flagprolong against the reference, and two
+    coarse steps of all levels within the oracle's tolerance, graph replay
+    and plain launches identical."""
+    g, levels, u0, params, dt = fmr_case("z4_fmr3_binary")
+    assert levels[2].desc.nboxes == 2
+    H = fmr.Hierarchy(levels, dt, params, abi.fmr_params(use_graph=0))
+    for l in (1, 2):
+        fp, _ = H.flags(l)
+        assert np.array_equal(fp, g["flagprolong_l%d" % l])
+        _, cr = oracle.fmr_flags(levels[l - 1], levels[l], 3)
+        assert np.array_equal(H.flags(l - 1)[1], cr)
+    rng = np.random.default_rng(7)
+    uc = rng.standard_normal((abi.Z4_NVARS, levels[1].npoints))
+    uf = rng.standard_normal((abi.Z4_NVARS, levels[2].npoints))
+    dc, df = to_dev(uc), to_dev(uf)
+    H.restrict_prolong_varlist(2, dc, df)
+    oracle.fmr_restrict_prolong(levels[1], levels[2], uc, uf, 4, 3)
+    assert np.array_equal(dc.cpu().numpy(), uc)
+    assert np.array_equal(df.cpu().numpy(), uf)
+    H.close()
+    st = oracle.FmrState(levels, u0, 1, params, dt)
+    st.advance(2)
+    runs = []
+    for use_graph in (0, 1):
+        H = fmr.Hierarchy(levels, dt, params, abi.fmr_params(use_graph=use_graph))
+        u = [to_dev(x) for x in u0]
+        H.advance(u, 1)
+        H.advance(u, 1)
+        torch.cuda.synchronize()
+        assert [H.iteration(l) for l in range(3)] == [2, 4, 8]
+        runs.append([x.cpu().numpy() for x in u])
+        H.close()
+    for a, b in zip(*runs):
+        assert np.array_equal(a, b)
+    for l in range(3):
+        a, b = runs[0][l], st.u[l]
+        err = np.abs(a - b).max(axis=1) / np.maximum(np.abs(b).max(axis=1), 1e-8)
+        assert err.max() < FMR_TOL, (l, err.max())

@@ -16,16 +16,15 @@ FMR_TOL = 2e-11
 
 
 def fmr_case(name="z4_fmr3"):
-    """Levels, initial states, per-level parameters and time steps of the
-    3-level golden run: dissipation_factor 0.1 on level 0 and 0.2 x 0.1 on
+    """Levels (with all their boxes), initial states, per-level parameters
+    and time steps of a 3-level golden run: dissipation_factor 0.1 on level 0 and 0.2 x 0.1 on
     finer levels (get_dissipation_factor, evolve.c:486-530, with
     amr_move_lcube = 0 and physics without "Z4d"), dt = dtfac dx."""
     g = load_golden(name)
     levels, u0, params, dt = [], [], [], []
     for l in range(3):
-        b = g["boxes_l%d" % l][0]
-        lev = abi.Level([(int(b[0]), int(b[1]), int(b[2]), b[4], b[5], b[6])], float(g["dx_l%d" % l]),
-                        g["boundary_l%d" % l])
+        boxes = [(int(b[0]), int(b[1]), int(b[2]), b[4], b[5], b[6]) for b in g["boxes_l%d" % l]]
+        lev = abi.Level(boxes, float(g["dx_l%d" % l]), g["boundary_l%d" % l])
         x, y, z = lev.coords()
         levels.append(lev)
         u0.append(synthetic.fourier_state(x, y, z, abi.Z4_NVARS, synthetic.Z4_UNIT, 8, 0.05, 16.0, 1))
@@ -59,5 +58,25 @@ def check_snapshots(g, run, tol=FMR_TOL):
 
 def test_three_level_evolution_matches_reference():
     g, levels, u0, params, dt = fmr_case()
+    st = oracle.FmrState(levels, u0, 1, params, dt)
+    check_snapshots(g, lambda snap: st.advance(2, snap))
+
+
+def test_binary_grid_flags_match_reference():
+    """The binary's grid: level 2 is two boxes, each with its own
+    flagprolong (from its own bounding box); level 1 is one box."""
+    g, levels, _, _, _ = fmr_case("z4_fmr3_binary")
+    assert levels[2].desc.nboxes == 2
+    for l in (1, 2):
+        fp, cr = oracle.fmr_flags(levels[l - 1], levels[l], 3)
+        assert np.array_equal(fp, g["flagprolong_l%d" % l])
+    fp, cr = oracle.fmr_flags(levels[0], levels[1], 3)
+    assert np.array_equal(cr, g["flagrestrict_l0"])
+
+
+def test_binary_grid_evolution_matches_reference():
+    """Two coarse steps of the binary's grid (level 2 in two boxes): chi and
+    alpha of every level at the end, against the reference's dumps."""
+    g, levels, u0, params, dt = fmr_case("z4_fmr3_binary")
     st = oracle.FmrState(levels, u0, 1, params, dt)
     check_snapshots(g, lambda snap: st.advance(2, snap))
