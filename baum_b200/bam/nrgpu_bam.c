@@ -16,8 +16,8 @@
  *                           after every step for ANALYZE/OUTPUT/checkpoint.
  *                           Set bssn_register_algcon = no with this mode.
  *   nrgpu_mode = fmr        the whole Berger-Oliger step of all levels (one
- *                           box each) runs on the GPU at level 0's EVOLVE
- *                           hook; set bssn/z4_register_algcon = no.
+ *                           or several boxes each) runs on the GPU at level
+ *                           0's EVOLVE hook; set bssn/z4_register_algcon = no.
  * physics with z4 selects the Z4c system (resident and fmr modes).
  *
  *   nrgpu_multigrid = yes   the puncture initial-data solve (punctures_solver
@@ -314,19 +314,21 @@ int nrgpu_evolve_fmr(tL *level)
   timer_start(level, "evolve");
   if (!fmr_h) {
     nrgpu_level_desc d[16];
-    nrgpu_box box[16];
+    nrgpu_box box[16][8];
     double dt[16];
     nrgpu_bssn_params bp[16];
     nrgpu_z4_params zp[16];
     nrgpu_fmr_params fp;
     for (l = 0; l < nl; l++) {
       tL *lv = g->level[l];
-      tB *bx;
-      if (lv->nboxes != 1) errorexit("nrgpu: the refinement mode takes one box per level");
-      bx = lv->box[0];
-      box[l].m = bx->m; box[l].n = bx->n; box[l].o = bx->o; box[l].noffset = bx->noffset;
-      box[l].x0 = bx->x0; box[l].y0 = bx->y0; box[l].z0 = bx->z0;
-      d[l].nboxes = 1; d[l].box = &box[l]; d[l].npoints = lv->npoints;
+      int b;
+      if (lv->nboxes < 1 || lv->nboxes > 8) errorexit("nrgpu: the refinement mode takes 1 to 8 boxes per level");
+      for (b = 0; b < lv->nboxes; b++) {
+        tB *bx = lv->box[b];
+        box[l][b].m = bx->m; box[l][b].n = bx->n; box[l][b].o = bx->o; box[l][b].noffset = bx->noffset;
+        box[l][b].x0 = bx->x0; box[l][b].y0 = bx->y0; box[l][b].z0 = bx->z0;
+      }
+      d[l].nboxes = lv->nboxes; d[l].box = box[l]; d[l].npoints = lv->npoints;
       d[l].dx = lv->dx; d[l].dy = lv->dy; d[l].dz = lv->dz; d[l].boundary = lv->boundary;
       dt[l] = lv->dt;
       u->level = lv;

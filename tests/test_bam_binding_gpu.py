@@ -114,11 +114,22 @@ nrharness_dump = 2 4 8
 """
 
 
-def run_fmr(binary, extra_physics, extra):
+# the binary's grid: punctures at x = +-2.75 place one level-1 box and two
+# separate level-2 boxes (the data are the harness's Fourier data)
+BINARY = ("physics = adm z4 nrharness", "physics = adm z4 punctures nrharness"), ("nxyz = 16", "nxyz = 32"), \
+    ("mass1 = 1\nmass2 = 0", "mass1 = 0.5\npx1 = 2.75\nmass2 = 0.5\npx2 = -2.75\npunctures_solver = none")
+
+
+def run_fmr(binary, extra_physics, extra, grid="single"):
     work = tempfile.mkdtemp(prefix="bamgpu_")
+    par = FMR_PAR
+    if grid == "binary":
+        for a, b in BINARY:
+            assert a in par
+            par = par.replace(a, b)
     try:
         with open(os.path.join(work, "t.par"), "w") as f:
-            f.write(FMR_PAR % (extra_physics, extra))
+            f.write(par % (extra_physics, extra))
         r = subprocess.run([binary, "-nt", "4", "t.par"], cwd=work, capture_output=True, text=True, timeout=600)
         assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
         return [dumpfile.read(os.path.join(work, "state_it%d_l%d.bin" % (2 * 2 ** l, l))) for l in range(3)], r.stdout
@@ -126,7 +137,8 @@ def run_fmr(binary, extra_physics, extra):
         shutil.rmtree(work, ignore_errors=True)
 
 
-def test_bam_fmr_mode_matches_bam(gpu, cpu_state):
+@pytest.mark.parametrize("grid", ["single", "binary"])
+def test_bam_fmr_mode_matches_bam(gpu, cpu_state, grid):
     """nrgpu_mode = fmr: the whole Berger-Oliger step of the 3-level Z4c grid
     on the GPU at level 0's EVOLVE hook.  BAM dumps every level right after
     the level's own step (POST_EVOLVE), before its child restricts into it
@@ -134,17 +146,18 @@ def test_bam_fmr_mode_matches_bam(gpu, cpu_state):
     the host arrays already hold the end of the coarse step.  So the levels
     are compared, after 2 coarse steps, on the points that this last
     restriction and prolongation do not write, within the refinement
-    tolerance of the oracle pin (2e-11)."""
+    tolerance of the oracle pin (2e-11).  The binary's grid has two boxes
+    on level 2."""
     from baum_b200 import abi
     from oracle import oracle
-    ref, _ = run_fmr(BAM, "", "")
-    got, out = run_fmr(BAM_GPU, " nrgpu", "nrgpu_mode = fmr\nz4_register_algcon = no")
+    ref, _ = run_fmr(BAM, "", "", grid)
+    got, out = run_fmr(BAM_GPU, " nrgpu", "nrgpu_mode = fmr\nz4_register_algcon = no", grid)
     assert "nrgpu: fmr mode" in out
     levels = []
     for d in ref:
-        b = d["boxes"][0]
-        levels.append(abi.Level([(int(b[0]), int(b[1]), int(b[2]), b[4], b[5], b[6])], float(d["dx"]),
-                                d["boundary"]))
+        levels.append(abi.Level([(int(b[0]), int(b[1]), int(b[2]), b[4], b[5], b[6]) for b in d["boxes"]],
+                                float(d["dx"]), d["boundary"]))
+    assert levels[2].desc.nboxes == (2 if grid == "binary" else 1)
     keep = [np.ones(lv.npoints, dtype=bool) for lv in levels]
     for l in (1, 2):
         uc = np.zeros((1, levels[l - 1].npoints))
