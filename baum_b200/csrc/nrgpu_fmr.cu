@@ -636,3 +636,75 @@ extern "C" int nrgpu_fmr_advance(nrgpu_fmr *F, double *const *u, int nsteps, voi
   }
   return NRGPU_OK;
 }
+
+// ---- checkpoint of the hierarchy's own state (no counterpart) -------------------
+// The reference's checkpoint (checkpoint.c:14-165) writes the level variables;
+// here the caller owns those, and the hierarchy owns the iteration counters,
+// and for every level with a child the previous step's copy and the time
+// interpolant.  Layout: a header (magic, version, levels, variables, the
+// levels' point counts), the counters, then per parent level u(n-1) and upp.
+namespace {
+constexpr uint32_t kCkptMagic = 0x4652474e;  // "NGRF"
+size_t ckpt_bytes(const nrgpu_fmr *F) {
+  size_t b = sizeof(uint32_t) * 4 + sizeof(long) * F->nl + sizeof(int) * F->nl;
+  for (int l = 0; l < F->nl - 1; ++l) b += 2 * sizeof(double) * F->nv * (size_t)F->L[l]->npoints;
+  return b;
+}
+}  // namespace
+
+extern "C" int nrgpu_fmr_state_size(nrgpu_fmr *F, size_t *bytes) {
+  if (!F || !bytes) return nrgpu_set_error(NRGPU_ERR_ARG, "null argument");
+  *bytes = ckpt_bytes(F);
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_fmr_save(nrgpu_fmr *F, void *host, size_t bytes) {
+  if (!F || !host || bytes < ckpt_bytes(F)) return nrgpu_set_error(NRGPU_ERR_ARG, "buffer of %zu bytes", bytes);
+  NRGPU_CUDA_TRY(cudaDeviceSynchronize());
+  char *c = (char *)host;
+  const uint32_t h[4] = {kCkptMagic, 1u, (uint32_t)F->nl, (uint32_t)F->nv};
+  memcpy(c, h, sizeof h);
+  c += sizeof h;
+  for (int l = 0; l < F->nl; ++l, c += sizeof(long)) {
+    const long np = F->L[l]->npoints;
+    memcpy(c, &np, sizeof np);
+  }
+  memcpy(c, F->iteration, sizeof(int) * F->nl);
+  c += sizeof(int) * F->nl;
+  for (int l = 0; l < F->nl - 1; ++l) {
+    const size_t b = sizeof(double) * F->nv * (size_t)F->L[l]->npoints;
+    NRGPU_CUDA_TRY(cudaMemcpy(c, F->up[l], b, cudaMemcpyDeviceToHost));
+    c += b;
+    NRGPU_CUDA_TRY(cudaMemcpy(c, F->upp[l], b, cudaMemcpyDeviceToHost));
+    c += b;
+  }
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_fmr_load(nrgpu_fmr *F, const void *host, size_t bytes) {
+  if (!F || !host || bytes < ckpt_bytes(F)) return nrgpu_set_error(NRGPU_ERR_ARG, "buffer of %zu bytes", bytes);
+  const char *c = (const char *)host;
+  uint32_t h[4];
+  memcpy(h, c, sizeof h);
+  c += sizeof h;
+  if (h[0] != kCkptMagic || h[1] != 1u || h[2] != (uint32_t)F->nl || h[3] != (uint32_t)F->nv)
+    return nrgpu_set_error(NRGPU_ERR_ARG, "checkpoint of another hierarchy (levels %u, variables %u)", h[2], h[3]);
+  for (int l = 0; l < F->nl; ++l, c += sizeof(long)) {
+    long np;
+    memcpy(&np, c, sizeof np);
+    if (np != F->L[l]->npoints) return nrgpu_set_error(NRGPU_ERR_ARG, "checkpoint level %d: %ld points", l, np);
+  }
+  int it[kMaxLevels];
+  memcpy(it, c, sizeof(int) * F->nl);
+  c += sizeof(int) * F->nl;
+  NRGPU_CUDA_TRY(cudaDeviceSynchronize());
+  for (int l = 0; l < F->nl - 1; ++l) {
+    const size_t b = sizeof(double) * F->nv * (size_t)F->L[l]->npoints;
+    NRGPU_CUDA_TRY(cudaMemcpy(F->up[l], c, b, cudaMemcpyHostToDevice));
+    c += b;
+    NRGPU_CUDA_TRY(cudaMemcpy(F->upp[l], c, b, cudaMemcpyHostToDevice));
+    c += b;
+  }
+  memcpy(F->iteration, it, sizeof(int) * F->nl);
+  return NRGPU_OK;
+}

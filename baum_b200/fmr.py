@@ -70,6 +70,20 @@ class Hierarchy:
         abi.check(abi.lib().nrgpu_fmr_block(self.handle, l, b))
         return tuple(b)
 
+    def save(self):
+        """The hierarchy's own state (iteration counters, previous-step
+        copies, time interpolants) as a numpy byte array (nrgpu_fmr_save)."""
+        n = C.c_size_t()
+        abi.check(abi.lib().nrgpu_fmr_state_size(self.handle, C.byref(n)))
+        buf = np.empty(n.value, dtype=np.uint8)
+        abi.check(abi.lib().nrgpu_fmr_save(self.handle, buf.ctypes.data, n.value))
+        return buf
+
+    def load(self, buf):
+        """Restore a state written by save() (nrgpu_fmr_load)."""
+        buf = np.ascontiguousarray(buf, dtype=np.uint8)
+        abi.check(abi.lib().nrgpu_fmr_load(self.handle, buf.ctypes.data, buf.size))
+
     def close(self):
         if self.handle:
             abi.lib().nrgpu_fmr_destroy(self.handle)

@@ -319,6 +319,19 @@ int nrgpu_fmr_iteration(nrgpu_fmr *fmr, int l);
 /* the rhs block shape (x, y, z) level l runs with, into block[3] */
 int nrgpu_fmr_block(nrgpu_fmr *fmr, int l, int *block);
 
+/* Checkpoint of the hierarchy's own state (no counterpart: the reference's
+ * checkpoint, main/main/checkpoint.c:14-165, writes the level variables,
+ * which stay with the caller here): the level iteration counters and, for
+ * every level with a child, the previous step's copy and the time
+ * interpolant.  nrgpu_fmr_state_size gives the bytes; nrgpu_fmr_save writes
+ * them to a host buffer and nrgpu_fmr_load restores them into a hierarchy
+ * created with the same levels and parameters (refused otherwise).  Both
+ * wait for the device.  With the caller's level states this resumes a run
+ * bit for bit. */
+int nrgpu_fmr_state_size(nrgpu_fmr *fmr, size_t *bytes);
+int nrgpu_fmr_save(nrgpu_fmr *fmr, void *host, size_t bytes);
+int nrgpu_fmr_load(nrgpu_fmr *fmr, const void *host, size_t bytes);
+
 /* the evolution systems */
 enum { NRGPU_SYSTEM_BSSN = 0, NRGPU_SYSTEM_Z4C = 1 };
 

@@ -141,3 +141,32 @@ def test_binary_grid_on_the_gpu(gpu):
         a, b = runs[0][l], st.u[l]
         err = np.abs(a - b).max(axis=1) / np.maximum(np.abs(b).max(axis=1), 1e-8)
         assert err.max() < FMR_TOL, (l, err.max())
+
+
+def test_checkpoint_resumes_bit_for_bit(gpu):
+    """nrgpu_fmr_save / nrgpu_fmr_load: two coarse steps, a checkpoint, two
+    more steps; a new hierarchy loaded from the checkpoint with the saved
+    level states gives the same states bit for bit (graph replay on both
+    sides).  A checkpoint of another hierarchy is refused."""
+    g, levels, u0, params, dt = fmr_case()
+    H = fmr.Hierarchy(levels, dt, params)
+    u = [to_dev(x) for x in u0]
+    H.advance(u, 2)
+    buf = H.save()
+    saved = [x.clone() for x in u]
+    H.advance(u, 2)
+    torch.cuda.synchronize()
+    ref = [x.cpu().numpy() for x in u]
+    H.close()
+    H2 = fmr.Hierarchy(levels, dt, params)
+    H2.load(buf)
+    assert [H2.iteration(l) for l in range(3)] == [2, 4, 8]
+    H2.advance(saved, 2)
+    torch.cuda.synchronize()
+    for a, b in zip(saved, ref):
+        assert np.array_equal(a.cpu().numpy(), b)
+    H2.close()
+    H3 = fmr.Hierarchy(levels[:2], dt[:2], params[:2])
+    with pytest.raises(RuntimeError):
+        H3.load(buf)
+    H3.close()
