@@ -34,7 +34,7 @@ class Box(C.Structure):
 class LevelDesc(C.Structure):
     _fields_ = [("nboxes", C.c_int), ("box", C.POINTER(Box)), ("npoints", C.c_int),
                 ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
-                ("boundary", C.POINTER(C.c_int))]
+                ("boundary", C.POINTER(C.c_int)), ("symmetry", C.c_int)]
 
 
 class BssnParams(C.Structure):
@@ -241,7 +241,7 @@ def mg_params(**over):
 class Level:
     """Host-side description of a level (keeps the ctypes arrays alive)."""
 
-    def __init__(self, boxes, dx, boundary, dy=None, dz=None):
+    def __init__(self, boxes, dx, boundary, dy=None, dz=None, symmetry=0):
         import numpy as np
         self.boxes = (Box * len(boxes))()
         off = 0
@@ -253,7 +253,7 @@ class Level:
         self.boundary = np.ascontiguousarray(boundary, dtype=np.int32)
         assert self.boundary.size == off
         self.desc = LevelDesc(len(boxes), self.boxes, off, dx, dy or dx, dz or dx,
-                              self.boundary.ctypes.data_as(C.POINTER(C.c_int)))
+                              self.boundary.ctypes.data_as(C.POINTER(C.c_int)), int(symmetry))
         self.dx = dx
 
     @staticmethod

@@ -160,6 +160,17 @@ static void read_params_z4(tL *level, tVarList *u, nrgpu_z4_params *p)
   }
 }
 
+/* the reflection axes of set_boundary_symmetry (symmetry.c:93-140) */
+static int grid_symmetry(void)
+{
+  if (Getv("grid", "quadrant") || Getv("grid", "rotant"))
+    errorexit("nrgpu: the inversion symmetry of grid = quadrant/rotant is not supported");
+  if (Getv("grid", "octant")) return 7;
+  if (Getv("grid", "qreflect")) return 6;
+  if (Getv("grid", "bitant")) return 4;
+  return 0;
+}
+
 static nrgpu_slot *slot_of(tL *level)
 {
   nrgpu_slot *s = &slots[level->l];
@@ -178,6 +189,7 @@ static nrgpu_slot *slot_of(tL *level)
     d.nboxes = level->nboxes; d.box = box; d.npoints = level->npoints;
     d.dx = level->dx; d.dy = level->dy; d.dz = level->dz;
     d.boundary = level->boundary;
+    d.symmetry = grid_symmetry();
     if (s->lev) nrgpu_level_destroy(s->lev);
     check(nrgpu_level_create(&d, &s->lev), "level");
     s->bamlevel = level;
@@ -330,6 +342,7 @@ int nrgpu_evolve_fmr(tL *level)
       }
       d[l].nboxes = lv->nboxes; d[l].box = box[l]; d[l].npoints = lv->npoints;
       d[l].dx = lv->dx; d[l].dy = lv->dy; d[l].dz = lv->dz; d[l].boundary = lv->boundary;
+      d[l].symmetry = grid_symmetry();
       dt[l] = lv->dt;
       u->level = lv;
       if (nrgpu_system_z4) read_params_z4(lv, u, &zp[l]);

@@ -718,7 +718,108 @@ __global__ void vlcopy_kernel(VarPtrs dst, CVarPtrs src, int npoints) {
 
 }  // namespace
 
+// set_boundary_symmetry (symmetry.c:93-140) as one pass over the symmetry
+// ghosts: each takes its mirror image's value times the variable's parity
+// under the reflected axes (the reference reflects axis after axis; the
+// product of the parities gives the same values, negation being exact)
+struct SymVars {
+  double *p[NRGPU_Z4_NVARS];
+};
+struct SymParity {
+  signed char s[NRGPU_Z4_NVARS][3];
+};
+__global__ void symmetry_kernel(SymVars u, int nv, SymParity par, const SymPoint *__restrict__ pts, int n) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * nv) return;
+  const int v = t % nv;
+  const SymPoint sp = pts[t / nv];
+  int sign = 1;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+    if (sp.mask >> a & 1) sign *= par.s[v][a];
+  const double x = u.p[v][sp.src];
+  u.p[v][sp.dst] = sign < 0 ? -x : x;
+}
+
 // ---- host side ----------------------------------------------------------------
+// the RK-stage updates of the fused epilogue (store(), EPI_RK) from a stored
+// rhs list, at every point: the unfused stages of a symmetry grid
+__global__ void rk_update_kernel(SymVars r, SymVars out, SymVars pre, SymVars acc, Epilogue E, int nv, long np) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= np * nv) return;
+  const int v = (int)(t / np);
+  const long x = t - (long)v * np;
+  const double rv = r.p[v][x];
+  if (E.accmode == ACC_FINAL) {
+    out.p[v][x] = acc.p[v][x] + E.wacc * rv;
+  } else if (E.accmode == ACC_INIT) {
+    const double u0 = pre.p[v][x];
+    acc.p[v][x] = u0 + E.wacc * rv;
+    if (E.has_v) out.p[v][x] = u0 + E.cv * rv;
+  } else {
+    acc.p[v][x] += E.wacc * rv;
+    if (E.has_v) out.p[v][x] = pre.p[v][x] + E.cv * rv;
+  }
+}
+
+// the rhs list of a symmetry grid's unfused stages (first use, zeroed: points
+// without a rhs keep 0, as the reference's evolution lists do)
+static int sym_rhs_list(nrgpu_level *L, int nv, SymVars *R) {
+  const size_t np = (size_t)L->npoints;
+  if (!L->rsym) {
+    if (cudaMalloc(&L->rsym, sizeof(double) * NRGPU_Z4_NVARS * np) != cudaSuccess) {
+      L->rsym = nullptr;
+      cudaGetLastError();
+      return nrgpu_set_error(NRGPU_ERR_NOMEM, "symmetry rhs list of %zu points", np);
+    }
+    NRGPU_CUDA_TRY(cudaMemset(L->rsym, 0, sizeof(double) * NRGPU_Z4_NVARS * np));
+  }
+  for (int v = 0; v < NRGPU_Z4_NVARS; ++v) R->p[v] = v < nv ? L->rsym + v * np : nullptr;
+  return NRGPU_OK;
+}
+
+static SymVars sym_vars(double *const *u, int nv) {
+  SymVars S;
+  for (int v = 0; v < NRGPU_Z4_NVARS; ++v) S.p[v] = v < nv ? u[v] : nullptr;
+  return S;
+}
+
+// the parity of each variable of a system under x -> -x, y -> -y, z -> -z:
+// VarSymmetry (variables.c) of the AddVar index strings, "ij+ji" for g~ and
+// A~ (xx xy xz yy yz zz), "I" for Gamma~, beta and B, scalars otherwise
+static SymParity parity_table(int system) {
+  SymParity P;
+  const int nv = system == NRGPU_SYSTEM_BSSN ? NRGPU_NV : NRGPU_Z4_NVARS;
+  static const int ij[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+  // first variable of g~, A~, Gamma~, beta, B in each list
+  const int g = 0, A = 7, G = 14, beta = system == NRGPU_SYSTEM_BSSN ? 18 : 19,
+            B = system == NRGPU_SYSTEM_BSSN ? 21 : 22;
+  for (int v = 0; v < NRGPU_Z4_NVARS; ++v)
+    for (int a = 0; a < 3; ++a) P.s[v][a] = 1;
+  for (int v = 0; v < nv; ++v)
+    for (int a = 0; a < 3; ++a) {
+      int s = 1;
+      if (v >= g && v < g + 6) s = (ij[v - g][0] == a ? -1 : 1) * (ij[v - g][1] == a ? -1 : 1);
+      else if (v >= A && v < A + 6) s = (ij[v - A][0] == a ? -1 : 1) * (ij[v - A][1] == a ? -1 : 1);
+      else if (v >= G && v < G + 3) s = v - G == a ? -1 : 1;
+      else if (v >= beta && v < beta + 3) s = v - beta == a ? -1 : 1;
+      else if (v >= B && v < B + 3) s = v - B == a ? -1 : 1;
+      P.s[v][a] = (signed char)s;
+    }
+  return P;
+}
+
+int nrgpu_level_symmetry(nrgpu_level *L, double *const *u, int system, cudaStream_t st) {
+  if (!L->nsym) return NRGPU_OK;
+  const int nv = system == NRGPU_SYSTEM_BSSN ? NRGPU_NV : NRGPU_Z4_NVARS;
+  SymVars U;
+  for (int v = 0; v < NRGPU_Z4_NVARS; ++v) U.p[v] = v < nv ? u[v] : nullptr;
+  const long n = (long)L->nsym * nv;
+  symmetry_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(U, nv, parity_table(system), L->d_sym, L->nsym);
+  NRGPU_CUDA_TRY(cudaGetLastError());
+  return NRGPU_OK;
+}
+
 static int check_params(const nrgpu_bssn_params *p) {
   if (!p) return nrgpu_set_error(NRGPU_ERR_ARG, "null parameters");
   if (p->order_centered != 2 && p->order_centered != 4 && p->order_centered != 6)
@@ -823,7 +924,8 @@ extern "C" int nrgpu_bssn_boundary(nrgpu_level *L, double *const *unew, double *
     pr = cu;
   }
   Epilogue E = {c != 0.0 ? EPI_ADDLINEAR : EPI_RHS, c, 0.0, 0.0, 0};
-  return launch_rhs(L, cptrs(cu), n, cptrs(pr), n, E, *p, (cudaStream_t)stream, false, true);
+  if ((e = launch_rhs(L, cptrs(cu), n, cptrs(pr), n, E, *p, (cudaStream_t)stream, false, true))) return e;
+  return nrgpu_level_symmetry(L, unew, NRGPU_SYSTEM_BSSN, (cudaStream_t)stream);
 }
 
 extern "C" int nrgpu_bssn_algcon(nrgpu_level *L, double *const *u, const nrgpu_bssn_params *p, void *stream) {
@@ -883,27 +985,56 @@ static RkLists rk_lists(const VarPtrs &U, double *scr, long np) {
 
 // stage sg (0..3) of the step, on the planes kb..ke of the interior and/or
 // the flagged points
+// the epilogue of RK4 stage sg (rk.c:231-255: weights dt/6, dt/3, dt/3,
+// dt/6 into u, dt/2, dt/2, dt into the next stage input)
+static Epilogue stage_epilogue(int sg, double dt) {
+  switch (sg) {
+    case 0: return Epilogue{EPI_RK, 0.0, dt / 6, dt / 2, 1, ACC_INIT};
+    case 1: return Epilogue{EPI_RK, 0.0, dt / 3, dt / 2, 1, ACC_ADD};
+    case 2: return Epilogue{EPI_RK, 0.0, dt / 3, dt, 1, ACC_ADD};
+    default: return Epilogue{EPI_RK, 0.0, dt / 6, 0.0, 0, ACC_FINAL};
+  }
+}
+
+static int rk_stage_parts(nrgpu_level *L, const RkLists &R, int sg, double dt, const nrgpu_bssn_params &p,
+                          cudaStream_t st, bool interior, bool flagged, int kb, int ke) {
+  const CVarPtrs cU = cptrs(R.U);
+  const Epilogue E = stage_epilogue(sg, dt);
+  switch (sg) {
+    case 0: return launch_rhs(L, cU, R.V1, cU, R.A, E, p, st, interior, flagged, kb, ke);
+    case 1: return launch_rhs(L, cptrs(R.V1), R.V2, cU, R.A, E, p, st, interior, flagged, kb, ke);
+    case 2: return launch_rhs(L, cptrs(R.V2), R.V1, cU, R.A, E, p, st, interior, flagged, kb, ke);
+    default: return launch_rhs(L, cptrs(R.V1), R.U, cU, R.A, E, p, st, interior, flagged, kb, ke);
+  }
+}
+
+// a stage, or part of one; after a whole stage the symmetry ghosts of its
+// output (the next stage's input, or u after the last) are reflected, which
+// gives the reference's values: it reflects the rhs (set_boundary), and the
+// RK updates are linear
 static int rk_stage(nrgpu_level *L, const RkLists &R, int sg, double dt, const nrgpu_bssn_params &p,
                     cudaStream_t st, bool interior, bool flagged, int kb = 1, int ke = 1 << 30) {
-  const CVarPtrs cU = cptrs(R.U);
-  switch (sg) {
-    case 0: {
-      const Epilogue E = {EPI_RK, 0.0, dt / 6, dt / 2, 1, ACC_INIT};
-      return launch_rhs(L, cU, R.V1, cU, R.A, E, p, st, interior, flagged, kb, ke);
-    }
-    case 1: {
-      const Epilogue E = {EPI_RK, 0.0, dt / 3, dt / 2, 1, ACC_ADD};
-      return launch_rhs(L, cptrs(R.V1), R.V2, cU, R.A, E, p, st, interior, flagged, kb, ke);
-    }
-    case 2: {
-      const Epilogue E = {EPI_RK, 0.0, dt / 3, dt, 1, ACC_ADD};
-      return launch_rhs(L, cptrs(R.V2), R.V1, cU, R.A, E, p, st, interior, flagged, kb, ke);
-    }
-    default: {
-      const Epilogue E = {EPI_RK, 0.0, dt / 6, 0.0, 0, ACC_FINAL};
-      return launch_rhs(L, cptrs(R.V1), R.U, cU, R.A, E, p, st, interior, flagged, kb, ke);
-    }
-  }
+  if (!L->nsym) return rk_stage_parts(L, R, sg, dt, p, st, interior, flagged, kb, ke);
+  // a symmetry grid: the reference's order, unfused: the rhs of the stage
+  // input, its radiative boundary and its reflection (set_boundary,
+  // boundary.c:221), then the updates of evolve_rk_rk4 at every point
+  const VarPtrs &in = sg == 0 ? R.U : (sg == 2 ? R.V2 : R.V1);
+  const VarPtrs &out = sg == 0 || sg == 2 ? R.V1 : (sg == 1 ? R.V2 : R.U);
+  const Epilogue E = stage_epilogue(sg, dt);
+  SymVars RS;
+  int e = sym_rhs_list(L, NRGPU_NV, &RS);
+  if (e) return e;
+  VarPtrs Rp;
+  for (int v = 0; v < NRGPU_NV; ++v) Rp.p[v] = RS.p[v];
+  const Epilogue Er = {EPI_RHS, 0.0, 0.0, 0.0, 0, 0};
+  if ((e = launch_rhs(L, cptrs(in), Rp, cptrs(in), Rp, Er, p, st, true, true))) return e;
+  if ((e = nrgpu_level_symmetry(L, Rp.p, NRGPU_SYSTEM_BSSN, st))) return e;
+  const long n = (long)NRGPU_NV * L->npoints;
+  rk_update_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(RS, sym_vars(out.p, NRGPU_NV),
+                                                                sym_vars(R.U.p, NRGPU_NV), sym_vars(R.A.p, NRGPU_NV),
+                                                                E, NRGPU_NV, L->npoints);
+  NRGPU_CUDA_TRY(cudaGetLastError());
+  return NRGPU_OK;
 }
 
 // fused RK4 (rk.c:220-257): stage s reads V_in, adds w_s*r to u and writes
@@ -1012,7 +1143,7 @@ extern "C" int nrgpu_bssn_evolve_host(nrgpu_level *L, double *const *host_u, int
   // slabs of ps planes; H = the stencils' reach in planes
   const BoxGeo &b0 = L->hbox[0];
   const long hp = host_pitch(host_u, np);
-  const bool pipe = L->nboxes == 1 && b0.o >= 2 * NRGPU_HOST_SLABS && nsteps > 0 && hp > 0;
+  const bool pipe = L->nboxes == 1 && b0.o >= 2 * NRGPU_HOST_SLABS && nsteps > 0 && hp > 0 && !L->nsym;
   const int ps = pipe ? (b0.o + NRGPU_HOST_SLABS - 1) / NRGPU_HOST_SLABS : b0.o;
   const int ns = pipe ? (b0.o + ps - 1) / ps : 1;
   const long mn = pipe ? (long)b0.m * b0.n : 0;
@@ -1346,7 +1477,8 @@ extern "C" int nrgpu_z4_boundary(nrgpu_level *L, double *const *unew, double *co
     pr = cu;
   }
   Epilogue E = {c != 0.0 ? EPI_ADDLINEAR : EPI_RHS, c, 0.0, 0.0, 0};
-  return z4_launch(L, z4_c(cu), n, z4_c(pr), n, E, *p, (cudaStream_t)stream, false, true);
+  if ((e = z4_launch(L, z4_c(cu), n, z4_c(pr), n, E, *p, (cudaStream_t)stream, false, true))) return e;
+  return nrgpu_level_symmetry(L, unew, NRGPU_SYSTEM_Z4C, (cudaStream_t)stream);
 }
 
 // evolve_rk_rk4 (rk.c:220) for the Z4c list + z4_algcon_wrapper (z4.c:49)
@@ -1372,6 +1504,26 @@ int nrgpu_z4_rk4_stages(nrgpu_level *L, double *const *u, double dt, const nrgpu
   const Epilogue E2 = {EPI_RK, 0.0, dt / 3, dt / 2, 1, ACC_ADD};
   const Epilogue E3 = {EPI_RK, 0.0, dt / 3, dt, 1, ACC_ADD};
   const Epilogue E4 = {EPI_RK, 0.0, dt / 6, 0.0, 0, ACC_FINAL};
+  if (L->nsym) {
+    // a symmetry grid: rhs, radiative boundary and reflection of the rhs,
+    // then the updates at every point (as for BSSN, rk_stage)
+    SymVars RS;
+    if ((e = sym_rhs_list(L, ZNV, &RS))) return e;
+    ZVarPtrs Rp;
+    for (int v = 0; v < ZNV; ++v) Rp.p[v] = RS.p[v];
+    const Epilogue Er = {EPI_RHS, 0.0, 0.0, 0.0, 0, 0};
+    const ZVarPtrs *ins[4] = {&U, &V1, &V2, &V1}, *outs[4] = {&V1, &V2, &V1, &U};
+    for (int sg = 0; sg < 4; ++sg) {
+      if ((e = z4_launch(L, z4_c(*ins[sg]), Rp, z4_c(*ins[sg]), Rp, Er, *p, st, true, true))) return e;
+      if ((e = nrgpu_level_symmetry(L, Rp.p, NRGPU_SYSTEM_Z4C, st))) return e;
+      const long n = (long)ZNV * L->npoints;
+      rk_update_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(RS, sym_vars(outs[sg]->p, ZNV), sym_vars(U.p, ZNV),
+                                                                    sym_vars(A.p, ZNV), stage_epilogue(sg, dt), ZNV,
+                                                                    L->npoints);
+      NRGPU_CUDA_TRY(cudaGetLastError());
+    }
+    return NRGPU_OK;
+  }
   if ((e = z4_launch(L, cU, V1, cU, A, E1, *p, st, true, true))) return e;
   if ((e = z4_launch(L, z4_c(V1), V2, cU, A, E2, *p, st, true, true))) return e;
   if ((e = z4_launch(L, z4_c(V2), V1, cU, A, E3, *p, st, true, true))) return e;

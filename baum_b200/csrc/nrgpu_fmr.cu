@@ -508,6 +508,8 @@ extern "C" int nrgpu_fmr_create(int nl, const nrgpu_level_desc *levels, const do
   for (int l = 0; l < nl && !e; ++l) {
     const nrgpu_level_desc &d = levels[l];
     if (d.nboxes < 1 || !d.box) e = nrgpu_set_error(NRGPU_ERR_ARG, "level %d: no boxes", l);
+    else if (d.symmetry)
+      e = nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "level %d: symmetry grids in the refinement driver", l);
     else if (dt[l] <= 0) e = nrgpu_set_error(NRGPU_ERR_ARG, "level %d: dt %g", l, dt[l]);
     if (e) break;
     F->box[l].clear();

@@ -12,6 +12,13 @@ struct FlagPoint {
 // z slabs of the pipelined host-buffer step (nrgpu_bssn_evolve_host)
 #define NRGPU_HOST_SLABS 8
 
+// a symmetry ghost (SYMBOUND point), its mirror image and the reflected
+// axes (bit 0 x, 1 y, 2 z): the value is the mirror's times the variable's
+// parity under those reflections
+struct SymPoint {
+  int dst, src, mask;
+};
+
 struct nrgpu_level {
   int device;
   int nboxes;
@@ -33,6 +40,11 @@ struct nrgpu_level {
   double *d_red;
   // extents of the rhs kernels' 128-thread blocks (x, y, z)
   int blk[3];
+  // reflection symmetry: the axes (desc.symmetry), the ghost list, and the
+  // rhs list of the unfused RK stages of a symmetry grid (first use)
+  int symmetry, nsym;
+  SymPoint *d_sym;
+  double *rsym;
   // copy and compute streams, and per-slab events, of the pipelined
   // host-buffer step (created on first use)
   cudaStream_t hs_copy, hs_comp;
@@ -47,3 +59,6 @@ int nrgpu_z4_rk4_stages(nrgpu_level *L, double *const *u, double dt, const nrgpu
 int nrgpu_z4_algcon(nrgpu_level *L, double *const *u, const nrgpu_z4_params *p, cudaStream_t st);
 // the level's three RK4 scratch lists, allocated on first use (nrgpu_lib.cu)
 int nrgpu_level_scratch(nrgpu_level *L, double **out);
+// set_boundary_symmetry on a list of nv variables of the given system
+// (NRGPU_SYSTEM_BSSN / _Z4C); nothing without symmetry (nrgpu_bssn.cu)
+int nrgpu_level_symmetry(nrgpu_level *L, double *const *u, int system, cudaStream_t st);

@@ -82,10 +82,39 @@ extern "C" int nrgpu_level_create(const nrgpu_level_desc *d, nrgpu_level **out) 
           const int ijk = bx.noffset + i + bx.m * (j + bx.n * k);
           const int f = d->boundary[ijk];
           if (f == 0) continue;
-          if (f != NRGPU_PHYBOUND && f != NRGPU_REFBOUND)
-            return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "boundary flag %d at point %d (only 0, PHYBOUND, REFBOUND)",
-                                   f, ijk);
+          if (f != NRGPU_PHYBOUND && f != NRGPU_REFBOUND && !(f == NRGPU_SYMBOUND && d->symmetry))
+            return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED,
+                                   "boundary flag %d at point %d (0, PHYBOUND, REFBOUND, SYMBOUND with symmetry)", f,
+                                   ijk);
           fl.push_back(FlagPoint{ijk, i, j, k, b, f});
+        }
+  }
+  // symmetry ghosts: set_boundary_reflection_one (symmetry.c:28-82) copies the
+  // nneg = (int)(1 - lo / h) planes below zero from planes 2 nneg - 1 - n, axis
+  // after axis; the result is the mirror image with the product of parities
+  if (d->symmetry < 0 || d->symmetry > 7) return nrgpu_set_error(NRGPU_ERR_ARG, "symmetry mask %d", d->symmetry);
+  std::vector<SymPoint> sym;
+  for (int b = 0; b < d->nboxes && d->symmetry; ++b) {
+    const nrgpu_box &bx = d->box[b];
+    const int n3[3] = {bx.m, bx.n, bx.o};
+    const double lo[3] = {bx.x0, bx.y0, bx.z0}, h[3] = {d->dx, d->dy, d->dz};
+    int nneg[3];
+    for (int a = 0; a < 3; ++a) {
+      nneg[a] = (d->symmetry >> a & 1) && lo[a] < 0 ? (int)(1 - lo[a] / h[a]) : 0;
+      if (2 * nneg[a] > n3[a]) return nrgpu_set_error(NRGPU_ERR_ARG, "box %d: no mirror for the symmetry ghosts", b);
+    }
+    for (int k = 0; k < bx.o; ++k)
+      for (int j = 0; j < bx.n; ++j)
+        for (int i = 0; i < bx.m; ++i) {
+          int idx[3] = {i, j, k}, src[3] = {i, j, k}, mask = 0;
+          for (int a = 0; a < 3; ++a)
+            if (idx[a] < nneg[a]) {
+              mask |= 1 << a;
+              src[a] = 2 * nneg[a] - 1 - idx[a];
+            }
+          if (!mask) continue;
+          sym.push_back(SymPoint{bx.noffset + i + bx.m * (j + bx.n * k),
+                                 bx.noffset + src[0] + bx.m * (src[1] + bx.n * src[2]), mask});
         }
   }
   nrgpu_level *L = (nrgpu_level *)calloc(1, sizeof(nrgpu_level));
@@ -101,16 +130,21 @@ extern "C" int nrgpu_level_create(const nrgpu_level_desc *d, nrgpu_level **out) 
   L->nflagpts = (int)fl.size();
   L->ninner = (long)d->npoints - (long)fl.size();
   L->blk[0] = 32; L->blk[1] = 4; L->blk[2] = 1;
+  L->symmetry = d->symmetry;
+  L->nsym = (int)sym.size();
   bool ok = cudaMalloc(&L->d_boundary, sizeof(int) * d->npoints) == cudaSuccess &&
             cudaMalloc(&L->d_box, sizeof(BoxGeo) * d->nboxes) == cudaSuccess &&
             cudaMalloc(&L->d_status, sizeof(int) * 4) == cudaSuccess &&
-            (fl.empty() || cudaMalloc(&L->d_flagpts, sizeof(FlagPoint) * fl.size()) == cudaSuccess);
+            (fl.empty() || cudaMalloc(&L->d_flagpts, sizeof(FlagPoint) * fl.size()) == cudaSuccess) &&
+            (sym.empty() || cudaMalloc(&L->d_sym, sizeof(SymPoint) * sym.size()) == cudaSuccess);
   if (ok)
     ok = cudaMemcpy(L->d_boundary, d->boundary, sizeof(int) * d->npoints, cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemcpy(L->d_box, L->hbox, sizeof(BoxGeo) * d->nboxes, cudaMemcpyHostToDevice) == cudaSuccess &&
          cudaMemset(L->d_status, 0, sizeof(int) * 4) == cudaSuccess &&
          (fl.empty() ||
-          cudaMemcpy(L->d_flagpts, fl.data(), sizeof(FlagPoint) * fl.size(), cudaMemcpyHostToDevice) == cudaSuccess);
+          cudaMemcpy(L->d_flagpts, fl.data(), sizeof(FlagPoint) * fl.size(), cudaMemcpyHostToDevice) == cudaSuccess) &&
+         (sym.empty() ||
+          cudaMemcpy(L->d_sym, sym.data(), sizeof(SymPoint) * sym.size(), cudaMemcpyHostToDevice) == cudaSuccess);
   if (!ok) {
     nrgpu_level_destroy(L);
     return nrgpu_set_error(NRGPU_ERR_NOMEM, "device allocation of the level mirror failed");
@@ -125,6 +159,8 @@ extern "C" int nrgpu_level_destroy(nrgpu_level *L) {
   cudaFree(L->d_box);
   cudaFree(L->d_status);
   cudaFree(L->d_flagpts);
+  cudaFree(L->d_sym);
+  cudaFree(L->rsym);
   cudaFree(L->scratch);
   cudaFree(L->hoststate);
   cudaFree(L->d_red);

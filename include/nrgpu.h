@@ -66,6 +66,11 @@ typedef struct {
   int npoints;            /* sum over boxes of m*n*o */
   double dx, dy, dz;
   const int *boundary;    /* host array [npoints], tL.boundary */
+  int symmetry;           /* reflections about x = 0 (bit 0), y = 0 (bit 1) and
+                             z = 0 (bit 2): grid = octant 7, bitant 4,
+                             qreflect 6 (set_boundary_symmetry, symmetry.c:93-140);
+                             the points below zero on those axes are the
+                             SYMBOUND ghosts.  0: none */
 } nrgpu_level_desc;
 
 typedef struct nrgpu_level nrgpu_level;  /* opaque device mirror of a level */

@@ -9,6 +9,7 @@
  *   bssn_rhs_movpunc_N   (spec bssn_rhs_movpunc_N.m:18-461; generated
  *                         bssn_rhs_movpunc_N.c:27-15516), non-shell branch
  *   set_boundary_rot_rad (radiative.c:105-300) with rot = 0
+ *   set_boundary_symmetry (symmetry.c:93-140), reflections only
  *   bssn_algcon          (bssn_algcon.c:25-230)
  *   evolve_rk_rk4        (rk.c:220-257) with vladd/vladdto (variables.c:650,721)
  * Finite-difference weights follow discretize.m:18-50 (centred),
@@ -559,9 +560,66 @@ static double computedel(const double *var, double vx, long ccc, long mcc, long 
 #undef LFT
 }
 
-/* set_boundary_rot_rad (radiative.c:105) without rotation, nv variables */
+/* VarSymmetry (variables.c) of the evolved variables, from their AddVar
+ * index strings: g~ and A~ "ij+ji" (xx xy xz yy yz zz), Gamma~, beta and B
+ * "I", the rest scalars; the sign of variable v under the reflection of
+ * axis dir.  Z4c lists put Theta before alpha. */
+static double var_parity(int nv, int v, int dir)
+{
+  static const int ij[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+  int beta = nv == NV ? 18 : 19, B = nv == NV ? 21 : 22;
+  if (v < 6) return (ij[v][0] == dir ? -1.0 : 1.0) * (ij[v][1] == dir ? -1.0 : 1.0);
+  if (v >= 7 && v < 13) return (ij[v - 7][0] == dir ? -1.0 : 1.0) * (ij[v - 7][1] == dir ? -1.0 : 1.0);
+  if (v >= 14 && v < 17) return v - 14 == dir ? -1.0 : 1.0;
+  if (v >= beta && v < beta + 3) return v - beta == dir ? -1.0 : 1.0;
+  if (v >= B && v < B + 3) return v - B == dir ? -1.0 : 1.0;
+  return 1.0;
+}
+
+/* set_boundary_symmetry (symmetry.c:93-140) for the reflections of the
+ * level's mask, x then y then z, each by set_boundary_reflection_one
+ * (symmetry.c:28-82): on every box whose lower bound is negative, the
+ * nneg = (int)(1 - lo/h) planes below zero take sign * the value of plane
+ * 2 nneg - 1 - n */
+static void symmetry_nv(const nrgpu_level_desc *L, int nv, double *const *u)
+{
+  for (int dir = 0; dir < 3; dir++) {
+    if (!(L->symmetry >> dir & 1)) continue;
+    double h = dir == 0 ? L->dx : (dir == 1 ? L->dy : L->dz);
+    for (int b = 0; b < L->nboxes; b++) {
+      const nrgpu_box *bx = &L->box[b];
+      double lo = dir == 0 ? bx->x0 : (dir == 1 ? bx->y0 : bx->z0);
+      int nneg = (int)(1 - lo / h), nmax = 2 * nneg - 1;
+      int n3[3] = {bx->m, bx->n, bx->o};
+      long st[3] = {1, bx->m, (long)bx->m * bx->n};
+      int a1 = dir == 0 ? 1 : 0, a2 = dir == 2 ? 1 : 2;
+      if (nneg <= 0) continue;
+      for (int v = 0; v < nv; v++) {
+        double sg = var_parity(nv, v, dir);
+        for (int p2 = 0; p2 < n3[a2]; p2++)
+          for (int p1 = 0; p1 < n3[a1]; p1++) {
+            long base = bx->noffset + p1 * st[a1] + p2 * st[a2];
+            for (int n = 0; n < nneg; n++) u[v][base + n * st[dir]] = sg * u[v][base + (nmax - n) * st[dir]];
+          }
+      }
+    }
+  }
+}
+
+/* set_boundary_rot_rad (radiative.c:105) without rotation, nv variables,
+ * then set_boundary_symmetry on unew (boundary.c:221) */
+static int boundary_rad_nv(const nrgpu_level_desc *L, int nv, double *const *unew, double *const *upre,
+                           double c, double *const *ucur, const double *bvar0, const double *bspeed);
 static int boundary_nv(const nrgpu_level_desc *L, int nv, double *const *unew, double *const *upre,
                        double c, double *const *ucur, const double *bvar0, const double *bspeed)
+{
+  int e = boundary_rad_nv(L, nv, unew, upre, c, ucur, bvar0, bspeed);
+  symmetry_nv(L, nv, unew);
+  return e;
+}
+
+static int boundary_rad_nv(const nrgpu_level_desc *L, int nv, double *const *unew, double *const *upre,
+                           double c, double *const *ucur, const double *bvar0, const double *bspeed)
 {
   int b;
   const double oo2d[3] = {1 / (2 * L->dx), 1 / (2 * L->dy), 1 / (2 * L->dz)};

@@ -19,10 +19,14 @@ def load_golden(name):
     return {k: z[k] for k in z.files}
 
 
-def golden_level(g):
+# the reflection symmetry of the golden grids (grid = box octant / bitant)
+GOLDEN_SYMMETRY = {"bssn_punc_octant": 7, "bssn_fourier_bitant": 4}
+
+
+def golden_level(g, symmetry=0):
     from baum_b200 import abi
     boxes = [(int(b[0]), int(b[1]), int(b[2]), b[4], b[5], b[6]) for b in g["boxes"]]
-    return abi.Level(boxes, float(g["dx"]), g["boundary"])
+    return abi.Level(boxes, float(g["dx"]), g["boundary"], symmetry=symmetry)
 
 
 def relerr(a, b, floor=1e-8):

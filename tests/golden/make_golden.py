@@ -107,6 +107,45 @@ order_dissipation = 6
 iterations = 4
 nrharness_dump = 0 4
 """,
+    # symmetry reflections (set_boundary_symmetry, symmetry.c:93-140): the
+    # puncture on an octant grid (two ghost planes below zero on each axis,
+    # reflected with each variable's parity), and the Fourier data on a
+    # bitant grid (z reflection only; the data themselves are not symmetric,
+    # so the ghosts differ from the reflection until the first stage)
+    "bssn_punc_octant": BSSN_COMMON.replace("grid = box", "grid = box octant") + """
+physics = adm bssn punctures nrharness
+mass1 = 1
+mass2 = 0
+punctures_solver = none
+bssn_initial_lapse = oochi05
+bssn_initial_shift = zero
+nxyz = 24
+dxyz = 0.25
+order_centered = 4
+order_advection = 4
+advection_lopsided = 1
+order_dissipation = 6
+iterations = 4
+nrharness_rhs = yes
+nrharness_dump = 0 4
+""",
+    "bssn_fourier_bitant": BSSN_COMMON.replace("grid = box", "grid = box bitant") + """
+physics = adm bssn nrharness
+adm_data = Minkowski
+nxyz = 14
+dxyz = 0.5
+order_centered = 4
+order_advection = 4
+advection_lopsided = 1
+order_dissipation = 6
+iterations = 2
+nrharness_dump = 0 2
+nrharness_rhs = yes
+nrharness_data = fourier
+nrharness_amp = 0.05
+nrharness_length = 4.5
+nrharness_seed = 3
+""",
     # puncture with generic shift and KO: ADM variables and constraints
     "bssn_punc_con": BSSN_COMMON + """
 physics = adm bssn punctures nrharness
