@@ -18,7 +18,7 @@
  *   nrgpu_mode = fmr        the whole Berger-Oliger step of all levels (one
  *                           or several boxes each) runs on the GPU at level
  *                           0's EVOLVE hook; set bssn/z4_register_algcon = no.
- * physics with z4 selects the Z4c system (resident and fmr modes).
+ * physics with z4 selects the Z4c system (all three modes).
  *
  *   nrgpu_multigrid = yes   the puncture initial-data solve (punctures_solver
  *                           = multigrid, PunctureSolve.c:282) runs on the
@@ -264,6 +264,46 @@ void nrgpu_bssn_boundary_cb(tVarList *unew, tVarList *upre, double c, tVarList *
   copy_vl(level, unew, s->d_a, 0);
 }
 
+/* "geometry" callback of the Z4c system: replaces z4_evolve /
+ * z4_rhs_movpunc_N (z4.c:17-19, registered at z4.c:245) */
+void nrgpu_z4_evolve_cb(tVarList *unew, tVarList *upre, double c, tVarList *ucur)
+{
+  tL *level = ucur->level;
+  nrgpu_slot *s = slot_of(level);
+  nrgpu_z4_params p;
+  double *n[ZNV], *pr[ZNV], *cu[ZNV];
+  timer_start(level, "z4_rhs");
+  read_params_z4(level, ucur, &p);
+  lists(s->d_a, level->npoints, n);
+  lists(s->d_b, level->npoints, pr);
+  lists(s->d_c, level->npoints, cu);
+  copy_vl(level, ucur, s->d_c, 1);
+  copy_vl(level, unew, s->d_a, 1);
+  if (c != 0.0) copy_vl(level, upre, s->d_b, 1);
+  check(nrgpu_z4_rhs(s->lev, n, c != 0.0 ? pr : cu, c, cu, &p, 0), "rhs");
+  copy_vl(level, unew, s->d_a, 0);
+  timer_stop(level, "z4_rhs");
+}
+
+/* "geometry_bound" callback of the Z4c system: replaces set_boundary
+ * (z4.c:248) with the radiative condition and the symmetry reflections */
+void nrgpu_z4_boundary_cb(tVarList *unew, tVarList *upre, double c, tVarList *ucur)
+{
+  tL *level = ucur->level;
+  nrgpu_slot *s = slot_of(level);
+  nrgpu_z4_params p;
+  double *n[ZNV], *pr[ZNV], *cu[ZNV];
+  read_params_z4(level, ucur, &p);
+  lists(s->d_a, level->npoints, n);
+  lists(s->d_b, level->npoints, pr);
+  lists(s->d_c, level->npoints, cu);
+  copy_vl(level, ucur, s->d_c, 1);
+  copy_vl(level, unew, s->d_a, 1);
+  if (c != 0.0) copy_vl(level, upre, s->d_b, 1);
+  check(nrgpu_z4_boundary(s->lev, n, c != 0.0 ? pr : cu, c, cu, &p, 0), "boundary");
+  copy_vl(level, unew, s->d_a, 0);
+}
+
 /* EVOLVE hook of the resident mode: evolve_rk_rk4 + algcon on the device */
 int nrgpu_evolve_resident(tL *level)
 {
@@ -475,7 +515,8 @@ int nrgpu_startup(tL *level)
     if (Getv(nrgpu_system_z4 ? "z4_register_algcon" : "bssn_register_algcon", "yes"))
       errorexit("nrgpu: the GPU runs the algebraic constraints in this mode, set bssn/z4_register_algcon = no");
   } else if (nrgpu_system_z4) {
-    errorexit("nrgpu: for z4 use nrgpu_mode = resident or fmr");
+    set_rhs_func_register("geometry", nrgpu_z4_evolve_cb);
+    set_rhs_func_register("geometry_bound", nrgpu_z4_boundary_cb);
   } else {
     set_rhs_func_register("geometry", nrgpu_bssn_evolve_cb);
     set_rhs_func_register("geometry_bound", nrgpu_bssn_boundary_cb);

@@ -208,3 +208,59 @@ def test_bam_multigrid_on_the_gpu_matches_bam(gpu, cpu_state):
     u_host, out_host = run_mg(BAM_GPU, " nrgpu", "nrgpu_multigrid = no")
     assert "multigrid on the host" in out_host
     assert np.abs(u_host - u_ref).max() <= 1e-12 * np.abs(u_ref).max()   # OpenMP sums may reorder
+
+
+Z4_PAR = """physics = adm z4 nrharness%s
+adm_data = Minkowski
+z4_lapse = 1+log withshift
+z4_shift = gamma0 withGadv withBadv withShiftadv withB
+z4_shiftdriver = 2.0
+z4_shiftgammacoeff = 0.75
+z4_kappa1 = 0.02
+z4_kappa2 = 0.0
+grid = %s
+nxyz = 20
+dxyz = 0.4
+order_centered = 4
+order_advection = 4
+advection_lopsided = 1
+order_dissipation = 6
+dissipation_factor = 0.1
+evolution_method = rk
+evolution_method_rk = rk4
+dtfac = 0.25
+boundary = radiative
+iterations = 4
+nrharness_dir = .
+nrharness_data = fourier
+nrharness_amp = 0.05
+nrharness_length = 8
+nrharness_dump = 4
+%s
+"""
+
+
+def run_z4(binary, extra_physics, grid, extra):
+    work = tempfile.mkdtemp(prefix="bamgpu_")
+    try:
+        with open(os.path.join(work, "t.par"), "w") as f:
+            f.write(Z4_PAR % (extra_physics, grid, extra))
+        r = subprocess.run([binary, "-nt", "4", "t.par"], cwd=work, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+        return dumpfile.read(os.path.join(work, "state_it4_l0.bin"))["data"], r.stdout
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+@pytest.mark.parametrize("grid", ["box", "box octant"])
+@pytest.mark.parametrize("mode,extra", [("callback", "nrgpu_mode = callback"),
+                                        ("resident", "nrgpu_mode = resident\nz4_register_algcon = no")])
+def test_bam_z4_with_the_gpu_path_matches_bam(gpu, cpu_state, grid, mode, extra):
+    """The Z4c system inside BAM: the GPU rhs and boundary callbacks (BAM
+    keeps its RK4 and algcon), or the whole RK4 step at the EVOLVE hook, on
+    a plain box and on an octant grid (symmetry reflections), against plain
+    BAM after 4 steps."""
+    ref, _ = run_z4(BAM, "", grid, "")
+    got, out = run_z4(BAM_GPU, " nrgpu", grid, extra)
+    assert "nrgpu: %s mode" % mode in out
+    assert relerr(got, ref).max() < 1e-12
