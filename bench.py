@@ -251,7 +251,7 @@ FMR_SIZES = [162, 136, 168, 104, 136, 72, 104]
 FMR_DX0 = 0.5
 
 
-def gpu_fmr(steps=2):
+def gpu_fmr(steps=2, variants=(("graph", 1, 1), ("launches", 0, 1), ("graph_untuned_32x4", 1, 0)), warm=2):
     import torch
     from baum_b200 import abi, fmr, synthetic
     levels = fmr.nested_levels(FMR_SIZES, FMR_DX0)
@@ -267,12 +267,13 @@ def gpu_fmr(steps=2):
            "rhs_point_updates_per_coarse_step": upd_per_coarse}
     # the product configuration (graph + per-level tuned block shapes), then
     # plain launches, then the graph with every level at the 32 x 4 default
-    for key, use_graph, tune in (("graph", 1, 1), ("launches", 0, 1), ("graph_untuned_32x4", 1, 0)):
+    for key, use_graph, tune in variants:
         H = fmr.Hierarchy(levels, dt, params, abi.fmr_params(use_graph=use_graph, autotune=tune))
         blocks = ["%dx%dx%d" % H.block(l) for l in range(len(levels))]
         u = [state(lev) for lev in levels]
         H.advance(u, 1)   # first coarse step: 2nd-order time interpolation, no graph
-        H.advance(u, 1)   # graph capture (with use_graph)
+        for _ in range(warm - 1):
+            H.advance(u, 1)   # graph capture (with use_graph)
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
@@ -599,15 +600,25 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--case", default="c1", choices=["c1", "c1-step", "mg", "z4c160"],
+    ap.add_argument("--case", default="c1", choices=["c1", "c1-step", "mg", "fmr", "z4c160"],
                     help="c1: the benchmark line; c1-step: only the 64^3 BSSN RK4 steps and the rhs "
                          "launches of that line (for profiling); mg: only the 130^3 multigrid solve of the "
-                         "first seeded binary (for profiling); z4c160: the 160^3 Z4c box alone")
+                         "first seeded binary (for profiling); fmr: only the 7-level Z4c step, graph replay with tuned "
+                         "blocks, --warmup and --steps coarse steps (for profiling); z4c160: the 160^3 Z4c box "
+                         "alone")
     ap.add_argument("--mg-cycles", type=int, default=0,
                     help="with --case mg: run exactly this many V cycles from the finest level (profiling)")
     args = ap.parse_args()
     if args.case == "z4c160":
         run_z4c160(args)
+        return
+    if args.case == "fmr":
+        import torch
+        from baum_b200 import build
+        build.build()
+        torch.cuda.set_device(0)
+        print(json.dumps({"case": "fmr", **gpu_fmr(args.steps, variants=(("graph", 1, 1),),
+                                                     warm=max(args.warmup, 2))}))
         return
     if args.case == "mg":
         import torch
