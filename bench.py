@@ -398,6 +398,18 @@ def oracle_port_cpu():
             "sample": "1 RK4 step of the 64^3-inner puncture box (oracle restatement, OpenMP)"}
 
 
+def max_over_ranks(values, device):
+    """Each value's maximum over the ranks of the process group (all-reduce
+    MAX; the values themselves when no group of more than one rank is
+    initialised)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -496,12 +508,8 @@ def run_ours(args, rank, world):
         e2e_t.append(time.perf_counter() - t0)
     state_bytes = abi.NVARS * lev.npoints * 8
 
-    if dist:
-        t = torch.tensor([ms, sum(e2e_t)], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_sum = t[0].item(), t[1].item()
-    else:
-        e2e_sum = sum(e2e_t)
+    # the job's times are the slowest rank's (replicas: no data-path exchange)
+    ms, e2e_sum = max_over_ranks([ms, sum(e2e_t)], "cuda")
     if rank != 0:
         return
     units = PTS_PER_RHS * RHS_PER_STEP * args.steps * world
