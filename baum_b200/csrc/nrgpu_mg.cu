@@ -57,14 +57,21 @@ __device__ __forceinline__ bool inner(int i, int j, int k, int m) {
 
 // Robin / Dirichlet gather on the boundary (set_boundary_robin): with far
 // limit 0 the Robin value is u_n (1-c)/(1+c); falloff 0 gives -u_n
+// (each kernel below is a per-point function, *_at(t, ...), called by one
+// grid thread per point, or in block-stride loops by the one-block bottom
+// of the V cycle, bottom_vcycle_kernel)
+__device__ __forceinline__ void robin_at(int t, double *u, const int *__restrict__ bidx,
+                                         const int *__restrict__ bnrm, const double *__restrict__ c1,
+                                         const double *__restrict__ c2, int nb, int dirichlet) {
+  if (t >= nb) return;
+  const double un = u[bnrm[t]];
+  u[bidx[t]] = dirichlet ? -un : un * c1[t] / c2[t];
+}
 __global__ void robin_kernel(double *u, const int *__restrict__ bidx, const int *__restrict__ bnrm,
                              const double *__restrict__ c1, const double *__restrict__ c2, int nb, int dirichlet,
                              const int *__restrict__ done) {
   if (done && *done) return;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nb) return;
-  const double un = u[bnrm[t]];
-  u[bidx[t]] = dirichlet ? -un : un * c1[t] / c2[t];
+  robin_at(blockIdx.x * blockDim.x + threadIdx.x, u, bidx, bnrm, c1, c2, nb, dirichlet);
 }
 
 // w^-7 and w^-8 by multiplication: the reference's pow(w, -7.0) and
@@ -124,12 +131,11 @@ __device__ __forceinline__ void fused_store(double *out, int q, int slot, double
 
 // one Jacobi sweep un = uo + (f - L uo)/L_ii on inner points (Lpuncture_GS),
 // followed by the Robin condition on un (relax.c:19-43 then robin.c:146-223)
-__global__ void jacobi_kernel(const double *__restrict__ uo, double *__restrict__ un, const double *__restrict__ f,
-                              const double *__restrict__ a, const double *__restrict__ b, int m, double cx,
-                              RobinFuse R, const int *__restrict__ done) {
-  if (done && *done) return;
+__device__ __forceinline__ void jacobi_at(int t, const double *__restrict__ uo, double *__restrict__ un,
+                                          const double *__restrict__ f, const double *__restrict__ a,
+                                          const double *__restrict__ b, int m, double cx, const RobinFuse &R) {
   int q, slot;
-  if (!fused_point(blockIdx.x * blockDim.x + threadIdx.x, m * m * m, R, q, slot)) return;
+  if (!fused_point(t, m * m * m, R, q, slot)) return;
   const int i = q % m, j = (q / m) % m, k = q / (m * m);
   if (!inner(i, j, k, m)) return;
   const double cc = -2.0 * (cx + cx + cx);
@@ -137,6 +143,12 @@ __global__ void jacobi_kernel(const double *__restrict__ uo, double *__restrict_
   const double lu = lop_point(uo, q, m, cc, cx, aq, bq);
   const double lii = cc - 7.0 * bq * aq * inv_pow8(1.0 + aq * (1.0 + uq));
   fused_store(un, q, slot, uq + (f[q] - lu) / lii, R);
+}
+__global__ void jacobi_kernel(const double *__restrict__ uo, double *__restrict__ un, const double *__restrict__ f,
+                              const double *__restrict__ a, const double *__restrict__ b, int m, double cx,
+                              RobinFuse R, const int *__restrict__ done) {
+  if (done && *done) return;
+  jacobi_at(blockIdx.x * blockDim.x + threadIdx.x, uo, un, f, a, b, m, cx, R);
 }
 
 // block partial sums of (L u - f)^2 over inner points
@@ -216,13 +228,13 @@ __global__ void restrict_kernel(const double *__restrict__ fv, double *__restric
 // inner coarse points are exactly the inner fine points, so every fine
 // operator value is computed once; the sums run in the order of
 // mg_restrict_var's eight terms.
-__global__ void fine_to_coarse_kernel(const double *__restrict__ uh, const double *__restrict__ fh,
-                                      const double *__restrict__ ah, const double *__restrict__ bh,
-                                      double *__restrict__ uH, double *__restrict__ RfH, double *__restrict__ RluH,
-                                      int mf, int mc, int off, double cxh, RobinFuse R, const int *__restrict__ done) {
-  if (done && *done) return;
+__device__ __forceinline__ void fine_to_coarse_at(int t, const double *__restrict__ uh,
+                                                  const double *__restrict__ fh, const double *__restrict__ ah,
+                                                  const double *__restrict__ bh, double *__restrict__ uH,
+                                                  double *__restrict__ RfH, double *__restrict__ RluH, int mf, int mc,
+                                                  int off, double cxh, const RobinFuse &R) {
   int q, slot;
-  if (!fused_point(blockIdx.x * blockDim.x + threadIdx.x, mc * mc * mc, R, q, slot)) return;
+  if (!fused_point(t, mc * mc * mc, R, q, slot)) return;
   const int I = q % mc, J = (q / mc) % mc, K = q / (mc * mc);
   if (!inner(I, J, K, mc)) return;
   const long mf2 = (long)mf * mf;
@@ -238,21 +250,33 @@ __global__ void fine_to_coarse_kernel(const double *__restrict__ uh, const doubl
   RluH[q] = 0.125 * (lu[0] + lu[1] + lu[2] + lu[3] + lu[4] + lu[5] + lu[6] + lu[7]);
   RfH[q] = 0.125 * (fh[c[0]] + fh[c[1]] + fh[c[2]] + fh[c[3]] + fh[c[4]] + fh[c[5]] + fh[c[6]] + fh[c[7]]);
 }
+__global__ void fine_to_coarse_kernel(const double *__restrict__ uh, const double *__restrict__ fh,
+                                      const double *__restrict__ ah, const double *__restrict__ bh,
+                                      double *__restrict__ uH, double *__restrict__ RfH, double *__restrict__ RluH,
+                                      int mf, int mc, int off, double cxh, RobinFuse R, const int *__restrict__ done) {
+  if (done && *done) return;
+  fine_to_coarse_at(blockIdx.x * blockDim.x + threadIdx.x, uh, fh, ah, bh, uH, RfH, RluH, mf, mc, off, cxh, R);
+}
 
 // the FAS coarse right-hand side fH = R fh + (L uH - R L uh) at inner coarse
 // points (fH holds R fh, RluH holds R L uh), and wH = uH at every point
-__global__ void coarse_rhs_kernel(const double *__restrict__ uH, double *__restrict__ fH,
-                                  const double *__restrict__ RluH, double *__restrict__ wH,
-                                  const double *__restrict__ aH, const double *__restrict__ bH, int mc, double cxH,
-                                  const int *__restrict__ done) {
-  if (done && *done) return;
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void coarse_rhs_at(int q, const double *__restrict__ uH, double *__restrict__ fH,
+                                              const double *__restrict__ RluH, double *__restrict__ wH,
+                                              const double *__restrict__ aH, const double *__restrict__ bH, int mc,
+                                              double cxH) {
   if (q >= mc * mc * mc) return;
   wH[q] = uH[q];
   const int I = q % mc, J = (q / mc) % mc, K = q / (mc * mc);
   if (!inner(I, J, K, mc)) return;
   const double luH = lop_point(uH, q, mc, -2.0 * (cxH + cxH + cxH), cxH, aH[q], bH[q]);
   fH[q] = fH[q] + (luH - RluH[q]);
+}
+__global__ void coarse_rhs_kernel(const double *__restrict__ uH, double *__restrict__ fH,
+                                  const double *__restrict__ RluH, double *__restrict__ wH,
+                                  const double *__restrict__ aH, const double *__restrict__ bH, int mc, double cxH,
+                                  const int *__restrict__ done) {
+  if (done && *done) return;
+  coarse_rhs_at(blockIdx.x * blockDim.x + threadIdx.x, uH, fH, RluH, wH, aH, bH, mc, cxH);
 }
 
 // wH = uH (all points), vH = uH - wH helpers
@@ -261,23 +285,25 @@ __global__ void copy_kernel(const double *__restrict__ s, double *__restrict__ d
   const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (q < n) d[q] = s[q];
 }
+__device__ __forceinline__ void sub_inner_at(int t, const double *__restrict__ x, const double *__restrict__ y,
+                                             double *__restrict__ r, int m, const RobinFuse &R) {
+  int q, slot;
+  if (!fused_point(t, m * m * m, R, q, slot)) return;
+  const int i = q % m, j = (q / m) % m, k = q / (m * m);
+  if (inner(i, j, k, m)) fused_store(r, q, slot, x[q] - y[q], R);
+}
 __global__ void sub_inner_kernel(const double *__restrict__ x, const double *__restrict__ y, double *__restrict__ r,
                                  int m, RobinFuse R, const int *__restrict__ done) {
   if (done && *done) return;
-  int q, slot;
-  if (!fused_point(blockIdx.x * blockDim.x + threadIdx.x, m * m * m, R, q, slot)) return;
-  const int i = q % m, j = (q / m) % m, k = q / (m * m);
-  if (inner(i, j, k, m)) fused_store(r, q, slot, x[q] - y[q], R);
+  sub_inner_at(blockIdx.x * blockDim.x + threadIdx.x, x, y, r, m, R);
 }
 
 // trilinear prolongation of the coarse correction, added to the inner fine
 // points (mg_prolong_var + add); weights 1/4, 3/4 from the cell-centred
 // staggering, coarse index ci = floor((i + off') / 2)
-__global__ void prolong_add_kernel(const double *__restrict__ cv, double *__restrict__ uf, int mf, int mc,
-                                   double fx0, double fdx, double cx0, double cdx, int add,
-                                   const int *__restrict__ done) {
-  if (done && *done) return;
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void prolong_add_at(int q, const double *__restrict__ cv, double *__restrict__ uf,
+                                               int mf, int mc, double fx0, double fdx, double cx0, double cdx,
+                                               int add) {
   if (q >= mf * mf * mf) return;
   const int i = q % mf, j = (q / mf) % mf, k = q / (mf * mf);
   if (!inner(i, j, k, mf)) return;
@@ -293,6 +319,12 @@ __global__ void prolong_add_kernel(const double *__restrict__ cv, double *__rest
                    kx1 * ky0 * kz1 * cv[c0 + 1 + mc2] + kx0 * ky1 * kz1 * cv[c0 + mc + mc2] +
                    kx1 * ky1 * kz1 * cv[c0 + 1 + mc + mc2];
   uf[q] = add ? uf[q] + p : p;
+}
+__global__ void prolong_add_kernel(const double *__restrict__ cv, double *__restrict__ uf, int mf, int mc,
+                                   double fx0, double fdx, double cx0, double cdx, int add,
+                                   const int *__restrict__ done) {
+  if (done && *done) return;
+  prolong_add_at(blockIdx.x * blockDim.x + threadIdx.x, cv, uf, mf, mc, fx0, fdx, cx0, cdx, add);
 }
 
 // "exact" solve of the coarsest level in one thread block (exactsolve):
@@ -366,13 +398,12 @@ __global__ void exact_solve_kernel(double *u, double *u2, const double *f, const
 // coarsest level is a handful of inner points (8 on the 4^3 level) swept up
 // to exact_nmax times per V cycle, so the sweep's latency is the cost.
 constexpr int NRGPU_MG_WARP_SOLVE_MAX = 1000;
-__global__ void __launch_bounds__(32) exact_solve_warp_kernel(double *u, const double *f, const double *a,
-                                                              const double *b, int m, double cx, const int *bidx,
-                                                              const int *bnrm, const double *c1, const double *c2,
-                                                              int nb, int nmin, int nmax, double tol10, MgStatus *st) {
-  if (st->done) return;
-  extern __shared__ double sm[];
-  const int np = m * m * m, lane = threadIdx.x;
+// run by the 32 threads of one warp (lane = threadIdx.x & 31), sm: the
+// level's shared-memory copy (warp_solve_smem bytes)
+__device__ void exact_solve_warp(double *u, const double *f, const double *a, const double *b, int m, double cx,
+                                 const int *bidx, const int *bnrm, const double *c1, const double *c2, int nb,
+                                 int nmin, int nmax, double tol10, MgStatus *st, double *sm) {
+  const int np = m * m * m, lane = threadIdx.x & 31;
   double *su = sm, *sv = su + np, *sa = sv + np, *sb = sa + np, *sf = sb + np, *sc1 = sf + np, *sc2 = sc1 + nb;
   int *sbi = (int *)(sc2 + nb), *sbn = sbi + nb;
   for (int q = lane; q < np; q += 32) {
@@ -436,10 +467,105 @@ __global__ void __launch_bounds__(32) exact_solve_warp_kernel(double *u, const d
   for (int q = lane; q < np; q += 32) u[q] = uo[q];
   if (lane == 0) st->exact_sweeps = it;
 }
+__global__ void __launch_bounds__(32) exact_solve_warp_kernel(double *u, const double *f, const double *a,
+                                                              const double *b, int m, double cx, const int *bidx,
+                                                              const int *bnrm, const double *c1, const double *c2,
+                                                              int nb, int nmin, int nmax, double tol10, MgStatus *st) {
+  if (st->done) return;
+  extern __shared__ double sm[];
+  exact_solve_warp(u, f, a, b, m, cx, bidx, bnrm, c1, c2, nb, nmin, nmax, tol10, st, sm);
+}
 
 static size_t warp_solve_smem(int m, int nb) {
   const size_t np = (size_t)m * m * m, ni = (size_t)(m - 2) * (m - 2) * (m - 2);
   return sizeof(double) * (5 * np + 2 * (size_t)nb) + sizeof(int) * (2 * (size_t)nb + ni);
+}
+
+// The bottom of the V cycle in one thread block: every level of at most
+// NRGPU_MG_BOTTOM_MAX points (10^3 and 6^3 of the 130^3 stack, and the 4^3
+// coarsest) runs the same steps as vcycle() with the same per-point
+// functions, in block-stride loops separated by __syncthreads, instead of
+// ~25 kernels of a few hundred threads.  Each level's u returns to its entry
+// buffer, as in vcycle().  (With the 18^3 level in the block too, one
+// block's sweeps took as long as the launches they replaced.)
+constexpr int NRGPU_MG_BOTTOM_MAX = 1000;
+constexpr int NRGPU_MG_BOTTOM_THREADS = 512;
+constexpr int NRGPU_MG_MAXLEV = 16;
+struct MgDev {
+  int m, nb;
+  double dx, x0;
+  double *u, *u2, *v, *w, *f, *a, *b;
+  const int *bidx, *bnrm;
+  const double *bc1, *bc2;
+};
+
+__global__ void __launch_bounds__(NRGPU_MG_BOTTOM_THREADS)
+    bottom_vcycle_kernel(const MgDev *__restrict__ lv, int top, int npre, int npost, int exact_nmin, int exact_nmax,
+                         double tol10, MgStatus *st, const int *__restrict__ done) {
+  if (done && *done) return;
+  extern __shared__ double sm[];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  double *U[NRGPU_MG_MAXLEV], *U2[NRGPU_MG_MAXLEV];
+  for (int l = 0; l <= top; ++l) {
+    U[l] = lv[l].u;
+    U2[l] = lv[l].u2;
+  }
+  // down: pre-sweeps, restriction and the FAS right-hand side
+  for (int l = top; l >= 1; --l) {
+    const MgDev &h = lv[l], &H = lv[l - 1];
+    const int np = h.m * h.m * h.m, npH = H.m * H.m * H.m;
+    const double cx = 1 / (h.dx * h.dx), cxH = 1 / (H.dx * H.dx);
+    const RobinFuse Rh = {h.bidx, h.bnrm, h.bc1, h.bc2, h.nb, 0}, RH = {H.bidx, H.bnrm, H.bc1, H.bc2, H.nb, 0};
+    for (int s = 0; s < npre; ++s) {
+      for (int t = tid; t < np + h.nb; t += nt) jacobi_at(t, U[l], U2[l], h.f, h.a, h.b, h.m, cx, Rh);
+      __syncthreads();
+      double *x = U[l];
+      U[l] = U2[l];
+      U2[l] = x;
+    }
+    if (npre == 0) {
+      for (int t = tid; t < h.nb; t += nt) robin_at(t, U[l], h.bidx, h.bnrm, h.bc1, h.bc2, h.nb, 0);
+      __syncthreads();
+    }
+    for (int t = tid; t < npH + H.nb; t += nt)
+      fine_to_coarse_at(t, U[l], h.f, h.a, h.b, U[l - 1], H.f, H.v, h.m, H.m, 1, cx, RH);
+    __syncthreads();
+    for (int t = tid; t < npH; t += nt) coarse_rhs_at(t, U[l - 1], H.f, H.v, H.w, H.a, H.b, H.m, cxH);
+    __syncthreads();
+  }
+  // the coarsest level, by the first warp
+  if (tid < 32) {
+    const MgDev &c = lv[0];
+    exact_solve_warp(U[0], c.f, c.a, c.b, c.m, 1 / (c.dx * c.dx), c.bidx, c.bnrm, c.bc1, c.bc2, c.nb, exact_nmin,
+                     exact_nmax, tol10, st, sm);
+  }
+  __syncthreads();
+  // up: correction, prolongation, Robin condition, post-sweeps
+  for (int l = 1; l <= top; ++l) {
+    const MgDev &h = lv[l], &H = lv[l - 1];
+    const int np = h.m * h.m * h.m, npH = H.m * H.m * H.m;
+    const double cx = 1 / (h.dx * h.dx);
+    const RobinFuse Rh = {h.bidx, h.bnrm, h.bc1, h.bc2, h.nb, 0}, RHd = {H.bidx, H.bnrm, H.bc1, H.bc2, H.nb, 1};
+    for (int t = tid; t < npH + H.nb; t += nt) sub_inner_at(t, U[l - 1], H.w, H.v, H.m, RHd);
+    __syncthreads();
+    for (int t = tid; t < np; t += nt) prolong_add_at(t, H.v, U[l], h.m, H.m, h.x0, h.dx, H.x0, H.dx, 1);
+    __syncthreads();
+    for (int t = tid; t < h.nb; t += nt) robin_at(t, U[l], h.bidx, h.bnrm, h.bc1, h.bc2, h.nb, 0);
+    __syncthreads();
+    for (int s = 0; s < npost; ++s) {
+      for (int t = tid; t < np + h.nb; t += nt) jacobi_at(t, U[l], U2[l], h.f, h.a, h.b, h.m, cx, Rh);
+      __syncthreads();
+      double *x = U[l];
+      U[l] = U2[l];
+      U2[l] = x;
+    }
+    if (U[l] != h.u) {
+      for (int t = tid; t < np; t += nt) h.u[t] = U[l][t];
+      __syncthreads();
+      U2[l] = U[l];
+      U[l] = h.u;
+    }
+  }
 }
 
 __global__ void robin_factors_kernel(const int *bidx, const int *bnrm, double *c1, double *c2, int nb, int m, double x0,
@@ -508,6 +634,9 @@ struct nrgpu_mg {
   cudaStream_t stream;  // library-owned (captured into CUDA graphs)
   cudaGraph_t graph[16];
   cudaGraphExec_t exec[16];
+  // the one-block bottom of the V cycle: levels 0..bottom (0: not used)
+  int bottom;
+  MgDev *d_lv;
 };
 
 // stack sizes (coarsegridsize, makestack.c:36-79) for one process
@@ -583,6 +712,7 @@ extern "C" int nrgpu_mg_destroy(nrgpu_mg *M) {
   }
   cudaFree(M->st);
   cudaFree(M->partial);
+  cudaFree(M->d_lv);
   if (M->stream) cudaStreamDestroy(M->stream);
   free(M);
   return NRGPU_OK;
@@ -628,7 +758,23 @@ extern "C" int nrgpu_mg_create(int m, double dx, const nrgpu_mg_params *p, nrgpu
     const size_t sm = warp_solve_smem(M->lv[0].m, M->lv[0].nb);
     if (sm > 48 * 1024)
       ok = cudaFuncSetAttribute(exact_solve_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) ==
-           cudaSuccess;
+               cudaSuccess &&
+           cudaFuncSetAttribute(bottom_vcycle_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) ==
+               cudaSuccess;
+    // the one-block bottom: the levels above the coarsest with at most
+    // NRGPU_MG_BOTTOM_MAX points
+    int top = 0;
+    while (top + 1 < nl && M->lv[top + 1].np <= NRGPU_MG_BOTTOM_MAX) ++top;
+    if (ok && top >= 1) {
+      MgDev dv[NRGPU_MG_MAXLEV];
+      for (int l = 0; l <= top; ++l) {
+        const MgLevel &L = M->lv[l];
+        dv[l] = MgDev{L.m, L.nb, L.dx, L.x0, L.u, L.u2, L.v, L.w, L.f, L.a, L.b, L.bidx, L.bnrm, L.bc1, L.bc2};
+      }
+      ok = cudaMalloc(&M->d_lv, sizeof(MgDev) * (top + 1)) == cudaSuccess &&
+           cudaMemcpy(M->d_lv, dv, sizeof(MgDev) * (top + 1), cudaMemcpyHostToDevice) == cudaSuccess;
+      if (ok) M->bottom = top;
+    }
   }
   M->npartial = (int)nblk(M->lv[nl - 1].np);
   ok = ok && cudaStreamCreateWithFlags(&M->stream, cudaStreamNonBlocking) == cudaSuccess &&
@@ -668,6 +814,11 @@ static void sweeps(nrgpu_mg *M, MgLevel &L, int n, const int *done) {
 constexpr int kChildOff = 1;
 
 static void vcycle(nrgpu_mg *M, int l, const int *done) {
+  if (l >= 1 && l <= M->bottom) {
+    bottom_vcycle_kernel<<<1, NRGPU_MG_BOTTOM_THREADS, warp_solve_smem(M->lv[0].m, M->lv[0].nb), M->stream>>>(
+        M->d_lv, l, M->p.npre, M->p.npost, M->p.exact_nmin, M->p.exact_nmax, M->p.tol / 10, M->st, done);
+    return;
+  }
   MgLevel &h = M->lv[l];
   if (l == 0) {
     if (h.np <= NRGPU_MG_WARP_SOLVE_MAX)
