@@ -118,15 +118,25 @@ nrharness_dump = 2 4 8
 # separate level-2 boxes (the data are the harness's Fourier data)
 BINARY = ("physics = adm z4 nrharness", "physics = adm z4 punctures nrharness"), ("nxyz = 16", "nxyz = 32"), \
     ("mass1 = 1\nmass2 = 0", "mass1 = 0.5\npx1 = 2.75\nmass2 = 0.5\npx2 = -2.75\npunctures_solver = none")
+# the BSSN system on the single-puncture grid
+BSSN_FMR = ("physics = adm z4 nrharness", "physics = adm bssn nrharness"), \
+    ("""z4_lapse = 1+log withshift
+z4_shift = gamma0 withGadv withBadv withShiftadv withB
+z4_shiftdriver = 2.0
+z4_shiftgammacoeff = 0.75
+z4_kappa1 = 0.02
+z4_kappa2 = 0.0""", """bssn_lapse = 1+log withshift
+bssn_shift = gamma0 withGadv withBadv withShiftadv
+bssn_shiftdriver = 2.0
+bssn_shiftgammacoeff = 0.75""")
 
 
 def run_fmr(binary, extra_physics, extra, grid="single"):
     work = tempfile.mkdtemp(prefix="bamgpu_")
     par = FMR_PAR
-    if grid == "binary":
-        for a, b in BINARY:
-            assert a in par
-            par = par.replace(a, b)
+    for a, b in (BINARY if grid == "binary" else BSSN_FMR if grid == "bssn" else ()):
+        assert a in par
+        par = par.replace(a, b)
     try:
         with open(os.path.join(work, "t.par"), "w") as f:
             f.write(par % (extra_physics, extra))
@@ -137,7 +147,7 @@ def run_fmr(binary, extra_physics, extra, grid="single"):
         shutil.rmtree(work, ignore_errors=True)
 
 
-@pytest.mark.parametrize("grid", ["single", "binary"])
+@pytest.mark.parametrize("grid", ["single", "binary", "bssn"])
 def test_bam_fmr_mode_matches_bam(gpu, cpu_state, grid):
     """nrgpu_mode = fmr: the whole Berger-Oliger step of the 3-level Z4c grid
     on the GPU at level 0's EVOLVE hook.  BAM dumps every level right after
@@ -147,11 +157,12 @@ def test_bam_fmr_mode_matches_bam(gpu, cpu_state, grid):
     are compared, after 2 coarse steps, on the points that this last
     restriction and prolongation do not write, within the refinement
     tolerance of the oracle pin (2e-11).  The binary's grid has two boxes
-    on level 2."""
+    on level 2; "bssn" runs the BSSN system on the single-puncture grid."""
     from baum_b200 import abi
     from oracle import oracle
     ref, _ = run_fmr(BAM, "", "", grid)
-    got, out = run_fmr(BAM_GPU, " nrgpu", "nrgpu_mode = fmr\nz4_register_algcon = no", grid)
+    algcon = "bssn_register_algcon = no" if grid == "bssn" else "z4_register_algcon = no"
+    got, out = run_fmr(BAM_GPU, " nrgpu", "nrgpu_mode = fmr\n" + algcon, grid)
     assert "nrgpu: fmr mode" in out
     levels = []
     for d in ref:
