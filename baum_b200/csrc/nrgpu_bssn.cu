@@ -855,6 +855,16 @@ static CVarPtrs cptrs(const VarPtrs &v) {
 static int launch_rhs(nrgpu_level *L, const CVarPtrs &U, const VarPtrs &out, const CVarPtrs &pre, const VarPtrs &acc,
                       const Epilogue &E, const nrgpu_bssn_params &p, cudaStream_t st, bool interior, bool flagged,
                       int kb = 1, int ke = 1 << 30) {
+  // with both parts, the boundary kernel runs on the level's side stream,
+  // launched after the interior kernel so that its blocks fill the
+  // interior kernel's last wave; they write disjoint points
+  const bool fork = interior && flagged && L->nflagpts > 0;
+  if (fork) {
+    int e = nrgpu_level_side(L);
+    if (e) return e;
+    NRGPU_CUDA_TRY(cudaEventRecord(L->ev_fork, st));
+    NRGPU_CUDA_TRY(cudaStreamWaitEvent(L->side, L->ev_fork, 0));
+  }
   if (interior) {
     for (int b = 0; b < L->nboxes; ++b) {
       const BoxGeo &bx = L->hbox[b];
@@ -888,8 +898,13 @@ static int launch_rhs(nrgpu_level *L, const CVarPtrs &U, const VarPtrs &out, con
   }
   if (flagged && L->nflagpts > 0) {
     const int n = L->nflagpts * NRGPU_NV;
-    bssn_flagged_kernel<<<(n + 255) / 256, 256, 0, st>>>(U, out, pre, acc, E, p, L->d_flagpts, L->nflagpts,
-                                                          L->d_box, L->dx, L->dy, L->dz);
+    bssn_flagged_kernel<<<(n + 255) / 256, 256, 0, fork ? L->side : st>>>(U, out, pre, acc, E, p, L->d_flagpts,
+                                                                           L->nflagpts, L->d_box, L->dx, L->dy,
+                                                                           L->dz);
+  }
+  if (fork) {
+    NRGPU_CUDA_TRY(cudaEventRecord(L->ev_join, L->side));
+    NRGPU_CUDA_TRY(cudaStreamWaitEvent(st, L->ev_join, 0));
   }
   NRGPU_CUDA_TRY(cudaGetLastError());
   return NRGPU_OK;
@@ -1411,6 +1426,14 @@ static void z4_interior_fp64(const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVa
 static int z4_launch(nrgpu_level *L, const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVarPtrs &pre,
                      const ZVarPtrs &acc, const Epilogue &E, const nrgpu_z4_params &p, cudaStream_t st, bool interior,
                      bool flagged) {
+  // the boundary kernel beside the interior kernel, as in launch_rhs
+  const bool fork = interior && flagged && L->nflagpts > 0;
+  if (fork) {
+    int e = nrgpu_level_side(L);
+    if (e) return e;
+    NRGPU_CUDA_TRY(cudaEventRecord(L->ev_fork, st));
+    NRGPU_CUDA_TRY(cudaStreamWaitEvent(L->side, L->ev_fork, 0));
+  }
   if (interior) {
     for (int b = 0; b < L->nboxes; ++b) {
       const BoxGeo &bx = L->hbox[b];
@@ -1442,8 +1465,12 @@ static int z4_launch(nrgpu_level *L, const ZCVarPtrs &U, const ZVarPtrs &out, co
   }
   if (flagged && L->nflagpts > 0) {
     const int n = L->nflagpts * ZNV;
-    z4_flagged_kernel<<<(n + 255) / 256, 256, 0, st>>>(U, out, pre, acc, E, p, L->d_flagpts, L->nflagpts, L->d_box,
-                                                        L->dx, L->dy, L->dz);
+    z4_flagged_kernel<<<(n + 255) / 256, 256, 0, fork ? L->side : st>>>(U, out, pre, acc, E, p, L->d_flagpts,
+                                                                         L->nflagpts, L->d_box, L->dx, L->dy, L->dz);
+  }
+  if (fork) {
+    NRGPU_CUDA_TRY(cudaEventRecord(L->ev_join, L->side));
+    NRGPU_CUDA_TRY(cudaStreamWaitEvent(st, L->ev_join, 0));
   }
   NRGPU_CUDA_TRY(cudaGetLastError());
   return NRGPU_OK;

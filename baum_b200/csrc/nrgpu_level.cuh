@@ -45,6 +45,10 @@ struct nrgpu_level {
   int symmetry, nsym;
   SymPoint *d_sym;
   double *rsym;
+  // side stream of the boundary kernel, which runs beside the interior
+  // kernel of the same stage (first use)
+  cudaStream_t side;
+  cudaEvent_t ev_fork, ev_join;
   // copy and compute streams, and per-slab events, of the pipelined
   // host-buffer step (created on first use)
   cudaStream_t hs_copy, hs_comp;
@@ -62,3 +66,5 @@ int nrgpu_level_scratch(nrgpu_level *L, double **out);
 // set_boundary_symmetry on a list of nv variables of the given system
 // (NRGPU_SYSTEM_BSSN / _Z4C); nothing without symmetry (nrgpu_bssn.cu)
 int nrgpu_level_symmetry(nrgpu_level *L, double *const *u, int system, cudaStream_t st);
+// the side stream of the boundary kernel (nrgpu_lib.cu)
+int nrgpu_level_side(nrgpu_level *L);

@@ -168,6 +168,9 @@ extern "C" int nrgpu_level_destroy(nrgpu_level *L) {
     if (L->hev_in[q]) cudaEventDestroy(L->hev_in[q]);
     if (L->hev_out[q]) cudaEventDestroy(L->hev_out[q]);
   }
+  if (L->side) cudaStreamDestroy(L->side);
+  if (L->ev_fork) cudaEventDestroy(L->ev_fork);
+  if (L->ev_join) cudaEventDestroy(L->ev_join);
   if (L->hs_copy) cudaStreamDestroy(L->hs_copy);
   if (L->hs_comp) cudaStreamDestroy(L->hs_comp);
   free(L->hbox);
@@ -188,6 +191,14 @@ int nrgpu_level_scratch(nrgpu_level *L, double **out) {
     L->scratch_points = (size_t)L->npoints;
   }
   *out = L->scratch;
+  return NRGPU_OK;
+}
+
+int nrgpu_level_side(nrgpu_level *L) {
+  if (L->side) return NRGPU_OK;
+  NRGPU_CUDA_TRY(cudaStreamCreateWithFlags(&L->side, cudaStreamNonBlocking));
+  NRGPU_CUDA_TRY(cudaEventCreateWithFlags(&L->ev_fork, cudaEventDisableTiming));
+  NRGPU_CUDA_TRY(cudaEventCreateWithFlags(&L->ev_join, cudaEventDisableTiming));
   return NRGPU_OK;
 }
 
