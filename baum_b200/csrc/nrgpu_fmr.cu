@@ -83,18 +83,20 @@ __global__ void restrict_kernel(Ptrs uc, Ptrs uf, Box3 cb, Box3 fb, RGeom G, int
   uc.p[v][at3(cb, I, J, K)] = dot_rn<N>(G.w, sx);
 }
 
-// one thread per (fine point of the prolongation box, variable)
+// one thread per (fine point written by the prolongation, variable): the
+// points of the prolongation box that prolong_boxtobox_N writes (it skips
+// the pairs whose first point lies in the inner box), listed at set-up as
+// offsets in the prolongation box
 template <int N>
-__global__ void prolong_kernel(Ptrs uc, Ptrs uf, Box3 cb, Box3 fb, PGeom G, int npts) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= npts) return;
+__global__ void prolong_kernel(Ptrs uc, Ptrs uf, Box3 cb, Box3 fb, PGeom G, const int *__restrict__ list,
+                               int npts) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= npts) return;
+  const int q = list[n];
   const int v = blockIdx.y;
   const int nI = G.fb[1] - G.fb[0] + 1, nJ = G.fb[3] - G.fb[2] + 1;
   const int t[3] = {q % nI, (q / nI) % nJ, q / (nI * nJ)};
   const int i = G.fb[0] + t[0], j = G.fb[2] + t[1], k = G.fb[4] + t[2];
-  // the reference tests the inner box on the first point of each x pair
-  const int i0 = G.fb[0] + 2 * (t[0] / 2);
-  if (i0 >= G.f0[0] && i0 <= G.f0[1] && j >= G.f0[2] && j <= G.f0[3] && k >= G.f0[4] && k <= G.f0[5]) return;
   int s[3];
   const double *w[3];
 #pragma unroll
@@ -154,6 +156,7 @@ struct FmrPair {
   RGeom rg;
   PGeom pg;
   int nr, npro;
+  int *d_plist;  // the prolonged points (offsets in the prolongation box), npro of them
 };
 
 struct nrgpu_fmr {
@@ -320,6 +323,7 @@ int setup_one_pair(nrgpu_fmr *F, int l, int fbi, std::vector<double> &cr) {
       }
   P.has_p = n > 0;
   P.npro = 0;
+  P.d_plist = nullptr;
   if (n) {
     memcpy(Q.fb, fb, sizeof fb);
     memcpy(Q.f0, f0, sizeof f0);
@@ -339,7 +343,24 @@ int setup_one_pair(nrgpu_fmr *F, int l, int fbi, std::vector<double> &cr) {
     }
     lagrange(F->p.order_RP, F->p.order_RP / 2.0 - 0.25, Q.c1);
     lagrange(F->p.order_RP, F->p.order_RP / 2.0 - 0.75, Q.c2);
-    P.npro = (fb[1] - fb[0] + 1) * (fb[3] - fb[2] + 1) * (fb[5] - fb[4] + 1);
+    // the points written: every point of the box but the pairs whose first
+    // point lies in the inner box (prolong_boxtobox_N's test)
+    std::vector<int> list;
+    const int nI = fb[1] - fb[0] + 1, nJ = fb[3] - fb[2] + 1, nK = fb[5] - fb[4] + 1;
+    for (int tk = 0; tk < nK; ++tk)
+      for (int tj = 0; tj < nJ; ++tj)
+        for (int ti = 0; ti < nI; ++ti) {
+          const int i0 = fb[0] + 2 * (ti / 2), j = fb[2] + tj, k = fb[4] + tk;
+          if (i0 >= f0[0] && i0 <= f0[1] && j >= f0[2] && j <= f0[3] && k >= f0[4] && k <= f0[5]) continue;
+          list.push_back(ti + nI * (tj + nJ * tk));
+        }
+    P.npro = (int)list.size();
+    P.d_plist = nullptr;
+    if (P.npro) {
+      NRGPU_CUDA_TRY(cudaMalloc(&P.d_plist, sizeof(int) * list.size()));
+      NRGPU_CUDA_TRY(cudaMemcpy(P.d_plist, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice));
+    }
+    P.has_p = P.npro > 0;
   }
   F->pairs[l].push_back(P);
   return NRGPU_OK;
@@ -349,6 +370,7 @@ int setup_one_pair(nrgpu_fmr *F, int l, int fbi, std::vector<double> &cr) {
 int setup_pair(nrgpu_fmr *F, int l) {
   F->fp[l].assign(F->L[l]->npoints, 0.0);
   F->fr[l - 1].assign(F->L[l - 1]->npoints, 0.0);
+  for (FmrPair &P : F->pairs[l]) cudaFree(P.d_plist);
   F->pairs[l].clear();
   std::vector<double> cr(F->L[l - 1]->npoints, 0.0);
   for (int fb = 0; fb < (int)F->box[l].size(); ++fb) {
@@ -382,9 +404,9 @@ int restrict_prolong(nrgpu_fmr *F, int l, const Ptrs &uc, const Ptrs &uf, cudaSt
     if (!P.has_p) continue;
     const Box3 &cb = F->box[l - 1][P.cbox], &fb = F->box[l][P.fbox];
     const dim3 g((P.npro + 127) / 128, F->nv);
-    if (o == 2) prolong_kernel<2><<<g, 128, 0, st>>>(uc, uf, cb, fb, P.pg, P.npro);
-    else if (o == 4) prolong_kernel<4><<<g, 128, 0, st>>>(uc, uf, cb, fb, P.pg, P.npro);
-    else prolong_kernel<6><<<g, 128, 0, st>>>(uc, uf, cb, fb, P.pg, P.npro);
+    if (o == 2) prolong_kernel<2><<<g, 128, 0, st>>>(uc, uf, cb, fb, P.pg, P.d_plist, P.npro);
+    else if (o == 4) prolong_kernel<4><<<g, 128, 0, st>>>(uc, uf, cb, fb, P.pg, P.d_plist, P.npro);
+    else prolong_kernel<6><<<g, 128, 0, st>>>(uc, uf, cb, fb, P.pg, P.d_plist, P.npro);
     NRGPU_CUDA_TRY(cudaGetLastError());
   }
   return NRGPU_OK;
@@ -473,6 +495,7 @@ extern "C" int nrgpu_fmr_destroy(nrgpu_fmr *F) {
   if (F->ev_in) cudaEventDestroy(F->ev_in);
   if (F->ev_out) cudaEventDestroy(F->ev_out);
   for (int l = 0; l < F->nl; ++l) {
+    for (FmrPair &P : F->pairs[l]) cudaFree(P.d_plist);
     cudaFree(F->up[l]);
     cudaFree(F->upp[l]);
     nrgpu_level_destroy(F->L[l]);
