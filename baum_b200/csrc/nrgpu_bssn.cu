@@ -1150,9 +1150,8 @@ extern "C" int nrgpu_bssn_evolve_host(nrgpu_level *L, double *const *host_u, int
   if ((e = nrgpu_level_scratch(L, &scr))) return e;
   if ((e = host_streams(L))) return e;
   const cudaStream_t cs = L->hs_copy, ks = L->hs_comp;
-  double *u[NRGPU_NV];
   VarPtrs U;
-  for (int v = 0; v < NRGPU_NV; ++v) U.p[v] = u[v] = L->hoststate + v * np;
+  for (int v = 0; v < NRGPU_NV; ++v) U.p[v] = L->hoststate + v * np;
   const RkLists R = rk_lists(U, scr, np);
 
   // slabs of ps planes; H = the stencils' reach in planes
@@ -1604,9 +1603,9 @@ extern "C" int nrgpu_level_autotune(nrgpu_level *L, int system, const void *para
                                                                        system == NRGPU_SYSTEM_BSSN ? 17 : 18);
   NRGPU_CUDA_TRY(cudaGetLastError());
   const Epilogue E = {EPI_RHS, 0.0, 0.0, 0.0, 0};
-  cudaEvent_t a, b;
-  NRGPU_CUDA_TRY(cudaEventCreate(&a));
-  NRGPU_CUDA_TRY(cudaEventCreate(&b));
+  cudaEvent_t ev0, ev1;
+  NRGPU_CUDA_TRY(cudaEventCreate(&ev0));
+  NRGPU_CUDA_TRY(cudaEventCreate(&ev1));
   // 128- and 256-thread shapes, flat (x, y) and with a z extent.  The
   // kernels wait on L1/L2: the larger and the more cubic the block, the
   // smaller its stencil halo per point, so more taps hit in L1 (a 256-thread
@@ -1622,7 +1621,7 @@ extern "C" int nrgpu_level_autotune(nrgpu_level *L, int system, const void *para
   for (int c = 0; c < ncand && !e; ++c) {
     for (int a = 0; a < 3; ++a) L->blk[a] = cand[c][a];
     for (int rep = 0; rep < 4 && !e; ++rep) {
-      if (rep == 1) cudaEventRecord(a, st);
+      if (rep == 1) cudaEventRecord(ev0, st);
       if (system == NRGPU_SYSTEM_BSSN) {
         VarPtrs P, O;
         for (int v = 0; v < NRGPU_NV; ++v) {
@@ -1639,17 +1638,17 @@ extern "C" int nrgpu_level_autotune(nrgpu_level *L, int system, const void *para
         e = z4_launch(L, z4_c(P), O, z4_c(P), O, E, *(const nrgpu_z4_params *)params, st, true, false);
       }
     }
-    cudaEventRecord(b, st);
-    cudaEventSynchronize(b);
+    cudaEventRecord(ev1, st);
+    cudaEventSynchronize(ev1);
     float ms = 0;
-    cudaEventElapsedTime(&ms, a, b);
+    cudaEventElapsedTime(&ms, ev0, ev1);
     if (ms < best) {
       best = ms;
       bb = c;
     }
   }
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
   for (int q = 0; q < 3; ++q) {
     L->blk[q] = cand[bb][q];
     if (best_block) best_block[q] = cand[bb][q];
