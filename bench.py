@@ -251,19 +251,31 @@ FMR_SIZES = [162, 136, 168, 104, 136, 72, 104]
 FMR_DX0 = 0.5
 
 
-def gpu_fmr(steps=2, variants=(("graph", 1, 1), ("launches", 0, 1), ("graph_untuned_32x4", 1, 0)), warm=2):
+# the full form's grid without its moving boxes: 9 nested 2:1 levels, a
+# 192^3-inner coarsest box and 128^3 interiors (plus 4 points per side) on
+# the 8 finer levels, Z4c 6th order + KO6 (as the precision-sweep box)
+C5_SIZES = [194] + [136] * 8
+C5_DX0 = 0.5
+
+
+def gpu_fmr(steps=2, variants=(("graph", 1, 1), ("launches", 0, 1), ("graph_untuned_32x4", 1, 0)), warm=2,
+            sizes=None, dx0=None, order=4):
     import torch
     from baum_b200 import abi, fmr, synthetic
-    levels = fmr.nested_levels(FMR_SIZES, FMR_DX0)
-    params = [abi.z4_params_from_par(dissfactor=(0.1 if l == 0 else 0.02) / 64) for l in range(len(levels))]
-    dt = [0.25 * FMR_DX0 / 2 ** l for l in range(len(levels))]
+    sizes = sizes or FMR_SIZES
+    dx0 = dx0 or FMR_DX0
+    levels = fmr.nested_levels(sizes, dx0)
+    params = [abi.z4_params_from_par(dissfactor=(0.1 if l == 0 else 0.02) / 64, order_centered=order,
+                                     order_advection=order) for l in range(len(levels))]
+    dt = [0.25 * dx0 / 2 ** l for l in range(len(levels))]
     def state(lev):
         x, y, z = (torch.from_numpy(c).cuda() for c in lev.coords())
         return synthetic.fourier_state_device(x, y, z, abi.Z4_NVARS, synthetic.Z4_UNIT, 8, 1e-3, 16.0, 1)
     inner = [int((lev.boundary == 0).sum()) for lev in levels]
     upd_per_coarse = sum(n * 4 * 2 ** l for l, n in enumerate(inner))
-    out = {"workload": "7 nested 2:1 levels, Z4c 4th order + KO6, Berger-Oliger, order_RP 4, nbuffer 3, "
-                       "box points per side %s, dx0 %.3g, Fourier data 1e-3" % (FMR_SIZES, FMR_DX0),
+    out = {"workload": "%d nested 2:1 levels, Z4c %s order + KO%d, Berger-Oliger, order_RP 4, nbuffer 3, "
+                       "box points per side %s, dx0 %.3g, Fourier data 1e-3"
+                       % (len(sizes), "4th" if order == 4 else "6th", 6, sizes, dx0),
            "rhs_point_updates_per_coarse_step": upd_per_coarse}
     # the product configuration (graph + per-level tuned block shapes), then
     # plain launches, then the graph with every level at the 32 x 4 default
@@ -608,7 +620,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--case", default="c1", choices=["c1", "c1-step", "mg", "fmr", "z4c160"],
+    ap.add_argument("--case", default="c1", choices=["c1", "c1-step", "mg", "fmr", "c5", "z4c160"],
                     help="c1: the benchmark line; c1-step: only the 64^3 BSSN RK4 steps and the rhs "
                          "launches of that line (for profiling); mg: only the 130^3 multigrid solve of the "
                          "first seeded binary (for profiling); fmr: only the 7-level Z4c step, graph replay with tuned "
@@ -627,6 +639,16 @@ def main():
         torch.cuda.set_device(0)
         print(json.dumps({"case": "fmr", **gpu_fmr(args.steps, variants=(("graph", 1, 1),),
                                                      warm=max(args.warmup, 2))}))
+        return
+    if args.case == "c5":
+        import torch
+        from baum_b200 import build
+        build.build()
+        torch.cuda.set_device(0)
+        r = gpu_fmr(args.steps, variants=(("graph", 1, 1),), warm=max(args.warmup, 2), sizes=C5_SIZES,
+                    dx0=C5_DX0, order=6)
+        r["note"] = "static boxes: the full form's moving boxes and warm-started initial data are not built"
+        print(json.dumps({"case": "c5", **r}))
         return
     if args.case == "mg":
         import torch
