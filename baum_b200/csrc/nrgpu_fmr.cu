@@ -173,6 +173,12 @@ struct nrgpu_fmr {
   std::vector<FmrPair> pairs[kMaxLevels];              // per fine level, one per fine box
   double *up[kMaxLevels], *upp[kMaxLevels];  // u(n-1) copy and time interpolant
   int iteration[kMaxLevels];
+  // puncture tracking on the finest level (lmaxpunc = amr_lmax, grid.c:
+  // 287-294): positions [3n] then the shift at the old positions [3n], and
+  // the status of the last step per puncture
+  int ntrack, track_fixz;
+  double *d_track;
+  int *d_tstatus;
   // graph of one coarse step for one set of state pointers
   cudaGraph_t graph;
   cudaGraphExec_t exec;
@@ -421,6 +427,10 @@ Ptrs upp_ptrs(nrgpu_fmr *F, int l) {
 
 // one step of level l: evolve() with the time interpolation of a level with
 // a child around the RK4 stages, then the algebraic constraints
+// first shift component in the evolved list: betax is variable 18 of BSSN
+// (bssn.c:315-322) and 19 of Z4c (z4.c:234-242)
+int shift_index(const nrgpu_fmr *F) { return F->p.system == NRGPU_SYSTEM_BSSN ? 18 : 19; }
+
 int step_level(nrgpu_fmr *F, int l, double *const *u, cudaStream_t st) {
   const bool child = l < F->nl - 1;
   const long np = F->L[l]->npoints;
@@ -435,6 +445,12 @@ int step_level(nrgpu_fmr *F, int l, double *const *u, cudaStream_t st) {
     ti_start_kernel<<<nb, 256, 0, st>>>(U, F->up[l], F->upp[l], ca, cb, np, F->nv);
     NRGPU_CUDA_TRY(cudaGetLastError());
   }
+  // the tracker reads the shift one step earlier at the old positions
+  // (betax_p in moving_punctures_integrate.c:62-64): taken before the step
+  if (l == F->nl - 1 && F->ntrack &&
+      (e = nrgpu_track_before_step(F->L[l], u + shift_index(F), F->p.order_RP, F->ntrack, F->d_track,
+                                   F->d_track + 3 * F->ntrack, st)))
+    return e;
   if (F->p.system == NRGPU_SYSTEM_BSSN) e = nrgpu_bssn_rk4_stages(F->L[l], u, F->dt[l], &F->bp[l], st);
   else e = nrgpu_z4_rk4_stages(F->L[l], u, F->dt[l], &F->zp[l], st);
   if (e) return e;
@@ -470,6 +486,11 @@ int advance(nrgpu_fmr *F, int l, double *const *u, cudaStream_t st) {
     }
     if ((e = restrict_prolong(F, l, uc, uf, st))) return e;
   }
+  // ANALYZE of the level (main.c:420-423): track_puncture on the finest level
+  if (l == F->nl - 1 && F->ntrack &&
+      (e = nrgpu_track_after_step(F->L[l], u + l * F->nv + shift_index(F), F->dt[l], F->p.order_RP, F->track_fixz,
+                                  F->ntrack, F->d_track, F->d_track + 3 * F->ntrack, F->d_tstatus, st)))
+    return e;
   return NRGPU_OK;
 }
 
@@ -500,6 +521,8 @@ extern "C" int nrgpu_fmr_destroy(nrgpu_fmr *F) {
     cudaFree(F->upp[l]);
     nrgpu_level_destroy(F->L[l]);
   }
+  cudaFree(F->d_track);
+  cudaFree(F->d_tstatus);
   delete F;
   return NRGPU_OK;
 }
@@ -524,6 +547,9 @@ extern "C" int nrgpu_fmr_create(int nl, const nrgpu_level_desc *levels, const do
   F->exec = nullptr;
   F->gst = nullptr;
   F->ev_in = F->ev_out = nullptr;
+  F->ntrack = F->track_fixz = 0;
+  F->d_track = nullptr;
+  F->d_tstatus = nullptr;
   F->nl = nl;
   F->p = *p;
   F->nv = p->system == NRGPU_SYSTEM_BSSN ? NRGPU_NV : NRGPU_Z4_NVARS;
@@ -670,9 +696,11 @@ extern "C" int nrgpu_fmr_advance(nrgpu_fmr *F, double *const *u, int nsteps, voi
 // levels' point counts), the counters, then per parent level u(n-1) and upp.
 namespace {
 constexpr uint32_t kCkptMagic = 0x4652474e;  // "NGRF"
+constexpr uint32_t kCkptVersion = 2;          // 2: the tracked positions at the end
 size_t ckpt_bytes(const nrgpu_fmr *F) {
   size_t b = sizeof(uint32_t) * 4 + sizeof(long) * F->nl + sizeof(int) * F->nl;
   for (int l = 0; l < F->nl - 1; ++l) b += 2 * sizeof(double) * F->nv * (size_t)F->L[l]->npoints;
+  b += sizeof(int) + sizeof(double) * 3 * F->ntrack;
   return b;
 }
 }  // namespace
@@ -687,7 +715,7 @@ extern "C" int nrgpu_fmr_save(nrgpu_fmr *F, void *host, size_t bytes) {
   if (!F || !host || bytes < ckpt_bytes(F)) return nrgpu_set_error(NRGPU_ERR_ARG, "buffer of %zu bytes", bytes);
   NRGPU_CUDA_TRY(cudaDeviceSynchronize());
   char *c = (char *)host;
-  const uint32_t h[4] = {kCkptMagic, 1u, (uint32_t)F->nl, (uint32_t)F->nv};
+  const uint32_t h[4] = {kCkptMagic, kCkptVersion, (uint32_t)F->nl, (uint32_t)F->nv};
   memcpy(c, h, sizeof h);
   c += sizeof h;
   for (int l = 0; l < F->nl; ++l, c += sizeof(long)) {
@@ -703,6 +731,9 @@ extern "C" int nrgpu_fmr_save(nrgpu_fmr *F, void *host, size_t bytes) {
     NRGPU_CUDA_TRY(cudaMemcpy(c, F->upp[l], b, cudaMemcpyDeviceToHost));
     c += b;
   }
+  memcpy(c, &F->ntrack, sizeof(int));
+  c += sizeof(int);
+  if (F->ntrack) NRGPU_CUDA_TRY(cudaMemcpy(c, F->d_track, sizeof(double) * 3 * F->ntrack, cudaMemcpyDeviceToHost));
   return NRGPU_OK;
 }
 
@@ -712,7 +743,7 @@ extern "C" int nrgpu_fmr_load(nrgpu_fmr *F, const void *host, size_t bytes) {
   uint32_t h[4];
   memcpy(h, c, sizeof h);
   c += sizeof h;
-  if (h[0] != kCkptMagic || h[1] != 1u || h[2] != (uint32_t)F->nl || h[3] != (uint32_t)F->nv)
+  if (h[0] != kCkptMagic || h[1] != kCkptVersion || h[2] != (uint32_t)F->nl || h[3] != (uint32_t)F->nv)
     return nrgpu_set_error(NRGPU_ERR_ARG, "checkpoint of another hierarchy (levels %u, variables %u)", h[2], h[3]);
   for (int l = 0; l < F->nl; ++l, c += sizeof(long)) {
     long np;
@@ -722,6 +753,14 @@ extern "C" int nrgpu_fmr_load(nrgpu_fmr *F, const void *host, size_t bytes) {
   int it[kMaxLevels];
   memcpy(it, c, sizeof(int) * F->nl);
   c += sizeof(int) * F->nl;
+  {
+    size_t off = 0;
+    for (int l = 0; l < F->nl - 1; ++l) off += 2 * sizeof(double) * F->nv * (size_t)F->L[l]->npoints;
+    int nt;
+    memcpy(&nt, c + off, sizeof nt);
+    if (nt != F->ntrack)
+      return nrgpu_set_error(NRGPU_ERR_ARG, "checkpoint tracks %d punctures, the hierarchy %d", nt, F->ntrack);
+  }
   NRGPU_CUDA_TRY(cudaDeviceSynchronize());
   for (int l = 0; l < F->nl - 1; ++l) {
     const size_t b = sizeof(double) * F->nv * (size_t)F->L[l]->npoints;
@@ -730,6 +769,48 @@ extern "C" int nrgpu_fmr_load(nrgpu_fmr *F, const void *host, size_t bytes) {
     NRGPU_CUDA_TRY(cudaMemcpy(F->upp[l], c, b, cudaMemcpyHostToDevice));
     c += b;
   }
+  c += sizeof(int);
+  if (F->ntrack) NRGPU_CUDA_TRY(cudaMemcpy(F->d_track, c, sizeof(double) * 3 * F->ntrack, cudaMemcpyHostToDevice));
   memcpy(F->iteration, it, sizeof(int) * F->nl);
+  return NRGPU_OK;
+}
+
+// ---- puncture tracking ----------------------------------------------------------
+extern "C" int nrgpu_fmr_track(nrgpu_fmr *F, int n, const double *pos, int fixz) {
+  if (!F || n < 0 || n > NRGPU_MAX_PUNCTURES || (n && !pos))
+    return nrgpu_set_error(NRGPU_ERR_ARG, "bad arguments (0 <= n <= %d)", NRGPU_MAX_PUNCTURES);
+  NRGPU_CUDA_TRY(cudaDeviceSynchronize());
+  cudaFree(F->d_track);
+  cudaFree(F->d_tstatus);
+  F->d_track = nullptr;
+  F->d_tstatus = nullptr;
+  F->ntrack = 0;
+  // the captured coarse step changes: capture it again at the next advance
+  if (F->exec) cudaGraphExecDestroy(F->exec);
+  if (F->graph) cudaGraphDestroy(F->graph);
+  F->exec = nullptr;
+  F->graph = nullptr;
+  F->graph_u.clear();
+  if (!n) return NRGPU_OK;
+  if (cudaMalloc(&F->d_track, sizeof(double) * 6 * n) != cudaSuccess ||
+      cudaMalloc(&F->d_tstatus, sizeof(int) * n) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(F->d_track);
+    F->d_track = nullptr;
+    return nrgpu_set_error(NRGPU_ERR_NOMEM, "tracking buffers");
+  }
+  NRGPU_CUDA_TRY(cudaMemcpy(F->d_track, pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice));
+  NRGPU_CUDA_TRY(cudaMemset(F->d_tstatus, 0, sizeof(int) * n));
+  F->ntrack = n;
+  F->track_fixz = fixz ? 1 : 0;
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_fmr_punctures(nrgpu_fmr *F, double *pos, int *status) {
+  if (!F || !pos) return nrgpu_set_error(NRGPU_ERR_ARG, "null argument");
+  if (!F->ntrack) return nrgpu_set_error(NRGPU_ERR_ARG, "no punctures tracked");
+  NRGPU_CUDA_TRY(cudaDeviceSynchronize());
+  NRGPU_CUDA_TRY(cudaMemcpy(pos, F->d_track, sizeof(double) * 3 * F->ntrack, cudaMemcpyDeviceToHost));
+  if (status) NRGPU_CUDA_TRY(cudaMemcpy(status, F->d_tstatus, sizeof(int) * F->ntrack, cudaMemcpyDeviceToHost));
   return NRGPU_OK;
 }

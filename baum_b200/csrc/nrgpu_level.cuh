@@ -68,3 +68,10 @@ int nrgpu_level_scratch(nrgpu_level *L, double **out);
 int nrgpu_level_symmetry(nrgpu_level *L, double *const *u, int system, cudaStream_t st);
 // the side stream of the boundary kernel (nrgpu_lib.cu)
 int nrgpu_level_side(nrgpu_level *L);
+// the two halves of a tracking step for a driver that keeps no copy of the
+// previous shift: before the step the shift at the old positions into b1,
+// after it the corrector passes from b1 (nrgpu_track.cu)
+int nrgpu_track_before_step(nrgpu_level *L, const double *const *beta, int order, int n, const double *pos,
+                            double *b1, cudaStream_t st);
+int nrgpu_track_after_step(nrgpu_level *L, const double *const *beta, double dt, int order, int fixz, int n,
+                           double *pos, const double *b1, int *status, cudaStream_t st);

@@ -84,6 +84,26 @@ class Hierarchy:
         buf = np.ascontiguousarray(buf, dtype=np.uint8)
         abi.check(abi.lib().nrgpu_fmr_load(self.handle, buf.ctypes.data, buf.size))
 
+    def track(self, positions, fixz=False):
+        """Track punctures from these start positions (n x 3) on the finest
+        level during the following steps (nrgpu_fmr_track; track_puncture
+        with the shift integrator); an empty list stops tracking."""
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+        abi.check(abi.lib().nrgpu_fmr_track(self.handle, pos.shape[0],
+                                            pos.ctypes.data_as(C.POINTER(C.c_double)), int(bool(fixz))))
+        self.ntrack = pos.shape[0]
+
+    def punctures(self):
+        """(positions n x 3, status per puncture) of the tracked punctures
+        (nrgpu_fmr_punctures): bit 0 the last step integrated, bit 1 the new
+        position lay on the level and was taken."""
+        n = getattr(self, "ntrack", 0)
+        pos = np.empty((n, 3))
+        st = np.empty(n, dtype=np.int32)
+        abi.check(abi.lib().nrgpu_fmr_punctures(self.handle, pos.ctypes.data_as(C.POINTER(C.c_double)),
+                                                st.ctypes.data_as(C.POINTER(C.c_int))))
+        return pos, st
+
     def close(self):
         if self.handle:
             abi.lib().nrgpu_fmr_destroy(self.handle)

@@ -328,14 +328,31 @@ int nrgpu_fmr_block(nrgpu_fmr *fmr, int l, int *block);
  * checkpoint, main/main/checkpoint.c:14-165, writes the level variables,
  * which stay with the caller here): the level iteration counters and, for
  * every level with a child, the previous step's copy and the time
- * interpolant.  nrgpu_fmr_state_size gives the bytes; nrgpu_fmr_save writes
- * them to a host buffer and nrgpu_fmr_load restores them into a hierarchy
- * created with the same levels and parameters (refused otherwise).  Both
+ * interpolant, and the tracked puncture positions.  nrgpu_fmr_state_size
+ * gives the bytes; nrgpu_fmr_save writes them to a host buffer and
+ * nrgpu_fmr_load restores them into a hierarchy created with the same
+ * levels and parameters and tracking as many punctures (refused otherwise).  Both
  * wait for the device.  With the caller's level states this resumes a run
  * bit for bit. */
 int nrgpu_fmr_state_size(nrgpu_fmr *fmr, size_t *bytes);
 int nrgpu_fmr_save(nrgpu_fmr *fmr, void *host, size_t bytes);
 int nrgpu_fmr_load(nrgpu_fmr *fmr, const void *host, size_t bytes);
+
+/* Puncture tracking inside the hierarchy's steps: track_puncture
+ * (projects/Gauge/moving_punctures.c:135-200) with the shift integrator
+ * (nrgpu_track_punctures) on the finest level, the reference's default
+ * lmaxpunc = amr_lmax (main/amr/grid.c:287-294), after each of its steps
+ * and its restriction/prolongation, where the reference's ANALYZE runs
+ * (main/main/main.c:397-423); interpolation order = order_RP.  The shift
+ * one step earlier is interpolated before the step, so no copy of it is
+ * kept.  nrgpu_fmr_track sets n <= NRGPU_MAX_PUNCTURES start positions
+ * (host [3n], the moving_punctureN_x/y/z of init_moving_puncture) and
+ * fixz; n = 0 stops tracking.  nrgpu_fmr_punctures waits for the device
+ * and returns the positions (host [3n]) and, if status is not NULL, the
+ * last step's status per puncture (nrgpu_track_punctures). */
+#define NRGPU_MAX_PUNCTURES 16
+int nrgpu_fmr_track(nrgpu_fmr *fmr, int n, const double *pos, int fixz);
+int nrgpu_fmr_punctures(nrgpu_fmr *fmr, double *pos, int *status);
 
 /* the evolution systems */
 enum { NRGPU_SYSTEM_BSSN = 0, NRGPU_SYSTEM_Z4C = 1 };
@@ -384,6 +401,25 @@ int nrgpu_adm_constraints(nrgpu_level *L, const double *const *adm, double *cons
  * results are in norm2[nvars], norminf[nvars] on return. */
 int nrgpu_norms(nrgpu_level *L, const double *const *vars, int nvars, double *norm2, double *norminf,
                 void *stream);
+
+/* ---- puncture tracking ----------------------------------------------------
+ * The shift-integration tracker, track_moving_puncture_integrate
+ * (projects/Gauge/moving_punctures_integrate.c:29-100) with the position
+ * test of track_puncture (projects/Gauge/moving_punctures.c:189-191), for n
+ * punctures on level L: x_new solves x' = -beta(x) by three corrector
+ * passes x0 = x1 - dt/2 (beta(x0) + beta_p(x1)); the shift is interpolated
+ * with Lagrange cubes of order^3 points (interpolate_xyz_scalar,
+ * utility/interpolate/interpolate.c:419-470; 2 <= order <= 8, the
+ * reference's order_RP), 0 where the cube does not fit in the box of its
+ * corner node.  A position below a symmetry plane of the level stays
+ * (grid->half); fixz keeps z (moving_puncture_fixz = BH or BHNS); a new
+ * position off the level is not taken.  beta, beta_p: 3 device pointers
+ * each (the level's shift now and one step earlier); pos: device [3n],
+ * updated in place; status: device [n] or NULL, per puncture bit 0 = the
+ * integration ran, bit 1 = the new position is on the level (taken).
+ * Positions equal the reference's bit for bit. */
+int nrgpu_track_punctures(nrgpu_level *L, const double *const *beta, const double *const *beta_p, double dt,
+                          int order, int fixz, int n, double *pos, int *status, void *stream);
 
 /* ---- learned warm start of the puncture solve ----------------------------
  * No counterpart in the reference.  A coordinate MLP (NRGPU_MLP_IN features

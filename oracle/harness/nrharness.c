@@ -15,6 +15,12 @@
  *   3. nrharness_dump = "i0 i1 ...": dump the evolved variables of every
  *      level after those level iterations (POST_EVOLVE), and after the
  *      initial data when 0 is listed.
+ *   4. nrharness_track = yes: with each of those dumps, run the reference's
+ *      shift-integration puncture tracker (track_moving_puncture_integrate,
+ *      Gauge/moving_punctures_integrate.c:29-100) from every start position
+ *      of nrharness_track_points on that level, with the z coordinate free
+ *      and pinned (moving_puncture_fixz), and write the results as text
+ *      (track_itN_lL.txt) beside a dump of the current and previous shift.
  * Dump format (little endian), one file per (tag, level):
  *   int64 magic 0x3147524e ("NRG1"), l, nboxes, nvars, npoints, iteration
  *   double time, dx, dy, dz, dt
@@ -191,6 +197,8 @@ int nrharness_post_initialdata(tL *level)
   return 0;
 }
 
+static void dump_track(tL *level, const char *tag);
+
 int nrharness_post_evolve(tL *level)
 {
   tVarList *u = 0;
@@ -207,8 +215,57 @@ int nrharness_post_evolve(tL *level)
       snprintf(tag, sizeof tag, "con_it%d", level->iteration + 1);
       dump_constraints(level, tag);
     }
+    if (Getv("nrharness_track", "yes")) {
+      snprintf(tag, sizeof tag, "track_it%d", level->iteration + 1);
+      dump_track(level, tag);
+    }
   }
   return 0;
+}
+
+/* the reference's tracker and the globals of moving_punctures.c:13-14 */
+int track_moving_puncture_integrate(tL *level, int np, double *pold, double *pnew);
+int xyzinsidelevel(tL *level, double x, double y, double z);
+extern int pintoxyplane;
+
+static void dump_track(tL *level, const char *tag)
+{
+  tVarList *vl = vlalloc(level);
+  char fn[1024];
+  const char *s = Gets("nrharness_track_points");
+  char *end;
+  double p[3], pnew[3];
+  int i, fix, moved, save;
+  FILE *f;
+  /* a vector is pushed by its first component: betax..z, betax_p..z_p */
+  vlpush(vl, Ind("betax"));
+  vlpush(vl, Ind("betax_p"));
+  dump_varlist(level, vl, tag);
+  vlfree(vl);
+  snprintf(fn, sizeof fn, "%s/%s_l%d.txt", Gets("nrharness_dir"), tag, level->l);
+  f = fopen(fn, "w");
+  if (!f) errorexits("nrharness: cannot open %s", fn);
+  /* the tracker runs on the level lmaxpunc names (grid.c:287-294) */
+  save = level->grid->lmaxpunc[0];
+  level->grid->lmaxpunc[0] = level->l;
+  for (;;) {
+    for (i = 0; i < 3; i++) {
+      p[i] = strtod(s, &end);
+      if (end == s) break;
+      s = end;
+    }
+    if (i < 3) break;
+    for (fix = 0; fix <= 2; fix += 2) {
+      pintoxyplane = fix;
+      moved = track_moving_puncture_integrate(level, 0, p, pnew);
+      fprintf(f, "%d %d %.17g %.17g %.17g %.17g %.17g %.17g %d\n", fix, moved, p[0], p[1], p[2],
+              pnew[0], pnew[1], pnew[2], xyzinsidelevel(level, pnew[0], pnew[1], pnew[2]));
+    }
+  }
+  pintoxyplane = 0;
+  level->grid->lmaxpunc[0] = save;
+  fclose(f);
+  printf("nrharness: wrote %s\n", fn);
 }
 
 void bam_nrharness(void)
@@ -221,6 +278,8 @@ void bam_nrharness(void)
   AddPar("nrharness_mg", "no", "dump punctures_u after the initial data solve [no,yes]");
   AddPar("nrharness_flags", "no", "dump the refinement flags of every level after the initial data [no,yes]");
   AddPar("nrharness_constraints", "no", "with each state dump also dump ADM variables and constraints [no,yes]");
+  AddPar("nrharness_track", "no", "with each state dump run the shift-integration tracker [no,yes]");
+  AddPar("nrharness_track_points", "", "start positions of the tracker, x y z per position");
   AddPar("nrharness_data", "none", "synthetic data over the evolved variables [none,fourier]");
   AddPar("nrharness_amp", "1e-3", "amplitude of the Fourier perturbation");
   AddPar("nrharness_nmodes", "8", "number of Fourier modes");

@@ -17,15 +17,16 @@ SRC = os.path.join(HERE, "nr_oracle.c")
 MGSRC = os.path.join(HERE, "mg_oracle.c")
 ADMSRC = os.path.join(HERE, "adm_oracle.c")
 FMRSRC = os.path.join(HERE, "fmr_oracle.c")
+TRACKSRC = os.path.join(HERE, "track_oracle.c")
 
 
 def build(force=False):
     """Compile the restatement with gcc (-O2, OpenMP, no fast-math)."""
-    deps = [SRC, MGSRC, ADMSRC, FMRSRC, os.path.join(HERE, "..", "include", "nrgpu.h")]
+    deps = [SRC, MGSRC, ADMSRC, FMRSRC, TRACKSRC, os.path.join(HERE, "..", "include", "nrgpu.h")]
     if not force and os.path.exists(SO) and all(os.path.getmtime(SO) >= os.path.getmtime(d) for d in deps):
         return SO
     cmd = ["gcc", "-O2", "-std=gnu99", "-fopenmp", "-fPIC", "-shared", "-ffp-contract=off",
-           SRC, MGSRC, ADMSRC, FMRSRC, "-o", SO, "-lm"]
+           SRC, MGSRC, ADMSRC, FMRSRC, TRACKSRC, "-o", SO, "-lm"]
     subprocess.run(cmd, check=True)
     return SO
 
@@ -55,6 +56,9 @@ def lib():
             "oracle_fmr_restrict_prolong": [LD, LD, C.c_int, pp, pp, C.c_int, C.c_int],
             "oracle_adm_constraints": [LD, pp, pp, C.c_int, C.c_int],
             "oracle_norms": [LD, pp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)],
+            "oracle_track_punctures": [LD, pp, pp, C.c_double, C.c_int, C.c_int, C.c_int,
+                                       C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int),
+                                       C.POINTER(C.c_int)],
         }.items():
             f = getattr(L, name)
             f.restype = C.c_int
@@ -234,3 +238,23 @@ class FmrState:
         for _ in range(nsteps):
             self._advance(0, snap)
         return self.u
+
+
+def track_punctures(level, beta, beta_p, dt, pos, order=4, fixz=0):
+    """track_moving_puncture_integrate for each row of pos (n x 3): the new
+    positions, the integrator's return values and the position test."""
+    beta = np.ascontiguousarray(beta, dtype=np.float64)
+    beta_p = np.ascontiguousarray(beta_p, dtype=np.float64)
+    pold = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+    n = pold.shape[0]
+    pnew = np.zeros_like(pold)
+    moved = np.zeros(n, dtype=np.int32)
+    inside = np.zeros(n, dtype=np.int32)
+    dp = C.POINTER(C.c_double)
+    ip = C.POINTER(C.c_int)
+    e = lib().oracle_track_punctures(C.byref(level.desc), _ptrs(beta), _ptrs(beta_p), dt, order, int(fixz), n,
+                                     pold.ctypes.data_as(dp), pnew.ctypes.data_as(dp), moved.ctypes.data_as(ip),
+                                     inside.ctypes.data_as(ip))
+    if e:
+        raise RuntimeError("oracle_track_punctures: %d" % e)
+    return pnew, moved, inside

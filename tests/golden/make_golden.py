@@ -327,6 +327,78 @@ FMR_VARS = [0, 6, 8, 13, 14, 17, 18, 19]
 FMR_KEEP_BY_CASE = {"z4_fmr3": (FMR_KEEP, FMR_VARS),
                     "z4_fmr3_binary": ({"state_it2_l0", "state_it4_l1", "state_it8_l2"}, [6, 18])}
 
+# the shift-integration puncture tracker (track_moving_puncture_integrate,
+# Gauge/moving_punctures_integrate.c:29-100) run by the reference from a list
+# of start positions after a state dump: a single box at order_RP 2, 4 and 6
+# (positions inside, on nodes, within dequaleps of a node, and with
+# interpolation cubes that leave the box), the octant (positions below the
+# symmetry planes stay), and the binary's two-box finest level (positions in
+# either box, between them, and with cubes that cross a box face)
+TRACK_BOX_POINTS = ("0.1 -0.3 0.7  0.5 0.5 -0.5  1.23456789 -1.87654321 0.333333333  -2.2 0.0 0.4  "
+                    "2.2 1.0 -1.0  1.74999999999 0.25 -0.75  -0.75 -0.75 -0.75  0.0 0.0 0.0  "
+                    "-1.1 0.9 1.3")
+TRACK_CASES = {
+    "track_box": CASES["bssn_fourier_o4"].replace("nrharness_rhs = yes\n", "").replace(
+        "nrharness_dump = 0 2", "nrharness_dump = 2\nnrharness_track = yes\nnrharness_track_points = "
+        + TRACK_BOX_POINTS),
+    "track_octant": CASES["bssn_punc_octant"].replace("nrharness_rhs = yes\n", "").replace(
+        "nrharness_dump = 0 4", "nrharness_dump = 4\nnrharness_track = yes\nnrharness_track_points = "
+        "0.3 0.4 0.2  -0.1 0.5 0.5  0.5 -0.2 0.6  0.6 0.7 -0.05  1.0 1.0 1.0  0.126 0.126 0.126  2.9 0.2 0.3"),
+    "track_fmr_binary": FMR_CASES["z4_fmr3_binary"].replace("nrharness_flags = yes\n", "").replace(
+        "nrharness_dump = 0 2 4 8", "nrharness_dump = 8\nnrharness_track = yes\nnrharness_track_points = "
+        "2.75 0.1 -0.2  -2.6 0.3 0.1  0.0 0.0 0.0  0.4 0.0 0.0  0.6 0.2 0.1  5.0 0.0 0.0  5.1 0.0 0.0  "
+        "-0.35 0.0 0.0  -2.9 -2.0 1.9  3.3 2.2 -2.2"),
+}
+for _o in (2, 6):
+    TRACK_CASES["track_box_rp%d" % _o] = TRACK_CASES["track_box"] + "order_RP = %d\n" % _o
+# the fields of a tracking fixture are kept within TRACK_HALO points of a
+# start position (the rest is zero): the tracker reads only the cubes
+# around the start positions, which the CPU pins check
+TRACK_HALO = 5
+
+
+def run_track_case(name, par):
+    work = tempfile.mkdtemp(prefix="golden_")
+    try:
+        with open(os.path.join(work, name + ".par"), "w") as f:
+            f.write(par)
+        r = subprocess.run([BAM, "-nt", "4", name + ".par"], cwd=work, capture_output=True, text=True)
+        if r.returncode:
+            raise RuntimeError(r.stdout[-3000:] + r.stderr[-3000:])
+        arrays = {}
+        for fn in sorted(os.listdir(work)):
+            if not (fn.startswith("track_") and fn.endswith(".txt")):
+                continue
+            tag = fn[:-4]
+            res = np.loadtxt(os.path.join(work, fn), ndmin=2)
+            d = dumpfile.read(os.path.join(work, tag + ".bin"))
+            keep = np.zeros(len(d["boundary"]), dtype=bool)
+            for bx in d["boxes"]:
+                m, n, o, off = (int(v) for v in bx[:4])
+                x0 = np.array(bx[4:7])
+                for p in res[::2, 2:5]:
+                    c = np.floor((p - x0) / np.array([d["dx"], d["dy"], d["dz"]]) + 0.5).astype(int)
+                    lo = np.maximum(c - TRACK_HALO, 0)
+                    hi = np.minimum(c + TRACK_HALO + 1, [m, n, o])
+                    if np.any(lo >= hi):
+                        continue
+                    k, j, i = np.meshgrid(np.arange(lo[2], hi[2]), np.arange(lo[1], hi[1]),
+                                          np.arange(lo[0], hi[0]), indexing="ij")
+                    keep[off + i + m * j + m * n * k] = True
+            idx = np.nonzero(keep)[0].astype(np.int32)
+            arrays[tag + "_idx"] = idx
+            arrays[tag + "_beta"] = d["data"][:, idx]
+            arrays[tag + "_boxes"] = np.array(d["boxes"], dtype=np.float64)
+            arrays[tag + "_h"] = np.array([d["dx"], d["dy"], d["dz"], d["dt"]])
+            arrays[tag + "_boundary"] = d["boundary"].astype(np.int8)
+            arrays[tag + "_result"] = res
+        np.savez_compressed(os.path.join(OUT, name + ".npz"), **arrays)
+        with open(os.path.join(OUT, name + ".par"), "w") as f:
+            f.write(par.lstrip())
+        print("wrote", name, sorted(arrays))
+    finally:
+        shutil.rmtree(work)
+
 
 def run_fmr_case(name, par):
     work = tempfile.mkdtemp(prefix="golden_")
@@ -422,3 +494,6 @@ if __name__ == "__main__":
     for n, p in FMR_CASES.items():
         if not only or n in only:
             run_fmr_case(n, p)
+    for n, p in TRACK_CASES.items():
+        if not only or n in only:
+            run_track_case(n, p)
