@@ -18,6 +18,8 @@
  *   nrgpu_mode = fmr        the whole Berger-Oliger step of all levels (one
  *                           or several boxes each) runs on the GPU at level
  *                           0's EVOLVE hook; set bssn/z4_register_algcon = no.
+ *                           With Gauge = moving_puncture the punctures are
+ *                           tracked on the device (nrgpu_fmr_track).
  * physics with z4 selects the Z4c system (all three modes).
  *
  *   nrgpu_multigrid = yes   the puncture initial-data solve (punctures_solver
@@ -351,6 +353,52 @@ int nrgpu_evolve_resident(tL *level)
  * every level at the end of the coarse step. */
 static nrgpu_fmr *fmr_h = 0;
 static double *fmr_state[64];
+/* puncture tracking in this mode (Gauge = moving_puncture): the device
+ * tracks on the finest level after each of its steps.  BAM's own
+ * track_puncture cannot run here: the host arrays already hold the end of
+ * the coarse step and the previous time level (betax_p) is never allocated,
+ * since BAM's evolve does not run.  So the set-up takes it out of the loop
+ * (lmaxpunc = -1: track_puncture skips every level,
+ * Gauge/moving_punctures.c:142) and nrgpu_track_fmr, an ANALYZE function,
+ * puts the device's positions in its place (grid->puncpos and the
+ * moving_punctureN_x/y/z parameters that BAM's checkpoint writes) */
+static int fmr_ntrack = 0;
+static double fmr_tpos[3 * NRGPU_MAX_PUNCTURES];
+
+static void fmr_track_setup(tG *g)
+{
+  int np, i, n;
+  if (!Getv("physics", "Gauge") || !Getv("Gauge", "moving_puncture") || !Getv("moving_puncture_track", "yes"))
+    return;
+  if (!Getv("moving_puncture_track_method", "int"))
+    errorexit("nrgpu: the fmr mode tracks punctures with the shift integrator only "
+              "(moving_puncture_track_method = int)");
+  n = Geti("nobjects");
+  if (n < 1 || n > NRGPU_MAX_PUNCTURES) errorexit("nrgpu: nobjects out of range for tracking");
+  for (np = 0; np < n; np++) {
+    if (g->lmaxpunc[np] != g->lmax) errorexit("nrgpu: the fmr mode tracks punctures on the finest level only");
+    for (i = 0; i < 3; i++) fmr_tpos[3 * np + i] = g->puncpos[np][i];
+    g->lmaxpunc[np] = -1;
+  }
+  check(nrgpu_fmr_track(fmr_h, n, fmr_tpos,
+                        Getv("moving_puncture_fixz", "BH") || Getv("moving_puncture_fixz", "BHNS")), "track");
+  fmr_ntrack = n;
+}
+
+int nrgpu_track_fmr(tL *level)
+{
+  tG *g = level->grid;
+  char str[100];
+  int np, i;
+  if (!nrgpu_mode_fmr || !fmr_ntrack || level->l != g->lmax) return 0;
+  for (np = 0; np < fmr_ntrack; np++)
+    for (i = 0; i < 3; i++) {
+      g->puncpos[np][i] = fmr_tpos[3 * np + i];
+      sprintf(str, "moving_puncture%d_%c", np + 1, 'x' + i);
+      if (ExistPar(str)) Setd(str, fmr_tpos[3 * np + i]);
+    }
+  return 0;
+}
 
 int nrgpu_evolve_fmr(tL *level)
 {
@@ -398,9 +446,16 @@ int nrgpu_evolve_fmr(tL *level)
     fp.order_RP = Geti("order_RP");
     fp.nbuffer = Geti("amr_nbuffer");
     check(nrgpu_fmr_create(nl, d, dt, nrgpu_system_z4 ? (void *)zp : (void *)bp, &fp, &fmr_h), "fmr");
+    fmr_track_setup(g);
   }
   for (l = 0; l < nl; l++) lists(fmr_state[l], g->level[l]->npoints, ptrs + l * nv);
   check(nrgpu_fmr_advance(fmr_h, ptrs, 1, 0), "fmr advance");
+  if (fmr_ntrack) {
+    check(nrgpu_fmr_punctures(fmr_h, fmr_tpos, 0), "punctures");
+    for (l = 0; l < fmr_ntrack; l++)
+      printf("nrgpu: puncture %d at %.17g %.17g %.17g\n", l + 1, fmr_tpos[3 * l], fmr_tpos[3 * l + 1],
+             fmr_tpos[3 * l + 2]);
+  }
   for (l = 0; l < nl; l++) {
     u->level = g->level[l];
     copy_vl(g->level[l], u, fmr_state[l], 0);
@@ -536,4 +591,5 @@ void bam_nrgpu(void)
   AddFun(POST_INITIALDATA, nrgpu_startup, "nrgpu: register the GPU evolution");
   AddFun(EVOLVE, nrgpu_evolve_resident, "nrgpu: resident RK4 step");
   AddFun(EVOLVE, nrgpu_evolve_fmr, "nrgpu: one coarse step of all levels");
+  AddFun(ANALYZE, nrgpu_track_fmr, "nrgpu: puncture positions tracked on the device");
 }

@@ -131,7 +131,10 @@ bssn_shiftdriver = 2.0
 bssn_shiftgammacoeff = 0.75""")
 
 
-def run_fmr(binary, extra_physics, extra, grid="single"):
+def run_fmr(binary, extra_physics, extra, grid="single", keep=None):
+    """Dumps of every level after 2 coarse steps and the run's stdout; with
+    keep, a list of output files (matched by name anywhere in the run
+    directory) whose text is also returned."""
     work = tempfile.mkdtemp(prefix="bamgpu_")
     par = FMR_PAR
     for a, b in (BINARY if grid == "binary" else BSSN_FMR if grid == "bssn" else ()):
@@ -142,7 +145,15 @@ def run_fmr(binary, extra_physics, extra, grid="single"):
             f.write(par % (extra_physics, extra))
         r = subprocess.run([binary, "-nt", "4", "t.par"], cwd=work, capture_output=True, text=True, timeout=600)
         assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
-        return [dumpfile.read(os.path.join(work, "state_it%d_l%d.bin" % (2 * 2 ** l, l))) for l in range(3)], r.stdout
+        dumps = [dumpfile.read(os.path.join(work, "state_it%d_l%d.bin" % (2 * 2 ** l, l))) for l in range(3)]
+        if keep is None:
+            return dumps, r.stdout
+        texts = {}
+        for root, _, files in os.walk(work):
+            for fn in files:
+                if fn in keep:
+                    texts[fn] = open(os.path.join(root, fn)).read()
+        return dumps, r.stdout, texts
     finally:
         shutil.rmtree(work, ignore_errors=True)
 
@@ -181,6 +192,32 @@ def test_bam_fmr_mode_matches_bam(gpu, cpu_state, grid):
         err = np.abs(a - b).max(axis=1) / np.maximum(np.abs(b).max(axis=1), 1e-8)
         assert keep[l].sum() > 0.3 * levels[l].npoints
         assert err.max() < 2e-11, (l, err.max())
+
+
+def test_bam_fmr_mode_tracks_punctures(gpu, cpu_state):
+    """nrgpu_mode = fmr with Gauge = moving_puncture on the binary's grid:
+    the punctures are tracked on the device after every finest-level step
+    and BAM's puncture positions are set from there.  The positions after 2
+    coarse steps (8 finest steps) match the reference's own tracker on the
+    CPU to the 7 digits of its output file (moving_punctureN_integrate,
+    written with %14.6e by write_tracked_puncture_N,
+    Gauge/moving_punctures.c:54-80)."""
+    gauge = "Gauge = moving_puncture\nmoving_puncture_fixz = none"
+    files = ["moving_puncture_integrate%d.lxyz2" % n for n in (1, 2)]
+    _, _, texts = run_fmr(BAM, " Gauge", gauge, "binary", keep=files)
+    _, out = run_fmr(BAM_GPU, " Gauge nrgpu", "nrgpu_mode = fmr\nz4_register_algcon = no\n" + gauge, "binary")
+    got = {}
+    for line in out.splitlines():
+        if line.startswith("nrgpu: puncture "):
+            w = line.split()
+            got[int(w[2])] = np.array([float(x) for x in w[4:7]])
+    assert sorted(got) == [1, 2]
+    for n in (1, 2):
+        rows = [r for r in texts[files[n - 1]].splitlines() if r.strip() and not r.startswith('"')]
+        want = np.array([float(x) for x in rows[-1].split()[:3]])
+        start = np.array([2.75 if n == 1 else -2.75, 0.0, 0.0])
+        assert np.abs(want - start).max() > 1e-5  # the reference's puncture moved
+        assert np.abs(got[n] - want).max() <= 1e-6 * max(1.0, np.abs(want).max()), (n, got[n], want)
 
 
 def run_mg(binary, extra_physics, extra):
