@@ -258,7 +258,13 @@ C5_SIZES = [194] + [136] * 8
 C5_DX0 = 0.5
 
 
-def gpu_fmr(steps=2, variants=(("graph", 1, 1), ("launches", 0, 1), ("graph_untuned_32x4", 1, 0)), warm=2,
+# start positions of the tracked punctures in the FMR workload (inside the
+# finest level of the nested boxes)
+TRACK_START = [[0.3, 0.1, 0.0], [-0.3, -0.1, 0.0]]
+
+
+def gpu_fmr(steps=2, variants=(("graph", 1, 1), ("launches", 0, 1), ("graph_untuned_32x4", 1, 0),
+                                ("graph_tracked", 1, 1, True)), warm=2,
             sizes=None, dx0=None, order=4):
     import torch
     from baum_b200 import abi, fmr, synthetic
@@ -278,9 +284,15 @@ def gpu_fmr(steps=2, variants=(("graph", 1, 1), ("launches", 0, 1), ("graph_untu
                        % (len(sizes), "4th" if order == 4 else "6th", 6, sizes, dx0),
            "rhs_point_updates_per_coarse_step": upd_per_coarse}
     # the product configuration (graph + per-level tuned block shapes), then
-    # plain launches, then the graph with every level at the 32 x 4 default
-    for key, use_graph, tune in variants:
+    # plain launches, then the graph with every level at the 32 x 4 default,
+    # then the product configuration tracking two punctures on the finest
+    # level (two tracker launches per finest-level step)
+    for v in variants:
+        key, use_graph, tune = v[:3]
+        track = len(v) > 3 and v[3]
         H = fmr.Hierarchy(levels, dt, params, abi.fmr_params(use_graph=use_graph, autotune=tune))
+        if track:
+            H.track(TRACK_START)
         blocks = ["%dx%dx%d" % H.block(l) for l in range(len(levels))]
         u = [state(lev) for lev in levels]
         H.advance(u, 1)   # first coarse step: 2nd-order time interpolation, no graph
@@ -296,6 +308,10 @@ def gpu_fmr(steps=2, variants=(("graph", 1, 1), ("launches", 0, 1), ("graph_untu
         out[key] = {"ms_per_coarse_step": ms, "value": upd_per_coarse / (ms * 1e-3), "blocks": blocks}
         finite = all(bool(torch.isfinite(t).all()) for t in u)
         out[key]["finite"] = finite
+        if track:
+            pos, st = H.punctures()
+            out[key]["punctures"] = pos.tolist()
+            out[key]["tracker_status"] = st.tolist()
         H.close()
         del u
         torch.cuda.empty_cache()
