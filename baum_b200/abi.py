@@ -351,6 +351,8 @@ def lib():
         "nrgpu_fmr_track": (C.c_int, [vp, C.c_int, C.POINTER(C.c_double), C.c_int]),
         "nrgpu_fmr_punctures": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
         "nrgpu_track_punctures": (C.c_int, [vp, pp, pp, C.c_double, C.c_int, C.c_int, C.c_int, vp, vp, vp]),
+        "nrgpu_track_punctures_extremum": (C.c_int, [vp, vp, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, vp, vp,
+                                                     vp]),
         "nrgpu_level_autotune": (C.c_int, [vp, C.c_int, vp, vp, C.POINTER(C.c_int)]),
         "nrgpu_level_block": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
         "nrgpu_level_get_block": (C.c_int, [vp, C.POINTER(C.c_int)]),

@@ -12,6 +12,12 @@
 // (lagrange.c:13-27).  track_puncture (Gauge/moving_punctures.c:135-200)
 // keeps the old position when the new one is off the level.
 //
+// The extremum search (track_moving_puncture_extremum,
+// moving_punctures_integrate.c:160-235, with findextremum, :105-140) fits a
+// parabola through the tracked variable at x - dx, x, x + dx per axis,
+// steps to its vertex (at most one spacing), and keeps the step only if the
+// variable improves and the step is at least minmove * dx.
+//
 // One thread per puncture.  Every product, quotient and sum is rounded
 // separately (no contraction into FMAs), in the reference's order, so the
 // positions equal the reference's bit for bit.
@@ -138,6 +144,51 @@ __global__ void track_kernel(TrackArgs A, int phase) {
   if (A.status) A.status[q] = (skip ? 0 : 1) | (in ? 2 : 0);
 }
 
+__device__ double findextremum(double vm, double v0, double vp, bool max) {
+  if (!isfinite(vm) || !isfinite(v0) || !isfinite(vp)) return 0.0;
+  const double curv = __dsub_rn(__dmul_rn(0.5, __dadd_rn(vp, vm)), v0);
+  double v;
+  if (fabs(curv) <= 1e-10) {
+    if ((vp > v0) && (vp > vm)) v = 1.0;
+    else if ((vm > v0) && (vm > vp)) v = -1.0;
+    else v = 0.0;
+    v = __dmul_rn(v, max ? 1.0 : -1.0);
+  } else {
+    v = __ddiv_rn(__dsub_rn(vm, vp), __dmul_rn(4.0, curv));
+    v = v > 1.0 ? 1.0 : v;
+    v = v < -1.0 ? -1.0 : v;
+  }
+  return v;
+}
+
+// extremum search of the tracked variable (passed as A.beta[0]) for a
+// maximum (find_max) or minimum; steps shorter than minimal_move are dropped;
+// A.fixz keeps z (pintoxyplane 1 or 3 in the reference)
+__global__ void extremum_kernel(TrackArgs A, int find_max, double minimal_move) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= A.n) return;
+  const double *var = A.beta[0];
+  double p0[3], p1[3], d[3];
+  for (int a = 0; a < 3; a++) p0[a] = A.pos[3 * q + a];
+  const double v0 = interpolate(A, var, p0);
+  for (int a = 0; a < 3; a++) {
+    double pm[3] = {p0[0], p0[1], p0[2]}, pp[3] = {p0[0], p0[1], p0[2]};
+    pm[a] = __dsub_rn(p0[a], A.h[a]);
+    pp[a] = __dadd_rn(p0[a], A.h[a]);
+    d[a] = __dmul_rn(findextremum(interpolate(A, var, pm), v0, interpolate(A, var, pp), find_max), A.h[a]);
+  }
+  for (int a = 0; a < 3; a++) p1[a] = __dadd_rn(p0[a], d[a]);
+  const double v = interpolate(A, var, p1);
+  const double len = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(d[0], d[0]), __dmul_rn(d[1], d[1])), __dmul_rn(d[2], d[2])));
+  if (!isfinite(v) || !isfinite(v0) || (find_max && v <= v0) || (!find_max && v >= v0) || len < minimal_move)
+    for (int a = 0; a < 3; a++) p1[a] = p0[a];
+  if (A.fixz) p1[2] = p0[2];
+  const bool in = on_level(A, p1);
+  if (in)
+    for (int a = 0; a < 3; a++) A.pos[3 * q + a] = p1[a];
+  if (A.status) A.status[q] = 1 | (in ? 2 : 0);
+}
+
 int make_args(nrgpu_level *L, const double *const *beta, const double *const *beta_p, double dt, int order, int fixz,
               int n, double *pos, double *b1, int *status, TrackArgs *A) {
   if (!L || !beta || !pos || n < 1) return nrgpu_set_error(NRGPU_ERR_ARG, "bad arguments");
@@ -204,6 +255,19 @@ extern "C" int nrgpu_track_punctures(nrgpu_level *L, const double *const *beta, 
   if (e) return e;
   NRGPU_CUDA_TRY(cudaSetDevice(L->device));
   track_kernel<<<(n + 31) / 32, 32, 0, (cudaStream_t)stream>>>(A, 0);
+  NRGPU_CUDA_TRY(cudaGetLastError());
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_track_punctures_extremum(nrgpu_level *L, const double *var, int find_max, double minmove,
+                                              int order, int fixz, int n, double *pos, int *status, void *stream) {
+  if (!var) return nrgpu_set_error(NRGPU_ERR_ARG, "null var");
+  const double *v3[3] = {var, var, var};
+  TrackArgs A;
+  int e = make_args(L, v3, nullptr, 0.0, order, fixz, n, pos, nullptr, status, &A);
+  if (e) return e;
+  NRGPU_CUDA_TRY(cudaSetDevice(L->device));
+  extremum_kernel<<<(n + 31) / 32, 32, 0, (cudaStream_t)stream>>>(A, find_max ? 1 : 0, minmove * L->dx);
   NRGPU_CUDA_TRY(cudaGetLastError());
   return NRGPU_OK;
 }

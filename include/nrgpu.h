@@ -420,6 +420,19 @@ int nrgpu_norms(nrgpu_level *L, const double *const *vars, int nvars, double *no
  * Positions equal the reference's bit for bit. */
 int nrgpu_track_punctures(nrgpu_level *L, const double *const *beta, const double *const *beta_p, double dt,
                           int order, int fixz, int n, double *pos, int *status, void *stream);
+/* The extremum search, track_moving_puncture_extremum
+ * (projects/Gauge/moving_punctures_integrate.c:160-235, with findextremum,
+ * :105-140; moving_puncture_track_method = ext), on the level variable var
+ * (device [npoints], moving_puncture_track_var, the lapse by default): per
+ * axis a parabola through var at x - h, x, x + h, a step to its vertex
+ * clamped to one spacing, kept only when var at the new point is larger
+ * (find_max) or smaller than at the old one and the step is at least
+ * minmove * dx (moving_puncture_track_minmove).  fixz keeps z
+ * (moving_puncture_fixz = NS or BHNS).  pos, status and the position test
+ * as for nrgpu_track_punctures (status bit 0 is always set).  Positions
+ * equal the reference's bit for bit. */
+int nrgpu_track_punctures_extremum(nrgpu_level *L, const double *var, int find_max, double minmove, int order,
+                                   int fixz, int n, double *pos, int *status, void *stream);
 
 /* ---- learned warm start of the puncture solve ----------------------------
  * No counterpart in the reference.  A coordinate MLP (NRGPU_MLP_IN features

@@ -223,8 +223,9 @@ int nrharness_post_evolve(tL *level)
   return 0;
 }
 
-/* the reference's tracker and the globals of moving_punctures.c:13-14 */
+/* the reference's trackers and the globals of moving_punctures.c:13-14 */
 int track_moving_puncture_integrate(tL *level, int np, double *pold, double *pnew);
+int track_moving_puncture_extremum(tL *level, int np, double *pold, double *pnew);
 int xyzinsidelevel(tL *level, double x, double y, double z);
 extern int pintoxyplane;
 
@@ -240,6 +241,7 @@ static void dump_track(tL *level, const char *tag)
   /* a vector is pushed by its first component: betax..z, betax_p..z_p */
   vlpush(vl, Ind("betax"));
   vlpush(vl, Ind("betax_p"));
+  vlpush(vl, Ind("alpha"));
   dump_varlist(level, vl, tag);
   vlfree(vl);
   snprintf(fn, sizeof fn, "%s/%s_l%d.txt", Gets("nrharness_dir"), tag, level->l);
@@ -261,6 +263,15 @@ static void dump_track(tL *level, const char *tag)
       fprintf(f, "%d %d %.17g %.17g %.17g %.17g %.17g %.17g %d\n", fix, moved, p[0], p[1], p[2],
               pnew[0], pnew[1], pnew[2], xyzinsidelevel(level, pnew[0], pnew[1], pnew[2]));
     }
+    /* the extremum search (moving_puncture_track_method = ext) on
+       moving_puncture_track_var, rows 10 (z free) and 11 (z pinned) */
+    if (Getv("physics", "Gauge"))
+      for (fix = 0; fix <= 1; fix++) {
+        pintoxyplane = fix;
+        moved = track_moving_puncture_extremum(level, 0, p, pnew);
+        fprintf(f, "%d %d %.17g %.17g %.17g %.17g %.17g %.17g %d\n", 10 + fix, moved, p[0], p[1], p[2],
+                pnew[0], pnew[1], pnew[2], xyzinsidelevel(level, pnew[0], pnew[1], pnew[2]));
+      }
   }
   pintoxyplane = 0;
   level->grid->lmaxpunc[0] = save;

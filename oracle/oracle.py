@@ -56,6 +56,8 @@ def lib():
             "oracle_fmr_restrict_prolong": [LD, LD, C.c_int, pp, pp, C.c_int, C.c_int],
             "oracle_adm_constraints": [LD, pp, pp, C.c_int, C.c_int],
             "oracle_norms": [LD, pp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)],
+            "oracle_track_extremum": [LD, C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int,
+                                      C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int)],
             "oracle_track_punctures": [LD, pp, pp, C.c_double, C.c_int, C.c_int, C.c_int,
                                        C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int),
                                        C.POINTER(C.c_int)],
@@ -258,3 +260,20 @@ def track_punctures(level, beta, beta_p, dt, pos, order=4, fixz=0):
     if e:
         raise RuntimeError("oracle_track_punctures: %d" % e)
     return pnew, moved, inside
+
+
+def track_extremum(level, var, pos, order=4, find_max=0, minmove=0.01, fixz=0):
+    """track_moving_puncture_extremum for each row of pos (n x 3): the new
+    positions and the position test."""
+    var = np.ascontiguousarray(var, dtype=np.float64)
+    pold = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+    n = pold.shape[0]
+    pnew = np.zeros_like(pold)
+    inside = np.zeros(n, dtype=np.int32)
+    dp = C.POINTER(C.c_double)
+    e = lib().oracle_track_extremum(C.byref(level.desc), var.ctypes.data, int(find_max), minmove, order, int(fixz), n,
+                                    pold.ctypes.data_as(dp), pnew.ctypes.data_as(dp),
+                                    inside.ctypes.data_as(C.POINTER(C.c_int)))
+    if e:
+        raise RuntimeError("oracle_track_extremum: %d" % e)
+    return pnew, inside

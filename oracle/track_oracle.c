@@ -16,6 +16,11 @@
  *     averaged corrector passes, z pinned for moving_puncture_fixz BH/BHNS)
  *   the position test of track_puncture  Gauge/moving_punctures.c:189-191
  *     (xyzinsidelevel, main/amr/points.c:100-133)
+ *   findextremum, track_moving_puncture_extremum
+ *                            moving_punctures_integrate.c:105-235
+ *     (a parabola through three interpolated values per axis, the step
+ *     clamped to one grid spacing, taken only if the value improves and the
+ *     step is at least minmove)
  */
 #include <math.h>
 
@@ -139,6 +144,57 @@ int oracle_track_punctures(const nrgpu_level_desc *L, const double *const *beta,
       if (fixz) p0[2] = p1[2];
     }
     inside[q] = inside_level(L, p0);
+  }
+  return 0;
+}
+
+/* the vertex of the parabola through (-1, vm), (0, v0), (1, vp), clamped to
+ * [-1, 1]; toward the larger neighbour when the curvature vanishes */
+static double findextremum(double vm, double v0, double vp, int max)
+{
+  double v;
+  if (!isfinite(vm) || !isfinite(v0) || !isfinite(vp)) return 0.;
+  if (fabs(0.5 * (vp + vm) - v0) <= 1e-10) {
+    if ((vp > v0) && (vp > vm)) v = 1.;
+    else if ((vm > v0) && (vm > vp)) v = -1.;
+    else v = 0.;
+    v *= max ? 1. : -1.;
+  } else {
+    v = (vm - vp) / (4. * (0.5 * (vp + vm) - v0));
+    v = v > 1. ? 1. : v;
+    v = v < -1. ? -1. : v;
+  }
+  return v;
+}
+
+/* extremum search of var around each old position: pnew, and the position
+ * test of the new location (the integrator's return value is always 1) */
+int oracle_track_extremum(const nrgpu_level_desc *L, const double *var, int find_max, double minmove, int order,
+                          int fixz, int np, const double *pold, double *pnew, int *inside)
+{
+  if (order < 2 || order > 8) return NRGPU_ERR_UNSUPPORTED;
+  const double h[3] = {L->dx, L->dy, L->dz};
+  const double minimal_move = minmove * L->dx;
+  for (int q = 0; q < np; q++) {
+    const double *p0 = pold + 3 * q;
+    double *p1 = pnew + 3 * q;
+    double d[3];
+    const double v0 = oracle_interpolate(L, var, p0[0], p0[1], p0[2], order);
+    for (int a = 0; a < 3; a++) {
+      double pm[3] = {p0[0], p0[1], p0[2]}, pp[3] = {p0[0], p0[1], p0[2]};
+      pm[a] = p0[a] - h[a];
+      pp[a] = p0[a] + h[a];
+      const double vm = oracle_interpolate(L, var, pm[0], pm[1], pm[2], order);
+      const double vp = oracle_interpolate(L, var, pp[0], pp[1], pp[2], order);
+      d[a] = findextremum(vm, v0, vp, find_max) * h[a];
+    }
+    const double v = oracle_interpolate(L, var, p0[0] + d[0], p0[1] + d[1], p0[2] + d[2], order);
+    if (!isfinite(v) || !isfinite(v0) || (find_max && v <= v0) || (!find_max && v >= v0) ||
+        sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) < minimal_move)
+      d[0] = d[1] = d[2] = 0.;
+    for (int a = 0; a < 3; a++) p1[a] = p0[a] + d[a];
+    if (fixz) p1[2] = p0[2];
+    inside[q] = inside_level(L, p1);
   }
   return 0;
 }

@@ -351,6 +351,15 @@ TRACK_CASES = {
 }
 for _o in (2, 6):
     TRACK_CASES["track_box_rp%d" % _o] = TRACK_CASES["track_box"] + "order_RP = %d\n" % _o
+# with the Gauge project the harness also runs the extremum search
+# (track_moving_puncture_extremum, moving_punctures_integrate.c:160-235) on
+# the lapse (its defaults: minimum, minimal move 0.01 dx)
+for _c in TRACK_CASES:
+    _p = TRACK_CASES[_c]
+    for _a in ("physics = adm bssn nrharness", "physics = adm bssn punctures nrharness",
+               "physics = adm z4 punctures nrharness"):
+        _p = _p.replace(_a, _a + " Gauge")
+    TRACK_CASES[_c] = _p + "Gauge = moving_puncture\n"
 # the fields of a tracking fixture are kept within TRACK_HALO points of a
 # start position (the rest is zero): the tracker reads only the cubes
 # around the start positions, which the CPU pins check

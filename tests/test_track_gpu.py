@@ -17,7 +17,7 @@ pytestmark = pytest.mark.gpu
 
 @pytest.mark.parametrize("case", sorted(TRACK_CASES))
 def test_level_tracker_matches_reference(gpu, case):
-    level, beta, beta_p, dt, res = track_fixture(case)
+    level, beta, beta_p, dt, res, alpha = track_fixture(case)
     dl = DeviceLevel(level)
     b = torch.from_numpy(beta).cuda()
     bp = torch.from_numpy(beta_p).cuda()
@@ -30,6 +30,17 @@ def test_level_tracker_matches_reference(gpu, case):
         assert np.array_equal(st & 1, rows[:, 1].astype(np.int32))
         assert np.array_equal((st >> 1) & 1, inside.astype(np.int32))
         # the reference's new position where it lies on the level, else the old one
+        want = np.where(inside[:, None], rows[:, 5:8], rows[:, 2:5])
+        assert np.array_equal(pos.cpu().numpy(), want)
+    # the extremum search on the lapse, z free and pinned
+    a = torch.from_numpy(alpha).cuda()
+    for fix in (10, 11):
+        rows = res[res[:, 0] == fix]
+        pos = torch.from_numpy(np.ascontiguousarray(rows[:, 2:5])).cuda()
+        st = tracking.track_moving_puncture_extremum(dl, a, pos, order=TRACK_CASES[case][0],
+                                                     fixz=fix == 11).cpu().numpy()
+        inside = rows[:, 8] == 1
+        assert np.array_equal((st >> 1) & 1, inside.astype(np.int32))
         want = np.where(inside[:, None], rows[:, 5:8], rows[:, 2:5])
         assert np.array_equal(pos.cpu().numpy(), want)
     dl.close()

@@ -20,22 +20,22 @@ TRACK_CASES = {"track_box": (4, 0), "track_box_rp2": (2, 0), "track_box_rp6": (6
 
 
 def track_fixture(case):
-    """(level, beta, beta_p, dt, result rows) of a tracking fixture: the
-    fields are the reference's, zero away from the start positions."""
+    """(level, beta, beta_p, dt, result rows, alpha) of a tracking fixture:
+    the fields are the reference's, zero away from the start positions."""
     g = np.load(os.path.join(GOLDEN, case + ".npz"))
     tag = [k[:-7] for k in g.files if k.endswith("_result")][0]
     boxes = [(int(b[0]), int(b[1]), int(b[2]), b[4], b[5], b[6]) for b in g[tag + "_boxes"]]
     h = g[tag + "_h"]
     level = abi.Level(boxes, float(h[0]), g[tag + "_boundary"].astype(np.int32), dy=float(h[1]), dz=float(h[2]),
                       symmetry=TRACK_CASES[case][1])
-    full = np.zeros((6, level.npoints))
+    full = np.zeros((7, level.npoints))
     full[:, g[tag + "_idx"]] = g[tag + "_beta"]
-    return level, full[:3].copy(), full[3:].copy(), float(h[3]), g[tag + "_result"]
+    return level, full[:3].copy(), full[3:6].copy(), float(h[3]), g[tag + "_result"], full[6].copy()
 
 
 @pytest.mark.parametrize("case", sorted(TRACK_CASES))
 def test_oracle_matches_reference_tracker(case):
-    level, beta, beta_p, dt, res = track_fixture(case)
+    level, beta, beta_p, dt, res, _ = track_fixture(case)
     order = TRACK_CASES[case][0]
     for fix in (0, 2):
         rows = res[res[:, 0] == fix]
@@ -45,12 +45,26 @@ def test_oracle_matches_reference_tracker(case):
         assert np.array_equal(pnew, rows[:, 5:8]), np.abs(pnew - rows[:, 5:8]).max()
 
 
+@pytest.mark.parametrize("case", sorted(TRACK_CASES))
+def test_oracle_matches_reference_extremum_search(case):
+    """track_moving_puncture_extremum on the lapse (minimum, minimal move
+    0.01 dx), z free (rows 10) and pinned (rows 11): bit for bit."""
+    level, _, _, _, res, alpha = track_fixture(case)
+    for fix in (10, 11):
+        rows = res[res[:, 0] == fix]
+        assert len(rows)
+        pnew, inside = oracle.track_extremum(level, alpha, rows[:, 2:5], TRACK_CASES[case][0], fixz=fix == 11)
+        assert np.array_equal(inside, rows[:, 8].astype(np.int32))
+        assert np.array_equal(pnew, rows[:, 5:8]), np.abs(pnew - rows[:, 5:8]).max()
+
+
 def test_fixtures_cover_the_edge_cases():
     """Moved and unmoved positions (cubes that leave a box, points below a
     symmetry plane), new positions off the level, several boxes."""
     seen = {"unmoved_cube": False, "half": False, "off_level": False, "moved": False}
     for case in TRACK_CASES:
-        level, _, _, _, res = track_fixture(case)
+        level, _, _, _, res, _ = track_fixture(case)
+        res = res[res[:, 0] < 10]
         moved = np.any(res[:, 2:5] != res[:, 5:8], axis=1)
         seen["moved"] |= bool(moved.any())
         seen["unmoved_cube"] |= bool(np.any(~moved & (res[:, 1] == 1) & (res[:, 8] == 1)))
