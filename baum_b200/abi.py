@@ -324,6 +324,7 @@ def lib():
         "nrgpu_to_adm": (C.c_int, [vp, pp, pp, C.c_double, vp]),
         "nrgpu_adm_constraints": (C.c_int, [vp, pp, pp, C.c_int, C.c_int, vp]),
         "nrgpu_norms": (C.c_int, [vp, pp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), vp]),
+        "nrgpu_output0d": (C.c_int, [vp, pp, C.c_int, C.POINTER(C.c_double), vp]),
         "nrgpu_mlp_nparams": (C.c_int, []),
         "nrgpu_mlp_create": (C.c_int, [C.c_int, C.POINTER(vp)]),
         "nrgpu_mlp_destroy": (C.c_int, [vp]),

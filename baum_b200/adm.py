@@ -66,6 +66,21 @@ def norms(dl, v, stream=None):
     return n2, ni
 
 
+# the output types of write_level_0d (utility/output/output0d.c:58-62)
+OUTPUT0D_TYPES = ("max", "min", "norm", "normInf", "integral")
+
+
+def write_level_0d(dl, v, stream=None):
+    """The 0d output scalars of each row of v over the flag-0 points
+    (nrgpu_output0d): a (nrows, 5) numpy array, columns in the order of
+    OUTPUT0D_TYPES."""
+    n = v.shape[0]
+    out = np.zeros((n, 5))
+    abi.check(abi.lib().nrgpu_output0d(dl.handle, _ptrs(v, n), n, out.ctypes.data_as(C.POINTER(C.c_double)),
+                                       _stream(stream)))
+    return out
+
+
 def computeadmconstraints(dl, u, order_centered, mode=PLAIN, chipsipower=-4.0, stream=None):
     """to_adm + constraints + norms of one level: returns (adm, con,
     {name: (norm2, normInf)}), the numbers the reference writes to its

@@ -10,6 +10,8 @@
 // point in registers and contracts them in the order of the spec.  The
 // reductions are two-pass and fixed-order, so a norm is bit-reproducible
 // from run to run.
+#include <cfloat>
+
 #include "nrgpu_level.cuh"
 #include "nrgpu_fd.cuh"
 
@@ -399,5 +401,105 @@ extern "C" int nrgpu_norms(nrgpu_level *L, const double *const *vars, int nvars,
     norm2[v] = h[2 * v];
     norminf[v] = h[2 * v + 1];
   }
+  return NRGPU_OK;
+}
+
+// ---- 0d output ---------------------------------------------------------------
+// write_level_0d (utility/output/output0d.c:28-116) through bampi_allreduce
+// (main/bampi/reduce.c:37-135) on one rank: over the flag-0 points, per
+// variable the maximum, the minimum, the RMS (the list's norm2 times
+// sqrt(nvars)), the maximum of |u| and the sum times dx^3.  Two passes as
+// for the norms: block partials, then a fixed-order fold, so the results do
+// not depend on scheduling.
+constexpr int kRed0d = 5;
+
+__global__ void __launch_bounds__(kRedThreads) red0d_partial_kernel(NormIn V, const int *__restrict__ boundary,
+                                                                    int np, double *part) {
+  const int v = blockIdx.y;
+  const double *u = V.p[v];
+  double mx = -DBL_MAX, mn = DBL_MAX, s = 0.0, s2 = 0.0, ma = -DBL_MAX;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
+    if (__ldg(boundary + i) != 0) continue;
+    const double x = ldg(u + i);
+    mx = fmax(mx, x);
+    mn = fmin(mn, x);
+    s += x;
+    s2 += x * x;
+    ma = fmax(ma, fabs(x));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    mn = fmin(mn, __shfl_down_sync(0xffffffffu, mn, o));
+    s += __shfl_down_sync(0xffffffffu, s, o);
+    s2 += __shfl_down_sync(0xffffffffu, s2, o);
+    ma = fmax(ma, __shfl_down_sync(0xffffffffu, ma, o));
+  }
+  __shared__ double w5[kRed0d][kRedThreads / 32];
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    w5[0][w] = mx; w5[1][w] = mn; w5[2][w] = s; w5[3][w] = s2; w5[4][w] = ma;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < kRedThreads / 32; ++q) {
+      mx = fmax(mx, w5[0][q]); mn = fmin(mn, w5[1][q]); s += w5[2][q]; s2 += w5[3][q]; ma = fmax(ma, w5[4][q]);
+    }
+    double *o = part + (size_t)kRed0d * (v * kRedBlocks + blockIdx.x);
+    o[0] = mx; o[1] = mn; o[2] = s; o[3] = s2; o[4] = ma;
+  }
+}
+
+__global__ void red0d_final_kernel(const double *part, double ninner, double dx3, double *res, int nv) {
+  const int v = blockIdx.x;
+  if (v >= nv) return;
+  double mx = -DBL_MAX, mn = DBL_MAX, s = 0.0, s2 = 0.0, ma = -DBL_MAX;
+  for (int b = threadIdx.x; b < kRedBlocks; b += 32) {
+    const double *q = part + (size_t)kRed0d * (v * kRedBlocks + b);
+    mx = fmax(mx, q[0]); mn = fmin(mn, q[1]); s += q[2]; s2 += q[3]; ma = fmax(ma, q[4]);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    mn = fmin(mn, __shfl_down_sync(0xffffffffu, mn, o));
+    s += __shfl_down_sync(0xffffffffu, s, o);
+    s2 += __shfl_down_sync(0xffffffffu, s2, o);
+    ma = fmax(ma, __shfl_down_sync(0xffffffffu, ma, o));
+  }
+  if (threadIdx.x == 0) {
+    double *r = res + kRed0d * v;
+    r[0] = mx;
+    r[1] = mn;
+    r[2] = ninner > 0 ? sqrt(s2 / ninner) : -1.0;
+    r[3] = ma;
+    r[4] = s * dx3;
+  }
+}
+
+extern "C" int nrgpu_output0d(nrgpu_level *L, const double *const *vars, int nvars, double *out, void *stream) {
+  if (!L || !vars || nvars < 1 || nvars > kMaxNormVars || !out)
+    return nrgpu_set_error(NRGPU_ERR_ARG, "bad arguments (1 <= nvars <= %d)", kMaxNormVars);
+  NormIn V;
+  for (int v = 0; v < kMaxNormVars; ++v) V.p[v] = v < nvars ? vars[v] : nullptr;
+  for (int v = 0; v < nvars; ++v)
+    if (!vars[v]) return nrgpu_set_error(NRGPU_ERR_ARG, "null vars[%d]", v);
+  NRGPU_CUDA_TRY(cudaSetDevice(L->device));
+  if (!L->d_red0d) {
+    const size_t bytes = sizeof(double) * kRed0d * (kRedBlocks + 1) * kMaxNormVars;
+    if (cudaMalloc(&L->d_red0d, bytes) != cudaSuccess) {
+      L->d_red0d = nullptr;
+      cudaGetLastError();
+      return nrgpu_set_error(NRGPU_ERR_NOMEM, "0d reduction buffer of %zu bytes", bytes);
+    }
+  }
+  double *part = L->d_red0d;
+  double *res = part + (size_t)kRed0d * kRedBlocks * kMaxNormVars;
+  const cudaStream_t st = (cudaStream_t)stream;
+  red0d_partial_kernel<<<dim3(kRedBlocks, nvars), kRedThreads, 0, st>>>(V, L->d_boundary, L->npoints, part);
+  NRGPU_CUDA_TRY(cudaGetLastError());
+  red0d_final_kernel<<<nvars, 32, 0, st>>>(part, (double)L->ninner, L->dx * L->dx * L->dx, res, nvars);
+  NRGPU_CUDA_TRY(cudaGetLastError());
+  NRGPU_CUDA_TRY(cudaMemcpyAsync(out, res, sizeof(double) * kRed0d * nvars, cudaMemcpyDeviceToHost, st));
+  NRGPU_CUDA_TRY(cudaStreamSynchronize(st));
   return NRGPU_OK;
 }

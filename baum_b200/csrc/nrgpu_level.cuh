@@ -38,6 +38,8 @@ struct nrgpu_level {
   // points with boundary flag 0, and the norm reduction buffer (first use)
   long ninner;
   double *d_red;
+  // partials and results of the 0d output reductions (first use)
+  double *d_red0d;
   // extents of the rhs kernels' 128-thread blocks (x, y, z)
   int blk[3];
   // reflection symmetry: the axes (desc.symmetry), the ghost list, and the

@@ -164,6 +164,7 @@ extern "C" int nrgpu_level_destroy(nrgpu_level *L) {
   cudaFree(L->scratch);
   cudaFree(L->hoststate);
   cudaFree(L->d_red);
+  cudaFree(L->d_red0d);
   for (int q = 0; q < NRGPU_HOST_SLABS; ++q) {
     if (L->hev_in[q]) cudaEventDestroy(L->hev_in[q]);
     if (L->hev_out[q]) cudaEventDestroy(L->hev_out[q]);

@@ -402,6 +402,15 @@ int nrgpu_adm_constraints(nrgpu_level *L, const double *const *adm, double *cons
 int nrgpu_norms(nrgpu_level *L, const double *const *vars, int nvars, double *norm2, double *norminf,
                 void *stream);
 
+/* The scalars of the 0d output, write_level_0d (utility/output/output0d.c:
+ * 28-116) with bampi_allreduce (main/bampi/reduce.c:37-135) on one rank,
+ * for nvars (<= 32) variables over the points with boundary flag 0:
+ * out[5 * v + t] for the output types t = 0 max, 1 min, 2 norm (RMS),
+ * 3 normInf (max |u|), 4 integral (sum times dx^3).  Without such points:
+ * -DBL_MAX, DBL_MAX, -1, -DBL_MAX, 0, as the reference.  Waits for the
+ * stream. */
+int nrgpu_output0d(nrgpu_level *L, const double *const *vars, int nvars, double *out, void *stream);
+
 /* ---- puncture tracking ----------------------------------------------------
  * The shift-integration tracker, track_moving_puncture_integrate
  * (projects/Gauge/moving_punctures_integrate.c:29-100) with the position

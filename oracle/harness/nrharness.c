@@ -198,6 +198,7 @@ int nrharness_post_initialdata(tL *level)
 }
 
 static void dump_track(tL *level, const char *tag);
+static void dump_0d(tL *level, tVarList *u, const char *tag);
 
 int nrharness_post_evolve(tL *level)
 {
@@ -214,6 +215,10 @@ int nrharness_post_evolve(tL *level)
     if (Getv("nrharness_constraints", "yes")) {
       snprintf(tag, sizeof tag, "con_it%d", level->iteration + 1);
       dump_constraints(level, tag);
+    }
+    if (Getv("nrharness_0d", "yes")) {
+      snprintf(tag, sizeof tag, "red0d_it%d", level->iteration + 1);
+      dump_0d(level, u, tag);
     }
     if (Getv("nrharness_track", "yes")) {
       snprintf(tag, sizeof tag, "track_it%d", level->iteration + 1);
@@ -279,6 +284,38 @@ static void dump_track(tL *level, const char *tag)
   printf("nrharness: wrote %s\n", fn);
 }
 
+/* the reductions of write_level_0d (utility/output/output0d.c:28-116) on
+ * the evolved list, one line per type 0..4 (max, min, norm, normInf,
+ * integral) with the same corrections (norm times sqrt(nvars), integral
+ * times dx^3) */
+static void dump_0d(tL *level, tVarList *u, const char *tag)
+{
+  char fn[1024];
+  double *r;
+  int t, j;
+  FILE *f;
+  snprintf(fn, sizeof fn, "%s/%s_l%d.txt", Gets("nrharness_dir"), tag, level->l);
+  f = fopen(fn, "w");
+  if (!f) errorexits("nrharness: cannot open %s", fn);
+  for (t = 0; t <= 4; t++) {
+    if (t == 0) bampi_allreduce_max(u, &r);
+    if (t == 1) bampi_allreduce_min(u, &r);
+    if (t == 2) bampi_allreduce_norm(u, &r);
+    if (t == 3) bampi_allreduce_normInf(u, &r);
+    if (t == 4) bampi_allreduce_sum(u, &r);
+    for (j = 0; j < u->n; j++) {
+      double v = r[j];
+      if (t == 2) v *= sqrt(u->n);
+      if (t == 4) v *= pow(level->dx, 3);
+      fprintf(f, "%.17g ", v);
+    }
+    fprintf(f, "\n");
+    free(r);
+  }
+  fclose(f);
+  printf("nrharness: wrote %s\n", fn);
+}
+
 void bam_nrharness(void)
 {
   if (!Getv("physics", "nrharness")) return;
@@ -289,6 +326,7 @@ void bam_nrharness(void)
   AddPar("nrharness_mg", "no", "dump punctures_u after the initial data solve [no,yes]");
   AddPar("nrharness_flags", "no", "dump the refinement flags of every level after the initial data [no,yes]");
   AddPar("nrharness_constraints", "no", "with each state dump also dump ADM variables and constraints [no,yes]");
+  AddPar("nrharness_0d", "no", "with each state dump write the 0d reductions of the evolved list [no,yes]");
   AddPar("nrharness_track", "no", "with each state dump run the shift-integration tracker [no,yes]");
   AddPar("nrharness_track_points", "", "start positions of the tracker, x y z per position");
   AddPar("nrharness_data", "none", "synthetic data over the evolved variables [none,fourier]");

@@ -360,6 +360,38 @@ for _c in TRACK_CASES:
                "physics = adm z4 punctures nrharness"):
         _p = _p.replace(_a, _a + " Gauge")
     TRACK_CASES[_c] = _p + "Gauge = moving_puncture\n"
+# the reductions of the 0d output (write_level_0d, output0d.c:28-116: max,
+# min, norm, normInf, integral over the flag-0 points) of the evolved list
+# after a state dump, on a box and on an octant grid (SYMBOUND points
+# excluded); the state and the reference's results are stored
+RED0D_CASES = {
+    "red0d_box": CASES["bssn_fourier_o4"].replace("nrharness_rhs = yes\n", "").replace(
+        "nrharness_dump = 0 2", "nrharness_dump = 2\nnrharness_0d = yes"),
+    "red0d_octant": CASES["bssn_punc_octant"].replace("nrharness_rhs = yes\n", "").replace(
+        "nrharness_dump = 0 4", "nrharness_dump = 4\nnrharness_0d = yes"),
+}
+
+
+def run_red0d_case(name, par):
+    work = tempfile.mkdtemp(prefix="golden_")
+    try:
+        with open(os.path.join(work, name + ".par"), "w") as f:
+            f.write(par)
+        r = subprocess.run([BAM, "-nt", "4", name + ".par"], cwd=work, capture_output=True, text=True)
+        if r.returncode:
+            raise RuntimeError(r.stdout[-3000:] + r.stderr[-3000:])
+        txt = [fn for fn in os.listdir(work) if fn.startswith("red0d_") and fn.endswith(".txt")][0]
+        d = dumpfile.read(os.path.join(work, txt.replace("red0d_", "state_").replace(".txt", ".bin")))
+        np.savez_compressed(os.path.join(OUT, name + ".npz"), state=d["data"], boundary=d["boundary"],
+                            boxes=np.array(d["boxes"], dtype=np.float64), dx=d["dx"],
+                            result=np.loadtxt(os.path.join(work, txt), ndmin=2))
+        with open(os.path.join(OUT, name + ".par"), "w") as f:
+            f.write(par.lstrip())
+        print("wrote", name)
+    finally:
+        shutil.rmtree(work)
+
+
 # the fields of a tracking fixture are kept within TRACK_HALO points of a
 # start position (the rest is zero): the tracker reads only the cubes
 # around the start positions, which the CPU pins check
@@ -506,3 +538,6 @@ if __name__ == "__main__":
     for n, p in TRACK_CASES.items():
         if not only or n in only:
             run_track_case(n, p)
+    for n, p in RED0D_CASES.items():
+        if not only or n in only:
+            run_red0d_case(n, p)
