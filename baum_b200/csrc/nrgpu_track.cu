@@ -18,9 +18,11 @@
 // steps to its vertex (at most one spacing), and keeps the step only if the
 // variable improves and the step is at least minmove * dx.
 //
-// One thread per puncture.  Every product, quotient and sum is rounded
-// separately (no contraction into FMAs), in the reference's order, so the
-// positions equal the reference's bit for bit.
+// One warp per puncture: the 32 lanes fetch each interpolation cube into
+// shared memory together (one round trip instead of order^2 dependent
+// ones), then every lane forms the same sums.  Every product, quotient and
+// sum is rounded separately (no contraction into FMAs), in the reference's
+// order, so the positions equal the reference's bit for bit.
 #include <math.h>
 
 #include "nrgpu_level.cuh"
@@ -68,7 +70,9 @@ __device__ int node_of(double c, double x0, double h, int n) {
   return i;
 }
 
-__device__ double interpolate(const TrackArgs &A, const double *v, const double p[3]) {
+// cube: the warp's shared buffer of kMaxOrder^3 values; all lanes call
+// with the same arguments
+__device__ double interpolate(const TrackArgs &A, const double *v, const double p[3], double *cube) {
   const int a = A.order, nh = (A.order - 1) / 2;
   double xc[3];
   for (int d = 0; d < 3; d++)
@@ -81,14 +85,20 @@ __device__ double interpolate(const TrackArgs &A, const double *v, const double 
     const int k = node_of(xc[2], B.z0, A.h[2], B.o);
     if (i < 0 || j < 0 || k < 0) continue;
     if (i + a > B.m || j + a > B.n || k + a > B.o) return 0.0;
+    const int lane = threadIdx.x & 31, a3 = a * a * a;
+    for (int t = lane; t < a3; t += 32) {
+      const int ii = t % a, jj = (t / a) % a, kk = t / (a * a);
+      cube[t] = v[(long)B.noffset + (i + ii) + (long)B.m * (j + jj) + (long)B.m * B.n * (k + kk)];
+    }
+    __syncwarp();
     double c[kMaxOrder], w[kMaxOrder], vv[kMaxOrder][kMaxOrder], line[kMaxOrder];
     lagrange(a, p[2], xc[2], A.h[2], c);
     for (int ii = 0; ii < a; ii++)
       for (int jj = 0; jj < a; jj++) {
-        const long base = (long)B.noffset + (i + ii) + (long)B.m * (j + jj) + (long)B.m * B.n * k;
-        for (int kk = 0; kk < a; kk++) line[kk] = v[base + (long)B.m * B.n * kk];
+        for (int kk = 0; kk < a; kk++) line[kk] = cube[ii + a * jj + a * a * kk];
         vv[ii][jj] = dot(a, c, line);
       }
+    __syncwarp();  // every lane has read the cube before the next fetch
     lagrange(a, p[1], xc[1], A.h[1], c);
     for (int ii = 0; ii < a; ii++) w[ii] = dot(a, c, vv[ii]);
     lagrange(a, p[0], xc[0], A.h[0], c);
@@ -118,27 +128,34 @@ __device__ bool below_half(const TrackArgs &A, const double p[3]) {
 
 // phase 0: one call with beta and beta_p; phase 1: before the step, the
 // shift at the old positions into b1; phase 2: after the step, from b1
-__global__ void track_kernel(TrackArgs A, int phase) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(32) track_kernel(TrackArgs A, int phase) {
+  __shared__ double cube[kMaxOrder * kMaxOrder * kMaxOrder];
+  const int q = blockIdx.x;
   if (q >= A.n) return;
+  const bool lead = threadIdx.x == 0;
   double p1[3], p0[3], b1[3], b0[3];
   for (int d = 0; d < 3; d++) p1[d] = A.pos[3 * q + d];
+  __syncwarp();  // every lane has read pos before lane 0 writes it
   const bool skip = below_half(A, p1);
   if (phase == 1) {
     if (!skip)
-      for (int d = 0; d < 3; d++) A.b1[3 * q + d] = interpolate(A, A.beta[d], p1);
+      for (int d = 0; d < 3; d++) {
+        const double b = interpolate(A, A.beta[d], p1, cube);
+        if (lead) A.b1[3 * q + d] = b;
+      }
     return;
   }
   for (int d = 0; d < 3; d++) p0[d] = p1[d];
   if (!skip) {
-    for (int d = 0; d < 3; d++) b1[d] = phase == 0 ? interpolate(A, A.beta_p[d], p1) : A.b1[3 * q + d];
+    for (int d = 0; d < 3; d++) b1[d] = phase == 0 ? interpolate(A, A.beta_p[d], p1, cube) : A.b1[3 * q + d];
     for (int it = 0; it < 3; it++) {
-      for (int d = 0; d < 3; d++) b0[d] = interpolate(A, A.beta[d], p0);
+      for (int d = 0; d < 3; d++) b0[d] = interpolate(A, A.beta[d], p0, cube);
       for (int d = 0; d < 3; d++) p0[d] = __dsub_rn(p1[d], __dmul_rn(__dmul_rn(A.dt, 0.5), __dadd_rn(b0[d], b1[d])));
     }
     if (A.fixz) p0[2] = p1[2];
   }
   const bool in = on_level(A, p0);
+  if (!lead) return;
   if (in)
     for (int d = 0; d < 3; d++) A.pos[3 * q + d] = p0[d];
   if (A.status) A.status[q] = (skip ? 0 : 1) | (in ? 2 : 0);
@@ -164,26 +181,31 @@ __device__ double findextremum(double vm, double v0, double vp, bool max) {
 // extremum search of the tracked variable (passed as A.beta[0]) for a
 // maximum (find_max) or minimum; steps shorter than minimal_move are dropped;
 // A.fixz keeps z (pintoxyplane 1 or 3 in the reference)
-__global__ void extremum_kernel(TrackArgs A, int find_max, double minimal_move) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(32) extremum_kernel(TrackArgs A, int find_max, double minimal_move) {
+  __shared__ double cube[kMaxOrder * kMaxOrder * kMaxOrder];
+  const int q = blockIdx.x;
   if (q >= A.n) return;
   const double *var = A.beta[0];
   double p0[3], p1[3], d[3];
   for (int a = 0; a < 3; a++) p0[a] = A.pos[3 * q + a];
-  const double v0 = interpolate(A, var, p0);
+  __syncwarp();
+  const double v0 = interpolate(A, var, p0, cube);
   for (int a = 0; a < 3; a++) {
     double pm[3] = {p0[0], p0[1], p0[2]}, pp[3] = {p0[0], p0[1], p0[2]};
     pm[a] = __dsub_rn(p0[a], A.h[a]);
     pp[a] = __dadd_rn(p0[a], A.h[a]);
-    d[a] = __dmul_rn(findextremum(interpolate(A, var, pm), v0, interpolate(A, var, pp), find_max), A.h[a]);
+    const double vm = interpolate(A, var, pm, cube);
+    const double vp = interpolate(A, var, pp, cube);
+    d[a] = __dmul_rn(findextremum(vm, v0, vp, find_max), A.h[a]);
   }
   for (int a = 0; a < 3; a++) p1[a] = __dadd_rn(p0[a], d[a]);
-  const double v = interpolate(A, var, p1);
+  const double v = interpolate(A, var, p1, cube);
   const double len = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(d[0], d[0]), __dmul_rn(d[1], d[1])), __dmul_rn(d[2], d[2])));
   if (!isfinite(v) || !isfinite(v0) || (find_max && v <= v0) || (!find_max && v >= v0) || len < minimal_move)
     for (int a = 0; a < 3; a++) p1[a] = p0[a];
   if (A.fixz) p1[2] = p0[2];
   const bool in = on_level(A, p1);
+  if (threadIdx.x != 0) return;
   if (in)
     for (int a = 0; a < 3; a++) A.pos[3 * q + a] = p1[a];
   if (A.status) A.status[q] = 1 | (in ? 2 : 0);
@@ -230,7 +252,7 @@ int nrgpu_track_before_step(nrgpu_level *L, const double *const *beta, int order
   TrackArgs A;
   int e = make_args(L, beta, nullptr, 0.0, order, 0, n, (double *)pos, b1, nullptr, &A);
   if (e) return e;
-  track_kernel<<<(n + 31) / 32, 32, 0, st>>>(A, 1);
+  track_kernel<<<n, 32, 0, st>>>(A, 1);
   NRGPU_CUDA_TRY(cudaGetLastError());
   return NRGPU_OK;
 }
@@ -240,7 +262,7 @@ int nrgpu_track_after_step(nrgpu_level *L, const double *const *beta, double dt,
   TrackArgs A;
   int e = make_args(L, beta, nullptr, dt, order, fixz, n, pos, (double *)b1, status, &A);
   if (e) return e;
-  track_kernel<<<(n + 31) / 32, 32, 0, st>>>(A, 2);
+  track_kernel<<<n, 32, 0, st>>>(A, 2);
   NRGPU_CUDA_TRY(cudaGetLastError());
   return NRGPU_OK;
 }
@@ -254,7 +276,7 @@ extern "C" int nrgpu_track_punctures(nrgpu_level *L, const double *const *beta, 
   int e = make_args(L, beta, beta_p, dt, order, fixz, n, pos, nullptr, status, &A);
   if (e) return e;
   NRGPU_CUDA_TRY(cudaSetDevice(L->device));
-  track_kernel<<<(n + 31) / 32, 32, 0, (cudaStream_t)stream>>>(A, 0);
+  track_kernel<<<n, 32, 0, (cudaStream_t)stream>>>(A, 0);
   NRGPU_CUDA_TRY(cudaGetLastError());
   return NRGPU_OK;
 }
@@ -267,7 +289,7 @@ extern "C" int nrgpu_track_punctures_extremum(nrgpu_level *L, const double *var,
   int e = make_args(L, v3, nullptr, 0.0, order, fixz, n, pos, nullptr, status, &A);
   if (e) return e;
   NRGPU_CUDA_TRY(cudaSetDevice(L->device));
-  extremum_kernel<<<(n + 31) / 32, 32, 0, (cudaStream_t)stream>>>(A, find_max ? 1 : 0, minmove * L->dx);
+  extremum_kernel<<<n, 32, 0, (cudaStream_t)stream>>>(A, find_max ? 1 : 0, minmove * L->dx);
   NRGPU_CUDA_TRY(cudaGetLastError());
   return NRGPU_OK;
 }
