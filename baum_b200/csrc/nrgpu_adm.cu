@@ -450,6 +450,9 @@ __global__ void __launch_bounds__(kRedThreads) red0d_partial_kernel(NormIn V, co
   }
 }
 
+// the norm as bampi_allreduce_norm2 and write_level_0d form it: the count n
+// is nvars x inner points (reduce.c:79-90, :215-216), the RMS sqrt(s2 / n)
+// times sqrt(nvars) (output0d.c:71-75); the integral times pow(dx, 3) (:86-89)
 __global__ void red0d_final_kernel(const double *part, double ninner, double dx3, double *res, int nv) {
   const int v = blockIdx.x;
   if (v >= nv) return;
@@ -470,7 +473,8 @@ __global__ void red0d_final_kernel(const double *part, double ninner, double dx3
     double *r = res + kRed0d * v;
     r[0] = mx;
     r[1] = mn;
-    r[2] = ninner > 0 ? sqrt(s2 / ninner) : -1.0;
+    const double n = (double)nv * ninner;
+    r[2] = (n > 0 ? sqrt(s2 / n) : -1.0) * sqrt((double)nv);
     r[3] = ma;
     r[4] = s * dx3;
   }
@@ -497,7 +501,7 @@ extern "C" int nrgpu_output0d(nrgpu_level *L, const double *const *vars, int nva
   const cudaStream_t st = (cudaStream_t)stream;
   red0d_partial_kernel<<<dim3(kRedBlocks, nvars), kRedThreads, 0, st>>>(V, L->d_boundary, L->npoints, part);
   NRGPU_CUDA_TRY(cudaGetLastError());
-  red0d_final_kernel<<<nvars, 32, 0, st>>>(part, (double)L->ninner, L->dx * L->dx * L->dx, res, nvars);
+  red0d_final_kernel<<<nvars, 32, 0, st>>>(part, (double)L->ninner, pow(L->dx, 3), res, nvars);
   NRGPU_CUDA_TRY(cudaGetLastError());
   NRGPU_CUDA_TRY(cudaMemcpyAsync(out, res, sizeof(double) * kRed0d * nvars, cudaMemcpyDeviceToHost, st));
   NRGPU_CUDA_TRY(cudaStreamSynchronize(st));

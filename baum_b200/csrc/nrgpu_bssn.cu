@@ -15,6 +15,7 @@
 // accumulators are the only long-lived state.  Algebraically this is the
 // reference's expression; it differs from it only in rounding.
 #include <cstdio>
+#include <mutex>
 #include "nrgpu_level.cuh"
 #include "nrgpu_fd.cuh"
 
@@ -1234,6 +1235,9 @@ extern "C" int nrgpu_bssn_evolve_host(nrgpu_level *L, double *const *host_u, int
 // loads the library, until the process exits.  All calls share the array:
 // calls that overlap on the GPU (different streams, or host threads using the
 // same device) race on it and must be serialised by the caller.
+// g_noalloc_status collects, over all calls since it was last read, bit 0 of
+// word 0 for a non-finite rhs and word 1 for an inner point without room for
+// its stencil; nrgpu_bssn_noalloc_status reads and clears it.
 #define NRGPU_NOALLOC_MAX_POINTS 16384
 static __device__ __align__(256) double g_noalloc_scratch[3 * NRGPU_NV * NRGPU_NOALLOC_MAX_POINTS];
 static __device__ __align__(256) int g_noalloc_status[4];
@@ -1309,9 +1313,29 @@ __global__ void bssn_surface_kernel(CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPt
 
 }  // namespace
 
-// device addresses of the static arrays, looked up once per device
+// device addresses of the static arrays, looked up once per device (under a
+// lock, so that host threads making their first call at once do not race);
+// a cudaDeviceReset between calls reloads the module and is not supported
 static double *g_noalloc_ptr[64];
 static int *g_noalloc_status_ptr[64];
+static std::mutex g_noalloc_setup;
+
+static int noalloc_setup(int *dev_out) {
+  int dev = 0;
+  NRGPU_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return nrgpu_set_error(NRGPU_ERR_ARG, "device %d out of range", dev);
+  std::lock_guard<std::mutex> lk(g_noalloc_setup);
+  if (!g_noalloc_ptr[dev]) {
+    // set-up on the first call on this device, with this device current
+    void *sp = nullptr, *st = nullptr;
+    NRGPU_CUDA_TRY(cudaGetSymbolAddress(&sp, g_noalloc_scratch));
+    NRGPU_CUDA_TRY(cudaGetSymbolAddress(&st, g_noalloc_status));
+    g_noalloc_status_ptr[dev] = (int *)st;
+    g_noalloc_ptr[dev] = (double *)sp;
+  }
+  *dev_out = dev;
+  return NRGPU_OK;
+}
 
 extern "C" int nrgpu_bssn_rk4_step_noalloc(const nrgpu_box *box, double dx, double dy, double dz,
                                            double *const *u, double dt, const nrgpu_bssn_params *p,
@@ -1329,20 +1353,10 @@ extern "C" int nrgpu_bssn_rk4_step_noalloc(const nrgpu_box *box, double dx, doub
                            NRGPU_NOALLOC_MAX_POINTS);
   if (!(dx > 0.0) || !(dy > 0.0) || !(dz > 0.0)) return nrgpu_set_error(NRGPU_ERR_ARG, "grid spacing must be > 0");
   int dev = 0;
-  NRGPU_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) return nrgpu_set_error(NRGPU_ERR_ARG, "device %d out of range", dev);
-  if (!g_noalloc_ptr[dev]) {
-    // set-up on the first call on this device, with this device current
-    void *sp = nullptr, *st = nullptr;
-    NRGPU_CUDA_TRY(cudaGetSymbolAddress(&sp, g_noalloc_scratch));
-    NRGPU_CUDA_TRY(cudaGetSymbolAddress(&st, g_noalloc_status));
-    g_noalloc_status_ptr[dev] = (int *)st;
-    g_noalloc_ptr[dev] = (double *)sp;
-  }
+  if ((e = noalloc_setup(&dev))) return e;
   double *scr = g_noalloc_ptr[dev];
   int *status = g_noalloc_status_ptr[dev];
   cudaStream_t s = (cudaStream_t)stream;
-  NRGPU_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int) * 4, s));
   VarPtrs P, V1, V2;
   for (int v = 0; v < NRGPU_NV; ++v) {
     P.p[v] = scr + (0 * NRGPU_NV + v) * np;
@@ -1366,6 +1380,23 @@ extern "C" int nrgpu_bssn_rk4_step_noalloc(const nrgpu_box *box, double dx, doub
   }
   bssn_algcon_kernel<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(U, 0, (int)np, p->subtractA, p->normalizedetg);
   NRGPU_CUDA_TRY(cudaGetLastError());
+  return NRGPU_OK;
+}
+
+// the status of the allocation-free step: read on the caller's stream, then
+// cleared; allocates nothing
+extern "C" int nrgpu_bssn_noalloc_status(int *flag, void *stream) {
+  if (!flag) return nrgpu_set_error(NRGPU_ERR_ARG, "null flag");
+  int dev = 0, e;
+  if ((e = noalloc_setup(&dev))) return e;
+  int *status = g_noalloc_status_ptr[dev];
+  cudaStream_t s = (cudaStream_t)stream;
+  int h[2] = {0, 0};
+  NRGPU_CUDA_TRY(cudaMemcpyAsync(h, status, sizeof h, cudaMemcpyDeviceToHost, s));
+  NRGPU_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof h, s));
+  NRGPU_CUDA_TRY(cudaStreamSynchronize(s));
+  *flag = h[0] ? 1 : 0;
+  if (h[1]) return nrgpu_set_error(NRGPU_ERR_ARG, "an inner point had no room for its stencil");
   return NRGPU_OK;
 }
 

@@ -213,10 +213,19 @@ int nrgpu_level_nan_flag(nrgpu_level *lev, int *flag);
  * make it before any stream capture.  All calls share the array: calls that
  * overlap on the GPU race and must be serialised by the caller.  The caller
  * passes u (24 device pointers, box->noffset == 0), updated in place.
+ * A non-finite rhs is recorded in a status word of the library image, kept
+ * over calls until nrgpu_bssn_noalloc_status reads it.  A cudaDeviceReset
+ * between calls is not supported (the array's address is looked up once).
  * No counterpart in the reference. */
 int nrgpu_bssn_rk4_step_noalloc(const nrgpu_box *box, double dx, double dy, double dz,
                                 double *const *u, double dt, const nrgpu_bssn_params *p,
                                 void *stream);
+/* Status of nrgpu_bssn_rk4_step_noalloc since the last read, allocating
+ * nothing: waits for `stream`, sets *flag = 1 if any rhs value was not
+ * finite, and clears the word; returns NRGPU_ERR_ARG if an inner point had
+ * no room for its stencil.  The companion of nrgpu_level_nan_flag for that
+ * entry point.  No counterpart in the reference. */
+int nrgpu_bssn_noalloc_status(int *flag, void *stream);
 
 /* ---- Z4c (device pointers, 25-variable lists) -------------------------------- */
 

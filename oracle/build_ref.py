@@ -98,7 +98,9 @@ def write_generated(ref, gen, extra=()):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    # the reference tree: --ref, else $BAM_REFERENCE_DIR, else the build
+    # container's read-only copy
+    ap.add_argument("--ref", default=os.environ.get("BAM_REFERENCE_DIR", "/root/reference"))
     ap.add_argument("-j", type=int, default=os.cpu_count() or 4)
     ap.add_argument("--cc", default="gcc")
     a = ap.parse_args()

@@ -4,8 +4,12 @@ against the reference's own values, written by the dump harness for its
 evolved list after a state dump (tests/golden/red0d_*.npz, a box and an
 octant grid whose SYMBOUND points are left out).  The CPU test restates the
 reductions in numpy against the reference; the GPU test runs
-nrgpu_output0d through the C ABI: max, min and normInf bit for bit, the
-sums within 1e-13 of their scale (summation order)."""
+nrgpu_output0d through the C ABI: max, min and normInf bit for bit; the
+norm in the reference's form, sqrt(sum u^2 / (nvars n)) sqrt(nvars), within
+5e-15 relative (the reference's own sequential sum is 1.6e-15 from the exact
+one on these cases, and the device sums in another order); the integral,
+times pow(dx, 3), within 1e-13 of the sum of |u| dx^3."""
+import math
 import os
 
 import numpy as np
@@ -29,7 +33,7 @@ def check(got, ref, g):
     u = g["state"][:, g["boundary"] == 0]
     for t in (0, 1, 3):
         assert np.array_equal(got[:, t], ref[:, t]), t
-    assert np.all(np.abs(got[:, 2] - ref[:, 2]) <= 1e-13 * ref[:, 2])
+    assert np.all(np.abs(got[:, 2] - ref[:, 2]) <= 5e-15 * ref[:, 2]), np.abs(got[:, 2] - ref[:, 2]) / ref[:, 2]
     scale = np.abs(u).sum(1) * float(g["dx"]) ** 3
     assert np.all(np.abs(got[:, 4] - ref[:, 4]) <= 1e-13 * scale), np.abs(got[:, 4] - ref[:, 4]) / scale
 
@@ -38,8 +42,9 @@ def check(got, ref, g):
 def test_restatement_matches_reference(name):
     level, g = case(name)
     u = g["state"][:, g["boundary"] == 0]
-    got = np.stack([u.max(1), u.min(1), np.sqrt((u * u).sum(1) / u.shape[1]), np.abs(u).max(1),
-                    u.sum(1) * float(g["dx"]) ** 3], axis=1)
+    nv = u.shape[0]
+    got = np.stack([u.max(1), u.min(1), np.sqrt((u * u).sum(1) / (nv * u.shape[1])) * math.sqrt(nv),
+                    np.abs(u).max(1), u.sum(1) * math.pow(float(g["dx"]), 3)], axis=1)
     check(got, g["result"].T, g)
 
 
