@@ -75,6 +75,14 @@ class DeviceLevel:
         abi.check(abi.lib().nrgpu_level_autotune(self.handle, int(system), C.byref(params), _stream(stream), b))
         return tuple(b)
 
+    def tile(self, on=-1):
+        """The staged-tile (TMA) interior rhs: on = 1 / 0 sets it, -1 only
+        queries; returns the setting."""
+        r = abi.lib().nrgpu_level_tile(self.handle, int(on))
+        if r < 0:
+            abi.check(r)
+        return bool(r)
+
     def nan_flag(self):
         f = C.c_int()
         abi.check(abi.lib().nrgpu_level_nan_flag(self.handle, C.byref(f)))

@@ -15,9 +15,11 @@
 // accumulators are the only long-lived state.  Algebraically this is the
 // reference's expression; it differs from it only in rounding.
 #include <cstdio>
+#include <cstring>
 #include <mutex>
 #include "nrgpu_level.cuh"
 #include "nrgpu_fd.cuh"
+#include "nrgpu_tma.cuh"
 
 namespace {
 
@@ -716,6 +718,7 @@ __global__ void vlcopy_kernel(VarPtrs dst, CVarPtrs src, int npoints) {
 
 
 #include "nrgpu_z4.cuh"
+#include "nrgpu_bssn_tile.cuh"
 
 }  // namespace
 
@@ -851,6 +854,116 @@ static CVarPtrs cptrs(const VarPtrs &v) {
   return c;
 }
 
+// ---- tensor maps of the staged tiles ----------------------------------------
+// cuTensorMapEncodeTiled from the driver, looked up once (no link-time
+// dependency on libcuda)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn tma_encoder() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)f;
+  });
+  return fn;
+}
+
+// the maps of the last few (variable list, box) pairs a level launched on
+struct TmaCacheEntry {
+  const double *key[NRGPU_Z4_NVARS];
+  int box, nv, valid;
+  CUtensorMap m[NRGPU_Z4_NVARS];
+};
+struct TmaCache {
+  int next;
+  TmaCacheEntry e[8];
+};
+
+// one 3-D map per variable over box b of the level: (m, n, o) FP64 points,
+// boxes of kBX x kBY x kBZ, zero fill outside the array
+static int tma_maps(nrgpu_level *L, int b, const double *const *ptr, int nv, const CUtensorMap **out) {
+  if (!L->tma_cache) {
+    L->tma_cache = calloc(1, sizeof(TmaCache));
+    if (!L->tma_cache) return nrgpu_set_error(NRGPU_ERR_NOMEM, "tensor-map cache");
+  }
+  TmaCache *C = (TmaCache *)L->tma_cache;
+  for (int q = 0; q < 8; ++q) {
+    TmaCacheEntry &E = C->e[q];
+    if (!E.valid || E.box != b || E.nv != nv) continue;
+    bool same = true;
+    for (int v = 0; v < nv && same; ++v) same = E.key[v] == ptr[v];
+    if (same) {
+      *out = E.m;
+      return NRGPU_OK;
+    }
+  }
+  EncodeTiledFn enc = tma_encoder();
+  if (!enc) return nrgpu_set_error(NRGPU_ERR_CUDA, "cuTensorMapEncodeTiled not available from the driver");
+  TmaCacheEntry &E = C->e[C->next];
+  C->next = (C->next + 1) % 8;
+  E.valid = 0;
+  const BoxGeo &bx = L->hbox[b];
+  const cuuint64_t dims[3] = {(cuuint64_t)bx.m, (cuuint64_t)bx.n, (cuuint64_t)bx.o};
+  const cuuint64_t strides[2] = {(cuuint64_t)bx.m * 8, (cuuint64_t)bx.m * bx.n * 8};
+  const cuuint32_t box[3] = {kBX, kBY, kBZ}, es[3] = {1, 1, 1};
+  for (int v = 0; v < nv; ++v) {
+    const CUresult r = enc(&E.m[v], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void *)(ptr[v] + bx.noffset), dims, strides,
+                           box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return nrgpu_set_error(NRGPU_ERR_CUDA, "cuTensorMapEncodeTiled: error %d", (int)r);
+    E.key[v] = ptr[v];
+  }
+  E.box = b;
+  E.nv = nv;
+  E.valid = 1;
+  *out = E.m;
+  return NRGPU_OK;
+}
+
+// whether the staged-tile kernel covers box b with these parameters: every
+// tap within the halo of 3 (lopsided advection shifted by 1 or 2 at 4th
+// order, centred 6th-order advection), row and plane strides and every
+// field's start on 16-byte boundaries (the copy engine's rule)
+static bool tile_eligible(const nrgpu_level *L, int b, const double *const *ptr, int nv, int order, int lop,
+                          int lop6) {
+  const BoxGeo &bx = L->hbox[b];
+  if (bx.m < 3 || bx.n < 3 || bx.o < 3 || (bx.m & 1)) return false;
+  if (order >= 4 && (lop < 1 || lop > 2)) return false;
+  if (order == 6 && lop6 != 3) return false;
+  for (int v = 0; v < nv; ++v)
+    if (((uintptr_t)(ptr[v] + bx.noffset)) & 15) return false;
+  return true;
+}
+
+static int launch_bssn_tile(nrgpu_level *L, int b, const CUtensorMap *maps, const CVarPtrs &U, const VarPtrs &out,
+                            const CVarPtrs &pre, const VarPtrs &acc, const Epilogue &E, const nrgpu_bssn_params &p,
+                            cudaStream_t st, int k0, int k1) {
+  const BoxGeo &bx = L->hbox[b];
+  BssnMaps M;
+  memcpy(M.m, maps, sizeof M.m);
+  const int ntiles = ((bx.m - 2 + kTX - 1) / kTX) * ((bx.n - 2 + kTY - 1) / kTY) * ((k1 - k0 + kTZ) / kTZ);
+  static std::once_flag attr4, attr6;
+  if (p.order_centered <= 4) {
+    std::call_once(attr4, [] {
+      cudaFuncSetAttribute(bssn_rhs_tile_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem);
+    });
+    bssn_rhs_tile_kernel<4><<<ntiles, kTileThreads, kTileSmem, st>>>(M, U, out, pre, acc, E, p, bx, L->d_boundary,
+                                                                      L->dx, L->dy, L->dz, L->d_status, k0, k1);
+  } else {
+    std::call_once(attr6, [] {
+      cudaFuncSetAttribute(bssn_rhs_tile_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem);
+    });
+    bssn_rhs_tile_kernel<6><<<ntiles, kTileThreads, kTileSmem, st>>>(M, U, out, pre, acc, E, p, bx, L->d_boundary,
+                                                                      L->dx, L->dy, L->dz, L->d_status, k0, k1);
+  }
+  return NRGPU_OK;
+}
+
 // launch the interior and flagged kernels of one rhs evaluation
 // (kb <= k <= ke: the planes of the interior launch, whole boxes by default)
 static int launch_rhs(nrgpu_level *L, const CVarPtrs &U, const VarPtrs &out, const CVarPtrs &pre, const VarPtrs &acc,
@@ -872,6 +985,14 @@ static int launch_rhs(nrgpu_level *L, const CVarPtrs &U, const VarPtrs &out, con
       if (bx.m < 3 || bx.n < 3 || bx.o < 3) continue;
       const int k0 = max(kb, 1), k1 = min(ke, bx.o - 2);
       if (k1 < k0) continue;
+      if (L->tile && tile_eligible(L, b, U.p, NRGPU_NV, p.order_centered, p.advection_lopsided,
+                                   p.advection_lopsided6)) {
+        const CUtensorMap *maps = nullptr;
+        int e = tma_maps(L, b, U.p, NRGPU_NV, &maps);
+        if (e) return e;
+        if ((e = launch_bssn_tile(L, b, maps, U, out, pre, acc, E, p, st, k0, k1))) return e;
+        continue;
+      }
       // the block shape of the level (32 x 4 x 1, or what nrgpu_level_autotune
       // measured fastest for this box); 128 or 256 threads, one point each
       const dim3 blk(L->blk[0], L->blk[1], L->blk[2]);
@@ -1678,12 +1799,37 @@ extern "C" int nrgpu_level_autotune(nrgpu_level *L, int system, const void *para
       bb = c;
     }
   }
+  for (int q = 0; q < 3; ++q) L->blk[q] = cand[bb][q];
+  // the staged-tile kernel (BSSN) against the fastest shape
+  L->tile = 0;
+  if (!e && system == NRGPU_SYSTEM_BSSN) {
+    const nrgpu_bssn_params &bp = *(const nrgpu_bssn_params *)params;
+    VarPtrs P, O;
+    for (int v = 0; v < NRGPU_NV; ++v) {
+      P.p[v] = scr + (long)v * np;
+      O.p[v] = scr + (long)(ZNV + v) * np;
+    }
+    bool elig = true;
+    for (int b = 0; b < L->nboxes; ++b)
+      elig = elig && tile_eligible(L, b, P.p, NRGPU_NV, bp.order_centered, bp.advection_lopsided,
+                                   bp.advection_lopsided6);
+    if (elig) {
+      L->tile = 1;
+      for (int rep = 0; rep < 4 && !e; ++rep) {
+        if (rep == 1) cudaEventRecord(ev0, st);
+        e = launch_rhs(L, cptrs(P), O, cptrs(P), O, E, bp, st, true, false);
+      }
+      cudaEventRecord(ev1, st);
+      cudaEventSynchronize(ev1);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ev0, ev1);
+      L->tile = !e && ms < best;
+    }
+  }
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
-  for (int q = 0; q < 3; ++q) {
-    L->blk[q] = cand[bb][q];
-    if (best_block) best_block[q] = cand[bb][q];
-  }
+  for (int q = 0; q < 3; ++q)
+    if (best_block) best_block[q] = L->tile ? 0 : cand[bb][q];
   if (e) return e;
   NRGPU_CUDA_TRY(cudaStreamSynchronize(st));
   return NRGPU_OK;
@@ -1694,7 +1840,14 @@ extern "C" int nrgpu_level_block(nrgpu_level *L, int bx, int by, int bz) {
   if (!L || !pow2(bx) || !pow2(by) || !pow2(bz) || (bx * by * bz != 128 && bx * by * bz != 256))
     return nrgpu_set_error(NRGPU_ERR_ARG, "block %d x %d x %d (powers of two, 128 or 256 threads)", bx, by, bz);
   L->blk[0] = bx; L->blk[1] = by; L->blk[2] = bz;
+  L->tile = 0;
   return NRGPU_OK;
+}
+
+extern "C" int nrgpu_level_tile(nrgpu_level *L, int on) {
+  if (!L) return nrgpu_set_error(NRGPU_ERR_ARG, "null level");
+  if (on >= 0) L->tile = on ? 1 : 0;
+  return L->tile;
 }
 
 extern "C" int nrgpu_level_get_block(nrgpu_level *L, int *block) {

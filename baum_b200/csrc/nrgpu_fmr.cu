@@ -577,7 +577,8 @@ extern "C" int nrgpu_fmr_create(int nl, const nrgpu_level_desc *levels, const do
     double *scr;
     if ((e = nrgpu_level_scratch(F->L[l], &scr))) break;  // no allocation later, inside a graph capture
     if (l > 0 && (e = setup_pair(F, l))) break;
-    if (p->autotune &&
+    if (p->autotune == 2) nrgpu_level_tile(F->L[l], 1);
+    if (p->autotune == 1 &&
         (e = nrgpu_level_autotune(F->L[l], p->system,
                                   p->system == NRGPU_SYSTEM_BSSN ? (const void *)&F->bp[l] : (const void *)&F->zp[l],
                                   nullptr, nullptr)))

@@ -55,6 +55,11 @@ struct nrgpu_level {
   // host-buffer step (created on first use)
   cudaStream_t hs_copy, hs_comp;
   cudaEvent_t hev_in[NRGPU_HOST_SLABS], hev_out[NRGPU_HOST_SLABS];
+  // interior rhs over TMA-staged tiles (1) instead of per-point global
+  // loads (0), where the level and the parameters allow it; the tensor maps
+  // of recently used variable lists (host memory, first use)
+  int tile;
+  void *tma_cache;
 };
 
 // library-internal pieces shared by the entry points and the mesh-refinement

@@ -174,6 +174,7 @@ extern "C" int nrgpu_level_destroy(nrgpu_level *L) {
   if (L->ev_join) cudaEventDestroy(L->ev_join);
   if (L->hs_copy) cudaStreamDestroy(L->hs_copy);
   if (L->hs_comp) cudaStreamDestroy(L->hs_comp);
+  free(L->tma_cache);
   free(L->hbox);
   free(L);
   return NRGPU_OK;
@@ -208,7 +209,8 @@ extern "C" int nrgpu_level_nan_flag(nrgpu_level *L, int *flag) {
   int h[2] = {0, 0};
   NRGPU_CUDA_TRY(cudaMemcpy(h, L->d_status, sizeof h, cudaMemcpyDeviceToHost));
   NRGPU_CUDA_TRY(cudaMemset(L->d_status, 0, sizeof h));
-  *flag = h[0] ? 1 : 0;
+  *flag = h[0] & 1;
+  if (h[0] & 2) return nrgpu_set_error(NRGPU_ERR_TIMEOUT, "a wait for a staged tile ran out of time");
   if (h[1]) return nrgpu_set_error(NRGPU_ERR_ARG, "an inner point had no room for its stencil");
   return NRGPU_OK;
 }

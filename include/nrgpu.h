@@ -198,7 +198,9 @@ int nrgpu_bssn_evolve_host(nrgpu_level *lev, double *const *host_u, int nsteps,
 
 /* Device NaN/Inf flag of the level: set by the RHS kernels when any rhs is
  * not finite (the reference prints per point, check.c:235).  Reads and
- * clears it; *flag = 1 if set. */
+ * clears it; *flag = 1 if set.  Returns NRGPU_ERR_TIMEOUT if a wait of the
+ * staged-tile kernel for its shared-memory tiles ran out of time (the
+ * kernel then stops computing and returns). */
 int nrgpu_level_nan_flag(nrgpu_level *lev, int *flag);
 
 /* One RK4 step of a single box (outer layer = physical boundary, inner
@@ -303,8 +305,10 @@ typedef struct {
   int nbuffer;                  /* amr_nbuffer (bam_amr.c) */
   int use_graph;                /* capture the coarse steps after the first
                                    in a CUDA graph and replay it */
-  int autotune;                 /* pick each level's rhs block shape with
-                                   nrgpu_level_autotune at creation */
+  int autotune;                 /* 1: pick each level's rhs launch shape with
+                                   nrgpu_level_autotune at creation; 2: the
+                                   staged-tile rhs (nrgpu_level_tile) on every
+                                   level it covers; 0: the default shape */
 } nrgpu_fmr_params;
 
 typedef struct nrgpu_fmr nrgpu_fmr;
@@ -374,12 +378,22 @@ enum { NRGPU_SYSTEM_BSSN = 0, NRGPU_SYSTEM_Z4C = 1 };
  * and the given system (NRGPU_SYSTEM_BSSN / _Z4C) and parameters, on a flat
  * state in the level's RK4 scratch (the user's arrays are not touched),
  * keeps the fastest for the level and returns it in best_block[3] (may be
- * NULL).  Waits for the stream.  nrgpu_level_block sets a shape directly
- * (powers of two, bx by bz = 128 or 256; default 32 x 4 x 1).  Results do
- * not depend on the shape. */
+ * NULL).  For BSSN it also times the staged-tile kernel (16 x 4 x 4 tiles
+ * whose fields are brought into shared memory by TMA loads) where the level
+ * and parameters allow it, and keeps it when faster; best_block is then
+ * {0, 0, 0}.  Waits for the stream.  nrgpu_level_block sets a shape
+ * directly (powers of two, bx by bz = 128 or 256; default 32 x 4 x 1) and
+ * turns the staged-tile kernel off.  Results do not depend on the shape;
+ * the staged-tile kernel adds the same terms in another order (rounding
+ * differences only). */
 int nrgpu_level_autotune(nrgpu_level *L, int system, const void *params, void *stream, int *best_block);
 int nrgpu_level_block(nrgpu_level *L, int bx, int by, int bz);
 int nrgpu_level_get_block(nrgpu_level *L, int *block);
+/* The BSSN interior rhs over TMA-staged tiles: on = 1 uses it on every box
+ * it covers (even row length, 16-byte aligned fields, advection shift 1 or
+ * 2 at 4th order, the centred 6th-order advection), the per-point kernel
+ * elsewhere; 0 turns it off; -1 only queries.  Returns the setting. */
+int nrgpu_level_tile(nrgpu_level *L, int on);
 
 /* ---- ADM diagnostics ------------------------------------------------------
  * ADM metric and extrinsic curvature from the conformal variables:
