@@ -453,8 +453,11 @@ def count_launches(fn):
         if "at::" in n or "Memcpy" in n or "Memset" in n or "memcpy" in n or "memset" in n:
             continue
         names.append(n)
-    short = sorted(set(n.split("<")[0].split("(")[-1] if "(" in n.split("<")[0] else n.split("<")[0] for n in names))
-    return len(names), short
+    short = set()
+    for n in names:
+        m = re.findall(r"([a-z][a-z0-9_]*_kernel)", n)
+        short.add(m[-1] if m else n[:40])
+    return len(names), sorted(short)
 
 
 def max_over_ranks(values, device):

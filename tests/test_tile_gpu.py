@@ -42,6 +42,8 @@ def tiled(lev):
 
 @pytest.mark.parametrize("case", sorted(CASES))
 def test_tile_rhs_and_rk4_match_reference(gpu, case):
+    """The reference's rhs; its RK4 states where the fixture holds them,
+    else the oracle's."""
     g = load_golden(case)
     lev = golden_level(g)
     p = abi.bssn_params(**CASES[case])
@@ -54,7 +56,9 @@ def test_tile_rhs_and_rk4_match_reference(gpu, case):
     for _ in range(2):
         bssn.evolve_rk_rk4(dl, u, float(g["dt"]), p)
     torch.cuda.synchronize()
-    assert relerr(u.cpu().numpy(), g["state_it2_l0"]).max() < TOL
+    want = g["state_it2_l0"] if "state_it2_l0" in g else \
+        oracle.bssn_evolve(lev, np.ascontiguousarray(g["state_it0_l0"]), float(g["dt"]), 2, p)
+    assert relerr(u.cpu().numpy(), want).max() < TOL
     assert not dl.nan_flag()
 
 

@@ -83,7 +83,7 @@ def test_noalloc_status_reports_a_non_finite_state(gpu):
     f, status = _entry(L)
     lev, u0 = _state()
     p = abi.bssn_params()
-    u0[13, lev.npoints // 2] = np.nan   # K at an inner point near the centre
+    u0[13, 11 + 22 * (11 + 22 * 11)] = np.nan   # K at the centre point (11, 11, 11)
     u = torch.from_numpy(u0).cuda()
     stream = torch.cuda.current_stream()
     flag = C.c_int(-1)
