@@ -561,7 +561,7 @@ __device__ __forceinline__ int ladder(int order, int d) {
 // (flag 0) only, the flagged ones are handled by bssn_flagged_kernel
 // CSY, CSZ: the box strides dj = m and dk = m n when known at compile time
 // (0 = read them from the box)
-template <int CSY = 0, int CSZ = 0, int MAXO = 6, int MINB = NRGPU_RHS_MINBLOCKS>
+template <int CSY = 0, int CSZ = 0, int ORD = 4, int MINB = NRGPU_RHS_MINBLOCKS>
 __global__ void __launch_bounds__(256, MINB) bssn_rhs_kernel(CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPtrs acc,
                                                       Epilogue E, const nrgpu_bssn_params p, BoxGeo box,
                                                       const int *__restrict__ boundary, double dx, double dy,
@@ -579,17 +579,49 @@ __global__ void __launch_bounds__(256, MINB) bssn_rhs_kernel(CVarPtrs U, VarPtrs
   P.h[0] = dx; P.h[1] = dy; P.h[2] = dz;
   int d = min(min(i, j), k);
   d = min(d, min(min(P.imax - i, P.jmax - j), P.kmax - k));
+  // points nearer the faces than the full stencil reaches take a lower
+  // order (the ladder): bssn_ladder_kernel computes them
+  if (d < ORD / 2) return;
   P.dist = d;
-  const int oc = ladder(p.order_centered, d);
-  const int oa = ladder(p.order_advection, d);
-  if (oc == 0 || oc != oa) {  // mixed orders are refused at the entry point
+  double r[NRGPU_NV];
+  bssn_point<ORD, CSY, CSZ>(U, P, p, r);
+  double s = 0.0;
+#pragma unroll
+  for (int v = 0; v < NRGPU_NV; ++v) s += r[v];
+  if (!isfinite(s)) atomicOr(status, 1);
+  store(r, P.ijk, out, pre, acc, E, p);
+}
+
+// the points of the order ladder (flag 0, within 2 of a box face, sorted by
+// that distance; the launch covers those below the full order's reach):
+// 2nd order one point in, 4th two points in for 6th-order runs, as
+// boundaryNaway/boundaryNormore select them (bam_amr_loops_box.h:215-220); a
+// flag-0 point on a face has no stencil at all and is refused
+__global__ void bssn_ladder_kernel(CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPtrs acc, Epilogue E,
+                                   const nrgpu_bssn_params p, const FlagPoint *__restrict__ pts, int n,
+                                   const BoxGeo *__restrict__ boxes, double dx, double dy, double dz, int *status,
+                                   int k0, int k1) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const FlagPoint fp = pts[t];
+  if (fp.k < k0 || fp.k > k1) return;
+  const BoxGeo b = boxes[fp.box];
+  PointCtx P;
+  P.i = fp.i; P.j = fp.j; P.k = fp.k;
+  P.imax = b.m - 1; P.jmax = b.n - 1; P.kmax = b.o - 1;
+  P.st[0] = 1; P.st[1] = b.m; P.st[2] = b.m * b.n;
+  P.ijk = fp.ijk;
+  P.h[0] = dx; P.h[1] = dy; P.h[2] = dz;
+  P.dist = fp.flag;
+  const int oc = ladder(p.order_centered, P.dist);
+  if (oc == 0 || oc != ladder(p.order_advection, P.dist)) {
     atomicOr(status + 1, 1);
     return;
   }
+  if (oc == p.order_centered) return;
   double r[NRGPU_NV];
-  if (oc == 2) bssn_point<2, CSY, CSZ>(U, P, p, r);
-  else if (oc == 4 || MAXO < 6) bssn_point<4, CSY, CSZ>(U, P, p, r);
-  else bssn_point<MAXO, CSY, CSZ>(U, P, p, r);
+  if (oc == 2) bssn_point<2>(U, P, p, r);
+  else bssn_point<4>(U, P, p, r);
   double s = 0.0;
 #pragma unroll
   for (int v = 0; v < NRGPU_NV; ++v) s += r[v];
@@ -925,16 +957,16 @@ static int tma_maps(nrgpu_level *L, int b, const double *const *ptr, int nv, con
   return NRGPU_OK;
 }
 
-// whether the staged-tile kernel covers box b with these parameters: every
-// tap within the halo of 3 (lopsided advection shifted by 1 or 2 at 4th
-// order, centred 6th-order advection), row and plane strides and every
+// whether the staged-tile kernel covers box b with these parameters: runs of
+// order 4 or 6 whose full-order taps stay within the halo of 3 (lopsided
+// advection shifted by 1 or 2 at 4th order, centred 6th-order advection;
+// the ladder points are computed apart), row and plane strides and every
 // field's start on 16-byte boundaries (the copy engine's rule)
 static bool tile_eligible(const nrgpu_level *L, int b, const double *const *ptr, int nv, int order, int lop,
                           int lop6) {
   const BoxGeo &bx = L->hbox[b];
   if (bx.m < 3 || bx.n < 3 || bx.o < 3 || (bx.m & 1)) return false;
-  if (order >= 4 && (lop < 1 || lop > 2)) return false;
-  if (order == 6 && lop6 != 3) return false;
+  if (order == 2 || (order == 4 && (lop < 1 || lop > 2)) || (order == 6 && lop6 != 3)) return false;
   for (int v = 0; v < nv; ++v)
     if (((uintptr_t)(ptr[v] + bx.noffset)) & 15) return false;
   return true;
@@ -998,25 +1030,25 @@ static int launch_rhs(nrgpu_level *L, const CVarPtrs &U, const VarPtrs &out, con
       const dim3 blk(L->blk[0], L->blk[1], L->blk[2]);
       const dim3 grd((bx.m - 2 + blk.x - 1) / blk.x, (bx.n - 2 + blk.y - 1) / blk.y, (k1 - k0 + blk.z) / blk.z);
       // box strides as compile-time constants for the sizes of the standard
-      // workloads: every stencil tap becomes one load with an immediate offset
-      // and, for runs of order <= 4, kernels without the 6th-order path
-      const bool o4 = p.order_centered <= 4;
-      if (bx.m == 66 && bx.n == 66 && o4)
-        bssn_rhs_kernel<66, 66 * 66, 4><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx,
-                                                              L->dy, L->dz, L->d_status, k0, k1);
-      else if (bx.m == 66 && bx.n == 66)
-        bssn_rhs_kernel<66, 66 * 66><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy,
-                                                           L->dz, L->d_status, k0, k1);
-      else if (bx.m == 162 && bx.n == 162)
-        bssn_rhs_kernel<162, 162 * 162><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx,
-                                                              L->dy, L->dz, L->d_status, k0, k1);
-      else if (o4)
-        bssn_rhs_kernel<0, 0, 4><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy,
-                                                       L->dz, L->d_status, k0, k1);
-      else
-        bssn_rhs_kernel<<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
-                                             L->d_status, k0, k1);
+      // workloads (every stencil tap becomes one load with an immediate
+      // offset), one kernel per stencil order
+      const int ord = p.order_centered;
+#define NR_BSSN_LDG(CSY_, CSZ_, ORD_)                                                                    \
+  bssn_rhs_kernel<CSY_, CSZ_, ORD_><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, \
+                                                        L->dz, L->d_status, k0, k1)
+      if (bx.m == 66 && bx.n == 66 && ord == 4) NR_BSSN_LDG(66, 66 * 66, 4);
+      else if (bx.m == 66 && bx.n == 66 && ord == 6) NR_BSSN_LDG(66, 66 * 66, 6);
+      else if (bx.m == 162 && bx.n == 162 && ord == 6) NR_BSSN_LDG(162, 162 * 162, 6);
+      else if (ord == 2) NR_BSSN_LDG(0, 0, 2);
+      else if (ord == 4) NR_BSSN_LDG(0, 0, 4);
+      else NR_BSSN_LDG(0, 0, 6);
+#undef NR_BSSN_LDG
     }
+    // the ladder points of all boxes (beside the interior kernel)
+    const int nlad = L->nladder[p.order_centered / 2 - 1];
+    if (nlad > 0)
+      bssn_ladder_kernel<<<(nlad + 127) / 128, 128, 0, fork ? L->side : st>>>(
+          U, out, pre, acc, E, p, L->d_ladder, nlad, L->d_box, L->dx, L->dy, L->dz, L->d_status, kb, ke);
   }
   if (flagged && L->nflagpts > 0) {
     const int n = L->nflagpts * NRGPU_NV;
@@ -1555,23 +1587,40 @@ static ZCVarPtrs z4_c(const ZVarPtrs &v) {
 
 // FP64 interior launch with compile-time strides for the box sizes of the
 // workloads (66, 162, and the finer levels of the batched refinement step),
-// generic strides otherwise; MAXO = 4 for runs of order <= 4 leaves the
-// 6th-order path out of the kernel (fewer registers, less spilling)
-template <int MAXO>
+// generic strides otherwise; one kernel per stencil order
+template <int ORD>
 static void z4_interior_fp64(const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVarPtrs &pre, const ZVarPtrs &acc,
                              const Epilogue &E, const nrgpu_z4_params &p, const BoxGeo &bx, nrgpu_level *L, dim3 grd,
                              dim3 blk, cudaStream_t st) {
 #define NRGPU_Z4_FIXED(M_)                                                                                   \
   if (bx.m == M_ && bx.n == M_) {                                                                           \
-    z4_rhs_kernel<M_, M_ * M_, 0, MAXO><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, \
-                                                             L->dy, L->dz, L->d_status, 1, bx.o - 2);                    \
+    z4_rhs_kernel<M_, M_ * M_, 0, ORD><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, \
+                                                            L->dy, L->dz, L->d_status, 1, bx.o - 2);        \
     return;                                                                                                  \
   }
-  NRGPU_Z4_FIXED(162) NRGPU_Z4_FIXED(168) NRGPU_Z4_FIXED(136) NRGPU_Z4_FIXED(104) NRGPU_Z4_FIXED(72)
-  NRGPU_Z4_FIXED(66)
+  if constexpr (ORD >= 4) {
+    NRGPU_Z4_FIXED(162) NRGPU_Z4_FIXED(168) NRGPU_Z4_FIXED(136) NRGPU_Z4_FIXED(104) NRGPU_Z4_FIXED(72)
+    NRGPU_Z4_FIXED(66)
+  }
 #undef NRGPU_Z4_FIXED
-  z4_rhs_kernel<0, 0, 0, MAXO><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
-                                                    L->d_status, 1, bx.o - 2);
+  z4_rhs_kernel<0, 0, 0, ORD><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
+                                                   L->d_status, 1, bx.o - 2);
+}
+
+// the FP32-stencil options (precision 1, 2): the 162^3 box of the
+// precision sweep with compile-time strides, generic strides otherwise
+template <int PREC>
+static void z4_interior_prec(const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVarPtrs &pre, const ZVarPtrs &acc,
+                             const Epilogue &E, const nrgpu_z4_params &p, const BoxGeo &bx, nrgpu_level *L, dim3 grd,
+                             dim3 blk, cudaStream_t st) {
+#define NR_Z4P(CSY_, CSZ_, ORD_)                                                                               \
+  z4_rhs_kernel<CSY_, CSZ_, PREC, ORD_><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, \
+                                                             L->dy, L->dz, L->d_status, 1, bx.o - 2)
+  if (p.order_centered == 6 && bx.m == 162 && bx.n == 162) NR_Z4P(162, 162 * 162, 6);
+  else if (p.order_centered == 6) NR_Z4P(0, 0, 6);
+  else if (p.order_centered == 4) NR_Z4P(0, 0, 4);
+  else NR_Z4P(0, 0, 2);
+#undef NR_Z4P
 }
 
 static int z4_launch(nrgpu_level *L, const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVarPtrs &pre,
@@ -1593,25 +1642,24 @@ static int z4_launch(nrgpu_level *L, const ZCVarPtrs &U, const ZVarPtrs &out, co
       // measured fastest for this box); 128 or 256 threads, one point each
       const dim3 blk(L->blk[0], L->blk[1], L->blk[2]);
       const dim3 grd((bx.m - 2 + blk.x - 1) / blk.x, (bx.n - 2 + blk.y - 1) / blk.y, (bx.o - 2 + blk.z - 1) / blk.z);
-      if (p.precision == 1) {
-        if (bx.m == 162 && bx.n == 162)
-          z4_rhs_kernel<162, 162 * 162, 1><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx,
-                                                                 L->dy, L->dz, L->d_status, 1, bx.o - 2);
-        else
-          z4_rhs_kernel<0, 0, 1><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
-                                                       L->d_status, 1, bx.o - 2);
-      } else if (p.precision == 2) {
-        if (bx.m == 162 && bx.n == 162)
-          z4_rhs_kernel<162, 162 * 162, 2><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx,
-                                                                 L->dy, L->dz, L->d_status, 1, bx.o - 2);
-        else
-          z4_rhs_kernel<0, 0, 2><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
-                                                       L->d_status, 1, bx.o - 2);
-      } else if (p.order_centered <= 4) {
-        z4_interior_fp64<4>(U, out, pre, acc, E, p, bx, L, grd, blk, st);
-      } else {
-        z4_interior_fp64<6>(U, out, pre, acc, E, p, bx, L, grd, blk, st);
-      }
+      if (p.precision == 1) z4_interior_prec<1>(U, out, pre, acc, E, p, bx, L, grd, blk, st);
+      else if (p.precision == 2) z4_interior_prec<2>(U, out, pre, acc, E, p, bx, L, grd, blk, st);
+      else if (p.order_centered == 2) z4_interior_fp64<2>(U, out, pre, acc, E, p, bx, L, grd, blk, st);
+      else if (p.order_centered == 4) z4_interior_fp64<4>(U, out, pre, acc, E, p, bx, L, grd, blk, st);
+      else z4_interior_fp64<6>(U, out, pre, acc, E, p, bx, L, grd, blk, st);
+    }
+    // the ladder points of all boxes (beside the interior kernel)
+    const int nlad = L->nladder[p.order_centered / 2 - 1];
+    if (nlad > 0) {
+      const cudaStream_t ls = fork ? L->side : st;
+      const unsigned g = (unsigned)((nlad + 127) / 128);
+#define NR_Z4L(P_)                                                                                                   \
+  z4_ladder_kernel<P_><<<g, 128, 0, ls>>>(U, out, pre, acc, E, p, L->d_ladder, nlad, L->d_box, L->dx, L->dy, L->dz, \
+                                          L->d_status, 1, 1 << 30)
+      if (p.precision == 1) NR_Z4L(1);
+      else if (p.precision == 2) NR_Z4L(2);
+      else NR_Z4L(0);
+#undef NR_Z4L
     }
   }
   if (flagged && L->nflagpts > 0) {

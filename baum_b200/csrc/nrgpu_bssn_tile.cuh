@@ -9,7 +9,8 @@
 //   22 x 10 x 10 box (the tile and a halo of 3, enough for 4th-order centred
 //   and mixed derivatives, lopsided advection with a shift of 1 or 2 and
 //   KO6, and 6th-order centred stencils with the centred 6th-order
-//   advection) by a single TMA load into a ring of 12 slots of 17.25 KB
+//   advection; the points nearer the box faces take lower orders and are
+//   left to the ladder kernel) by a single TMA load into a ring of 12 slots of 17.25 KB
 //   (207 KB of shared memory, one block per SM).
 // * The 24 fields pass through the ring in two rounds, in the order the
 //   computation consumes them: round A = g~ (6), Gamma~ (3), chi, alpha, K;
@@ -501,8 +502,9 @@ __device__ __forceinline__ void tg_B(const double *sb, const AdvDir ad[3], const
 #undef NR_O2
 #undef NR_OOH
 
-// one block per tile (the tiles of planes k0..k1 of one box, x fastest)
-template <int MAXO>
+// one block per tile (the tiles of planes k0..k1 of one box, x fastest);
+// ORD: the run's stencil order, computed where it fits
+template <int ORD>
 __global__ void __launch_bounds__(kTileThreads, 1)
     bssn_rhs_tile_kernel(const __grid_constant__ BssnMaps maps, CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPtrs acc,
                          Epilogue E, const nrgpu_bssn_params p, BoxGeo box, const int *__restrict__ boundary,
@@ -568,23 +570,20 @@ __global__ void __launch_bounds__(kTileThreads, 1)
   const int imax = box.m - 1, jmax = box.n - 1, kmax = box.o - 1;
   int d = min(min(i, j), k);
   d = min(d, min(min(imax - i, jmax - j), kmax - k));
-  const int oc = ladder(p.order_centered, d);
-  if (act && (oc == 0 || oc != ladder(p.order_advection, d))) {
-    atomicOr(status + 1, 1);
-    act = false;
-  }
+  // points nearer the faces than the full stencil reaches: bssn_ladder_kernel
+  if (d < ORD / 2) act = false;
   const double h[3] = {dx, dy, dz};
   // lopsided advection directions at this point (shared-memory strides)
   AdvDir ad[3];
   double cw[3];
   if (act) {
-    const int lop = oc == 2 ? 0 : (oc == 6 ? p.advection_lopsided6 : p.advection_lopsided);
+    const int lop = ORD == 2 ? 0 : (ORD == 6 ? p.advection_lopsided6 : p.advection_lopsided);
     const int idx[3] = {i, j, k}, mx[3] = {imax, jmax, kmax};
-    const double oad = oc == 2 ? 0.5 : (oc == 4 ? 1.0 / 12.0 : 1.0 / 60.0);
+    const double oad = 1.0 / den1<ORD>();
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const double w = ldg(U.p[BETA1 + a] + ijk) / h[a];
-      ad[a] = adv_dir(idx[a], mx[a], w, oc, lop, tstr(a));
+      ad[a] = adv_dir(idx[a], mx[a], w, ORD, lop, tstr(a));
       const int ws = w < 0 ? -1 : (w > 0 ? 1 : 0);
       cw[a] = -ws * w * oad;
     }
@@ -593,11 +592,10 @@ __global__ void __launch_bounds__(kTileThreads, 1)
   const double *sb = tsm + (lx + kTH) + kTSY * (ly + kTH) + kTSZ * (lz + kTH);
   TileCarry T;
   double r[NRGPU_NV];
-#define NR_TILE_DISPATCH(call_)                                    \
-  if (act && ok) {                                                 \
-    if (oc == 2) { constexpr int O_ = 2; call_; }                  \
-    else if (oc == 4 || MAXO < 6) { constexpr int O_ = 4; call_; } \
-    else { constexpr int O_ = MAXO; call_; }                       \
+#define NR_TILE_DISPATCH(call_) \
+  if (act && ok) {              \
+    constexpr int O_ = ORD;     \
+    call_;                      \
   }
   // round A
   wait_full(SL_G, SL_G + 6, 0);

@@ -28,6 +28,11 @@ struct nrgpu_level {
   int *d_boundary;         // [npoints] flags on the device
   FlagPoint *d_flagpts;    // points with flag != 0
   int nflagpts;
+  // flag-0 points within 2 of a box face (the order ladder: lower-order
+  // stencils there), sorted by that distance d (FlagPoint.flag = d);
+  // nladder[d] = points with distance <= d
+  FlagPoint *d_ladder;
+  int nladder[3];
   BoxGeo *d_box;           // boxes on the device
   int *d_status;           // [0]: NaN flag, [1]: inner point without stencil room
   // RK4 scratch: three full 24-variable lists, allocated on first use

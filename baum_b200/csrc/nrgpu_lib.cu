@@ -1,4 +1,5 @@
 // nrgpu_lib.cu -- library state, errors, level mirrors and host-buffer calls.
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -89,6 +90,29 @@ extern "C" int nrgpu_level_create(const nrgpu_level_desc *d, nrgpu_level **out) 
           fl.push_back(FlagPoint{ijk, i, j, k, b, f});
         }
   }
+  // flag-0 points within 2 of their box's faces, by distance: the interior
+  // kernels compute the points where the full stencil order fits, a list
+  // kernel the others (boundaryNaway ladder, bam_amr_loops_box.h:215-220)
+  std::vector<FlagPoint> lad[3];
+  for (int b = 0; b < d->nboxes; ++b) {
+    const nrgpu_box &bx = d->box[b];
+    for (int k = 0; k < bx.o; ++k)
+      for (int j = 0; j < bx.n; ++j)
+        for (int i = 0; i < bx.m; ++i) {
+          const int dd = std::min(std::min(std::min(i, j), k), std::min(std::min(bx.m - 1 - i, bx.n - 1 - j),
+                                                                         bx.o - 1 - k));
+          if (dd > 2) continue;
+          const int ijk = bx.noffset + i + bx.m * (j + bx.n * k);
+          if (d->boundary[ijk] != 0) continue;
+          lad[dd].push_back(FlagPoint{ijk, i, j, k, b, dd});
+        }
+  }
+  std::vector<FlagPoint> ladder;
+  int nlad[3];
+  for (int q = 0; q < 3; ++q) {
+    ladder.insert(ladder.end(), lad[q].begin(), lad[q].end());
+    nlad[q] = (int)ladder.size();
+  }
   // symmetry ghosts: set_boundary_reflection_one (symmetry.c:28-82) copies the
   // nneg = (int)(1 - lo / h) planes below zero from planes 2 nneg - 1 - n, axis
   // after axis; the result is the mirror image with the product of parities
@@ -128,6 +152,7 @@ extern "C" int nrgpu_level_create(const nrgpu_level_desc *d, nrgpu_level **out) 
     L->hbox[b] = BoxGeo{d->box[b].m, d->box[b].n, d->box[b].o, d->box[b].noffset, d->box[b].x0, d->box[b].y0,
                         d->box[b].z0};
   L->nflagpts = (int)fl.size();
+  for (int q = 0; q < 3; ++q) L->nladder[q] = nlad[q];
   L->ninner = (long)d->npoints - (long)fl.size();
   L->blk[0] = 32; L->blk[1] = 4; L->blk[2] = 1;
   L->symmetry = d->symmetry;
@@ -136,6 +161,7 @@ extern "C" int nrgpu_level_create(const nrgpu_level_desc *d, nrgpu_level **out) 
             cudaMalloc(&L->d_box, sizeof(BoxGeo) * d->nboxes) == cudaSuccess &&
             cudaMalloc(&L->d_status, sizeof(int) * 4) == cudaSuccess &&
             (fl.empty() || cudaMalloc(&L->d_flagpts, sizeof(FlagPoint) * fl.size()) == cudaSuccess) &&
+            (ladder.empty() || cudaMalloc(&L->d_ladder, sizeof(FlagPoint) * ladder.size()) == cudaSuccess) &&
             (sym.empty() || cudaMalloc(&L->d_sym, sizeof(SymPoint) * sym.size()) == cudaSuccess);
   if (ok)
     ok = cudaMemcpy(L->d_boundary, d->boundary, sizeof(int) * d->npoints, cudaMemcpyHostToDevice) == cudaSuccess &&
@@ -143,6 +169,8 @@ extern "C" int nrgpu_level_create(const nrgpu_level_desc *d, nrgpu_level **out) 
          cudaMemset(L->d_status, 0, sizeof(int) * 4) == cudaSuccess &&
          (fl.empty() ||
           cudaMemcpy(L->d_flagpts, fl.data(), sizeof(FlagPoint) * fl.size(), cudaMemcpyHostToDevice) == cudaSuccess) &&
+         (ladder.empty() || cudaMemcpy(L->d_ladder, ladder.data(), sizeof(FlagPoint) * ladder.size(),
+                                       cudaMemcpyHostToDevice) == cudaSuccess) &&
          (sym.empty() ||
           cudaMemcpy(L->d_sym, sym.data(), sizeof(SymPoint) * sym.size(), cudaMemcpyHostToDevice) == cudaSuccess);
   if (!ok) {
@@ -159,6 +187,7 @@ extern "C" int nrgpu_level_destroy(nrgpu_level *L) {
   cudaFree(L->d_box);
   cudaFree(L->d_status);
   cudaFree(L->d_flagpts);
+  cudaFree(L->d_ladder);
   cudaFree(L->d_sym);
   cudaFree(L->rsym);
   cudaFree(L->scratch);

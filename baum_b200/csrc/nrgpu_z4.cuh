@@ -395,7 +395,7 @@ __device__ __forceinline__ void z4_store(const double r[ZNV], int x, const ZVarP
   }
 }
 
-template <int CSY = 0, int CSZ = 0, int PREC = 0, int MAXO = 6>
+template <int CSY = 0, int CSZ = 0, int PREC = 0, int ORD = 4>
 __global__ void __launch_bounds__(256, NRGPU_RHS_MINBLOCKS) z4_rhs_kernel(ZCVarPtrs U, ZVarPtrs out, ZCVarPtrs pre, ZVarPtrs acc, Epilogue E,
                                                     const nrgpu_z4_params p, BoxGeo box,
                                                     const int *__restrict__ boundary, double dx, double dy, double dz,
@@ -413,18 +413,45 @@ __global__ void __launch_bounds__(256, NRGPU_RHS_MINBLOCKS) z4_rhs_kernel(ZCVarP
   P.h[0] = dx; P.h[1] = dy; P.h[2] = dz;
   int d = min(min(i, j), k);
   d = min(d, min(min(P.imax - i, P.jmax - j), P.kmax - k));
+  // the points of the order ladder are z4_ladder_kernel's
+  if (d < ORD / 2) return;
   P.dist = d;
-  const int oc = ladder(p.order_centered, d);
-  if (oc == 0 || oc != ladder(p.order_advection, d)) {
+  double r[ZNV];
+  z4_point<ORD, CSY, CSZ, PREC>(U, P, p, r);
+  double s = 0.0;
+#pragma unroll
+  for (int v = 0; v < ZNV; ++v) s += r[v];
+  if (!isfinite(s)) atomicOr(status, 1);
+  z4_store(r, P.ijk, out, pre, acc, E, p);
+}
+
+// the order-ladder points of a level (see bssn_ladder_kernel)
+template <int PREC>
+__global__ void z4_ladder_kernel(ZCVarPtrs U, ZVarPtrs out, ZCVarPtrs pre, ZVarPtrs acc, Epilogue E,
+                                 const nrgpu_z4_params p, const FlagPoint *__restrict__ pts, int n,
+                                 const BoxGeo *__restrict__ boxes, double dx, double dy, double dz, int *status,
+                                 int k0, int k1) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const FlagPoint fp = pts[t];
+  if (fp.k < k0 || fp.k > k1) return;
+  const BoxGeo b = boxes[fp.box];
+  PointCtx P;
+  P.i = fp.i; P.j = fp.j; P.k = fp.k;
+  P.imax = b.m - 1; P.jmax = b.n - 1; P.kmax = b.o - 1;
+  P.st[0] = 1; P.st[1] = b.m; P.st[2] = b.m * b.n;
+  P.ijk = fp.ijk;
+  P.h[0] = dx; P.h[1] = dy; P.h[2] = dz;
+  P.dist = fp.flag;
+  const int oc = ladder(p.order_centered, P.dist);
+  if (oc == 0 || oc != ladder(p.order_advection, P.dist)) {
     atomicOr(status + 1, 1);
     return;
   }
+  if (oc == p.order_centered) return;
   double r[ZNV];
-  // MAXO = 4 leaves the 6th-order path out of kernels for 4th-order runs
-  // (the ladder never asks for more than the requested order)
-  if (oc == 4 || (MAXO < 6 && oc == 6)) z4_point<4, CSY, CSZ, PREC>(U, P, p, r);
-  else if (oc == 2) z4_point<2, CSY, CSZ, PREC>(U, P, p, r);
-  else z4_point<MAXO, CSY, CSZ, PREC>(U, P, p, r);
+  if (oc == 2) z4_point<2, 0, 0, PREC>(U, P, p, r);
+  else z4_point<4, 0, 0, PREC>(U, P, p, r);
   double s = 0.0;
 #pragma unroll
   for (int v = 0; v < ZNV; ++v) s += r[v];

@@ -61,19 +61,32 @@ def sample_points(npoints, n, seed):
     return np.sort(rng.choice(npoints, size=min(n, npoints), replace=False)).astype(np.int64)
 
 
+# Tolerance of a refinement level's state against the oracle, relative to
+# each field's size: 2e-11 on level 0 (the pin of the 3-level runs against
+# the reference), 4x per finer level.  The device and the oracle add the
+# stencil terms in different orders; the rounding of a second difference of
+# a field of unit background (g~, chi, alpha) is ~eps sum|w| |u| / dx^2, 4x
+# per level, and reaches the fields of size 1e-3 through the rhs.  Measured
+# on the 7-level grid after one coarse step: 6.5e-13 on level 0, 8e-10 on
+# level 6 (Khat: 6e-13 absolute).
+def level_tolerance(level):
+    return 2e-11 * 4.0 ** level
+
+
 def stored_state_deviation(u, fixture):
-    """Largest deviation of device states u (one (nvars, npoints) tensor per
-    level) from a stored state (tests/golden/make_fmr_c3_fixture.py): at the
-    sampled points relative to each field's size (its largest |u| over the
-    level), and of the per-variable sums relative to the sums of |u|."""
+    """Deviation of device states u (one (nvars, npoints) tensor per level)
+    from a stored state (tests/golden/make_fmr_c3_fixture.py), per level: at
+    the sampled points relative to each field's size (its largest |u| over
+    the level), and of the per-variable sums relative to the sums of |u|.
+    Returns two lists, one entry per level."""
     import torch
     g = np.load(fixture)
-    e_pts, e_sum = 0.0, 0.0
+    e_pts, e_sum = [], []
     for l in range(len(g["sizes"])):
         idx = torch.from_numpy(g["idx_l%d" % l]).to(u[l].device)
         a = u[l][:, idx].cpu().numpy()
         b = g["u_l%d" % l]
-        e_pts = max(e_pts, float((np.abs(a - b).max(axis=1) / np.maximum(g["max_l%d" % l], 1e-8)).max()))
+        e_pts.append(float((np.abs(a - b).max(axis=1) / np.maximum(g["max_l%d" % l], 1e-8)).max()))
         s = u[l].sum(dim=1).cpu().numpy()
-        e_sum = max(e_sum, float((np.abs(s - g["sum_l%d" % l]) / g["abssum_l%d" % l]).max()))
+        e_sum.append(float((np.abs(s - g["sum_l%d" % l]) / g["abssum_l%d" % l]).max()))
     return e_pts, e_sum

@@ -12,6 +12,9 @@ compared with the oracle at reduced size (the same uneven pattern of
 levels, every level stepped 2^l times per coarse step, restriction,
 prolongation and time interpolation in between), and at its full size
 through the stored oracle state that the benchmark also reports against.
+The refinement levels are held to workloads.level_tolerance(l): 2e-11 of
+each field's size on level 0, 4x per finer level, the growth of the
+rounding of second differences with 1/dx^2.
 """
 import os
 
@@ -20,7 +23,6 @@ import pytest
 import torch
 
 from conftest import GOLDEN, relerr
-from test_fmr_oracle_pin import FMR_TOL
 from baum_b200 import abi, fmr, punctures, workloads, z4
 from oracle import oracle
 
@@ -82,7 +84,7 @@ def test_seven_level_grid_matches_oracle(gpu):
     st.advance(2)
     for l in range(7):
         err = np.abs(got[l] - st.u[l]).max(axis=1) / np.maximum(np.abs(st.u[l]).max(axis=1), 1e-8)
-        assert err.max() < FMR_TOL, (l, err.max())
+        assert err.max() < workloads.level_tolerance(l), (l, err.max())
 
 
 def test_benchmarked_seven_level_grid_matches_stored_oracle_state(gpu):
@@ -94,4 +96,5 @@ def test_benchmarked_seven_level_grid_matches_stored_oracle_state(gpu):
     torch.cuda.synchronize()
     H.close()
     e_pts, e_sum = workloads.stored_state_deviation(u, fixture)
-    assert e_pts < FMR_TOL and e_sum < 1e-12, (e_pts, e_sum)
+    for l in range(7):
+        assert e_pts[l] < workloads.level_tolerance(l) and e_sum[l] < 1e-12, (l, e_pts, e_sum)
