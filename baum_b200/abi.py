@@ -321,6 +321,7 @@ def lib():
         "nrgpu_mg_create": (C.c_int, [C.c_int, C.c_double, C.POINTER(MgParams), C.POINTER(vp)]),
         "nrgpu_mg_destroy": (C.c_int, [vp]),
         "nrgpu_mg_solve": (C.c_int, [vp, vp, vp, vp, C.POINTER(C.c_int), C.POINTER(C.c_double), vp]),
+        "nrgpu_mg_smooth": (C.c_int, [vp, vp, vp, vp, C.c_int, C.c_double, vp]),
         "nrgpu_to_adm": (C.c_int, [vp, pp, pp, C.c_double, vp]),
         "nrgpu_adm_constraints": (C.c_int, [vp, pp, pp, C.c_int, C.c_int, vp]),
         "nrgpu_norms": (C.c_int, [vp, pp, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), vp]),
@@ -337,6 +338,7 @@ def lib():
         "nrgpu_mlp_gradients": (C.c_int, [vp, C.POINTER(C.c_float), C.c_int]),
         "nrgpu_mlp_forward": (C.c_int, [vp, C.c_int, vp, vp]),
         "nrgpu_mlp_predict_u": (C.c_int, [vp, C.POINTER(C.c_double), C.c_int, C.c_double, C.c_double, vp, vp]),
+        "nrgpu_mlp_predict_u_fp32": (C.c_int, [vp, C.POINTER(C.c_double), C.c_int, C.c_double, C.c_double, vp, vp]),
         "nrgpu_fmr_params_default": (C.c_int, [C.POINTER(FmrParams)]),
         "nrgpu_fmr_create": (C.c_int, [C.c_int, C.POINTER(LevelDesc), C.POINTER(C.c_double), vp,
                                        C.POINTER(FmrParams), C.POINTER(vp)]),

@@ -76,12 +76,12 @@ class DeviceLevel:
         return tuple(b)
 
     def tile(self, on=-1):
-        """The staged-tile (TMA) interior rhs: on = 1 / 0 sets it, -1 only
-        queries; returns the setting."""
+        """The staged-tile (TMA) interior rhs: on = 1 (a block per tile), 2
+        (persistent), 0 (off); -1 only queries; returns the setting."""
         r = abi.lib().nrgpu_level_tile(self.handle, int(on))
         if r < 0:
             abi.check(r)
-        return bool(r)
+        return int(r)
 
     def nan_flag(self):
         f = C.c_int()

@@ -979,20 +979,29 @@ static int launch_bssn_tile(nrgpu_level *L, int b, const CUtensorMap *maps, cons
   BssnMaps M;
   memcpy(M.m, maps, sizeof M.m);
   const int ntiles = ((bx.m - 2 + kTX - 1) / kTX) * ((bx.n - 2 + kTY - 1) / kTY) * ((k1 - k0 + kTZ) / kTZ);
-  static std::once_flag attr4, attr6;
+  // L->tile 1: one block per tile; 2: the persistent form, one block per SM
+  const bool pers = L->tile == 2;
+  const int grid = pers ? (ntiles < L->nsm ? ntiles : L->nsm) : ntiles;
+  static std::once_flag attr;
+  std::call_once(attr, [] {
+    cudaFuncSetAttribute(bssn_rhs_tile_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem);
+    cudaFuncSetAttribute(bssn_rhs_tile_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem);
+    cudaFuncSetAttribute(bssn_rhs_tile_persistent_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kTileSmem);
+    cudaFuncSetAttribute(bssn_rhs_tile_persistent_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kTileSmem);
+  });
+#define NR_TILE_LAUNCH(K_)                                                                                     \
+  K_<<<grid, kTileThreads, kTileSmem, st>>>(M, U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz, \
+                                            L->d_status, k0, k1)
   if (p.order_centered <= 4) {
-    std::call_once(attr4, [] {
-      cudaFuncSetAttribute(bssn_rhs_tile_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem);
-    });
-    bssn_rhs_tile_kernel<4><<<ntiles, kTileThreads, kTileSmem, st>>>(M, U, out, pre, acc, E, p, bx, L->d_boundary,
-                                                                      L->dx, L->dy, L->dz, L->d_status, k0, k1);
+    if (pers) NR_TILE_LAUNCH(bssn_rhs_tile_persistent_kernel<4>);
+    else NR_TILE_LAUNCH(bssn_rhs_tile_kernel<4>);
   } else {
-    std::call_once(attr6, [] {
-      cudaFuncSetAttribute(bssn_rhs_tile_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem);
-    });
-    bssn_rhs_tile_kernel<6><<<ntiles, kTileThreads, kTileSmem, st>>>(M, U, out, pre, acc, E, p, bx, L->d_boundary,
-                                                                      L->dx, L->dy, L->dz, L->d_status, k0, k1);
+    if (pers) NR_TILE_LAUNCH(bssn_rhs_tile_persistent_kernel<6>);
+    else NR_TILE_LAUNCH(bssn_rhs_tile_kernel<6>);
   }
+#undef NR_TILE_LAUNCH
   return NRGPU_OK;
 }
 
@@ -1861,8 +1870,9 @@ extern "C" int nrgpu_level_autotune(nrgpu_level *L, int system, const void *para
     for (int b = 0; b < L->nboxes; ++b)
       elig = elig && tile_eligible(L, b, P.p, NRGPU_NV, bp.order_centered, bp.advection_lopsided,
                                    bp.advection_lopsided6);
-    if (elig) {
-      L->tile = 1;
+    int pick = 0;
+    for (int mode = 1; mode <= 2 && elig && !e; ++mode) {
+      L->tile = mode;
       for (int rep = 0; rep < 4 && !e; ++rep) {
         if (rep == 1) cudaEventRecord(ev0, st);
         e = launch_rhs(L, cptrs(P), O, cptrs(P), O, E, bp, st, true, false);
@@ -1871,8 +1881,12 @@ extern "C" int nrgpu_level_autotune(nrgpu_level *L, int system, const void *para
       cudaEventSynchronize(ev1);
       float ms = 0;
       cudaEventElapsedTime(&ms, ev0, ev1);
-      L->tile = !e && ms < best;
+      if (!e && ms < best) {
+        best = ms;
+        pick = mode;
+      }
     }
+    L->tile = pick;
   }
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
@@ -1894,7 +1908,8 @@ extern "C" int nrgpu_level_block(nrgpu_level *L, int bx, int by, int bz) {
 
 extern "C" int nrgpu_level_tile(nrgpu_level *L, int on) {
   if (!L) return nrgpu_set_error(NRGPU_ERR_ARG, "null level");
-  if (on >= 0) L->tile = on ? 1 : 0;
+  if (on > 2) return nrgpu_set_error(NRGPU_ERR_ARG, "staged-tile mode %d (0, 1, 2)", on);
+  if (on >= 0) L->tile = on;
   return L->tile;
 }
 

@@ -631,3 +631,136 @@ __global__ void __launch_bounds__(kTileThreads, 1)
   if (tid == 0)
     for (int s = 0; s < kNSlot; ++s) tma::mbar_wait(&full[s], (roundB >> s) & 1u);
 }
+
+// the persistent form: one block per SM computes tiles b, b + gridDim.x,
+// ...; the next tile's round A is loaded while this tile's round B is
+// consumed.  The grid spacing passes through an empty asm each tile so
+// that the compiler recomputes the stencil weights instead of keeping them
+// live across the whole loop.
+template <int ORD>
+__global__ void __launch_bounds__(kTileThreads, 1)
+    bssn_rhs_tile_persistent_kernel(const __grid_constant__ BssnMaps maps, CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPtrs acc,
+                         Epilogue E, const nrgpu_bssn_params p, BoxGeo box, const int *__restrict__ boundary,
+                         double dx, double dy, double dz, int *status, int k0, int k1) {
+  extern __shared__ __align__(128) double tsm_raw[];
+  double *tsm = tsm_raw + ((128 - (tma::smem_addr(tsm_raw) & 127)) & 127) / 8;
+  uint64_t *full = reinterpret_cast<uint64_t *>(tsm + kNSlot * kSlot);
+  uint64_t *empty = full + kNSlot;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int lx = tid % kTX, ly = (tid / kTX) % kTY, lz = tid / (kTX * kTY);
+  const int ntx = (box.m - 2 + kTX - 1) / kTX, nty = (box.n - 2 + kTY - 1) / kTY;
+  const int ntiles = ntx * nty * ((k1 - k0 + kTZ) / kTZ);
+  bool ok = true;
+  unsigned last = 0;   // thread 0: parity of the last load issued into each slot
+  auto issue = [&](int s, int f, int tt) {
+    const int tx = tt % ntx, rr = tt / ntx, ty = rr % nty, tz = rr / nty;
+    tma::mbar_arrive_expect_tx(&full[s], kTileBoxBytes);
+    tma::load_3d(tsm + s * kSlot, &maps.m[f], kTX * tx - 2, kTY * ty - 2, k0 + kTZ * tz - kTH, &full[s]);
+  };
+  if (tid == 0) {
+    for (int s = 0; s < kNSlot; ++s) {
+      tma::mbar_init(&full[s], 1);
+      tma::mbar_init(&empty[s], kTileThreads / 32);
+    }
+    tma::mbar_fence_init();
+    if ((int)blockIdx.x < ntiles)
+      for (int s = 0; s < kNSlot; ++s) issue(s, kRoundA[s], blockIdx.x);
+  }
+  __syncthreads();
+  auto wait_full = [&](int s0, int s1, unsigned par) {
+    for (int s = s0; s < s1; ++s)
+      if (ok && !tma::mbar_wait(&full[s], par)) {
+        ok = false;
+        atomicOr(status, 2);
+      }
+  };
+  // all warps done with slots s0..s1-1 (phase par): thread 0 loads the
+  // next fields into them (round B of this tile, or round A of tile tt)
+  auto release_refill = [&](int s0, int s1, unsigned par, bool roundB, int tt) {
+    __syncwarp();
+    if (lane == 0)
+      for (int s = s0; s < s1; ++s) tma::mbar_arrive(&empty[s]);
+    if (tid == 0 && tt < ntiles)
+      for (int s = s0; s < s1; ++s) {
+        if (ok && !tma::mbar_wait(&empty[s], par)) {
+          ok = false;
+          atomicOr(status, 2);
+        }
+        if (ok) {
+          issue(s, roundB ? kRoundB[s] : kRoundA[s], tt);
+          last ^= 1u << s;
+        }
+      }
+    __syncwarp();
+  };
+  const int co = (lx + kTH) + kTSY * (ly + kTH) + kTSZ * (lz + kTH);
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int tn = t + gridDim.x;
+    const int tx = t % ntx, rr = t / ntx, ty = rr % nty, tz = rr / nty;
+    const int i = 1 + kTX * tx + lx, j = 1 + kTY * ty + ly, k = k0 + kTZ * tz + lz;
+    const int ijk = box.noffset + i + box.m * (j + box.n * k);
+    bool act = i <= box.m - 2 && j <= box.n - 2 && k <= k1;
+    if (act && __ldg(boundary + ijk) != 0) act = false;
+    const int imax = box.m - 1, jmax = box.n - 1, kmax = box.o - 1;
+    int d = min(min(i, j), k);
+    d = min(d, min(min(imax - i, jmax - j), kmax - k));
+    if (d < ORD / 2) act = false;
+    double h[3] = {dx, dy, dz};
+    asm volatile("" : "+d"(h[0]), "+d"(h[1]), "+d"(h[2]));
+    AdvDir ad[3];
+    double cw[3];
+    if (act) {
+      const int lop = ORD == 2 ? 0 : (ORD == 6 ? p.advection_lopsided6 : p.advection_lopsided);
+      const int idx[3] = {i, j, k}, mx[3] = {imax, jmax, kmax};
+      const double oad = 1.0 / den1<ORD>();
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const double w = ldg(U.p[BETA1 + a] + ijk) / h[a];
+        ad[a] = adv_dir(idx[a], mx[a], w, ORD, lop, tstr(a));
+        const int ws = w < 0 ? -1 : (w > 0 ? 1 : 0);
+        cw[a] = -ws * w * oad;
+      }
+    }
+    const bool with_ko = (p.order_dissipation == 4 && d >= 2) || (p.order_dissipation == 6 && d >= 3);
+    const double *sb = tsm + co;
+    TileCarry T;
+    double r[NRGPU_NV];
+#define NR_TILE_DISPATCH(call_) \
+  if (act && ok) {              \
+    constexpr int O_ = ORD;     \
+    call_;                      \
+  }
+    wait_full(SL_G, SL_G + 6, 0);
+    NR_TILE_DISPATCH(tg_metric<O_>(sb, T, h, ad, cw, p, with_ko));
+    release_refill(SL_G, SL_G + 6, 0, true, t);
+    wait_full(SL_GA, SL_GA + 3, 0);
+    NR_TILE_DISPATCH(tg_gamma<O_>(sb, T, h, ad, cw, p, with_ko));
+    wait_full(SL_CHI, SL_CHI + 1, 0);
+    NR_TILE_DISPATCH(tg_chi<O_>(sb, T, h, ad, cw, p, with_ko));
+    wait_full(SL_ALPHA, SL_ALPHA + 1, 0);
+    NR_TILE_DISPATCH(tg_alpha<O_>(sb, T, h, ad, cw));
+    wait_full(SL_K, SL_K + 1, 0);
+    NR_TILE_DISPATCH(tg_K<O_>(sb, T, h, ad, cw, p, with_ko));
+    release_refill(SL_GA, kNSlot, 0, true, t);
+    if (act && ok) tg_algebra(T, p, U, ijk, r);
+    wait_full(SL_BETA, SL_BETA + 3, 1);
+    NR_TILE_DISPATCH(tg_shift<O_>(sb, T, h, ad, cw, p, U, ijk, r));
+    release_refill(SL_BETA, SL_BETA + 3, 1, false, tn);
+    wait_full(SL_A, SL_A + 6, 1);
+    NR_TILE_DISPATCH(tg_A<O_>(sb, T, h, ad, cw, p, with_ko, r));
+    release_refill(SL_A, SL_A + 6, 1, false, tn);
+    wait_full(SL_B, SL_B + 3, 1);
+    NR_TILE_DISPATCH(tg_B<O_>(sb, ad, cw, p, r));
+    release_refill(SL_B, kNSlot, 1, false, tn);
+#undef NR_TILE_DISPATCH
+    if (act && ok) {
+      double s = 0.0;
+#pragma unroll
+      for (int v = 0; v < NRGPU_NV; ++v) s += r[v];
+      if (!isfinite(s)) atomicOr(status, 1);
+      store(r, ijk, out, pre, acc, E, p);
+    }
+  }
+  if (tid == 0)
+    for (int s = 0; s < kNSlot; ++s) tma::mbar_wait(&full[s], ((last >> s) & 1u));
+}

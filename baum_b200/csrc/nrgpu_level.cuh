@@ -65,6 +65,7 @@ struct nrgpu_level {
   // of recently used variable lists (host memory, first use)
   int tile;
   void *tma_cache;
+  int nsm;   // multiprocessors of the level's device
 };
 
 // library-internal pieces shared by the entry points and the mesh-refinement

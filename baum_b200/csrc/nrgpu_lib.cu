@@ -155,6 +155,8 @@ extern "C" int nrgpu_level_create(const nrgpu_level_desc *d, nrgpu_level **out) 
   for (int q = 0; q < 3; ++q) L->nladder[q] = nlad[q];
   L->ninner = (long)d->npoints - (long)fl.size();
   L->blk[0] = 32; L->blk[1] = 4; L->blk[2] = 1;
+  if (cudaDeviceGetAttribute(&L->nsm, cudaDevAttrMultiProcessorCount, L->device) != cudaSuccess || L->nsm < 1)
+    L->nsm = 148;
   L->symmetry = d->symmetry;
   L->nsym = (int)sym.size();
   bool ok = cudaMalloc(&L->d_boundary, sizeof(int) * d->npoints) == cudaSuccess &&

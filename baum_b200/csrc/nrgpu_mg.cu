@@ -151,6 +151,24 @@ __global__ void jacobi_kernel(const double *__restrict__ uo, double *__restrict_
   jacobi_at(blockIdx.x * blockDim.x + threadIdx.x, uo, un, f, a, b, m, cx, R);
 }
 
+// a damped Jacobi sweep un = uo + omega (f - L uo)/L_ii with the Robin
+// condition fused in: the smoothing of an initial guess before the V cycles
+// (nrgpu_mg_smooth; no counterpart in the reference, whose sweeps are
+// undamped)
+__global__ void damped_jacobi_kernel(const double *__restrict__ uo, double *__restrict__ un,
+                                     const double *__restrict__ f, const double *__restrict__ a,
+                                     const double *__restrict__ b, int m, double cx, double omega, RobinFuse R) {
+  int q, slot;
+  if (!fused_point(blockIdx.x * blockDim.x + threadIdx.x, m * m * m, R, q, slot)) return;
+  const int i = q % m, j = (q / m) % m, k = q / (m * m);
+  if (!inner(i, j, k, m)) return;
+  const double cc = -2.0 * (cx + cx + cx);
+  const double aq = a[q], bq = b[q], uq = uo[q];
+  const double lu = lop_point(uo, q, m, cc, cx, aq, bq);
+  const double lii = cc - 7.0 * bq * aq * inv_pow8(1.0 + aq * (1.0 + uq));
+  fused_store(un, q, slot, uq + omega * ((f[q] - lu) / lii), R);
+}
+
 // block partial sums of (L u - f)^2 over inner points
 __global__ void residual_partial_kernel(const double *__restrict__ u, const double *__restrict__ f,
                                         const double *__restrict__ a, const double *__restrict__ b, int m,
@@ -941,6 +959,28 @@ extern "C" int nrgpu_mg_solve(nrgpu_mg *M, const double *a, const double *b, dou
   NRGPU_CUDA_TRY(cudaGetLastError());
   // like the reference, running out of V cycles is not an error: the caller
   // sees ncycles == vcycle_nmax and normres > tol
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_mg_smooth(nrgpu_mg *M, const double *a, const double *b, double *u, int nsweeps, double omega,
+                               void *stream) {
+  if (!M || !a || !b || !u || nsweeps < 0 || !(omega > 0.0 && omega <= 1.0))
+    return nrgpu_set_error(NRGPU_ERR_ARG, "bad smoothing arguments (nsweeps >= 0, 0 < omega <= 1)");
+  NRGPU_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  MgLevel &T = M->lv[M->nl - 1];
+  const size_t by = sizeof(double) * T.np;
+  NRGPU_CUDA_TRY(cudaMemcpyAsync(T.u, u, by, cudaMemcpyDeviceToDevice, M->stream));
+  NRGPU_CUDA_TRY(cudaMemcpyAsync(T.a, a, by, cudaMemcpyDeviceToDevice, M->stream));
+  NRGPU_CUDA_TRY(cudaMemcpyAsync(T.b, b, by, cudaMemcpyDeviceToDevice, M->stream));
+  NRGPU_CUDA_TRY(cudaMemsetAsync(T.f, 0, by, M->stream));
+  for (int s = 0; s < nsweeps; ++s) {
+    damped_jacobi_kernel<<<nblk(T.np + T.nb), RB, 0, M->stream>>>(T.u, T.u2, T.f, T.a, T.b, T.m, cxof(T), omega,
+                                                                   robin_of(T, 0));
+    std::swap(T.u, T.u2);
+  }
+  NRGPU_CUDA_TRY(cudaMemcpyAsync(u, T.u, by, cudaMemcpyDeviceToDevice, M->stream));
+  NRGPU_CUDA_TRY(cudaStreamSynchronize(M->stream));
+  NRGPU_CUDA_TRY(cudaGetLastError());
   return NRGPU_OK;
 }
 

@@ -298,6 +298,94 @@ __global__ void refresh_bf16_kernel(const float *__restrict__ P, __nv_bfloat16 *
   Wb[i] = __float2bfloat16_rn(P[off_w(l) + q]);
 }
 
+// ---- FP32 inference (CUDA cores) ------------------------------------------------
+// The whole forward pass for 32 grid points per block, in FP32 from the FP32
+// master weights: features rounded to FP32 only (not BF16), hidden products
+// as a 32 x 128 x K register-tiled SIMT product (thread: 2 rows x 8
+// columns), bias + SiLU, the output layer by a warp reduction; u = s out.
+// Used to evaluate the trained network without the BF16 rounding of the
+// training path (whose grid-scale noise the undamped Jacobi smoother of the
+// multigrid does not remove).
+constexpr int kFR = 32;   // rows (grid points) per block
+__global__ void __launch_bounds__(256) mlp_forward_fp32_kernel(const double *__restrict__ cond, int m, double dx,
+                                                               const float *__restrict__ P, double s, double *u,
+                                                               long np) {
+  __shared__ float act[2][kFR][HID];
+  const int t = threadIdx.x;
+  const long first = (long)blockIdx.x * kFR;
+  // features of the block's rows (the formulas of mlp_features_kernel)
+  if (t < kFR) {
+    float *f = act[0][t];
+    const long p = min(first + t, np - 1);
+    const double h0 = -0.5 * (m - 1) * dx;
+    const int i = (int)(p % m), j = (int)((p / m) % m), k = (int)(p / ((long)m * m));
+    const double x[3] = {h0 + i * dx, h0 + j * dx, h0 + k * dx};
+    const double sc = 1.0 / 8.0;
+    f[0] = (float)(x[0] * sc);
+    f[1] = (float)(x[1] * sc);
+    f[2] = (float)(x[2] * sc);
+    for (int q = 0; q < 2; ++q) {
+      const double mq = cond[q];
+      const double d0 = x[0] - cond[2 + 3 * q], d1 = x[1] - cond[3 + 3 * q], d2 = x[2] - cond[4 + 3 * q];
+      const double rr = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+      float *g = f + 3 + 12 * q;
+      g[0] = (float)(d0 * sc);
+      g[1] = (float)(d1 * sc);
+      g[2] = (float)(d2 * sc);
+      g[3] = (float)(rr * sc);
+      g[4] = (float)(mq / (rr + mq));
+      g[5] = (float)(2.0 * mq);
+      for (int a = 0; a < 3; ++a) {
+        g[6 + a] = (float)(5.0 * cond[8 + 3 * q + a]);
+        g[9 + a] = (float)(5.0 * cond[14 + 3 * q + a]);
+      }
+    }
+    for (int q = 27; q < IN; ++q) f[q] = 0.0f;
+  }
+  __syncthreads();
+  const int cg = t % 16, rg = t / 16;   // columns 8 cg .. 8 cg + 7, rows 2 rg, 2 rg + 1
+  int cur = 0;
+  for (int l = 0; l < 4; ++l) {
+    const int K = fan_in(l);
+    const float *W = P + off_w(l), *bias = P + off_b(l);
+    float acc[2][8];
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+      for (int c = 0; c < 8; ++c) acc[r][c] = 0.0f;
+    for (int k = 0; k < K; ++k) {
+      float w[8], a[2];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) w[c] = __ldg(W + (long)k * HID + 8 * cg + c);
+#pragma unroll
+      for (int r = 0; r < 2; ++r) a[r] = act[cur][2 * rg + r][k];
+#pragma unroll
+      for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int c = 0; c < 8; ++c) acc[r][c] = fmaf(a[r], w[c], acc[r][c]);
+    }
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const float z = acc[r][c] + __ldg(bias + 8 * cg + c);
+        act[cur ^ 1][2 * rg + r][8 * cg + c] = z * sigm(z);
+      }
+    __syncthreads();
+    cur ^= 1;
+  }
+  // out = A4 w5 + b5: warp w reduces rows 4 w .. 4 w + 3
+  const int w = t >> 5, lane = t & 31;
+  const float *w5 = P + kOffW5;
+  for (int r = 4 * w; r < 4 * w + 4; ++r) {
+    float v = 0.0f;
+    for (int k = lane; k < HID; k += 32) v = fmaf(act[cur][r][k], __ldg(w5 + k), v);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0 && first + r < np) u[first + r] = s * (double)(v + __ldg(w5 + HID));
+  }
+}
+
 __global__ void scale_to_u_kernel(const float *__restrict__ o, double s, double *u, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) u[i] = s * (double)o[i];
@@ -555,5 +643,18 @@ extern "C" int nrgpu_mlp_predict_u(nrgpu_mlp *M, const double *host_cond, int m,
     scale_to_u_kernel<<<nb(n), 256, 0, st>>>(M->out, uscale, u + first, n);
     NRGPU_CUDA_TRY(cudaGetLastError());
   }
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_mlp_predict_u_fp32(nrgpu_mlp *M, const double *host_cond, int m, double dx, double uscale,
+                                        double *u, void *stream) {
+  if (!M || !host_cond || !u || m < 2) return nrgpu_set_error(NRGPU_ERR_ARG, "bad prediction arguments");
+  const cudaStream_t st = (cudaStream_t)stream;
+  NRGPU_CUDA_TRY(cudaStreamSynchronize(st));  // the table is replaced below
+  int e = set_cond(M, host_cond, 1);
+  if (e) return e;
+  const long np = (long)m * m * m;
+  mlp_forward_fp32_kernel<<<(unsigned)((np + kFR - 1) / kFR), 256, 0, st>>>(M->cond, m, dx, M->P, uscale, u, np);
+  NRGPU_CUDA_TRY(cudaGetLastError());
   return NRGPU_OK;
 }

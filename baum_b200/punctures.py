@@ -109,6 +109,15 @@ class Multigrid:
                                            C.c_void_p(u.data_ptr()), C.byref(nc), C.byref(res), s))
         return nc.value, res.value
 
+    def smooth(self, a, b, u, nsweeps, omega=2.0 / 3.0, stream=None):
+        """nsweeps damped Jacobi sweeps of the puncture equation on u (in
+        place), each with the Robin condition: smoothing of a guess."""
+        import ctypes as C
+        import torch
+        s = C.c_void_p((stream or torch.cuda.current_stream()).cuda_stream)
+        abi.check(abi.lib().nrgpu_mg_smooth(self.handle, C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()),
+                                            C.c_void_p(u.data_ptr()), int(nsweeps), float(omega), s))
+
     def close(self):
         if self.handle:
             abi.lib().nrgpu_mg_destroy(self.handle)

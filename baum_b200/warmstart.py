@@ -30,7 +30,10 @@ from .punctures import Binary, Multigrid
 
 WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "warmstart_c2.npz")
 USCALE = 0.1
-C2_M, C2_DX = 130, 0.125   # nxyz = 128 inner + Robin layer, x in [-8.06, 8.06]
+C2_M, C2_DX = 130, 0.25    # nxyz = 128 inner + Robin layer, x in [-16.1, 16.1]
+# smoothing of the network's guess before the V cycles: damped Jacobi
+# sweeps (the solver itself, undamped Jacobi in FAS V cycles, is unchanged)
+NSMOOTH, OMEGA = 8, 2.0 / 3.0
 
 
 def cond_vector(b):
@@ -107,6 +110,16 @@ class Network:
         abi.check(abi.lib().nrgpu_mlp_predict_u(self.handle, cv.ctypes.data_as(C.POINTER(C.c_double)), int(m),
                                                 float(dx), float(self.uscale), C.c_void_p(u.data_ptr()),
                                                 _stream()))
+        return u
+
+    def predict_u_fp32(self, binary, m, dx, out=None):
+        """The same prediction in FP32 from the FP32 master weights (no BF16
+        rounding of features or activations)."""
+        cv = cond_vector(binary)
+        u = torch.empty(m ** 3, dtype=torch.float64, device="cuda") if out is None else out
+        abi.check(abi.lib().nrgpu_mlp_predict_u_fp32(self.handle, cv.ctypes.data_as(C.POINTER(C.c_double)), int(m),
+                                                     float(dx), float(self.uscale), C.c_void_p(u.data_ptr()),
+                                                     _stream()))
         return u
 
     def save(self, path, **meta):
@@ -224,30 +237,55 @@ def train(net, data, m=C2_M, dx=C2_DX, epochs=12, batch=16384, lr0=2e-3, lr1=2e-
     return hist
 
 
-def evaluate(net, binaries, m=C2_M, dx=C2_DX, nmax=2000, log=print):
-    """V cycles to 1e-10 for each binary: full-V from u = 0 (the reference's
-    default), V cycles from u = 0, V cycles from the network's u."""
+def warm_guess(net, mg, b, m, dx, nsmooth=NSMOOTH, omega=OMEGA):
+    """The product warm start: the network's u in FP32, then nsmooth damped
+    Jacobi sweeps on the finest level."""
+    g = net.predict_u_fp32(b, m, dx)
+    if nsmooth:
+        a, bb = mg.coefficients(b)
+        mg.smooth(a, bb, g, nsmooth, omega)
+    return g
+
+
+def evaluate(net, binaries, m=C2_M, dx=C2_DX, nmax=2000, nsmooth=NSMOOTH, log=print):
+    """V cycles (and ms) to 1e-10 for each binary from five starts: full-V
+    from u = 0 (the reference's default), V cycles from u = 0, V cycles from
+    the network's u as trained (BF16), in FP32, and in FP32 followed by
+    nsmooth damped Jacobi sweeps (the warm start, "V_from_mlp").  A count of
+    nmax means the cap was reached (res_* > 1e-10)."""
     mg = Multigrid(m, dx, abi.mg_params(vcycle_nmax=nmax))
     mgv = Multigrid(m, dx, abi.mg_params(vcycle_nmax=nmax, fullV=0))
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        return r, 1e3 * (time.perf_counter() - t0)
+
     rows = []
     for b in binaries:
-        _, n_full, r_full = solve_binary(mg, b)
-        u0, n_v, r_v = solve_binary(mgv, b)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        g = net.predict_u(b, m, dx)
-        torch.cuda.synchronize()
-        t_inf = time.perf_counter() - t0
-        err = (g - u0).norm().item() / u0.norm().item()
-        t0 = time.perf_counter()
-        _, n_w, r_w = solve_binary(mgv, b, u=g)
-        torch.cuda.synchronize()
-        t_w = time.perf_counter() - t0
-        rows.append({"cond": cond_vector(b).tolist(), "fullV_from_zero": n_full, "V_from_zero": n_v,
-                     "V_from_mlp": n_w, "res_fullV": r_full, "res_V": r_v, "res_mlp": r_w,
-                     "mlp_rel_l2_error": err, "inference_ms": 1e3 * t_inf, "solve_from_mlp_ms": 1e3 * t_w})
+        (_, n_full, r_full), t_full = timed(lambda: solve_binary(mg, b))
+        (u0, n_v, r_v), t_v = timed(lambda: solve_binary(mgv, b))
+        g16, t_inf16 = timed(lambda: net.predict_u(b, m, dx))
+        g32, t_inf32 = timed(lambda: net.predict_u_fp32(b, m, dx))
+        gs, t_guess = timed(lambda: warm_guess(net, mgv, b, m, dx, nsmooth))
+        nrm = u0.norm().item()
+        errs = [(g - u0).norm().item() / nrm for g in (g16, g32, gs)]
+        (_, n_16, r_16), t_16 = timed(lambda: solve_binary(mgv, b, u=g16))
+        (_, n_32, r_32), t_32 = timed(lambda: solve_binary(mgv, b, u=g32))
+        (_, n_w, r_w), t_w = timed(lambda: solve_binary(mgv, b, u=gs))
+        rows.append({"cond": cond_vector(b).tolist(),
+                     "fullV_from_zero": n_full, "V_from_zero": n_v, "V_from_mlp_bf16": n_16,
+                     "V_from_mlp_fp32": n_32, "V_from_mlp": n_w,
+                     "res_fullV": r_full, "res_V": r_v, "res_mlp_bf16": r_16, "res_mlp_fp32": r_32, "res_mlp": r_w,
+                     "ms_fullV": t_full, "ms_V": t_v, "ms_mlp": t_w + t_guess,
+                     "mlp_rel_l2_error_bf16": errs[0], "mlp_rel_l2_error_fp32": errs[1],
+                     "mlp_rel_l2_error_smoothed": errs[2], "inference_ms_bf16": t_inf16, "inference_ms_fp32": t_inf32,
+                     "guess_ms": t_guess, "nsmooth": nsmooth})
         if log:
-            log("  fullV %4d  V %4d  V(mlp) %4d   |u_mlp-u|/|u| %.2e" % (n_full, n_v, n_w, err))
+            log("  fullV %4d  V %4d  V(mlp bf16) %4d  V(mlp fp32) %4d  V(mlp fp32 + %d sweeps) %4d   |u_mlp-u|/|u| "
+                "%.2e %.2e %.2e" % (n_full, n_v, n_16, n_32, nsmooth, n_w, *errs))
     mg.close()
     mgv.close()
     return rows
@@ -260,7 +298,9 @@ def main():
     ap.add_argument("--npts", type=int, default=16384)
     ap.add_argument("--cycles", type=int, default=80)
     ap.add_argument("--epochs", type=int, default=12)
-    ap.add_argument("--seed", type=int, default=2024)
+    # training draws from this seed, held-out draws from seed + 1 + i; the
+    # benchmark's draws come from another stream (seed 2024)
+    ap.add_argument("--seed", type=int, default=11)
     ap.add_argument("--frac-near", type=float, default=0.5)
     ap.add_argument("--eval-nmax", type=int, default=2000)
     ap.add_argument("--out", default=os.path.dirname(WEIGHTS))

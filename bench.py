@@ -198,9 +198,10 @@ iterations = 0
 
 
 def mg_binaries(n):
-    """The binary the reference converges on in a few hundred cycles
-    (m = 0.5 each at x = +-4, P_y = +-0.1, S_z = +-0.1), then n - 1 seeded
-    draws of the workload's parameter distribution."""
+    """The survey's binary (m = 0.5 each at x = +-4, P_y = +-0.1,
+    S_z = +-0.1), then n - 1 seeded draws of the workload's parameter
+    distribution (they are not among the warm start's training draws, which
+    use other seeds)."""
     import numpy as np
     from baum_b200 import punctures
     rng = np.random.default_rng(MG_BINARIES_SEED)
@@ -234,22 +235,42 @@ def reference_mg(binary, nxyz, dx, cores=None):
         shutil.rmtree(work, ignore_errors=True)
 
 
-def gpu_mg(m, dx, binaries):
+def gpu_mg(m, dx, binaries, warm=False, nmax=2000):
+    """V cycles, ms and final RMS residual to 1e-10 for each binary: full-V
+    from u = 0 (the reference's default); with warm, also V cycles from
+    u = 0 and from the learned warm start (the network's u in FP32 and its
+    smoothing sweeps, timed with the solve).  A count of nmax is the cap
+    ("capped": the residual stayed above 1e-10)."""
     import torch
-    from baum_b200 import punctures
-    mg = punctures.Multigrid(m, dx)
+    from baum_b200 import abi, punctures, warmstart
+    mg = punctures.Multigrid(m, dx, abi.mg_params(vcycle_nmax=nmax))
+    mgv = punctures.Multigrid(m, dx, abi.mg_params(vcycle_nmax=nmax, fullV=0)) if warm else None
+    net = warmstart.Network.load() if warm else None
     out = []
-    for b in binaries:
-        a, bb = mg.coefficients(b)
-        u = torch.zeros(m ** 3, dtype=torch.float64, device="cuda")
-        mg.solve(a, bb, u)  # warm-up: stack, graphs
-        u.zero_()
+
+    def run(solver, a, bb, start):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        n, res = mg.solve(a, bb, u)
+        u = start()
+        n, res = solver.solve(a, bb, u)
         torch.cuda.synchronize()
-        out.append({"vcycles": n, "ms": 1e3 * (time.perf_counter() - t0), "residual": res})
+        return {"vcycles": n, "ms": round(1e3 * (time.perf_counter() - t0), 2), "residual": res,
+                "capped": bool(res > 1e-10)}
+
+    zeros = lambda: torch.zeros(m ** 3, dtype=torch.float64, device="cuda")  # noqa: E731
+    for b in binaries:
+        a, bb = mg.coefficients(b)
+        mg.solve(a, bb, zeros())  # warm-up: stack, graphs
+        row = {"fullV_from_zero": run(mg, a, bb, zeros)}
+        if warm:
+            mgv.solve(a, bb, zeros())
+            row["V_from_zero"] = run(mgv, a, bb, zeros)
+            row["V_from_warm_start"] = run(mgv, a, bb, lambda: warmstart.warm_guess(net, mgv, b, m, dx))
+        out.append(row)
     mg.close()
+    if warm:
+        mgv.close()
+        net.close()
     return out
 
 
@@ -589,24 +610,34 @@ def run_ours(args, rank, world):
         c = oracle_port_cpu()
         cpu = {"value": c["value"], "unit": UNIT, "cores": c["cores"], "kind": "port", "sample": c["sample"]}
     # the multigrid half of the metric: V cycles and ms to the 1e-10 RMS
-    # residual on the 129^3-cell binary-puncture grid (dx = 0.125), seeded
-    # parameter sets; full-V cycling from u = 0 as the reference does
-    bins = mg_binaries(3)
-    mg130 = gpu_mg(130, 0.125, bins)
-    mg66 = gpu_mg(66, 0.25, bins[:1])
-    ref66 = reference_mg(bins[0], 64, 0.25) if not args.no_cpu else None
+    # residual on the 129^3-cell binary-puncture grid (dx = 0.25, x in
+    # [-16.1, 16.1]): the survey's binary and 9 seeded draws of the
+    # workload's distribution, full-V from u = 0 as the reference does, V
+    # cycles from u = 0 and from the learned warm start; the reference on
+    # the same binaries at 66^3 (dx = 0.5, the same domain) for the first two
+    from baum_b200 import warmstart
+    bins = mg_binaries(10)
+    mg130 = gpu_mg(warmstart.C2_M, warmstart.C2_DX, bins, warm=True)
+    mg66 = gpu_mg(66, 0.5, bins[:2])
+    ref66 = [reference_mg(b, 64, 0.5) for b in bins[:2]] if not args.no_cpu else [None, None]
     fmr_line = gpu_fmr(2)
     if world == 1 and not args.no_cpu:
         fmr_line["same_grid_reference"] = fmr_same_grid()
+    fv = [r["fullV_from_zero"] for r in mg130]
     multigrid = {
-        "workload": "binary punctures, Bowen-York, 130^3 points (129^3 cells), dx=0.125, tol 1e-10 RMS, full-V",
-        "vcycles": [r["vcycles"] for r in mg130], "ms": [round(r["ms"], 2) for r in mg130],
-        "ms_per_vcycle": sum(r["ms"] for r in mg130) / max(1, sum(r["vcycles"] for r in mg130)),
-        "seed": MG_BINARIES_SEED,
-        "same_grid_66": {"gpu_vcycles": mg66[0]["vcycles"], "gpu_ms": round(mg66[0]["ms"], 2),
-                         "reference_vcycles": ref66["vcycles"] if ref66 else None,
-                         "reference_s": round(ref66["seconds"], 2) if ref66 else None,
-                         "reference_cores": os.cpu_count()},
+        "workload": "binary punctures, Bowen-York, 130^3 points (129^3 cells), dx=0.25 (x in [-16.1, 16.1]), "
+                    "tol 1e-10 RMS, cap 2000 V cycles",
+        "vcycles": [r["vcycles"] for r in fv], "ms": [r["ms"] for r in fv],
+        "capped": [r["capped"] for r in fv], "final_residual": [r["residual"] for r in fv],
+        "ms_per_vcycle": sum(r["ms"] for r in fv) / max(1, sum(r["vcycles"] for r in fv)),
+        "seed": MG_BINARIES_SEED, "per_binary": mg130,
+        "warm_start": "network u in FP32 + %d damped Jacobi sweeps (omega %.3g), then V cycles"
+                      % (warmstart.NSMOOTH, warmstart.OMEGA),
+        "same_grid_66": [{"gpu_vcycles": g["fullV_from_zero"]["vcycles"], "gpu_ms": g["fullV_from_zero"]["ms"],
+                          "gpu_residual": g["fullV_from_zero"]["residual"],
+                          "reference_vcycles": r["vcycles"] if r else None,
+                          "reference_s": round(r["seconds"], 2) if r else None,
+                          "reference_cores": os.cpu_count()} for g, r in zip(mg66, ref66)],
     }
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -715,7 +746,7 @@ def main():
             # profiling: exactly K V cycles from the finest level (no full-V
             # start, tolerance 0): the first kernels are the 130^3 sweeps
             from baum_b200 import abi, punctures
-            mg = punctures.Multigrid(130, 0.125, abi.mg_params(fullV=0, tol=0.0, vcycle_nmax=args.mg_cycles))
+            mg = punctures.Multigrid(130, 0.25, abi.mg_params(fullV=0, tol=0.0, vcycle_nmax=args.mg_cycles))
             a, bb = mg.coefficients(mg_binaries(1)[0])
             u = torch.zeros(130 ** 3, dtype=torch.float64, device="cuda")
             torch.cuda.synchronize()
@@ -725,8 +756,9 @@ def main():
             print(json.dumps({"case": "mg", "vcycles": n, "ms": 1e3 * (time.perf_counter() - t0), "residual": res}))
             mg.close()
             return
-        r = gpu_mg(130, 0.125, mg_binaries(1))[0]
-        print(json.dumps({"case": "mg", "workload": "binary punctures, Bowen-York, 130^3 points, dx=0.125, "
+        from baum_b200 import warmstart
+        r = gpu_mg(warmstart.C2_M, warmstart.C2_DX, mg_binaries(1))[0]["fullV_from_zero"]
+        print(json.dumps({"case": "mg", "workload": "binary punctures, Bowen-York, 130^3 points, dx=0.25, "
                                                      "tol 1e-10 RMS, full-V", "seed": MG_BINARIES_SEED, **r,
                           "ms_per_vcycle": r["ms"] / max(1, r["vcycles"])}))
         return

@@ -276,6 +276,13 @@ int nrgpu_mg_destroy(nrgpu_mg *mg);
  * cycles, *normres = the final RMS residual. */
 int nrgpu_mg_solve(nrgpu_mg *mg, const double *a, const double *b, double *u, int *ncycles,
                    double *normres, void *stream);
+/* nsweeps damped Jacobi sweeps u <- u + omega (0 - L u) / L_ii of the
+ * puncture equation on the finest level, each followed by the Robin
+ * condition: smooths the grid-scale error of an initial guess (the learned
+ * warm start) before nrgpu_mg_solve.  0 < omega <= 1.  No counterpart in the
+ * reference (its smoother is undamped and runs only inside the V cycles). */
+int nrgpu_mg_smooth(nrgpu_mg *mg, const double *a, const double *b, double *u, int nsweeps, double omega,
+                    void *stream);
 
 /* Brill-Lindquist + Bowen-York coefficients a = 1/(psi_BL - 1) and
  * b = a^7 K_ij K^ij / 8 on the m^3 cube (SetMWBL, SetBYK,
@@ -389,10 +396,12 @@ enum { NRGPU_SYSTEM_BSSN = 0, NRGPU_SYSTEM_Z4C = 1 };
 int nrgpu_level_autotune(nrgpu_level *L, int system, const void *params, void *stream, int *best_block);
 int nrgpu_level_block(nrgpu_level *L, int bx, int by, int bz);
 int nrgpu_level_get_block(nrgpu_level *L, int *block);
-/* The BSSN interior rhs over TMA-staged tiles: on = 1 uses it on every box
- * it covers (even row length, 16-byte aligned fields, advection shift 1 or
- * 2 at 4th order, the centred 6th-order advection), the per-point kernel
- * elsewhere; 0 turns it off; -1 only queries.  Returns the setting. */
+/* The BSSN interior rhs over TMA-staged tiles on every box it covers (runs
+ * of order 4 or 6, even row length, 16-byte aligned fields, advection shift
+ * 1 or 2 at 4th order, the centred 6th-order advection), the per-point
+ * kernel elsewhere: on = 1 one block per tile, 2 the persistent form (one
+ * block per SM walking the tiles, the next tile's fields loaded during the
+ * current one), 0 off, -1 only queries.  Returns the setting. */
 int nrgpu_level_tile(nrgpu_level *L, int on);
 
 /* ---- ADM diagnostics ------------------------------------------------------
@@ -504,6 +513,11 @@ int nrgpu_mlp_forward(nrgpu_mlp *mlp, int n, float *d_out, void *stream);
  * point of the m^3 cube, for one binary (replaces the conditioning table) */
 int nrgpu_mlp_predict_u(nrgpu_mlp *mlp, const double *host_cond, int m, double dx, double uscale, double *u,
                         void *stream);
+/* The same prediction in FP32 on the CUDA cores from the FP32 master
+ * weights (features rounded to FP32, not BF16): the evaluation path, whose
+ * guess carries no BF16 grid-scale noise. */
+int nrgpu_mlp_predict_u_fp32(nrgpu_mlp *mlp, const double *host_cond, int m, double dx, double uscale, double *u,
+                             void *stream);
 
 /* ---- diagnostics -------------------------------------------------------- */
 

@@ -83,11 +83,48 @@ def test_training_reduces_loss(gpu):
 def test_predict_u_matches_oracle(gpu):
     net = warmstart.Network.load()
     b = Binary.sample(np.random.default_rng(99))
-    m, dx = 66, 0.25
+    m, dx = 66, 0.5
     u = net.predict_u(b, m, dx).cpu().numpy()
     idx = np.random.default_rng(1).integers(0, m ** 3, 4096)
     ref, _ = mo.forward(net.params().astype(np.float64), mo.features(warmstart.cond_vector(b), idx, m, dx))
     assert np.abs(u[idx] - net.uscale * ref).max() <= 2e-3 * np.abs(net.uscale * ref).max()
+
+
+def test_predict_u_fp32_matches_fp64_forward(gpu):
+    """The FP32 evaluation path against an FP64 forward of the same FP32
+    weights on unrounded features (numpy): FP32 rounding only, far below
+    the BF16 path's 2e-3."""
+    net = warmstart.Network.load()
+    b = Binary.sample(np.random.default_rng(98))
+    m, dx = 66, 0.5
+    u = net.predict_u_fp32(b, m, dx).cpu().numpy()
+    idx = np.random.default_rng(2).integers(0, m ** 3, 4096)
+    P = net.params().astype(np.float64)
+    c = warmstart.cond_vector(b)
+    h0 = -0.5 * (m - 1) * dx
+    x = np.stack([h0 + (idx % m) * dx, h0 + (idx // m % m) * dx, h0 + (idx // (m * m)) * dx], 1)
+    f = np.zeros((idx.size, 32))
+    f[:, :3] = x / 8
+    for q in range(2):
+        d = x - c[2 + 3 * q:5 + 3 * q]
+        r = np.sqrt((d * d).sum(1))
+        g = 3 + 12 * q
+        f[:, g:g + 3] = d / 8
+        f[:, g + 3] = r / 8
+        f[:, g + 4] = c[q] / (r + c[q])
+        f[:, g + 5] = 2 * c[q]
+        f[:, g + 6:g + 9] = 5 * c[8 + 3 * q:11 + 3 * q]
+        f[:, g + 9:g + 12] = 5 * c[14 + 3 * q:17 + 3 * q]
+    a, o = f, 0
+    for l in range(4):
+        k = 32 if l == 0 else 128
+        W = P[o:o + k * 128].reshape(k, 128)
+        bias = P[o + k * 128:o + k * 128 + 128]
+        o += k * 128 + 128
+        z = a @ W + bias
+        a = z / (1 + np.exp(-z))
+    ref = net.uscale * (a @ P[o:o + 128] + P[o + 128])
+    assert np.abs(u[idx] - ref).max() <= 2e-5 * np.abs(ref).max()
 
 
 SURVEY_BINARY = Binary([0.5, 0.5], [[4, 0, 0], [-4, 0, 0]], [[0, 0.1, 0], [0, -0.1, 0]], [[0, 0, 0.1], [0, 0, -0.1]])
@@ -101,11 +138,12 @@ def test_warm_start_is_close_and_lowers_the_initial_residual(gpu):
     from baum_b200.punctures import Multigrid
     net = warmstart.Network.load()
     rng = np.random.default_rng(424242)
-    mg = Multigrid(130, 0.125, abi.mg_params(fullV=0, vcycle_nmax=1))
-    ref = Multigrid(130, 0.125, abi.mg_params(vcycle_nmax=300))
+    m, dx = warmstart.C2_M, warmstart.C2_DX
+    mg = Multigrid(m, dx, abi.mg_params(fullV=0, vcycle_nmax=1))
+    ref = Multigrid(m, dx, abi.mg_params(vcycle_nmax=300))
     for b in [SURVEY_BINARY, Binary.sample(rng)]:
         u_ref, _, _ = warmstart.solve_binary(ref, b)
-        g = net.predict_u(b, 130, 0.125)
+        g = net.predict_u(b, m, dx)
         assert (g - u_ref).norm().item() <= 0.05 * u_ref.norm().item()
         # one V cycle from each start: the RMS residual is tested before it
         a, bb = mg.coefficients(b)

@@ -2,7 +2,8 @@
 reference's outputs and the CPU oracle, at the tolerance of every rhs parity
 test (1e-12 relative per variable).
 
-The staged-tile kernel stages each field's 22 x 10 x 10 box (a 16 x 4 x 4
+Both forms are run: one block per tile, and the persistent kernel (one
+block per SM walking the tiles).  The staged-tile kernel stages each field's 22 x 10 x 10 box (a 16 x 4 x 4
 tile and a halo of 3) in shared memory with one TMA load and forms the same
 terms as the per-point kernel in another order, so it is compared with the
 reference and the oracle, not bit for bit with the per-point kernel.  The
@@ -34,20 +35,24 @@ def to_dev(a):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
 
-def tiled(lev):
+def tiled(lev, mode):
     dl = bssn.DeviceLevel(lev)
-    assert dl.tile(1)
+    assert dl.tile(mode) == mode
     return dl
 
 
+MODES = pytest.mark.parametrize("mode", [1, 2], ids=["per_tile", "persistent"])
+
+
 @pytest.mark.parametrize("case", sorted(CASES))
-def test_tile_rhs_and_rk4_match_reference(gpu, case):
+@MODES
+def test_tile_rhs_and_rk4_match_reference(gpu, case, mode):
     """The reference's rhs; its RK4 states where the fixture holds them,
     else the oracle's."""
     g = load_golden(case)
     lev = golden_level(g)
     p = abi.bssn_params(**CASES[case])
-    dl = tiled(lev)
+    dl = tiled(lev, mode)
     u = to_dev(g["state_it0_l0"])
     r = dl.empty()
     bssn.evolve_rhs(dl, r, u, 0.0, u, p)
@@ -62,11 +67,12 @@ def test_tile_rhs_and_rk4_match_reference(gpu, case):
     assert not dl.nan_flag()
 
 
-def test_tile_puncture_rk4_matches_reference(gpu):
+@MODES
+def test_tile_puncture_rk4_matches_reference(gpu, mode):
     g = load_golden("bssn_punc_o4")
     lev = golden_level(g)
     p = abi.bssn_params()
-    dl = tiled(lev)
+    dl = tiled(lev, mode)
     u = to_dev(g["state_it0_l0"])
     for _ in range(4):
         bssn.evolve_rk_rk4(dl, u, float(g["dt"]), p)
@@ -74,13 +80,14 @@ def test_tile_puncture_rk4_matches_reference(gpu):
     assert relerr(u.cpu().numpy(), g["state_it4_l0"]).max() < TOL
 
 
-def test_tile_c1_schwarzschild_50_steps_matches_oracle(gpu):
+@MODES
+def test_tile_c1_schwarzschild_50_steps_matches_oracle(gpu, mode):
     """The benchmarked workload at full size: 64^3 inner points, 50 RK4
     steps with the staged-tile rhs."""
     lev, u0 = punctures.schwarzschild_c1()
     p = abi.bssn_params()
     dt = 0.25 * 0.25
-    dl = tiled(lev)
+    dl = tiled(lev, mode)
     u = to_dev(u0)
     for _ in range(50):
         bssn.evolve_rk_rk4(dl, u, dt, p)
@@ -92,7 +99,8 @@ def test_tile_c1_schwarzschild_50_steps_matches_oracle(gpu):
 
 
 @pytest.mark.parametrize("m,order", [(40, 4), (40, 6), (26, 4)])
-def test_tile_partial_tiles_and_orders_match_oracle(gpu, m, order):
+@MODES
+def test_tile_partial_tiles_and_orders_match_oracle(gpu, m, order, mode):
     """38 inner points per side (partial tiles in x, y and z), 24 (one
     partial tile in x); 4th order with lopsided advection and KO6, 6th order
     with the centred 6th-order advection; the order ladder near every face.
@@ -102,7 +110,7 @@ def test_tile_partial_tiles_and_orders_match_oracle(gpu, m, order):
     u0 = synthetic.fourier_state(x, y, z, abi.NVARS, synthetic.BSSN_UNIT, 8, 0.05, 16.0, 9)
     over = dict(order_centered=order, order_advection=order, advection_lopsided6=3) if order == 6 else {}
     p = abi.bssn_params(**over)
-    dl = tiled(lev)
+    dl = tiled(lev, mode)
     u = to_dev(u0)
     r = dl.empty()
     bssn.evolve_rhs(dl, r, u, 0.0, u, p)
@@ -121,12 +129,13 @@ def test_tile_partial_tiles_and_orders_match_oracle(gpu, m, order):
     assert not dl.nan_flag()
 
 
-def test_tile_host_buffer_slabs_equal_device_path(gpu):
+@MODES
+def test_tile_host_buffer_slabs_equal_device_path(gpu, mode):
     """The host-buffer step launches the interior in z slabs (planes
     k0..k1); with the staged-tile rhs it equals the device step bit for bit."""
     lev, u0 = punctures.schwarzschild_c1(n_inner=40, dx=0.5)
     p = abi.bssn_params()
-    dl = tiled(lev)
+    dl = tiled(lev, mode)
     u = to_dev(u0)
     for _ in range(2):
         bssn.evolve_rk_rk4(dl, u, 0.125, p)
@@ -136,11 +145,12 @@ def test_tile_host_buffer_slabs_equal_device_path(gpu):
 
 
 @pytest.mark.parametrize("case,steps", [("bssn_punc_octant", 4), ("bssn_fourier_bitant", 2)])
-def test_tile_symmetry_grids_match_reference(gpu, case, steps):
+@MODES
+def test_tile_symmetry_grids_match_reference(gpu, case, steps, mode):
     g = load_golden(case)
     lev = golden_level(g, GOLDEN_SYMMETRY[case])
     p = abi.bssn_params()
-    dl = tiled(lev)
+    dl = tiled(lev, mode)
     u = to_dev(g["state_it0_l0"])
     r = dl.empty()
     bssn.evolve_rhs(dl, r, u, 0.0, u, p)
