@@ -3,9 +3,9 @@ with FP32 accumulation) against its CPU FP64 oracle with the same BF16
 operand rounding (oracle/mlp_oracle.py): features bit-exact, forward and
 gradients within the FP32-accumulation error; training reduces the loss;
 the trained weights shipped with the package predict u within 5 % on
-binaries outside the training seeds and lower the initial residual; the
-north-star target of halving the V cycles to 1e-10 is recorded as a known
-failure (strict xfail), with the measured reason."""
+binaries outside the training seeds; the FP32 inference matches an FP64
+forward; the warm start (FP32 guess + damped Jacobi smoothing) lowers the
+initial residual and at least halves the V cycles to 1e-10."""
 import numpy as np
 import pytest
 import torch
@@ -87,7 +87,10 @@ def test_predict_u_matches_oracle(gpu):
     u = net.predict_u(b, m, dx).cpu().numpy()
     idx = np.random.default_rng(1).integers(0, m ** 3, 4096)
     ref, _ = mo.forward(net.params().astype(np.float64), mo.features(warmstart.cond_vector(b), idx, m, dx))
-    assert np.abs(u[idx] - net.uscale * ref).max() <= 2e-3 * np.abs(net.uscale * ref).max()
+    # the oracle rounds the same activations to BF16 after FP64 sums, the
+    # device after FP32 sums: an activation may round to the neighbouring
+    # BF16 value (2^-8 relative), hence a few 1e-3 of the largest output
+    assert np.abs(u[idx] - net.uscale * ref).max() <= 5e-3 * np.abs(net.uscale * ref).max()
 
 
 def test_predict_u_fp32_matches_fp64_forward(gpu):
@@ -132,8 +135,9 @@ SURVEY_BINARY = Binary([0.5, 0.5], [[4, 0, 0], [-4, 0, 0]], [[0, 0.1, 0], [0, -0
 
 def test_warm_start_is_close_and_lowers_the_initial_residual(gpu):
     """On binaries outside the training seeds, at the workload's 130^3 grid,
-    the network's u is within 5 % (relative L2) of the multigrid solution
-    and starts the V cycles from a lower RMS residual than u = 0."""
+    the network's u is within 5 % (relative L2) of the multigrid solution,
+    and the warm start (that u in FP32, smoothed) starts the V cycles from a
+    lower RMS residual than u = 0."""
     from baum_b200 import abi
     from baum_b200.punctures import Multigrid
     net = warmstart.Network.load()
@@ -148,22 +152,23 @@ def test_warm_start_is_close_and_lowers_the_initial_residual(gpu):
         # one V cycle from each start: the RMS residual is tested before it
         a, bb = mg.coefficients(b)
         r0 = mg.solve(a, bb, torch.zeros_like(g))[1]
-        rg = mg.solve(a, bb, g.clone())[1]
+        rg = mg.solve(a, bb, warmstart.warm_guess(net, mg, b, m, dx))[1]
         assert rg < r0, (rg, r0)
     mg.close()
     ref.close()
 
 
-@pytest.mark.xfail(strict=True, reason=(
-    "The puncture multigrid (undamped Jacobi, FAS V cycles) has a slow global mode "
-    "(~0.993 per cycle); from u = 0 its content is ~1e-6 of u, far below what a learned "
-    "guess accurate to 1e-2..1e-3 leaves, and the BF16 network adds grid-scale noise that "
-    "undamped Jacobi does not damp.  Measured: more cycles from the guess, not fewer."))
 def test_warm_start_halves_vcycles(gpu):
-    """The north-star target: V cycles from the network's u at most half of
-    those from u = 0 (V cycles) and of the reference's full-V from u = 0."""
+    """The north-star target on the workload's grid (130^3, x in
+    [-16.1, 16.1]): V cycles to the 1e-10 RMS residual from the warm start
+    (the network's u in FP32, 32 damped Jacobi sweeps) at most half of
+    those from u = 0, both V cycles and the reference's full-V.  The survey's
+    binary (measured 329 full-V, 342 V, 75 from the warm start) and a
+    held-out draw (4760, 4831, 149)."""
+    from baum_b200.punctures import Binary
     net = warmstart.Network.load()
-    rows = warmstart.evaluate(net, [SURVEY_BINARY], nmax=8000, log=None)
+    held = Binary.sample(np.random.default_rng(12))
+    rows = warmstart.evaluate(net, [SURVEY_BINARY, held], nmax=8000, log=None)
     for r in rows:
-        assert r["res_mlp"] <= 1e-10
+        assert r["res_mlp"] <= 1e-10 and r["res_V"] <= 1e-10 and r["res_fullV"] <= 1e-10, r
         assert 2 * r["V_from_mlp"] <= min(r["V_from_zero"], r["fullV_from_zero"]), r
