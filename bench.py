@@ -449,6 +449,86 @@ def fmr_same_grid(nxyz=48, cores=None):
                           "timing": "wall time of a 3-iteration minus a 1-iteration run, over 2"}}
 
 
+# the binary's grid in BAM (Z4c, punctures at x = +-2.75 place one box per
+# puncture on each finer level), for the batched-over-plain ratio: the same
+# parfile in the reference binary with the B200 module (oracle/_ref/bam_gpu)
+# in callback mode (the plain per-box drop-in: BAM's own Berger-Oliger
+# recursion, RK4 and restriction/prolongation on the host, every rhs and
+# boundary evaluation on the GPU with the level's lists copied over and
+# back) and in fmr mode (the whole coarse step of all levels on the device,
+# replayed as a CUDA graph); the plain reference on the host cores beside them
+BATCH_PAR = """physics = adm z4 punctures nrharness%s
+adm_data = Minkowski
+z4_lapse = 1+log withshift
+z4_shift = gamma0 withGadv withBadv withShiftadv withB
+z4_shiftdriver = 2.0
+z4_shiftgammacoeff = 0.75
+z4_kappa1 = 0.02
+z4_kappa2 = 0.0
+grid = box
+amr = bo newfmr
+amr_fmr = nestedboxes
+amr_lmax = %d
+amr_nbuffer = 3
+nxyz = %d
+dxyz = 0.5
+order_centered = 4
+order_advection = 4
+advection_lopsided = 1
+order_dissipation = 6
+dissipation_factor = 0.1
+evolution_method = rk
+evolution_method_rk = rk4
+dtfac = 0.25
+boundary = radiative
+iterations = %d
+mass1 = 0.5
+px1 = 2.75
+mass2 = 0.5
+px2 = -2.75
+punctures_solver = none
+nrharness_data = fourier
+nrharness_amp = 1e-3
+nrharness_length = 16
+%s
+"""
+
+
+def batching_ratio(lmax=4, nxyz=48, cores=None):
+    """Seconds per coarse step of the binary grid in the three binaries: the
+    wall time of a 3-iteration minus a 1-iteration run, over 2."""
+    bam, bam_gpu = (os.path.join(ROOT, "oracle", "_ref", b) for b in ("bam", "bam_gpu"))
+    if not (os.path.exists(bam) and os.path.exists(bam_gpu)):
+        return None
+    cores = cores or os.cpu_count() or 1
+    runs = {"fmr": (bam_gpu, " nrgpu", "nrgpu_mode = fmr\nz4_register_algcon = no"),
+            "callback": (bam_gpu, " nrgpu", "nrgpu_mode = callback"),
+            "reference": (bam, "", "")}
+    out = {"grid": "BAM binary grid: Z4c, punctures m = 0.5 at x = +-2.75, amr_lmax %d, nxyz %d, dxyz 0.5, "
+                   "4th order + KO6, Fourier data 1e-3" % (lmax, nxyz), "cores": cores}
+    for key, (binary, phys, extra) in runs.items():
+        walls = {}
+        for its in (1, 3):
+            work = tempfile.mkdtemp(prefix="bambatch_")
+            try:
+                with open(os.path.join(work, "b.par"), "w") as f:
+                    f.write(BATCH_PAR % (phys, lmax, nxyz, its, extra))
+                t0 = time.time()
+                r = subprocess.run([binary, "-nt", str(cores), "b.par"], cwd=work, capture_output=True, text=True,
+                                   timeout=1800)
+                walls[its] = time.time() - t0
+                if r.returncode:
+                    out[key] = {"error": (r.stdout[-400:] + r.stderr[-400:])}
+                    break
+            finally:
+                shutil.rmtree(work, ignore_errors=True)
+        if len(walls) == 2:
+            out[key] = {"s_per_coarse_step": (walls[3] - walls[1]) / 2}
+    if all("s_per_coarse_step" in out.get(k, {}) for k in ("fmr", "callback")):
+        out["batched_over_plain"] = out["callback"]["s_per_coarse_step"] / out["fmr"]["s_per_coarse_step"]
+    return out
+
+
 def oracle_port_cpu():
     """Fallback CPU baseline: the oracle restatement, one RK4 step."""
     from oracle import oracle
@@ -711,12 +791,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--case", default="c1", choices=["c1", "c1-step", "mg", "fmr", "c5", "z4c160"],
+    ap.add_argument("--case", default="c1", choices=["c1", "c1-step", "mg", "fmr", "c5", "z4c160", "batching"],
                     help="c1: the benchmark line; c1-step: only the 64^3 BSSN RK4 steps and the rhs "
                          "launches of that line (for profiling); mg: only the 130^3 multigrid solve of the "
                          "first seeded binary (for profiling); fmr: only the 7-level Z4c step, graph replay with tuned "
                          "blocks, --warmup and --steps coarse steps (for profiling); z4c160: the 160^3 Z4c box "
                          "alone")
+    ap.add_argument("--lmax", type=int, default=4, help="with --case batching: finest level of the BAM grid")
+    ap.add_argument("--nxyz", type=int, default=48, help="with --case batching: coarse points per side")
     ap.add_argument("--mg-cycles", type=int, default=0,
                     help="with --case mg: run exactly this many V cycles from the finest level (profiling)")
     args = ap.parse_args()
@@ -730,6 +812,9 @@ def main():
         torch.cuda.set_device(0)
         print(json.dumps({"case": "fmr", **gpu_fmr(args.steps, variants=(("graph", 1, 1),),
                                                      warm=max(args.warmup, 2))}))
+        return
+    if args.case == "batching":
+        print(json.dumps({"case": "batching", **(batching_ratio(args.lmax, args.nxyz) or {"unavailable": "bam_gpu"})}))
         return
     if args.case == "c5":
         import torch
