@@ -496,19 +496,22 @@ nrharness_length = 16
 
 def batching_ratio(lmax=4, nxyz=48, cores=None):
     """Seconds per coarse step of the binary grid in the three binaries: the
-    wall time of a 3-iteration minus a 1-iteration run, over 2."""
+    wall-time difference of two runs of different lengths over the extra
+    coarse steps (1 and 3 for the slow binaries; 2 and 42 for the fmr mode,
+    whose coarse step is far shorter than the run-to-run spread of start-up,
+    level set-up and autotuning)."""
     bam, bam_gpu = (os.path.join(ROOT, "oracle", "_ref", b) for b in ("bam", "bam_gpu"))
     if not (os.path.exists(bam) and os.path.exists(bam_gpu)):
         return None
     cores = cores or os.cpu_count() or 1
-    runs = {"fmr": (bam_gpu, " nrgpu", "nrgpu_mode = fmr\nz4_register_algcon = no"),
-            "callback": (bam_gpu, " nrgpu", "nrgpu_mode = callback"),
-            "reference": (bam, "", "")}
+    runs = {"fmr": (bam_gpu, " nrgpu", "nrgpu_mode = fmr\nz4_register_algcon = no", (2, 42)),
+            "callback": (bam_gpu, " nrgpu", "nrgpu_mode = callback", (1, 3)),
+            "reference": (bam, "", "", (1, 3))}
     out = {"grid": "BAM binary grid: Z4c, punctures m = 0.5 at x = +-2.75, amr_lmax %d, nxyz %d, dxyz 0.5, "
                    "4th order + KO6, Fourier data 1e-3" % (lmax, nxyz), "cores": cores}
-    for key, (binary, phys, extra) in runs.items():
+    for key, (binary, phys, extra, lens) in runs.items():
         walls = {}
-        for its in (1, 3):
+        for its in lens:
             work = tempfile.mkdtemp(prefix="bambatch_")
             try:
                 with open(os.path.join(work, "b.par"), "w") as f:
@@ -523,7 +526,8 @@ def batching_ratio(lmax=4, nxyz=48, cores=None):
             finally:
                 shutil.rmtree(work, ignore_errors=True)
         if len(walls) == 2:
-            out[key] = {"s_per_coarse_step": (walls[3] - walls[1]) / 2}
+            out[key] = {"s_per_coarse_step": (walls[lens[1]] - walls[lens[0]]) / (lens[1] - lens[0]),
+                        "runs": {str(k): round(v, 2) for k, v in walls.items()}}
     if all("s_per_coarse_step" in out.get(k, {}) for k in ("fmr", "callback")):
         out["batched_over_plain"] = out["callback"]["s_per_coarse_step"] / out["fmr"]["s_per_coarse_step"]
     return out
@@ -747,6 +751,54 @@ def run_ours(args, rank, world):
     print(json.dumps(line))
 
 
+def run_c1_kernels(args):
+    """The interior rhs of the 64^3 BSSN box in its three forms, each timed
+    alone (rhs evaluation, CUDA events, L2 flushed before each launch):
+    the per-point kernel with the tuned block shape (64 x 4 x 1), the staged-tile kernel
+    one block per tile, and its persistent form.  A shift is set so that
+    every term takes part.  For profiling (ncu -k regex:bssn_rhs)."""
+    import numpy as np
+    import torch
+    from baum_b200 import abi, build, bssn, punctures
+    build.build()
+    torch.cuda.set_device(0)
+    lev, u0 = punctures.schwarzschild_c1(N_INNER, DX)
+    x, _, _ = lev.coords()
+    u0[18] = 0.05 * np.sin(0.3 * x)
+    p = abi.bssn_params()
+    u = torch.from_numpy(u0).cuda()
+    flush = torch.empty(256 * 2 ** 20 // 4, dtype=torch.float32, device="cuda")
+    out = {"case": "c1-kernels"}
+    ref = None
+    for mode in (0, 1, 2):
+        dl = bssn.DeviceLevel(lev)
+        if mode == 0:
+            dl.set_block(64, 4, 1)   # the shape the tuner picks for this box
+            out["block"] = "64x4x1"
+        else:
+            dl.tile(mode)
+        r = dl.empty()
+        ts = []
+        for i in range(args.warmup + args.steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            bssn.bssn_rhs_movpunc_N(dl, r, u, 0.0, u, p)
+            b.record()
+            torch.cuda.synchronize()
+            if i >= args.warmup:
+                ts.append(a.elapsed_time(b))
+        ms = float(np.median(ts))
+        rh = r.cpu().numpy()
+        if ref is None:
+            ref = rh
+        err = max(float(np.abs(rh[v] - ref[v]).max() / max(np.abs(ref[v]).max(), 1e-8)) for v in range(abi.NVARS))
+        out[["per_point", "tile", "tile_persistent"][mode]] = {
+            "rhs_ms": ms, "tflops": FLOP_PER_POINT * PTS_PER_RHS / (ms * 1e-3) / 1e12, "rel_err_vs_per_point": err}
+        dl.close()
+    print(json.dumps(out))
+
+
 def run_z4c160(args):
     """The precision-sweep box as a throughput case: Z4c, 6th order + KO6,
     160^3 inner points (162^3 with the boundary layer), dx 0.15,
@@ -791,7 +843,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--case", default="c1", choices=["c1", "c1-step", "mg", "fmr", "c5", "z4c160", "batching"],
+    ap.add_argument("--case", default="c1", choices=["c1", "c1-step", "c1-kernels", "mg", "fmr", "c5", "z4c160",
+                                                      "batching"],
                     help="c1: the benchmark line; c1-step: only the 64^3 BSSN RK4 steps and the rhs "
                          "launches of that line (for profiling); mg: only the 130^3 multigrid solve of the "
                          "first seeded binary (for profiling); fmr: only the 7-level Z4c step, graph replay with tuned "
@@ -812,6 +865,9 @@ def main():
         torch.cuda.set_device(0)
         print(json.dumps({"case": "fmr", **gpu_fmr(args.steps, variants=(("graph", 1, 1),),
                                                      warm=max(args.warmup, 2))}))
+        return
+    if args.case == "c1-kernels":
+        run_c1_kernels(args)
         return
     if args.case == "batching":
         print(json.dumps({"case": "batching", **(batching_ratio(args.lmax, args.nxyz) or {"unavailable": "bam_gpu"})}))
