@@ -799,6 +799,64 @@ def run_c1_kernels(args):
     print(json.dumps(out))
 
 
+def run_precision_fmr(args):
+    """The FP32-stencil option where it is meant to apply: the batched
+    7-level Z4c grid with precision 1 (KO sums in FP32) or 2 (KO and centred
+    derivative sums in FP32) on the outer levels 0-2 only, the inner levels
+    FP64.  After --steps coarse steps (the first with 2nd-order time
+    interpolation) from the same data: per level and variable the largest
+    difference to the FP64 run relative to the variable's size, the change
+    of the Hamiltonian and momentum constraint norms on levels 0-2, and the
+    time per coarse step (graph replay, tuned shapes)."""
+    import copy
+    import numpy as np
+    import torch
+    from baum_b200 import abi, adm, build, bssn, fmr, workloads
+    build.build()
+    torch.cuda.set_device(0)
+    levels, params, dt = workloads.fmr_setup()
+    out = {"case": "precision-fmr", "levels_with_option": [0, 1, 2], "coarse_steps": args.steps}
+    ref = None
+    for prec in (0, 1, 2):
+        pp = [copy.copy(q) for q in params]
+        for l in (0, 1, 2):
+            pp[l].precision = prec
+        H = fmr.Hierarchy(levels, dt, pp)
+        u = [workloads.fmr_state_device(lev) for lev in levels]
+        H.advance(u, 1)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        H.advance(u, args.steps - 1)
+        b.record()
+        torch.cuda.synchronize()
+        H.close()
+        row = {"ms_per_coarse_step": a.elapsed_time(b) / max(1, args.steps - 1)}
+        cons = []
+        for l in (0, 1, 2):
+            dl = bssn.DeviceLevel(levels[l])
+            _, _, nrm = adm.computeadmconstraints(dl, u[l], 4)
+            cons.append([nrm["ham"][0], max(nrm[k][0] for k in ("momx", "momy", "momz"))])
+            dl.close()
+        row["constraint_norms_l012"] = cons
+        if ref is None:
+            ref = u
+        else:
+            per = []
+            for l in range(len(levels)):
+                d = (u[l] - ref[l]).abs().amax(dim=1) / ref[l].abs().amax(dim=1).clamp_min(1e-8)
+                per.append(d.cpu().numpy().tolist())
+            row["rel_err_per_level_per_variable"] = per
+            row["max_rel_err_per_level"] = [max(x) for x in per]
+            rc = out["precision_0"]["constraint_norms_l012"]
+            row["constraint_norm_rel_change_l012"] = [[abs(c[i] - r[i]) / r[i] for i in range(2)]
+                                                      for c, r in zip(cons, rc)]
+            del u
+        out["precision_%d" % prec] = row
+        torch.cuda.empty_cache()
+    print(json.dumps(out))
+
+
 def run_z4c160(args):
     """The precision-sweep box as a throughput case: Z4c, 6th order + KO6,
     160^3 inner points (162^3 with the boundary layer), dx 0.15,
@@ -844,7 +902,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--case", default="c1", choices=["c1", "c1-step", "c1-kernels", "mg", "fmr", "c5", "z4c160",
-                                                      "batching"],
+                                                      "batching", "precision-fmr"],
                     help="c1: the benchmark line; c1-step: only the 64^3 BSSN RK4 steps and the rhs "
                          "launches of that line (for profiling); mg: only the 130^3 multigrid solve of the "
                          "first seeded binary (for profiling); fmr: only the 7-level Z4c step, graph replay with tuned "
@@ -865,6 +923,9 @@ def main():
         torch.cuda.set_device(0)
         print(json.dumps({"case": "fmr", **gpu_fmr(args.steps, variants=(("graph", 1, 1),),
                                                      warm=max(args.warmup, 2))}))
+        return
+    if args.case == "precision-fmr":
+        run_precision_fmr(args)
         return
     if args.case == "c1-kernels":
         run_c1_kernels(args)
