@@ -90,3 +90,29 @@ def test_z4_fixed_stride_box_matches_oracle(gpu):
     torch.cuda.synchronize()
     uo = oracle.z4_evolve(lev, np.ascontiguousarray(u0.copy()), 0.075, 1, p)
     assert relerr(u.cpu().numpy(), uo).max() < TOL
+
+
+@pytest.mark.parametrize("precision,bound", [(1, 1e-8), (2, 5e-7)])
+def test_fp32_option_on_outer_levels(gpu, precision, bound):
+    """The FP32-stencil option on the outer levels 0-2 of the batched
+    workload's hierarchy (shrunk to 42, 40, 44, 32, 40, 24, 32 points per
+    side), the inner levels FP64, 2 coarse steps: every level within the
+    bound of the FP64 run (measured at full size after 3 coarse steps:
+    2.4e-9 for option 1, 1.1e-7 for option 2), and different from it."""
+    import copy
+    from baum_b200 import fmr, workloads
+    levels, params, dt = workloads.fmr_setup(workloads.FMR_SIZES_SMALL)
+    u0 = [workloads.fmr_state_host(lev) for lev in levels]
+    out = []
+    for prec in (0, precision):
+        pp = [copy.copy(q) for q in params]
+        for l in (0, 1, 2):
+            pp[l].precision = prec
+        H = fmr.Hierarchy(levels, dt, pp)
+        u = [torch.from_numpy(x.copy()).cuda() for x in u0]
+        H.advance(u, 2)
+        torch.cuda.synchronize()
+        out.append([x.cpu().numpy() for x in u])
+        H.close()
+    worst = max(relerr(a, b).max() for a, b in zip(out[1], out[0]))
+    assert 0 < worst < bound, worst
