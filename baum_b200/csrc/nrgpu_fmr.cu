@@ -4,7 +4,7 @@
 //   flags            setRPflags (flag.c:122-255), host, once
 //   restrict_kernel  restrict_boxtobox_N (interpolate_boxtobox_N.c:1055-1223)
 //   prolong_kernel   prolong_boxtobox_N (interpolate_boxtobox_N.c:585-869)
-//   ti_start/finish  evolve.c:292-340, 371-380 (orders 2 and 3)
+//   ti_start/finish  evolve.c:292-340, 371-380 (orders 2 to 6)
 //   nrgpu_fmr_advance advance_levelandsublevels (main.c:397-418) with
 //                    restrict_prolong_evolve (inject.c:116-132)
 // The reference does restriction and prolongation as three 1-D sweeps
@@ -137,6 +137,46 @@ __global__ void ti_start_kernel(Ptrs u, double *up, double *upp, double ca, doub
   up[t] = a;
 }
 
+// vladd (variables.c:650) of two terms with its special cases
+__device__ __forceinline__ double vladd_rn(double ca, double a, double cb, double b) {
+  if (ca == 0.0 && cb == 0.0) return 0.0;
+  if (ca == 0.0) return __dmul_rn(cb, b);
+  if (cb == 0.0) return __dmul_rn(ca, a);
+  return __dadd_rn(__dmul_rn(ca, a), __dmul_rn(cb, b));
+}
+
+// the start of the time interpolation of order o = 4, 5, 6 (evolve.c:
+// 316-333): the vladd chain onto upp, then the time levels shifted back
+// (:336-338) and the RK4 step's u_p copy, element by element
+__global__ void ti_start_hist_kernel(Ptrs u, double *up, double *upp, double *p2, double *p3, double *p4, int o,
+                                     long np, int nv) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= np * nv) return;
+  const int v = (int)(t / np);
+  const long i = t - (long)v * np;
+  const double a = u.p[v][i], b = up[t], h2 = p2[t];
+  const double h3 = o >= 5 ? p3[t] : 0.0, h4 = o >= 6 ? p4[t] : 0.0;
+  double r;
+  if (o == 4) {
+    r = vladd_rn(15.0 / 16, a, -5.0 / 16, b);
+    r = vladd_rn(1.0, r, 1.0 / 16, h2);
+  } else if (o == 5) {
+    r = vladd_rn(140.0 / 128, a, -70.0 / 128, b);
+    r = vladd_rn(1.0, r, 28.0 / 128, h2);
+    r = vladd_rn(1.0, r, -5.0 / 128, h3);
+  } else {
+    r = vladd_rn(315.0 / 256, a, -210.0 / 256, b);
+    r = vladd_rn(1.0, r, 126.0 / 256, h2);
+    r = vladd_rn(1.0, r, -45.0 / 256, h3);
+    r = vladd_rn(1.0, r, 7.0 / 256, h4);
+  }
+  upp[t] = r;
+  if (o >= 6) p4[t] = h3;
+  if (o >= 5) p3[t] = h2;
+  p2[t] = b;
+  up[t] = a;
+}
+
 // upp = 1.0 upp + c u
 __global__ void ti_finish_kernel(Ptrs u, double *upp, double c, long np, int nv) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -172,6 +212,9 @@ struct nrgpu_fmr {
   std::vector<double> fp[kMaxLevels], fr[kMaxLevels];  // flagprolong, flagrestrict (level-wide)
   std::vector<FmrPair> pairs[kMaxLevels];              // per fine level, one per fine box
   double *up[kMaxLevels], *upp[kMaxLevels];  // u(n-1) copy and time interpolant
+  // u(n-2), u(n-3), u(n-4) for time interpolation of orders 4-6 (u_p2, u_p3,
+  // u_p4 of evolve.c:289-294), order_timeinterpolation - 3 of them
+  double *hist[kMaxLevels][3];
   int iteration[kMaxLevels];
   // puncture tracking on the finest level (lmaxpunc = amr_lmax, grid.c:
   // 287-294): positions [3n] then the shift at the old positions [3n], and
@@ -441,8 +484,13 @@ int step_level(nrgpu_fmr *F, int l, double *const *u, cudaStream_t st) {
   int o = 0;
   if (child) {
     o = F->iteration[l] + 2 > F->p.order_timeinterpolation ? F->p.order_timeinterpolation : F->iteration[l] + 2;
-    const double ca = o == 2 ? 0.5 : 0.75, cb = o == 2 ? 0.0 : -0.125;
-    ti_start_kernel<<<nb, 256, 0, st>>>(U, F->up[l], F->upp[l], ca, cb, np, F->nv);
+    if (o <= 3) {
+      const double ca = o == 2 ? 0.5 : 0.75, cb = o == 2 ? 0.0 : -0.125;
+      ti_start_kernel<<<nb, 256, 0, st>>>(U, F->up[l], F->upp[l], ca, cb, np, F->nv);
+    } else {
+      ti_start_hist_kernel<<<nb, 256, 0, st>>>(U, F->up[l], F->upp[l], F->hist[l][0], F->hist[l][1],
+                                               F->hist[l][2], o, np, F->nv);
+    }
     NRGPU_CUDA_TRY(cudaGetLastError());
   }
   // the tracker reads the shift one step earlier at the old positions
@@ -455,7 +503,8 @@ int step_level(nrgpu_fmr *F, int l, double *const *u, cudaStream_t st) {
   else e = nrgpu_z4_rk4_stages(F->L[l], u, F->dt[l], &F->zp[l], st);
   if (e) return e;
   if (child) {
-    ti_finish_kernel<<<nb, 256, 0, st>>>(U, F->upp[l], o == 2 ? 1.0 / 2 : 3. / 8, np, F->nv);
+    static const double cfin[7] = {0, 0, 1.0 / 2, 3. / 8, 5. / 16, 35. / 128, 63. / 256};
+    ti_finish_kernel<<<nb, 256, 0, st>>>(U, F->upp[l], cfin[o], np, F->nv);
     NRGPU_CUDA_TRY(cudaGetLastError());
   }
   if (F->p.system == NRGPU_SYSTEM_BSSN) e = nrgpu_bssn_algcon(F->L[l], u, &F->bp[l], st);
@@ -519,6 +568,7 @@ extern "C" int nrgpu_fmr_destroy(nrgpu_fmr *F) {
     for (FmrPair &P : F->pairs[l]) cudaFree(P.d_plist);
     cudaFree(F->up[l]);
     cudaFree(F->upp[l]);
+    for (int h = 0; h < 3; ++h) cudaFree(F->hist[l][h]);
     nrgpu_level_destroy(F->L[l]);
   }
   cudaFree(F->d_track);
@@ -533,8 +583,8 @@ extern "C" int nrgpu_fmr_create(int nl, const nrgpu_level_desc *levels, const do
     return nrgpu_set_error(NRGPU_ERR_ARG, "bad arguments (1 <= nlevels <= %d)", kMaxLevels);
   if (p->system != NRGPU_SYSTEM_BSSN && p->system != NRGPU_SYSTEM_Z4C)
     return nrgpu_set_error(NRGPU_ERR_ARG, "system %d", p->system);
-  if (p->order_timeinterpolation < 2 || p->order_timeinterpolation > 3)
-    return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "order_timeinterpolation %d (2 or 3)", p->order_timeinterpolation);
+  if (p->order_timeinterpolation < 2 || p->order_timeinterpolation > 6)
+    return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "order_timeinterpolation %d (2 to 6)", p->order_timeinterpolation);
   if (p->order_RP != 2 && p->order_RP != 4 && p->order_RP != 6)
     return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "order_RP %d (2, 4 or 6)", p->order_RP);
   if (p->nbuffer < 1 || p->lbo < 0) return nrgpu_set_error(NRGPU_ERR_ARG, "nbuffer %d, lbo %d", p->nbuffer, p->lbo);
@@ -542,6 +592,7 @@ extern "C" int nrgpu_fmr_create(int nl, const nrgpu_level_desc *levels, const do
   memset(F->L, 0, sizeof F->L);
   memset(F->up, 0, sizeof F->up);
   memset(F->upp, 0, sizeof F->upp);
+  memset(F->hist, 0, sizeof F->hist);
   memset(F->iteration, 0, sizeof F->iteration);
   F->graph = nullptr;
   F->exec = nullptr;
@@ -590,6 +641,15 @@ extern "C" int nrgpu_fmr_create(int nl, const nrgpu_level_desc *levels, const do
         e = nrgpu_set_error(NRGPU_ERR_NOMEM, "time interpolation buffers of level %d", l);
       } else if (cudaMemset(F->up[l], 0, bytes) != cudaSuccess || cudaMemset(F->upp[l], 0, bytes) != cudaSuccess) {
         e = nrgpu_set_error(NRGPU_ERR_CUDA, "memset");
+      }
+      for (int h = 0; h < p->order_timeinterpolation - 3 && !e; ++h) {
+        if (cudaMalloc(&F->hist[l][h], bytes) != cudaSuccess) {
+          cudaGetLastError();
+          F->hist[l][h] = nullptr;
+          e = nrgpu_set_error(NRGPU_ERR_NOMEM, "time levels of level %d", l);
+        } else if (cudaMemset(F->hist[l][h], 0, bytes) != cudaSuccess) {
+          e = nrgpu_set_error(NRGPU_ERR_CUDA, "memset");
+        }
       }
     }
   }
@@ -647,7 +707,8 @@ extern "C" int nrgpu_fmr_advance(nrgpu_fmr *F, double *const *u, int nsteps, voi
     // no level is in its first iteration (time interpolation order) and
     // the state pointers are the same
     bool steady = true;
-    for (int l = 0; l < F->nl; ++l) steady = steady && F->iteration[l] >= 1;
+    const int full = F->p.order_timeinterpolation - 2 > 1 ? F->p.order_timeinterpolation - 2 : 1;
+    for (int l = 0; l < F->nl; ++l) steady = steady && F->iteration[l] >= full;
     if (!F->p.use_graph || !steady) {
       int e = advance(F, 0, u, st);
       if (e) return e;
@@ -697,10 +758,13 @@ extern "C" int nrgpu_fmr_advance(nrgpu_fmr *F, double *const *u, int nsteps, voi
 // levels' point counts), the counters, then per parent level u(n-1) and upp.
 namespace {
 constexpr uint32_t kCkptMagic = 0x4652474e;  // "NGRF"
-constexpr uint32_t kCkptVersion = 2;          // 2: the tracked positions at the end
+// 2: the tracked positions at the end; 3: the older time levels of
+// interpolation orders 4-6 after each level's u(n-1) and interpolant
+uint32_t ckpt_version(const nrgpu_fmr *F) { return F->p.order_timeinterpolation > 3 ? 3 : 2; }
+int ckpt_nbuf(const nrgpu_fmr *F) { return 2 + (F->p.order_timeinterpolation > 3 ? F->p.order_timeinterpolation - 3 : 0); }
 size_t ckpt_bytes(const nrgpu_fmr *F) {
   size_t b = sizeof(uint32_t) * 4 + sizeof(long) * F->nl + sizeof(int) * F->nl;
-  for (int l = 0; l < F->nl - 1; ++l) b += 2 * sizeof(double) * F->nv * (size_t)F->L[l]->npoints;
+  for (int l = 0; l < F->nl - 1; ++l) b += ckpt_nbuf(F) * sizeof(double) * F->nv * (size_t)F->L[l]->npoints;
   b += sizeof(int) + sizeof(double) * 3 * F->ntrack;
   return b;
 }
@@ -716,7 +780,7 @@ extern "C" int nrgpu_fmr_save(nrgpu_fmr *F, void *host, size_t bytes) {
   if (!F || !host || bytes < ckpt_bytes(F)) return nrgpu_set_error(NRGPU_ERR_ARG, "buffer of %zu bytes", bytes);
   NRGPU_CUDA_TRY(cudaDeviceSynchronize());
   char *c = (char *)host;
-  const uint32_t h[4] = {kCkptMagic, kCkptVersion, (uint32_t)F->nl, (uint32_t)F->nv};
+  const uint32_t h[4] = {kCkptMagic, ckpt_version(F), (uint32_t)F->nl, (uint32_t)F->nv};
   memcpy(c, h, sizeof h);
   c += sizeof h;
   for (int l = 0; l < F->nl; ++l, c += sizeof(long)) {
@@ -731,6 +795,8 @@ extern "C" int nrgpu_fmr_save(nrgpu_fmr *F, void *host, size_t bytes) {
     c += b;
     NRGPU_CUDA_TRY(cudaMemcpy(c, F->upp[l], b, cudaMemcpyDeviceToHost));
     c += b;
+    for (int q = 0; q < ckpt_nbuf(F) - 2; ++q, c += b)
+      NRGPU_CUDA_TRY(cudaMemcpy(c, F->hist[l][q], b, cudaMemcpyDeviceToHost));
   }
   memcpy(c, &F->ntrack, sizeof(int));
   c += sizeof(int);
@@ -744,7 +810,7 @@ extern "C" int nrgpu_fmr_load(nrgpu_fmr *F, const void *host, size_t bytes) {
   uint32_t h[4];
   memcpy(h, c, sizeof h);
   c += sizeof h;
-  if (h[0] != kCkptMagic || h[1] != kCkptVersion || h[2] != (uint32_t)F->nl || h[3] != (uint32_t)F->nv)
+  if (h[0] != kCkptMagic || h[1] != ckpt_version(F) || h[2] != (uint32_t)F->nl || h[3] != (uint32_t)F->nv)
     return nrgpu_set_error(NRGPU_ERR_ARG, "checkpoint of another hierarchy (levels %u, variables %u)", h[2], h[3]);
   for (int l = 0; l < F->nl; ++l, c += sizeof(long)) {
     long np;
@@ -756,7 +822,7 @@ extern "C" int nrgpu_fmr_load(nrgpu_fmr *F, const void *host, size_t bytes) {
   c += sizeof(int) * F->nl;
   {
     size_t off = 0;
-    for (int l = 0; l < F->nl - 1; ++l) off += 2 * sizeof(double) * F->nv * (size_t)F->L[l]->npoints;
+    for (int l = 0; l < F->nl - 1; ++l) off += ckpt_nbuf(F) * sizeof(double) * F->nv * (size_t)F->L[l]->npoints;
     int nt;
     memcpy(&nt, c + off, sizeof nt);
     if (nt != F->ntrack)
@@ -769,6 +835,8 @@ extern "C" int nrgpu_fmr_load(nrgpu_fmr *F, const void *host, size_t bytes) {
     c += b;
     NRGPU_CUDA_TRY(cudaMemcpy(F->upp[l], c, b, cudaMemcpyHostToDevice));
     c += b;
+    for (int q = 0; q < ckpt_nbuf(F) - 2; ++q, c += b)
+      NRGPU_CUDA_TRY(cudaMemcpy(F->hist[l][q], c, b, cudaMemcpyHostToDevice));
   }
   c += sizeof(int);
   if (F->ntrack) NRGPU_CUDA_TRY(cudaMemcpy(F->d_track, c, sizeof(double) * 3 * F->ntrack, cudaMemcpyHostToDevice));

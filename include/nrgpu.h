@@ -307,7 +307,7 @@ int nrgpu_puncture_coefficients(int m, double dx, int npunc, const double *mass,
 typedef struct {
   int system;                   /* NRGPU_SYSTEM_BSSN or NRGPU_SYSTEM_Z4C */
   int lbo;                      /* levels l >= lbo subcycle (regrid.c:51-78) */
-  int order_timeinterpolation;  /* 2 or 3 (bam_main.c:62, default 3) */
+  int order_timeinterpolation;  /* 2 to 6 (bam_main.c:62, default 3) */
   int order_RP;                 /* 2, 4 or 6 (bam_main.c:58, default 4) */
   int nbuffer;                  /* amr_nbuffer (bam_amr.c) */
   int use_graph;                /* capture the coarse steps after the first

@@ -323,28 +323,60 @@ static void vl_add(long np, int nv, double *const *r, double ca, double *const *
  * algebraic constraints (the EVOLVE functions after evolve).  system 0:
  * BSSN with nrgpu_bssn_params, 1: Z4c with nrgpu_z4_params.  iteration is
  * the level's iteration before the step; with_child = 0 skips the
- * interpolant (uprev, upp unused). */
-int oracle_fmr_evolve_level(const nrgpu_level_desc *L, int system, const void *params, int nv, double *const *u,
-                            double *const *uprev, double *const *upp, double dt, int iteration, int with_child,
-                            int order_ti)
+ * interpolant (uprev, upp unused).  order_ti 2..6; for orders 4-6, hist
+ * holds the older time levels u(n-2), u(n-3), u(n-4) (u_p2, u_p3, u_p4 of
+ * evolve.c:289-294), shifted back as the reference does (:336-338). */
+int oracle_fmr_evolve_level_h(const nrgpu_level_desc *L, int system, const void *params, int nv, double *const *u,
+                              double *const *uprev, double *const *upp, double *const *p2, double *const *p3,
+                              double *const *p4, double dt, int iteration, int with_child, int order_ti)
 {
   const long np = L->npoints;
   int o = 0, err = 0;
   if (with_child) {
-    if (order_ti < 2 || order_ti > 3) return -5;
+    if (order_ti < 2 || order_ti > 6) return -5;
+    if ((order_ti >= 4 && !p2) || (order_ti >= 5 && !p3) || (order_ti >= 6 && !p4)) return -1;
     o = iteration + 2 > order_ti ? order_ti : iteration + 2;
     if (o == 2) vl_add(np, nv, upp, 0.5, u, 0.0, u);
     if (o == 3) vl_add(np, nv, upp, 0.75, u, -0.125, uprev);
-    /* the RK4 step's u_p copy, kept as u(n-1) for the next step */
-    for (int v = 0; v < nv; v++) memcpy(uprev[v], u[v], sizeof(double) * np);
+    if (o == 4) {
+      vl_add(np, nv, upp, 15.0 / 16, u, -5.0 / 16, uprev);
+      vl_add(np, nv, upp, 1.0, upp, 1.0 / 16, p2);
+    }
+    if (o == 5) {
+      vl_add(np, nv, upp, 140.0 / 128, u, -70.0 / 128, uprev);
+      vl_add(np, nv, upp, 1.0, upp, 28.0 / 128, p2);
+      vl_add(np, nv, upp, 1.0, upp, -5.0 / 128, p3);
+    }
+    if (o == 6) {
+      vl_add(np, nv, upp, 315.0 / 256, u, -210.0 / 256, uprev);
+      vl_add(np, nv, upp, 1.0, upp, 126.0 / 256, p2);
+      vl_add(np, nv, upp, 1.0, upp, -45.0 / 256, p3);
+      vl_add(np, nv, upp, 1.0, upp, 7.0 / 256, p4);
+    }
+    for (int v = 0; v < nv; v++) {
+      if (o >= 6) memcpy(p4[v], p3[v], sizeof(double) * np);
+      if (o >= 5) memcpy(p3[v], p2[v], sizeof(double) * np);
+      if (o >= 4) memcpy(p2[v], uprev[v], sizeof(double) * np);
+      /* the RK4 step's u_p copy, kept as u(n-1) for the next step */
+      memcpy(uprev[v], u[v], sizeof(double) * np);
+    }
   }
   if (system == 0) err |= oracle_bssn_rk4_stages(L, u, dt, (const nrgpu_bssn_params *)params);
   else err |= oracle_z4_rk4_stages(L, u, dt, (const nrgpu_z4_params *)params);
   if (with_child) {
-    static const double c[4] = {0, 0, 1.0 / 2, 3. / 8};
+    static const double c[7] = {0, 0, 1.0 / 2, 3. / 8, 5. / 16, 35. / 128, 63. / 256};
     vl_add(np, nv, upp, 1.0, upp, c[o], u);
   }
   if (system == 0) oracle_bssn_algcon(L, u, (const nrgpu_bssn_params *)params);
   else oracle_z4_algcon(L, u, (const nrgpu_z4_params *)params);
   return err;
+}
+
+int oracle_fmr_evolve_level(const nrgpu_level_desc *L, int system, const void *params, int nv, double *const *u,
+                            double *const *uprev, double *const *upp, double dt, int iteration, int with_child,
+                            int order_ti)
+{
+  if (with_child && (order_ti < 2 || order_ti > 3)) return -5;
+  return oracle_fmr_evolve_level_h(L, system, params, nv, u, uprev, upp, 0, 0, 0, dt, iteration, with_child,
+                                   order_ti);
 }

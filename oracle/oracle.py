@@ -206,17 +206,20 @@ class FmrState:
         self.u = [np.ascontiguousarray(x, dtype=np.float64).copy() for x in u0]
         self.up = [np.zeros_like(x) for x in self.u]
         self.upp = [np.zeros_like(x) for x in self.u]
+        # u(n-2), u(n-3), u(n-4) for time interpolation of orders 4-6
+        self.hist = [[np.zeros_like(x) for _ in range(max(0, order_ti - 3))] for x in self.u]
         self.dt = [float(x) for x in dt]
         self.iteration = [0] * len(levels)
         self.lbo, self.order_ti, self.order_rp, self.nbuffer = lbo, order_ti, order_rp, nbuffer
 
     def step_level(self, l):
-        f = lib().oracle_fmr_evolve_level
+        f = lib().oracle_fmr_evolve_level_h
         f.restype = C.c_int
         child = l < len(self.levels) - 1
+        h = [_ptrs(x) for x in self.hist[l]] + [None] * (3 - len(self.hist[l]))
         e = f(C.byref(self.levels[l].desc), self.system, C.byref(self.params[l]), self.nv, _ptrs(self.u[l]),
-              _ptrs(self.up[l]), _ptrs(self.upp[l]), C.c_double(self.dt[l]), self.iteration[l], int(child),
-              self.order_ti)
+              _ptrs(self.up[l]), _ptrs(self.upp[l]), h[0], h[1], h[2], C.c_double(self.dt[l]), self.iteration[l],
+              int(child), self.order_ti)
         if e:
             raise RuntimeError("oracle level step failed (%d)" % e)
         self.iteration[l] += 1

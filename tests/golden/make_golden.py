@@ -317,6 +317,13 @@ px1 = 2.75
 mass2 = 0.5
 px2 = -2.75
 punctures_solver = none""")
+# time interpolation of orders 4 and 6 (evolve.c:298-340) on the same grid:
+# enough coarse steps that level 0 reaches the full order (iteration + 2 >
+# order_timeinterpolation) and level 1 runs at it for several steps
+for _o, _its in ((4, 4), (6, 6)):
+    FMR_CASES["z4_fmr3_ti%d" % _o] = FMR_CASES["z4_fmr3"].replace(
+        "iterations = 2", "iterations = %d\norder_timeinterpolation = %d" % (_its, _o)).replace(
+        "nrharness_dump = 0 2 4 8", "nrharness_dump = 0 %d %d %d" % (_its, 2 * _its, 4 * _its))
 # the dumps and fields kept: the end of the second coarse step on every
 # level and the finest level after its second step; g11, chi, A12, Khat,
 # Gamma1, Theta, alpha, beta1 (the initial state is regenerated by
@@ -325,6 +332,8 @@ punctures_solver = none""")
 FMR_KEEP = {"state_it2_l0", "state_it4_l1", "state_it8_l2", "state_it2_l2"}
 FMR_VARS = [0, 6, 8, 13, 14, 17, 18, 19]
 FMR_KEEP_BY_CASE = {"z4_fmr3": (FMR_KEEP, FMR_VARS),
+                    "z4_fmr3_ti4": ({"state_it4_l0", "state_it8_l1", "state_it16_l2"}, FMR_VARS),
+                    "z4_fmr3_ti6": ({"state_it6_l0", "state_it12_l1", "state_it24_l2"}, FMR_VARS),
                     "z4_fmr3_binary": ({"state_it2_l0", "state_it4_l1", "state_it8_l2"}, [6, 18])}
 
 # the shift-integration puncture tracker (track_moving_puncture_integrate,

@@ -170,3 +170,50 @@ def test_checkpoint_resumes_bit_for_bit(gpu):
     with pytest.raises(RuntimeError):
         H3.load(buf)
     H3.close()
+
+
+@pytest.mark.parametrize("order,steps", [(4, 4), (6, 6)])
+def test_time_interpolation_orders_4_and_6(gpu, order, steps):
+    """order_timeinterpolation 4 and 6 (evolve.c:298-340) on the device:
+    every level against the reference's dumps (the dump times of its 3-level
+    run) and against the oracle at the end, within the tolerance of the
+    3rd-order runs; graph replay equals plain launches bit for bit (the
+    graph is captured once every level runs at the full order); a checkpoint
+    taken half way resumes bit for bit (it carries the older time levels)."""
+    from test_fmr_oracle_pin import check_snapshots
+    g, levels, u0, params, dt = fmr_case("z4_fmr3_ti%d" % order)
+    runs = []
+    for use_graph in (0, 1):
+        H = fmr.Hierarchy(levels, dt, params, abi.fmr_params(order_timeinterpolation=order, use_graph=use_graph))
+        u = [to_dev(x) for x in u0]
+        H.advance(u, steps)
+        torch.cuda.synchronize()
+        runs.append([x.cpu().numpy() for x in u])
+        H.close()
+    for a, b in zip(*runs):
+        assert np.array_equal(a, b)
+    got = runs[1]
+    for l, key in enumerate(["state_it%d_l0" % steps, "state_it%d_l1" % (2 * steps), "state_it%d_l2" % (4 * steps)]):
+        ref = g[key]
+        err = np.abs(got[l][g["vars"]] - ref).max(axis=1) / np.abs(ref).max(axis=1)
+        assert err.max() < FMR_TOL, (l, err.max())
+    st = oracle.FmrState(levels, u0, 1, params, dt, order_ti=order)
+    st.advance(steps)
+    for l in range(3):
+        err = np.abs(got[l] - st.u[l]).max(axis=1) / np.maximum(np.abs(st.u[l]).max(axis=1), 1e-8)
+        assert err.max() < FMR_TOL, (l, err.max())
+    # checkpoint half way
+    fp = abi.fmr_params(order_timeinterpolation=order)
+    H = fmr.Hierarchy(levels, dt, params, fp)
+    u = [to_dev(x) for x in u0]
+    H.advance(u, steps // 2)
+    buf = H.save()
+    saved = [x.clone() for x in u]
+    H.close()
+    H2 = fmr.Hierarchy(levels, dt, params, fp)
+    H2.load(buf)
+    H2.advance(saved, steps - steps // 2)
+    torch.cuda.synchronize()
+    for a, b in zip(saved, got):
+        assert np.array_equal(a.cpu().numpy(), b)
+    H2.close()

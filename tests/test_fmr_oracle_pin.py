@@ -80,3 +80,15 @@ def test_binary_grid_evolution_matches_reference():
     g, levels, u0, params, dt = fmr_case("z4_fmr3_binary")
     st = oracle.FmrState(levels, u0, 1, params, dt)
     check_snapshots(g, lambda snap: st.advance(2, snap))
+
+
+@pytest.mark.parametrize("order,steps", [(4, 4), (6, 6)])
+def test_time_interpolation_orders_4_and_6_match_reference(order, steps):
+    """order_timeinterpolation 4 and 6 (evolve.c:298-340: the half-step
+    interpolant from u(n+1) and three to five earlier time levels, shifted
+    back each step): the reference's 3-level run for enough coarse steps
+    that level 0 reaches the full order; every level within the same
+    tolerance as the 3rd-order runs."""
+    g, levels, u0, params, dt = fmr_case("z4_fmr3_ti%d" % order)
+    st = oracle.FmrState(levels, u0, 1, params, dt, order_ti=order)
+    check_snapshots(g, lambda snap: st.advance(steps, snap))
