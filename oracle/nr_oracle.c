@@ -1215,3 +1215,19 @@ int oracle_z4_evolve(const nrgpu_level_desc *L, double *const *u, double dt, int
   for (s = 0; s < nsteps; s++) e |= oracle_z4_rk4_step(L, u, dt, p);
   return e;
 }
+
+#ifdef ORACLE_COUNT_FLOPS
+/* the same for the Z4c rhs */
+extern "C" void oracle_count_z4_point(const nrgpu_level_desc *L, double *const *u, int i, int j, int k,
+                                      const nrgpu_z4_params *p, long long *flops, long long *transc)
+{
+  const double h[3] = {L->dx, L->dy, L->dz};
+  int m = L->box[0].m, n = L->box[0].n, o = L->box[0].o;
+  long ijk = i + (long)m * (j + (long)n * k);
+  real r[25];
+  g_fc.flops = g_fc.transc = 0;
+  z4_point((const double *const *)u, ijk, i, j, k, m - 1, n - 1, o - 1, 1, m, (long)m * n, h, p, r);
+  *flops = g_fc.flops;
+  *transc = g_fc.transc;
+}
+#endif
