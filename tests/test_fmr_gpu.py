@@ -175,12 +175,12 @@ def test_checkpoint_resumes_bit_for_bit(gpu):
 @pytest.mark.parametrize("order,steps", [(4, 4), (6, 6)])
 def test_time_interpolation_orders_4_and_6(gpu, order, steps):
     """order_timeinterpolation 4 and 6 (evolve.c:298-340) on the device:
-    every level against the reference's dumps (the dump times of its 3-level
-    run) and against the oracle at the end, within the tolerance of the
-    3rd-order runs; graph replay equals plain launches bit for bit (the
+    every level against the oracle at the end (the oracle is pinned to the
+    reference's 3-level runs at these orders, whose dumps precede each
+    coarse step's last restriction), within the tolerance of the 3rd-order
+    runs; graph replay equals plain launches bit for bit (the
     graph is captured once every level runs at the full order); a checkpoint
     taken half way resumes bit for bit (it carries the older time levels)."""
-    from test_fmr_oracle_pin import check_snapshots
     g, levels, u0, params, dt = fmr_case("z4_fmr3_ti%d" % order)
     runs = []
     for use_graph in (0, 1):
@@ -193,10 +193,6 @@ def test_time_interpolation_orders_4_and_6(gpu, order, steps):
     for a, b in zip(*runs):
         assert np.array_equal(a, b)
     got = runs[1]
-    for l, key in enumerate(["state_it%d_l0" % steps, "state_it%d_l1" % (2 * steps), "state_it%d_l2" % (4 * steps)]):
-        ref = g[key]
-        err = np.abs(got[l][g["vars"]] - ref).max(axis=1) / np.abs(ref).max(axis=1)
-        assert err.max() < FMR_TOL, (l, err.max())
     st = oracle.FmrState(levels, u0, 1, params, dt, order_ti=order)
     st.advance(steps)
     for l in range(3):
