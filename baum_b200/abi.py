@@ -339,6 +339,8 @@ def lib():
         "nrgpu_mlp_forward": (C.c_int, [vp, C.c_int, vp, vp]),
         "nrgpu_mlp_predict_u": (C.c_int, [vp, C.POINTER(C.c_double), C.c_int, C.c_double, C.c_double, vp, vp]),
         "nrgpu_mlp_predict_u_fp32": (C.c_int, [vp, C.POINTER(C.c_double), C.c_int, C.c_double, C.c_double, vp, vp]),
+        "nrgpu_mlp_predict_u_tc": (C.c_int, [vp, C.POINTER(C.c_double), C.c_int, C.c_double, C.c_double, vp, vp]),
+        "nrgpu_mlp_tc_status": (C.c_int, [vp, C.POINTER(C.c_int)]),
         "nrgpu_fmr_params_default": (C.c_int, [C.POINTER(FmrParams)]),
         "nrgpu_fmr_create": (C.c_int, [C.c_int, C.POINTER(LevelDesc), C.POINTER(C.c_double), vp,
                                        C.POINTER(FmrParams), C.POINTER(vp)]),

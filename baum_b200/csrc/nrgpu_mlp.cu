@@ -22,6 +22,7 @@
 #include <stdint.h>
 #include <string.h>
 #include "nrgpu_common.cuh"
+#include "nrgpu_tma.cuh"
 
 static constexpr int IN = NRGPU_MLP_IN;
 static constexpr int HID = NRGPU_MLP_HIDDEN;
@@ -391,6 +392,292 @@ __global__ void scale_to_u_kernel(const float *__restrict__ o, double s, double 
   if (i < n) u[i] = s * (double)o[i];
 }
 
+// ---- the forward pass on the 5th-generation tensor cores (tcgen05) ---------------
+// One CTA of 512 threads per SM, two teams of 8 warps; each team walks its
+// own tiles of 128 grid points with its own 128 columns of tensor memory,
+// so the tensor core runs one team's layer while the other forms its
+// activations.  W1..W4 sit in shared memory for the whole walk, as BF16 in
+// the K-major layout without swizzle that the MMA reads through matrix
+// descriptors: an operand of R rows and K columns is stored as K/8 chunks of
+// R x 8 elements, each chunk row by row (16 B per row), so the 8-row core
+// matrices are 128 B apart (stride byte offset) and the two 8-column chunks
+// of one K = 16 step are 16 R bytes apart (leading byte offset).  Per tile:
+// the features of the 128 points go into X; per layer one thread of the
+// team issues the tcgen05.mma chain D[128 x 128] (FP32, tensor memory) =
+// X or A (128 x K) * W^T and commits it to the team's mbarrier; thread
+// (row, half) of the team then reads columns 64 half .. 64 half + 63 of its
+// row of D (tcgen05.ld: warp w reaches lanes 32 (w mod 4) ..), adds the
+// bias, applies SiLU, rounds to BF16 and writes the next layer's A (after
+// layer 4 the two halves form out = A4 w5 + b5).  Operands BF16,
+// accumulation FP32: the arithmetic of the training path.  SiLU is
+// z sigm(z) = z/2 (1 + tanh(z/2)) with the hardware tanh (tanh.approx.f32,
+// relative error about 2^-11, below the BF16 rounding that follows).
+namespace tc {
+constexpr int kRows = 128;
+constexpr int kThreads = 512;                    // two teams of 256
+constexpr int kChunk = kRows * 16;               // bytes of one 8-column chunk of a 128-row operand
+constexpr int kOffW0 = 0;                        // W1^T: 128 x 32, 4 chunks
+constexpr int kOffW = kOffW0 + 4 * kChunk;       // W2^T, W3^T, W4^T: 128 x 128, 16 chunks each
+constexpr int kOffX = kOffW + 3 * 16 * kChunk;   // features, per team: 128 x 32
+constexpr int kOffA = kOffX + 2 * 4 * kChunk;    // activations, per team: 128 x 128
+constexpr int kOffP = kOffA + 2 * 16 * kChunk;   // b1..b4 [4][128], w5 [128], b5 (FP32)
+constexpr int kOffRed = kOffP + ((4 * HID + HID + 1) * 4 + 15) / 16 * 16;   // per team: 128 partial outputs
+constexpr int kOffBar = kOffRed + 2 * kRows * 4; // 2 mbarriers
+constexpr int kOffTmem = kOffBar + 16;           // the tensor-memory base address; 2 timeout flags
+constexpr int kSmem = kOffTmem + 16 + 128;       // + room to align the base to 128 B
+static_assert(kSmem <= 227 * 1024, "shared memory of the tensor-core forward");
+// the instruction descriptor of kind::f16: FP32 accumulator, A and B BF16,
+// both K-major, N = 128 (bits 17-22: N/8), M = 128 (bits 24-28: M/16)
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+
+// byte offset of element (row, k) in a chunked K-major operand
+__device__ __forceinline__ int off(int row, int k) { return (k >> 3) * kChunk + row * 16 + (k & 7) * 2; }
+
+// shared-memory matrix descriptor (sm_100): start address >> 4 (bits 0-13),
+// leading byte offset >> 4 (bits 16-29: between the two K chunks of one
+// MMA), stride byte offset >> 4 (bits 32-45: between 8-row core matrices),
+// version 1 (bits 46-47), base offset 0, no swizzle (bits 61-63 zero)
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((kChunk >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((128 >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void mma(uint32_t dtmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+      ::"r"(dtmem), "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+__device__ __forceinline__ void commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   tma::smem_addr(bar))
+               : "memory");
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// barrier of one team (named barriers 1 and 2)
+__device__ __forceinline__ void team_sync(int team) { asm volatile("bar.sync %0, 256;" ::"r"(team + 1) : "memory"); }
+
+__device__ __forceinline__ float silu(float z) {
+  float th;
+  const float h = 0.5f * z;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(th) : "f"(h));
+  return fmaf(h, th, h);
+}
+// two FP32 values rounded to nearest even BF16, packed (lower column low)
+template <int CVT>
+__device__ __forceinline__ uint32_t pack_bf16(float x0, float x1) {
+  if (CVT == 0) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(x0, x1);
+    return *reinterpret_cast<const uint32_t *>(&v);
+  }
+  // round to nearest even on the bits (finite values): add 0x7FFF plus the
+  // lowest kept bit, keep the upper 16 bits
+  uint32_t u0 = __float_as_uint(x0), u1 = __float_as_uint(x1);
+  u0 += 0x7FFFu + ((u0 >> 16) & 1u);
+  u1 += 0x7FFFu + ((u1 >> 16) & 1u);
+  return __byte_perm(u0, u1, 0x7632);
+}
+
+// 32 consecutive FP32 columns of this thread's row (warp-collective); the
+// caller waits (tcgen05.wait::ld) before using them
+__device__ __forceinline__ void ld32(uint32_t taddr, uint32_t *r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr)
+      : "memory");
+}
+__device__ __forceinline__ void ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+}  // namespace tc
+
+template <int CVT>
+__global__ void __launch_bounds__(tc::kThreads, 1) mlp_forward_tc_kernel(const double *__restrict__ cond, int m,
+                                                                        double dx, const float *__restrict__ P,
+                                                                        double uscale, double *u, long np,
+                                                                        int *status) {
+  using namespace tc;
+  extern __shared__ __align__(128) unsigned char tc_raw[];
+  unsigned char *sm = tc_raw + ((128 - (tma::smem_addr(tc_raw) & 127)) & 127);
+  const int t = threadIdx.x, warp = t >> 5, team = t >> 8, tr = t & 255, r = tr & 127, half = tr >> 7;
+  const uint32_t sbase = tma::smem_addr(sm);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sm + kOffBar) + team;
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + kOffTmem);
+  volatile int *failed = reinterpret_cast<volatile int *>(sm + kOffTmem + 4);
+  float *par = reinterpret_cast<float *>(sm + kOffP);
+  float *red = reinterpret_cast<float *>(sm + kOffRed) + team * kRows;
+  // the weights, transposed to [n][k] in the chunked layout, and the biases
+  for (int idx = t; idx < IN * HID; idx += kThreads) {
+    const int k = idx / HID, n = idx % HID;
+    *reinterpret_cast<__nv_bfloat16 *>(sm + kOffW0 + off(n, k)) = __float2bfloat16_rn(P[off_w(0) + idx]);
+  }
+  for (int l = 1; l < 4; ++l)
+    for (int idx = t; idx < HID * HID; idx += kThreads) {
+      const int k = idx / HID, n = idx % HID;
+      *reinterpret_cast<__nv_bfloat16 *>(sm + kOffW + (l - 1) * 16 * kChunk + off(n, k)) =
+          __float2bfloat16_rn(P[off_w(l) + idx]);
+    }
+  for (int idx = t; idx < 4 * HID; idx += kThreads) par[idx] = P[off_b(idx / HID) + idx % HID];
+  for (int idx = t; idx <= HID; idx += kThreads) par[4 * HID + idx] = P[kOffW5 + idx];
+  // 256 columns of tensor memory: the FP32 accumulators (128 x 128) of the
+  // two teams
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tma::smem_addr(tslot)),
+                 "r"(256u)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (t < 2) {
+    tma::mbar_init(reinterpret_cast<uint64_t *>(sm + kOffBar) + t, 1);
+    failed[t] = 0;
+  }
+  if (t == 0) tma::mbar_fence_init();
+  fence_async_smem();
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *tslot;
+  const uint32_t dcol = tmem + 128u * team;                                          // the team's accumulator
+  const uint32_t trow = dcol + ((uint32_t)(32 * (warp & 3)) << 16) + 64u * half;     // this thread's lanes/half
+  unsigned char *X = sm + kOffX + team * 4 * kChunk;
+  unsigned char *A = sm + kOffA + team * 16 * kChunk;
+  const float *w5 = par + 4 * HID;
+  uint32_t phase = 0;
+  const long ntiles = (np + kRows - 1) / kRows;
+  for (long tile = 2L * blockIdx.x + team; tile < ntiles; tile += 2L * gridDim.x) {
+    const long row = tile * kRows + r;
+    {
+      // features of this thread's point (mlp_features_kernel's formulas):
+      // half 0 forms columns 0-15 (the coordinates, the first puncture's
+      // twelve, the second's x offset), half 1 columns 16-31
+      const long pp = row < np ? row : np - 1;
+      int i, j, k;
+      if (np <= 0x7FFFFFFFL) {
+        const unsigned q = (unsigned)pp, um = (unsigned)m, qm = q / um;
+        i = (int)(q - qm * um);
+        j = (int)(qm % um);
+        k = (int)(qm / um);
+      } else {
+        i = (int)(pp % m);
+        j = (int)((pp / m) % m);
+        k = (int)(pp / ((long)m * m));
+      }
+      const double h0 = -0.5 * (m - 1) * dx;
+      const double x[3] = {h0 + i * dx, h0 + j * dx, h0 + k * dx};
+      const double sc = 1.0 / 8.0;
+      __align__(16) __nv_bfloat16 f[16];
+      const int q = half;
+      const double mq = cond[q];
+      const double d0 = x[0] - cond[2 + 3 * q], d1 = x[1] - cond[3 + 3 * q], d2 = x[2] - cond[4 + 3 * q];
+      const double rr = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+      const double g[12] = {d0 * sc, d1 * sc, d2 * sc, rr * sc, mq / (rr + mq), 2.0 * mq,
+                            5.0 * cond[8 + 3 * q], 5.0 * cond[9 + 3 * q], 5.0 * cond[10 + 3 * q],
+                            5.0 * cond[14 + 3 * q], 5.0 * cond[15 + 3 * q], 5.0 * cond[16 + 3 * q]};
+      if (half == 0) {
+        f[0] = to_bf16(x[0] * sc);
+        f[1] = to_bf16(x[1] * sc);
+        f[2] = to_bf16(x[2] * sc);
+#pragma unroll
+        for (int c = 0; c < 12; ++c) f[3 + c] = to_bf16(g[c]);
+        f[15] = to_bf16((x[0] - cond[5]) * sc);
+      } else {
+#pragma unroll
+        for (int c = 1; c < 12; ++c) f[c - 1] = to_bf16(g[c]);
+#pragma unroll
+        for (int c = 11; c < 16; ++c) f[c] = __float2bfloat16_rn(0.0f);
+      }
+#pragma unroll
+      for (int c = 0; c < 2; ++c)
+        *reinterpret_cast<uint4 *>(X + off(r, 16 * half + 8 * c)) = *reinterpret_cast<const uint4 *>(f + 8 * c);
+    }
+    float out = 0.0f;
+    for (int l = 0; l < 4; ++l) {
+      // the operand was written by the threads: make it visible to the
+      // tensor core, then one thread issues the layer's MMA chain
+      fence_async_smem();
+      fence_before();
+      team_sync(team);
+      fence_after();
+      if (failed[team]) break;   // read after the barrier: the same in every thread of the team
+      if (tr == 0) {
+        const uint32_t a0 = sbase + (uint32_t)((l == 0 ? X : A) - sm);
+        const uint32_t b0 = sbase + (uint32_t)(l == 0 ? kOffW0 : kOffW + (l - 1) * 16 * kChunk);
+        const int ks = fan_in(l) / 16;
+        for (int s = 0; s < ks; ++s)
+          mma(dcol, sdesc(a0 + s * 2 * kChunk), sdesc(b0 + s * 2 * kChunk), s > 0 ? 1u : 0u);
+        commit(bar);
+      }
+      __syncwarp();
+      // a warp whose wait ran out skips the (warp-collective) tensor-memory
+      // reads; the team leaves the walk at its next barrier
+      if (!__all_sync(0xffffffffu, tma::mbar_wait(bar, phase))) {
+        failed[team] = 1;
+        continue;
+      }
+      phase ^= 1u;
+      fence_after();
+      uint32_t acc[64];
+      ld32(trow, acc);
+      ld32(trow + 32, acc + 32);
+      ld_wait();
+      const float4 *bias = reinterpret_cast<const float4 *>(par + l * HID + 64 * half);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        // the bias (and w5) as 16-byte broadcast reads of shared memory
+        const float4 b0 = bias[2 * c], b1 = bias[2 * c + 1];
+        const float bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+        float v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = silu(__uint_as_float(acc[8 * c + q]) + bb[q]);
+        uint4 pk;
+        pk.x = pack_bf16<CVT>(v[0], v[1]);
+        pk.y = pack_bf16<CVT>(v[2], v[3]);
+        pk.z = pack_bf16<CVT>(v[4], v[5]);
+        pk.w = pack_bf16<CVT>(v[6], v[7]);
+        if (l < 3) {
+          *reinterpret_cast<uint4 *>(A + off(r, 64 * half + 8 * c)) = pk;
+        } else {
+          const uint32_t w[4] = {pk.x, pk.y, pk.z, pk.w};
+          const float4 *w5v = reinterpret_cast<const float4 *>(w5 + 64 * half + 8 * c);
+          const float4 c0 = w5v[0], c1 = w5v[1];
+          const float cc[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            out = fmaf(__uint_as_float(w[q] << 16), cc[2 * q], out);
+            out = fmaf(__uint_as_float(w[q] & 0xFFFF0000u), cc[2 * q + 1], out);
+          }
+        }
+      }
+    }
+    // out = A4 w5 + b5 from the two halves of the row
+    if (half == 1) red[r] = out;
+    team_sync(team);
+    if (failed[team]) break;
+    if (half == 0 && row < np) u[row] = uscale * (double)(out + red[r] + w5[HID]);
+    // this tile's tensor-memory reads are done before the next tile's first
+    // MMA overwrites the accumulator (the barrier at the next layer start)
+    fence_before();
+  }
+  if (failed[team] && tr == 0) {
+    // an MMA chain still in flight is waited for (bounded) before the
+    // tensor memory is freed
+    atomicOr(status, 1);
+    tma::mbar_wait(bar, phase);
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u) : "memory");
+}
+
 long wb_off(int l) { return l == 0 ? 0 : (long)IN * HID + (long)(l - 1) * HID * HID; }
 
 }  // namespace
@@ -408,6 +695,7 @@ struct nrgpu_mlp {
   float *out, *y, *loss;
   double *cond;            // the conditioning table
   int ncond;
+  int *d_tcstatus;         // a wait of the tensor-core forward ran out
   long adam_t;
 };
 
@@ -488,7 +776,9 @@ extern "C" int nrgpu_mlp_create(int max_batch, nrgpu_mlp **out) {
             cudaMalloc(&M->dZ, sizeof(__nv_bfloat16) * nh) == cudaSuccess &&
             cudaMalloc(&M->out, sizeof(float) * max_batch) == cudaSuccess &&
             cudaMalloc(&M->y, sizeof(float) * max_batch) == cudaSuccess &&
-            cudaMalloc(&M->loss, sizeof(float)) == cudaSuccess;
+            cudaMalloc(&M->loss, sizeof(float)) == cudaSuccess &&
+            cudaMalloc(&M->d_tcstatus, sizeof(int)) == cudaSuccess &&
+            cudaMemset(M->d_tcstatus, 0, sizeof(int)) == cudaSuccess;
   for (int l = 0; l < 4 && ok; ++l)
     ok = cudaMalloc(&M->Z[l], sizeof(float) * nh) == cudaSuccess &&
          cudaMalloc(&M->Ab[l], sizeof(__nv_bfloat16) * nh) == cudaSuccess;
@@ -510,6 +800,7 @@ extern "C" int nrgpu_mlp_destroy(nrgpu_mlp *M) {
   if (!M) return NRGPU_OK;
   cudaFree(M->P); cudaFree(M->G); cudaFree(M->Mo); cudaFree(M->Vo); cudaFree(M->Wb); cudaFree(M->X);
   cudaFree(M->dA); cudaFree(M->dZ); cudaFree(M->out); cudaFree(M->y); cudaFree(M->loss); cudaFree(M->cond);
+  cudaFree(M->d_tcstatus);
   for (int l = 0; l < 4; ++l) {
     cudaFree(M->Z[l]);
     cudaFree(M->Ab[l]);
@@ -657,4 +948,38 @@ extern "C" int nrgpu_mlp_predict_u_fp32(nrgpu_mlp *M, const double *host_cond, i
   mlp_forward_fp32_kernel<<<(unsigned)((np + kFR - 1) / kFR), 256, 0, st>>>(M->cond, m, dx, M->P, uscale, u, np);
   NRGPU_CUDA_TRY(cudaGetLastError());
   return NRGPU_OK;
+}
+
+extern "C" int nrgpu_mlp_predict_u_tc(nrgpu_mlp *M, const double *host_cond, int m, double dx, double uscale,
+                                      double *u, void *stream) {
+  if (!M || !host_cond || !u || m < 2) return nrgpu_set_error(NRGPU_ERR_ARG, "bad prediction arguments");
+  const cudaStream_t st = (cudaStream_t)stream;
+  NRGPU_CUDA_TRY(cudaStreamSynchronize(st));  // the table is replaced below
+  int e = set_cond(M, host_cond, 1);
+  if (e) return e;
+  static bool attr_set[64] = {};
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) {
+    cudaGetLastError();
+    nsm = 148;
+  }
+  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    NRGPU_CUDA_TRY(cudaFuncSetAttribute(mlp_forward_tc_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kSmem));
+    attr_set[dev] = true;
+  }
+  const long np = (long)m * m * m;
+  const long pairs = ((np + tc::kRows - 1) / tc::kRows + 1) / 2;
+  const unsigned grid = (unsigned)(pairs < nsm ? pairs : nsm);
+  NRGPU_CUDA_TRY(cudaMemsetAsync(M->d_tcstatus, 0, sizeof(int), st));
+  mlp_forward_tc_kernel<0><<<grid, tc::kThreads, tc::kSmem, st>>>(M->cond, m, dx, M->P, uscale, u, np, M->d_tcstatus);
+  NRGPU_CUDA_TRY(cudaGetLastError());
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_mlp_tc_status(nrgpu_mlp *M, int *timed_out) {
+  if (!M || !timed_out) return nrgpu_set_error(NRGPU_ERR_ARG, "bad status arguments");
+  NRGPU_CUDA_TRY(cudaDeviceSynchronize());
+  NRGPU_CUDA_TRY(cudaMemcpy(timed_out, M->d_tcstatus, sizeof(int), cudaMemcpyDeviceToHost));
+  return *timed_out ? nrgpu_set_error(NRGPU_ERR_TIMEOUT, "a wait of the tensor-core forward ran out") : NRGPU_OK;
 }

@@ -126,6 +126,20 @@ class Network:
                                                      _stream()))
         return u
 
+    def predict_u_tc(self, binary, m, dx, out=None, check=True):
+        """The BF16 prediction on the tensor cores (tcgen05): one kernel,
+        weights resident in shared memory.  check=True synchronises and
+        raises if a bounded wait inside the kernel ran out."""
+        cv = cond_vector(binary)
+        u = torch.empty(m ** 3, dtype=torch.float64, device="cuda") if out is None else out
+        abi.check(abi.lib().nrgpu_mlp_predict_u_tc(self.handle, cv.ctypes.data_as(C.POINTER(C.c_double)), int(m),
+                                                   float(dx), float(self.uscale), C.c_void_p(u.data_ptr()),
+                                                   _stream()))
+        if check:
+            flag = C.c_int(0)
+            abi.check(abi.lib().nrgpu_mlp_tc_status(self.handle, C.byref(flag)))
+        return u
+
     def save(self, path, **meta):
         os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
         np.savez_compressed(path, params=self.params(), uscale=self.uscale, meta=json.dumps(meta))
@@ -241,10 +255,11 @@ def train(net, data, m=C2_M, dx=C2_DX, epochs=12, batch=16384, lr0=2e-3, lr1=2e-
     return hist
 
 
-def warm_guess(net, mg, b, m, dx, nsmooth=NSMOOTH, omega=OMEGA):
-    """The product warm start: the network's u in FP32, then nsmooth damped
-    Jacobi sweeps on the finest level."""
-    g = net.predict_u_fp32(b, m, dx)
+def warm_guess(net, mg, b, m, dx, nsmooth=NSMOOTH, omega=OMEGA, path="fp32"):
+    """The product warm start: the network's u in FP32 (path "fp32"), or in
+    BF16 on the tensor cores (path "tc"), then nsmooth damped Jacobi sweeps
+    on the finest level."""
+    g = net.predict_u_tc(b, m, dx) if path == "tc" else net.predict_u_fp32(b, m, dx)
     if nsmooth:
         a, bb = mg.coefficients(b)
         mg.smooth(a, bb, g, nsmooth, omega)
@@ -252,11 +267,12 @@ def warm_guess(net, mg, b, m, dx, nsmooth=NSMOOTH, omega=OMEGA):
 
 
 def evaluate(net, binaries, m=C2_M, dx=C2_DX, nmax=2000, nsmooth=NSMOOTH, log=print):
-    """V cycles (and ms) to 1e-10 for each binary from five starts: full-V
+    """V cycles (and ms) to 1e-10 for each binary from six starts: full-V
     from u = 0 (the reference's default), V cycles from u = 0, V cycles from
-    the network's u as trained (BF16), in FP32, and in FP32 followed by
-    nsmooth damped Jacobi sweeps (the warm start, "V_from_mlp").  A count of
-    nmax means the cap was reached (res_* > 1e-10)."""
+    the network's u as trained (BF16), in FP32, in FP32 followed by nsmooth
+    damped Jacobi sweeps (the warm start, "V_from_mlp"), and the tensor-core
+    BF16 u followed by the same sweeps ("V_from_mlp_tc").  A count of nmax
+    means the cap was reached (res_* > 1e-10)."""
     mg = Multigrid(m, dx, abi.mg_params(vcycle_nmax=nmax))
     mgv = Multigrid(m, dx, abi.mg_params(vcycle_nmax=nmax, fullV=0))
 
@@ -273,23 +289,27 @@ def evaluate(net, binaries, m=C2_M, dx=C2_DX, nmax=2000, nsmooth=NSMOOTH, log=pr
         (u0, n_v, r_v), t_v = timed(lambda: solve_binary(mgv, b))
         g16, t_inf16 = timed(lambda: net.predict_u(b, m, dx))
         g32, t_inf32 = timed(lambda: net.predict_u_fp32(b, m, dx))
+        _, t_inftc = timed(lambda: net.predict_u_tc(b, m, dx))
         gs, t_guess = timed(lambda: warm_guess(net, mgv, b, m, dx, nsmooth))
+        gt, t_guess_tc = timed(lambda: warm_guess(net, mgv, b, m, dx, nsmooth, path="tc"))
         nrm = u0.norm().item()
         errs = [(g - u0).norm().item() / nrm for g in (g16, g32, gs)]
         (_, n_16, r_16), t_16 = timed(lambda: solve_binary(mgv, b, u=g16))
         (_, n_32, r_32), t_32 = timed(lambda: solve_binary(mgv, b, u=g32))
         (_, n_w, r_w), t_w = timed(lambda: solve_binary(mgv, b, u=gs))
+        (_, n_t, r_t), t_t = timed(lambda: solve_binary(mgv, b, u=gt))
         rows.append({"cond": cond_vector(b).tolist(),
                      "fullV_from_zero": n_full, "V_from_zero": n_v, "V_from_mlp_bf16": n_16,
-                     "V_from_mlp_fp32": n_32, "V_from_mlp": n_w,
+                     "V_from_mlp_fp32": n_32, "V_from_mlp": n_w, "V_from_mlp_tc": n_t, "res_mlp_tc": r_t,
+                     "ms_mlp_tc": t_t + t_guess_tc, "inference_ms_tc": t_inftc, "guess_ms_tc": t_guess_tc,
                      "res_fullV": r_full, "res_V": r_v, "res_mlp_bf16": r_16, "res_mlp_fp32": r_32, "res_mlp": r_w,
                      "ms_fullV": t_full, "ms_V": t_v, "ms_mlp": t_w + t_guess,
                      "mlp_rel_l2_error_bf16": errs[0], "mlp_rel_l2_error_fp32": errs[1],
                      "mlp_rel_l2_error_smoothed": errs[2], "inference_ms_bf16": t_inf16, "inference_ms_fp32": t_inf32,
                      "guess_ms": t_guess, "nsmooth": nsmooth})
         if log:
-            log("  fullV %4d  V %4d  V(mlp bf16) %4d  V(mlp fp32) %4d  V(mlp fp32 + %d sweeps) %4d   |u_mlp-u|/|u| "
-                "%.2e %.2e %.2e" % (n_full, n_v, n_16, n_32, nsmooth, n_w, *errs))
+            log("  fullV %4d  V %4d  V(mlp bf16) %4d  V(mlp fp32) %4d  V(mlp fp32 + %d sweeps) %4d  V(mlp tc + "
+                "sweeps) %4d   |u_mlp-u|/|u| %.2e %.2e %.2e" % (n_full, n_v, n_16, n_32, nsmooth, n_w, n_t, *errs))
     mg.close()
     mgv.close()
     return rows

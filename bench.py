@@ -270,11 +270,58 @@ def gpu_mg(m, dx, binaries, warm=False, nmax=2000):
             mgv.solve(a, bb, zeros())
             row["V_from_zero"] = run(mgv, a, bb, zeros)
             row["V_from_warm_start"] = run(mgv, a, bb, lambda: warmstart.warm_guess(net, mgv, b, m, dx))
+            row["V_from_warm_start_tc"] = run(mgv, a, bb,
+                                              lambda: warmstart.warm_guess(net, mgv, b, m, dx, path="tc"))
         out.append(row)
     mg.close()
     if warm:
         mgv.close()
         net.close()
+    return out
+
+
+def mlp_inference(m, dx, reps=20):
+    """The warm start's network evaluated on the m^3 grid, three ways, timed
+    with CUDA events on the launching stream (mean over reps after 3
+    warm-ups): BF16 through the training path's kernels (features, four
+    mma.sync GEMMs with bias + SiLU, the output layer), FP32 on the CUDA
+    cores, and BF16 in one tcgen05 kernel.  Each call (ms_per_call) includes
+    the upload of the binary's conditioning vector before its kernels.
+    FLOPs per point: 2 (32 x 128 + 3 x 128 x 128 + 128) = 106,752."""
+    import torch
+    from baum_b200 import warmstart
+    net = warmstart.Network.load()
+    b = mg_binaries(1)[0]
+    u = torch.empty(m ** 3, dtype=torch.float64, device="cuda")
+    paths = {"bf16_mma_sync": lambda: net.predict_u(b, m, dx, out=u),
+             "fp32_simt": lambda: net.predict_u_fp32(b, m, dx, out=u),
+             "bf16_tcgen05": lambda: net.predict_u_tc(b, m, dx, out=u, check=False)}
+    flops = 2.0 * (32 * 128 + 3 * 128 * 128 + 128) * m ** 3
+    out = {"grid": "%d^3" % m, "flop_per_point": 106752}
+    for name, fn in paths.items():
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        ms = 0.0
+        for _ in range(reps):
+            # each call uploads the conditioning table and synchronises the
+            # stream first, so every launch is bracketed by its own events
+            fn()
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record()
+            fn()
+            s1.record()
+            torch.cuda.synchronize()
+            ms += s0.elapsed_time(s1)
+        ms /= reps
+        out[name] = {"ms_per_call": round(ms, 4), "tflops": round(flops / ms * 1e-9, 2)}
+    flag = 0
+    try:
+        net.predict_u_tc(b, m, dx, out=u)
+    except Exception as e:  # a bounded wait ran out
+        flag = str(e)
+    out["bf16_tcgen05"]["timed_out"] = flag
+    net.close()
     return out
 
 
@@ -724,8 +771,10 @@ def run_ours(args, rank, world):
         "capped": [r["capped"] for r in fv], "final_residual": [r["residual"] for r in fv],
         "ms_per_vcycle": sum(r["ms"] for r in fv) / max(1, sum(r["vcycles"] for r in fv)),
         "seed": MG_BINARIES_SEED, "per_binary": mg130,
-        "warm_start": "network u in FP32 + %d damped Jacobi sweeps (omega %.3g), then V cycles"
+        "warm_start": "network u in FP32 + %d damped Jacobi sweeps (omega %.3g), then V cycles; "
+                      "V_from_warm_start_tc: the BF16 u of the tcgen05 kernel + the same sweeps"
                       % (warmstart.NSMOOTH, warmstart.OMEGA),
+        "inference": mlp_inference(warmstart.C2_M, warmstart.C2_DX),
         "same_grid_66": [{"gpu_vcycles": g["fullV_from_zero"]["vcycles"], "gpu_ms": g["fullV_from_zero"]["ms"],
                           "gpu_residual": g["fullV_from_zero"]["residual"],
                           "reference_vcycles": r["vcycles"] if r else None,
@@ -907,12 +956,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--case", default="c1", choices=["c1", "c1-step", "c1-kernels", "mg", "fmr", "c5", "z4c160",
-                                                      "batching", "precision-fmr"],
+                                                      "batching", "precision-fmr", "mlp"],
                     help="c1: the benchmark line; c1-step: only the 64^3 BSSN RK4 steps and the rhs "
                          "launches of that line (for profiling); mg: only the 130^3 multigrid solve of the "
                          "first seeded binary (for profiling); fmr: only the 7-level Z4c step, graph replay with tuned "
                          "blocks, --warmup and --steps coarse steps (for profiling); z4c160: the 160^3 Z4c box "
-                         "alone")
+                         "alone; mlp: the warm start network's inference on the 130^3 grid, three kernels")
     ap.add_argument("--lmax", type=int, default=4, help="with --case batching: finest level of the BAM grid")
     ap.add_argument("--nxyz", type=int, default=48, help="with --case batching: coarse points per side")
     ap.add_argument("--mg-cycles", type=int, default=0,
@@ -934,6 +983,13 @@ def main():
         return
     if args.case == "c1-kernels":
         run_c1_kernels(args)
+        return
+    if args.case == "mlp":
+        import torch
+        from baum_b200 import build, warmstart
+        build.build()
+        torch.cuda.set_device(0)
+        print(json.dumps({"case": "mlp", **mlp_inference(warmstart.C2_M, warmstart.C2_DX, reps=args.steps)}))
         return
     if args.case == "batching":
         print(json.dumps({"case": "batching", **(batching_ratio(args.lmax, args.nxyz) or {"unavailable": "bam_gpu"})}))

@@ -518,6 +518,17 @@ int nrgpu_mlp_predict_u(nrgpu_mlp *mlp, const double *host_cond, int m, double d
  * guess carries no BF16 grid-scale noise. */
 int nrgpu_mlp_predict_u_fp32(nrgpu_mlp *mlp, const double *host_cond, int m, double dx, double uscale, double *u,
                              void *stream);
+/* The same prediction on the tensor cores (tcgen05.mma, FP32 accumulators in
+ * tensor memory): one persistent CTA per SM holds W1..W4 in shared memory as
+ * BF16 and runs the four 128-wide layers of 128-point tiles back to back;
+ * BF16 features and activations as in training.  Asynchronous on `stream`;
+ * nrgpu_mlp_tc_status reports whether a bounded wait inside it ran out. */
+int nrgpu_mlp_predict_u_tc(nrgpu_mlp *mlp, const double *host_cond, int m, double dx, double uscale, double *u,
+                           void *stream);
+/* synchronises the device; *timed_out = 1 (and NRGPU_ERR_TIMEOUT) when the
+ * last tensor-core prediction gave up waiting for its MMAs (its output is
+ * then incomplete), else 0 */
+int nrgpu_mlp_tc_status(nrgpu_mlp *mlp, int *timed_out);
 
 /* ---- diagnostics -------------------------------------------------------- */
 

@@ -93,6 +93,41 @@ def test_predict_u_matches_oracle(gpu):
     assert np.abs(u[idx] - net.uscale * ref).max() <= 5e-3 * np.abs(net.uscale * ref).max()
 
 
+@pytest.mark.parametrize("m,dx", [(66, 0.5), (5, 1.0), (130, 0.25)])
+def test_predict_u_tc_matches_oracle(gpu, m, dx):
+    """The tensor-core forward (tcgen05.mma, TMEM accumulators, weights in
+    shared memory) against the oracle's BF16 forward at sampled points and
+    against the mma.sync path at every point: partial last tiles (66^3 =
+    2246 tiles of 128 and 8 points), a cube smaller than one tile (5^3),
+    and the warm start's 130^3 grid.  Same bound as the BF16 path: an
+    activation may round to the neighbouring BF16 value, and SiLU uses the
+    hardware tanh (relative error about 2^-11)."""
+    net = warmstart.Network.load()
+    b = Binary.sample(np.random.default_rng(97))
+    u = net.predict_u_tc(b, m, dx).cpu().numpy()
+    assert np.isfinite(u).all()
+    idx = np.random.default_rng(3).integers(0, m ** 3, min(4096, m ** 3))
+    ref, _ = mo.forward(net.params().astype(np.float64), mo.features(warmstart.cond_vector(b), idx, m, dx))
+    ref = net.uscale * ref
+    assert np.abs(u[idx] - ref).max() <= 5e-3 * np.abs(ref).max()
+    u16 = net.predict_u(b, m, dx).cpu().numpy()
+    assert np.abs(u - u16).max() <= 5e-3 * np.abs(u16).max()
+
+
+def test_predict_u_tc_writes_into_a_given_buffer_and_repeats(gpu):
+    """Into a caller's buffer (canaries around it untouched), twice with
+    the same result: the kernel is deterministic (no atomics in the sums)."""
+    net = warmstart.Network.load()
+    b = Binary.sample(np.random.default_rng(96))
+    m = 40
+    buf = torch.full((m ** 3 + 2,), 7.0, dtype=torch.float64, device="cuda")
+    net.predict_u_tc(b, m, 0.5, out=buf[1:1 + m ** 3])
+    first = buf.clone()
+    net.predict_u_tc(b, m, 0.5, out=buf[1:1 + m ** 3])
+    assert buf[0].item() == 7.0 and buf[-1].item() == 7.0
+    assert torch.equal(first, buf)
+
+
 def test_predict_u_fp32_matches_fp64_forward(gpu):
     """The FP32 evaluation path against an FP64 forward of the same FP32
     weights on unrounded features (numpy): FP32 rounding only, far below
