@@ -279,6 +279,10 @@ class Level:
         return np.concatenate(xs), np.concatenate(ys), np.concatenate(zs)
 
 
+# nrgpu_fmr_move_fn: int (*)(void *user, nrgpu_fmr *fmr, int l, void *stream)
+FMR_MOVE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p)
+
+
 def ptr_array(ptrs):
     arr = (C.c_void_p * len(ptrs))()
     for i, p in enumerate(ptrs):
@@ -355,6 +359,8 @@ def lib():
         "nrgpu_fmr_load": (C.c_int, [vp, vp, C.c_size_t]),
         "nrgpu_fmr_track": (C.c_int, [vp, C.c_int, C.POINTER(C.c_double), C.c_int]),
         "nrgpu_fmr_punctures": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+        "nrgpu_fmr_set_move": (C.c_int, [vp, vp, vp]),
+        "nrgpu_fmr_regrid": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(LevelDesc), pp, pp, vp]),
         "nrgpu_track_punctures": (C.c_int, [vp, pp, pp, C.c_double, C.c_int, C.c_int, C.c_int, vp, vp, vp]),
         "nrgpu_track_punctures_extremum": (C.c_int, [vp, vp, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, vp, vp,
                                                      vp]),

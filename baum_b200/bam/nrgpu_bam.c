@@ -400,12 +400,128 @@ int nrgpu_track_fmr(tL *level)
   return 0;
 }
 
+/* Moving boxes in this mode (amr = ... move): BAM's own move_box
+ * (main/amr/move.c:808-986) moves the host levels and their host data; here
+ * the data live on the device.  So BAM's call (main.c:428) is sent to
+ * __wrap_move_box, which does nothing in this mode, and the device
+ * hierarchy calls fmr_move at the same points of its recursion
+ * (nrgpu_fmr_set_move).  fmr_move replays move_box's decisions with BAM's
+ * own functions: find_nested_bboxes on each parent, at the parent's time on
+ * the device and with the device's tracked positions, and make_level_bboxes
+ * for every level whose boxes change; then one nrgpu_fmr_regrid moves the
+ * device data of those levels (the copy and prolongation of move_overlap)
+ * and the old host levels are freed as move_box frees them. */
+void find_nested_bboxes(tL *level, int *pnboxes, tSBox *box);
+tL *make_level_bboxes(tL *level, int nboxes, tSBox *box, int pr);
+
+static double *fmr_ptrs[64 * ZNV]; /* the state pointers given to nrgpu_fmr_advance */
+
+/* box_equal (move.c:20-27) */
+static int sbox_equal(const double *a, const double *b)
+{
+  int i;
+  for (i = 0; i < 6; i++)
+    if (!dequal(a[i], b[i])) return 0;
+  return 1;
+}
+
+static int fmr_move(void *user, nrgpu_fmr *F, int l, void *stream)
+{
+  tG *g = (tG *)user;
+  nrgpu_level_desc d[16];
+  nrgpu_box box[16][8];
+  double *unew[16 * ZNV];
+  double *fresh[16];
+  tL *old[16];
+  int lv, b, j, np, nv = nvars(), nmove = 0, nlev = g->lmax - l + 1;
+  if (nlev < 1) return 0;
+  if (fmr_ntrack) {
+    check(nrgpu_fmr_punctures(F, fmr_tpos, 0), "punctures");
+    for (np = 0; np < fmr_ntrack; np++)
+      for (j = 0; j < 3; j++) g->puncpos[np][j] = fmr_tpos[3 * np + j];
+  }
+  memset(unew, 0, sizeof unew);
+  for (lv = l; lv <= g->lmax; lv++) {
+    tL *lc = g->level[lv - 1], *lold = g->level[lv], *lnew;
+    tSBox *sb = bcalloc(3 * sizeof(tSBox));
+    double tsave = lc->time;
+    int itsave = lc->iteration, nboxes;
+    int i = lv - l;
+    d[i].nboxes = 0;
+    fresh[i] = 0;
+    old[i] = 0;
+    /* the parent's time on the device (main.c:482-483) */
+    lc->iteration = nrgpu_fmr_iteration(F, lv - 1);
+    lc->time = lc->iteration * lc->dt;
+    find_nested_bboxes(lc, &nboxes, sb);
+    lc->time = tsave;
+    lc->iteration = itsave;
+    if (lc->sbox && lc->nsboxes == nboxes) {
+      for (j = 0; j < nboxes; j++)
+        if (!sbox_equal(lc->sbox[j].bbox, sb[j].bbox)) break;
+      if (j == nboxes) {
+        free(sb);
+        continue;
+      }
+    }
+    free(lc->sbox);
+    lc->sbox = sb;
+    lc->nsboxes = nboxes;
+    if (lold->prlocal) {
+      if (lold->nboxes > 1) free_level(lold->prlocal);
+      lold->prlocal = 0;
+    }
+    lnew = make_level_bboxes(lc, nboxes, sb, 0);
+    lnew->time = lold->time;
+    lnew->iteration = lold->iteration;
+    lnew->dt = lold->dt;
+    test_box_consistency_level(lc, lnew);
+    if (lnew->nboxes < 1 || lnew->nboxes > 8) errorexit("nrgpu: the refinement mode takes 1 to 8 boxes per level");
+    for (b = 0; b < lnew->nboxes; b++) {
+      tB *bx = lnew->box[b];
+      box[i][b].m = bx->m; box[i][b].n = bx->n; box[i][b].o = bx->o; box[i][b].noffset = bx->noffset;
+      box[i][b].x0 = bx->x0; box[i][b].y0 = bx->y0; box[i][b].z0 = bx->z0;
+    }
+    d[i].nboxes = lnew->nboxes; d[i].box = box[i]; d[i].npoints = lnew->npoints;
+    d[i].dx = lnew->dx; d[i].dy = lnew->dy; d[i].dz = lnew->dz; d[i].boundary = lnew->boundary;
+    d[i].symmetry = grid_symmetry();
+    if (cudaMalloc((void **)&fresh[i], sizeof(double) * nv * lnew->npoints))
+      errorexit("nrgpu: device allocation failed");
+    lists(fresh[i], lnew->npoints, unew + i * nv);
+    old[i] = lold;
+    nmove++;
+  }
+  if (!nmove) return 0;
+  check(nrgpu_fmr_regrid(F, l, nlev, d, fmr_ptrs, unew, stream), "regrid");
+  for (lv = l; lv <= g->lmax; lv++) {
+    int i = lv - l;
+    if (!fresh[i]) continue;
+    cudaFree(fmr_state[lv]);
+    fmr_state[lv] = fresh[i];
+    lists(fresh[i], g->level[lv]->npoints, fmr_ptrs + lv * nv);
+    free_level(old[i]);
+  }
+  if (Getv("amr_verbose", "move") || Getv("amr_verbose", "all"))
+    printf("nrgpu: moved %d level(s) from level %d on\n", nmove, l);
+  return 0;
+}
+
+#ifdef NRGPU_WRAP_MOVE_BOX
+/* the wrapped move_box of a build linked with -Wl,--wrap=move_box */
+int __real_move_box(tG *g, int l);
+int __wrap_move_box(tG *g, int l)
+{
+  if (nrgpu_mode_fmr) return 0;  /* moved inside the device's coarse step */
+  return __real_move_box(g, l);
+}
+#endif
+
 int nrgpu_evolve_fmr(tL *level)
 {
   tG *g = level->grid;
   tVarList *u = 0;
   int l, nl, nv = nvars();
-  double *ptrs[64 * ZNV];
+  double **ptrs = fmr_ptrs;
   if (!nrgpu_mode_fmr || level->l != 0) return 0;
   nl = g->lmax + 1;
   if (g->lmin != 0 || nl > 16) errorexit("nrgpu: levels 0..lmax with lmax < 16");
@@ -447,6 +563,12 @@ int nrgpu_evolve_fmr(tL *level)
     fp.nbuffer = Geti("amr_nbuffer");
     check(nrgpu_fmr_create(nl, d, dt, nrgpu_system_z4 ? (void *)zp : (void *)bp, &fp, &fmr_h), "fmr");
     fmr_track_setup(g);
+    if (Getv("amr", "move")) {
+#ifndef NRGPU_WRAP_MOVE_BOX
+      errorexit("nrgpu: moving boxes in the fmr mode need a build linked with -Wl,--wrap=move_box");
+#endif
+      check(nrgpu_fmr_set_move(fmr_h, fmr_move, g), "move");
+    }
   }
   for (l = 0; l < nl; l++) lists(fmr_state[l], g->level[l]->npoints, ptrs + l * nv);
   check(nrgpu_fmr_advance(fmr_h, ptrs, 1, 0), "fmr advance");

@@ -186,6 +186,17 @@ __global__ void ti_finish_kernel(Ptrs u, double *upp, double c, long np, int nv)
   upp[t] = __dadd_rn(__dmul_rn(1.0, upp[t]), __dmul_rn(c, u.p[v][i]));
 }
 
+// move_overlap_nonparallel (move.c:603-640): the points of an old box that
+// a new box of the same level also holds, copied for every variable; one
+// thread per (point of the index range, variable)
+__global__ void copy_range_kernel(Ptrs src, Ptrs dst, Box3 sb, Box3 db, int3 s0, int3 d0, int3 n, long npts) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts) return;
+  const int v = blockIdx.y;
+  const int i = (int)(t % n.x), j = (int)((t / n.x) % n.y), k = (int)(t / ((long)n.x * n.y));
+  dst.p[v][at3(db, d0.x + i, d0.y + j, d0.z + k)] = src.p[v][at3(sb, s0.x + i, s0.y + j, s0.z + k)];
+}
+
 }  // namespace
 
 // one fine box and the coarse box that holds it (BAM's box->pr): the
@@ -222,6 +233,12 @@ struct nrgpu_fmr {
   int ntrack, track_fixz;
   double *d_track;
   int *d_tstatus;
+  // moving boxes: the caller's hook, called where the reference calls
+  // move_box (main.c:428), and the levels whose pairs with their parent
+  // wait to be set up again after a regrid of that parent
+  nrgpu_fmr_move_fn move_fn;
+  void *move_user;
+  bool pair_stale[kMaxLevels];
   // graph of one coarse step for one set of state pointers
   cudaGraph_t graph;
   cudaGraphExec_t exec;
@@ -540,6 +557,242 @@ int advance(nrgpu_fmr *F, int l, double *const *u, cudaStream_t st) {
       (e = nrgpu_track_after_step(F->L[l], u + l * F->nv + shift_index(F), F->dt[l], F->p.order_RP, F->track_fixz,
                                   F->ntrack, F->d_track, F->d_track + 3 * F->ntrack, F->d_tstatus, st)))
     return e;
+  // move_box(g, l + 1) (move.c:808-856): the levels above l may move once l
+  // and its sublevels are done, unless l is aligned in time with its parent
+  if (F->move_fn && l + 1 < F->nl) {
+    bool go = l == 0;
+    if (!go) {
+      const double tl = F->iteration[l] * F->dt[l], tp = F->iteration[l - 1] * F->dt[l - 1];
+      go = tl < tp - 1e-10;
+    }
+    if (go) {
+      const int r = F->move_fn(F->move_user, F, l + 1, (void *)st);
+      if (r) return r < 0 ? r : nrgpu_set_error(NRGPU_ERR_ARG, "move hook of level %d returned %d", l + 1, r);
+      for (int q = 1; q < F->nl; ++q)
+        if (F->pair_stale[q])
+          return nrgpu_set_error(NRGPU_ERR_ARG, "level %d was not set up again after its parent moved", q);
+    }
+  }
+  return NRGPU_OK;
+}
+
+// ---- moving boxes: one level to a new set of boxes ---------------------------
+// move_overlap (move.c:712-800) for every time level of the level: the new
+// points are prolonged from the parent (prolong_varlist with flag -3 or -1,
+// interpolate_boxtobox_N.c:870-1010, order_RP), then every point that an old
+// box also holds is copied from it.  The parent's state is the new one when
+// the parent moved first (levels move coarsest first, move.c:874-983).
+struct Buffers {
+  Ptrs p;
+  bool ok;
+};
+
+// the state of level p during a regrid of levels lmin..: the new buffers if
+// p moved in this regrid, else the current ones
+double *const *unew_or_u(const nrgpu_fmr *F, int lmin, int p, double *const *u, double *const *unew,
+                         const nrgpu_level_desc *desc) {
+  if (p >= lmin && desc[p - lmin].nboxes > 0) return unew + (long)(p - lmin) * F->nv;
+  return u + (long)p * F->nv;
+}
+
+Buffers level_set(double *base, long np, int nv) {
+  Buffers b;
+  b.ok = base != nullptr;
+  for (int v = 0; v < kMaxVars; ++v) b.p.p[v] = base && v < nv ? base + (long)v * np : nullptr;
+  return b;
+}
+
+// index range of the overlap of two boxes of one level (box_overlap_range,
+// move.c:518-566): false when empty
+bool overlap_range(const Box3 &a, const double *ax0, const Box3 &b, const double *bx0, const double *dx, int *ia,
+                   int *ib) {
+  for (int d = 0; d < 3; ++d) {
+    const double alo = ax0[d], ahi = ax0[d] + (a.n[d] - 1) * dx[d];
+    const double blo = bx0[d], bhi = bx0[d] + (b.n[d] - 1) * dx[d];
+    const double lo = alo > blo ? alo : blo, hi = ahi < bhi ? ahi : bhi;
+    if (hi < lo - 1e-10 * dx[d]) return false;
+    ia[2 * d] = (int)floor((lo - alo + 1e-10) / dx[d]);
+    ia[2 * d + 1] = (int)floor((hi - alo + 1e-10) / dx[d]);
+    ib[2 * d] = (int)floor((lo - blo + 1e-10) / dx[d]);
+    ib[2 * d + 1] = (int)floor((hi - blo + 1e-10) / dx[d]);
+  }
+  return true;
+}
+
+template <int N>
+void launch_prolong(const Ptrs &uc, const Ptrs &uf, const Box3 &cb, const Box3 &fb, const PGeom &G, const int *list,
+                    int n, int nv, cudaStream_t st) {
+  prolong_kernel<N><<<dim3((n + 127) / 128, nv), 128, 0, st>>>(uc, uf, cb, fb, G, list, n);
+}
+
+int regrid_level(nrgpu_fmr *F, int m, const nrgpu_level_desc &d, double *const *uold, double *const *unew,
+                 double *const *uparent, cudaStream_t st) {
+  if (d.symmetry) return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "level %d: symmetry grids", m);
+  if (d.dx != F->dx[m][0] || d.dy != F->dx[m][1] || d.dz != F->dx[m][2])
+    return nrgpu_set_error(NRGPU_ERR_ARG, "level %d: a move keeps the grid spacing", m);
+  for (int v = 0; v < F->nv; ++v)
+    if (!unew[v] || !uold[v] || !uparent[v]) return nrgpu_set_error(NRGPU_ERR_ARG, "level %d: null state pointer", m);
+  const int nv = F->nv;
+  const bool parent_role = m < F->nl - 1;
+  const int nh = F->p.order_timeinterpolation > 3 ? F->p.order_timeinterpolation - 3 : 0;
+  // the old level
+  std::vector<Box3> obox = F->box[m];
+  std::vector<double> obx0 = F->bx0[m];
+  nrgpu_level *oL = F->L[m];
+  const long onp = oL->npoints;
+  // the new level
+  nrgpu_level *nL = nullptr;
+  int e = nrgpu_level_create(&d, &nL);
+  if (e) return e;
+  double *scr;
+  if ((e = nrgpu_level_scratch(nL, &scr))) {
+    nrgpu_level_destroy(nL);
+    return e;
+  }
+  int blk[3];
+  if (!nrgpu_level_get_block(oL, blk)) nrgpu_level_block(nL, blk[0], blk[1], blk[2]);
+  nrgpu_level_tile(nL, nrgpu_level_tile(oL, -1));
+  const long nnp = d.npoints;
+  // time levels of a parent level: u_p, u_pp and u_p2..u_p4 (evolve.c:
+  // 250-258), moved with u (move.c:930-939)
+  double *nup = nullptr, *nupp = nullptr, *nhist[3] = {nullptr, nullptr, nullptr};
+  auto fail = [&](int err) {
+    cudaFree(nup);
+    cudaFree(nupp);
+    for (int h = 0; h < 3; ++h) cudaFree(nhist[h]);
+    nrgpu_level_destroy(nL);
+    F->box[m] = obox;
+    F->bx0[m] = obx0;
+    return err;
+  };
+  if (parent_role) {
+    const size_t bytes = sizeof(double) * nv * (size_t)nnp;
+    bool ok = cudaMalloc(&nup, bytes) == cudaSuccess && cudaMalloc(&nupp, bytes) == cudaSuccess;
+    for (int h = 0; h < nh && ok; ++h) ok = cudaMalloc(&nhist[h], bytes) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      return fail(nrgpu_set_error(NRGPU_ERR_NOMEM, "time levels of the moved level %d", m));
+    }
+  }
+  F->box[m].clear();
+  F->bx0[m].clear();
+  for (int b = 0; b < d.nboxes; ++b) {
+    F->box[m].push_back(Box3{{d.box[b].m, d.box[b].n, d.box[b].o}, (long)d.box[b].noffset});
+    F->bx0[m].push_back(d.box[b].x0);
+    F->bx0[m].push_back(d.box[b].y0);
+    F->bx0[m].push_back(d.box[b].z0);
+  }
+  // the buffer sets: (parent source, old, new)
+  const long pnp = F->L[m - 1]->npoints;
+  struct Set {
+    Buffers par, old, neu;
+  };
+  std::vector<Set> sets;
+  {
+    Set u;
+    for (int v = 0; v < kMaxVars; ++v) {
+      u.par.p.p[v] = v < nv ? uparent[v] : nullptr;
+      u.old.p.p[v] = v < nv ? uold[v] : nullptr;
+      u.neu.p.p[v] = v < nv ? unew[v] : nullptr;
+    }
+    u.par.ok = u.old.ok = u.neu.ok = true;
+    sets.push_back(u);
+  }
+  if (parent_role) {
+    sets.push_back(Set{level_set(F->up[m - 1], pnp, nv), level_set(F->up[m], onp, nv), level_set(nup, nnp, nv)});
+    sets.push_back(Set{level_set(F->upp[m - 1], pnp, nv), level_set(F->upp[m], onp, nv), level_set(nupp, nnp, nv)});
+    for (int h = 0; h < nh; ++h)
+      sets.push_back(Set{level_set(F->hist[m - 1][h], pnp, nv), level_set(F->hist[m][h], onp, nv),
+                         level_set(nhist[h], nnp, nv)});
+  }
+  const int o = F->p.order_RP, b = o / 2;
+  std::vector<int *> lists;
+  for (int j = 0; j < d.nboxes && !e; ++j) {
+    const Box3 &f = F->box[m][j];
+    const double *fx0 = &F->bx0[m][3 * j];
+    // the points an old box holds are copied, the others prolonged
+    const long nfp = (long)f.n[0] * f.n[1] * f.n[2];
+    std::vector<char> held(nfp, 0);
+    for (int i = 0; i < (int)obox.size(); ++i) {
+      int io[6], in[6];
+      if (!overlap_range(obox[i], &obx0[3 * i], f, fx0, F->dx[m], io, in)) continue;
+      for (int k = in[4]; k <= in[5]; ++k)
+        for (int jj = in[2]; jj <= in[3]; ++jj)
+          for (int ii = in[0]; ii <= in[1]; ++ii) held[ii + (long)f.n[0] * (jj + (long)f.n[1] * k)] = 1;
+    }
+    std::vector<int> list;
+    for (long q = 0; q < nfp; ++q)
+      if (!held[q]) list.push_back((int)q);
+    if (list.empty()) continue;
+    const int cbi = parent_box(F, m, j);
+    if (cbi < 0) {
+      e = nrgpu_set_error(NRGPU_ERR_ARG, "moved box %d of level %d does not nest in level %d", j, m, m - 1);
+      break;
+    }
+    const Box3 &c = F->box[m - 1][cbi];
+    const double *cx0 = &F->bx0[m - 1][3 * cbi];
+    PGeom G;
+    for (int dd = 0; dd < 3; ++dd) {
+      G.fb[2 * dd] = 0;
+      G.fb[2 * dd + 1] = f.n[dd] - 1;
+      G.f0[2 * dd] = 1 << 30;
+      G.f0[2 * dd + 1] = -(1 << 30);
+      const int lo = point_index(cx0[dd], F->dx[m - 1][dd], fx0[dd], F->dx[m][dd], 0) - b + 1;
+      const int hi = point_index(cx0[dd], F->dx[m - 1][dd], fx0[dd], F->dx[m][dd], f.n[dd] - 1) + b;
+      if (lo < 0 || hi >= c.n[dd]) e = nrgpu_set_error(NRGPU_ERR_ARG, "moved level %d: boxes too small", m);
+      else if (f.n[dd] % 2 || point_index(cx0[dd], F->dx[m - 1][dd], fx0[dd], F->dx[m][dd], 0) !=
+                                  parent_index(cx0[dd], F->dx[m - 1][dd], fx0[dd], F->dx[m][dd], 0) - 1)
+        e = nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "moved level %d is not aligned with its parent's cells", m);
+      G.cs[dd] = lo;
+    }
+    if (e) break;
+    lagrange(o, o / 2.0 - 0.25, G.c1);
+    lagrange(o, o / 2.0 - 0.75, G.c2);
+    int *dl = nullptr;
+    if (cudaMalloc(&dl, sizeof(int) * list.size()) != cudaSuccess ||
+        cudaMemcpy(dl, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFree(dl);
+      e = nrgpu_set_error(NRGPU_ERR_NOMEM, "prolongation list of the moved level %d", m);
+      break;
+    }
+    lists.push_back(dl);
+    for (const Set &S : sets) {
+      if (o == 2) launch_prolong<2>(S.par.p, S.neu.p, c, f, G, dl, (int)list.size(), nv, st);
+      else if (o == 4) launch_prolong<4>(S.par.p, S.neu.p, c, f, G, dl, (int)list.size(), nv, st);
+      else launch_prolong<6>(S.par.p, S.neu.p, c, f, G, dl, (int)list.size(), nv, st);
+    }
+    if (cudaGetLastError() != cudaSuccess) e = nrgpu_set_error(NRGPU_ERR_CUDA, "prolongation of the moved level %d", m);
+  }
+  // copy what the old boxes hold (all pairs of old and new boxes)
+  for (int j = 0; j < d.nboxes && !e; ++j)
+    for (int i = 0; i < (int)obox.size() && !e; ++i) {
+      int io[6], in[6];
+      if (!overlap_range(obox[i], &obx0[3 * i], F->box[m][j], &F->bx0[m][3 * j], F->dx[m], io, in)) continue;
+      const int3 s0 = make_int3(io[0], io[2], io[4]), d0 = make_int3(in[0], in[2], in[4]);
+      const int3 n = make_int3(io[1] - io[0] + 1, io[3] - io[2] + 1, io[5] - io[4] + 1);
+      const long npts = (long)n.x * n.y * n.z;
+      for (const Set &S : sets)
+        copy_range_kernel<<<dim3((unsigned)((npts + 255) / 256), nv), 256, 0, st>>>(S.old.p, S.neu.p, obox[i],
+                                                                                      F->box[m][j], s0, d0, n, npts);
+      if (cudaGetLastError() != cudaSuccess) e = nrgpu_set_error(NRGPU_ERR_CUDA, "copy into the moved level %d", m);
+    }
+  // the old buffers are read above: the stream finishes before they go
+  if (!e && cudaStreamSynchronize(st) != cudaSuccess) e = nrgpu_set_error(NRGPU_ERR_CUDA, "regrid of level %d", m);
+  for (int *dl : lists) cudaFree(dl);
+  if (e) return fail(e);
+  nrgpu_level_destroy(oL);
+  F->L[m] = nL;
+  if (parent_role) {
+    cudaFree(F->up[m]);
+    cudaFree(F->upp[m]);
+    F->up[m] = nup;
+    F->upp[m] = nupp;
+    for (int h = 0; h < 3; ++h) {
+      cudaFree(F->hist[m][h]);
+      F->hist[m][h] = nhist[h];
+    }
+  }
   return NRGPU_OK;
 }
 
@@ -599,6 +852,9 @@ extern "C" int nrgpu_fmr_create(int nl, const nrgpu_level_desc *levels, const do
   F->gst = nullptr;
   F->ev_in = F->ev_out = nullptr;
   F->ntrack = F->track_fixz = 0;
+  F->move_fn = nullptr;
+  F->move_user = nullptr;
+  memset(F->pair_stale, 0, sizeof F->pair_stale);
   F->d_track = nullptr;
   F->d_tstatus = nullptr;
   F->nl = nl;
@@ -709,7 +965,7 @@ extern "C" int nrgpu_fmr_advance(nrgpu_fmr *F, double *const *u, int nsteps, voi
     bool steady = true;
     const int full = F->p.order_timeinterpolation - 2 > 1 ? F->p.order_timeinterpolation - 2 : 1;
     for (int l = 0; l < F->nl; ++l) steady = steady && F->iteration[l] >= full;
-    if (!F->p.use_graph || !steady) {
+    if (!F->p.use_graph || !steady || F->move_fn) {
       int e = advance(F, 0, u, st);
       if (e) return e;
       continue;
@@ -746,6 +1002,53 @@ extern "C" int nrgpu_fmr_advance(nrgpu_fmr *F, double *const *u, int nsteps, voi
       for (int q = 1; q <= l; ++q) times *= (q - 1 >= F->p.lbo) ? 2 : 1;
       F->iteration[l] += times;
     }
+  }
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_fmr_set_move(nrgpu_fmr *F, nrgpu_fmr_move_fn fn, void *user) {
+  if (!F) return nrgpu_set_error(NRGPU_ERR_ARG, "null hierarchy");
+  F->move_fn = fn;
+  F->move_user = user;
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_fmr_regrid(nrgpu_fmr *F, int lmin, int nlev, const nrgpu_level_desc *desc, double *const *u,
+                                double *const *unew, void *stream) {
+  if (!F || !desc || !u || !unew || lmin < 1 || nlev < 1 || lmin + nlev > F->nl)
+    return nrgpu_set_error(NRGPU_ERR_ARG, "bad regrid arguments (levels 1 to %d)", F ? F->nl - 1 : 0);
+  const cudaStream_t st = (cudaStream_t)stream;
+  bool moved = false;
+  for (int i = 0; i < nlev; ++i) {
+    const int m = lmin + i;
+    int e;
+    if (desc[i].nboxes > 0) {
+      if ((e = regrid_level(F, m, desc[i], u + (long)m * F->nv, unew + (long)i * F->nv, unew_or_u(F, lmin, m - 1, u,
+                                                                                                  unew, desc),
+                            st)))
+        return e;
+      F->pair_stale[m] = true;
+      if (m + 1 < F->nl) F->pair_stale[m + 1] = true;
+      moved = true;
+    }
+    if (F->pair_stale[m]) {
+      if ((e = setup_pair(F, m))) return e;
+      F->pair_stale[m] = false;
+    }
+  }
+  // a child of the last level given keeps its boxes but gets new pairs
+  const int c = lmin + nlev;
+  if (c < F->nl && F->pair_stale[c]) {
+    const int e = setup_pair(F, c);
+    if (e) return e;
+    F->pair_stale[c] = false;
+  }
+  if (moved) {
+    if (F->exec) cudaGraphExecDestroy(F->exec);
+    if (F->graph) cudaGraphDestroy(F->graph);
+    F->exec = nullptr;
+    F->graph = nullptr;
+    F->graph_u.clear();
   }
   return NRGPU_OK;
 }

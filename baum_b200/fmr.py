@@ -21,7 +21,7 @@ class Hierarchy:
     def __init__(self, levels, dt, sysparams, params=None):
         """levels: abi.Level per level, coarsest first; dt: per-level time
         steps; sysparams: per-level abi.BssnParams or abi.Z4Params."""
-        self.levels = levels
+        self.levels = list(levels)  # regrid replaces entries of this copy
         self.params = params or abi.fmr_params(
             system=abi.SYSTEM_BSSN if isinstance(sysparams[0], abi.BssnParams) else abi.SYSTEM_Z4C)
         self.nv = abi.NVARS if self.params.system == abi.SYSTEM_BSSN else abi.Z4_NVARS
@@ -58,8 +58,68 @@ class Hierarchy:
             if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous() and t.shape[0] == self.nv):
                 raise ValueError("each level state is a contiguous float64 CUDA tensor (nvars, npoints)")
         self._uptrs = abi.ptr_array(ptrs)
-        abi.check(abi.lib().nrgpu_fmr_advance(self.handle, self._uptrs, int(nsteps), _stream(stream)))
+        self.move_error = None
+        status = abi.lib().nrgpu_fmr_advance(self.handle, self._uptrs, int(nsteps), _stream(stream))
+        if self.move_error is not None:
+            raise self.move_error
+        abi.check(status)
         return u
+
+    def regrid(self, lmin, new_levels, u, stream=None):
+        """Move levels lmin.. to new boxes (nrgpu_fmr_regrid; move_box,
+        move.c:808-986): new_levels[i] is an abi.Level for level lmin + i, or
+        None to keep it.  The moved levels' states in u (the list given to
+        advance) are replaced by new tensors holding the moved data; inside
+        a move hook the pointer table of the running advance is updated
+        too."""
+        nl = len(new_levels)
+        descs = (abi.LevelDesc * nl)()
+        fresh = []
+        for i, lv in enumerate(new_levels):
+            if lv is None:
+                descs[i].nboxes = 0
+                fresh.append(None)
+            else:
+                descs[i] = lv.desc
+                fresh.append(torch.empty((self.nv, lv.npoints), dtype=torch.float64, device="cuda"))
+        cur = [t.data_ptr() + v * t.stride(0) * 8 for t in u for v in range(self.nv)]
+        new = []
+        for t in fresh:
+            new += [0] * self.nv if t is None else [t.data_ptr() + v * t.stride(0) * 8 for v in range(self.nv)]
+        self._keep = (descs, new_levels)
+        # inside a move hook the stream arrives as the raw handle
+        st = C.c_void_p(stream) if isinstance(stream, int) else _stream(stream)
+        abi.check(abi.lib().nrgpu_fmr_regrid(self.handle, int(lmin), nl, descs, abi.ptr_array(cur),
+                                             abi.ptr_array(new), st))
+        for i, t in enumerate(fresh):
+            if t is None:
+                continue
+            l = lmin + i
+            u[l] = t
+            self.levels[l] = new_levels[i]
+            if self._uptrs is not None:
+                for v in range(self.nv):
+                    self._uptrs[l * self.nv + v] = t.data_ptr() + v * t.stride(0) * 8
+        return u
+
+    def set_move(self, fn):
+        """fn(l, stream) is called where the reference calls move_box(g, l)
+        during advance (nrgpu_fmr_set_move); it may call regrid(l.., ...) on
+        the list being advanced.  None removes it."""
+        if fn is None:
+            self._move = None
+            abi.check(abi.lib().nrgpu_fmr_set_move(self.handle, None, None))
+            return
+
+        def hook(user, fmr, l, stream):
+            try:
+                fn(int(l), stream)
+                return 0
+            except Exception as e:  # reported as an error of the advance
+                self.move_error = e
+                return -1  # NRGPU_ERR_ARG
+        self._move = abi.FMR_MOVE_FN(hook)
+        abi.check(abi.lib().nrgpu_fmr_set_move(self.handle, C.cast(self._move, C.c_void_p), None))
 
     def iteration(self, l):
         return abi.lib().nrgpu_fmr_iteration(self.handle, l)

@@ -374,6 +374,43 @@ int nrgpu_fmr_load(nrgpu_fmr *fmr, const void *host, size_t bytes);
 int nrgpu_fmr_track(nrgpu_fmr *fmr, int n, const double *pos, int fixz);
 int nrgpu_fmr_punctures(nrgpu_fmr *fmr, double *pos, int *status);
 
+/* Moving boxes (move_box, main/amr/move.c:808-986).  A level moves by a
+ * regrid: the caller gives the level's new boxes (same spacing, each made of
+ * whole cells of a box of the parent, as make_level_bboxes builds them,
+ * box.c:465-560) and new state buffers; the library moves every time level
+ * of the level (the state u, and on a level with a child the previous step,
+ * the time interpolant and the older time levels of order_timeinterpolation
+ * 4-6) as move_overlap does (move.c:712-800): the points that an old box of
+ * the level also holds are copied from it, all others are prolonged from
+ * the parent at order_RP (prolong_varlist, interpolate_boxtobox_N.c:
+ * 870-1010, into the points that no old box holds).  The refinement flags
+ * and pairs with the parent, and with the child, are set up again.
+ *
+ * nrgpu_fmr_regrid moves levels lmin .. lmin + nlev - 1 (lmin >= 1),
+ * coarsest first so that each prolongs from its parent's new state:
+ * desc[i] holds level lmin + i's new boxes, or nboxes = 0 to keep the level
+ * (its pairs are still set up again when its parent moved); u is the
+ * caller's table of all levels' current state pointers (nlevels * nvars),
+ * unew[i * nvars + v] the new buffers of level lmin + i (desc[i].npoints
+ * points each; ignored for kept levels).  It waits for the stream; the
+ * caller then puts unew into its table and frees the old buffers.
+ *
+ * nrgpu_fmr_set_move installs a hook that nrgpu_fmr_advance calls where the
+ * reference calls move_box(g, l) (main/main/main.c:428): after level l - 1,
+ * its sublevels, their restriction and prolongation and the puncture
+ * tracking are done, when level l - 1 is not aligned in time with its own
+ * parent (or l = 1).  The hook decides which of the levels l .. nlevels-1
+ * move (find_nested_bboxes, move.c:121-463, is the reference's rule; the
+ * tracked positions come from nrgpu_fmr_punctures), calls nrgpu_fmr_regrid
+ * on `stream`, updates the pointer table that it gave to nrgpu_fmr_advance
+ * (the advance reads the table after the hook returns) and returns 0, or
+ * an error code that ends the advance.  With a hook, coarse steps run
+ * without the CUDA graph.  fn = NULL removes the hook. */
+typedef int (*nrgpu_fmr_move_fn)(void *user, nrgpu_fmr *fmr, int l, void *stream);
+int nrgpu_fmr_set_move(nrgpu_fmr *fmr, nrgpu_fmr_move_fn fn, void *user);
+int nrgpu_fmr_regrid(nrgpu_fmr *fmr, int lmin, int nlev, const nrgpu_level_desc *desc, double *const *u,
+                     double *const *unew, void *stream);
+
 /* the evolution systems */
 enum { NRGPU_SYSTEM_BSSN = 0, NRGPU_SYSTEM_Z4C = 1 };
 

@@ -179,16 +179,18 @@ def build_gpu_variant(ref, a, base, obj, entry, lib):
     for src, o, inc in [(os.path.join(ref, "src/main/main/main.c"), main_o, os.path.join(ref, "src/main/main")),
                         (os.path.join(repo, "baum_b200", "bam", "nrgpu_bam.c"), bind_o,
                          os.path.join(ref, "src/projects/bssn"))]:
-        r = subprocess.run(bgen + ["-I" + inc, "-DNRGPU_WRAP_MULTIGRID", "-c", src, "-o", o], capture_output=True,
-                           text=True)
+        r = subprocess.run(bgen + ["-I" + inc, "-DNRGPU_WRAP_MULTIGRID", "-DNRGPU_WRAP_MOVE_BOX", "-c", src, "-o", o],
+                           capture_output=True, text=True)
         if r.returncode:
             print(r.stderr[-4000:])
             return 1
     cuda = "/usr/local/cuda/lib64"
     exe = os.path.join(OUT, "bam_gpu")
     # --wrap=multigrid: PickEllipticSolver's pointer to multigrid() lands on
-    # the module's __wrap_multigrid (device solve under nrgpu_multigrid = yes)
-    r = subprocess.run([a.cc, "-fopenmp", "-o", exe, main_o, bind_o, "-Wl,--wrap=multigrid",
+    # the module's __wrap_multigrid (device solve under nrgpu_multigrid = yes);
+    # --wrap=move_box: main.c's move_box lands on __wrap_move_box (the device
+    # moves the boxes in nrgpu_mode = fmr)
+    r = subprocess.run([a.cc, "-fopenmp", "-o", exe, main_o, bind_o, "-Wl,--wrap=multigrid", "-Wl,--wrap=move_box",
                         "-Wl,--start-group", lib, "-Wl,--end-group",
                         "-L" + os.path.dirname(so), "-lnrgpu", "-Wl,-rpath,$ORIGIN/../../baum_b200",
                         "-L" + cuda, "-lcudart", "-Wl,-rpath," + cuda, "-lm"], capture_output=True, text=True)

@@ -131,13 +131,20 @@ bssn_shiftdriver = 2.0
 bssn_shiftgammacoeff = 0.75""")
 
 
+# the single-puncture grid with moving boxes: amr_move_force = 4 moves the
+# puncture along x at speed amr_move_force_o (move.c:187-192), and level 2's
+# box follows it by one level-1 cell at t = 0.1875 (level 2's 6th step)
+MOVING = (("amr = bo newfmr", "amr = bo newfmr move\namr_move_force = 4\namr_move_force_o = 1.5\n"
+                              "amr_verbose = move"),)
+
+
 def run_fmr(binary, extra_physics, extra, grid="single", keep=None):
     """Dumps of every level after 2 coarse steps and the run's stdout; with
     keep, a list of output files (matched by name anywhere in the run
     directory) whose text is also returned."""
     work = tempfile.mkdtemp(prefix="bamgpu_")
     par = FMR_PAR
-    for a, b in (BINARY if grid == "binary" else BSSN_FMR if grid == "bssn" else ()):
+    for a, b in {"binary": BINARY, "bssn": BSSN_FMR, "moving": MOVING}.get(grid, ()):
         assert a in par
         par = par.replace(a, b)
     try:
@@ -158,7 +165,7 @@ def run_fmr(binary, extra_physics, extra, grid="single", keep=None):
         shutil.rmtree(work, ignore_errors=True)
 
 
-@pytest.mark.parametrize("grid", ["single", "binary", "bssn"])
+@pytest.mark.parametrize("grid", ["single", "binary", "bssn", "moving"])
 def test_bam_fmr_mode_matches_bam(gpu, cpu_state, grid):
     """nrgpu_mode = fmr: the whole Berger-Oliger step of the 3-level Z4c grid
     on the GPU at level 0's EVOLVE hook.  BAM dumps every level right after
@@ -168,13 +175,24 @@ def test_bam_fmr_mode_matches_bam(gpu, cpu_state, grid):
     are compared, after 2 coarse steps, on the points that this last
     restriction and prolongation do not write, within the refinement
     tolerance of the oracle pin (2e-11).  The binary's grid has two boxes
-    on level 2; "bssn" runs the BSSN system on the single-puncture grid."""
+    on level 2; "bssn" runs the BSSN system on the single-puncture grid;
+    "moving" moves level 2's box once during the run (amr = bo newfmr move,
+    forced motion), BAM on the host and the device hierarchy inside its
+    coarse step, and the moved box is compared too."""
     from baum_b200 import abi
     from oracle import oracle
-    ref, _ = run_fmr(BAM, "", "", grid)
+    ref, ref_out = run_fmr(BAM, "", "", grid)
     algcon = "bssn_register_algcon = no" if grid == "bssn" else "z4_register_algcon = no"
     got, out = run_fmr(BAM_GPU, " nrgpu", "nrgpu_mode = fmr\n" + algcon, grid)
     assert "nrgpu: fmr mode" in out
+    if grid == "moving":
+        assert "moving box(es) on level 2" in ref_out
+        assert out.count("nrgpu: moved 1 level(s) from level 2 on") == ref_out.count("moving box(es) on level 2")
+        for a, b in zip(got, ref):
+            assert np.array_equal(np.asarray(a["boxes"]), np.asarray(b["boxes"]))
+        # the box moved: its origin differs from the unmoved run's
+        still, _ = run_fmr(BAM, "", "", "single")
+        assert not np.array_equal(np.asarray(ref[2]["boxes"]), np.asarray(still[2]["boxes"]))
     levels = []
     for d in ref:
         levels.append(abi.Level([(int(b[0]), int(b[1]), int(b[2]), b[4], b[5], b[6]) for b in d["boxes"]],
