@@ -27,6 +27,7 @@ class Hierarchy:
         self.nv = abi.NVARS if self.params.system == abi.SYSTEM_BSSN else abi.Z4_NVARS
         nl = len(levels)
         self._descs = (abi.LevelDesc * nl)(*[lv.desc for lv in levels])
+        self.dt = list(dt)
         self._dt = (C.c_double * nl)(*dt)
         self._sp = (type(sysparams[0]) * nl)(*sysparams)
         h = C.c_void_p()

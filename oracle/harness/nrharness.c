@@ -15,6 +15,8 @@
  *   3. nrharness_dump = "i0 i1 ...": dump the evolved variables of every
  *      level after those level iterations (POST_EVOLVE), and after the
  *      initial data when 0 is listed.
+ *   5. nrharness_dump_moved = yes: dump every level that move_box moved,
+ *      after the move (POST_MOVEBOX), as moved_itN_lL.bin.
  *   4. nrharness_track = yes: with each of those dumps, run the reference's
  *      shift-integration puncture tracker (track_moving_puncture_integrate,
  *      Gauge/moving_punctures_integrate.c:29-100) from every start position
@@ -228,6 +230,22 @@ int nrharness_post_evolve(tL *level)
   return 0;
 }
 
+/* after move_box (main.c:428-435, POST_MOVEBOX on every moved level): the
+   moved level's state, the state at the end of the coarse step for a level
+   that moved after its last POST_EVOLVE */
+int nrharness_post_movebox(tL *level)
+{
+  tVarList *u = 0;
+  char tag[64];
+  if (!Getv("nrharness_dump_moved", "yes")) return 0;
+  evolve_vlretrieve(&u, 0, 0);
+  if (!u) return 0;
+  u->level = level;
+  snprintf(tag, sizeof tag, "moved_it%d", level->iteration);
+  dump_varlist(level, u, tag);
+  return 0;
+}
+
 /* the reference's trackers and the globals of moving_punctures.c:13-14 */
 int track_moving_puncture_integrate(tL *level, int np, double *pold, double *pnew);
 int track_moving_puncture_extremum(tL *level, int np, double *pold, double *pnew);
@@ -336,4 +354,6 @@ void bam_nrharness(void)
   AddPar("nrharness_length", "16", "box length that sets the wave numbers");
   AddFun(POST_INITIALDATA, nrharness_post_initialdata, "oracle harness: synthetic data and dumps");
   AddFun(POST_EVOLVE, nrharness_post_evolve, "oracle harness: dumps");
+  AddPar("nrharness_dump_moved", "no", "dump every level that move_box moved, after the move [no,yes]");
+  AddFun(POST_MOVEBOX, nrharness_post_movebox, "oracle harness: dumps of moved levels");
 }

@@ -7,6 +7,7 @@ variable after the run agrees within 1e-12 relative.  Two modes:
 RK4, vladd and algcon), "resident" runs the whole RK4 step + algcon on the
 GPU at the EVOLVE hook."""
 import os
+import re
 import shutil
 import subprocess
 import tempfile
@@ -330,3 +331,68 @@ def test_bam_z4_with_the_gpu_path_matches_bam(gpu, cpu_state, grid, mode, extra)
     got, out = run_z4(BAM_GPU, " nrgpu", grid, extra)
     assert "nrgpu: %s mode" % mode in out
     assert relerr(got, ref).max() < 1e-12
+
+
+def run_moving(binary, extra_physics, extra):
+    """tests/test_moving_policy.py's 4-level grid with two puncture boxes
+    on the forced circular motion, 2 coarse steps: the run's stdout and,
+    per level, the dump after its last step and the dump after its last
+    move, if it moved after that step (nrharness_dump_moved)."""
+    from test_moving_policy import MOVING_PAR
+    work = tempfile.mkdtemp(prefix="bamgpu_")
+    try:
+        with open(os.path.join(work, "t.par"), "w") as f:
+            f.write(MOVING_PAR % (extra_physics, extra))
+        r = subprocess.run([binary, "-nt", "4", "t.par"], cwd=work, capture_output=True, text=True, timeout=900)
+        assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+        state, moved = [], []
+        for l in range(4):
+            it = 2 * 2 ** l
+            state.append(dumpfile.read(os.path.join(work, "state_it%d_l%d.bin" % (it, l))))
+            fn = os.path.join(work, "moved_it%d_l%d.bin" % (it, l))
+            moved.append(dumpfile.read(fn) if os.path.exists(fn) else None)
+        return state, moved, r.stdout
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+def test_bam_fmr_mode_moving_cascade_matches_bam(gpu, cpu_state):
+    """Moving boxes inside the device's coarse step against BAM's own
+    move_box: 4 levels, two puncture boxes on level 3 and joined boxes
+    below, every level following the forced motion, 2 coarse steps with
+    12 moves (cascades from level 1 at the end of each coarse step and
+    moves of level 3 within it).  The module's hook decides with BAM's
+    find_nested_bboxes and make_level_bboxes and moves the device data with
+    nrgpu_fmr_regrid.  After the run every level has the reference's boxes;
+    the levels that moved at the end of the last coarse step are compared
+    at every point with the reference's state after that move, level 0 on
+    the points that the last restriction does not write; tolerance
+    2e-11 x 4^level (workloads.level_tolerance)."""
+    from baum_b200 import abi, workloads
+    from oracle import oracle
+    ref, ref_moved, ref_out = run_moving(BAM, "", "")
+    got, _, out = run_moving(BAM_GPU, " nrgpu", "nrgpu_mode = fmr\nz4_register_algcon = no")
+    assert "nrgpu: fmr mode" in out
+    nref = len(re.findall(r"(moving|setting) box\(es\) on level", ref_out))
+    ngot = sum(int(x) for x in re.findall(r"nrgpu: moved (\d+) level", out))
+    assert nref >= 10 and ngot == nref, (ngot, nref)
+    for l in range(4):
+        want = ref_moved[l] if ref_moved[l] is not None else ref[l]
+        assert np.array_equal(np.asarray(got[l]["boxes"]), np.asarray(want["boxes"])), l
+        tol = workloads.level_tolerance(l)
+        if ref_moved[l] is not None:
+            a, b = got[l]["data"], want["data"]
+            err = np.abs(a - b).max(axis=1) / np.maximum(np.abs(b).max(axis=1), 1e-8)
+            assert err.max() < tol, (l, err.max())
+            continue
+        # level 0: its restricted points come from level 1 before level 1's last move
+        lv = [abi.Level([(int(b[0]), int(b[1]), int(b[2]), b[4], b[5], b[6]) for b in d["boxes"]],
+                        float(d["dx"]), d["boundary"]) for d in (ref[l], ref[l + 1])]
+        uc = np.zeros((1, lv[0].npoints))
+        uf = np.ones((1, lv[1].npoints))
+        oracle.fmr_restrict_prolong(lv[0], lv[1], uc, uf, 4, 3)
+        keep = uc[0] < 0.5
+        a, b = got[l]["data"][:, keep], ref[l]["data"][:, keep]
+        err = np.abs(a - b).max(axis=1) / np.maximum(np.abs(b).max(axis=1), 1e-8)
+        assert keep.sum() > 0.3 * lv[0].npoints
+        assert err.max() < tol, (l, err.max())
