@@ -403,6 +403,59 @@ def gpu_fmr(steps=2, variants=(("graph", 1, 1), ("launches", 0, 1), ("graph_untu
     return out
 
 
+def gpu_fmr_moving(steps=1, warm=1, order=6, omega=0.3, radius=1.0):
+    """The full form's grid with moving boxes: 9 nested 2:1 levels, level 0
+    a 192^3-inner box (dx 0.5), levels 1-4 the fixed 136^3 cubes about the
+    origin (amr_move_lcube = 4), levels 5-8 a 72^3 box around each of two
+    punctures (amr_nxyz = 192 128 128 128 128 64), which follow the forced
+    circular motion amr_move_force = 3 (radius 1, angular velocity 0.3;
+    Fourier data carry no punctures to track).  Z4c 6th order + KO6.  The
+    boxes move where the reference's move_box would (baum_b200/moving.py,
+    nrgpu_fmr_regrid); coarse steps run without the CUDA graph."""
+    import torch
+    from baum_b200 import abi, fmr, moving, workloads
+    nxyz = [192, 128, 128, 128, 128, 64]
+    sizes = lambda lp: moving.box_size(lp, 192, lcube=4, nxyz_list=nxyz)  # noqa: E731
+    pos = moving.circle_positions(radius, omega)
+    levels = fmr.nested_levels([194], C5_DX0)
+    for lp in range(8):
+        h = levels[lp].dx
+        boxes, ibox = moving.nested_bboxes(h, sizes(lp), pos(0.0), moving=lp + 1 > 4)
+        levels.append(moving.level_of_bboxes(boxes, ibox, h))
+    params = [abi.z4_params_from_par(dissfactor=(0.1 if l == 0 else 0.02) / 64, order_centered=order,
+                                     order_advection=order) for l in range(9)]
+    dt = [0.25 * C5_DX0 / 2 ** l for l in range(9)]
+    H = fmr.Hierarchy(levels, dt, params, abi.fmr_params(use_graph=1, autotune=1))
+    policy = moving.MovingBoxes(H, pos, sizes, lcube=4)
+    u = [workloads.fmr_state_device(lev) for lev in levels]
+    policy.u = u
+    H.set_move(policy.hook)
+    for _ in range(warm):
+        H.advance(u, 1)
+    torch.cuda.synchronize()
+    nmoves0 = len(policy.moves)
+    upd = sum(int((H.levels[l].boundary == 0).sum()) * 4 * 2 ** l for l in range(9))
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    H.advance(u, steps)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / steps
+    out = {"workload": "9 levels: 194^3 (dx 0.5), 4 fixed 136^3 cubes, 4 levels of two 72^3 puncture boxes on "
+                       "a forced circular motion (radius %.3g, omega %.3g), Z4c %s order + KO6" %
+                       (radius, omega, "6th" if order == 6 else "4th"),
+           "ms_per_coarse_step": ms, "rhs_point_updates_per_coarse_step_at_end": upd,
+           "value": upd / (ms * 1e-3), "unit": UNIT,
+           "moves_per_coarse_step": (len(policy.moves) - nmoves0) / steps,
+           "levels_moved_per_coarse_step": sum(sum(x is not None for x in m[2]) for m in policy.moves[nmoves0:]) /
+           steps,
+           "boxes_per_level_at_end": [H.levels[l].desc.nboxes for l in range(9)],
+           "finite": all(bool(torch.isfinite(t).all()) for t in u)}
+    H.set_move(None)
+    H.close()
+    return out
+
+
 FMR_REF_PAR = """physics = adm z4 nrharness
 adm_data = Minkowski
 z4_lapse = 1+log withshift
@@ -1001,7 +1054,9 @@ def main():
         torch.cuda.set_device(0)
         r = gpu_fmr(args.steps, variants=(("graph", 1, 1),), warm=max(args.warmup, 2), sizes=C5_SIZES,
                     dx0=C5_DX0, order=6)
-        r["note"] = "static boxes: the full form's moving boxes and warm-started initial data are not built"
+        r["note"] = "static boxes (value); moving: the same depth with moving puncture boxes on the finest levels"
+        torch.cuda.empty_cache()
+        r["moving"] = gpu_fmr_moving(max(1, args.steps), 1)
         print(json.dumps({"case": "c5", **r}))
         return
     if args.case == "mg":

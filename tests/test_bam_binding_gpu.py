@@ -363,11 +363,14 @@ def test_bam_fmr_mode_moving_cascade_matches_bam(gpu, cpu_state):
     12 moves (cascades from level 1 at the end of each coarse step and
     moves of level 3 within it).  The module's hook decides with BAM's
     find_nested_bboxes and make_level_bboxes and moves the device data with
-    nrgpu_fmr_regrid.  After the run every level has the reference's boxes;
-    the levels that moved at the end of the last coarse step are compared
-    at every point with the reference's state after that move, level 0 on
-    the points that the last restriction does not write; tolerance
-    2e-11 x 4^level (workloads.level_tolerance)."""
+    nrgpu_fmr_regrid.  After the run every level has the reference's boxes
+    and the reference's state: after its last move for the levels that
+    moved at the end of the last coarse step, else after its last step.
+    The points compared are those that no restriction or prolongation
+    writes after the reference's dump (with the GPU hook BAM's host
+    recursion still runs its own restriction and prolongation on the host
+    arrays, from time levels it never computed); tolerance 2e-11 x 4^level
+    (workloads.level_tolerance)."""
     from baum_b200 import abi, workloads
     from oracle import oracle
     ref, ref_moved, ref_out = run_moving(BAM, "", "")
@@ -376,23 +379,28 @@ def test_bam_fmr_mode_moving_cascade_matches_bam(gpu, cpu_state):
     nref = len(re.findall(r"(moving|setting) box\(es\) on level", ref_out))
     ngot = sum(int(x) for x in re.findall(r"nrgpu: moved (\d+) level", out))
     assert nref >= 10 and ngot == nref, (ngot, nref)
+    final = [m if m is not None else d for m, d in zip(ref_moved, ref)]
+    assert sum(m is not None for m in ref_moved) >= 2
+
+    def level(d):
+        return abi.Level([(int(b[0]), int(b[1]), int(b[2]), b[4], b[5], b[6]) for b in d["boxes"]],
+                         float(d["dx"]), d["boundary"])
+
+    lv = [level(d) for d in final]
+    keep = [np.ones(x.npoints, dtype=bool) for x in lv]
+    for l in range(1, 4):
+        uf = np.ones((1, lv[l].npoints))
+        oracle.fmr_restrict_prolong(lv[l - 1], lv[l], np.zeros((1, lv[l - 1].npoints)), uf, 4, 3)
+        keep[l] &= uf[0] > 0.5  # prolonged buffer points
+        # restricted points of the parent: from the child's boxes before its
+        # last move (the reference's restriction) and after it (the host's)
+        for child in (level(ref[l]), lv[l]):
+            uc = np.zeros((1, lv[l - 1].npoints))
+            oracle.fmr_restrict_prolong(lv[l - 1], child, uc, np.ones((1, child.npoints)), 4, 3)
+            keep[l - 1] &= uc[0] < 0.5
     for l in range(4):
-        want = ref_moved[l] if ref_moved[l] is not None else ref[l]
-        assert np.array_equal(np.asarray(got[l]["boxes"]), np.asarray(want["boxes"])), l
-        tol = workloads.level_tolerance(l)
-        if ref_moved[l] is not None:
-            a, b = got[l]["data"], want["data"]
-            err = np.abs(a - b).max(axis=1) / np.maximum(np.abs(b).max(axis=1), 1e-8)
-            assert err.max() < tol, (l, err.max())
-            continue
-        # level 0: its restricted points come from level 1 before level 1's last move
-        lv = [abi.Level([(int(b[0]), int(b[1]), int(b[2]), b[4], b[5], b[6]) for b in d["boxes"]],
-                        float(d["dx"]), d["boundary"]) for d in (ref[l], ref[l + 1])]
-        uc = np.zeros((1, lv[0].npoints))
-        uf = np.ones((1, lv[1].npoints))
-        oracle.fmr_restrict_prolong(lv[0], lv[1], uc, uf, 4, 3)
-        keep = uc[0] < 0.5
-        a, b = got[l]["data"][:, keep], ref[l]["data"][:, keep]
+        assert np.array_equal(np.asarray(got[l]["boxes"]), np.asarray(final[l]["boxes"])), l
+        a, b = got[l]["data"][:, keep[l]], final[l]["data"][:, keep[l]]
         err = np.abs(a - b).max(axis=1) / np.maximum(np.abs(b).max(axis=1), 1e-8)
-        assert keep.sum() > 0.3 * lv[0].npoints
-        assert err.max() < tol, (l, err.max())
+        assert keep[l].sum() > 0.2 * lv[l].npoints, l
+        assert err.max() < workloads.level_tolerance(l), (l, err.max())
