@@ -360,6 +360,10 @@ def lib():
         "nrgpu_fmr_track": (C.c_int, [vp, C.c_int, C.POINTER(C.c_double), C.c_int]),
         "nrgpu_fmr_punctures": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
         "nrgpu_fmr_set_move": (C.c_int, [vp, vp, vp]),
+        "nrgpu_fmr_restrict_prolong_vars": (C.c_int, [vp, C.c_int, C.c_int, pp, pp, vp]),
+        "nrgpu_adm_mass_integrands": (C.c_int, [vp, pp, vp, vp, pp, vp]),
+        "nrgpu_sphere_integral": (C.c_int, [vp, vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+                                            C.c_int, C.c_int, C.POINTER(C.c_double), vp]),
         "nrgpu_fmr_regrid": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(LevelDesc), pp, pp, vp]),
         "nrgpu_track_punctures": (C.c_int, [vp, pp, pp, C.c_double, C.c_int, C.c_int, C.c_int, vp, vp, vp]),
         "nrgpu_track_punctures_extremum": (C.c_int, [vp, vp, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, vp, vp,

@@ -90,3 +90,48 @@ def computeadmconstraints(dl, u, order_centered, mode=PLAIN, chipsipower=-4.0, s
     adm_constraints_N(dl, con, adm, order_centered, mode, stream)
     n2, ni = norms(dl, con, stream)
     return adm, con, {name: (n2[i], ni[i]) for i, name in enumerate(CON_VARS[:con.shape[0]])}
+
+
+MASS_VARS = ["ADM_mass_integrand", "ADM_mass_integrand_chi", "ADM_mass_Pxint", "ADM_mass_Pyint",
+             "ADM_mass_Pzint", "ADM_mass_Jxint", "ADM_mass_Jyint", "ADM_mass_Jzint"]
+
+
+def adm_mass_integrands(dl, uadm, trK, chi, out=None, stream=None):
+    """The eight integrands of ADM_mass (ADM_mass.c:80-87) into out (8,
+    npoints; zero where not computed when out is None) at the flag-0 points,
+    from the ADM metric and curvature uadm (12, npoints) and the evolved
+    trace K and chi (npoints each)."""
+    out = torch.zeros((8, dl.level.npoints), dtype=torch.float64, device="cuda") if out is None else out
+    for t in (trK, chi):
+        if not (t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+            raise ValueError("trK and chi are contiguous float64 CUDA tensors")
+    abi.check(abi.lib().nrgpu_adm_mass_integrands(dl.handle, _ptrs(uadm, 12), C.c_void_p(trK.data_ptr()),
+                                                  C.c_void_p(chi.data_ptr()), _ptrs(out, 8), _stream(stream)))
+    return out
+
+
+def integral_over_sphere(dl, f, r, ntheta, nphi, order, center=(0.0, 0.0, 0.0), stream=None):
+    """integral_over_sphere_Simpson (Integral_over_sphere.c:197-357) of the
+    level array f (npoints) over the sphere of radius r; 0 when a point of
+    the sphere cannot be interpolated on the level."""
+    res = C.c_double()
+    abi.check(abi.lib().nrgpu_sphere_integral(dl.handle, C.c_void_p(f.data_ptr()), float(center[0]),
+                                              float(center[1]), float(center[2]), float(r), int(ntheta), int(nphi),
+                                              int(order), C.byref(res), _stream(stream)))
+    return res.value
+
+
+def sphere_safely_inside(level, r, order_RP):
+    """centered_sphere_safely_inside_level (main/amr/points.c:188-250): a
+    one-box level whose bounding box (mirrored about the symmetry planes)
+    holds the sphere of radius r + order_RP dx about the origin."""
+    if len(level.boxes) > 1:
+        return False
+    b = level.boxes[0]
+    rr = r + order_RP * level.dx
+    lo = [b.x0, b.y0, b.z0]
+    hi = [b.x0 + (b.m - 1) * level.dx, b.y0 + (b.n - 1) * level.desc.dy, b.z0 + (b.o - 1) * level.desc.dz]
+    for d in range(3):
+        if level.desc.symmetry >> d & 1:
+            lo[d] = -hi[d]
+    return all(not (-rr < lo[d] - 1e-10 or hi[d] < rr - 1e-10) for d in range(3))

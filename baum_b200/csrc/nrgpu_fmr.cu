@@ -455,12 +455,13 @@ int fill(Ptrs *P, double *const *u, int nv) {
 
 // restrict_prolong_varlist between level l and its parent (nbuffer 3):
 // every pair restricted, then every pair prolonged (inject.c:63-100)
-int restrict_prolong(nrgpu_fmr *F, int l, const Ptrs &uc, const Ptrs &uf, cudaStream_t st) {
+int restrict_prolong(nrgpu_fmr *F, int l, const Ptrs &uc, const Ptrs &uf, cudaStream_t st, int nvars = -1) {
   const int o = F->p.order_RP;
+  const int nv = nvars < 0 ? F->nv : nvars;
   for (const FmrPair &P : F->pairs[l]) {
     if (!P.has_r) continue;
     const Box3 &cb = F->box[l - 1][P.cbox], &fb = F->box[l][P.fbox];
-    const dim3 g((P.nr + 127) / 128, F->nv);
+    const dim3 g((P.nr + 127) / 128, nv);
     if (o == 2) restrict_kernel<2><<<g, 128, 0, st>>>(uc, uf, cb, fb, P.rg, P.nr);
     else if (o == 4) restrict_kernel<4><<<g, 128, 0, st>>>(uc, uf, cb, fb, P.rg, P.nr);
     else restrict_kernel<6><<<g, 128, 0, st>>>(uc, uf, cb, fb, P.rg, P.nr);
@@ -469,7 +470,7 @@ int restrict_prolong(nrgpu_fmr *F, int l, const Ptrs &uc, const Ptrs &uf, cudaSt
   for (const FmrPair &P : F->pairs[l]) {
     if (!P.has_p) continue;
     const Box3 &cb = F->box[l - 1][P.cbox], &fb = F->box[l][P.fbox];
-    const dim3 g((P.npro + 127) / 128, F->nv);
+    const dim3 g((P.npro + 127) / 128, nv);
     if (o == 2) prolong_kernel<2><<<g, 128, 0, st>>>(uc, uf, cb, fb, P.pg, P.d_plist, P.npro);
     else if (o == 4) prolong_kernel<4><<<g, 128, 0, st>>>(uc, uf, cb, fb, P.pg, P.d_plist, P.npro);
     else prolong_kernel<6><<<g, 128, 0, st>>>(uc, uf, cb, fb, P.pg, P.d_plist, P.npro);
@@ -942,6 +943,20 @@ extern "C" int nrgpu_fmr_restrict_prolong(nrgpu_fmr *F, int lfine, double *const
   int e;
   if ((e = fill(&C, uc, F->nv)) || (e = fill(&P, uf, F->nv))) return e;
   return restrict_prolong(F, lfine, C, P, (cudaStream_t)stream);
+}
+
+extern "C" int nrgpu_fmr_restrict_prolong_vars(nrgpu_fmr *F, int lfine, int nvars, double *const *uc,
+                                               double *const *uf, void *stream) {
+  if (!F || !uc || !uf || lfine < 1 || lfine >= F->nl || nvars < 1 || nvars > kMaxVars)
+    return nrgpu_set_error(NRGPU_ERR_ARG, "bad arguments (1 <= nvars <= %d)", kMaxVars);
+  Ptrs C, P;
+  for (int v = 0; v < kMaxVars; ++v) {
+    C.p[v] = v < nvars ? uc[v] : nullptr;
+    P.p[v] = v < nvars ? uf[v] : nullptr;
+  }
+  for (int v = 0; v < nvars; ++v)
+    if (!uc[v] || !uf[v]) return nrgpu_set_error(NRGPU_ERR_ARG, "null variable pointer %d", v);
+  return restrict_prolong(F, lfine, C, P, (cudaStream_t)stream, nvars);
 }
 
 extern "C" int nrgpu_fmr_block(nrgpu_fmr *F, int l, int *block) {

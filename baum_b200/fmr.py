@@ -52,6 +52,14 @@ class Hierarchy:
         abi.check(abi.lib().nrgpu_fmr_restrict_prolong(self.handle, lfine, _ptrs(uc, self.nv), _ptrs(uf, self.nv),
                                                        _stream(stream)))
 
+    def restrict_prolong_vars(self, lfine, uc, uf, stream=None):
+        """restrict_prolong_varlist with nbuffer 3 on other variables
+        (set_boundary_refinement_cf, inject.c:179-189): uc, uf of shape
+        (nvars, npoints) on levels lfine - 1 and lfine."""
+        nv = uc.shape[0]
+        abi.check(abi.lib().nrgpu_fmr_restrict_prolong_vars(self.handle, int(lfine), nv, _ptrs(uc, nv),
+                                                            _ptrs(uf, nv), _stream(stream)))
+
     def advance(self, u, nsteps=1, stream=None):
         """nsteps coarse steps of the per-level states u (list of tensors)."""
         ptrs = [t.data_ptr() + v * t.stride(0) * 8 for t in u for v in range(self.nv)]

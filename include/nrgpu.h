@@ -336,6 +336,11 @@ int nrgpu_fmr_flags(nrgpu_fmr *fmr, int l, double *flagprolong, double *flagrest
  * lfine and its parent: restrict lfine's uf into uc, then prolong uc into
  * lfine's buffer zone (nvars device pointers each) */
 int nrgpu_fmr_restrict_prolong(nrgpu_fmr *fmr, int lfine, double *const *uc, double *const *uf, void *stream);
+/* the same for a list of nvars (<= 25) other variables, as
+ * set_boundary_refinement_cf (main/amr/inject.c:179-189) applies it to
+ * analysis fields (the ADM mass integrands, ADM_mass.c:103-104) */
+int nrgpu_fmr_restrict_prolong_vars(nrgpu_fmr *fmr, int lfine, int nvars, double *const *uc, double *const *uf,
+                                    void *stream);
 /* nsteps coarse steps of the hierarchy; u holds nlevels * nvars device
  * pointers, level-major.  The caller keeps the same u for a run. */
 int nrgpu_fmr_advance(nrgpu_fmr *fmr, double *const *u, int nsteps, void *stream);
@@ -410,6 +415,32 @@ typedef int (*nrgpu_fmr_move_fn)(void *user, nrgpu_fmr *fmr, int l, void *stream
 int nrgpu_fmr_set_move(nrgpu_fmr *fmr, nrgpu_fmr_move_fn fn, void *user);
 int nrgpu_fmr_regrid(nrgpu_fmr *fmr, int lmin, int nlev, const nrgpu_level_desc *desc, double *const *u,
                      double *const *unew, void *stream);
+
+/* ---- analysis: ADM mass, momentum and angular momentum ---------------------
+ * ADM_mass (projects/ADM_mass/ADM_mass.c:11-225).  nrgpu_adm_mass_integrands
+ * writes its eight integrands at the flag-0 points of a level (the other
+ * points are left as they are): out[0] the ADM mass (adm_mass_integrand.c),
+ * out[1] the mass from chi alone (adm_mass_integrand_chi.c), out[2..4] Px,
+ * Py, Pz and out[5..7] Jx, Jy, Jz (adm_pj_integrand.c).  gK holds 12 device
+ * arrays, the ADM metric gxx..gzz and curvature Kxx..Kzz (nrgpu_to_adm);
+ * trK is the evolved trace K, chi the conformal factor (bssn_K, bssn_chi).
+ * First derivatives by the 2nd-order centred stencil, as the reference's
+ * integrands take them.  On a hierarchy the reference then fills every
+ * level's boundary from its parent and its covered interior from its child,
+ * finest first (nrgpu_fmr_restrict_prolong_vars with nvars = 8).
+ *
+ * nrgpu_sphere_integral: integral_over_sphere with Simpson weights
+ * (utility/NumericUtils/Integral_over_sphere.c:197-357) of the device array
+ * f of a level over the sphere of radius r about (x0, y0, z0): ntheta
+ * circles (odd) of nphi + 1 points (nphi even), values by Lagrange
+ * interpolation of the given order (order_centered in ADM_mass); on
+ * bitant, qreflect and octant grids the covered part times the symmetry
+ * factor.  *result is 0 when a sphere point's interpolation cube is not on
+ * the level, as in the reference.  Synchronises the stream. */
+int nrgpu_adm_mass_integrands(nrgpu_level *L, const double *const *gK, const double *trK, const double *chi,
+                              double *const *out, void *stream);
+int nrgpu_sphere_integral(nrgpu_level *L, const double *f, double x0, double y0, double z0, double r, int ntheta,
+                          int nphi, int order, double *result, void *stream);
 
 /* the evolution systems */
 enum { NRGPU_SYSTEM_BSSN = 0, NRGPU_SYSTEM_Z4C = 1 };

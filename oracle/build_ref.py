@@ -53,6 +53,8 @@ MODULES = [
                                "forMovingPunctures PunctureData_with_given_M_ADM"),
     ("src/projects/Gauge", "bam_Gauge moving_punctures moving_punctures_integrate puncture_properties "
                            "puncture_properties_integrand"),
+    ("src/projects/ADM_mass", "bam_ADM_mass ADM_mass adm_mass_integrand adm_mass_integrand_chi adm_pj_integrand"),
+    ("src/projects/Invariants", "bam_Invariants Invariants curvature_invariants_N dphi_int2_psi4_N"),
     # bampi and main go last, as in the reference Makefile
     ("src/main/bampi", "bam_bampi bampi copy debug output openmp profile reduce split_box synchronize "
                        "synchronize_fmr timer"),
@@ -128,9 +130,16 @@ def main():
                  os.path.join(HERE, "mpi_stub")))
     stub_h = os.path.join(HERE, "mpi_stub", "mpi.h")
 
+    # the generated module lists are included by main.c: a change of the
+    # module list rebuilds it
+    gen_t = max(os.path.getmtime(os.path.join(gen, f)) for f in os.listdir(gen))
+
     def compile_one(job):
         src, o, incdir = job
-        if os.path.exists(o) and os.path.getmtime(o) >= max(os.path.getmtime(src), os.path.getmtime(stub_h)):
+        deps = [os.path.getmtime(src), os.path.getmtime(stub_h)]
+        if src.endswith(os.path.join("main", "main", "main.c")):
+            deps.append(gen_t)
+        if os.path.exists(o) and os.path.getmtime(o) >= max(deps):
             return None
         cmd = base + ["-I" + incdir, "-c", src, "-o", o]
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -15,6 +15,9 @@
  *   3. nrharness_dump = "i0 i1 ...": dump the evolved variables of every
  *      level after those level iterations (POST_EVOLVE), and after the
  *      initial data when 0 is listed.
+ *   6. nrharness_admmass = yes: with the reference's ADM_mass project, dump
+ *      its integrands and their inputs and write its sphere integrals with
+ *      all digits (admmass_itN_lL.bin/.txt).
  *   5. nrharness_dump_moved = yes: dump every level that move_box moved,
  *      after the move (POST_MOVEBOX), as moved_itN_lL.bin.
  *   4. nrharness_track = yes: with each of those dumps, run the reference's
@@ -246,6 +249,55 @@ int nrharness_post_movebox(tL *level)
   return 0;
 }
 
+/* ANALYZE after ADM_mass (projects/ADM_mass/ADM_mass.c:11-225, run with
+   ADM_mass_persist = yes so its integrands stay): on the coarsest level of
+   a time-aligned stack, at a dump iteration, every level of the stack is
+   dumped with the integrands and their inputs (admmass_itN_lL.bin), and the
+   reference's integral_over_sphere of each integrand at each radius of
+   ADM_mass_r that lies safely inside the level is written with all digits
+   (admmass_itN_lL.txt: radius, then the 8 integrals) */
+double integral_over_sphere(tL *level, double x0, double y0, double z0, int ntheta, int nphi, double r,
+                            int index, int order);
+int nrharness_analyze(tL *level)
+{
+  static const char *names[8] = {"ADM_mass_integrand", "ADM_mass_integrand_chi", "ADM_mass_Pxint",
+                                 "ADM_mass_Pyint", "ADM_mass_Pzint", "ADM_mass_Jxint", "ADM_mass_Jyint",
+                                 "ADM_mass_Jzint"};
+  tG *g = level->grid;
+  char tag[64], fn[1024];
+  int l, v;
+  if (!Getv("nrharness_admmass", "yes") || !dump_requested(level->iteration) || parentaligned(level)) return 0;
+  for (l = level->l; l <= g->lmax; l++) {
+    tL *lv = g->level[l];
+    tVarList *vl = vlalloc(lv);
+    char *rs, *r1;
+    FILE *f;
+    for (v = 0; v < 8; v++) vlpush(vl, Ind(names[v]));
+    vlpush(vl, Ind("adm_gxx"));
+    vlpush(vl, Ind("adm_Kxx"));
+    vlpush(vl, Ind("bssn_K"));
+    vlpush(vl, Ind("bssn_chi"));
+    snprintf(tag, sizeof tag, "admmass_it%d", lv->iteration);
+    dump_varlist(lv, vl, tag);
+    vlfree(vl);
+    snprintf(fn, sizeof fn, "%s/%s_l%d.txt", Gets("nrharness_dir"), tag, l);
+    f = fopen(fn, "w");
+    if (!f) errorexits("nrharness: cannot open %s", fn);
+    rs = Gets("ADM_mass_r");
+    while ((r1 = NextEntry(rs))) {
+      double r = atof(r1);
+      if (!centered_sphere_safely_inside_level(lv, r)) continue;
+      fprintf(f, "%.17e", r);
+      for (v = 0; v < 8; v++)
+        fprintf(f, " %.17e", integral_over_sphere(lv, 0, 0, 0, Geti("ADM_mass_ncircles"), Geti("ADM_mass_npoints"),
+                                                  r, Ind(names[v]), Geti("order_centered")));
+      fprintf(f, "\n");
+    }
+    fclose(f);
+  }
+  return 0;
+}
+
 /* the reference's trackers and the globals of moving_punctures.c:13-14 */
 int track_moving_puncture_integrate(tL *level, int np, double *pold, double *pnew);
 int track_moving_puncture_extremum(tL *level, int np, double *pold, double *pnew);
@@ -355,5 +407,7 @@ void bam_nrharness(void)
   AddFun(POST_INITIALDATA, nrharness_post_initialdata, "oracle harness: synthetic data and dumps");
   AddFun(POST_EVOLVE, nrharness_post_evolve, "oracle harness: dumps");
   AddPar("nrharness_dump_moved", "no", "dump every level that move_box moved, after the move [no,yes]");
+  AddPar("nrharness_admmass", "no", "with ADM_mass: dump its integrands and full-precision integrals [no,yes]");
+  AddFun(ANALYZE, nrharness_analyze, "oracle harness: ADM mass integrands and integrals");
   AddFun(POST_MOVEBOX, nrharness_post_movebox, "oracle harness: dumps of moved levels");
 }

@@ -381,6 +381,90 @@ RED0D_CASES = {
 }
 
 
+ADMMASS_COMMON = """
+physics = adm bssn punctures ADM_mass nrharness
+mass1 = 0.5
+px1 = 1.0
+my1 = 0.2
+sz1 = 0.1
+mass2 = 0.6
+px2 = -1.2
+my2 = -0.15
+sx2 = 0.05
+sz2 = -0.08
+punctures_solver = none
+bssn_initial_lapse = oochi05
+bssn_initial_shift = zero
+order_centered = 4
+order_advection = 4
+advection_lopsided = 1
+order_dissipation = 6
+iterations = 1
+0doutiter = 1
+ADM_mass_persist = yes
+ADM_mass_ncircles = 21
+ADM_mass_npoints = 40
+nrharness_dump = 1
+nrharness_admmass = yes
+"""
+ADMMASS_CASES = {
+    # one box: a Bowen-York binary (momenta and spins) without the
+    # Hamiltonian-constraint solve, after one RK4 step
+    "admmass_box": BSSN_COMMON + ADMMASS_COMMON + """
+nxyz = 24
+dxyz = 0.4
+ADM_mass_r = 2 3
+""",
+    # three nested levels: the integrands filled from parents and children
+    # (set_boundary_refinement_cf) before the spheres of each level
+    "admmass_fmr": BSSN_COMMON + ADMMASS_COMMON + """
+nxyz = 16
+dxyz = 0.8
+amr = bo newfmr
+amr_fmr = nestedboxes
+amr_lmax = 2
+amr_nbuffer = 3
+ADM_mass_r = 1 2.5 3.5
+""",
+}
+
+
+def run_admmass_case(name, par):
+    """Per level of the final time-aligned stack: geometry, the ADM mass
+    inputs and the reference's integrands (admmass_itN_lL.bin), and its
+    sphere integrals (admmass_itN_lL.txt: radius, 8 integrals)."""
+    work = tempfile.mkdtemp(prefix="golden_")
+    try:
+        with open(os.path.join(work, name + ".par"), "w") as f:
+            f.write(par)
+        r = subprocess.run([BAM, "-nt", "4", name + ".par"], cwd=work, capture_output=True, text=True)
+        if r.returncode:
+            raise RuntimeError(r.stdout[-3000:] + r.stderr[-3000:])
+        arrays = {}
+        l = 0
+        while os.path.exists(os.path.join(work, "admmass_it%d_l%d.bin" % (2 ** l, l))):
+            tag = "admmass_it%d_l%d" % (2 ** l, l)
+            d = dumpfile.read(os.path.join(work, tag + ".bin"))
+            arrays["boxes_l%d" % l] = np.array(d["boxes"], dtype=np.float64)
+            arrays["dx_l%d" % l] = d["dx"]
+            arrays["boundary_l%d" % l] = d["boundary"]
+            # the 14 inputs in full; the reference's 8 integrands at 1024
+            # seeded points (all of them on the points its spheres read
+            # would make the fixture large)
+            arrays["inputs_l%d" % l] = d["data"][8:]
+            idx = np.sort(np.random.default_rng(l).choice(len(d["boundary"]), 1024, replace=False))
+            arrays["sample_l%d" % l] = idx.astype(np.int32)
+            arrays["integrands_l%d" % l] = d["data"][:8, idx]
+            arrays["integrals_l%d" % l] = np.loadtxt(os.path.join(work, tag + ".txt"), ndmin=2).reshape(-1, 9)
+            l += 1
+        np.savez_compressed(os.path.join(OUT, name + ".npz"), nlevels=l, names=np.array(d["names"]), **arrays)
+        with open(os.path.join(OUT, name + ".par"), "w") as f:
+            f.write(par.lstrip())
+        print("wrote", name, l, "levels", [arrays["integrals_l%d" % q].shape[0] for q in range(l)])
+    finally:
+        shutil.rmtree(work)
+
+
 def run_red0d_case(name, par):
     work = tempfile.mkdtemp(prefix="golden_")
     try:
@@ -550,3 +634,6 @@ if __name__ == "__main__":
     for n, p in RED0D_CASES.items():
         if not only or n in only:
             run_red0d_case(n, p)
+    for n, p in ADMMASS_CASES.items():
+        if not only or n in only:
+            run_admmass_case(n, p)
