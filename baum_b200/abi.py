@@ -362,6 +362,12 @@ def lib():
         "nrgpu_fmr_set_move": (C.c_int, [vp, vp, vp]),
         "nrgpu_fmr_restrict_prolong_vars": (C.c_int, [vp, C.c_int, C.c_int, pp, pp, vp]),
         "nrgpu_adm_mass_integrands": (C.c_int, [vp, pp, vp, vp, pp, vp]),
+        "nrgpu_psi4": (C.c_int, [vp, pp, vp, pp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double), vp, vp, vp,
+                                 vp]),
+        "nrgpu_psi4_rescale": (C.c_int, [vp, vp, vp, C.POINTER(C.c_double), vp]),
+        "nrgpu_psi4_modes": (C.c_int, [vp, vp, vp, C.POINTER(C.c_double), C.c_int, C.c_int,
+                                       C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int, C.c_int,
+                                       C.POINTER(C.c_double), vp]),
         "nrgpu_sphere_integral": (C.c_int, [vp, vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
                                             C.c_int, C.c_int, C.POINTER(C.c_double), vp]),
         "nrgpu_fmr_regrid": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(LevelDesc), pp, pp, vp]),

@@ -135,3 +135,42 @@ def sphere_safely_inside(level, r, order_RP):
         if level.desc.symmetry >> d & 1:
             lo[d] = -hi[d]
     return all(not (-rr < lo[d] - 1e-10 or hi[d] < rr - 1e-10) for d in range(3))
+
+
+def _origin(o):
+    return (C.c_double * 3)(*[float(v) for v in o])
+
+
+def psi4(dl, uadm, alpha, beta, order_centered, kinnersley=False, flat=False, origin=(0.0, 0.0, 0.0), out=None,
+         csqr=True, stream=None):
+    """rpsi4, ipsi4, Csqr (3, npoints) of curvature_invariants_N at the
+    flag-0 points (zeros elsewhere when out is None) from the ADM metric and
+    curvature uadm (12, npoints), the lapse (npoints) and the shift (3,
+    npoints)."""
+    out = torch.zeros((3, dl.level.npoints), dtype=torch.float64, device="cuda") if out is None else out
+    abi.check(abi.lib().nrgpu_psi4(dl.handle, _ptrs(uadm, 12), C.c_void_p(alpha.data_ptr()), _ptrs(beta, 3),
+                                   int(order_centered), int(bool(kinnersley)), int(bool(flat)), _origin(origin),
+                                   C.c_void_p(out[0].data_ptr()), C.c_void_p(out[1].data_ptr()),
+                                   C.c_void_p(out[2].data_ptr()) if csqr else None, _stream(stream)))
+    return out
+
+
+def rescale_psi4(dl, p, origin=(0.0, 0.0, 0.0), stream=None):
+    """rescale_psi4 (Invariants.c:263-284) on rows 0, 1 of p."""
+    abi.check(abi.lib().nrgpu_psi4_rescale(dl.handle, C.c_void_p(p[0].data_ptr()), C.c_void_p(p[1].data_ptr()),
+                                           _origin(origin), _stream(stream)))
+
+
+def psi4_modes(dl, p, radii, lmin=2, lmax=4, ntheta=47, nphi=46, order=4, origin=(0.0, 0.0, 0.0), stream=None):
+    """compute_modes (Invariants.c:367-540): (len(radii), nmodes, 2) with the
+    modes in the reference's column order (l ascending, m = -l..l)."""
+    nr = len(radii)
+    lnum, mnum = lmax - lmin + 1, 2 * lmax + 1
+    buf = np.zeros(nr * lnum * mnum * 2)
+    rad = (C.c_double * nr)(*[float(r) for r in radii])
+    abi.check(abi.lib().nrgpu_psi4_modes(dl.handle, C.c_void_p(p[0].data_ptr()), C.c_void_p(p[1].data_ptr()),
+                                         _origin(origin), int(lmin), int(lmax), rad, nr, int(ntheta), int(nphi),
+                                         int(order), buf.ctypes.data_as(C.POINTER(C.c_double)), _stream(stream)))
+    buf = buf.reshape(nr, lnum, mnum, 2)
+    cols = [buf[:, l - lmin, m + l, :] for l in range(lmin, lmax + 1) for m in range(-l, l + 1)]
+    return np.stack(cols, axis=1)

@@ -442,6 +442,35 @@ int nrgpu_adm_mass_integrands(nrgpu_level *L, const double *const *gK, const dou
 int nrgpu_sphere_integral(nrgpu_level *L, const double *f, double x0, double y0, double z0, double r, int ntheta,
                           int nphi, int order, double *result, void *stream);
 
+/* ---- analysis: Psi4 and its modes -----------------------------------------
+ * compute_curvature_invariants (projects/Invariants/Invariants.c:48-252).
+ * nrgpu_psi4: rpsi4, ipsi4 (and Csqr, the square of the Weyl tensor, when
+ * csqr is not NULL) of curvature_invariants_N (curvature_invariants_N.m:
+ * 14-208) at the flag-0 points, from the ADM metric and curvature gK (12
+ * device arrays), the lapse and the shift (3); derivatives at
+ * order_centered (2, 4, 6) with the order ladder near box faces; tetrad
+ * kinnersley = 0 (Gram-Schmidt, invariants_tetrad = GS) or 1; flat = 1 for
+ * gauss_codacci_mainardi = flat; origin (NULL: 0) is the sphere origin
+ * (sphere_x0..z0).  On a hierarchy the reference then restricts and
+ * prolongs rpsi4, ipsi4 and Csqr finest first
+ * (nrgpu_fmr_restrict_prolong_vars) and multiplies psi4 by the distance to
+ * invariants_x0..z0 (nrgpu_psi4_rescale, rescale_psi4, Invariants.c:
+ * 263-284).
+ * nrgpu_psi4_modes: compute_modes (Invariants.c:367-540): for l = lmin..lmax
+ * (2 <= lmin, lmax <= 12) and every m, the spin-weight -2 harmonic
+ * projection conj(Y_lm) psi4 formed at every point and integrated over the
+ * sphere of each radius (nrgpu_sphere_integral with ntheta, nphi, order =
+ * invariants_ntheta, _nphi, _order); out[((n * (lmax-lmin+1) + l-lmin) *
+ * (2 lmax + 1) + m + l) * 2 + {0, 1}] = (real, imaginary) part.  No
+ * symmetry grids.  Synchronises the stream. */
+int nrgpu_psi4(nrgpu_level *L, const double *const *gK, const double *alpha, const double *const *beta,
+               int order_centered, int kinnersley, int flat, const double *origin, double *rpsi4, double *ipsi4,
+               double *csqr, void *stream);
+int nrgpu_psi4_rescale(nrgpu_level *L, double *rpsi4, double *ipsi4, const double *origin, void *stream);
+int nrgpu_psi4_modes(nrgpu_level *L, const double *rpsi4, const double *ipsi4, const double *origin, int lmin,
+                     int lmax, const double *radii, int nr, int ntheta, int nphi, int order, double *out,
+                     void *stream);
+
 /* the evolution systems */
 enum { NRGPU_SYSTEM_BSSN = 0, NRGPU_SYSTEM_Z4C = 1 };
 

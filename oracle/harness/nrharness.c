@@ -258,8 +258,34 @@ int nrharness_post_movebox(tL *level)
    (admmass_itN_lL.txt: radius, then the 8 integrals) */
 double integral_over_sphere(tL *level, double x0, double y0, double z0, int ntheta, int nphi, double r,
                             int index, int order);
+/* after Invariants (projects/Invariants/Invariants.c:48-252, run with
+   invariants_persist = yes): rpsi4, ipsi4 (restricted, prolonged and
+   rescaled by r) and Csqr with their inputs on every level of the stack */
+static void dump_psi4(tL *level)
+{
+  tG *g = level->grid;
+  char tag[64];
+  int l;
+  for (l = level->l; l <= g->lmax; l++) {
+    tL *lv = g->level[l];
+    tVarList *vl = vlalloc(lv);
+    vlpush(vl, Ind("rpsi4"));
+    vlpush(vl, Ind("ipsi4"));
+    vlpush(vl, Ind("Csqr"));
+    vlpush(vl, Ind("adm_gxx"));
+    vlpush(vl, Ind("adm_Kxx"));
+    vlpush(vl, Ind("alpha"));
+    vlpush(vl, Ind("betax"));
+    snprintf(tag, sizeof tag, "psi4_it%d", lv->iteration);
+    dump_varlist(lv, vl, tag);
+    vlfree(vl);
+  }
+}
+
 int nrharness_analyze(tL *level)
 {
+  if (Getv("nrharness_psi4", "yes") && dump_requested(level->iteration) && !parentaligned(level))
+    dump_psi4(level);
   static const char *names[8] = {"ADM_mass_integrand", "ADM_mass_integrand_chi", "ADM_mass_Pxint",
                                  "ADM_mass_Pyint", "ADM_mass_Pzint", "ADM_mass_Jxint", "ADM_mass_Jyint",
                                  "ADM_mass_Jzint"};
@@ -408,6 +434,7 @@ void bam_nrharness(void)
   AddFun(POST_EVOLVE, nrharness_post_evolve, "oracle harness: dumps");
   AddPar("nrharness_dump_moved", "no", "dump every level that move_box moved, after the move [no,yes]");
   AddPar("nrharness_admmass", "no", "with ADM_mass: dump its integrands and full-precision integrals [no,yes]");
+  AddPar("nrharness_psi4", "no", "with Invariants: dump rpsi4, ipsi4, Csqr and their inputs [no,yes]");
   AddFun(ANALYZE, nrharness_analyze, "oracle harness: ADM mass integrands and integrals");
   AddFun(POST_MOVEBOX, nrharness_post_movebox, "oracle harness: dumps of moved levels");
 }

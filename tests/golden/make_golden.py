@@ -429,6 +429,66 @@ ADM_mass_r = 1 2.5 3.5
 }
 
 
+PSI4_EXTRA = """
+nrharness_psi4 = yes
+0doutput = rpsi4 ipsi4 Csqr
+invariants_persist = yes
+"""
+PSI4_CASES = {
+    # psi4, Csqr and the l = 2..4 modes of the same data
+    "psi4_box": ADMMASS_CASES["admmass_box"].replace("physics = adm bssn punctures ADM_mass nrharness",
+                                                     "physics = adm bssn punctures Invariants nrharness")
+    .replace("nrharness_admmass = yes\n", PSI4_EXTRA.lstrip()).replace("ADM_mass_r = 2 3", "invariants_modes_r = 2 3"),
+    "psi4_fmr": ADMMASS_CASES["admmass_fmr"].replace("physics = adm bssn punctures ADM_mass nrharness",
+                                                     "physics = adm bssn punctures Invariants nrharness")
+    .replace("nrharness_admmass = yes\n", PSI4_EXTRA.lstrip())
+    .replace("ADM_mass_r = 1 2.5 3.5", "invariants_modes_r = 1 2.5 3.5"),
+}
+
+
+def run_psi4_case(name, par):
+    """Per level of the final stack: geometry, the 16 inputs of the psi4
+    computation (adm g, K, alpha, beta) in full, the reference's rpsi4,
+    ipsi4 (restricted, prolonged, times r) and Csqr at 2048 seeded points,
+    and its l = 2..4 modes at each radius from rpsi4_modes_rN.lL /
+    ipsi4_modes_rN.lL (written with 17 digits, Invariants.c:580-600)."""
+    work = tempfile.mkdtemp(prefix="golden_")
+    try:
+        with open(os.path.join(work, name + ".par"), "w") as f:
+            f.write(par)
+        r = subprocess.run([BAM, "-nt", "4", name + ".par"], cwd=work, capture_output=True, text=True)
+        if r.returncode:
+            raise RuntimeError(r.stdout[-3000:] + r.stderr[-3000:])
+        arrays = {}
+        l = 0
+        inv = os.path.join(work, name, "Invariants")
+        while os.path.exists(os.path.join(work, "psi4_it%d_l%d.bin" % (2 ** l, l))):
+            d = dumpfile.read(os.path.join(work, "psi4_it%d_l%d.bin" % (2 ** l, l)))
+            arrays["boxes_l%d" % l] = np.array(d["boxes"], dtype=np.float64)
+            arrays["dx_l%d" % l] = d["dx"]
+            arrays["boundary_l%d" % l] = d["boundary"]
+            arrays["inputs_l%d" % l] = d["data"][3:]
+            idx = np.sort(np.random.default_rng(10 + l).choice(len(d["boundary"]), 2048, replace=False))
+            arrays["sample_l%d" % l] = idx.astype(np.int32)
+            arrays["psi4_l%d" % l] = d["data"][:3, idx]
+            n = 1
+            modes = []
+            while os.path.exists(os.path.join(inv, "rpsi4_modes_r%d.l%d" % (n, l))):
+                rr = np.loadtxt(os.path.join(inv, "rpsi4_modes_r%d.l%d" % (n, l)), comments='"', ndmin=2)[-1]
+                ii = np.loadtxt(os.path.join(inv, "ipsi4_modes_r%d.l%d" % (n, l)), comments='"', ndmin=2)[-1]
+                modes.append(np.stack([rr[1:], ii[1:]], axis=1))
+                n += 1
+            arrays["modes_l%d" % l] = np.array(modes)
+            arrays["time_l%d" % l] = d["time"]
+            l += 1
+        np.savez_compressed(os.path.join(OUT, name + ".npz"), nlevels=l, **arrays)
+        with open(os.path.join(OUT, name + ".par"), "w") as f:
+            f.write(par.lstrip())
+        print("wrote", name, l, "levels", [arrays["modes_l%d" % q].shape for q in range(l)])
+    finally:
+        shutil.rmtree(work)
+
+
 def run_admmass_case(name, par):
     """Per level of the final time-aligned stack: geometry, the ADM mass
     inputs and the reference's integrands (admmass_itN_lL.bin), and its
@@ -637,3 +697,6 @@ if __name__ == "__main__":
     for n, p in ADMMASS_CASES.items():
         if not only or n in only:
             run_admmass_case(n, p)
+    for n, p in PSI4_CASES.items():
+        if not only or n in only:
+            run_psi4_case(n, p)
