@@ -147,7 +147,7 @@ class Z4Params(C.Structure):
                 ("withB", C.c_double), ("lapseharmonicf", C.c_double), ("shiftalphapower", C.c_double),
                 ("shiftgammacoeff", C.c_double), ("shiftdriver", C.c_double), ("chiDivFloor", C.c_double),
                 ("chipsipower", C.c_double), ("bc_var0", C.c_double * Z4_NVARS),
-                ("bc_speed", C.c_double * Z4_NVARS), ("precision", C.c_int)]
+                ("bc_speed", C.c_double * Z4_NVARS), ("precision", C.c_int), ("boundary", C.c_int)]
 
 
 def z4_params(**over):

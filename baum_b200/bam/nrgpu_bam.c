@@ -155,10 +155,18 @@ static void read_params_z4(tL *level, tVarList *u, nrgpu_z4_params *p)
   p->chipsipower = Getd("z4_chi_psipower");
   if (Getv("z4_forceKzero", "yes")) errorexit("nrgpu: z4_forceKzero is not supported");
   if (level->shells) errorexit("nrgpu: shells are not supported");
+  /* set_boundary's background branch on level 0 (boundary.c:190-210, z4.c:
+     251-271): radcentered or CPBC2 */
+  if (Getv("boundary", "background") && level->l == 0) {
+    if (Getv("boundary", "radiative")) errorexit("nrgpu: boundary = radiative and background together");
+    p->boundary = Getv("boundary", "radcentered") ? 1 : 2;
+  }
+  /* the radiative condition's far limits and speeds (boundary_radconstant
+     exists only where the radiative boundary is registered) */
   for (j = 0; j < ZNV; j++) {
     int i = u->index[METRIC_z4_INDX_VAR + j];
     p->bc_var0[j] = VarFarLimit(i);
-    p->bc_speed[j] = Getv("boundary_radconstant", VarName(i)) ? 0.0 : VarPropSpeed(i);
+    p->bc_speed[j] = GetvLax("boundary_radconstant", VarName(i)) ? 0.0 : VarPropSpeed(i);
   }
 }
 
@@ -284,11 +292,15 @@ void nrgpu_z4_evolve_cb(tVarList *unew, tVarList *upre, double c, tVarList *ucur
   if (c != 0.0) copy_vl(level, upre, s->d_b, 1);
   check(nrgpu_z4_rhs(s->lev, n, c != 0.0 ? pr : cu, c, cu, &p, 0), "rhs");
   copy_vl(level, unew, s->d_a, 0);
+  /* the background boundary extrapolates the state itself onto the
+     boundary (z4_rhs_movpunc_N.c:148-152); BAM's RK4 keeps those values */
+  if (p.boundary) copy_vl(level, ucur, s->d_c, 0);
   timer_stop(level, "z4_rhs");
 }
 
 /* "geometry_bound" callback of the Z4c system: replaces set_boundary
- * (z4.c:248) with the radiative condition and the symmetry reflections */
+ * (z4.c:248) with the radiative condition and the symmetry reflections, or
+ * on level 0 with its background branch (radcentered or CPBC2) */
 void nrgpu_z4_boundary_cb(tVarList *unew, tVarList *upre, double c, tVarList *ucur)
 {
   tL *level = ucur->level;
@@ -304,6 +316,7 @@ void nrgpu_z4_boundary_cb(tVarList *unew, tVarList *upre, double c, tVarList *uc
   if (c != 0.0) copy_vl(level, upre, s->d_b, 1);
   check(nrgpu_z4_boundary(s->lev, n, c != 0.0 ? pr : cu, c, cu, &p, 0), "boundary");
   copy_vl(level, unew, s->d_a, 0);
+  if (p.boundary) copy_vl(level, ucur, s->d_c, 0);
 }
 
 /* EVOLVE hook of the resident mode: evolve_rk_rk4 + algcon on the device */

@@ -1574,6 +1574,7 @@ static int z4_check_params(const nrgpu_z4_params *p) {
     return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "order_dissipation %d not in {0,4,6}", p->order_dissipation);
   if (p->useNPTs) return nrgpu_set_error(NRGPU_ERR_UNSUPPORTED, "z4_useNPTs = yes is not supported");
   if (p->precision < 0 || p->precision > 2) return nrgpu_set_error(NRGPU_ERR_ARG, "precision %d", p->precision);
+  if (p->boundary < 0 || p->boundary > 2) return nrgpu_set_error(NRGPU_ERR_ARG, "boundary %d", p->boundary);
   if (p->advection_lopsided < 0 || p->advection_lopsided > 2 || p->advection_lopsided6 < 0 ||
       p->advection_lopsided6 > 3)
     return nrgpu_set_error(NRGPU_ERR_ARG, "advection lopsidedness out of range");
@@ -1696,6 +1697,8 @@ extern "C" int nrgpu_z4_rhs(nrgpu_level *L, double *const *unew, double *const *
   } else {
     pr = cu;
   }
+  // the background boundary extrapolates the state onto the boundary first
+  if (p->boundary && (e = nrgpu_z4_background_extrapolate(L, ucur, (cudaStream_t)stream))) return e;
   Epilogue E = {c != 0.0 ? EPI_ADDLINEAR : EPI_RHS, c, 0.0, 0.0, 0};
   return z4_launch(L, z4_c(cu), n, z4_c(pr), n, E, *p, (cudaStream_t)stream, true, false);
 }
@@ -1711,6 +1714,7 @@ extern "C" int nrgpu_z4_boundary(nrgpu_level *L, double *const *unew, double *co
   } else {
     pr = cu;
   }
+  if (p->boundary) return nrgpu_z4_background_boundary(L, unew, upre, c, ucur, p, (cudaStream_t)stream);
   Epilogue E = {c != 0.0 ? EPI_ADDLINEAR : EPI_RHS, c, 0.0, 0.0, 0};
   if ((e = z4_launch(L, z4_c(cu), n, z4_c(pr), n, E, *p, (cudaStream_t)stream, false, true))) return e;
   return nrgpu_level_symmetry(L, unew, NRGPU_SYSTEM_Z4C, (cudaStream_t)stream);
@@ -1721,6 +1725,7 @@ int nrgpu_z4_rk4_stages(nrgpu_level *L, double *const *u, double dt, const nrgpu
   if (!L) return nrgpu_set_error(NRGPU_ERR_ARG, "null level");
   int e;
   if ((e = z4_check_params(p))) return e;
+  if (p->boundary) return nrgpu_z4_rk4_background(L, u, dt, p, st);
   ZVarPtrs U;
   if ((e = z4_fill(&U, u, "u"))) return e;
   double *scr = nullptr;

@@ -74,6 +74,13 @@ int nrgpu_bssn_rk4_stages(nrgpu_level *L, double *const *u, double dt, const nrg
                           cudaStream_t st);
 int nrgpu_z4_rk4_stages(nrgpu_level *L, double *const *u, double dt, const nrgpu_z4_params *p, cudaStream_t st);
 int nrgpu_z4_algcon(nrgpu_level *L, double *const *u, const nrgpu_z4_params *p, cudaStream_t st);
+// set_boundary's background branch for Z4c and the RK4 step that it needs
+// (the state's copy kept apart from the extrapolated stage input)
+// (nrgpu_z4bg.cu)
+int nrgpu_z4_background_extrapolate(nrgpu_level *L, double *const *u, cudaStream_t st);
+int nrgpu_z4_background_boundary(nrgpu_level *L, double *const *unew, double *const *upre, double c,
+                                 double *const *ucur, const nrgpu_z4_params *p, cudaStream_t st);
+int nrgpu_z4_rk4_background(nrgpu_level *L, double *const *u, double dt, const nrgpu_z4_params *p, cudaStream_t st);
 // the level's three RK4 scratch lists, allocated on first use (nrgpu_lib.cu)
 int nrgpu_level_scratch(nrgpu_level *L, double **out);
 // set_boundary_symmetry on a list of nv variables of the given system

@@ -126,6 +126,14 @@ typedef struct {
    * FP64 differences to the centre value rounded to FP32; state, algebra,
    * advection and RK4 stay FP64. */
   int precision;
+  /* the box boundary on PHYBOUND points: 0 radiative (set_boundary's
+   * radiative branch with bc_var0/bc_speed); 1 "background radcentered"
+   * (z4_boundary_box_rad.c) and 2 "background" (CPBC2, z4_boundary_box.c):
+   * set_boundary's background branch (utility/boundary/boundary.c:190-210),
+   * which extrapolates the state on the boundary, sets the rhs of A, G,
+   * Khat and Theta one point inside from the boundary conditions and
+   * extrapolates the rhs onto the boundary (no symmetry grids) */
+  int boundary;
 } nrgpu_z4_params;
 
 /* ---- library ---------------------------------------------------------- */

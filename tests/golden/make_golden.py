@@ -188,7 +188,26 @@ nrharness_data = fourier
 nrharness_amp = 0.05
 """
 
+Z4_BG = Z4_COMMON.replace("boundary = radiative", "boundary = background radcentered") + """
+nxyz = 12
+dxyz = 0.5
+order_centered = 4
+order_advection = 4
+advection_lopsided = 1
+order_dissipation = 6
+nrharness_length = 6.5
+nrharness_seed = 3
+"""
+
 CASES.update({
+    # the Z4c "background" box boundaries (set_boundary's background branch,
+    # z4_boundary_box_rad / z4_boundary_box): one rhs with the boundary
+    # callback, and 3 RK4 steps from the same data
+    "z4_bg_rad_rhs": Z4_BG + "iterations = 0\nnrharness_dump = 0\nnrharness_rhs = yes\n",
+    "z4_bg_rad": Z4_BG + "iterations = 3\nnrharness_dump = 0 3\n",
+    "z4_bg_cpbc_rhs": Z4_BG.replace("background radcentered", "background") +
+                      "iterations = 0\nnrharness_dump = 0\nnrharness_rhs = yes\n",
+    "z4_bg_cpbc": Z4_BG.replace("background radcentered", "background") + "iterations = 3\nnrharness_dump = 0 3\n",
     "z4_fourier_o4": Z4_COMMON + """
 nxyz = 10
 dxyz = 0.5

@@ -307,11 +307,11 @@ nrharness_dump = 4
 """
 
 
-def run_z4(binary, extra_physics, grid, extra):
+def run_z4(binary, extra_physics, grid, extra, boundary="radiative"):
     work = tempfile.mkdtemp(prefix="bamgpu_")
     try:
         with open(os.path.join(work, "t.par"), "w") as f:
-            f.write(Z4_PAR % (extra_physics, grid, extra))
+            f.write((Z4_PAR % (extra_physics, grid, extra)).replace("boundary = radiative", "boundary = " + boundary))
         r = subprocess.run([binary, "-nt", "4", "t.par"], cwd=work, capture_output=True, text=True, timeout=600)
         assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
         return dumpfile.read(os.path.join(work, "state_it4_l0.bin"))["data"], r.stdout
@@ -329,6 +329,20 @@ def test_bam_z4_with_the_gpu_path_matches_bam(gpu, cpu_state, grid, mode, extra)
     BAM after 4 steps."""
     ref, _ = run_z4(BAM, "", grid, "")
     got, out = run_z4(BAM_GPU, " nrgpu", grid, extra)
+    assert "nrgpu: %s mode" % mode in out
+    assert relerr(got, ref).max() < 1e-12
+
+
+@pytest.mark.parametrize("boundary", ["background", "background radcentered"])
+@pytest.mark.parametrize("mode,extra", [("callback", "nrgpu_mode = callback"),
+                                        ("resident", "nrgpu_mode = resident\nz4_register_algcon = no")])
+def test_bam_z4_background_boundary_matches_bam(gpu, cpu_state, boundary, mode, extra):
+    """The Z4c background box boundaries inside BAM (CPBC2 and the centred
+    radiative condition): the state extrapolated by the rhs persists through
+    BAM's RK4 in the callback mode, and the resident step writes out
+    evolve_rk_rk4; against plain BAM after 4 steps."""
+    ref, _ = run_z4(BAM, "", "box", "", boundary)
+    got, out = run_z4(BAM_GPU, " nrgpu", "box", extra, boundary)
     assert "nrgpu: %s mode" % mode in out
     assert relerr(got, ref).max() < 1e-12
 
