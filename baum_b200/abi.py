@@ -358,6 +358,7 @@ def lib():
         "nrgpu_fmr_save": (C.c_int, [vp, vp, C.c_size_t]),
         "nrgpu_fmr_load": (C.c_int, [vp, vp, C.c_size_t]),
         "nrgpu_fmr_track": (C.c_int, [vp, C.c_int, C.POINTER(C.c_double), C.c_int]),
+        "nrgpu_fmr_track_method": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int]),
         "nrgpu_fmr_punctures": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
         "nrgpu_fmr_set_move": (C.c_int, [vp, vp, vp]),
         "nrgpu_fmr_restrict_prolong_vars": (C.c_int, [vp, C.c_int, C.c_int, pp, pp, vp]),

@@ -378,14 +378,28 @@ static double *fmr_state[64];
 static int fmr_ntrack = 0;
 static double fmr_tpos[3 * NRGPU_MAX_PUNCTURES];
 
-static void fmr_track_setup(tG *g)
+static void fmr_track_setup(tG *g, tVarList *u)
 {
-  int np, i, n;
+  int np, i, n, method, var = -1, fixz;
   if (!Getv("physics", "Gauge") || !Getv("Gauge", "moving_puncture") || !Getv("moving_puncture_track", "yes"))
     return;
-  if (!Getv("moving_puncture_track_method", "int"))
-    errorexit("nrgpu: the fmr mode tracks punctures with the shift integrator only "
-              "(moving_puncture_track_method = int)");
+  /* track_puncture's choices (Gauge/moving_punctures.c:123-134) */
+  if (Getv("moving_puncture_track_method", "ext")) method = 0;
+  else if (Getv("moving_puncture_track_method", "int")) method = 1;
+  else if (Getv("moving_puncture_track_method", "extint")) method = 2;
+  else errorexit("nrgpu: moving_puncture_track_method is not ext, int or extint");
+  if (Getv("moving_puncture_fixz", "NS")) fixz = 1;
+  else if (Getv("moving_puncture_fixz", "BH")) fixz = 2;
+  else if (Getv("moving_puncture_fixz", "BHNS")) fixz = 3;
+  else if (Getv("moving_puncture_fixz", "none")) fixz = 0;
+  else errorexit("nrgpu: moving_puncture_fixz is not NS, BH, BHNS or none");
+  if (method != 1) {
+    /* the searched variable must be one the device evolves */
+    int k = Ind(Gets("moving_puncture_track_var"));
+    for (i = 0; i < nvars(); i++)
+      if (u->index[first_var() + i] == k) var = i;
+    if (var < 0) errorexit("nrgpu: moving_puncture_track_var is not in the evolved list");
+  }
   n = Geti("nobjects");
   if (n < 1 || n > NRGPU_MAX_PUNCTURES) errorexit("nrgpu: nobjects out of range for tracking");
   for (np = 0; np < n; np++) {
@@ -393,8 +407,9 @@ static void fmr_track_setup(tG *g)
     for (i = 0; i < 3; i++) fmr_tpos[3 * np + i] = g->puncpos[np][i];
     g->lmaxpunc[np] = -1;
   }
-  check(nrgpu_fmr_track(fmr_h, n, fmr_tpos,
-                        Getv("moving_puncture_fixz", "BH") || Getv("moving_puncture_fixz", "BHNS")), "track");
+  check(nrgpu_fmr_track(fmr_h, n, fmr_tpos, fixz == 2 || fixz == 3), "track");
+  check(nrgpu_fmr_track_method(fmr_h, method, var < 0 ? 0 : var, Getv("moving_puncture_track_mode", "max"),
+                               Getd("moving_puncture_track_minmove"), fixz == 1 || fixz == 3), "track method");
   fmr_ntrack = n;
 }
 
@@ -575,7 +590,7 @@ int nrgpu_evolve_fmr(tL *level)
     fp.order_RP = Geti("order_RP");
     fp.nbuffer = Geti("amr_nbuffer");
     check(nrgpu_fmr_create(nl, d, dt, nrgpu_system_z4 ? (void *)zp : (void *)bp, &fp, &fmr_h), "fmr");
-    fmr_track_setup(g);
+    fmr_track_setup(g, u);
     if (Getv("amr", "move")) {
 #ifndef NRGPU_WRAP_MOVE_BOX
       errorexit("nrgpu: moving boxes in the fmr mode need a build linked with -Wl,--wrap=move_box");

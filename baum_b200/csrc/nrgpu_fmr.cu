@@ -233,6 +233,11 @@ struct nrgpu_fmr {
   int ntrack, track_fixz;
   double *d_track;
   int *d_tstatus;
+  // the tracker per puncture (moving_puncture_track_method,
+  // moving_punctures.c:123-180): the first next_ext punctures by the
+  // extremum search on variable track_var, the rest by the shift integrator
+  int track_method, track_var, track_max, track_fixz_ext;
+  double track_minmove;
   // moving boxes: the caller's hook, called where the reference calls
   // move_box (main.c:428), and the levels whose pairs with their parent
   // wait to be set up again after a regrid of that parent
@@ -492,6 +497,13 @@ Ptrs upp_ptrs(nrgpu_fmr *F, int l) {
 // (bssn.c:315-322) and 19 of Z4c (z4.c:234-242)
 int shift_index(const nrgpu_fmr *F) { return F->p.system == NRGPU_SYSTEM_BSSN ? 18 : 19; }
 
+// how many of the tracked punctures (the first ones) the extremum search
+// moves: all for "ext", the first for "extint", none for "int"
+int n_extremum(const nrgpu_fmr *F) {
+  if (!F->ntrack) return 0;
+  return F->track_method == 0 ? F->ntrack : (F->track_method == 2 ? 1 : 0);
+}
+
 int step_level(nrgpu_fmr *F, int l, double *const *u, cudaStream_t st) {
   const bool child = l < F->nl - 1;
   const long np = F->L[l]->npoints;
@@ -511,11 +523,12 @@ int step_level(nrgpu_fmr *F, int l, double *const *u, cudaStream_t st) {
     }
     NRGPU_CUDA_TRY(cudaGetLastError());
   }
-  // the tracker reads the shift one step earlier at the old positions
+  // the integrator reads the shift one step earlier at the old positions
   // (betax_p in moving_punctures_integrate.c:62-64): taken before the step
-  if (l == F->nl - 1 && F->ntrack &&
-      (e = nrgpu_track_before_step(F->L[l], u + shift_index(F), F->p.order_RP, F->ntrack, F->d_track,
-                                   F->d_track + 3 * F->ntrack, st)))
+  const int next = n_extremum(F), nint = F->ntrack - next;
+  if (l == F->nl - 1 && nint > 0 &&
+      (e = nrgpu_track_before_step(F->L[l], u + shift_index(F), F->p.order_RP, nint, F->d_track + 3 * next,
+                                   F->d_track + 3 * F->ntrack + 3 * next, st)))
     return e;
   if (F->p.system == NRGPU_SYSTEM_BSSN) e = nrgpu_bssn_rk4_stages(F->L[l], u, F->dt[l], &F->bp[l], st);
   else e = nrgpu_z4_rk4_stages(F->L[l], u, F->dt[l], &F->zp[l], st);
@@ -554,10 +567,17 @@ int advance(nrgpu_fmr *F, int l, double *const *u, cudaStream_t st) {
     if ((e = restrict_prolong(F, l, uc, uf, st))) return e;
   }
   // ANALYZE of the level (main.c:420-423): track_puncture on the finest level
-  if (l == F->nl - 1 && F->ntrack &&
-      (e = nrgpu_track_after_step(F->L[l], u + l * F->nv + shift_index(F), F->dt[l], F->p.order_RP, F->track_fixz,
-                                  F->ntrack, F->d_track, F->d_track + 3 * F->ntrack, F->d_tstatus, st)))
-    return e;
+  if (l == F->nl - 1 && F->ntrack) {
+    const int next = n_extremum(F), nint = F->ntrack - next;
+    if (next && (e = nrgpu_track_extremum_on(F->L[l], u[l * F->nv + F->track_var], F->track_max, F->track_minmove,
+                                             F->p.order_RP, F->track_fixz_ext, next, F->d_track, F->d_tstatus,
+                                             st)))
+      return e;
+    if (nint && (e = nrgpu_track_after_step(F->L[l], u + l * F->nv + shift_index(F), F->dt[l], F->p.order_RP,
+                                            F->track_fixz, nint, F->d_track + 3 * next,
+                                            F->d_track + 3 * F->ntrack + 3 * next, F->d_tstatus + next, st)))
+      return e;
+  }
   // move_box(g, l + 1) (move.c:808-856): the levels above l may move once l
   // and its sublevels are done, unless l is aligned in time with its parent
   if (F->move_fn && l + 1 < F->nl) {
@@ -853,6 +873,7 @@ extern "C" int nrgpu_fmr_create(int nl, const nrgpu_level_desc *levels, const do
   F->gst = nullptr;
   F->ev_in = F->ev_out = nullptr;
   F->ntrack = F->track_fixz = 0;
+  F->track_method = 1;  // the shift integrator ("int")
   F->move_fn = nullptr;
   F->move_user = nullptr;
   memset(F->pair_stale, 0, sizeof F->pair_stale);
@@ -1163,6 +1184,17 @@ extern "C" int nrgpu_fmr_load(nrgpu_fmr *F, const void *host, size_t bytes) {
 }
 
 // ---- puncture tracking ----------------------------------------------------------
+namespace {
+// the captured coarse step changes: capture it again at the next advance
+void drop_graph(nrgpu_fmr *F) {
+  if (F->exec) cudaGraphExecDestroy(F->exec);
+  if (F->graph) cudaGraphDestroy(F->graph);
+  F->exec = nullptr;
+  F->graph = nullptr;
+  F->graph_u.clear();
+}
+}  // namespace
+
 extern "C" int nrgpu_fmr_track(nrgpu_fmr *F, int n, const double *pos, int fixz) {
   if (!F || n < 0 || n > NRGPU_MAX_PUNCTURES || (n && !pos))
     return nrgpu_set_error(NRGPU_ERR_ARG, "bad arguments (0 <= n <= %d)", NRGPU_MAX_PUNCTURES);
@@ -1172,12 +1204,7 @@ extern "C" int nrgpu_fmr_track(nrgpu_fmr *F, int n, const double *pos, int fixz)
   F->d_track = nullptr;
   F->d_tstatus = nullptr;
   F->ntrack = 0;
-  // the captured coarse step changes: capture it again at the next advance
-  if (F->exec) cudaGraphExecDestroy(F->exec);
-  if (F->graph) cudaGraphDestroy(F->graph);
-  F->exec = nullptr;
-  F->graph = nullptr;
-  F->graph_u.clear();
+  drop_graph(F);
   if (!n) return NRGPU_OK;
   if (cudaMalloc(&F->d_track, sizeof(double) * 6 * n) != cudaSuccess ||
       cudaMalloc(&F->d_tstatus, sizeof(int) * n) != cudaSuccess) {
@@ -1190,6 +1217,24 @@ extern "C" int nrgpu_fmr_track(nrgpu_fmr *F, int n, const double *pos, int fixz)
   NRGPU_CUDA_TRY(cudaMemset(F->d_tstatus, 0, sizeof(int) * n));
   F->ntrack = n;
   F->track_fixz = fixz ? 1 : 0;
+  return NRGPU_OK;
+}
+
+extern "C" int nrgpu_fmr_track_method(nrgpu_fmr *F, int method, int var, int find_max, double minmove,
+                                      int fixz_ext) {
+  if (!F) return nrgpu_set_error(NRGPU_ERR_ARG, "null hierarchy");
+  if (method < 0 || method > 2)
+    return nrgpu_set_error(NRGPU_ERR_ARG, "tracking method %d (0 ext, 1 int, 2 extint)", method);
+  if (method != 1 && (var < 0 || var >= F->nv))
+    return nrgpu_set_error(NRGPU_ERR_ARG, "tracked variable %d (0..%d)", var, F->nv - 1);
+  if (method != 1 && !(minmove >= 0.0)) return nrgpu_set_error(NRGPU_ERR_ARG, "minmove %g", minmove);
+  NRGPU_CUDA_TRY(cudaDeviceSynchronize());
+  F->track_method = method;
+  F->track_var = method == 1 ? 0 : var;
+  F->track_max = find_max ? 1 : 0;
+  F->track_minmove = minmove;
+  F->track_fixz_ext = fixz_ext ? 1 : 0;
+  drop_graph(F);
   return NRGPU_OK;
 }
 

@@ -91,6 +91,9 @@ int nrgpu_level_side(nrgpu_level *L);
 // the two halves of a tracking step for a driver that keeps no copy of the
 // previous shift: before the step the shift at the old positions into b1,
 // after it the corrector passes from b1 (nrgpu_track.cu)
+// the extremum search on the given stream (no device switch: graph capture)
+int nrgpu_track_extremum_on(nrgpu_level *L, const double *var, int find_max, double minmove, int order, int fixz,
+                            int n, double *pos, int *status, cudaStream_t st);
 int nrgpu_track_before_step(nrgpu_level *L, const double *const *beta, int order, int n, const double *pos,
                             double *b1, cudaStream_t st);
 int nrgpu_track_after_step(nrgpu_level *L, const double *const *beta, double dt, int order, int fixz, int n,

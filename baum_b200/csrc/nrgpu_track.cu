@@ -281,15 +281,21 @@ extern "C" int nrgpu_track_punctures(nrgpu_level *L, const double *const *beta, 
   return NRGPU_OK;
 }
 
-extern "C" int nrgpu_track_punctures_extremum(nrgpu_level *L, const double *var, int find_max, double minmove,
-                                              int order, int fixz, int n, double *pos, int *status, void *stream) {
+int nrgpu_track_extremum_on(nrgpu_level *L, const double *var, int find_max, double minmove, int order, int fixz,
+                            int n, double *pos, int *status, cudaStream_t st) {
   if (!var) return nrgpu_set_error(NRGPU_ERR_ARG, "null var");
   const double *v3[3] = {var, var, var};
   TrackArgs A;
   int e = make_args(L, v3, nullptr, 0.0, order, fixz, n, pos, nullptr, status, &A);
   if (e) return e;
-  NRGPU_CUDA_TRY(cudaSetDevice(L->device));
-  extremum_kernel<<<n, 32, 0, (cudaStream_t)stream>>>(A, find_max ? 1 : 0, minmove * L->dx);
+  extremum_kernel<<<n, 32, 0, st>>>(A, find_max ? 1 : 0, minmove * L->dx);
   NRGPU_CUDA_TRY(cudaGetLastError());
   return NRGPU_OK;
+}
+
+extern "C" int nrgpu_track_punctures_extremum(nrgpu_level *L, const double *var, int find_max, double minmove,
+                                              int order, int fixz, int n, double *pos, int *status, void *stream) {
+  if (!L) return nrgpu_set_error(NRGPU_ERR_ARG, "null level");
+  NRGPU_CUDA_TRY(cudaSetDevice(L->device));
+  return nrgpu_track_extremum_on(L, var, find_max, minmove, order, fixz, n, pos, status, (cudaStream_t)stream);
 }

@@ -162,6 +162,19 @@ class Hierarchy:
                                             pos.ctypes.data_as(C.POINTER(C.c_double)), int(bool(fixz))))
         self.ntrack = pos.shape[0]
 
+    TRACK_METHODS = {"ext": 0, "int": 1, "extint": 2}
+
+    def track_method(self, method="int", var=None, find_max=False, minmove=0.01, fixz_ext=False):
+        """The tracker per puncture (nrgpu_fmr_track_method,
+        moving_puncture_track_method): "int" (the shift integrator), "ext"
+        (the extremum search of variable var, the lapse by default, for every
+        puncture) or "extint" (the search for the first puncture, the
+        integrator for the rest)."""
+        if var is None:
+            var = 17 if self.params.system == abi.SYSTEM_BSSN else 18
+        abi.check(abi.lib().nrgpu_fmr_track_method(self.handle, self.TRACK_METHODS[method], int(var),
+                                                   int(bool(find_max)), float(minmove), int(bool(fixz_ext))))
+
     def punctures(self):
         """(positions n x 3, status per puncture) of the tracked punctures
         (nrgpu_fmr_punctures): bit 0 the last step integrated, bit 1 the new

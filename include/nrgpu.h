@@ -386,6 +386,17 @@ int nrgpu_fmr_load(nrgpu_fmr *fmr, const void *host, size_t bytes);
 #define NRGPU_MAX_PUNCTURES 16
 int nrgpu_fmr_track(nrgpu_fmr *fmr, int n, const double *pos, int fixz);
 int nrgpu_fmr_punctures(nrgpu_fmr *fmr, double *pos, int *status);
+/* The tracker per puncture, moving_puncture_track_method
+ * (projects/Gauge/moving_punctures.c:123-180): method 1 "int" (the default:
+ * the shift integrator for every puncture), 0 "ext" (the extremum search,
+ * nrgpu_track_punctures_extremum, for every puncture), 2 "extint" (the
+ * extremum search for the first puncture, the integrator for the rest).
+ * The search runs on variable var of the system's list
+ * (moving_puncture_track_var), a maximum if find_max
+ * (moving_puncture_track_mode = max), with minmove
+ * (moving_puncture_track_minmove) and fixz_ext (moving_puncture_fixz = NS
+ * or BHNS); the integrator keeps the fixz of nrgpu_fmr_track. */
+int nrgpu_fmr_track_method(nrgpu_fmr *fmr, int method, int var, int find_max, double minmove, int fixz_ext);
 
 /* Moving boxes (move_box, main/amr/move.c:808-986).  A level moves by a
  * regrid: the caller gives the level's new boxes (same spacing, each made of

@@ -50,9 +50,11 @@ class TrackedState(oracle.FmrState):
     """The oracle driver with track_puncture after each finest-level step
     and its restriction/prolongation (ANALYZE, main.c:420-423)."""
 
-    def __init__(self, *a, pos, ib=19, **k):
+    def __init__(self, *a, pos, ib=19, next_=0, ia=18, **k):
         super().__init__(*a, **k)
         self.pos, self.ib = np.array(pos, dtype=np.float64), ib
+        # the first next_ punctures by the extremum search on variable ia
+        self.next, self.ia = next_, ia
 
     def _advance(self, l, snap):
         last = l == len(self.levels) - 1
@@ -60,9 +62,16 @@ class TrackedState(oracle.FmrState):
             beta_p = self.u[l][self.ib:self.ib + 3].copy()
         super()._advance(l, snap)
         if last:
-            pnew, _, inside = oracle.track_punctures(self.levels[l], self.u[l][self.ib:self.ib + 3], beta_p,
-                                                     self.dt[l], self.pos, self.order_rp)
-            self.pos = np.where(inside[:, None] == 1, pnew, self.pos)
+            new = self.pos.copy()
+            k = self.next
+            if k < len(self.pos):
+                pnew, _, inside = oracle.track_punctures(self.levels[l], self.u[l][self.ib:self.ib + 3], beta_p,
+                                                         self.dt[l], self.pos[k:], self.order_rp)
+                new[k:] = np.where(inside[:, None] == 1, pnew, self.pos[k:])
+            if k:
+                pnew, inside = oracle.track_extremum(self.levels[l], self.u[l][self.ia], self.pos[:k], self.order_rp)
+                new[:k] = np.where(inside[:, None] == 1, pnew, self.pos[:k])
+            self.pos = new
 
 
 START = [[2.75, 0.1, -0.2], [-2.6, 0.3, 0.1], [0.6, 0.2, 0.1]]
@@ -97,3 +106,32 @@ def test_fmr_tracking_matches_oracle(gpu):
     assert np.array_equal(runs[0], runs[1])
     assert np.abs(runs[0] - st.pos).max() <= 1e-11, np.abs(runs[0] - st.pos).max()
     assert np.abs(st.pos - np.array(START)).max() > 1e-4  # the punctures moved
+
+
+@pytest.mark.parametrize("method", ["ext", "extint"])
+def test_fmr_extremum_tracking_matches_oracle(gpu, method):
+    """moving_puncture_track_method = ext / extint inside the refinement
+    run: the extremum search on the lapse for every puncture, or for the
+    first one and the shift integrator for the rest, after every
+    finest-level step; two coarse steps of the binary's 3-level grid against
+    the oracle driver with the oracle trackers, graph replay and plain
+    launches identical."""
+    g, levels, u0, params, dt = fmr_case("z4_fmr3_binary")
+    start = [[-2.6, 0.1, 0.05], [2.75, 0.1, -0.2], [0.6, 0.2, 0.1]]
+    nx = len(start) if method == "ext" else 1
+    st = TrackedState(levels, u0, 1, params, dt, pos=start, next_=nx)
+    st.advance(2)
+    runs = []
+    for use_graph in (0, 1):
+        H = fmr.Hierarchy(levels, dt, params, abi.fmr_params(use_graph=use_graph))
+        H.track(start)
+        H.track_method(method)
+        u = [torch.from_numpy(x.copy()).cuda() for x in u0]
+        H.advance(u, 2)
+        pos, status = H.punctures()
+        assert np.all(status & 1), status
+        runs.append(pos)
+        H.close()
+    assert np.array_equal(runs[0], runs[1])
+    assert np.abs(runs[0] - st.pos).max() <= 1e-9, np.abs(runs[0] - st.pos).max()
+    assert np.abs(st.pos[:nx] - np.array(start)[:nx]).max() > 1e-4  # the searched punctures moved
