@@ -139,13 +139,17 @@ MOVING = (("amr = bo newfmr", "amr = bo newfmr move\namr_move_force = 4\namr_mov
                               "amr_verbose = move"),)
 
 
+# the single-puncture grid with the CPBC2 background boundary on level 0
+BACKGROUND = (("boundary = radiative", "boundary = background"),)
+
+
 def run_fmr(binary, extra_physics, extra, grid="single", keep=None):
     """Dumps of every level after 2 coarse steps and the run's stdout; with
     keep, a list of output files (matched by name anywhere in the run
     directory) whose text is also returned."""
     work = tempfile.mkdtemp(prefix="bamgpu_")
     par = FMR_PAR
-    for a, b in {"binary": BINARY, "bssn": BSSN_FMR, "moving": MOVING}.get(grid, ()):
+    for a, b in {"binary": BINARY, "bssn": BSSN_FMR, "moving": MOVING, "background": BACKGROUND}.get(grid, ()):
         assert a in par
         par = par.replace(a, b)
     try:
@@ -166,7 +170,7 @@ def run_fmr(binary, extra_physics, extra, grid="single", keep=None):
         shutil.rmtree(work, ignore_errors=True)
 
 
-@pytest.mark.parametrize("grid", ["single", "binary", "bssn", "moving"])
+@pytest.mark.parametrize("grid", ["single", "binary", "bssn", "moving", "background"])
 def test_bam_fmr_mode_matches_bam(gpu, cpu_state, grid):
     """nrgpu_mode = fmr: the whole Berger-Oliger step of the 3-level Z4c grid
     on the GPU at level 0's EVOLVE hook.  BAM dumps every level right after
@@ -179,7 +183,8 @@ def test_bam_fmr_mode_matches_bam(gpu, cpu_state, grid):
     on level 2; "bssn" runs the BSSN system on the single-puncture grid;
     "moving" moves level 2's box once during the run (amr = bo newfmr move,
     forced motion), BAM on the host and the device hierarchy inside its
-    coarse step, and the moved box is compared too."""
+    coarse step, and the moved box is compared too; "background" runs
+    level 0 with the CPBC2 box boundary."""
     from baum_b200 import abi
     from oracle import oracle
     ref, ref_out = run_fmr(BAM, "", "", grid)
