@@ -51,6 +51,31 @@ __device__ __forceinline__ void z4_point(const ZCVarPtrs &U, const PointCtx &P, 
   gi[4] = detginv * (g[1] * g[2] - g[0] * g[4]);
   gi[5] = detginv * (g[0] * g[3] - g[1] * g[1]);
 
+  // Ricci tensor R_ab.  Its -1/2 g^cd d_c d_d g_ab part: with compile-time
+  // strides it comes first, so that its many stencil loads have no
+  // connection values live beside them (the 6th-order kernel then keeps
+  // almost everything in registers); with run-time strides, whose tap
+  // addresses take registers of their own, after the connection terms
+  double Rt[6];
+#pragma unroll
+  for (int a = 0; a < 6; ++a) Rt[a] = 0.0;
+  auto ricci_dd = [&]() {
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int d = c; d < 3; ++d) {
+        const double w = (c == d ? -0.5 : -1.0) * gi[sy(c, d)] * (c == d ? o2[c] : o1[c] * o1[d]);
+#pragma unroll
+        for (int a = 0; a < 6; ++a) {
+          const double dd = c == d ? d2p<ORD, PREC>(U.p[ZG11 + a], x, ZSTR(c))
+                                   : d11p<ORD, PREC>(U.p[ZG11 + a], x, ZSTR(c), ZSTR(d));
+          Rt[a] += w * dd;
+        }
+      }
+  };
+  constexpr bool kDdFirst = CSY > 0;
+  if constexpr (kDdFirst) ricci_dd();
+
   // connection
   double gdo[3][6], gam[3][6], Gfg[3];
   {
@@ -77,8 +102,7 @@ __device__ __forceinline__ void z4_point(const ZCVarPtrs &U, const PointCtx &P, 
     Gfg[a] = gi[0] * gam[a][0] + gi[3] * gam[a][3] + gi[5] * gam[a][5] +
              2.0 * (gi[1] * gam[a][1] + gi[2] * gam[a][2] + gi[4] * gam[a][4]);
 
-  // Ricci tensor R_ab (+ the chi part below)
-  double Rt[6];
+  // the connection terms of R_ab (+ the chi part below)
 #pragma unroll
   for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -95,19 +119,9 @@ __device__ __forceinline__ void z4_point(const ZCVarPtrs &U, const PointCtx &P, 
                  gam[e][sy(a, d)] * gdo[e][sy(c, b)];
           t += gi[sy(c, d)] * q;
         }
-      Rt[sy(a, b)] = t;
+      Rt[sy(a, b)] += t;
     }
-#pragma unroll
-  for (int c = 0; c < 3; ++c)
-#pragma unroll
-    for (int d = c; d < 3; ++d) {
-      const double w = (c == d ? -0.5 : -1.0) * gi[sy(c, d)] * (c == d ? o2[c] : o1[c] * o1[d]);
-#pragma unroll
-      for (int a = 0; a < 6; ++a) {
-        const double dd = c == d ? d2p<ORD, PREC>(U.p[ZG11 + a], x, ZSTR(c)) : d11p<ORD, PREC>(U.p[ZG11 + a], x, ZSTR(c), ZSTR(d));
-        Rt[a] += w * dd;
-      }
-    }
+  if constexpr (!kDdFirst) ricci_dd();
   {
     double dG[3][3];
 #pragma unroll
