@@ -1596,7 +1596,8 @@ static ZCVarPtrs z4_c(const ZVarPtrs &v) {
 }
 
 // FP64 interior launch with compile-time strides for the box sizes of the
-// workloads (66, 162, and the finer levels of the batched refinement step),
+// workloads (66, 162, the finer levels of the batched refinement step, and
+// 194, the coarsest level of the full form's grid),
 // generic strides otherwise; one kernel per stencil order
 template <int ORD>
 static void z4_interior_fp64(const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVarPtrs &pre, const ZVarPtrs &acc,
@@ -1610,7 +1611,7 @@ static void z4_interior_fp64(const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVa
   }
   if constexpr (ORD >= 4) {
     NRGPU_Z4_FIXED(162) NRGPU_Z4_FIXED(168) NRGPU_Z4_FIXED(136) NRGPU_Z4_FIXED(104) NRGPU_Z4_FIXED(72)
-    NRGPU_Z4_FIXED(66)
+    NRGPU_Z4_FIXED(66) NRGPU_Z4_FIXED(194)
   }
 #undef NRGPU_Z4_FIXED
   z4_rhs_kernel<0, 0, 0, ORD><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
