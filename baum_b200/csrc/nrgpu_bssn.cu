@@ -149,6 +149,32 @@ __device__ __forceinline__ void bssn_point(const CVarPtrs &U, const PointCtx &P,
   gi[4] = detginv * (g[1] * g[2] - g[0] * g[4]);
   gi[5] = detginv * (g[0] * g[3] - g[1] * g[1]);
 
+  // Ricci tensor of the conformal metric.  Its -1/2 ginv^cd d_c d_d g_ab
+  // part (folded over the symmetric pair c, d): with compile-time strides it
+  // comes first, so that its stencil loads have no connection values live
+  // beside them; with run-time strides after the connection terms
+  double Rt[6];
+#pragma unroll
+  for (int a = 0; a < 6; ++a) Rt[a] = 0.0;
+  auto ricci_dd = [&]() {
+    const double o2[3] = {1.0 / (den2<ORD>() * P.h[0] * P.h[0]), 1.0 / (den2<ORD>() * P.h[1] * P.h[1]),
+                          1.0 / (den2<ORD>() * P.h[2] * P.h[2])};
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int d = c; d < 3; ++d) {
+        const double w = (c == d ? -0.5 : -1.0) * gi[sy(c, d)] * (c == d ? o2[c] : o1[c] * o1[d]);
+#pragma unroll
+        for (int a = 0; a < 6; ++a) {
+          const double dd = c == d ? d2n<ORD>(U.p[G11 + a], x, STR(c))
+                                   : d11n<ORD>(U.p[G11 + a], x, STR(c), STR(d));
+          Rt[a] += w * dd;
+        }
+      }
+  };
+  constexpr bool kDdFirst = CSY > 0;
+  if constexpr (kDdFirst) ricci_dd();
+
   // connection: gdo[c][ab] = 1/2 (d_a g_bc + d_b g_ac - d_c g_ab), gam = ginv gdo
   double gdo[3][6], gam[3][6], Gfg[3];
   {
@@ -175,8 +201,7 @@ __device__ __forceinline__ void bssn_point(const CVarPtrs &U, const PointCtx &P,
     Gfg[a] = gi[0] * gam[a][0] + gi[3] * gam[a][3] + gi[5] * gam[a][5] +
              2.0 * (gi[1] * gam[a][1] + gi[2] * gam[a][2] + gi[4] * gam[a][4]);
 
-  // Ricci tensor of the conformal metric plus, later, the chi part
-  double Rt[6];
+  // the connection terms of the Ricci tensor plus, later, the chi part
 #pragma unroll
   for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -193,24 +218,10 @@ __device__ __forceinline__ void bssn_point(const CVarPtrs &U, const PointCtx &P,
                  gam[e][sy(a, d)] * gdo[e][sy(c, b)];
           t += gi[sy(c, d)] * q;
         }
-      Rt[sy(a, b)] = t;
+      Rt[sy(a, b)] += t;
     }
+  if constexpr (!kDdFirst) ricci_dd();
   {
-    // -1/2 ginv^cd d_c d_d g_ab, folded over the symmetric pair (c,d)
-    const double o2[3] = {1.0 / (den2<ORD>() * P.h[0] * P.h[0]), 1.0 / (den2<ORD>() * P.h[1] * P.h[1]),
-                          1.0 / (den2<ORD>() * P.h[2] * P.h[2])};
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-      for (int d = c; d < 3; ++d) {
-        const double w = (c == d ? -0.5 : -1.0) * gi[sy(c, d)] * (c == d ? o2[c] : o1[c] * o1[d]);
-#pragma unroll
-        for (int a = 0; a < 6; ++a) {
-          const double dd = c == d ? d2n<ORD>(U.p[G11 + a], x, STR(c))
-                                   : d11n<ORD>(U.p[G11 + a], x, STR(c), STR(d));
-          Rt[a] += w * dd;
-        }
-      }
     // 1/2 (g_ca d_b G^c + g_cb d_a G^c + G^c (gdo_abc + gdo_bac))
     double dG[3][3];
 #pragma unroll
