@@ -1608,25 +1608,45 @@ static ZCVarPtrs z4_c(const ZVarPtrs &v) {
 
 // FP64 interior launch with compile-time strides for the box sizes of the
 // workloads (66, 162, the finer levels of the batched refinement step, and
-// 194, the coarsest level of the full form's grid),
-// generic strides otherwise; one kernel per stencil order
+// 194, the coarsest level of the full form's grid).  A box of another size
+// up to 194 points per side is staged first into the level's padding
+// buffer with the strides of the next such size (nrgpu_level_pad), whose
+// kernel then reads it: with run-time strides the kernel's tap addresses
+// take registers of their own, it spills, and it runs about half as fast.
+// Generic strides remain for larger boxes; one kernel per stencil order.
 template <int ORD>
 static void z4_interior_fp64(const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVarPtrs &pre, const ZVarPtrs &acc,
                              const Epilogue &E, const nrgpu_z4_params &p, const BoxGeo &bx, nrgpu_level *L, dim3 grd,
                              dim3 blk, cudaStream_t st) {
 #define NRGPU_Z4_FIXED(M_)                                                                                   \
-  if (bx.m == M_ && bx.n == M_) {                                                                           \
-    z4_rhs_kernel<M_, M_ * M_, 0, ORD><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, \
-                                                            L->dy, L->dz, L->d_status, 1, bx.o - 2);        \
+  if (P == M_) {                                                                                             \
+    z4_rhs_kernel<M_, M_ * M_, 0, ORD><<<grd, blk, 0, st>>>(In, out, pre, acc, E, p, bx, L->d_boundary, L->dx, \
+                                                            L->dy, L->dz, L->d_status, 1, bx.o - 2, in_off); \
     return;                                                                                                  \
   }
   if constexpr (ORD >= 4) {
+    ZCVarPtrs In = U;
+    long in_off = bx.noffset;
+    int P = bx.m == bx.n ? bx.m : 0;  // a kernel of its own, if one below matches
+    const int Q = nrgpu_pad_size(bx.m, bx.n);
+    if (Q && L->pad) {
+      P = Q;
+      const long fs = (long)P * P * bx.o;
+      if ((size_t)(NRGPU_Z4_NVARS * fs) <= L->pad_doubles) {
+        const long nb = (long)bx.m * bx.n * bx.o;
+        z4_pad_copy_kernel<<<dim3((unsigned)((nb + 255) / 256), NRGPU_Z4_NVARS), 256, 0, st>>>(U, L->pad, bx, P, fs);
+        for (int v = 0; v < NRGPU_Z4_NVARS; ++v) In.p[v] = L->pad + v * fs;
+        in_off = 0;
+      } else {
+        P = 0;
+      }
+    }
     NRGPU_Z4_FIXED(162) NRGPU_Z4_FIXED(168) NRGPU_Z4_FIXED(136) NRGPU_Z4_FIXED(104) NRGPU_Z4_FIXED(72)
     NRGPU_Z4_FIXED(66) NRGPU_Z4_FIXED(194)
   }
 #undef NRGPU_Z4_FIXED
   z4_rhs_kernel<0, 0, 0, ORD><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
-                                                   L->d_status, 1, bx.o - 2);
+                                                   L->d_status, 1, bx.o - 2, bx.noffset);
 }
 
 // the FP32-stencil options (precision 1, 2): the 162^3 box of the
@@ -1637,7 +1657,7 @@ static void z4_interior_prec(const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVa
                              dim3 blk, cudaStream_t st) {
 #define NR_Z4P(CSY_, CSZ_, ORD_)                                                                               \
   z4_rhs_kernel<CSY_, CSZ_, PREC, ORD_><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, \
-                                                             L->dy, L->dz, L->d_status, 1, bx.o - 2)
+                                                             L->dy, L->dz, L->d_status, 1, bx.o - 2, bx.noffset)
   if (p.order_centered == 6 && bx.m == 162 && bx.n == 162) NR_Z4P(162, 162 * 162, 6);
   else if (p.order_centered == 6) NR_Z4P(0, 0, 6);
   else if (p.order_centered == 4) NR_Z4P(0, 0, 4);
@@ -1657,6 +1677,13 @@ static int z4_launch(nrgpu_level *L, const ZCVarPtrs &U, const ZVarPtrs &out, co
     NRGPU_CUDA_TRY(cudaStreamWaitEvent(L->side, L->ev_fork, 0));
   }
   if (interior) {
+    // the staging buffer of off-size boxes, allocated here unless a graph
+    // is being captured (the refinement driver allocates it beforehand)
+    if (!L->pad_tried) {
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) nrgpu_level_pad(L);
+      cudaGetLastError();
+    }
     for (int b = 0; b < L->nboxes; ++b) {
       const BoxGeo &bx = L->hbox[b];
       if (bx.m < 3 || bx.n < 3 || bx.o < 3) continue;

@@ -38,6 +38,11 @@ struct nrgpu_level {
   // RK4 scratch: three full 24-variable lists, allocated on first use
   double *scratch;
   size_t scratch_points;
+  // staging buffer of a box whose size has no compile-time-stride kernel
+  // (z4_pad_copy_kernel), allocated with the scratch when a box needs it
+  double *pad;
+  size_t pad_doubles;
+  int pad_tried;
   // device copy of a host state for the host-buffer entry points
   double *hoststate;
   // points with boundary flag 0, and the norm reduction buffer (first use)
@@ -83,6 +88,21 @@ int nrgpu_z4_background_boundary(nrgpu_level *L, double *const *unew, double *co
 int nrgpu_z4_rk4_background(nrgpu_level *L, double *const *u, double dt, const nrgpu_z4_params *p, cudaStream_t st);
 // the level's three RK4 scratch lists, allocated on first use (nrgpu_lib.cu)
 int nrgpu_level_scratch(nrgpu_level *L, double **out);
+// the box sizes with a compile-time-stride Z4c rhs kernel; a box of another
+// size up to the largest is staged into a copy with the strides of the next
+// one (nrgpu_level_pad)
+constexpr int kPadSizes[] = {66, 72, 104, 136, 162, 168, 194};
+// the staging size of an m x n box: 0 when it has a kernel of its own or is
+// too large
+inline int nrgpu_pad_size(int m, int n) {
+  if (m == n)
+    for (int c : kPadSizes)
+      if (c == m) return 0;
+  for (int c : kPadSizes)
+    if (c >= m && c >= n) return c;
+  return 0;
+}
+void nrgpu_level_pad(nrgpu_level *L);
 // set_boundary_symmetry on a list of nv variables of the given system
 // (NRGPU_SYSTEM_BSSN / _Z4C); nothing without symmetry (nrgpu_bssn.cu)
 int nrgpu_level_symmetry(nrgpu_level *L, double *const *u, int system, cudaStream_t st);

@@ -193,6 +193,7 @@ extern "C" int nrgpu_level_destroy(nrgpu_level *L) {
   cudaFree(L->d_sym);
   cudaFree(L->rsym);
   cudaFree(L->scratch);
+  cudaFree(L->pad);
   cudaFree(L->hoststate);
   cudaFree(L->d_red);
   cudaFree(L->d_red0d);
@@ -213,6 +214,27 @@ extern "C" int nrgpu_level_destroy(nrgpu_level *L) {
 
 // three variable lists of RK4 scratch (room for the 25 Z4c variables),
 // allocated once per level
+// the staging buffer for boxes of up to 194 points per side without a
+// compile-time-stride kernel of their own: 25 lists with strides (1, P, P P),
+// P the next kernel size (kPadSizes); tried once per level, and a level
+// without it runs those boxes with the run-time-stride kernel
+void nrgpu_level_pad(nrgpu_level *L) {
+  if (L->pad_tried) return;
+  L->pad_tried = 1;
+  size_t need = 0;
+  for (int b = 0; b < L->nboxes; ++b) {
+    const int P = nrgpu_pad_size(L->hbox[b].m, L->hbox[b].n);
+    if (P > 0) need = std::max(need, (size_t)NRGPU_Z4_NVARS * P * P * L->hbox[b].o);
+  }
+  if (need && cudaMalloc(&L->pad, sizeof(double) * need) == cudaSuccess) {
+    L->pad_doubles = need;
+  } else {
+    cudaGetLastError();
+    L->pad = nullptr;
+    L->pad_doubles = 0;
+  }
+}
+
 int nrgpu_level_scratch(nrgpu_level *L, double **out) {
   if (!L->scratch) {
     const size_t bytes = sizeof(double) * 3 * NRGPU_Z4_NVARS * (size_t)L->npoints;
@@ -222,6 +244,7 @@ int nrgpu_level_scratch(nrgpu_level *L, double **out) {
       return nrgpu_set_error(NRGPU_ERR_NOMEM, "RK4 scratch of %zu bytes", bytes);
     }
     L->scratch_points = (size_t)L->npoints;
+    nrgpu_level_pad(L);
   }
   *out = L->scratch;
   return NRGPU_OK;
