@@ -572,11 +572,14 @@ __device__ __forceinline__ int ladder(int order, int d) {
 // (flag 0) only, the flagged ones are handled by bssn_flagged_kernel
 // CSY, CSZ: the box strides dj = m and dk = m n when known at compile time
 // (0 = read them from the box)
+// the input lists are read at in.x + i + in.y (j + in.z k): the box itself,
+// or its staged copy (as for z4_rhs_kernel); the outputs, the previous
+// state and the flags at the box's own index
 template <int CSY = 0, int CSZ = 0, int ORD = 4, int MINB = NRGPU_RHS_MINBLOCKS>
 __global__ void __launch_bounds__(256, MINB) bssn_rhs_kernel(CVarPtrs U, VarPtrs out, CVarPtrs pre, VarPtrs acc,
                                                       Epilogue E, const nrgpu_bssn_params p, BoxGeo box,
                                                       const int *__restrict__ boundary, double dx, double dy,
-                                                      double dz, int *status, int k0, int k1) {
+                                                      double dz, int *status, int k0, int k1, int3 in) {
   const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = k0 + blockIdx.z * blockDim.z + threadIdx.z;
@@ -585,8 +588,9 @@ __global__ void __launch_bounds__(256, MINB) bssn_rhs_kernel(CVarPtrs U, VarPtrs
   P.i = i; P.j = j; P.k = k;
   P.imax = box.m - 1; P.jmax = box.n - 1; P.kmax = box.o - 1;
   P.st[0] = 1; P.st[1] = box.m; P.st[2] = box.m * box.n;
-  P.ijk = box.noffset + i + box.m * (j + box.n * k);
-  if (__ldg(boundary + P.ijk) != 0) return;
+  const int xo = box.noffset + i + box.m * (j + box.n * k);
+  P.ijk = in.x + i + in.y * (j + in.z * k);
+  if (__ldg(boundary + xo) != 0) return;
   P.h[0] = dx; P.h[1] = dy; P.h[2] = dz;
   int d = min(min(i, j), k);
   d = min(d, min(min(P.imax - i, P.jmax - j), P.kmax - k));
@@ -600,7 +604,19 @@ __global__ void __launch_bounds__(256, MINB) bssn_rhs_kernel(CVarPtrs U, VarPtrs
 #pragma unroll
   for (int v = 0; v < NRGPU_NV; ++v) s += r[v];
   if (!isfinite(s)) atomicOr(status, 1);
-  store(r, P.ijk, out, pre, acc, E, p);
+  store(r, xo, out, pre, acc, E, p);
+}
+
+// a box's nv input lists into the staging buffer with strides (1, P, P P):
+// field v at pad + v fs, point (i, j, k) at i + P (j + P k)
+template <class CP>
+__global__ void pad_copy_kernel(CP U, double *__restrict__ pad, BoxGeo box, int P, long fs) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long nb = (long)box.m * box.n * box.o;
+  if (t >= nb) return;
+  const int v = blockIdx.y;
+  const int i = (int)(t % box.m), j = (int)((t / box.m) % box.n), k = (int)(t / ((long)box.m * box.n));
+  pad[v * fs + i + (long)P * (j + (long)P * k)] = ldg(U.p[v] + box.noffset + t);
 }
 
 // the points of the order ladder (flag 0, within 2 of a box face, sorted by
@@ -1032,6 +1048,13 @@ static int launch_rhs(nrgpu_level *L, const CVarPtrs &U, const VarPtrs &out, con
     NRGPU_CUDA_TRY(cudaStreamWaitEvent(L->side, L->ev_fork, 0));
   }
   if (interior) {
+    // the staging buffer of off-size boxes, allocated here unless a graph
+    // is being captured (the refinement driver allocates it beforehand)
+    if (!L->pad_tried) {
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) nrgpu_level_pad(L);
+      cudaGetLastError();
+    }
     for (int b = 0; b < L->nboxes; ++b) {
       const BoxGeo &bx = L->hbox[b];
       if (bx.m < 3 || bx.n < 3 || bx.o < 3) continue;
@@ -1049,19 +1072,46 @@ static int launch_rhs(nrgpu_level *L, const CVarPtrs &U, const VarPtrs &out, con
       // measured fastest for this box); 128 or 256 threads, one point each
       const dim3 blk(L->blk[0], L->blk[1], L->blk[2]);
       const dim3 grd((bx.m - 2 + blk.x - 1) / blk.x, (bx.n - 2 + blk.y - 1) / blk.y, (k1 - k0 + blk.z) / blk.z);
-      // box strides as compile-time constants for the sizes of the standard
-      // workloads (every stencil tap becomes one load with an immediate
-      // offset), one kernel per stencil order
+      // box strides as compile-time constants (every stencil tap becomes one
+      // load with an immediate offset) for the box sizes of kPadSizes; a box
+      // of another size up to the largest is staged into the level's padding
+      // buffer with the strides of the next one (as for Z4c); run-time
+      // strides otherwise; one kernel per stencil order
       const int ord = p.order_centered;
-#define NR_BSSN_LDG(CSY_, CSZ_, ORD_)                                                                    \
-  bssn_rhs_kernel<CSY_, CSZ_, ORD_><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, \
-                                                        L->dz, L->d_status, k0, k1)
-      if (bx.m == 66 && bx.n == 66 && ord == 4) NR_BSSN_LDG(66, 66 * 66, 4);
-      else if (bx.m == 66 && bx.n == 66 && ord == 6) NR_BSSN_LDG(66, 66 * 66, 6);
-      else if (bx.m == 162 && bx.n == 162 && ord == 6) NR_BSSN_LDG(162, 162 * 162, 6);
-      else if (ord == 2) NR_BSSN_LDG(0, 0, 2);
-      else if (ord == 4) NR_BSSN_LDG(0, 0, 4);
-      else NR_BSSN_LDG(0, 0, 6);
+      CVarPtrs In = U;
+      int3 in = make_int3(bx.noffset, bx.m, bx.n);
+      int P = ord >= 4 && bx.m == bx.n ? bx.m : 0;
+      const int Q = ord >= 4 ? nrgpu_pad_size(bx.m, bx.n) : 0;
+      if (Q && L->pad) {
+        const long fs = (long)Q * Q * bx.o;
+        P = 0;
+        if ((size_t)(NRGPU_NV * fs) <= L->pad_doubles) {
+          const long nb = (long)bx.m * bx.n * bx.o;
+          pad_copy_kernel<<<dim3((unsigned)((nb + 255) / 256), NRGPU_NV), 256, 0, st>>>(U, L->pad, bx, Q, fs);
+          for (int v = 0; v < NRGPU_NV; ++v) In.p[v] = L->pad + v * fs;
+          in = make_int3(0, Q, Q);
+          P = Q;
+        }
+      }
+#define NR_BSSN_LDG(CSY_, CSZ_, ORD_)                                                                          \
+  bssn_rhs_kernel<CSY_, CSZ_, ORD_><<<grd, blk, 0, st>>>(In, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, \
+                                                        L->dz, L->d_status, k0, k1, in)
+#define NR_BSSN_SIZE(M_)                          \
+  else if (P == M_ && ord == 4) NR_BSSN_LDG(M_, M_ * M_, 4); \
+  else if (P == M_ && ord == 6) NR_BSSN_LDG(M_, M_ * M_, 6);
+      if (false) {
+      }
+      NR_BSSN_SIZE(66) NR_BSSN_SIZE(72) NR_BSSN_SIZE(104) NR_BSSN_SIZE(136) NR_BSSN_SIZE(162) NR_BSSN_SIZE(168)
+      NR_BSSN_SIZE(194)
+      else if (ord == 2) bssn_rhs_kernel<0, 0, 2><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary,
+                                                                       L->dx, L->dy, L->dz, L->d_status, k0, k1,
+                                                                       make_int3(bx.noffset, bx.m, bx.n));
+      else if (ord == 4) bssn_rhs_kernel<0, 0, 4><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary,
+                                                                       L->dx, L->dy, L->dz, L->d_status, k0, k1,
+                                                                       make_int3(bx.noffset, bx.m, bx.n));
+      else bssn_rhs_kernel<0, 0, 6><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy,
+                                                         L->dz, L->d_status, k0, k1, make_int3(bx.noffset, bx.m, bx.n));
+#undef NR_BSSN_SIZE
 #undef NR_BSSN_LDG
     }
     // the ladder points of all boxes (beside the interior kernel)
@@ -1621,12 +1671,12 @@ static void z4_interior_fp64(const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVa
 #define NRGPU_Z4_FIXED(M_)                                                                                   \
   if (P == M_) {                                                                                             \
     z4_rhs_kernel<M_, M_ * M_, 0, ORD><<<grd, blk, 0, st>>>(In, out, pre, acc, E, p, bx, L->d_boundary, L->dx, \
-                                                            L->dy, L->dz, L->d_status, 1, bx.o - 2, in_off); \
+                                                            L->dy, L->dz, L->d_status, 1, bx.o - 2, in);     \
     return;                                                                                                  \
   }
   if constexpr (ORD >= 4) {
     ZCVarPtrs In = U;
-    long in_off = bx.noffset;
+    int3 in = make_int3(bx.noffset, bx.m, bx.n);
     int P = bx.m == bx.n ? bx.m : 0;  // a kernel of its own, if one below matches
     const int Q = nrgpu_pad_size(bx.m, bx.n);
     if (Q && L->pad) {
@@ -1634,9 +1684,9 @@ static void z4_interior_fp64(const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVa
       const long fs = (long)P * P * bx.o;
       if ((size_t)(NRGPU_Z4_NVARS * fs) <= L->pad_doubles) {
         const long nb = (long)bx.m * bx.n * bx.o;
-        z4_pad_copy_kernel<<<dim3((unsigned)((nb + 255) / 256), NRGPU_Z4_NVARS), 256, 0, st>>>(U, L->pad, bx, P, fs);
+        pad_copy_kernel<<<dim3((unsigned)((nb + 255) / 256), NRGPU_Z4_NVARS), 256, 0, st>>>(U, L->pad, bx, P, fs);
         for (int v = 0; v < NRGPU_Z4_NVARS; ++v) In.p[v] = L->pad + v * fs;
-        in_off = 0;
+        in = make_int3(0, P, P);
       } else {
         P = 0;
       }
@@ -1646,7 +1696,7 @@ static void z4_interior_fp64(const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVa
   }
 #undef NRGPU_Z4_FIXED
   z4_rhs_kernel<0, 0, 0, ORD><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, L->dy, L->dz,
-                                                   L->d_status, 1, bx.o - 2, bx.noffset);
+                                                   L->d_status, 1, bx.o - 2, make_int3(bx.noffset, bx.m, bx.n));
 }
 
 // the FP32-stencil options (precision 1, 2): the 162^3 box of the
@@ -1657,7 +1707,8 @@ static void z4_interior_prec(const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVa
                              dim3 blk, cudaStream_t st) {
 #define NR_Z4P(CSY_, CSZ_, ORD_)                                                                               \
   z4_rhs_kernel<CSY_, CSZ_, PREC, ORD_><<<grd, blk, 0, st>>>(U, out, pre, acc, E, p, bx, L->d_boundary, L->dx, \
-                                                             L->dy, L->dz, L->d_status, 1, bx.o - 2, bx.noffset)
+                                                             L->dy, L->dz, L->d_status, 1, bx.o - 2,       \
+                                                             make_int3(bx.noffset, bx.m, bx.n))
   if (p.order_centered == 6 && bx.m == 162 && bx.n == 162) NR_Z4P(162, 162 * 162, 6);
   else if (p.order_centered == 6) NR_Z4P(0, 0, 6);
   else if (p.order_centered == 4) NR_Z4P(0, 0, 4);

@@ -39,7 +39,7 @@ struct nrgpu_level {
   double *scratch;
   size_t scratch_points;
   // staging buffer of a box whose size has no compile-time-stride kernel
-  // (z4_pad_copy_kernel), allocated with the scratch when a box needs it
+  // (pad_copy_kernel), allocated with the scratch when a box needs it
   double *pad;
   size_t pad_doubles;
   int pad_tried;

@@ -409,15 +409,15 @@ __device__ __forceinline__ void z4_store(const double r[ZNV], int x, const ZVarP
   }
 }
 
-// With compile-time strides (CSY, CSZ) the input lists U are read at
-// in_off + i + CSY j + CSZ k: the box's own place when its size is CSY, or a
-// staged copy of the box with those strides (z4_pad_copy_kernel); the
-// outputs, the previous state and the flags are at the box's own index.
+// The input lists U are read at in.x + i + in.y (j + in.z k): the box's
+// own place, or a staged copy of the box whose strides are the kernel's
+// compile-time ones (pad_copy_kernel); the outputs, the previous state and
+// the flags are at the box's own index.
 template <int CSY = 0, int CSZ = 0, int PREC = 0, int ORD = 4>
 __global__ void __launch_bounds__(256, NRGPU_RHS_MINBLOCKS) z4_rhs_kernel(ZCVarPtrs U, ZVarPtrs out, ZCVarPtrs pre, ZVarPtrs acc, Epilogue E,
                                                     const nrgpu_z4_params p, BoxGeo box,
                                                     const int *__restrict__ boundary, double dx, double dy, double dz,
-                                                    int *status, int k0, int k1, long in_off) {
+                                                    int *status, int k0, int k1, int3 in) {
   const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = k0 + blockIdx.z * blockDim.z + threadIdx.z;
@@ -427,7 +427,7 @@ __global__ void __launch_bounds__(256, NRGPU_RHS_MINBLOCKS) z4_rhs_kernel(ZCVarP
   P.imax = box.m - 1; P.jmax = box.n - 1; P.kmax = box.o - 1;
   P.st[0] = 1; P.st[1] = box.m; P.st[2] = box.m * box.n;
   const int xo = box.noffset + i + box.m * (j + box.n * k);
-  P.ijk = CSY > 0 ? (int)(in_off + i + (long)CSY * j + (long)CSZ * k) : xo;
+  P.ijk = in.x + i + in.y * (j + in.z * k);
   if (__ldg(boundary + xo) != 0) return;
   P.h[0] = dx; P.h[1] = dy; P.h[2] = dz;
   int d = min(min(i, j), k);
@@ -442,17 +442,6 @@ __global__ void __launch_bounds__(256, NRGPU_RHS_MINBLOCKS) z4_rhs_kernel(ZCVarP
   for (int v = 0; v < ZNV; ++v) s += r[v];
   if (!isfinite(s)) atomicOr(status, 1);
   z4_store(r, xo, out, pre, acc, E, p);
-}
-
-// a box's 25 input lists into the staging buffer with strides (1, P, P P):
-// field v at pad + v fs, point (i, j, k) at i + P (j + P k)
-__global__ void z4_pad_copy_kernel(ZCVarPtrs U, double *__restrict__ pad, BoxGeo box, int P, long fs) {
-  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long nb = (long)box.m * box.n * box.o;
-  if (t >= nb) return;
-  const int v = blockIdx.y;
-  const int i = (int)(t % box.m), j = (int)((t / box.m) % box.n), k = (int)(t / ((long)box.m * box.n));
-  pad[v * fs + i + (long)P * (j + (long)P * k)] = ldg(U.p[v] + box.noffset + t);
 }
 
 // the order-ladder points of a level (see bssn_ladder_kernel)
