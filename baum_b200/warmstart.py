@@ -5,7 +5,7 @@ Bowen-York momenta and spins) predicts the correction u of the puncture
 method; the multigrid then runs V cycles from that guess on the finest level
 (cycle type "V", not the full-V driver, which would overwrite the guess from
 the coarsest level up: solve.c:40,89-91, utility.c:61-82), to the same
-1e-10 RMS residual.  The multigrid stays the judge: the guess only changes
+1e-10 RMS residual.  The multigrid stays the arbiter: the guess only changes
 where it starts.
 
 Everything numeric runs in libnrgpu.so (nrgpu_mlp_*, nrgpu_mg_*): features,

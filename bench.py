@@ -202,7 +202,7 @@ iterations = 0
 
 
 def mg_binaries(n):
-    """The survey's binary (m = 0.5 each at x = +-4, P_y = +-0.1,
+    """The standard binary (m = 0.5 each at x = +-4, P_y = +-0.1,
     S_z = +-0.1), then n - 1 seeded draws of the workload's parameter
     distribution (they are not among the warm start's training draws, which
     use other seeds)."""
@@ -801,7 +801,7 @@ def run_ours(args, rank, world):
         cpu = {"value": c["value"], "unit": UNIT, "cores": c["cores"], "kind": "port", "sample": c["sample"]}
     # the multigrid half of the metric: V cycles and ms to the 1e-10 RMS
     # residual on the 129^3-cell binary-puncture grid (dx = 0.25, x in
-    # [-16.1, 16.1]): the survey's binary and 5 seeded draws of the
+    # [-16.1, 16.1]): the standard binary and 5 seeded draws of the
     # workload's distribution, full-V from u = 0 as the reference does, V
     # cycles from u = 0 and from the learned warm start; the reference on
     # the same binaries at 66^3 (dx = 0.5, the same domain) for the first two

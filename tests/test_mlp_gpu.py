@@ -165,7 +165,7 @@ def test_predict_u_fp32_matches_fp64_forward(gpu):
     assert np.abs(u[idx] - ref).max() <= 2e-5 * np.abs(ref).max()
 
 
-SURVEY_BINARY = Binary([0.5, 0.5], [[4, 0, 0], [-4, 0, 0]], [[0, 0.1, 0], [0, -0.1, 0]], [[0, 0, 0.1], [0, 0, -0.1]])
+STANDARD_BINARY = Binary([0.5, 0.5], [[4, 0, 0], [-4, 0, 0]], [[0, 0.1, 0], [0, -0.1, 0]], [[0, 0, 0.1], [0, 0, -0.1]])
 
 
 def test_warm_start_is_close_and_lowers_the_initial_residual(gpu):
@@ -180,7 +180,7 @@ def test_warm_start_is_close_and_lowers_the_initial_residual(gpu):
     m, dx = warmstart.C2_M, warmstart.C2_DX
     mg = Multigrid(m, dx, abi.mg_params(fullV=0, vcycle_nmax=1))
     ref = Multigrid(m, dx, abi.mg_params(vcycle_nmax=300))
-    for b in [SURVEY_BINARY, Binary.sample(rng)]:
+    for b in [STANDARD_BINARY, Binary.sample(rng)]:
         u_ref, _, _ = warmstart.solve_binary(ref, b)
         g = net.predict_u(b, m, dx)
         assert (g - u_ref).norm().item() <= 0.05 * u_ref.norm().item()
@@ -197,13 +197,13 @@ def test_warm_start_halves_vcycles(gpu):
     """The north-star target on the workload's grid (130^3, x in
     [-16.1, 16.1]): V cycles to the 1e-10 RMS residual from the warm start
     (the network's u in FP32, 32 damped Jacobi sweeps) at most half of
-    those from u = 0, both V cycles and the reference's full-V.  The survey's
+    those from u = 0, both V cycles and the reference's full-V.  The standard
     binary (measured 329 full-V, 342 V, 75 from the warm start) and a
     held-out draw (4760, 4831, 149)."""
     from baum_b200.punctures import Binary
     net = warmstart.Network.load()
     held = Binary.sample(np.random.default_rng(12))
-    rows = warmstart.evaluate(net, [SURVEY_BINARY, held], nmax=8000, log=None)
+    rows = warmstart.evaluate(net, [STANDARD_BINARY, held], nmax=8000, log=None)
     for r in rows:
         assert r["res_mlp"] <= 1e-10 and r["res_V"] <= 1e-10 and r["res_fullV"] <= 1e-10, r
         assert 2 * r["V_from_mlp"] <= min(r["V_from_zero"], r["fullV_from_zero"]), r
