@@ -1081,7 +1081,9 @@ static int launch_rhs(nrgpu_level *L, const CVarPtrs &U, const VarPtrs &out, con
       CVarPtrs In = U;
       int3 in = make_int3(bx.noffset, bx.m, bx.n);
       int P = ord >= 4 && bx.m == bx.n ? bx.m : 0;
-      const int Q = ord >= 4 ? nrgpu_pad_size(bx.m, bx.n) : 0;
+      // (a launch on some planes only, the host-buffer step's slabs, reads
+      // the box in place)
+      const int Q = ord >= 4 && k0 == 1 && k1 == bx.o - 2 ? nrgpu_pad_size(bx.m, bx.n) : 0;
       if (Q && L->pad) {
         const long fs = (long)Q * Q * bx.o;
         P = 0;
