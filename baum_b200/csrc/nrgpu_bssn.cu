@@ -607,16 +607,17 @@ __global__ void __launch_bounds__(256, MINB) bssn_rhs_kernel(CVarPtrs U, VarPtrs
   store(r, xo, out, pre, acc, E, p);
 }
 
-// a box's nv input lists into the staging buffer with strides (1, P, P P):
-// field v at pad + v fs, point (i, j, k) at i + P (j + P k)
+// planes klo..khi of a box's nv input lists into the staging buffer with
+// strides (1, P, P P): field v at pad + v fs, point (i, j, k) at
+// i + P (j + P k)
 template <class CP>
-__global__ void pad_copy_kernel(CP U, double *__restrict__ pad, BoxGeo box, int P, long fs) {
+__global__ void pad_copy_kernel(CP U, double *__restrict__ pad, BoxGeo box, int P, long fs, int klo, int khi) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long nb = (long)box.m * box.n * box.o;
-  if (t >= nb) return;
+  const long mn = (long)box.m * box.n;
+  if (t >= mn * (khi - klo + 1)) return;
   const int v = blockIdx.y;
-  const int i = (int)(t % box.m), j = (int)((t / box.m) % box.n), k = (int)(t / ((long)box.m * box.n));
-  pad[v * fs + i + (long)P * (j + (long)P * k)] = ldg(U.p[v] + box.noffset + t);
+  const int i = (int)(t % box.m), j = (int)((t / box.m) % box.n), k = klo + (int)(t / mn);
+  pad[v * fs + i + (long)P * (j + (long)P * k)] = ldg(U.p[v] + box.noffset + i + mn * k + (long)box.m * j);
 }
 
 // the points of the order ladder (flag 0, within 2 of a box face, sorted by
@@ -1081,15 +1082,18 @@ static int launch_rhs(nrgpu_level *L, const CVarPtrs &U, const VarPtrs &out, con
       CVarPtrs In = U;
       int3 in = make_int3(bx.noffset, bx.m, bx.n);
       int P = ord >= 4 && bx.m == bx.n ? bx.m : 0;
-      // (a launch on some planes only, the host-buffer step's slabs, reads
-      // the box in place)
-      const int Q = ord >= 4 && k0 == 1 && k1 == bx.o - 2 ? nrgpu_pad_size(bx.m, bx.n) : 0;
+      const int Q = ord >= 4 ? nrgpu_pad_size(bx.m, bx.n) : 0;
       if (Q && L->pad) {
         const long fs = (long)Q * Q * bx.o;
         P = 0;
         if ((size_t)(NRGPU_NV * fs) <= L->pad_doubles) {
-          const long nb = (long)bx.m * bx.n * bx.o;
-          pad_copy_kernel<<<dim3((unsigned)((nb + 255) / 256), NRGPU_NV), 256, 0, st>>>(U, L->pad, bx, Q, fs);
+          // the planes the launch's stencils reach (a launch on some planes:
+          // the host-buffer step's slabs)
+          const int H = max(max(p.order_advection, p.order_centered / 2 + 1), p.order_dissipation / 2 + 1);
+          const int klo = max(0, k0 - H), khi = min(bx.o - 1, k1 + H);
+          const long nb = (long)bx.m * bx.n * (khi - klo + 1);
+          pad_copy_kernel<<<dim3((unsigned)((nb + 255) / 256), NRGPU_NV), 256, 0, st>>>(U, L->pad, bx, Q, fs, klo,
+                                                                                        khi);
           for (int v = 0; v < NRGPU_NV; ++v) In.p[v] = L->pad + v * fs;
           in = make_int3(0, Q, Q);
           P = Q;
@@ -1686,7 +1690,8 @@ static void z4_interior_fp64(const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVa
       const long fs = (long)P * P * bx.o;
       if ((size_t)(NRGPU_Z4_NVARS * fs) <= L->pad_doubles) {
         const long nb = (long)bx.m * bx.n * bx.o;
-        pad_copy_kernel<<<dim3((unsigned)((nb + 255) / 256), NRGPU_Z4_NVARS), 256, 0, st>>>(U, L->pad, bx, P, fs);
+        pad_copy_kernel<<<dim3((unsigned)((nb + 255) / 256), NRGPU_Z4_NVARS), 256, 0, st>>>(U, L->pad, bx, P, fs, 0,
+                                                                                              bx.o - 1);
         for (int v = 0; v < NRGPU_Z4_NVARS; ++v) In.p[v] = L->pad + v * fs;
         in = make_int3(0, P, P);
       } else {
