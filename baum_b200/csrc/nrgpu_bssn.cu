@@ -491,6 +491,10 @@ __device__ __forceinline__ void bssn_point(const CVarPtrs &U, const PointCtx &P,
 }
 
 // ---- epilogues ----------------------------------------------------------------
+// a hint that the line holding p will be read soon: fetched into L2, no
+// register written (PTX prefetch.global.L2)
+__device__ __forceinline__ void l2_prefetch(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 enum { EPI_RHS = 0, EPI_ADDLINEAR = 1, EPI_RK = 2 };
 
 // EPI_RK accumulator modes: ACC_ADD acc += wacc rhs; ACC_INIT acc = upre +
@@ -598,6 +602,15 @@ __global__ void __launch_bounds__(256, MINB) bssn_rhs_kernel(CVarPtrs U, VarPtrs
   // order (the ladder): bssn_ladder_kernel computes them
   if (d < ORD / 2) return;
   P.dist = d;
+  // the RK epilogue reads the accumulator and the previous state at the
+  // end; ask L2 for their lines now, so that those loads do not wait on DRAM
+  if (E.mode == EPI_RK) {
+#pragma unroll
+    for (int v = 0; v < NRGPU_NV; ++v) {
+      if (E.accmode != ACC_INIT) l2_prefetch(acc.p[v] + xo);
+      if (E.accmode == ACC_INIT || E.has_v) l2_prefetch(pre.p[v] + xo);
+    }
+  }
   double r[NRGPU_NV];
   bssn_point<ORD, CSY, CSZ>(U, P, p, r);
   double s = 0.0;

@@ -435,6 +435,15 @@ __global__ void __launch_bounds__(256, NRGPU_RHS_MINBLOCKS) z4_rhs_kernel(ZCVarP
   // the points of the order ladder are z4_ladder_kernel's
   if (d < ORD / 2) return;
   P.dist = d;
+  // the RK epilogue's accumulator and previous state into L2 now (as in
+  // bssn_rhs_kernel)
+  if (E.mode == EPI_RK) {
+#pragma unroll
+    for (int v = 0; v < ZNV; ++v) {
+      if (E.accmode != ACC_INIT) l2_prefetch(acc.p[v] + xo);
+      if (E.accmode == ACC_INIT || E.has_v) l2_prefetch(pre.p[v] + xo);
+    }
+  }
   double r[ZNV];
   z4_point<ORD, CSY, CSZ, PREC>(U, P, p, r);
   double s = 0.0;
