@@ -602,6 +602,11 @@ __global__ void __launch_bounds__(256, MINB) bssn_rhs_kernel(CVarPtrs U, VarPtrs
   // order (the ladder): bssn_ladder_kernel computes them
   if (d < ORD / 2) return;
   P.dist = d;
+  // the point's own values of every input list, which its stencils and its
+  // neighbours' stencils read one field after another: all their lines
+  // requested from DRAM at once
+#pragma unroll
+  for (int v = 0; v < NRGPU_NV; ++v) l2_prefetch(U.p[v] + P.ijk);
   // the RK epilogue reads the accumulator and the previous state at the
   // end; ask L2 for their lines now, so that those loads do not wait on DRAM
   if (E.mode == EPI_RK) {
