@@ -379,6 +379,7 @@ def lib():
         "nrgpu_level_block": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
         "nrgpu_level_get_block": (C.c_int, [vp, C.POINTER(C.c_int)]),
         "nrgpu_level_tile": (C.c_int, [vp, C.c_int]),
+        "nrgpu_level_queue": (C.c_int, [vp, C.c_int]),
         "nrgpu_puncture_coefficients": (C.c_int, [C.c_int, C.c_double, C.c_int, C.POINTER(C.c_double),
                                                   C.POINTER(C.c_double), C.POINTER(C.c_double),
                                                   C.POINTER(C.c_double), vp, vp, vp]),

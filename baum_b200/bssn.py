@@ -75,6 +75,14 @@ class DeviceLevel:
         abi.check(abi.lib().nrgpu_level_autotune(self.handle, int(system), C.byref(params), _stream(stream), b))
         return tuple(b)
 
+    def queue(self, on=-1):
+        """The Z4c interior of all boxes in one persistent launch over a
+        queue of tiles (nrgpu_level_queue): on = 1, 0, or -1 to query."""
+        r = abi.lib().nrgpu_level_queue(self.handle, int(on))
+        if r < 0:
+            abi.check(r)
+        return int(r)
+
     def tile(self, on=-1):
         """The staged-tile (TMA) interior rhs: on = 1 (a block per tile), 2
         (persistent), 0 (off); -1 only queries; returns the setting."""

@@ -1741,6 +1741,48 @@ static void z4_interior_prec(const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVa
 #undef NR_Z4P
 }
 
+// the box size of a level that the queue kernel can run: all boxes m x m
+// in x and y with m a compile-time-stride size, at 4th or 6th order, FP64,
+// more than one box; 0 otherwise
+static int z4_queue_size(const nrgpu_level *L, const nrgpu_z4_params &p) {
+  if (L->nboxes < 2 || p.precision || p.order_centered < 4) return 0;
+  const int m = L->hbox[0].m;
+  for (int b = 0; b < L->nboxes; ++b)
+    if (L->hbox[b].m != m || L->hbox[b].n != m || L->hbox[b].o != L->hbox[0].o) return 0;
+  for (int c : kPadSizes)
+    if (c == m) return m;
+  return 0;
+}
+
+// the interior of all boxes of the level by z4_rhs_queue_kernel
+static int z4_queue_launch(nrgpu_level *L, int m, const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVarPtrs &pre,
+                           const ZVarPtrs &acc, const Epilogue &E, const nrgpu_z4_params &p, cudaStream_t st) {
+  const BoxGeo &b0 = L->hbox[0];
+  const dim3 blk(L->blk[0], L->blk[1], L->blk[2]);
+  const int3 tiles = make_int3((b0.m - 2 + blk.x - 1) / blk.x, (b0.n - 2 + blk.y - 1) / blk.y,
+                               (b0.o - 2 + blk.z - 1) / blk.z);
+  const int total = tiles.x * tiles.y * tiles.z * L->nboxes;
+  // resident blocks: one or two per SM at 255 registers; more would wait
+  const int per_sm = blk.x * blk.y * blk.z <= 128 ? 2 : 1;
+  const int grid = min(total, L->nsm * per_sm);
+  int *counter = L->d_status + 2;
+  NRGPU_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(int), st));
+#define NR_Z4Q(M_, O_)                                                                                               \
+  z4_rhs_queue_kernel<M_, M_ * M_, O_><<<grid, blk, 0, st>>>(U, out, pre, acc, E, p, L->d_box, L->nboxes, tiles,       \
+                                                             L->d_boundary, L->dx, L->dy, L->dz, L->d_status, counter)
+#define NR_Z4Q_SIZE(M_)                                    \
+  if (m == M_) {                                           \
+    if (p.order_centered == 4) NR_Z4Q(M_, 4);              \
+    else NR_Z4Q(M_, 6);                                    \
+  }
+  NR_Z4Q_SIZE(66) NR_Z4Q_SIZE(72) NR_Z4Q_SIZE(104) NR_Z4Q_SIZE(136) NR_Z4Q_SIZE(162) NR_Z4Q_SIZE(168)
+  NR_Z4Q_SIZE(194)
+#undef NR_Z4Q_SIZE
+#undef NR_Z4Q
+  NRGPU_CUDA_TRY(cudaGetLastError());
+  return NRGPU_OK;
+}
+
 static int z4_launch(nrgpu_level *L, const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVarPtrs &pre,
                      const ZVarPtrs &acc, const Epilogue &E, const nrgpu_z4_params &p, cudaStream_t st, bool interior,
                      bool flagged) {
@@ -1760,7 +1802,13 @@ static int z4_launch(nrgpu_level *L, const ZCVarPtrs &U, const ZVarPtrs &out, co
       if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone) nrgpu_level_pad(L);
       cudaGetLastError();
     }
-    for (int b = 0; b < L->nboxes; ++b) {
+    // all boxes in one persistent launch (nrgpu_level_queue), or one launch per box
+    const int qm = L->queue ? z4_queue_size(L, p) : 0;
+    if (qm) {
+      int e = z4_queue_launch(L, qm, U, out, pre, acc, E, p, st);
+      if (e) return e;
+    }
+    for (int b = 0; b < L->nboxes && !qm; ++b) {
       const BoxGeo &bx = L->hbox[b];
       if (bx.m < 3 || bx.n < 3 || bx.o < 3) continue;
       // the block shape of the level (32 x 4 x 1, or what nrgpu_level_autotune
@@ -2008,6 +2056,27 @@ extern "C" int nrgpu_level_autotune(nrgpu_level *L, int system, const void *para
     }
     L->tile = pick;
   }
+  // the box work-queue kernel (Z4c levels of several equal boxes) against
+  // one launch per box with the fastest shape
+  L->queue = 0;
+  if (!e && system == NRGPU_SYSTEM_Z4C && z4_queue_size(L, *(const nrgpu_z4_params *)params)) {
+    const nrgpu_z4_params &zp = *(const nrgpu_z4_params *)params;
+    ZVarPtrs P, O;
+    for (int v = 0; v < ZNV; ++v) {
+      P.p[v] = scr + (long)v * np;
+      O.p[v] = scr + (long)(ZNV + v) * np;
+    }
+    L->queue = 1;
+    for (int rep = 0; rep < 4 && !e; ++rep) {
+      if (rep == 1) cudaEventRecord(ev0, st);
+      e = z4_launch(L, z4_c(P), O, z4_c(P), O, E, zp, st, true, false);
+    }
+    cudaEventRecord(ev1, st);
+    cudaEventSynchronize(ev1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    if (e || ms >= best) L->queue = 0;
+  }
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
   for (int q = 0; q < 3; ++q)
@@ -2024,6 +2093,13 @@ extern "C" int nrgpu_level_block(nrgpu_level *L, int bx, int by, int bz) {
   L->blk[0] = bx; L->blk[1] = by; L->blk[2] = bz;
   L->tile = 0;
   return NRGPU_OK;
+}
+
+extern "C" int nrgpu_level_queue(nrgpu_level *L, int on) {
+  if (!L) return nrgpu_set_error(NRGPU_ERR_ARG, "null level");
+  if (on > 1) return nrgpu_set_error(NRGPU_ERR_ARG, "queue mode %d (0, 1)", on);
+  if (on >= 0) L->queue = on;
+  return L->queue;
 }
 
 extern "C" int nrgpu_level_tile(nrgpu_level *L, int on) {

@@ -673,6 +673,7 @@ int regrid_level(nrgpu_fmr *F, int m, const nrgpu_level_desc &d, double *const *
   int blk[3];
   if (!nrgpu_level_get_block(oL, blk)) nrgpu_level_block(nL, blk[0], blk[1], blk[2]);
   nrgpu_level_tile(nL, nrgpu_level_tile(oL, -1));
+  nrgpu_level_queue(nL, nrgpu_level_queue(oL, -1));
   const long nnp = d.npoints;
   // time levels of a parent level: u_p, u_pp and u_p2..u_p4 (evolve.c:
   // 250-258), moved with u (move.c:930-939)

@@ -69,6 +69,9 @@ struct nrgpu_level {
   // loads (0), where the level and the parameters allow it; the tensor maps
   // of recently used variable lists (host memory, first use)
   int tile;
+  // 1: the Z4c interior of all boxes in one persistent launch over a queue
+  // of tiles (nrgpu_level_queue), where the boxes allow it
+  int queue;
   void *tma_cache;
   int nsm;   // multiprocessors of the level's device
 };

@@ -409,19 +409,16 @@ __device__ __forceinline__ void z4_store(const double r[ZNV], int x, const ZVarP
   }
 }
 
-// The input lists U are read at in.x + i + in.y (j + in.z k): the box's
-// own place, or a staged copy of the box whose strides are the kernel's
-// compile-time ones (pad_copy_kernel); the outputs, the previous state and
-// the flags are at the box's own index.
-template <int CSY = 0, int CSZ = 0, int PREC = 0, int ORD = 4>
-__global__ void __launch_bounds__(256, NRGPU_RHS_MINBLOCKS) z4_rhs_kernel(ZCVarPtrs U, ZVarPtrs out, ZCVarPtrs pre, ZVarPtrs acc, Epilogue E,
-                                                    const nrgpu_z4_params p, BoxGeo box,
-                                                    const int *__restrict__ boundary, double dx, double dy, double dz,
-                                                    int *status, int k0, int k1, int3 in) {
-  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
-  const int k = k0 + blockIdx.z * blockDim.z + threadIdx.z;
-  if (i > box.m - 2 || j > box.n - 2 || k > k1) return;
+// One inner point (i, j, k) of a box: the input lists U are read at
+// in.x + i + in.y (j + in.z k) (the box's own place, or a staged copy of the
+// box whose strides are the kernel's compile-time ones, pad_copy_kernel);
+// the outputs, the previous state and the flags at the box's own index.
+template <int CSY, int CSZ, int PREC, int ORD>
+__device__ __forceinline__ void z4_interior_point(int i, int j, int k, const BoxGeo &box, int3 in,
+                                                  const ZCVarPtrs &U, const ZVarPtrs &out, const ZCVarPtrs &pre,
+                                                  const ZVarPtrs &acc, const Epilogue &E, const nrgpu_z4_params &p,
+                                                  const int *__restrict__ boundary, double dx, double dy, double dz,
+                                                  int *status) {
   PointCtx P;
   P.i = i; P.j = j; P.k = k;
   P.imax = box.m - 1; P.jmax = box.n - 1; P.kmax = box.o - 1;
@@ -451,6 +448,51 @@ __global__ void __launch_bounds__(256, NRGPU_RHS_MINBLOCKS) z4_rhs_kernel(ZCVarP
   for (int v = 0; v < ZNV; ++v) s += r[v];
   if (!isfinite(s)) atomicOr(status, 1);
   z4_store(r, xo, out, pre, acc, E, p);
+}
+
+template <int CSY = 0, int CSZ = 0, int PREC = 0, int ORD = 4>
+__global__ void __launch_bounds__(256, NRGPU_RHS_MINBLOCKS) z4_rhs_kernel(ZCVarPtrs U, ZVarPtrs out, ZCVarPtrs pre, ZVarPtrs acc, Epilogue E,
+                                                    const nrgpu_z4_params p, BoxGeo box,
+                                                    const int *__restrict__ boundary, double dx, double dy, double dz,
+                                                    int *status, int k0, int k1, int3 in) {
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int k = k0 + blockIdx.z * blockDim.z + threadIdx.z;
+  if (i > box.m - 2 || j > box.n - 2 || k > k1) return;
+  z4_interior_point<CSY, CSZ, PREC, ORD>(i, j, k, box, in, U, out, pre, acc, E, p, boundary, dx, dy, dz, status);
+}
+
+// The interior of every box of a level in one persistent launch: a queue of
+// tiles (the level's block shape) over the boxes, which the blocks take in
+// turn from an atomic counter until it runs past the last; each point as in
+// z4_rhs_kernel, so the results are those of one launch per box.  For levels
+// whose boxes share one size with a compile-time-stride kernel (CSY = m = n):
+// the two puncture boxes per level of the full form's finer levels.  No
+// block waits on another.
+template <int CSY, int CSZ, int ORD>
+__global__ void __launch_bounds__(256, NRGPU_RHS_MINBLOCKS)
+    z4_rhs_queue_kernel(ZCVarPtrs U, ZVarPtrs out, ZCVarPtrs pre, ZVarPtrs acc, Epilogue E, const nrgpu_z4_params p,
+                        const BoxGeo *__restrict__ boxes, int nboxes, int3 tiles, const int *__restrict__ boundary,
+                        double dx, double dy, double dz, int *status, int *counter) {
+  __shared__ int item;
+  const int per_box = tiles.x * tiles.y * tiles.z, total = per_box * nboxes;
+  const bool lead = threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0;
+  for (;;) {
+    if (lead) item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int t = item;
+    __syncthreads();  // every thread has read item before the next take
+    if (t >= total) return;
+    const int b = t / per_box, r = t - b * per_box;
+    const int tx = r % tiles.x, ty = (r / tiles.x) % tiles.y, tz = r / (tiles.x * tiles.y);
+    const BoxGeo box = boxes[b];
+    const int i = 1 + tx * blockDim.x + threadIdx.x;
+    const int j = 1 + ty * blockDim.y + threadIdx.y;
+    const int k = 1 + tz * blockDim.z + threadIdx.z;
+    if (i <= box.m - 2 && j <= box.n - 2 && k <= box.o - 2)
+      z4_interior_point<CSY, CSZ, 0, ORD>(i, j, k, box, make_int3(box.noffset, box.m, box.n), U, out, pre, acc, E,
+                                          p, boundary, dx, dy, dz, status);
+  }
 }
 
 // the order-ladder points of a level (see bssn_ladder_kernel)

@@ -519,6 +519,17 @@ int nrgpu_level_get_block(nrgpu_level *L, int *block);
  * block per SM walking the tiles, the next tile's fields loaded during the
  * current one), 0 off, -1 only queries.  Returns the setting. */
 int nrgpu_level_tile(nrgpu_level *L, int on);
+/* The Z4c interior rhs of all boxes of a level in one persistent launch:
+ * the blocks take tiles from a queue over the boxes (an atomic counter)
+ * until it is empty, each point computed as by the per-box kernel, so the
+ * results are identical.  For levels of two or more boxes of one size that
+ * has a compile-time-stride kernel (66, 72, 104, 136, 162, 168, 194 points
+ * in x and y), 4th or 6th order, FP64; one launch per box otherwise.
+ * on = 1 on, 0 off, -1 only queries; returns the setting.
+ * nrgpu_level_autotune turns it on where it measures faster.  No
+ * counterpart in the reference (advance_levelandsublevels, main.c:397-418,
+ * steps the boxes of a level one after another). */
+int nrgpu_level_queue(nrgpu_level *L, int on);
 
 /* ---- ADM diagnostics ------------------------------------------------------
  * ADM metric and extrinsic curvature from the conformal variables:
