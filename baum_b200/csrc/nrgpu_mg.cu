@@ -129,14 +129,27 @@ __device__ __forceinline__ void fused_store(double *out, int q, int slot, double
   else out[R.bidx[slot]] = R.dirichlet ? -v : v * R.c1[slot] / R.c2[slot];
 }
 
+// (i, j, k) of point q of an m^3 cube from FP64 products with rm = 1/m and
+// rmm = 1/m^2 instead of integer divisions: (q + 1/2) / m^2 lies at least
+// 1/(2 m^2) from an integer, far above the products' rounding, so the
+// truncations are the exact quotients
+__device__ __forceinline__ void cube_ijk(int q, int m, double rm, double rmm, int &i, int &j, int &k) {
+  k = (int)(((double)q + 0.5) * rmm);
+  const int r = q - k * m * m;
+  j = (int)(((double)r + 0.5) * rm);
+  i = r - j * m;
+}
+
 // one Jacobi sweep un = uo + (f - L uo)/L_ii on inner points (Lpuncture_GS),
 // followed by the Robin condition on un (relax.c:19-43 then robin.c:146-223)
 __device__ __forceinline__ void jacobi_at(int t, const double *__restrict__ uo, double *__restrict__ un,
                                           const double *__restrict__ f, const double *__restrict__ a,
-                                          const double *__restrict__ b, int m, double cx, const RobinFuse &R) {
+                                          const double *__restrict__ b, int m, double cx, const RobinFuse &R,
+                                          double rm, double rmm) {
   int q, slot;
   if (!fused_point(t, m * m * m, R, q, slot)) return;
-  const int i = q % m, j = (q / m) % m, k = q / (m * m);
+  int i, j, k;
+  cube_ijk(q, m, rm, rmm, i, j, k);
   if (!inner(i, j, k, m)) return;
   const double cc = -2.0 * (cx + cx + cx);
   const double aq = a[q], bq = b[q], uq = uo[q];
@@ -146,9 +159,9 @@ __device__ __forceinline__ void jacobi_at(int t, const double *__restrict__ uo, 
 }
 __global__ void jacobi_kernel(const double *__restrict__ uo, double *__restrict__ un, const double *__restrict__ f,
                               const double *__restrict__ a, const double *__restrict__ b, int m, double cx,
-                              RobinFuse R, const int *__restrict__ done) {
+                              RobinFuse R, const int *__restrict__ done, double rm, double rmm) {
   if (done && *done) return;
-  jacobi_at(blockIdx.x * blockDim.x + threadIdx.x, uo, un, f, a, b, m, cx, R);
+  jacobi_at(blockIdx.x * blockDim.x + threadIdx.x, uo, un, f, a, b, m, cx, R, rm, rmm);
 }
 
 // a damped Jacobi sweep un = uo + omega (f - L uo)/L_ii with the Robin
@@ -533,9 +546,10 @@ __global__ void __launch_bounds__(NRGPU_MG_BOTTOM_THREADS)
     const MgDev &h = lv[l], &H = lv[l - 1];
     const int np = h.m * h.m * h.m, npH = H.m * H.m * H.m;
     const double cx = 1 / (h.dx * h.dx), cxH = 1 / (H.dx * H.dx);
+    const double rm = 1.0 / h.m, rmm = 1.0 / ((double)h.m * h.m);
     const RobinFuse Rh = {h.bidx, h.bnrm, h.bc1, h.bc2, h.nb, 0}, RH = {H.bidx, H.bnrm, H.bc1, H.bc2, H.nb, 0};
     for (int s = 0; s < npre; ++s) {
-      for (int t = tid; t < np + h.nb; t += nt) jacobi_at(t, U[l], U2[l], h.f, h.a, h.b, h.m, cx, Rh);
+      for (int t = tid; t < np + h.nb; t += nt) jacobi_at(t, U[l], U2[l], h.f, h.a, h.b, h.m, cx, Rh, rm, rmm);
       __syncthreads();
       double *x = U[l];
       U[l] = U2[l];
@@ -563,6 +577,7 @@ __global__ void __launch_bounds__(NRGPU_MG_BOTTOM_THREADS)
     const MgDev &h = lv[l], &H = lv[l - 1];
     const int np = h.m * h.m * h.m, npH = H.m * H.m * H.m;
     const double cx = 1 / (h.dx * h.dx);
+    const double rm = 1.0 / h.m, rmm = 1.0 / ((double)h.m * h.m);
     const RobinFuse Rh = {h.bidx, h.bnrm, h.bc1, h.bc2, h.nb, 0}, RHd = {H.bidx, H.bnrm, H.bc1, H.bc2, H.nb, 1};
     for (int t = tid; t < npH + H.nb; t += nt) sub_inner_at(t, U[l - 1], H.w, H.v, H.m, RHd);
     __syncthreads();
@@ -571,7 +586,7 @@ __global__ void __launch_bounds__(NRGPU_MG_BOTTOM_THREADS)
     for (int t = tid; t < h.nb; t += nt) robin_at(t, U[l], h.bidx, h.bnrm, h.bc1, h.bc2, h.nb, 0);
     __syncthreads();
     for (int s = 0; s < npost; ++s) {
-      for (int t = tid; t < np + h.nb; t += nt) jacobi_at(t, U[l], U2[l], h.f, h.a, h.b, h.m, cx, Rh);
+      for (int t = tid; t < np + h.nb; t += nt) jacobi_at(t, U[l], U2[l], h.f, h.a, h.b, h.m, cx, Rh, rm, rmm);
       __syncthreads();
       double *x = U[l];
       U[l] = U2[l];
@@ -821,7 +836,7 @@ static const RobinFuse kNoRobin = {nullptr, nullptr, nullptr, nullptr, 0, 0};
 static void sweeps(nrgpu_mg *M, MgLevel &L, int n, const int *done) {
   for (int s = 0; s < n; ++s) {
     jacobi_kernel<<<nblk(L.np + L.nb), RB, 0, M->stream>>>(L.u, L.u2, L.f, L.a, L.b, L.m, cxof(L), robin_of(L, 0),
-                                                           done);
+                                                           done, 1.0 / L.m, 1.0 / ((double)L.m * L.m));
     std::swap(L.u, L.u2);
   }
 }
