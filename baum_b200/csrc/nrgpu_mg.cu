@@ -140,6 +140,13 @@ __device__ __forceinline__ void cube_ijk(int q, int m, double rm, double rmm, in
   i = r - j * m;
 }
 
+// the same with the reciprocals formed here (1/m rounded, squared: the
+// margin above holds with that product's rounding too)
+__device__ __forceinline__ void cube_ijk(int q, int m, int &i, int &j, int &k) {
+  const double rm = 1.0 / m;
+  cube_ijk(q, m, rm, rm * rm, i, j, k);
+}
+
 // one Jacobi sweep un = uo + (f - L uo)/L_ii on inner points (Lpuncture_GS),
 // followed by the Robin condition on un (relax.c:19-43 then robin.c:146-223)
 __device__ __forceinline__ void jacobi_at(int t, const double *__restrict__ uo, double *__restrict__ un,
@@ -173,7 +180,8 @@ __global__ void damped_jacobi_kernel(const double *__restrict__ uo, double *__re
                                      const double *__restrict__ b, int m, double cx, double omega, RobinFuse R) {
   int q, slot;
   if (!fused_point(blockIdx.x * blockDim.x + threadIdx.x, m * m * m, R, q, slot)) return;
-  const int i = q % m, j = (q / m) % m, k = q / (m * m);
+  int i, j, k;
+  cube_ijk(q, m, i, j, k);
   if (!inner(i, j, k, m)) return;
   const double cc = -2.0 * (cx + cx + cx);
   const double aq = a[q], bq = b[q], uq = uo[q];
@@ -191,7 +199,8 @@ __global__ void residual_partial_kernel(const double *__restrict__ u, const doub
   const long np = (long)m * m * m;
   double s = 0.0;
   if (q < np) {
-    const int i = q % m, j = (q / m) % m, k = q / (m * m);
+    int i, j, k;
+    cube_ijk(q, m, i, j, k);
     if (inner(i, j, k, m)) {
       const double r = lop_point(u, q, m, -2.0 * (cx + cx + cx), cx, a[q], b[q]) - f[q];
       s = r * r;
@@ -242,7 +251,8 @@ __global__ void restrict_kernel(const double *__restrict__ fv, double *__restric
   if (done && *done) return;
   int q, slot;
   if (!fused_point(blockIdx.x * blockDim.x + threadIdx.x, mc * mc * mc, R, q, slot)) return;
-  const int I = q % mc, J = (q / mc) % mc, K = q / (mc * mc);
+  int I, J, K;
+  cube_ijk(q, mc, I, J, K);
   if (!inner(I, J, K, mc)) return;
   const long mf2 = (long)mf * mf;
   const long f0 = (long)(2 * I - off) + mf * (long)(2 * J - off) + mf2 * (long)(2 * K - off);
@@ -266,7 +276,8 @@ __device__ __forceinline__ void fine_to_coarse_at(int t, const double *__restric
                                                   int off, double cxh, const RobinFuse &R) {
   int q, slot;
   if (!fused_point(t, mc * mc * mc, R, q, slot)) return;
-  const int I = q % mc, J = (q / mc) % mc, K = q / (mc * mc);
+  int I, J, K;
+  cube_ijk(q, mc, I, J, K);
   if (!inner(I, J, K, mc)) return;
   const long mf2 = (long)mf * mf;
   const long f0 = (long)(2 * I - off) + mf * (long)(2 * J - off) + mf2 * (long)(2 * K - off);
@@ -297,7 +308,8 @@ __device__ __forceinline__ void coarse_rhs_at(int q, const double *__restrict__ 
                                               double cxH) {
   if (q >= mc * mc * mc) return;
   wH[q] = uH[q];
-  const int I = q % mc, J = (q / mc) % mc, K = q / (mc * mc);
+  int I, J, K;
+  cube_ijk(q, mc, I, J, K);
   if (!inner(I, J, K, mc)) return;
   const double luH = lop_point(uH, q, mc, -2.0 * (cxH + cxH + cxH), cxH, aH[q], bH[q]);
   fH[q] = fH[q] + (luH - RluH[q]);
@@ -320,7 +332,8 @@ __device__ __forceinline__ void sub_inner_at(int t, const double *__restrict__ x
                                              double *__restrict__ r, int m, const RobinFuse &R) {
   int q, slot;
   if (!fused_point(t, m * m * m, R, q, slot)) return;
-  const int i = q % m, j = (q / m) % m, k = q / (m * m);
+  int i, j, k;
+  cube_ijk(q, m, i, j, k);
   if (inner(i, j, k, m)) fused_store(r, q, slot, x[q] - y[q], R);
 }
 __global__ void sub_inner_kernel(const double *__restrict__ x, const double *__restrict__ y, double *__restrict__ r,
@@ -336,7 +349,8 @@ __device__ __forceinline__ void prolong_add_at(int q, const double *__restrict__
                                                int mf, int mc, double fx0, double fdx, double cx0, double cdx,
                                                int add) {
   if (q >= mf * mf * mf) return;
-  const int i = q % mf, j = (q / mf) % mf, k = q / (mf * mf);
+  int i, j, k;
+  cube_ijk(q, mf, i, j, k);
   if (!inner(i, j, k, mf)) return;
   const double xf = fx0 + i * fdx, yf = fx0 + j * fdx, zf = fx0 + k * fdx;
   const int ci = (int)((xf - cx0) / cdx), cj = (int)((yf - cx0) / cdx), ck = (int)((zf - cx0) / cdx);
