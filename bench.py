@@ -39,8 +39,8 @@ RHS_PER_STEP = 4
 FLOP_PER_POINT = 4973
 # DRAM bytes of one RK-stage launch of bssn_rhs_kernel on the 64^3 box, block 32 x 8 x 1
 # (dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture, mean of
-# the two captured launches, stages 1 and 2: 112.9 MB and 217.4 MB)
-RHS_TRAFFIC_BYTES = 165.2e6
+# the two captured launches, stages 1 and 2: 108.6 MB and 216.5 MB)
+RHS_TRAFFIC_BYTES = 162.6e6
 CONFIG = {"workload": "bssn_schwarzschild_64^3_rk4", "box": "66^3 (64^3 inner + boundary layer)",
           "dx": DX, "dt": DT, "order": 4, "dissipation": "KO6 eps=0.1", "gauge": "1+log, Gamma-driver eta=2",
           "l2": "flushed (256 MiB write) before every timed step", "parallelism": "replicas"}
