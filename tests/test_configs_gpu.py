@@ -4,7 +4,8 @@ The Z4c rhs kernel is compiled with fixed box strides for the boxes of the
 benchmarked grids (162^3: the precision-sweep box and level 0 of the batched
 refinement grid; 168^3, 136^3, 104^3, 72^3: its finer levels; 194^3 and
 136^3 at 6th order: the levels of the full form's grid, 72^3 at 6th order its
-moving puncture boxes).  Each instance is run here
+moving puncture boxes; 106^3 and 98^3: boxes of other sizes, staged into
+a copy with the strides of the next size).  Each instance is run here
 on a single box of its size through the C ABI and compared with the CPU
 oracle (1e-12 relative per variable, the bar of every rhs parity test): the
 precision-sweep box at its full size (160^3 inner points, 6th order) for
@@ -46,7 +47,7 @@ def shifted_binary(lev, sep):
 
 
 @pytest.mark.parametrize("m,order,steps", [(162, 6, 2), (162, 4, 1), (168, 4, 1), (136, 4, 1), (104, 4, 1),
-                                           (72, 6, 1), (136, 6, 1), (194, 6, 1)])
+                                           (72, 6, 1), (136, 6, 1), (194, 6, 1), (106, 6, 1), (98, 4, 1)])
 def test_fixed_stride_instance_matches_oracle(gpu, m, order, steps):
     dx = 24.0 / (m - 2)
     lev = abi.Level.single_box(m, dx)
